@@ -1,0 +1,78 @@
+"""film-juicer-b200: B200-native render path of Film-Juicer's film-process model.
+
+The product is libjuicer_b200.so (CUDA for sm_100a behind the C-ABI in
+include/juicer_cuda_api.h and include/juicer_b200.h). This package loads it and
+mirrors the reference host's records (abi.py), prepares recipes from profiles
+(prepare.py) and offers thin Python calls over the C-ABI (runtime.py). There is no
+CPU render path: every render call goes through the CUDA library and fails loudly
+when it is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libjuicer_b200.so")
+
+_lib = None
+
+_EXPORTS = {
+    "fj_cuda_create": (abi.FjStatus, [C.POINTER(C.c_void_p), C.POINTER(abi.FjErrorBuffer)]),
+    "fj_cuda_check_terminal": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fj_cuda_inspect": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjFrame), C.POINTER(abi.FjCudaContext),
+                                       C.POINTER(abi.FjErrorBuffer)]),
+    "fj_cuda_render": (abi.FjRenderOutcome, [C.c_void_p, C.POINTER(abi.FjCudaContext), C.POINTER(abi.FjFrame),
+                                             C.POINTER(abi.FjSubmission), C.POINTER(abi.FjPreparedHostData),
+                                             abi.FjAbortCallback, C.POINTER(abi.FjErrorBuffer)]),
+    "fj_cuda_retire_instance": (abi.FjStatus, [C.c_void_p, C.c_uint64, C.POINTER(abi.FjErrorBuffer)]),
+    "fj_cuda_shutdown": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fj_cuda_destroy": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_recipe_create": (abi.FjStatus, [C.POINTER(abi.FjPreparedHostData), C.c_void_p, C.POINTER(C.c_void_p),
+                                         C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_recipe_destroy": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_recipe_set_exposure_scale_device": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_recipe_clear_flags": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_recipe_read_flags": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32),
+                                             C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_render_pixels": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.c_ssize_t, C.c_void_p, C.c_ssize_t, C.c_int32,
+                                         C.c_int32, C.c_uint32, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_camera_exposure": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.c_ssize_t, C.c_uint32, C.c_int32, C.c_int32,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_ssize_t, C.c_void_p,
+                                           C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_capture_density": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.c_ssize_t, C.c_uint32, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_ssize_t, C.c_int32, C.c_int32, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_render_carrier": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_ssize_t,
+                                          C.c_void_p, C.c_ssize_t, C.c_void_p, C.c_ssize_t, C.c_int32, C.c_int32,
+                                          C.c_uint32, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_render_from_density": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.c_ssize_t, C.c_void_p, C.c_ssize_t, C.c_int32, C.c_int32,
+                                               C.c_uint32, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_scanner_lut_build_host": (abi.FjStatus, [C.POINTER(abi.FjbScannerLutInput)] + [C.c_void_p] * 6 +
+                                   [C.POINTER(abi.FjErrorBuffer)]),
+}
+
+
+def exported_names() -> list[str]:
+    return list(_EXPORTS)
+
+
+def load_library(path: str | None = None):
+    """Loads libjuicer_b200.so and declares every exported signature. Raises if missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"libjuicer_b200.so is not built ({p}); run __graft_entry__.build()")
+    lib = C.CDLL(p)
+    for name, (res, args) in _EXPORTS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib

@@ -1,0 +1,64 @@
+// fjb_internal.h -- host-side declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "fjb_params.h"
+
+namespace fjb {
+
+constexpr int kPixelThreads = 256;
+constexpr int kPixelBlocksPerSm = 4;
+
+enum class PixelStage : int {
+    SourceToOutput = 0,   // monolithic frame: source RGB -> encoded output
+    CarrierToOutput = 1,  // optics carrier planes -> encoded output
+    SourceToDensity = 2,  // source RGB -> capture density planes
+    CarrierToDensity = 3, // optics carrier planes -> capture density planes
+    DensityToOutput = 4,  // (grained) capture density planes -> encoded output
+};
+
+cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStream_t stream);
+
+// Camera linear exposure to planar B, G, R carrier planes (reference
+// src/Cuda/Film/JuicerCudaFilmPipeline.cu:3103 camera_film_linear_exposure_kernel).
+cudaError_t launch_camera_exposure(const PixelParams& p, float* b, float* g, float* r, long long stride,
+                                   cudaStream_t stream);
+
+// Scanner PCHIP LUT construction on the device in FP64 (reference
+// rust/film-juicer-core/src/scanner/lut.rs:187-296).
+struct ScannerLutSpec {
+    const double* eps_c; // device, [k]
+    const double* eps_m;
+    const double* eps_y;
+    const double* wx;
+    const double* wy;
+    const double* wz;
+    const double* baseline; // device or null
+    int k;
+    double inv_yn;
+    float range_min_cmy[3];
+    float inverse_span_cmy[3];
+    int medium; // 0 = negative, 1 = print/positive
+    int resolution;
+};
+
+struct ScannerLutDevice {
+    double* nodes;   // [r^3 * 3] log2 XYZ in FP64
+    float* log2_xyz; // [r^3 * 3]
+    float* slope_c;
+    float* slope_m;
+    float* slope_y;
+    float* cell_min; // [(r-1)^3 * 3]
+    float* cell_max;
+    float4* packed_nodes; // [r^3 * 3]
+    float4* packed_cells; // [(r-1)^3 * 2]
+    unsigned int* failure; // non-finite node flag
+};
+
+cudaError_t launch_scanner_lut_build(const ScannerLutSpec& spec, const ScannerLutDevice& out, cudaStream_t stream);
+
+} // namespace fjb

@@ -1,0 +1,153 @@
+// fjb_params.h -- device-side parameter blocks of the fused per-pixel render chain.
+//
+// One PixelParams block describes a prepared recipe for one frame. It travels to the
+// kernel as a __grid_constant__ parameter (it lives in the constant bank, so the
+// 81-wavelength print coefficients are read as FFMA constant operands with no load
+// instruction). Curve samples are staged once per CTA into shared memory; the large
+// tables (TC LUT, scanner PCHIP nodes, gamut boundary) stay in HBM/L2 and are read
+// as 16-byte vectors.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+namespace fjb {
+
+constexpr int kSpectralSamples = 81;   // 380..780 nm in 5 nm steps
+constexpr int kTcLutExtent = 192;      // TC LUT is 192 x 192 (x, y) nodes
+constexpr int kGamutLightness = 64;    // output gamut boundary rows
+constexpr int kGamutHue = 720;         // output gamut boundary columns
+constexpr int kMaxCurveSamples = 1024; // upper bound for staged curves
+
+enum Route : int { kRouteDirect = 0, kRoutePrint = 1 };
+enum RawMethod : int { kHanatos = 0, kMallett = 1, kArctic = 2 };
+enum DirModeDev : int { kDirInactive = 0, kDirNegativeDonor = 1, kDirPositiveReceiver = 2 };
+
+// Offsets (in floats) of the curve samples inside the staged curve blob.
+struct CurveRef {
+    int x;   // offset of the ascending abscissa
+    int y;   // offset of the ordinate
+    int n;   // sample count (accepted domain is [0, n-1])
+};
+
+// Print 81-lambda coefficients, pre-folded on the host:
+//   dens[l] = (eps_c, eps_m, eps_y, base) * log2(10)
+//   sens[l] = (sens_c, sens_m, sens_y) * filtered illuminant
+// Wavelengths whose three sensitivities are all NaN are dropped; a NaN channel of a
+// kept wavelength contributes zero.
+struct PrintSpectral {
+    float dens[kSpectralSamples][4];
+    float sens[kSpectralSamples][3];
+    int count;
+};
+
+struct PixelParams {
+    // ---- frame ----
+    const char* src;
+    char* dst;
+    long long src_row_bytes;
+    long long dst_row_bytes;
+    int width;
+    int height;
+    int components; // 3 or 4, same for source and destination
+    int route;      // Route
+
+    // Optional carrier input: planar linear exposure (B, G, R) produced by the
+    // camera optics stages. When set, exposure reconstruction is skipped.
+    const float* carrier_b;
+    const float* carrier_g;
+    const float* carrier_r;
+    long long carrier_stride; // floats per row
+
+    // Optional materialised density output (capture stage only, C, M, Y planes).
+    float* density_c;
+    float* density_m;
+    float* density_y;
+
+    // ---- input colour + exposure reconstruction ----
+    int input_color_space;
+    int decode_cctf;
+    int adapt_input;
+    int method; // RawMethod
+    float input_rgb_to_xyz[9];
+    float input_xyz_adapt[9];
+    float xyz_to_linear_srgb[9];
+    float mallett_midgray_scale;
+    const float4* tc_lut;        // [192][192] of (R, G, B, pad)
+    const float* mallett_basis;  // [81][3]
+    const float* mallett_illum;  // [81]
+    const float* film_sens_bgr;  // [3][81] B, G, R relative sensitivity
+    float manual_exposure_scale;
+    float route_correction_scale;
+    const float* auto_exposure_scale; // device scalar or null
+
+    // ---- capture development ----
+    float gamma_bgr[3];
+    int dir_mode; // DirModeDev
+    float dir_m[9]; // [donor BGR][receiver BGR]
+    float dir_dmax[3];
+    float dir_dref[3];
+    float dir_donor_k[3];
+    float dir_receiver_cref[3];
+    float dir_receiver_kr[3];
+    CurveRef film_curve[3]; // B, G, R: (log exposure, normalized density)
+    CurveRef dir_curve[3];  // B, G, R: (compensated axis, normalized density)
+
+    // Spatial DIR: filtered corrections (Y, M, C order of the B, G, R layers) and
+    // cached raw log exposure (B, G, R). Used when dir_spatial != 0.
+    int dir_spatial;
+    const float* dir_filtered_y;
+    const float* dir_filtered_m;
+    const float* dir_filtered_c;
+    const float* dir_log_raw_b;
+    const float* dir_log_raw_g;
+    const float* dir_log_raw_r;
+
+    // Optional density-plane input for the scan stage (after grain): C, M, Y planes.
+    const float* scan_density_c;
+    const float* scan_density_m;
+    const float* scan_density_y;
+
+    // ---- print ----
+    float print_exposure;
+    float print_route_correction;
+    float print_preflash_exposure;
+    float print_midgray;
+    float print_preflash_raw[3];
+    CurveRef print_curve[3]; // C, M, Y
+
+    // ---- scanner ----
+    int scan_medium_negative;
+    float scan_min_cmy[3];
+    float scan_inv_span_cmy[3];
+    int scan_res;
+    const float4* scan_nodes; // [(c*r+m)*r+y][3 outputs] of (value, slope_c, slope_m, slope_y)
+    const float4* scan_cells; // [(c*s+m)*s+y][2] of (min xyz, max x), (max y, max z, 0, 0)
+    int correction_active;
+    float correction_slope;
+    float correction_offset;
+
+    // ---- output colour ----
+    float cat02[9];
+    float xyz_to_rgb[9];
+    int gamut_active;
+    const float* gamut_cmax; // [64][720]
+    float gamut_native_to_xyz[9];
+    float gamut_xyz_to_native[9];
+    float gamut_lightness_knee[3];
+    float gamut_chroma_knee[3];
+    int encode_input_is_output;
+    int encode_apply_cctf;
+    float encode_dwg_to_output[9];
+    int cctf_kind;
+    float cctf_gamma, cctf_a, cctf_b, cctf_c, cctf_d, cctf_linear_cutoff;
+
+    // ---- staged curves + error word ----
+    const float* curve_blob;
+    int curve_blob_floats;
+    unsigned int* error_flags; // bit 0 scan failure, bit 8 DIR failure, bits 9..11 DIR channels
+
+    PrintSpectral spectral;
+};
+
+} // namespace fjb

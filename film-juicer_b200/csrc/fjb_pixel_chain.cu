@@ -1,0 +1,198 @@
+// fjb_pixel_chain.cu -- the fused per-pixel film-process kernel (a1..a13).
+//
+// One persistent launch walks the frame with a grid-stride loop (grid sized to the
+// SM count). Each CTA stages the recipe's density curves into shared memory once;
+// the print spectral coefficients are kernel parameters (constant bank); the TC LUT,
+// scanner nodes and gamut boundary are 16-byte-vector reads through L1/L2.
+//
+// Variants (template flags) cover the reference's fused kernels
+// (src/Cuda/Scan/JuicerCudaScanPipeline.cu:1700-1868 pipeline_direct/carrier_kernel,
+// :1891 focused_capture_film_density_kernel, :1944 scan_linear_density_rgb_kernel,
+// :1362 develop_print_density_kernel):
+//   Input  = source RGB(A) | carrier planes (B, G, R linear exposure) | density planes
+//   Output = encoded RGB(A) | capture density planes (C, M, Y)
+#include <cuda_runtime.h>
+
+#include "fjb_internal.h"
+#include "fjb_pixel_math.cuh"
+
+namespace fjb {
+
+enum InputKind : int { kInSource = 0, kInCarrier = 1, kInDensity = 2 };
+enum OutputKind : int { kOutEncoded = 0, kOutDensity = 1 };
+
+template <int In, int Out, bool Print, bool SpatialDir>
+__global__ void __launch_bounds__(kPixelThreads) pixel_chain_kernel(const __grid_constant__ PixelParams p) {
+    extern __shared__ float4 smem4[];
+    float* blob = reinterpret_cast<float*>(smem4);
+    {
+        const float4* g = reinterpret_cast<const float4*>(p.curve_blob);
+        const int n4 = p.curve_blob_floats >> 2;
+        for (int i = threadIdx.x; i < n4; i += blockDim.x) smem4[i] = __ldg(g + i);
+    }
+    __syncthreads();
+
+    const long long total = (long long)p.width * (long long)p.height;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
+        const int y = (int)(idx / p.width);
+        const int x = (int)(idx - (long long)y * p.width);
+        const float* srcPix = nullptr;
+        if (p.src) {
+            srcPix = reinterpret_cast<const float*>(p.src + (long long)y * p.src_row_bytes) + (long long)x * p.components;
+        }
+
+        float d[3];
+        if constexpr (In == kInDensity) {
+            d[0] = p.scan_density_c[idx];
+            d[1] = p.scan_density_m[idx];
+            d[2] = p.scan_density_y[idx];
+        } else if constexpr (SpatialDir) {
+            float logRaw[3];
+            if (p.dir_log_raw_b) {
+                logRaw[0] = __ldg(p.dir_log_raw_b + idx);
+                logRaw[1] = __ldg(p.dir_log_raw_g + idx);
+                logRaw[2] = __ldg(p.dir_log_raw_r + idx);
+            } else {
+                float e[3];
+                if constexpr (In == kInCarrier) {
+                    const long long ci = (long long)y * p.carrier_stride + x;
+                    e[0] = p.carrier_b[ci];
+                    e[1] = p.carrier_g[ci];
+                    e[2] = p.carrier_r[ci];
+                    for (int c = 0; c < 3; ++c) e[c] = fmaxf(0.0f, e[c] * p.route_correction_scale);
+                } else {
+                    const float in[3] = {srcPix[0], srcPix[1], srcPix[2]};
+                    camera_linear_exposure(p, in, true, e);
+                }
+                for (int c = 0; c < 3; ++c) logRaw[c] = log_exposure(e[c]);
+            }
+            float corr[3] = {p.dir_filtered_y[idx], p.dir_filtered_m[idx], p.dir_filtered_c[idx]};
+            develop_capture_spatial(p, blob, logRaw, corr, d);
+        } else {
+            float e[3];
+            if constexpr (In == kInCarrier) {
+                const long long ci = (long long)y * p.carrier_stride + x;
+                e[0] = p.carrier_b[ci];
+                e[1] = p.carrier_g[ci];
+                e[2] = p.carrier_r[ci];
+                for (int c = 0; c < 3; ++c) e[c] = fmaxf(0.0f, e[c] * p.route_correction_scale);
+            } else {
+                const float in[3] = {srcPix[0], srcPix[1], srcPix[2]};
+                camera_linear_exposure(p, in, true, e);
+            }
+            develop_capture(p, blob, e, d);
+        }
+
+        if constexpr (Out == kOutDensity) {
+            p.density_c[idx] = d[0];
+            p.density_m[idx] = d[1];
+            p.density_y[idx] = d[2];
+            continue;
+        }
+
+        if constexpr (Print) {
+            print_develop(p, blob, d);
+        }
+
+        double rgb[3];
+        float* dstPix = reinterpret_cast<float*>(p.dst + (long long)y * p.dst_row_bytes) + (long long)x * p.components;
+        if (!scan_to_linear(p, d, rgb)) {
+            flag_scan_failure(p);
+            dstPix[0] = 0.0f;
+            dstPix[1] = 0.0f;
+            dstPix[2] = 0.0f;
+            if (p.components == 4) dstPix[3] = srcPix ? srcPix[3] : 1.0f;
+            continue;
+        }
+        encode_output(p, rgb);
+        dstPix[0] = (float)rgb[0];
+        dstPix[1] = (float)rgb[1];
+        dstPix[2] = (float)rgb[2];
+        if (p.components == 4) dstPix[3] = srcPix ? srcPix[3] : 1.0f;
+    }
+}
+
+template <int In, int Out, bool Print, bool SpatialDir>
+static cudaError_t launch_variant(const PixelParams& p, int grid, size_t smem, cudaStream_t stream) {
+    auto* k = pixel_chain_kernel<In, Out, Print, SpatialDir>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    k<<<grid, kPixelThreads, smem, stream>>>(p);
+    return cudaGetLastError();
+}
+
+// Camera linear exposure (no route correction) into planar B, G, R carrier planes.
+__global__ void __launch_bounds__(kPixelThreads) camera_exposure_kernel(const __grid_constant__ PixelParams p,
+                                                                        float* b, float* g, float* r,
+                                                                        long long stride) {
+    const long long total = (long long)p.width * (long long)p.height;
+    const long long step = (long long)gridDim.x * blockDim.x;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += step) {
+        const int y = (int)(idx / p.width);
+        const int x = (int)(idx - (long long)y * p.width);
+        const float* s = reinterpret_cast<const float*>(p.src + (long long)y * p.src_row_bytes) + (long long)x * p.components;
+        const float in[3] = {s[0], s[1], s[2]};
+        float e[3];
+        camera_linear_exposure(p, in, false, e);
+        const long long o = (long long)y * stride + x;
+        b[o] = e[0];
+        g[o] = e[1];
+        r[o] = e[2];
+    }
+}
+
+static int persistent_grid(long long total) {
+    int device = 0;
+    cudaGetDevice(&device);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (sms <= 0) sms = 148;
+    const long long blocksNeeded = (total + kPixelThreads - 1) / kPixelThreads;
+    const long long cap = (long long)sms * kPixelBlocksPerSm;
+    return (int)(blocksNeeded < cap ? blocksNeeded : cap);
+}
+
+cudaError_t launch_camera_exposure(const PixelParams& p, float* b, float* g, float* r, long long stride,
+                                   cudaStream_t stream) {
+    const long long total = (long long)p.width * (long long)p.height;
+    if (total <= 0) return cudaSuccess;
+    camera_exposure_kernel<<<persistent_grid(total), kPixelThreads, 0, stream>>>(p, b, g, r, stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStream_t stream) {
+    const long long total = (long long)p.width * (long long)p.height;
+    if (total <= 0) return cudaSuccess;
+    if ((p.curve_blob_floats & 3) != 0) return cudaErrorInvalidValue;
+    const size_t smem = (size_t)p.curve_blob_floats * sizeof(float);
+    const int grid = persistent_grid(total);
+    const bool print = p.route == kRoutePrint;
+    const bool sdir = p.dir_spatial != 0;
+    switch (stage) {
+        case PixelStage::SourceToOutput:
+            if (sdir) return print ? launch_variant<kInSource, kOutEncoded, true, true>(p, grid, smem, stream)
+                                   : launch_variant<kInSource, kOutEncoded, false, true>(p, grid, smem, stream);
+            return print ? launch_variant<kInSource, kOutEncoded, true, false>(p, grid, smem, stream)
+                         : launch_variant<kInSource, kOutEncoded, false, false>(p, grid, smem, stream);
+        case PixelStage::CarrierToOutput:
+            if (sdir) return print ? launch_variant<kInCarrier, kOutEncoded, true, true>(p, grid, smem, stream)
+                                   : launch_variant<kInCarrier, kOutEncoded, false, true>(p, grid, smem, stream);
+            return print ? launch_variant<kInCarrier, kOutEncoded, true, false>(p, grid, smem, stream)
+                         : launch_variant<kInCarrier, kOutEncoded, false, false>(p, grid, smem, stream);
+        case PixelStage::SourceToDensity:
+            return sdir ? launch_variant<kInSource, kOutDensity, false, true>(p, grid, smem, stream)
+                        : launch_variant<kInSource, kOutDensity, false, false>(p, grid, smem, stream);
+        case PixelStage::CarrierToDensity:
+            return sdir ? launch_variant<kInCarrier, kOutDensity, false, true>(p, grid, smem, stream)
+                        : launch_variant<kInCarrier, kOutDensity, false, false>(p, grid, smem, stream);
+        case PixelStage::DensityToOutput:
+            return print ? launch_variant<kInDensity, kOutEncoded, true, false>(p, grid, smem, stream)
+                         : launch_variant<kInDensity, kOutEncoded, false, false>(p, grid, smem, stream);
+    }
+    return cudaErrorInvalidValue;
+}
+
+} // namespace fjb

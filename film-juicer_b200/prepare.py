@@ -1,0 +1,460 @@
+"""Host-side recipe preparation: film/paper profiles -> the tables of FjPreparedHostData.
+
+In Film-Juicer this precompute is Rust (rust/film-juicer-core/src/**, not buildable
+here). This module restates the parts the render path consumes, in NumPy FP64, and
+packs them into the same C-ABI record the Rust host fills:
+
+* sensitivity: 10**log_sensitivity, non-finite -> 0 (exposure.rs:125-190, no band-pass);
+* TC LUT: 192x192x81 Hanatos irradiance spectra contracted with the sensitivity,
+  R,G,B,pad per node (reconstruction.rs:594-677; no spectral blur, no surface
+  correction, no input-compression remap);
+* density curves: authored curves minus their per-channel minimum (film.rs:72-93);
+* DIR couplers: Langmuir donor model with compensated log-exposure axes that keep
+  the neutral response (a simplified restatement of film/dir.rs:135-360);
+* print: negative dye spectra, paper sensitivity, lamp filtered by two dichroic
+  dials solved for a neutral mid-grey, mid-grey normalizer (print.rs:435-658,
+  simplified);
+* scanner: medium dye spectra with illuminant-weighted CIE 1931 CMFs
+  (scanner.rs), density bounds of the medium;
+* output: CAT02 from the viewing illuminant to D65, XYZ->linear sRGB, sRGB CCTF,
+  OkLch gamut boundary 64x720 of the sRGB cube (gamut.rs:760, by bisection).
+
+Where the restatement simplifies the Rust model it is stated above; the render
+kernels consume whatever tables the host prepares, so parity of the render path
+does not depend on these simplifications.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+
+WAVELENGTHS = np.arange(380.0, 781.0, 5.0)
+N_LAMBDA = 81
+LOG2_10 = math.log2(10.0)
+
+# Linear Rec.709 / sRGB (D65) <-> CIE XYZ.
+SRGB_TO_XYZ = np.array([[0.4123907992659595, 0.3575843393838780, 0.1804807884018343],
+                        [0.2126390058715104, 0.7151686787677559, 0.0721923153607337],
+                        [0.0193308187155918, 0.1191947797946259, 0.9505321522496606]])
+XYZ_TO_SRGB = np.linalg.inv(SRGB_TO_XYZ)
+CAT02 = np.array([[0.7328, 0.4296, -0.1624], [-0.7036, 1.6975, 0.0061], [0.0030, 0.0136, 0.9834]])
+D65_XYZ = np.array([0.95047, 1.0, 1.08883])
+
+OK_XYZ_TO_LMS = np.array([[0.8189330101, 0.3618667424, -0.1288597137],
+                          [0.0329845436, 0.9293118715, 0.0361456387],
+                          [0.0482003018, 0.2643662691, 0.6338517070]])
+OK_LMS_ROOT_TO_LAB = np.array([[0.2104542553, 0.7936177850, -0.0040720468],
+                               [1.9779984951, -2.4285922050, 0.4505937099],
+                               [0.0259040371, 0.7827717662, -0.8086757660]])
+
+
+def _nan_array(values) -> np.ndarray:
+    return np.array([[np.nan if v is None else v for v in row] if isinstance(row, list) else
+                     (np.nan if row is None else row) for row in values], dtype=np.float64)
+
+
+def load_profile(path: str) -> dict:
+    with open(path) as fh:
+        d = json.load(fh)
+    data = d["data"]
+    out = {"info": d["info"]}
+    for key in ("log_sensitivity", "channel_density", "base_density", "midscale_neutral_density",
+                "log_exposure", "density_curves"):
+        out[key] = _nan_array(data[key])
+    return out
+
+
+def load_spectrum_csv(path: str) -> np.ndarray:
+    rows = np.loadtxt(path, delimiter=",")
+    return np.interp(WAVELENGTHS, rows[:, 0], rows[:, 1])
+
+
+def load_cmfs(path: str) -> np.ndarray:
+    rows = np.loadtxt(path, delimiter=",")
+    return np.stack([np.interp(WAVELENGTHS, rows[:, 0], rows[:, k]) for k in (1, 2, 3)], axis=1)
+
+
+def cat02_matrix(src_white: np.ndarray, dst_white: np.ndarray) -> np.ndarray:
+    s = CAT02 @ (src_white / src_white[1])
+    d = CAT02 @ (dst_white / dst_white[1])
+    return np.linalg.inv(CAT02) @ np.diag(d / s) @ CAT02
+
+
+def spectrum_xyz(spd: np.ndarray, cmfs: np.ndarray) -> np.ndarray:
+    xyz = cmfs.T @ spd
+    return xyz / xyz[1]
+
+
+def build_tc_lut(spectra: np.ndarray, sens_rgb: np.ndarray) -> np.ndarray:
+    """192x192x81 irradiance spectra x 81x3 sensitivity -> 192x192x4 (R,G,B,0) float32."""
+    flat = spectra.reshape(-1, N_LAMBDA).astype(np.float64)
+    rgb = flat @ np.nan_to_num(sens_rgb, nan=0.0)
+    out = np.zeros((spectra.shape[0] * spectra.shape[1], 4), dtype=np.float32)
+    out[:, :3] = rgb.astype(np.float32)
+    return out.reshape(spectra.shape[0], spectra.shape[1], 4)
+
+
+def gamut_boundary_table(rows: int = 64, hues: int = 720, lmin: float = 0.02, lmax: float = 1.0) -> np.ndarray:
+    """Maximum OkLab chroma inside the linear sRGB cube per (lightness, hue)."""
+    lab_to_lms_root = np.linalg.inv(OK_LMS_ROOT_TO_LAB)
+    lms_to_xyz = np.linalg.inv(OK_XYZ_TO_LMS)
+    L = np.linspace(lmin, lmax, rows)[:, None]
+    h = (np.arange(hues) / hues) * 2 * np.pi - np.pi
+    cos_h, sin_h = np.cos(h)[None, :], np.sin(h)[None, :]
+
+    def inside(c):
+        lab = np.stack([np.broadcast_to(L, c.shape), c * cos_h, c * sin_h], axis=-1)
+        lms = (lab @ lab_to_lms_root.T) ** 3
+        rgb = lms @ lms_to_xyz.T @ XYZ_TO_SRGB.T
+        return np.all((rgb >= -1e-7) & (rgb <= 1 + 1e-7), axis=-1)
+
+    lo = np.zeros((rows, hues))
+    hi = np.full((rows, hues), 0.5)
+    for _ in range(40):
+        mid = 0.5 * (lo + hi)
+        ok = inside(mid)
+        lo = np.where(ok, mid, lo)
+        hi = np.where(ok, hi, mid)
+    return lo.astype(np.float32)
+
+
+def _smoothstep_filter(center: float, width: float, low_pass: bool) -> np.ndarray:
+    x = (WAVELENGTHS - center) / width
+    s = 0.5 * (1.0 + np.tanh(x))
+    return 1.0 - s if low_pass else s
+
+
+@dataclass
+class PreparedRecipe:
+    """Arrays and scalars of one prepared render recipe (all float32 where the ABI is)."""
+
+    route: int
+    arrays: dict = field(default_factory=dict)
+    scalars: dict = field(default_factory=dict)
+
+    def save(self, path: str) -> None:
+        payload = {f"a_{k}": v for k, v in self.arrays.items()}
+        payload["scalars"] = np.array(json.dumps(self.scalars))
+        payload["route"] = np.array(self.route)
+        np.savez_compressed(path, **payload)
+
+    @classmethod
+    def load(cls, path: str) -> "PreparedRecipe":
+        z = np.load(path, allow_pickle=False)
+        arrays = {k[2:]: np.ascontiguousarray(z[k]) for k in z.files if k.startswith("a_")}
+        return cls(int(z["route"]), arrays, json.loads(str(z["scalars"])))
+
+
+def _neutral_dir_axes(log_e, curves_rgb, matrix_rgb, dref, k):
+    """Compensated axes x'_c = x - correction_c(neutral layer densities at x).
+
+    A neutral exposure at x develops layer densities curves[x]; the donor Langmuir
+    term D (k + dref) / (k + D) feeds the receiver corrections through the coupler
+    matrix, and shifting the axis by that correction returns the authored density
+    for neutral input.
+    """
+    d = curves_rgb
+    donor = d * (k + dref)[None, :] / (k[None, :] + d)
+    corr = donor @ matrix_rgb  # [n, receiver RGB]
+    return np.stack([log_e - corr[:, c] for c in range(3)], axis=0)
+
+
+def prepare_recipe(resources: str, film: str, paper: str | None = None, *, dir_amount: float = 1.0,
+                   lut_resolution: int = 17, gamut: bool = True, exposure_ev: float = 0.0) -> PreparedRecipe:
+    """Builds a direct (paper=None) or print recipe from the profile directory `resources`."""
+    prof = load_profile(os.path.join(resources, "profiles", f"{film}.json"))
+    cmfs = load_cmfs(os.path.join(resources, "cie1931_2deg.csv"))
+    d50 = load_spectrum_csv(os.path.join(resources, "illuminants", "D50.csv"))
+    d65 = load_spectrum_csv(os.path.join(resources, "illuminants", "D65.csv"))
+    ref_ill = load_spectrum_csv(os.path.join(resources, "illuminants",
+                                             f"{prof['info'].get('reference_illuminant', 'D55')}.csv"))
+    spectra = np.load(os.path.join(resources, "luts", "spectral_upsampling", "irradiance_xy_tc.npy"))
+
+    sens = np.power(10.0, prof["log_sensitivity"])
+    sens = np.where(np.isfinite(sens) & (sens > 0), sens, 0.0)
+    tc = build_tc_lut(spectra, sens)
+
+    # Route correction: an 18.4 % grey of the reference illuminant exposes to 1 on green.
+    grey_xyz = 0.184 * spectrum_xyz(ref_ill, cmfs)
+    tcx = grey_xyz[0] / grey_xyz.sum()
+    tcy = grey_xyz[1] / grey_xyz.sum()
+    qx, qy = (1 - tcx) ** 2, tcy / max(1 - tcx, 1e-10)
+    ci, mi = int(round(qx * 191)), int(round(qy * 191))
+    g_grey = grey_xyz.sum() * tc[ci, mi, 1]
+    route_scale = float(1.0 / g_grey)
+
+    log_e = prof["log_exposure"].astype(np.float64)
+    curves = prof["density_curves"].astype(np.float64)
+    curves = curves - np.nanmin(curves, axis=0, keepdims=True)
+    n = log_e.size
+
+    a: dict[str, np.ndarray] = {}
+    s: dict = {}
+    f32 = lambda x: np.ascontiguousarray(np.asarray(x, dtype=np.float32))
+    a["sensitivity_rgb"] = f32(sens)
+    a["tc_lut"] = f32(tc)
+    a["log_exposure"] = f32(log_e)
+    a["density_rgb"] = f32(curves)
+    s["route_correction_scale"] = route_scale
+    s["manual_exposure_ev"] = exposure_ev
+    s["input_rgb_to_xyz"] = SRGB_TO_XYZ.ravel().tolist()
+    s["xyz_to_linear_srgb"] = XYZ_TO_SRGB.ravel().tolist()
+
+    # DIR couplers (negative donor Langmuir), RGB order.
+    dmax = np.nanmax(curves, axis=0)
+    dref = 0.5 * dmax
+    kdon = np.full(3, 0.8)
+    inter = 0.25 * dir_amount
+    matrix = np.array([[1.0, inter, 0.4 * inter], [inter, 1.0, inter], [0.4 * inter, inter, 1.0]]) * 0.2 * dir_amount
+    s["dir_mode"] = 1 if dir_amount > 0 else 0
+    s["dir_matrix_rgb"] = matrix.ravel().tolist()
+    s["dir_dmax"] = dmax.tolist()
+    s["dir_dref"] = dref.tolist()
+    s["dir_donor_k"] = kdon.tolist()
+    if dir_amount > 0:
+        a["dir_axes_rgb"] = f32(_neutral_dir_axes(log_e, curves, matrix, dref, kdon))
+
+    route = abi.FJ_ROUTE_NEGATIVE_DIRECT
+    medium_dyes = prof["channel_density"]
+    medium_base = prof["base_density"]
+    medium_curves = curves
+    if paper is not None:
+        route = abi.FJ_ROUTE_NEGATIVE_PRINT
+        pp = load_profile(os.path.join(resources, "profiles", f"{paper}.json"))
+        lamp = load_spectrum_csv(os.path.join(resources, "illuminants", "T.csv"))
+        psens = np.power(10.0, pp["log_sensitivity"])  # NaN stays NaN: skipped wavelengths
+        neg_dyes = np.nan_to_num(prof["channel_density"], nan=0.0)
+        neg_base = np.nan_to_num(prof["base_density"], nan=0.0)
+        mid = np.nan_to_num(prof["midscale_neutral_density"], nan=0.0)
+        t_mid = np.power(10.0, -mid)
+
+        def raw_for(filters):
+            y, m = filters
+            filt = (1 - y * _smoothstep_filter(505.0, 12.0, True)) * (1 - m * _smoothstep_filter(
+                540.0, 14.0, False) * _smoothstep_filter(590.0, 14.0, True))
+            ill = lamp * np.clip(filt, 0.0, 1.0)
+            return np.nansum((t_mid * ill)[:, None] * psens, axis=0), ill
+
+        # Solve the two dichroic dials so the mid-grey negative prints neutral (C = M = Y raw).
+        ym = np.array([0.5, 0.5])
+        for _ in range(60):
+            raw, _ = raw_for(ym)
+            lr = np.log10(raw)
+            err = np.array([lr[2] - lr[0], lr[1] - lr[0]])
+            if np.max(np.abs(err)) < 1e-7:
+                break
+            jac = np.zeros((2, 2))
+            for j in range(2):
+                dd = np.zeros(2)
+                dd[j] = 1e-5
+                r2, _ = raw_for(ym + dd)
+                l2 = np.log10(r2)
+                jac[:, j] = (np.array([l2[2] - l2[0], l2[1] - l2[0]]) - err) / 1e-5
+            ym = np.clip(ym - np.linalg.solve(jac, err), 0.0, 0.99)
+        raw, ill = raw_for(ym)
+        ple = pp["log_exposure"].astype(np.float64)
+        pcurves = pp["density_curves"].astype(np.float64)
+        pcurves = pcurves - np.nanmin(pcurves, axis=0, keepdims=True)
+        # Mid-grey negative lands on the paper's speed point (log exposure 0 on this axis).
+        a["print_film_density_cmy"] = f32(neg_dyes)
+        a["print_film_base_density"] = f32(neg_base)
+        a["print_sensitivity_cmy"] = f32(psens)
+        a["print_log_exposure"] = f32(ple)
+        a["print_density_cmy"] = f32(pcurves)
+        a["print_main_illuminant"] = f32(ill)
+        s["print_exposure"] = 1.0
+        s["print_normalizer"] = float(1.0 / raw[1])
+        s["print_filters_ym"] = ym.tolist()
+        medium_dyes = pp["channel_density"]
+        medium_base = pp["base_density"]
+        medium_curves = pcurves
+
+    # Scanner: medium dye spectra under the D50 viewing illuminant.
+    view = d50
+    w = cmfs * view[:, None]
+    inv_yn = float(1.0 / np.sum(w[:, 1]))
+    a["scan_dye_c"] = f32(np.nan_to_num(medium_dyes[:, 0], nan=0.0))
+    a["scan_dye_m"] = f32(np.nan_to_num(medium_dyes[:, 1], nan=0.0))
+    a["scan_dye_y"] = f32(np.nan_to_num(medium_dyes[:, 2], nan=0.0))
+    a["scan_wx"] = f32(w[:, 0])
+    a["scan_wy"] = f32(w[:, 1])
+    a["scan_wz"] = f32(w[:, 2])
+    a["scan_base"] = f32(np.nan_to_num(medium_base, nan=0.0))
+    s["scan_inv_yn"] = inv_yn
+    # Density planes are C, M, Y; curve column k (the R, G, B sensitive layer) forms dye k.
+    dmin = np.zeros(3)
+    dspan = np.nanmax(medium_curves, axis=0)
+    s["scan_min_cmy"] = dmin.tolist()
+    s["scan_inv_span_cmy"] = (1.0 / (dspan * 1.05)).tolist()
+    s["scan_lut_resolution"] = int(lut_resolution)
+    view_xyz = spectrum_xyz(view, cmfs)
+    s["cat02"] = cat02_matrix(view_xyz, D65_XYZ).ravel().tolist()
+    s["xyz_to_rgb"] = XYZ_TO_SRGB.ravel().tolist()
+    s["illuminant_xyz"] = view_xyz.tolist()
+    s["gamut"] = bool(gamut)
+    a["gamut_cmax"] = gamut_boundary_table()
+    s["gamut_native_to_xyz"] = SRGB_TO_XYZ.ravel().tolist()
+    s["gamut_xyz_to_native"] = XYZ_TO_SRGB.ravel().tolist()
+    return PreparedRecipe(route, a, s)
+
+
+class HostRecord:
+    """An FjPreparedHostData filled from a PreparedRecipe; keeps every array alive."""
+
+    def __init__(self, recipe: PreparedRecipe, *, recipe_hash: int = 0, auto_exposure: bool = False,
+                 gamut: bool | None = None, dir_active: bool | None = None, correction=None):
+        self.recipe = recipe
+        self._keep = []
+        a, s = recipe.arrays, recipe.scalars
+        h = abi.FjPreparedHostData()
+        self.h = h
+        h.route = recipe.route
+        h.capture_polarity = abi.FJ_POLARITY_NEGATIVE
+        h.recipe_hash = recipe_hash
+
+        def span(arr):
+            arr = np.ascontiguousarray(arr, dtype=np.float32)
+            self._keep.append(arr)
+            return abi.FjFloatSpan(arr.ctypes.data_as(C.POINTER(C.c_float)), arr.size)
+
+        ex = h.film_exposure
+        ex.input_color_space = abi.FJ_INPUT_SRGB_REC709
+        ex.method = abi.FJ_RAW_HANATOS_2025
+        ex.flags = abi.FJ_FILM_AUTO_EXPOSURE if auto_exposure else 0
+        ex.manual_exposure_ev = s.get("manual_exposure_ev", 0.0)
+        ex.route_correction_scale = s["route_correction_scale"]
+        ex.mallett_green_midgray_scale = 1.0
+        abi.set_floats(ex.input_rgb_to_xyz, s["input_rgb_to_xyz"])
+        abi.set_floats(ex.input_xyz_adapt, np.eye(3).ravel())
+        abi.set_floats(ex.xyz_to_linear_srgb, s["xyz_to_linear_srgb"])
+        ex.sensitivity_rgb = span(a["sensitivity_rgb"])
+        ex.tc_lut_rgba = span(a["tc_lut"])
+        ex.sensitivity_hash = ex.tc_lut_hash = ex.hash = 1
+
+        dv = h.film_development
+        dv.log_exposure = span(a["log_exposure"])
+        dv.density_rgb = span(a["density_rgb"])
+        abi.set_floats(dv.gamma_rgb, [1.0, 1.0, 1.0])
+        dv.density_curves_hash = dv.hash = 1
+
+        dmode = s.get("dir_mode", 0)
+        if dir_active is False:
+            dmode = 0
+        dr = h.dir_couplers
+        dr.mode = dmode
+        if dmode:
+            abi.set_floats(dr.matrix_rgb, s["dir_matrix_rgb"])
+            abi.set_floats(dr.density_max_rgb, s["dir_dmax"])
+            abi.set_floats(dr.density_ref_rgb, s["dir_dref"])
+            abi.set_floats(dr.donor_k_rgb, s["dir_donor_k"])
+            for c in range(3):
+                dr.compensated_axes_rgb[c] = span(a["dir_axes_rgb"][c])
+            dr.compensated_axes_hash = dr.hash = 1
+
+        sb = h.scanner_bounds
+        abi.set_floats(sb.min_cmy, s["scan_min_cmy"])
+        abi.set_floats(sb.inv_span_cmy, s["scan_inv_span_cmy"])
+        sb.hash = 1
+        sp = h.scanner_spectra
+        sp.dye_c = span(a["scan_dye_c"])
+        sp.dye_m = span(a["scan_dye_m"])
+        sp.dye_y = span(a["scan_dye_y"])
+        sp.weighted_x = span(a["scan_wx"])
+        sp.weighted_y = span(a["scan_wy"])
+        sp.weighted_z = span(a["scan_wz"])
+        sp.base_density = span(a["scan_base"])
+        sp.inverse_y_normalization = s["scan_inv_yn"]
+        h.scanner_lut.resolution = s["scan_lut_resolution"]
+        h.scanner_lut.hash = h.scanner_lut.density_bounds_hash = 1
+        cr = h.scanner_correction
+        cr.exposure_scale = 1.0
+        cr.xyz_slope = 1.0
+        if correction is not None:
+            cr.flags = abi.FJ_CORRECTION_ACTIVE
+            cr.xyz_slope, cr.xyz_offset = correction
+
+        oc = h.output_color
+        abi.set_floats(oc.cat02, s["cat02"])
+        abi.set_floats(oc.xyz_to_rgb, s["xyz_to_rgb"])
+        abi.set_floats(oc.illuminant_xyz, s["illuminant_xyz"])
+        oc.color_space = abi.FJ_OUTPUT_SRGB
+        use_gamut = s.get("gamut", True) if gamut is None else gamut
+        oc.flags = abi.FJ_COLOR_ENCODE_CCTF | abi.FJ_COLOR_INPUT_IS_OUTPUT_SPACE | (
+            abi.FJ_COLOR_GAMUT_COMPRESSION if use_gamut else 0)
+        abi.set_floats(oc.native_rgb_to_d65_xyz, s["gamut_native_to_xyz"])
+        abi.set_floats(oc.d65_xyz_to_native_rgb, s["gamut_xyz_to_native"])
+        abi.set_floats(oc.lightness_knee, [0.95, 1.0, 1.6])
+        abi.set_floats(oc.chroma_knee, [0.95, 1.0, 1.6])
+        oc.gamut_cmax = span(a["gamut_cmax"])
+        oc.encoding.schema = abi.FJ_OUTPUT_ENCODING_SCHEMA
+        oc.encoding.cctf_kind = abi.FJ_CCTF_SRGB
+        oc.encoding.gamma = 1.0 / 2.4
+        abi.set_floats(oc.encoding.dwg_to_output, np.eye(3).ravel())
+
+        if recipe.route in (abi.FJ_ROUTE_NEGATIVE_PRINT, abi.FJ_ROUTE_POSITIVE_PRINT):
+            pr = h.print
+            pr.film_density_cmy = span(a["print_film_density_cmy"])
+            pr.film_base_density = span(a["print_film_base_density"])
+            pr.sensitivity_cmy = span(a["print_sensitivity_cmy"])
+            pr.log_exposure = span(a["print_log_exposure"])
+            pr.density_cmy = span(a["print_density_cmy"])
+            pr.main_illuminant = span(a["print_main_illuminant"])
+            pr.exposure = s["print_exposure"]
+            pr.normalizer = s["print_normalizer"]
+            pr.hash = pr.balance_hash = pr.film_density_hash = pr.profile_tables_hash = pr.main_illuminant_hash = 1
+
+        ae = h.auto_exposure
+        ae.method = abi.FJ_METER_CENTER_WEIGHTED
+        ae.hash = 1
+
+    def pointer(self):
+        return C.pointer(self.h)
+
+
+def synthetic_frame(width: int, height: int, seed: int, frame_index: int = 0) -> np.ndarray:
+    """Seeded smooth test scene, float32 linear Rec.709 RGB, shape (height, width, 3).
+
+    Three fields u1, u2, u3 in [0, 1], each 0.5 * a linear ramp at a random angle plus
+    0.5 * a sum of 16 Gaussian blobs (sigma 2-12 % of the width), normalised;
+    log2 Y = -8 + 12 u1, hue = 2 pi u2, chroma = 0.3 u3; RGB = Y (1 + chroma
+    (cos h a + sin h b)) with a, b unit opponent axes orthogonal to the Rec.709
+    luminance weights; negatives clamped to zero.
+    """
+    rng = np.random.Generator(np.random.PCG64(seed + frame_index))
+    yy, xx = np.mgrid[0:height, 0:width].astype(np.float32)
+    xn, yn = xx / max(width, 1), yy / max(width, 1)
+
+    def field_():
+        ang = rng.uniform(0, 2 * np.pi)
+        ramp = np.cos(ang) * xn + np.sin(ang) * yn
+        ramp = (ramp - ramp.min()) / max(float(np.ptp(ramp)), 1e-6)
+        blobs = np.zeros_like(xn)
+        for _ in range(16):
+            cx, cy = rng.uniform(0, 1), rng.uniform(0, height / max(width, 1))
+            sg = rng.uniform(0.02, 0.12)
+            blobs += rng.uniform(0.2, 1.0) * np.exp(-((xn - cx) ** 2 + (yn - cy) ** 2) / (2 * sg * sg))
+        blobs = (blobs - blobs.min()) / max(float(np.ptp(blobs)), 1e-6)
+        f = 0.5 * ramp + 0.5 * blobs
+        return (f - f.min()) / max(float(np.ptp(f)), 1e-6)
+
+    u1, u2, u3 = field_(), field_(), field_()
+    lum = np.exp2(-8.0 + 12.0 * u1)
+    hue = 2 * np.pi * u2
+    chroma = 0.3 * u3
+    wts = np.array([0.2126, 0.7152, 0.0722])
+    a_ax = np.array([1.0, -1.0, 0.0])
+    a_ax -= wts * (a_ax @ wts) / (wts @ wts)
+    a_ax /= np.linalg.norm(a_ax)
+    b_ax = np.cross(wts, a_ax)
+    b_ax -= wts * (b_ax @ wts) / (wts @ wts)
+    b_ax /= np.linalg.norm(b_ax)
+    mod = 1.0 + chroma[..., None] * (np.cos(hue)[..., None] * a_ax + np.sin(hue)[..., None] * b_ax)
+    rgb = lum[..., None] * mod
+    return np.ascontiguousarray(np.maximum(rgb, 0.0).astype(np.float32))

@@ -1,0 +1,163 @@
+"""Python calls over the C-ABI of libjuicer_b200.so.
+
+torch supplies device memory and streams here (plumbing only); every pixel is
+computed by the CUDA library. Nothing in this module has a CPU fallback: without the
+library or a GPU it raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi, load_library
+
+
+class FjError(RuntimeError):
+    def __init__(self, where: str, status, text: str):
+        super().__init__(f"{where}: status category {status.category} (api {status.api}, code "
+                         f"{status.native_code}): {text}")
+        self.status = status
+
+
+def _check(where: str, status, err: abi.ErrorText):
+    if status.category != abi.FJ_STATUS_SUCCESS:
+        raise FjError(where, status, err.text)
+
+
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("CUDA device required: the render path has no CPU implementation")
+    return torch
+
+
+def _ptr(t) -> int:
+    return int(t.data_ptr())
+
+
+def _stream_handle(stream) -> int:
+    return int(stream.cuda_stream) if stream is not None else 0
+
+
+class DeviceRecipe:
+    """Device tables of one prepared recipe (fjb_recipe_create / fjb_recipe_destroy)."""
+
+    def __init__(self, record, stream=None):
+        self.lib = load_library()
+        self.record = record
+        self.handle = C.c_void_p()
+        err = abi.ErrorText()
+        st = self.lib.fjb_recipe_create(record.pointer(), C.c_void_p(_stream_handle(stream)),
+                                        C.byref(self.handle), C.byref(err.buf))
+        _check("fjb_recipe_create", st, err)
+
+    def close(self):
+        if self.handle:
+            err = abi.ErrorText()
+            self.lib.fjb_recipe_destroy(self.handle, C.byref(err.buf))
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_exposure_scale_device(self, tensor):
+        err = abi.ErrorText()
+        st = self.lib.fjb_recipe_set_exposure_scale_device(self.handle, C.c_void_p(_ptr(tensor) if tensor is not None
+                                                                                    else 0), C.byref(err.buf))
+        _check("fjb_recipe_set_exposure_scale_device", st, err)
+
+    def clear_flags(self, stream=None):
+        err = abi.ErrorText()
+        _check("fjb_recipe_clear_flags",
+               self.lib.fjb_recipe_clear_flags(self.handle, C.c_void_p(_stream_handle(stream)), C.byref(err.buf)), err)
+
+    def read_flags(self, stream=None) -> int:
+        err = abi.ErrorText()
+        v = C.c_uint32()
+        _check("fjb_recipe_read_flags", self.lib.fjb_recipe_read_flags(
+            self.handle, C.c_void_p(_stream_handle(stream)), C.byref(v), C.byref(err.buf)), err)
+        return int(v.value)
+
+    def render(self, src, dst, stream=None):
+        """src/dst: contiguous float32 CUDA tensors of shape (H, W, 3|4)."""
+        h, w, comps = src.shape
+        err = abi.ErrorText()
+        st = self.lib.fjb_render_pixels(self.handle, C.c_void_p(_ptr(src)), src.stride(0) * 4,
+                                        C.c_void_p(_ptr(dst)), dst.stride(0) * 4, w, h, comps,
+                                        C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+        _check("fjb_render_pixels", st, err)
+
+    def camera_exposure(self, src, planes, stream=None):
+        h, w, comps = src.shape
+        b, g, r = planes
+        err = abi.ErrorText()
+        st = self.lib.fjb_camera_exposure(self.handle, C.c_void_p(_ptr(src)), src.stride(0) * 4, comps, w, h,
+                                          C.c_void_p(_ptr(b)), C.c_void_p(_ptr(g)), C.c_void_p(_ptr(r)),
+                                          b.stride(0), C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+        _check("fjb_camera_exposure", st, err)
+
+    def capture_density(self, src, density, carrier=None, stream=None):
+        c, m, y = density
+        h, w = c.shape
+        comps = src.shape[2] if src is not None else 3
+        cb, cg, cr = carrier if carrier is not None else (None, None, None)
+        err = abi.ErrorText()
+        st = self.lib.fjb_capture_density(
+            self.handle, C.c_void_p(_ptr(src) if src is not None else 0), (src.stride(0) * 4) if src is not None else 0,
+            comps, C.c_void_p(_ptr(cb) if cb is not None else 0), C.c_void_p(_ptr(cg) if cg is not None else 0),
+            C.c_void_p(_ptr(cr) if cr is not None else 0), cb.stride(0) if cb is not None else 0, w, h,
+            C.c_void_p(_ptr(c)), C.c_void_p(_ptr(m)), C.c_void_p(_ptr(y)), C.c_void_p(_stream_handle(stream)),
+            C.byref(err.buf))
+        _check("fjb_capture_density", st, err)
+
+    def render_carrier(self, carrier, src, dst, stream=None):
+        b, g, r = carrier
+        h, w, comps = dst.shape
+        err = abi.ErrorText()
+        st = self.lib.fjb_render_carrier(self.handle, C.c_void_p(_ptr(b)), C.c_void_p(_ptr(g)), C.c_void_p(_ptr(r)),
+                                         b.stride(0), C.c_void_p(_ptr(src) if src is not None else 0),
+                                         (src.stride(0) * 4) if src is not None else 0, C.c_void_p(_ptr(dst)),
+                                         dst.stride(0) * 4, w, h, comps, C.c_void_p(_stream_handle(stream)),
+                                         C.byref(err.buf))
+        _check("fjb_render_carrier", st, err)
+
+    def render_from_density(self, density, src, dst, stream=None):
+        c, m, y = density
+        h, w, comps = dst.shape
+        err = abi.ErrorText()
+        st = self.lib.fjb_render_from_density(self.handle, C.c_void_p(_ptr(c)), C.c_void_p(_ptr(m)),
+                                              C.c_void_p(_ptr(y)), C.c_void_p(_ptr(src) if src is not None else 0),
+                                              (src.stride(0) * 4) if src is not None else 0, C.c_void_p(_ptr(dst)),
+                                              dst.stride(0) * 4, w, h, comps, C.c_void_p(_stream_handle(stream)),
+                                              C.byref(err.buf))
+        _check("fjb_render_from_density", st, err)
+
+
+def render_pixels_numpy(record, src: np.ndarray) -> np.ndarray:
+    """One fused per-pixel render of a host image (H, W, 3|4) through the C-ABI."""
+    torch = _torch()
+    rec = DeviceRecipe(record)
+    s = torch.from_numpy(np.ascontiguousarray(src, dtype=np.float32)).cuda()
+    d = torch.empty_like(s)
+    rec.render(s, d)
+    torch.cuda.synchronize()
+    out = d.cpu().numpy()
+    rec.close()
+    return out
+
+
+def scanner_lut_build_host(inp: "abi.FjbScannerLutInput"):
+    """Six scanner PCHIP arrays built on the device (FP64) and returned as numpy arrays."""
+    lib = load_library()
+    r = int(inp.resolution)
+    nodes, cells = 3 * r ** 3, 3 * (r - 1) ** 3
+    outs = [np.zeros(nodes, np.float32) for _ in range(4)] + [np.zeros(cells, np.float32) for _ in range(2)]
+    err = abi.ErrorText()
+    st = lib.fjb_scanner_lut_build_host(C.byref(inp), *[C.c_void_p(o.ctypes.data) for o in outs], C.byref(err.buf))
+    _check("fjb_scanner_lut_build_host", st, err)
+    return outs

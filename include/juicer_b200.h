@@ -1,0 +1,102 @@
+/* juicer_b200.h -- stage-level entry points of libjuicer_b200.so.
+ *
+ * fj_cuda_render (juicer_cuda_api.h) renders a whole frame. The functions below
+ * expose the same device work one stage at a time, for hosts that schedule stages
+ * themselves and for parity testing. Every image/plane pointer is a device address;
+ * every function enqueues on `stream` (a cudaStream_t, 0 = legacy default stream)
+ * and returns without synchronising unless it says otherwise. No torch or CUDA C++
+ * types appear in these signatures.
+ */
+#ifndef JUICER_B200_H
+#define JUICER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "juicer_cuda_api.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Device-resident tables of one prepared recipe (TC LUT, curves, print spectra,
+ * scanner PCHIP LUT, gamut boundary). Opaque. */
+typedef struct FjbRecipe FjbRecipe;
+
+/* Uploads the tables named by `prepared` and builds the scanner LUT on the device
+ * (FP64). Replaces the reference's per-recipe preparation
+ * (src/Cuda/JuicerCudaExecutor.cpp:2873 Root::prepare_cuda_frame with the
+ * scanner-LUT host callback native/juicer_host_preparation.cpp:28). Synchronises
+ * `stream` before returning so that the borrowed spans may be released. */
+FjStatus fjb_recipe_create(const FjPreparedHostData* prepared, void* stream, FjbRecipe** out_recipe,
+                           FjErrorBuffer* error);
+FjStatus fjb_recipe_destroy(FjbRecipe* recipe, FjErrorBuffer* error);
+
+/* Device scalar read by the exposure step as the auto-exposure scale (NULL = 1). */
+FjStatus fjb_recipe_set_exposure_scale_device(FjbRecipe* recipe, const float* device_scale, FjErrorBuffer* error);
+
+/* Device error word (bit 0 scan failure, bit 8 DIR failure, bits 9..11 DIR
+ * channels B,G,R). Cleared by fjb_recipe_clear_flags, read by fjb_recipe_read_flags
+ * (which synchronises `stream`). */
+FjStatus fjb_recipe_clear_flags(FjbRecipe* recipe, void* stream, FjErrorBuffer* error);
+FjStatus fjb_recipe_read_flags(FjbRecipe* recipe, void* stream, uint32_t* out_flags, FjErrorBuffer* error);
+
+/* Fused per-pixel chain, source RGB(A) float32 -> encoded output RGB(A) float32,
+ * for the direct and print routes with runtime DIR (reference
+ * src/Cuda/Scan/JuicerCudaScanPipeline.cu:2244 juicer_cuda_negative_pipeline and
+ * :3759 juicer_cuda_print_pipeline). components is 3 or 4 for both images. */
+FjStatus fjb_render_pixels(FjbRecipe* recipe, const float* src, ptrdiff_t src_row_bytes, float* dst,
+                           ptrdiff_t dst_row_bytes, int32_t width, int32_t height, uint32_t components,
+                           void* stream, FjErrorBuffer* error);
+
+/* Camera exposure to carrier planes B, G, R (stride in floats), without the route
+ * correction (reference src/Cuda/Film/JuicerCudaFilmPipeline.cu:3103). */
+FjStatus fjb_camera_exposure(FjbRecipe* recipe, const float* src, ptrdiff_t src_row_bytes, uint32_t components,
+                             int32_t width, int32_t height, float* carrier_b, float* carrier_g, float* carrier_r,
+                             ptrdiff_t carrier_stride, void* stream, FjErrorBuffer* error);
+
+/* Carrier planes (may be NULL: then `src` is exposed) -> capture density planes
+ * C, M, Y (reference :2880 juicer_cuda_direct_focused_capture_density). */
+FjStatus fjb_capture_density(FjbRecipe* recipe, const float* src, ptrdiff_t src_row_bytes, uint32_t components,
+                             const float* carrier_b, const float* carrier_g, const float* carrier_r,
+                             ptrdiff_t carrier_stride, int32_t width, int32_t height, float* density_c,
+                             float* density_m, float* density_y, void* stream, FjErrorBuffer* error);
+
+/* Carrier planes -> encoded output (monolithic carrier kernel, reference :1867). */
+FjStatus fjb_render_carrier(FjbRecipe* recipe, const float* carrier_b, const float* carrier_g,
+                            const float* carrier_r, ptrdiff_t carrier_stride, const float* src_alpha_source,
+                            ptrdiff_t src_row_bytes, float* dst, ptrdiff_t dst_row_bytes, int32_t width,
+                            int32_t height, uint32_t components, void* stream, FjErrorBuffer* error);
+
+/* Capture density planes -> (print when the recipe's route prints) -> scan ->
+ * encoded output (reference :2908 continue_from_capture_density + :2586 scan).
+ * `src` supplies alpha when components == 4 (may be NULL: alpha 1). */
+FjStatus fjb_render_from_density(FjbRecipe* recipe, const float* density_c, const float* density_m,
+                                 const float* density_y, const float* src, ptrdiff_t src_row_bytes, float* dst,
+                                 ptrdiff_t dst_row_bytes, int32_t width, int32_t height, uint32_t components,
+                                 void* stream, FjErrorBuffer* error);
+
+/* Scanner LUT input record (reference native/juicer_cuda_frame_values.h FjScannerLutInput). */
+typedef struct FjbScannerLutInput {
+    FjFloatSpan eps_c, eps_m, eps_y;
+    FjFloatSpan weighted_x, weighted_y, weighted_z, baseline_min;
+    float range_min_cmy[3], inverse_span_cmy[3];
+    int32_t sample_count;
+    float inv_yn;
+    uint32_t has_baseline, medium, resolution;
+} FjbScannerLutInput;
+
+/* Builds the six scanner PCHIP arrays on the device (FP64) and copies them into the
+ * caller's HOST buffers: log2_xyz/slope_c/slope_m/slope_y hold 3*r^3 floats,
+ * cell_min/cell_max 3*(r-1)^3. Synchronous. Replaces the Rust host build
+ * rust/film-juicer-core/src/scanner/lut.rs:187 behind the callback
+ * native/juicer_cuda_call_scope.h:14. */
+FjStatus fjb_scanner_lut_build_host(const FjbScannerLutInput* input, float* log2_xyz, float* slope_c,
+                                    float* slope_m, float* slope_y, float* cell_min, float* cell_max,
+                                    FjErrorBuffer* error);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JUICER_B200_H */

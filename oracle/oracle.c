@@ -1,0 +1,832 @@
+/* oracle.c -- CPU restatement of Film-Juicer's per-pixel render chain (TEST ORACLE).
+ *
+ * This file is test infrastructure. Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / reference legs of bench.py load it, and only as the checker or the
+ * timed CPU baseline; the product (libjuicer_b200.so) never calls it.
+ *
+ * It restates, in plain C with no fused multiply-add (built with -ffp-contract=off),
+ * the reference's device math for the render path, step by step, and the reference's
+ * host packing of FjPreparedHostData into kernel payloads. Each function cites the
+ * reference file:line it follows. Scalar FP32/FP64 choices follow the reference:
+ * FP32 for exposure, curves, DIR, print and LUT interpolation; FP64 for the scan
+ * normalisation, scanner colour matrices and the output encoding; the scanner LUT
+ * build is FP64 (rust/film-juicer-core/src/scanner/lut.rs). libm's expf/log10f/...
+ * replace CUDA's device functions, so FP32 results may differ from a GPU in the
+ * last bits; integer work (interval searches, LUT cells, failure masks) is exact.
+ */
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../include/juicer_b200.h"
+#include "../include/juicer_cuda_api.h"
+
+#define NL 81
+#define TC 192
+
+typedef struct {
+    const float* x;
+    const float* y; /* strided */
+    int ystride;
+    int n;
+} Curve;
+
+typedef struct {
+    /* film */
+    int method, input_cs, decode, adapt;
+    float m_rgb_xyz[9], m_adapt[9], m_xyz_srgb[9];
+    const float* tc; /* [192][192][4] */
+    const float* mallett_basis;
+    const float* mallett_illum;
+    float sens_bgr[3][NL];
+    float mallett_midgray;
+    float manual, route;
+    float gamma_bgr[3];
+    int dir_mode;
+    float M[9], dmax[3], dref[3], dk[3], rcref[3], rkr[3];
+    Curve dens[3], dirc[3];
+    /* print */
+    int print;
+    const float *eps_c_src, *base_src, *pillum, *psens; /* strided [81][3] */
+    float print_exposure, print_route, preflash, midgray, preflash_raw[3];
+    Curve pdc[3];
+    /* scan */
+    int medium_negative;
+    float min_cmy[3], inv_cmy[3];
+    int res;
+    float *lut_v, *lut_sc, *lut_sm, *lut_sy, *cell_lo, *cell_hi;
+    int corr_active;
+    float corr_slope, corr_offset;
+    float cat02[9], xyz_rgb[9];
+    int gamut;
+    const float* cmax;
+    float g_to_xyz[9], g_from_xyz[9], lknee[3], cknee[3];
+    int enc_iso, enc_cctf;
+    float dwg[9];
+    int cctf_kind;
+    float cg, ca, cb, cc, cd, ccut;
+} Pack;
+
+/* ---------------- scanner LUT (rust/film-juicer-core/src/scanner/lut.rs:108-296) ---------------- */
+
+static void pchip_slopes(const double* v, int n, double* out, double* d) {
+    for (int i = 0; i < n - 1; ++i) d[i] = v[i + 1] - v[i];
+    if (n == 2) {
+        out[0] = out[1] = d[0];
+        return;
+    }
+#define ENDPOINT(a, b, res)                                                          \
+    do {                                                                             \
+        double s_ = 0.5 * (3.0 * (a) - (b));                                         \
+        if (s_ * (a) <= 0.0) res = 0.0;                                              \
+        else if ((a) * (b) < 0.0 && fabs(s_) > fabs(3.0 * (a))) res = 3.0 * (a);     \
+        else res = s_;                                                               \
+    } while (0)
+    ENDPOINT(d[0], d[1], out[0]);
+    for (int i = 1; i < n - 1; ++i) {
+        double p = d[i - 1], q = d[i];
+        out[i] = (p == 0.0 || q == 0.0 || p * q <= 0.0) ? 0.0 : 2.0 * p * q / (p + q);
+    }
+    ENDPOINT(d[n - 2], d[n - 3], out[n - 1]);
+#undef ENDPOINT
+}
+
+/* Returns 0 on success, 1 when a node is not finite. */
+int oracle_scanner_lut(const FjbScannerLutInput* in, float* log2_xyz, float* sc, float* sm, float* sy, float* cmin,
+                       float* cmax) {
+    const int r = (int)in->resolution;
+    const int k = in->sample_count;
+    if (r < 2) return 2;
+    const size_t count = (size_t)r * r * r * 3;
+    double* nodes = (double*)malloc(count * sizeof(double));
+    double* line = (double*)malloc((size_t)r * sizeof(double));
+    double* lsl = (double*)malloc((size_t)r * sizeof(double));
+    double* del = (double*)malloc((size_t)r * sizeof(double));
+    int fail = 0;
+    for (int c = 0; c < r && !fail; ++c)
+        for (int m = 0; m < r && !fail; ++m)
+            for (int y = 0; y < r && !fail; ++y) {
+                const int idx[3] = {c, m, y};
+                double dens[3];
+                for (int ch = 0; ch < 3; ++ch) {
+                    double nrm = (double)idx[ch] / (double)(r - 1);
+                    double scaled = nrm / (double)in->inverse_span_cmy[ch];
+                    dens[ch] = in->medium == 0 ? scaled - (double)in->range_min_cmy[ch]
+                                               : scaled + (double)in->range_min_cmy[ch];
+                }
+                double xyz[3] = {0, 0, 0};
+                const float* w[3] = {in->weighted_x.data, in->weighted_y.data, in->weighted_z.data};
+                for (int s = 0; s < k; ++s) {
+                    double base = in->has_baseline ? (double)in->baseline_min.data[s] : 0.0;
+                    double spectral = dens[0] * (double)in->eps_c.data[s] + dens[1] * (double)in->eps_m.data[s] +
+                                      dens[2] * (double)in->eps_y.data[s] + base;
+                    double t = pow(10.0, -spectral);
+                    for (int ch = 0; ch < 3; ++ch) {
+                        double wk = (double)w[ch][s];
+                        if (isfinite(wk)) {
+                            double p = t * wk;
+                            if (!isnan(p)) xyz[ch] += p;
+                        }
+                    }
+                }
+                for (int ch = 0; ch < 3; ++ch) {
+                    double sum = xyz[ch] * (double)in->inv_yn;
+                    double lg = log10(fmax(sum, 0.0) + 1e-10);
+                    if (!isfinite(lg)) fail = 1;
+                    size_t i = ((((size_t)c * r + m) * r + y) * 3) + ch;
+                    nodes[i] = lg * 3.32192809488736234787;
+                    log2_xyz[i] = (float)nodes[i];
+                }
+            }
+    if (!fail) {
+        float* outs[3] = {sc, sm, sy};
+        for (int axis = 0; axis < 3; ++axis)
+            for (int a = 0; a < r; ++a)
+                for (int b = 0; b < r; ++b)
+                    for (int ch = 0; ch < 3; ++ch) {
+                        for (int i = 0; i < r; ++i) {
+                            int cc = axis == 0 ? i : a, mm = axis == 0 ? a : (axis == 1 ? i : b),
+                                yy = axis == 2 ? i : b;
+                            line[i] = nodes[((((size_t)cc * r + mm) * r + yy) * 3) + ch];
+                        }
+                        pchip_slopes(line, r, lsl, del);
+                        for (int i = 0; i < r; ++i) {
+                            int cc = axis == 0 ? i : a, mm = axis == 0 ? a : (axis == 1 ? i : b),
+                                yy = axis == 2 ? i : b;
+                            outs[axis][((((size_t)cc * r + mm) * r + yy) * 3) + ch] = (float)lsl[i];
+                        }
+                    }
+        const int s = r - 1;
+        for (int c = 0; c < s; ++c)
+            for (int m = 0; m < s; ++m)
+                for (int y = 0; y < s; ++y)
+                    for (int ch = 0; ch < 3; ++ch) {
+                        double lo = nodes[((((size_t)c * r + m) * r + y) * 3) + ch], hi = lo;
+                        for (int dc = 0; dc < 2; ++dc)
+                            for (int dm = 0; dm < 2; ++dm)
+                                for (int dy = 0; dy < 2; ++dy) {
+                                    double v = nodes[((((size_t)(c + dc) * r + (m + dm)) * r + (y + dy)) * 3) + ch];
+                                    if (v < lo) lo = v;
+                                    if (hi < v) hi = v;
+                                }
+                        size_t i = ((((size_t)c * s + m) * s + y) * 3) + ch;
+                        cmin[i] = (float)lo;
+                        cmax[i] = (float)hi;
+                    }
+    }
+    free(nodes);
+    free(line);
+    free(lsl);
+    free(del);
+    return fail;
+}
+
+/* ---------------- device math (src/Cuda/JuicerCudaDeviceHelpers.cuh) ---------------- */
+
+static float keepf(float v) { return isfinite(v) ? v : 0.0f; }
+
+static void mat3(const float* m, const float* v, float* o) {
+    o[0] = m[0] * v[0] + m[1] * v[1] + m[2] * v[2];
+    o[1] = m[3] * v[0] + m[4] * v[1] + m[5] * v[2];
+    o[2] = m[6] * v[0] + m[7] * v[1] + m[8] * v[2];
+}
+
+static void mat3d(const float* m, const double* v, double* o) {
+    o[0] = (double)m[0] * v[0] + (double)m[1] * v[1] + (double)m[2] * v[2];
+    o[1] = (double)m[3] * v[0] + (double)m[4] * v[1] + (double)m[5] * v[2];
+    o[2] = (double)m[6] * v[0] + (double)m[7] * v[1] + (double)m[8] * v[2];
+}
+
+/* :175-196 */
+static float dec_bt2020(float v) {
+    float x = fmaxf(0.0f, keepf(v));
+    const float a = 1.09929681f;
+    if (x < 0.0812428791f) return x / 4.5f;
+    return powf((x + (a - 1.0f)) / a, 1.0f / 0.45f);
+}
+static float dec_srgb(float v) {
+    float x = fmaxf(0.0f, keepf(v));
+    if (x <= 0.04045f) return x / 12.92f;
+    return powf((x + 0.055f) / 1.055f, 2.4f);
+}
+/* :198-225 */
+static void decode(const Pack* p, const float* in, float* out) {
+    for (int c = 0; c < 3; ++c) {
+        if (p->decode && p->input_cs == 1) out[c] = dec_bt2020(in[c]);
+        else if (p->decode && p->input_cs == 3) out[c] = dec_srgb(in[c]);
+        else out[c] = keepf(in[c]);
+    }
+}
+
+/* :254-275 */
+static float mitchell(float t) {
+    const float B = 1.0f / 3.0f, C = 1.0f / 3.0f;
+    float x = fabsf(t);
+    if (x < 1.0f)
+        return (1.0f / 6.0f) * ((12.0f - 9.0f * B - 6.0f * C) * x * x * x + (-18.0f + 12.0f * B + 6.0f * C) * x * x +
+                                (6.0f - 2.0f * B));
+    if (x < 2.0f)
+        return (1.0f / 6.0f) * ((-B - 6.0f * C) * x * x * x + (6.0f * B + 30.0f * C) * x * x +
+                                (-12.0f * B - 48.0f * C) * x + (8.0f * B + 24.0f * C));
+    return 0.0f;
+}
+/* :277-289 */
+static void tc_coord(float nrm, int* base, float* frac) {
+    float coord = fminf(1.0f, fmaxf(0.0f, nrm)) * (float)(TC - 1);
+    if (coord >= (float)(TC - 1)) {
+        *base = TC - 2;
+        *frac = 1.0f;
+        return;
+    }
+    *base = (int)floorf(coord);
+    *frac = coord - (float)*base;
+}
+static int reflect(int i) {
+    if (i < 0) return -i;
+    if (i >= TC) return 2 * (TC - 1) - i;
+    return i;
+}
+/* :291-327 */
+static float tc_sample(const float* lut, int ch, float qc, float qm) {
+    int cb, mb;
+    float cf, mf;
+    tc_coord(qc, &cb, &cf);
+    tc_coord(qm, &mb, &mf);
+    float wc[4] = {mitchell(cf + 1.0f), mitchell(cf), mitchell(cf - 1.0f), mitchell(cf - 2.0f)};
+    float wm[4] = {mitchell(mf + 1.0f), mitchell(mf), mitchell(mf - 1.0f), mitchell(mf - 2.0f)};
+    float v = 0.0f, ws = 0.0f;
+    for (int dc = 0; dc < 4; ++dc) {
+        int c = reflect(cb - 1 + dc);
+        for (int dm = 0; dm < 4; ++dm) {
+            int m = reflect(mb - 1 + dm);
+            float w = wc[dc] * wm[dm];
+            ws += w;
+            v += w * lut[((size_t)c * TC + m) * 4 + ch];
+        }
+    }
+    return ws != 0.0f ? v / ws : 0.0f;
+}
+
+/* :537-617 */
+static void tc_exposure(const Pack* p, const float* in, float* e) {
+    float lin[3], xyz[3], w[3];
+    decode(p, in, lin);
+    mat3(p->m_rgb_xyz, lin, xyz);
+    if (p->adapt) mat3(p->m_adapt, xyz, w);
+    else memcpy(w, xyz, sizeof(w));
+    for (int c = 0; c < 3; ++c) w[c] = keepf(w[c]);
+    float X = keepf(w[0]), Y = keepf(w[1]), Z = keepf(w[2]);
+    float sum = X + Y + Z;
+    float den = fmaxf(sum, 1e-10f);
+    float x = X / den, y = Y / den;
+    float qd = fmaxf(1.0f - x, 1e-10f);
+    float qx = (1.0f - x);
+    qx = qx * qx;
+    float qy = y / qd;
+    qx = fminf(1.0f, fmaxf(0.0f, qx));
+    qy = fminf(1.0f, fmaxf(0.0f, qy));
+    float r = tc_sample(p->tc, 0, qx, qy), g = tc_sample(p->tc, 1, qx, qy), b = tc_sample(p->tc, 2, qx, qy);
+    e[0] = keepf(sum * keepf(b));
+    e[1] = keepf(sum * keepf(g));
+    e[2] = keepf(sum * keepf(r));
+}
+
+/* :509-535, :619-668 */
+static void mallett_exposure(const Pack* p, const float* in, float* e) {
+    float lin[3], xyz[3], ad[3], s[3];
+    decode(p, in, lin);
+    mat3(p->m_rgb_xyz, lin, xyz);
+    const float* src = xyz;
+    if (p->adapt) {
+        mat3(p->m_adapt, xyz, ad);
+        src = ad;
+    }
+    mat3(p->m_xyz_srgb, src, s);
+    for (int c = 0; c < 3; ++c) s[c] = keepf(s[c]);
+    float r = fmaxf(0.0f, keepf(s[0])), g = fmaxf(0.0f, keepf(s[1])), b = fmaxf(0.0f, keepf(s[2]));
+    float eb = 0, eg = 0, er = 0;
+    for (int i = 0; i < NL; ++i) {
+        float il = p->mallett_illum[i];
+        float spd = (r * p->mallett_basis[3 * i] + g * p->mallett_basis[3 * i + 1] + b * p->mallett_basis[3 * i + 2]) * il;
+        if (!isfinite(spd)) continue;
+        if (isfinite(p->sens_bgr[0][i])) eb += spd * p->sens_bgr[0][i];
+        if (isfinite(p->sens_bgr[1][i])) eg += spd * p->sens_bgr[1][i];
+        if (isfinite(p->sens_bgr[2][i])) er += spd * p->sens_bgr[2][i];
+    }
+    e[0] = isfinite(eb) ? fmaxf(0.0f, eb) : 0.0f;
+    e[1] = isfinite(eg) ? fmaxf(0.0f, eg) : 0.0f;
+    e[2] = isfinite(er) ? fmaxf(0.0f, er) : 0.0f;
+    for (int c = 0; c < 3; ++c) e[c] = fmaxf(0.0f, e[c] * p->mallett_midgray);
+}
+
+/* :710-736 */
+static void film_exposure(const Pack* p, const float* in, float ae, int with_route, float* e) {
+    if (p->method == FJ_RAW_MALLETT_2019) mallett_exposure(p, in, e);
+    else tc_exposure(p, in, e);
+    float a = 1.0f;
+    if (isfinite(ae) && ae > 0.0f) a = ae;
+    float s = a * p->manual;
+    if (with_route) s *= p->route;
+    s = (isfinite(s) && s > 0.0f) ? s : 1.0f;
+    for (int c = 0; c < 3; ++c) e[c] = fmaxf(0.0f, e[c] * s);
+}
+
+/* :34-89 */
+static float curve_at(const Curve* c, float logE, float gamma) {
+    if (!isfinite(logE)) return nanf("");
+    float xq = logE * gamma;
+    int last = c->n - 1;
+    float xmin = c->x[0], xmax = c->x[last];
+    if (!(xmax >= xmin)) return c->y[0];
+    if (xq <= xmin) return c->y[0];
+    if (xq >= xmax) return c->y[(size_t)last * c->ystride];
+    int lo = 1, hi = last, i1 = last + 1;
+    while (lo <= hi) {
+        int mid = lo + ((hi - lo) >> 1);
+        if (xq < c->x[mid]) {
+            i1 = mid;
+            hi = mid - 1;
+        } else lo = mid + 1;
+    }
+    if (i1 > last) return c->y[(size_t)last * c->ystride];
+    int i0 = i1 - 1;
+    float x0 = c->x[i0], x1 = c->x[i1], y0 = c->y[(size_t)i0 * c->ystride], y1 = c->y[(size_t)i1 * c->ystride];
+    float den = x1 - x0;
+    if (!(den > 0.0f) || !isfinite(den)) return y0;
+    float t = (xq - x0) / den;
+    return y0 + t * (y1 - y0);
+}
+/* :91-105 */
+static float inf_clamp(const Curve* c, float logE) {
+    if (isfinite(logE) || isnan(logE)) return logE;
+    float xmin = c->x[0], xmax = c->x[c->n - 1];
+    if (!(xmax >= xmin)) return logE;
+    return logE > 0.0f ? xmax : xmin;
+}
+
+/* :1073-1123 */
+static int langmuir(float v, float k, float ref, float* out) {
+    *out = nanf("");
+    if (!isfinite(v) || !isfinite(k) || !(k > 0.0f) || !isfinite(ref)) return 0;
+    float den = k + v, kr = k + ref;
+    int direct = isfinite(den) && den != 0.0f && isfinite(kr) && (v == 0.0f || fabsf(v) <= FLT_MAX / fabsf(kr));
+    if (direct) {
+        *out = v * kr / den;
+        return isfinite(*out);
+    }
+    float ns = 1.0f + ref / k;
+    if (!isfinite(ns)) return 0;
+    if (v >= 0.0f) {
+        float ds = 1.0f + v / k;
+        if (!isfinite(ds) || ds == 0.0f) return 0;
+        *out = (v / ds) * ns;
+        return isfinite(*out);
+    }
+    if (!isfinite(den) || den == 0.0f) return 0;
+    float ds = den / k;
+    if (!isfinite(ds) || ds == 0.0f) return 0;
+    if (fabsf(v) <= FLT_MAX / fabsf(ns)) *out = v * ns / ds;
+    else *out = (v / ds) * ns;
+    return isfinite(*out);
+}
+
+/* :1125-1241 */
+static unsigned dir_runtime(const Pack* p, float* logE, const float* layer) {
+    float donor[3] = {p->dmax[0] - layer[0], p->dmax[1] - layer[1], p->dmax[2] - layer[2]};
+    unsigned fail = 0;
+    if (p->dir_mode == FJ_DIR_NEGATIVE_DONOR_LANGMUIR)
+        for (int c = 0; c < 3; ++c)
+            if (!langmuir(layer[c], p->dk[c], p->dref[c], &donor[c])) fail |= 1u << c;
+    float corr[3];
+    corr[0] = p->M[0] * donor[0] + p->M[3] * donor[1] + p->M[6] * donor[2];
+    corr[1] = p->M[1] * donor[0] + p->M[4] * donor[1] + p->M[7] * donor[2];
+    corr[2] = p->M[2] * donor[0] + p->M[5] * donor[1] + p->M[8] * donor[2];
+    for (int c = 0; c < 3; ++c)
+        if (!isfinite(corr[c])) fail |= 1u << c;
+    if (p->dir_mode == FJ_DIR_POSITIVE_RECEIVER_LANGMUIR) {
+        for (int c = 0; c < 3; ++c) {
+            if (p->rcref[c] == 0.0f) {
+                corr[c] = 0.0f;
+                continue;
+            }
+            float v = corr[c];
+            if (!langmuir(v, p->rkr[c], p->rcref[c], &corr[c])) fail |= 1u << c;
+        }
+    }
+    if (fail) return fail;
+    unsigned sf = 0;
+    for (int c = 0; c < 3; ++c) {
+        float o = logE[c];
+        if (isnan(o)) {
+            sf |= 1u << c;
+            continue;
+        }
+        logE[c] = o - corr[c];
+        if ((!isinf(o) && !isfinite(logE[c])) || (isinf(o) && (!isinf(logE[c]) || signbit(o) != signbit(logE[c]))))
+            sf |= 1u << c;
+    }
+    return sf;
+}
+
+/* src/Cuda/Scan/JuicerCudaScanPipeline.cu:1622-1698 with :766-846 of the helpers */
+static unsigned capture_density(const Pack* p, const float* e_in, float* d) {
+    float logE[3], logS[3], layer[3];
+    for (int c = 0; c < 3; ++c) {
+        logE[c] = log10f(fmaxf(e_in[c], 0.0f) + 1e-10f);
+        logS[c] = inf_clamp(&p->dens[c], logE[c]);
+        layer[c] = curve_at(&p->dens[c], logS[c], p->gamma_bgr[c]);
+    }
+    if (p->dir_mode == FJ_DIR_INACTIVE) {
+        d[0] = layer[2];
+        d[1] = layer[1];
+        d[2] = layer[0];
+        return 0;
+    }
+    float lc[3] = {logS[0], logS[1], logS[2]};
+    unsigned f = dir_runtime(p, lc, layer);
+    if (f) {
+        d[0] = d[1] = d[2] = nanf("");
+        return f;
+    }
+    d[2] = curve_at(&p->dirc[0], lc[0], p->gamma_bgr[0]);
+    d[1] = curve_at(&p->dirc[1], lc[1], p->gamma_bgr[1]);
+    d[0] = curve_at(&p->dirc[2], lc[2], p->gamma_bgr[2]);
+    return 0;
+}
+
+/* :866-1071 (FP32, same accumulation order as the reference loop) */
+static void print_stage(const Pack* p, float* D) {
+    float ac = 0, am = 0, ay = 0;
+    for (int i = 0; i < NL; ++i) {
+        float sC = p->psens[i * 3], sM = p->psens[i * 3 + 1], sY = p->psens[i * 3 + 2];
+        int aC = !isnan(sC), aM = !isnan(sM), aY = !isnan(sY);
+        if (!aC && !aM && !aY) continue;
+        float base = p->base_src[i];
+        float ds = D[0] * p->eps_c_src[i * 3] + D[1] * p->eps_c_src[i * 3 + 1] + D[2] * p->eps_c_src[i * 3 + 2] + base;
+        float t = exp2f(-ds * 3.32192809488736234787f) * p->pillum[i];
+        float e = isnan(t) ? 0.0f : t;
+        if (aC) ac += e * sC;
+        if (aM) am += e * sM;
+        if (aY) ay += e * sY;
+    }
+    float raw[3] = {ac, am, ay};
+    for (int c = 0; c < 3; ++c) raw[c] *= p->midgray;
+    if (isfinite(p->preflash) && p->preflash > 0.0f)
+        for (int c = 0; c < 3; ++c) raw[c] += p->preflash_raw[c] * p->preflash;
+    for (int c = 0; c < 3; ++c) raw[c] *= p->print_exposure;
+    for (int c = 0; c < 3; ++c) raw[c] *= p->print_route;
+    for (int c = 0; c < 3; ++c) D[c] = curve_at(&p->pdc[c], log10f(raw[c] + 1e-10f), 1.0f);
+}
+
+/* :357-506 */
+static void pchip_coord(float nrm, int res, int* base, float* frac) {
+    float coord = nrm * (float)(res - 1);
+    coord = fminf((float)(res - 1), fmaxf(0.0f, coord));
+    if (coord >= (float)(res - 1)) {
+        *base = res - 2;
+        *frac = 1.0f;
+        return;
+    }
+    *base = (int)floorf(coord);
+    *frac = coord - (float)*base;
+}
+static float herm(float y0, float y1, float m0, float m1, float t) {
+    float t2 = t * t, t3 = t2 * t;
+    float h00 = 2.0f * t3 - 3.0f * t2 + 1.0f, h10 = t3 - 2.0f * t2 + t, h01 = -2.0f * t3 + 3.0f * t2, h11 = t3 - t2;
+    return h00 * y0 + h10 * m0 + h01 * y1 + h11 * m1;
+}
+static float lmix(float a, float b, float t) { return a + t * (b - a); }
+
+static int scan_lut(const Pack* p, const double* n, float* out) {
+    if (!isfinite(n[0]) || !isfinite(n[1]) || !isfinite(n[2])) return 0;
+    int r = p->res, c, m, y;
+    float tc, tm, ty;
+    pchip_coord((float)n[0], r, &c, &tc);
+    pchip_coord((float)n[1], r, &m, &tm);
+    pchip_coord((float)n[2], r, &y, &ty);
+#define AT(T, cc, mm, yy, o) (T)[((((size_t)(cc) * r + (mm)) * r + (yy)) * 3) + (o)]
+    for (int o = 0; o < 3; ++o) {
+        float v000 = herm(AT(p->lut_v, c, m, y, o), AT(p->lut_v, c + 1, m, y, o), AT(p->lut_sc, c, m, y, o),
+                          AT(p->lut_sc, c + 1, m, y, o), tc);
+        float v010 = herm(AT(p->lut_v, c, m + 1, y, o), AT(p->lut_v, c + 1, m + 1, y, o),
+                          AT(p->lut_sc, c, m + 1, y, o), AT(p->lut_sc, c + 1, m + 1, y, o), tc);
+        float v001 = herm(AT(p->lut_v, c, m, y + 1, o), AT(p->lut_v, c + 1, m, y + 1, o),
+                          AT(p->lut_sc, c, m, y + 1, o), AT(p->lut_sc, c + 1, m, y + 1, o), tc);
+        float v011 = herm(AT(p->lut_v, c, m + 1, y + 1, o), AT(p->lut_v, c + 1, m + 1, y + 1, o),
+                          AT(p->lut_sc, c, m + 1, y + 1, o), AT(p->lut_sc, c + 1, m + 1, y + 1, o), tc);
+        float sm00 = lmix(AT(p->lut_sm, c, m, y, o), AT(p->lut_sm, c + 1, m, y, o), tc);
+        float sm10 = lmix(AT(p->lut_sm, c, m + 1, y, o), AT(p->lut_sm, c + 1, m + 1, y, o), tc);
+        float sm01 = lmix(AT(p->lut_sm, c, m, y + 1, o), AT(p->lut_sm, c + 1, m, y + 1, o), tc);
+        float sm11 = lmix(AT(p->lut_sm, c, m + 1, y + 1, o), AT(p->lut_sm, c + 1, m + 1, y + 1, o), tc);
+        float vy0 = herm(v000, v010, sm00, sm10, tm);
+        float vy1 = herm(v001, v011, sm01, sm11, tm);
+        float sy0 = lmix(lmix(AT(p->lut_sy, c, m, y, o), AT(p->lut_sy, c + 1, m, y, o), tc),
+                         lmix(AT(p->lut_sy, c, m + 1, y, o), AT(p->lut_sy, c + 1, m + 1, y, o), tc), tm);
+        float sy1 = lmix(lmix(AT(p->lut_sy, c, m, y + 1, o), AT(p->lut_sy, c + 1, m, y + 1, o), tc),
+                         lmix(AT(p->lut_sy, c, m + 1, y + 1, o), AT(p->lut_sy, c + 1, m + 1, y + 1, o), tc), tm);
+        float v = herm(vy0, vy1, sy0, sy1, ty);
+        int s = r - 1;
+        size_t ci = ((((size_t)c * s + m) * s + y) * 3) + o;
+        out[o] = fminf(p->cell_hi[ci], fmaxf(p->cell_lo[ci], v));
+    }
+#undef AT
+    return 1;
+}
+
+/* src/GamutCompression.h:110-216 */
+static const float OK_XL[9] = {0.8189330101f, 0.3618667424f, -0.1288597137f, 0.0329845436f, 0.9293118715f,
+                               0.0361456387f, 0.0482003018f, 0.2643662691f, 0.6338517070f};
+static const float OK_LX[9] = {1.2270138511f,  -0.5577999807f, 0.2812561490f,  -0.0405801784f, 1.1122568696f,
+                               -0.0716766787f, -0.0763812845f, -0.4214819784f, 1.5861632204f};
+static const float OK_RL[9] = {0.2104542553f, 0.7936177850f, -0.0040720468f, 1.9779984951f, -2.4285922050f,
+                               0.4505937099f, 0.0259040371f, 0.7827717662f, -0.8086757660f};
+static const float OK_LR[9] = {1.0f, 0.3963377774f,  0.2158037573f,  1.0f, -0.1055613458f,
+                               -0.0638541728f, 1.0f, -0.0894841775f, -1.2914855480f};
+static float scbrt(float v) { return v < 0.0f ? -cbrtf(-v) : cbrtf(v); }
+static float knee(float v, const float* k) {
+    if (!(v > k[0])) return v;
+    float span = k[1] - k[0], nrm = (v - k[0]) / span;
+    return k[0] + span * nrm / powf(1.0f + powf(nrm, k[2]), 1.0f / k[2]);
+}
+static float boundary(const float* cmax, float L, float h) {
+    const float PI = 3.14159265358979323846f, TWO_PI = 2.0f * PI;
+    float Lc = fminf(fmaxf(L, 0.02f), 1.0f);
+    float lp = (Lc - 0.02f) / (1.0f - 0.02f) * 63.0f;
+    int l0 = (int)floorf(lp), l1 = l0 + 1 < 64 ? l0 + 1 : l0;
+    float lf = lp - (float)l0;
+    float wh = fmodf(h + PI, TWO_PI);
+    if (wh < 0.0f) wh += TWO_PI;
+    float hp = wh / TWO_PI * 720.0f;
+    int h0 = (int)floorf(hp) % 720, h1 = (h0 + 1) % 720;
+    float hf = hp - floorf(hp);
+    int r0 = l0 * 720, r1 = l1 * 720;
+    float a = cmax[r0 + h0] + hf * (cmax[r0 + h1] - cmax[r0 + h0]);
+    float b = cmax[r1 + h0] + hf * (cmax[r1 + h1] - cmax[r1 + h0]);
+    return a + lf * (b - a);
+}
+static void gamut(const Pack* p, float* rgb) {
+    float xyz[3], lms[3], lab[3];
+    mat3(p->g_to_xyz, rgb, xyz);
+    mat3(OK_XL, xyz, lms);
+    for (int c = 0; c < 3; ++c) lms[c] = scbrt(lms[c]);
+    mat3(OK_RL, lms, lab);
+    lab[0] = knee(lab[0], p->lknee);
+    float ch = hypotf(lab[1], lab[2]);
+    if (ch > 0.0f) {
+        float hue = atan2f(lab[2], lab[1]);
+        float b = fmaxf(boundary(p->cmax, lab[0], hue), 1.0e-9f);
+        float cmp = knee(ch / b, p->cknee) * b;
+        float s = cmp / ch;
+        lab[1] *= s;
+        lab[2] *= s;
+    }
+    mat3(OK_LR, lab, lms);
+    for (int c = 0; c < 3; ++c) lms[c] = lms[c] * lms[c] * lms[c];
+    mat3(OK_LX, lms, xyz);
+    mat3(p->g_from_xyz, xyz, rgb);
+}
+
+/* src/Cuda/Scan/JuicerCudaScanPipeline.cu:99-192 */
+static double clamp01(double v) { return v <= 0.0 ? 0.0 : (v >= 1.0 ? 1.0 : v); }
+static float enc(const Pack* p, float v) {
+    switch (p->cctf_kind) {
+        case 0: return v;
+        case 1: return copysignf(powf(fabsf(v), p->cg), v);
+        case 2: return v <= 0.0031308f ? 12.92f * v : 1.055f * powf(v, 1.0f / 2.4f) - 0.055f;
+        case 3: return v < p->cb ? v * 4.5f : p->ca * powf(v, 0.45f) - (p->ca - 1.0f);
+        case 4: return v < p->ccut ? v * 16.0f : powf(v, p->cg);
+        case 5: {
+            float l = fmaxf(0.0f, v);
+            return l <= p->ccut ? l * p->cd : (log2f(l + p->ca) + p->cb) * p->cc;
+        }
+        default: return (float)clamp01(v);
+    }
+}
+
+/* :1700-1858: density -> encoded RGB; returns 0 on a scan failure */
+static int scan_out(const Pack* p, const float* D, double* rgb) {
+    double n[3];
+    for (int c = 0; c < 3; ++c)
+        n[c] = p->medium_negative ? ((double)D[c] + (double)p->min_cmy[c]) * (double)p->inv_cmy[c]
+                                  : ((double)D[c] - (double)p->min_cmy[c]) * (double)p->inv_cmy[c];
+    float l2[3];
+    if (!scan_lut(p, n, l2)) return 0;
+    double xyz[3] = {(double)exp2f(l2[0]), (double)exp2f(l2[1]), (double)exp2f(l2[2])};
+    if (p->corr_active) {
+        double cy = fmin(fmax((double)p->corr_slope * xyz[1] + (double)p->corr_offset, 0.0), 1.0);
+        double s = cy / (xyz[1] + 1e-10);
+        for (int c = 0; c < 3; ++c) xyz[c] *= s;
+    }
+    double ad[3];
+    mat3d(p->cat02, xyz, ad);
+    mat3d(p->xyz_rgb, ad, rgb);
+    if (!isfinite(rgb[0]) || !isfinite(rgb[1]) || !isfinite(rgb[2])) return 0;
+    if (p->gamut) {
+        float f[3] = {(float)rgb[0], (float)rgb[1], (float)rgb[2]};
+        gamut(p, f);
+        if (!isfinite(f[0]) || !isfinite(f[1]) || !isfinite(f[2])) return 0;
+        for (int c = 0; c < 3; ++c) rgb[c] = f[c];
+    }
+    double lin[3];
+    if (p->enc_iso) memcpy(lin, rgb, sizeof(lin));
+    else mat3d(p->dwg, rgb, lin);
+    for (int c = 0; c < 3; ++c) rgb[c] = p->enc_cctf ? (double)enc(p, (float)lin[c]) : lin[c];
+    for (int c = 0; c < 3; ++c) rgb[c] = clamp01(rgb[c]);
+    return 1;
+}
+
+/* ---------------- packing (JuicerCudaFilmPayloads.cpp:28-197, JuicerCudaResources.cpp) ---------------- */
+
+typedef struct {
+    Pack p;
+    float* lut_store;
+} Packed;
+
+static int pack(const FjPreparedHostData* h, Packed* out) {
+    memset(out, 0, sizeof(*out));
+    Pack* p = &out->p;
+    const FjFilmExposure* ex = &h->film_exposure;
+    p->method = (int)ex->method;
+    p->input_cs = (int)ex->input_color_space;
+    p->decode = (ex->flags & FJ_FILM_DECODE_CCTF) != 0;
+    p->adapt = (ex->flags & FJ_FILM_ADAPT_INPUT) != 0;
+    memcpy(p->m_rgb_xyz, ex->input_rgb_to_xyz, 36);
+    memcpy(p->m_adapt, ex->input_xyz_adapt, 36);
+    memcpy(p->m_xyz_srgb, ex->xyz_to_linear_srgb, 36);
+    p->tc = ex->tc_lut_rgba.data;
+    p->mallett_basis = ex->mallett_basis.data;
+    p->mallett_illum = ex->mallett_illuminant.data;
+    for (int i = 0; i < NL; ++i)
+        for (int bgr = 0; bgr < 3; ++bgr) p->sens_bgr[bgr][i] = ex->sensitivity_rgb.data[i * 3 + (2 - bgr)];
+    p->mallett_midgray = ex->mallett_green_midgray_scale;
+    p->manual = exp2f(ex->manual_exposure_ev);
+    p->route = ex->route_correction_scale;
+    const FjFilmDevelopment* dv = &h->film_development;
+    const int n = (int)dv->log_exposure.count;
+    for (int bgr = 0; bgr < 3; ++bgr) {
+        int rgb = 2 - bgr;
+        p->gamma_bgr[bgr] = dv->gamma_rgb[rgb];
+        p->dens[bgr] = (Curve){dv->log_exposure.data, dv->density_rgb.data + rgb, 3, n};
+    }
+    const FjDirCouplers* dir = &h->dir_couplers;
+    p->dir_mode = (int)dir->mode;
+    if (dir->mode != FJ_DIR_INACTIVE) {
+        for (int d = 0; d < 3; ++d) {
+            for (int r = 0; r < 3; ++r) p->M[d * 3 + r] = dir->matrix_rgb[(2 - d) * 3 + (2 - r)];
+            p->dmax[d] = dir->density_max_rgb[2 - d];
+            p->dref[d] = dir->density_ref_rgb[2 - d];
+            p->dk[d] = dir->donor_k_rgb[2 - d];
+            p->rcref[d] = dir->receiver_c_ref_rgb[2 - d];
+            p->rkr[d] = dir->receiver_kr_rgb[2 - d];
+            p->dirc[d] = (Curve){dir->compensated_axes_rgb[2 - d].data, dv->density_rgb.data + (2 - d), 3, n};
+        }
+    }
+    p->print = h->route == FJ_ROUTE_NEGATIVE_PRINT || h->route == FJ_ROUTE_POSITIVE_PRINT;
+    if (p->print) {
+        const FjPrint* pr = &h->print;
+        p->eps_c_src = pr->film_density_cmy.data;
+        p->base_src = pr->film_base_density.data;
+        p->pillum = pr->main_illuminant.data;
+        p->psens = pr->sensitivity_cmy.data;
+        p->print_exposure = pr->exposure;
+        p->print_route = h->scanner_correction.exposure_scale;
+        int pf = (pr->flags & FJ_PRINT_PREFLASH) != 0;
+        p->preflash = pf ? pr->preflash_exposure : 0.0f;
+        for (int c = 0; c < 3; ++c) p->preflash_raw[c] = pf ? pr->preflash_raw_cmy[c] : 0.0f;
+        p->midgray = pr->normalizer;
+        int np = (int)pr->log_exposure.count;
+        for (int c = 0; c < 3; ++c) p->pdc[c] = (Curve){pr->log_exposure.data, pr->density_cmy.data + c, 3, np};
+    }
+    p->medium_negative = p->print ? 0 : 1;
+    for (int c = 0; c < 3; ++c) {
+        p->min_cmy[c] = p->print ? h->scanner_bounds.min_cmy[c] : -h->scanner_bounds.min_cmy[c];
+        p->inv_cmy[c] = h->scanner_bounds.inv_span_cmy[c];
+    }
+    /* scanner LUT built on the host in FP64 */
+    const FjScannerSpectra* sp = &h->scanner_spectra;
+    int r = (int)h->scanner_lut.resolution;
+    size_t nodes = (size_t)r * r * r * 3, cells = (size_t)(r - 1) * (r - 1) * (r - 1) * 3;
+    out->lut_store = (float*)malloc((nodes * 4 + cells * 2) * sizeof(float));
+    if (!out->lut_store) return 1;
+    p->lut_v = out->lut_store;
+    p->lut_sc = p->lut_v + nodes;
+    p->lut_sm = p->lut_sc + nodes;
+    p->lut_sy = p->lut_sm + nodes;
+    p->cell_lo = p->lut_sy + nodes;
+    p->cell_hi = p->cell_lo + cells;
+    FjbScannerLutInput in;
+    memset(&in, 0, sizeof(in));
+    in.eps_c = sp->dye_c;
+    in.eps_m = sp->dye_m;
+    in.eps_y = sp->dye_y;
+    in.weighted_x = sp->weighted_x;
+    in.weighted_y = sp->weighted_y;
+    in.weighted_z = sp->weighted_z;
+    in.baseline_min = sp->base_density;
+    in.has_baseline = sp->base_density.count != 0;
+    in.sample_count = (int32_t)sp->dye_c.count;
+    in.inv_yn = sp->inverse_y_normalization;
+    for (int c = 0; c < 3; ++c) {
+        in.range_min_cmy[c] = p->min_cmy[c];
+        in.inverse_span_cmy[c] = p->inv_cmy[c];
+    }
+    in.medium = p->print ? 1u : 0u;
+    in.resolution = (uint32_t)r;
+    if (oracle_scanner_lut(&in, p->lut_v, p->lut_sc, p->lut_sm, p->lut_sy, p->cell_lo, p->cell_hi) != 0) return 2;
+    p->res = r;
+    p->corr_active = (h->scanner_correction.flags & FJ_CORRECTION_ACTIVE) != 0;
+    p->corr_slope = h->scanner_correction.xyz_slope;
+    p->corr_offset = h->scanner_correction.xyz_offset;
+    const FjOutputColor* oc = &h->output_color;
+    memcpy(p->cat02, oc->cat02, 36);
+    memcpy(p->xyz_rgb, oc->xyz_to_rgb, 36);
+    p->gamut = (oc->flags & FJ_COLOR_GAMUT_COMPRESSION) != 0;
+    p->cmax = oc->gamut_cmax.data;
+    memcpy(p->g_to_xyz, oc->native_rgb_to_d65_xyz, 36);
+    memcpy(p->g_from_xyz, oc->d65_xyz_to_native_rgb, 36);
+    memcpy(p->lknee, oc->lightness_knee, 12);
+    memcpy(p->cknee, oc->chroma_knee, 12);
+    p->enc_iso = (oc->flags & FJ_COLOR_INPUT_IS_OUTPUT_SPACE) != 0;
+    p->enc_cctf = (oc->flags & FJ_COLOR_ENCODE_CCTF) != 0;
+    memcpy(p->dwg, oc->encoding.dwg_to_output, 36);
+    p->cctf_kind = (int)oc->encoding.cctf_kind;
+    p->cg = oc->encoding.gamma;
+    p->ca = oc->encoding.a;
+    p->cb = oc->encoding.b;
+    p->cc = oc->encoding.c;
+    p->cd = oc->encoding.d;
+    p->ccut = oc->encoding.linear_cutoff;
+    return 0;
+}
+
+/* ---------------- entry points ---------------- */
+
+/* Stage selector: 0 = source -> encoded output; 1 = source -> capture density planes;
+ * 2 = density planes -> encoded output; 3 = source -> camera exposure planes (B,G,R, no
+ * route correction); 4 = carrier planes -> encoded output. */
+int oracle_render(const FjPreparedHostData* h, int stage, const float* src, long src_row_floats, int width,
+                  int height, int comps, float* dst, long dst_row_floats, float* p0, float* p1, float* p2,
+                  float auto_scale, int threads, unsigned* flags_out) {
+    Packed pk;
+    int rc = pack(h, &pk);
+    if (rc) {
+        free(pk.lut_store);
+        return rc;
+    }
+    const Pack* p = &pk.p;
+    unsigned flags = 0;
+#if defined(_OPENMP)
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threads > 0 ? threads : 1) reduction(| : flags)
+#endif
+    for (int y = 0; y < height; ++y) {
+        for (int x = 0; x < width; ++x) {
+            size_t i = (size_t)y * width + x;
+            const float* s = src ? src + (size_t)y * src_row_floats + (size_t)x * comps : NULL;
+            float D[3];
+            if (stage == 2) {
+                D[0] = p0[i];
+                D[1] = p1[i];
+                D[2] = p2[i];
+            } else if (stage == 4) {
+                float e[3] = {p0[i], p1[i], p2[i]};
+                for (int c = 0; c < 3; ++c) e[c] = fmaxf(0.0f, e[c] * p->route);
+                unsigned f = capture_density(p, e, D);
+                if (f) flags |= (1u << 8) | ((f & 7u) << 9);
+            } else {
+                float e[3];
+                film_exposure(p, s, auto_scale, stage == 3 ? 0 : 1, e);
+                if (stage == 3) {
+                    p0[i] = e[0];
+                    p1[i] = e[1];
+                    p2[i] = e[2];
+                    continue;
+                }
+                unsigned f = capture_density(p, e, D);
+                if (f) flags |= (1u << 8) | ((f & 7u) << 9);
+            }
+            if (stage == 1) {
+                p0[i] = D[0];
+                p1[i] = D[1];
+                p2[i] = D[2];
+                continue;
+            }
+            if (p->print) print_stage(p, D);
+            double rgb[3];
+            float* o = dst + (size_t)y * dst_row_floats + (size_t)x * comps;
+            if (!scan_out(p, D, rgb)) {
+                flags |= 1u;
+                o[0] = o[1] = o[2] = 0.0f;
+            } else {
+                o[0] = (float)rgb[0];
+                o[1] = (float)rgb[1];
+                o[2] = (float)rgb[2];
+            }
+            if (comps == 4) o[3] = s ? s[3] : 1.0f;
+        }
+    }
+    free(pk.lut_store);
+    if (flags_out) *flags_out = flags;
+    return 0;
+}
