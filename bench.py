@@ -73,9 +73,9 @@ class ClockSampler:
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                         stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except (OSError, FileNotFoundError):
@@ -110,7 +110,8 @@ class ClockSampler:
                 if flag.lower() == "active":
                     reasons.add(name)
         if not mhz:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "error": (self.lines[0][:200] if self.lines else "no nvidia-smi output")}
         return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": max(maxes), "reasons": sorted(reasons),
                 "samples": len(mhz)}
 

@@ -1,0 +1,254 @@
+// ref_shim.cu -- drives the reference's own CUDA render kernels (TEST INFRASTRUCTURE).
+//
+// Built by oracle/build_ref.py against the read-only reference sources
+// (src/Cuda/Scan/JuicerCudaScanPipeline.cu, src/Cuda/Film/JuicerCudaFilmPipeline.cu)
+// into oracle/_ref/libjuicer_ref.so. It fills the reference's internal payload
+// structs (src/Cuda/JuicerCudaPayloads.h) from an FjPreparedHostData exactly as the
+// reference's host packing does (src/Cuda/JuicerCudaFilmPayloads.cpp:28-197,
+// src/Cuda/JuicerCudaResources.cpp:3838-3840, :3910-3922, :4186-4254, :4335-4420,
+// src/Cuda/JuicerCudaExecutor.cpp:962-1011, :1575-1607), uploads the tables, and
+// calls the reference launchers juicer_cuda_negative_pipeline /
+// juicer_cuda_print_pipeline / juicer_cuda_direct_focused_capture_density. Only the
+// GPU parity tests load it; the product never does.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "Cuda/JuicerCudaPayloads.h"
+#include "GamutCompression.h"
+#include "juicer_cuda_api.h"
+
+extern "C" cudaError_t juicer_cuda_negative_pipeline(const JuicerCuda::PipelineRunParams*, void*);
+extern "C" cudaError_t juicer_cuda_print_pipeline(const JuicerCuda::PipelineRunParams*, void*);
+extern "C" cudaError_t juicer_cuda_print_focused_capture_density(const JuicerCuda::PrintPipelineRunParams*, float*,
+                                                                  float*, float*, void*);
+
+namespace {
+
+struct Arena {
+    std::vector<void*> ptrs;
+    ~Arena() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+    template <typename T>
+    const T* put(const T* host, size_t count) {
+        void* d = nullptr;
+        if (count == 0) return nullptr;
+        if (cudaMalloc(&d, count * sizeof(T)) != cudaSuccess) return nullptr;
+        cudaMemcpy(d, host, count * sizeof(T), cudaMemcpyHostToDevice);
+        ptrs.push_back(d);
+        return static_cast<const T*>(d);
+    }
+    const float* column(const float* src, size_t n, int stride, int col) {
+        std::vector<float> v(n);
+        for (size_t i = 0; i < n; ++i) v[i] = src[i * stride + col];
+        return put(v.data(), n);
+    }
+};
+
+JuicerCuda::DeviceCurveView curve(const float* x, const float* y, int n) {
+    JuicerCuda::DeviceCurveView c{};
+    c.x = x;
+    c.y = y;
+    c.n = n;
+    c.domainBegin = 0;
+    c.domainEnd = n - 1;
+    return c;
+}
+
+// Fills a PipelineRunParams the way the reference host does. Returns false on a
+// malformed record.
+bool pack(const FjPreparedHostData& h, const float* const lut[6], Arena& a, JuicerCuda::PipelineRunParams& p,
+          unsigned* d_flags) {
+    using namespace JuicerCuda;
+    p = PipelineRunParams{};
+    const FjFilmExposure& ex = h.film_exposure;
+    p.filmRaw.inputColorSpaceIndex = (int)ex.input_color_space;
+    p.filmRaw.applyCctfDecoding = (ex.flags & FJ_FILM_DECODE_CCTF) ? 1 : 0;
+    p.filmRaw.applyInputChromaticAdapt = (ex.flags & FJ_FILM_ADAPT_INPUT) ? 1 : 0;
+    p.filmRaw.rgbToRawMethod = (int)ex.method;
+    p.filmRaw.mallettGreenMidgrayScale = ex.mallett_green_midgray_scale;
+    std::memcpy(p.filmRaw.inputRGBToXYZ, ex.input_rgb_to_xyz, 36);
+    std::memcpy(p.filmRaw.inputXYZAdapt, ex.input_xyz_adapt, 36);
+    std::memcpy(p.filmRaw.xyzToLinearSrgb, ex.xyz_to_linear_srgb, 36);
+    p.filmExpose.manualExposureScale = std::exp2(ex.manual_exposure_ev);
+    p.filmExpose.routeCorrectionScale = ex.route_correction_scale;
+    auto& rc = p.filmExpose.reconstruction;
+    rc.sensB = curve(nullptr, a.column(ex.sensitivity_rgb.data, 81, 3, 2), 81);
+    rc.sensG = curve(nullptr, a.column(ex.sensitivity_rgb.data, 81, 3, 1), 81);
+    rc.sensR = curve(nullptr, a.column(ex.sensitivity_rgb.data, 81, 3, 0), 81);
+    if (ex.method == FJ_RAW_MALLETT_2019) {
+        rc.tablesIllum = a.put(ex.mallett_illuminant.data, 81);
+        rc.tablesK = 81;
+        rc.mallettBasis = a.put(ex.mallett_basis.data, 243);
+        rc.mallettBasisK = 81;
+    } else {
+        rc.filmTcLut = a.put(ex.tc_lut_rgba.data, ex.tc_lut_rgba.count);
+        rc.filmTcLutExtent = kFilmTcLutExtent;
+    }
+    const FjFilmDevelopment& dv = h.film_development;
+    const int n = (int)dv.log_exposure.count;
+    const float* dx = a.put(dv.log_exposure.data, n);
+    const float* yB = a.column(dv.density_rgb.data, n, 3, 2);
+    const float* yG = a.column(dv.density_rgb.data, n, 3, 1);
+    const float* yR = a.column(dv.density_rgb.data, n, 3, 0);
+    p.filmDevelop.gammaFactorB = dv.gamma_rgb[2];
+    p.filmDevelop.gammaFactorG = dv.gamma_rgb[1];
+    p.filmDevelop.gammaFactorR = dv.gamma_rgb[0];
+    p.filmDevelop.densB = curve(dx, yB, n);
+    p.filmDevelop.densG = curve(dx, yG, n);
+    p.filmDevelop.densR = curve(dx, yR, n);
+    const FjDirCouplers& dir = h.dir_couplers;
+    if (dir.mode != FJ_DIR_INACTIVE) {
+        p.filmDevelop.dir.mode = static_cast<DirMode>(dir.mode);
+        for (int d = 0; d < 3; ++d) {
+            for (int r = 0; r < 3; ++r) p.filmDevelop.dir.M[d * 3 + r] = dir.matrix_rgb[(2 - d) * 3 + (2 - r)];
+            p.filmDevelop.dir.dMax[d] = dir.density_max_rgb[2 - d];
+            p.filmDevelop.dir.dRef[d] = dir.density_ref_rgb[2 - d];
+            p.filmDevelop.dir.donorK[d] = dir.donor_k_rgb[2 - d];
+            p.filmDevelop.dir.receiverCRef[d] = dir.receiver_c_ref_rgb[2 - d];
+            p.filmDevelop.dir.receiverKr[d] = dir.receiver_kr_rgb[2 - d];
+        }
+        p.filmDevelop.dirDensB = curve(a.put(dir.compensated_axes_rgb[2].data, n), yB, n);
+        p.filmDevelop.dirDensG = curve(a.put(dir.compensated_axes_rgb[1].data, n), yG, n);
+        p.filmDevelop.dirDensR = curve(a.put(dir.compensated_axes_rgb[0].data, n), yR, n);
+    }
+    const bool print = h.route == FJ_ROUTE_NEGATIVE_PRINT || h.route == FJ_ROUTE_POSITIVE_PRINT;
+    if (print) {
+        const FjPrint& pr = h.print;
+        p.printExpose.active = 1;
+        auto& nt = p.printExpose.negTables;
+        nt.epsC = a.column(pr.film_density_cmy.data, 81, 3, 0);
+        nt.epsM = a.column(pr.film_density_cmy.data, 81, 3, 1);
+        nt.epsY = a.column(pr.film_density_cmy.data, 81, 3, 2);
+        nt.baseDensityMin = a.put(pr.film_base_density.data, 81);
+        nt.K = 81;
+        nt.hasBaseline = 1;
+        nt.invYn = 1.0f;
+        p.printExpose.printIllumFiltered = a.put(pr.main_illuminant.data, 81);
+        p.printExpose.printIllumK = 81;
+        p.printExpose.printSensC = curve(nullptr, a.column(pr.sensitivity_cmy.data, 81, 3, 0), 81);
+        p.printExpose.printSensM = curve(nullptr, a.column(pr.sensitivity_cmy.data, 81, 3, 1), 81);
+        p.printExpose.printSensY = curve(nullptr, a.column(pr.sensitivity_cmy.data, 81, 3, 2), 81);
+        p.printExpose.printExposure = pr.exposure;
+        p.printExpose.routeCorrectionScale = h.scanner_correction.exposure_scale;
+        const bool pf = (pr.flags & FJ_PRINT_PREFLASH) != 0;
+        p.printExpose.printPreflashExposure = pf ? pr.preflash_exposure : 0.0f;
+        p.printExpose.printMidgrayFactor = pr.normalizer;
+        for (int c = 0; c < 3; ++c) p.printExpose.printPreflashRaw[c] = pf ? pr.preflash_raw_cmy[c] : 0.0f;
+        const int np = (int)pr.log_exposure.count;
+        const float* px = a.put(pr.log_exposure.data, np);
+        p.printDevelop.printDcC = curve(px, a.column(pr.density_cmy.data, np, 3, 0), np);
+        p.printDevelop.printDcM = curve(px, a.column(pr.density_cmy.data, np, 3, 1), np);
+        p.printDevelop.printDcY = curve(px, a.column(pr.density_cmy.data, np, 3, 2), np);
+    }
+    auto& sc = p.scanStage;
+    const int r = (int)h.scanner_lut.resolution;
+    const size_t nodes = (size_t)r * r * r * 3, cells = (size_t)(r - 1) * (r - 1) * (r - 1) * 3;
+    sc.scanLutLog2PchipXYZ = a.put(lut[0], nodes);
+    sc.scanLutPchipSlopeC = a.put(lut[1], nodes);
+    sc.scanLutPchipSlopeM = a.put(lut[2], nodes);
+    sc.scanLutPchipSlopeY = a.put(lut[3], nodes);
+    sc.scanLutPchipCellMin = a.put(lut[4], cells);
+    sc.scanLutPchipCellMax = a.put(lut[5], cells);
+    sc.scanLutRes = r;
+    sc.densityRange.mediumIsNegative = print ? 0 : 1;
+    for (int c = 0; c < 3; ++c) {
+        sc.densityRange.min_cmy[c] = print ? h.scanner_bounds.min_cmy[c] : -h.scanner_bounds.min_cmy[c];
+        sc.densityRange.inv_max_cmy[c] = h.scanner_bounds.inv_span_cmy[c];
+    }
+    const FjOutputColor& oc = h.output_color;
+    std::memcpy(sc.scanColor.cat02, oc.cat02, 36);
+    std::memcpy(sc.scanColor.xyzToRgb, oc.xyz_to_rgb, 36);
+    std::memcpy(sc.scanColor.illuminantXYZ, oc.illuminant_xyz, 12);
+    if (oc.flags & FJ_COLOR_GAMUT_COMPRESSION) {
+        sc.scanColor.outputGamutCmax = a.put(oc.gamut_cmax.data, oc.gamut_cmax.count);
+        std::memcpy(sc.scanColor.outputGamutNativeRgbToD65Xyz, oc.native_rgb_to_d65_xyz, 36);
+        std::memcpy(sc.scanColor.outputGamutD65XyzToNativeRgb, oc.d65_xyz_to_native_rgb, 36);
+        std::memcpy(sc.scanColor.outputGamutOklabXyzToLms, Gamut::kOklabXyzToLms.data(), 36);
+        std::memcpy(sc.scanColor.outputGamutOklabLmsToXyz, Gamut::kOklabLmsToXyz.data(), 36);
+        std::memcpy(sc.scanColor.outputGamutOklabLmsRootToLab, Gamut::kOklabLmsRootToLab.data(), 36);
+        std::memcpy(sc.scanColor.outputGamutOklabLabToLmsRoot, Gamut::kOklabLabToLmsRoot.data(), 36);
+        std::memcpy(sc.scanColor.outputGamutLightnessKnee, oc.lightness_knee, 12);
+        std::memcpy(sc.scanColor.outputGamutChromaKnee, oc.chroma_knee, 12);
+        sc.scanColor.outputGamutActive = 1;
+    }
+    sc.scanColor.encoding.outputColorSpaceIndex = (int)oc.color_space;
+    sc.scanColor.encoding.applyCctfEncoding = (oc.flags & FJ_COLOR_ENCODE_CCTF) ? 1 : 0;
+    sc.scanColor.encoding.inputIsOutputSpace = (oc.flags & FJ_COLOR_INPUT_IS_OUTPUT_SPACE) ? 1 : 0;
+    sc.scanColor.encoding.cctf.kind = (int)oc.encoding.cctf_kind;
+    sc.scanColor.encoding.cctf.gamma = oc.encoding.gamma;
+    sc.scanColor.encoding.cctf.a = oc.encoding.a;
+    sc.scanColor.encoding.cctf.b = oc.encoding.b;
+    sc.scanColor.encoding.cctf.c = oc.encoding.c;
+    sc.scanColor.encoding.cctf.d = oc.encoding.d;
+    sc.scanColor.encoding.cctf.linearCutoff = oc.encoding.linear_cutoff;
+    std::memcpy(sc.scanColor.encoding.dwgToOutput, oc.encoding.dwg_to_output, 36);
+    sc.correctionActive = (h.scanner_correction.flags & FJ_CORRECTION_ACTIVE) ? 1 : 0;
+    sc.correctionSlope = h.scanner_correction.xyz_slope;
+    sc.correctionOffset = h.scanner_correction.xyz_offset;
+    sc.scanErrorFlag = reinterpret_cast<int*>(d_flags);
+    return true;
+}
+
+} // namespace
+
+// Renders with the reference kernels. src/dst are device pointers; lut holds the six
+// host arrays of the scanner LUT. Synchronous. Returns a cudaError_t value.
+extern "C" int ref_render(const FjPreparedHostData* h, const float* const* lut, const float* src,
+                          long src_row_bytes, float* dst, long dst_row_bytes, int width, int height, int comps,
+                          unsigned* flags_out) {
+    Arena a;
+    unsigned* d_flags = nullptr;
+    if (cudaMalloc(&d_flags, sizeof(unsigned)) != cudaSuccess) return 2;
+    cudaMemset(d_flags, 0, sizeof(unsigned));
+    a.ptrs.push_back(d_flags);
+    JuicerCuda::PipelineRunParams p;
+    if (!pack(*h, lut, a, p, d_flags)) return 1;
+    p.src = src;
+    p.srcRowBytes = (size_t)src_row_bytes;
+    p.dst = dst;
+    p.dstRowBytes = (size_t)dst_row_bytes;
+    p.width = width;
+    p.height = height;
+    p.nComponents = comps;
+    cudaError_t e = p.printExpose.active ? juicer_cuda_print_pipeline(&p, nullptr)
+                                         : juicer_cuda_negative_pipeline(&p, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    unsigned f = 0;
+    cudaMemcpy(&f, d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (flags_out) *flags_out = f;
+    return (int)e;
+}
+
+// Capture density (C, M, Y planes) with the reference kernel.
+extern "C" int ref_capture_density(const FjPreparedHostData* h, const float* const* lut, const float* src,
+                                   long src_row_bytes, int width, int height, int comps, float* c, float* m,
+                                   float* y) {
+    Arena a;
+    unsigned* d_flags = nullptr;
+    if (cudaMalloc(&d_flags, sizeof(unsigned)) != cudaSuccess) return 2;
+    cudaMemset(d_flags, 0, sizeof(unsigned));
+    a.ptrs.push_back(d_flags);
+    JuicerCuda::PipelineRunParams p;
+    if (!pack(*h, lut, a, p, d_flags)) return 1;
+    JuicerCuda::PrintPipelineRunParams q{};
+    q.src = src;
+    q.srcRowBytes = (size_t)src_row_bytes;
+    q.dst = c; // unused by the capture kernel but must be non-null for some guards
+    q.dstRowBytes = (size_t)src_row_bytes;
+    q.width = width;
+    q.height = height;
+    q.nComponents = comps;
+    q.filmExpose = p.filmExpose;
+    q.filmDevelop = p.filmDevelop;
+    q.printExpose = p.printExpose;
+    q.printDevelop = p.printDevelop;
+    q.scanStage = p.scanStage;
+    q.filmRaw = p.filmRaw;
+    cudaError_t e = juicer_cuda_print_focused_capture_density(&q, c, m, y, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return (int)e;
+}

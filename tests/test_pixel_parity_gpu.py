@@ -119,9 +119,11 @@ def test_carrier_path_matches_oracle(torch_cuda, device_recipes, prepare, oracle
 
 
 def test_dir_failure_sets_deferred_flag(torch_cuda, recipes, prepare, oracle):
-    """An invalid donor knee makes every DIR evaluation fail: bit 8 plus the channel
-    mask is raised (src/Cuda/JuicerCudaDeviceHelpers.cuh:1195-1204), the pixel's density
-    becomes NaN and the scan then reports failure (bit 0) and writes black."""
+    """An invalid donor knee on the green layer makes its Langmuir term fail; the NaN
+    donor then reaches every receiver through the coupler matrix, so bit 8 plus the
+    full B,G,R channel mask is raised (src/Cuda/JuicerCudaDeviceHelpers.cuh:1125-1204),
+    the pixel's density becomes NaN and the scan reports failure (bit 0), writing
+    black."""
     torch = torch_cuda
     from film_juicer_b200 import runtime
 
@@ -136,7 +138,7 @@ def test_dir_failure_sets_deferred_flag(torch_cuda, recipes, prepare, oracle):
     flags = dr.read_flags()
     ref, rflags = oracle.render(rec, src)
     assert flags == rflags
-    assert flags & (1 << 8) and (flags >> 9) & 7 == 0b010 and flags & 1
+    assert flags & (1 << 8) and (flags >> 9) & 7 == 0b111 and flags & 1
     assert np.array_equal(d.cpu().numpy(), ref)
     dr.close()
 
