@@ -243,6 +243,23 @@ FjStatus fjb_render_from_density(FjbRecipe* recipe, const float* density_c, cons
     return launch_stage(recipe, p, fjb::PixelStage::DensityToOutput, stream, error);
 }
 
+FjStatus fjb_auto_exposure(FjbRecipe* recipe, const float* src, ptrdiff_t src_row_bytes, uint32_t components,
+                           const FjAutoExposure* meter, float* device_scale, void* stream, FjErrorBuffer* error) {
+    if (!recipe || !src || !meter || !device_scale) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    fjb::MeterSpec m{};
+    std::string why;
+    if (!valid_components(components) || !fjb::meter_spec_from(*meter, m, why))
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, why.empty() ? "components" : why);
+    fjb::PixelParams p = recipe->r.params;
+    p.src = reinterpret_cast<const char*>(src);
+    p.src_row_bytes = src_row_bytes;
+    p.components = (int)components;
+    cudaError_t e = fjb::launch_auto_exposure(p, m, recipe->r.meter_scratch, device_scale, as_stream(stream));
+    if (e != cudaSuccess) return cuda_status(e, error, "auto exposure launch");
+    write_error(error, "");
+    return ok_status();
+}
+
 FjStatus fjb_scanner_lut_build_host(const FjbScannerLutInput* in, float* log2_xyz, float* slope_c, float* slope_m,
                                     float* slope_y, float* cell_min, float* cell_max, FjErrorBuffer* error) {
     try {

@@ -61,4 +61,33 @@ struct ScannerLutDevice {
 
 cudaError_t launch_scanner_lut_build(const ScannerLutSpec& spec, const ScannerLutDevice& out, cudaStream_t stream);
 
+// Auto-exposure metering (FJ_METER_* numbering).
+enum MeterMethod : int {
+    kMeterCenterWeighted = 0,
+    kMeterAverage = 1,
+    kMeterMedian = 2,
+    kMeterPartial = 3,
+    kMeterMatrix = 4,
+    kMeterMultiZone = 5,
+    kMeterHighlightWeighted = 6,
+};
+constexpr int kMeterBlocks = 148; // one CTA per SM at most
+
+// Preview metering grid: `source` is the image's bounds, `meter` the metered window,
+// preview_* the sample grid laid over the meter window (reference
+// src/Cuda/JuicerCudaResources.h:169-184). p.src points at pixel (source_x1, source_y1).
+struct MeterSpec {
+    int source_x1, source_y1, source_x2, source_y2;
+    int meter_x1, meter_y1, meter_x2, meter_y2;
+    int preview_width, preview_height;
+    int method;
+};
+
+size_t meter_scratch_bytes();
+// Writes the exposure scale (float, device) for the frame. `scratch` holds
+// meter_scratch_bytes() of device memory whose ticket word must be zero on entry (the
+// kernel leaves it zero again).
+cudaError_t launch_auto_exposure(const PixelParams& p, const MeterSpec& m, void* scratch, float* scale,
+                                 cudaStream_t stream);
+
 } // namespace fjb

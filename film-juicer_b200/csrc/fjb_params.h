@@ -28,15 +28,20 @@ struct CurveRef {
     int x;   // offset of the ascending abscissa
     int y;   // offset of the ordinate
     int n;   // sample count (accepted domain is [0, n-1])
+    int guess;    // 1: the abscissa is strictly increasing and close to uniform
+    float x0;     // first abscissa
+    float inv_dx; // (n - 1) / (x[n-1] - x[0])
 };
 
 // Print 81-lambda coefficients, pre-folded on the host:
-//   dens[l] = (eps_c, eps_m, eps_y, base) * log2(10)
+//   nd[l]   = -(eps_c, eps_m, eps_y, base) * log2(10)   (so T = 2^(D . nd))
 //   sens[l] = (sens_c, sens_m, sens_y) * filtered illuminant
-// Wavelengths whose three sensitivities are all NaN are dropped; a NaN channel of a
-// kept wavelength contributes zero.
+// Wavelengths whose three sensitivities are all NaN are dropped and the remaining
+// ones packed first; the unused tail slots hold (0, 0, 0, -inf) and zero
+// sensitivities, so they contribute exactly +0 for finite densities. A NaN channel of
+// a kept wavelength contributes zero.
 struct PrintSpectral {
-    float dens[kSpectralSamples][4];
+    float nd[kSpectralSamples][4];
     float sens[kSpectralSamples][3];
     int count;
 };

@@ -96,6 +96,32 @@ __device__ __forceinline__ int tc_reflect(int i) {
     return i;
 }
 
+// Footprints that touch the LUT border reflect their indices (cold path, out of line).
+static __device__ __noinline__ void tc_lut_edge(const float4* __restrict__ lut, int cb, int mb, float cf, float mf,
+                                         float acc[3], float& wsum) {
+    const float wc[4] = {mitchell(cf + 1.0f), mitchell(cf), mitchell(cf - 1.0f), mitchell(cf - 2.0f)};
+    const float wm[4] = {mitchell(mf + 1.0f), mitchell(mf), mitchell(mf - 1.0f), mitchell(mf - 2.0f)};
+    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, ws = 0.0f;
+#pragma unroll
+    for (int dc = 0; dc < 4; ++dc) {
+        const int c = tc_reflect(cb - 1 + dc);
+#pragma unroll
+        for (int dm = 0; dm < 4; ++dm) {
+            const int m = tc_reflect(mb - 1 + dm);
+            const float w = wc[dc] * wm[dm];
+            ws += w;
+            const float4 t = __ldg(lut + c * kTcLutExtent + m);
+            a0 += w * t.x;
+            a1 += w * t.y;
+            a2 += w * t.z;
+        }
+    }
+    acc[0] = a0;
+    acc[1] = a1;
+    acc[2] = a2;
+    wsum = ws;
+}
+
 // All three channels of one tap come from one 16-byte load.
 __device__ __forceinline__ void tc_lut_sample(const float4* __restrict__ lut, float qx, float qy, float rgb[3]) {
     int cb, mb;
@@ -106,19 +132,24 @@ __device__ __forceinline__ void tc_lut_sample(const float4* __restrict__ lut, fl
     const float wm[4] = {mitchell(mf + 1.0f), mitchell(mf), mitchell(mf - 1.0f), mitchell(mf - 2.0f)};
     float acc[3] = {0.0f, 0.0f, 0.0f};
     float wsum = 0.0f;
+    if (cb >= 1 && cb <= kTcLutExtent - 3 && mb >= 1 && mb <= kTcLutExtent - 3) {
+        // Interior cell: the 4x4 footprint needs no reflection; one base pointer with
+        // compile-time offsets.
+        const float4* base = lut + (cb - 1) * kTcLutExtent + (mb - 1);
 #pragma unroll
-    for (int dc = 0; dc < 4; ++dc) {
-        const int c = tc_reflect(cb - 1 + dc);
+        for (int dc = 0; dc < 4; ++dc) {
 #pragma unroll
-        for (int dm = 0; dm < 4; ++dm) {
-            const int m = tc_reflect(mb - 1 + dm);
-            const float w = wc[dc] * wm[dm];
-            wsum += w;
-            const float4 t = __ldg(lut + c * kTcLutExtent + m);
-            acc[0] += w * t.x;
-            acc[1] += w * t.y;
-            acc[2] += w * t.z;
+            for (int dm = 0; dm < 4; ++dm) {
+                const float w = wc[dc] * wm[dm];
+                wsum += w;
+                const float4 t = __ldg(base + dc * kTcLutExtent + dm);
+                acc[0] += w * t.x;
+                acc[1] += w * t.y;
+                acc[2] += w * t.z;
+            }
         }
+    } else {
+        tc_lut_edge(lut, cb, mb, cf, mf, acc, wsum);
     }
     for (int k = 0; k < 3; ++k) rgb[k] = wsum != 0.0f ? acc[k] / wsum : 0.0f;
 }
@@ -160,7 +191,7 @@ __device__ __forceinline__ void tc_exposure(const PixelParams& p, const float in
 // ---------------------------------------------------------------------------
 // a3: Mallett 2019 81-lambda basis exposure (src/Cuda/JuicerCudaDeviceHelpers.cuh:619-668)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void mallett_exposure(const PixelParams& p, const float in[3], float e_bgr[3]) {
+static __device__ __noinline__ void mallett_exposure(const PixelParams& p, const float in[3], float e_bgr[3]) {
     float lin[3], xyz[3], ad[3], srgb[3];
     decode_input(p, in, lin);
     mat3_apply(p.input_rgb_to_xyz, lin, xyz);
@@ -229,17 +260,9 @@ __device__ __forceinline__ void camera_linear_exposure(const PixelParams& p, con
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float log_exposure(float e) { return log10f(fmaxf(e, 0.0f) + 1e-10f); }
 
-__device__ __forceinline__ float curve_sample(const float* __restrict__ blob, CurveRef c, float logE, float gamma) {
-    if (!isfinite(logE)) return nanf("");
-    const float* x = blob + c.x;
-    const float* y = blob + c.y;
-    const int last = c.n - 1;
-    const float xq = logE * gamma;
-    const float xmin = x[0];
-    const float xmax = x[last];
-    if (!(xmax >= xmin)) return y[0];
-    if (xq <= xmin) return y[0];
-    if (xq >= xmax) return y[last];
+// First index i1 in [1, last] with xq < x[i1] (last + 1 when none): the reference's
+// binary search (src/Cuda/JuicerCudaDeviceHelpers.cuh:59-71).
+static __device__ __noinline__ int curve_interval_search(const float* x, int last, float xq) {
     int lo = 1, hi = last, i1 = last + 1;
     while (lo <= hi) {
         const int mid = lo + ((hi - lo) >> 1);
@@ -250,6 +273,41 @@ __device__ __forceinline__ float curve_sample(const float* __restrict__ blob, Cu
             lo = mid + 1;
         }
     }
+    return i1;
+}
+
+__device__ __forceinline__ float curve_sample(const float* __restrict__ blob, const CurveRef& c, float logE,
+                                              float gamma) {
+    if (!isfinite(logE)) return nanf("");
+    const float* x = blob + c.x;
+    const float* y = blob + c.y;
+    const int last = c.n - 1;
+    const float xq = logE * gamma;
+    const float xmin = x[0];
+    const float xmax = x[last];
+    if (!(xmax >= xmin)) return y[0];
+    if (xq <= xmin) return y[0];
+    if (xq >= xmax) return y[last];
+    int i1 = last + 1;
+    bool found = false;
+    if (c.guess) {
+        // Strictly increasing, near-uniform abscissa: start from the uniform-grid cell
+        // and step to the unique i1 with x[i1-1] <= xq < x[i1] (the interval the
+        // reference's binary search selects). Two steps either way cover the spacing
+        // jitter the host admitted; otherwise fall through to the binary search.
+        int g = (int)((xq - c.x0) * c.inv_dx);
+        g = g < 0 ? 0 : (g > last - 1 ? last - 1 : g);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (g > 0 && xq < x[g]) --g;
+            if (g < last - 1 && xq >= x[g + 1]) ++g;
+        }
+        if (x[g] <= xq && xq < x[g + 1]) {
+            i1 = g + 1;
+            found = true;
+        }
+    }
+    if (!found) i1 = curve_interval_search(x, last, xq);
     if (i1 > last) return y[last];
     const int i0 = i1 - 1;
     const float x0 = x[i0], x1 = x[i1], y0 = y[i0], y1 = y[i1];
@@ -270,17 +328,9 @@ __device__ __forceinline__ float clamp_infinite_log(const float* __restrict__ bl
 // ---------------------------------------------------------------------------
 // a6: DIR coupler chemistry (src/Cuda/JuicerCudaDeviceHelpers.cuh:1073-1265)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool langmuir(float value, float knee, float ref, float& out) {
-    out = nanf("");
-    if (!isfinite(value) || !isfinite(knee) || !(knee > 0.0f) || !isfinite(ref)) return false;
-    const float den = knee + value;
-    const float kr = knee + ref;
-    const bool direct = isfinite(den) && den != 0.0f && isfinite(kr) &&
-                        (value == 0.0f || fabsf(value) <= FLT_MAX / fabsf(kr));
-    if (direct) {
-        out = value * kr / den;
-        return isfinite(out);
-    }
+// Overflow-safe evaluation of the Langmuir term when the direct product could
+// overflow or hit the receiver pole (cold path, kept out of line).
+static __device__ __noinline__ bool langmuir_guarded(float value, float knee, float ref, float den, float& out) {
     const float num_scale = 1.0f + ref / knee;
     if (!isfinite(num_scale)) return false;
     if (value >= 0.0f) {
@@ -298,6 +348,20 @@ __device__ __forceinline__ bool langmuir(float value, float knee, float ref, flo
         out = (value / den_scale) * num_scale;
     }
     return isfinite(out);
+}
+
+__device__ __forceinline__ bool langmuir(float value, float knee, float ref, float& out) {
+    out = nanf("");
+    if (!isfinite(value) || !isfinite(knee) || !(knee > 0.0f) || !isfinite(ref)) return false;
+    const float den = knee + value;
+    const float kr = knee + ref;
+    const bool direct = isfinite(den) && den != 0.0f && isfinite(kr) &&
+                        (value == 0.0f || fabsf(value) <= FLT_MAX / fabsf(kr));
+    if (direct) {
+        out = value * kr / den;
+        return isfinite(out);
+    }
+    return langmuir_guarded(value, knee, ref, den, out);
 }
 
 // Donor corrections for layer densities (B, G, R); returns a channel failure mask.
@@ -426,13 +490,21 @@ __device__ __forceinline__ void develop_capture_spatial(const PixelParams& p, co
 // a8: enlarger print exposure + development (src/Cuda/JuicerCudaDeviceHelpers.cuh:860-1071)
 // The 81-wavelength coefficients are read straight from the constant bank.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void print_spectral(const PrintSpectral& s, const float d[3], float raw[3]) {
+// 2^x on the MUFU (ex2.approx.ftz.f32: relative error about 2^-22, flushes subnormal
+// results to zero; transmittances here are >= 2^-40, far above the subnormal range).
+__device__ __forceinline__ float mufu_exp2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Non-finite density (a failed DIR pixel): the reference's per-sample NaN rule
+// (src/Cuda/JuicerCudaDeviceHelpers.cuh:856-864). Cold path, out of line.
+static __device__ __noinline__ void print_spectral_nonfinite(const PrintSpectral& s, const float d[3], float raw[3]) {
     float ac = 0.0f, am = 0.0f, ay = 0.0f;
-#pragma unroll
-    for (int i = 0; i < kSpectralSamples; ++i) {
-        if (i >= s.count) break;
-        const float dl = d[0] * s.dens[i][0] + d[1] * s.dens[i][1] + d[2] * s.dens[i][2] + s.dens[i][3];
-        float t = exp2f(-dl);
+    for (int i = 0; i < s.count; ++i) {
+        const float dl = d[0] * s.nd[i][0] + d[1] * s.nd[i][1] + d[2] * s.nd[i][2] + s.nd[i][3];
+        float t = exp2f(dl);
         t = isnan(t) ? 0.0f : t;
         ac += t * s.sens[i][0];
         am += t * s.sens[i][1];
@@ -441,6 +513,31 @@ __device__ __forceinline__ void print_spectral(const PrintSpectral& s, const flo
     raw[0] = ac;
     raw[1] = am;
     raw[2] = ay;
+}
+
+__device__ __forceinline__ void print_spectral(const PrintSpectral& s, const float d[3], float raw[3]) {
+    if (isfinite(d[0]) && isfinite(d[1]) && isfinite(d[2])) {
+        // Fast path: all 81 slots unrolled, coefficients are constant-bank operands.
+        // Finite densities give finite exponents, so no NaN guard is needed; padded
+        // slots evaluate 2^-inf * 0 = +0. Two partial sums per channel (even / odd
+        // wavelength) halve the dependent FMA chain.
+        float a0[3] = {0.0f, 0.0f, 0.0f}, a1[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int i = 0; i < kSpectralSamples; ++i) {
+            const float dl = fmaf(d[0], s.nd[i][0], fmaf(d[1], s.nd[i][1], fmaf(d[2], s.nd[i][2], s.nd[i][3])));
+            const float t = mufu_exp2(dl);
+            float* a = (i & 1) ? a1 : a0;
+            a[0] = fmaf(t, s.sens[i][0], a[0]);
+            a[1] = fmaf(t, s.sens[i][1], a[1]);
+            a[2] = fmaf(t, s.sens[i][2], a[2]);
+        }
+        const float ac = a0[0] + a1[0], am = a0[1] + a1[1], ay = a0[2] + a1[2];
+        raw[0] = ac;
+        raw[1] = am;
+        raw[2] = ay;
+    } else {
+        print_spectral_nonfinite(s, d, raw);
+    }
 }
 
 __device__ __forceinline__ void print_develop(const PixelParams& p, const float* __restrict__ blob, float d[3]) {
@@ -614,7 +711,18 @@ __device__ __forceinline__ double clamp01(double v) {
     return v;
 }
 
+static __device__ __noinline__ float encode_channel_other(const PixelParams& p, float v);
+
 __device__ __forceinline__ float encode_channel(const PixelParams& p, float v) {
+    if (p.cctf_kind == 2) {
+        if (v <= 0.0031308f) return 12.92f * v;
+        return 1.055f * powf(v, 1.0f / 2.4f) - 0.055f;
+    }
+    return encode_channel_other(p, v);
+}
+
+// The other transfer functions, out of line to keep the hot kernel's code small.
+static __device__ __noinline__ float encode_channel_other(const PixelParams& p, float v) {
     switch (p.cctf_kind) {
         case 0:
             return v;

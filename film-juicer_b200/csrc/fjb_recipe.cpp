@@ -43,12 +43,31 @@ cudaError_t upload(T** dst, const void* src, size_t bytes, cudaStream_t stream) 
     return cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream);
 }
 
+// Enables the uniform-grid interval guess for a curve whose abscissa is strictly
+// increasing with every step within 25 % of the mean step (then the guessed cell is
+// at most one off and two correction steps always land on the exact interval).
+void set_curve_guess(const std::vector<float>& blob, CurveRef& c) {
+    c.guess = 0;
+    if (c.n < 2) return;
+    const float* x = blob.data() + c.x;
+    const double span = (double)x[c.n - 1] - (double)x[0];
+    if (!(span > 0.0) || !std::isfinite(span)) return;
+    const double mean = span / (c.n - 1);
+    for (int i = 0; i + 1 < c.n; ++i) {
+        const double d = (double)x[i + 1] - (double)x[i];
+        if (!(d > 0.0) || std::fabs(d - mean) > 0.25 * mean) return;
+    }
+    c.x0 = x[0];
+    c.inv_dx = (float)((c.n - 1) / span);
+    c.guess = 1;
+}
+
 } // namespace
 
 void Recipe::release() noexcept {
     void* ptrs[] = {curves, tc_lut, mallett_basis, mallett_illum, film_sens_bgr, gamut_cmax, flags,
                     lut.nodes, lut.log2_xyz, lut.slope_c, lut.slope_m, lut.slope_y, lut.cell_min, lut.cell_max,
-                    lut.packed_nodes, lut.packed_cells, lut.failure, lut_spectra};
+                    lut.packed_nodes, lut.packed_cells, lut.failure, lut_spectra, meter_scratch};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     curves = nullptr;
@@ -284,14 +303,22 @@ bool create_recipe(const FjPreparedHostData& h, cudaStream_t stream, Recipe& r, 
                                     pr.sensitivity_cmy.data[l * 3 + 2]};
                 if (std::isnan(s[0]) && std::isnan(s[1]) && std::isnan(s[2])) continue;
                 const float il = pr.main_illuminant.data[l];
-                for (int c = 0; c < 3; ++c) p.spectral.dens[count][c] = pr.film_density_cmy.data[l * 3 + c] * kLog2Of10;
-                p.spectral.dens[count][3] = pr.film_base_density.data[l] * kLog2Of10;
+                for (int c = 0; c < 3; ++c) p.spectral.nd[count][c] = -(pr.film_density_cmy.data[l * 3 + c] * kLog2Of10);
+                p.spectral.nd[count][3] = -(pr.film_base_density.data[l] * kLog2Of10);
                 for (int c = 0; c < 3; ++c)
                     p.spectral.sens[count][c] = (std::isnan(s[c]) || std::isnan(il)) ? 0.0f : s[c] * il;
                 ++count;
             }
             p.spectral.count = count;
+            for (int l = count; l < kSpectralSamples; ++l) {
+                p.spectral.nd[l][0] = p.spectral.nd[l][1] = p.spectral.nd[l][2] = 0.0f;
+                p.spectral.nd[l][3] = -INFINITY;
+                p.spectral.sens[l][0] = p.spectral.sens[l][1] = p.spectral.sens[l][2] = 0.0f;
+            }
         }
+        for (CurveRef* c : {&p.film_curve[0], &p.film_curve[1], &p.film_curve[2], &p.dir_curve[0], &p.dir_curve[1],
+                            &p.dir_curve[2], &p.print_curve[0], &p.print_curve[1], &p.print_curve[2]})
+            set_curve_guess(blob, *c);
         while (blob.size() % 4) blob.push_back(0.0f);
         if ((e = upload(&r.curves, blob.data(), blob.size() * 4, stream)) != cudaSuccess) goto cuda_fail;
         p.curve_blob = r.curves;
@@ -385,6 +412,8 @@ bool create_recipe(const FjPreparedHostData& h, cudaStream_t stream, Recipe& r, 
         p.cctf_linear_cutoff = oc.encoding.linear_cutoff;
     }
 
+    if ((e = cudaMalloc(&r.meter_scratch, meter_scratch_bytes())) != cudaSuccess) goto cuda_fail;
+    if ((e = cudaMemsetAsync(r.meter_scratch, 0, meter_scratch_bytes(), stream)) != cudaSuccess) goto cuda_fail;
     if ((e = cudaMalloc(&r.flags, sizeof(unsigned))) != cudaSuccess) goto cuda_fail;
     if ((e = cudaMemsetAsync(r.flags, 0, sizeof(unsigned), stream)) != cudaSuccess) goto cuda_fail;
     p.error_flags = r.flags;

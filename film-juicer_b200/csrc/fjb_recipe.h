@@ -39,11 +39,35 @@ struct Recipe {
     float* gamut_cmax = nullptr;
     unsigned* flags = nullptr;
     double* lut_spectra = nullptr;
+    void* meter_scratch = nullptr; // auto-exposure partial sums + ticket
     ScannerLutDevice lut{};
     void release() noexcept;
 };
 
 bool create_recipe(const FjPreparedHostData& h, cudaStream_t stream, Recipe& r, std::string& why, FjStatus& status);
+
+// FjAutoExposure -> metering grid; false (with a reason) for rejected records:
+// median metering, empty preview or meter window, meter window outside the source.
+inline bool meter_spec_from(const FjAutoExposure& a, MeterSpec& m, std::string& why) {
+    if (a.method == FJ_METER_MEDIAN) {
+        why = "median metering is not supported";
+        return false;
+    }
+    if (a.method > FJ_METER_HIGHLIGHT_WEIGHTED) {
+        why = "unknown metering method";
+        return false;
+    }
+    if (a.preview_width <= 0 || a.preview_height <= 0 || a.meter_bounds.x2 <= a.meter_bounds.x1 ||
+        a.meter_bounds.y2 <= a.meter_bounds.y1 || a.source_bounds.x2 <= a.source_bounds.x1 ||
+        a.source_bounds.y2 <= a.source_bounds.y1) {
+        why = "auto exposure preview or meter window is empty";
+        return false;
+    }
+    m = MeterSpec{a.source_bounds.x1, a.source_bounds.y1, a.source_bounds.x2, a.source_bounds.y2,
+                  a.meter_bounds.x1,  a.meter_bounds.y1,  a.meter_bounds.x2,  a.meter_bounds.y2,
+                  a.preview_width,    a.preview_height,   (int)a.method};
+    return true;
+}
 
 cudaError_t alloc_scanner_lut(int r, ScannerLutDevice& lut);
 void free_scanner_lut(ScannerLutDevice& lut);

@@ -161,3 +161,29 @@ def scanner_lut_build_host(inp: "abi.FjbScannerLutInput"):
     st = lib.fjb_scanner_lut_build_host(C.byref(inp), *[C.c_void_p(o.ctypes.data) for o in outs], C.byref(err.buf))
     _check("fjb_scanner_lut_build_host", st, err)
     return outs
+
+
+def meter_record(width: int, height: int, *, method: int = 0, preview: tuple[int, int] | None = None,
+                 meter: tuple[int, int, int, int] | None = None) -> "abi.FjAutoExposure":
+    """FjAutoExposure over a width x height source (preview long edge <= 256, as the host uses)."""
+    m = abi.FjAutoExposure()
+    m.source_bounds = abi.FjRect(0, 0, width, height)
+    mx1, my1, mx2, my2 = meter if meter is not None else (0, 0, width, height)
+    m.meter_bounds = abi.FjRect(mx1, my1, mx2, my2)
+    if preview is None:
+        mw, mh = mx2 - mx1, my2 - my1
+        s = min(1.0, 256.0 / max(mw, mh))
+        preview = (max(1, int(round(mw * s))), max(1, int(round(mh * s))))
+    m.preview_width, m.preview_height = preview
+    m.method = method
+    m.hash = 1
+    return m
+
+
+def auto_exposure(recipe: "DeviceRecipe", src, meter: "abi.FjAutoExposure", scale_out, stream=None):
+    """Meters `src` (CUDA tensor H x W x comps) into the device float `scale_out`."""
+    err = abi.ErrorText()
+    st = recipe.lib.fjb_auto_exposure(recipe.handle, C.c_void_p(_ptr(src)), src.stride(0) * 4, src.shape[2],
+                                      C.byref(meter), C.c_void_p(_ptr(scale_out)), C.c_void_p(_stream_handle(stream)),
+                                      C.byref(err.buf))
+    _check("fjb_auto_exposure", st, err)

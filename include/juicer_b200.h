@@ -76,6 +76,16 @@ FjStatus fjb_render_from_density(FjbRecipe* recipe, const float* density_c, cons
                                  ptrdiff_t dst_row_bytes, int32_t width, int32_t height, uint32_t components,
                                  void* stream, FjErrorBuffer* error);
 
+/* Camera auto-exposure metering (reference src/Cuda/JuicerCudaAutoExposure.cu:314-520,
+ * run by src/Cuda/JuicerCudaExecutor.cpp:1013 meter_camera_exposure). `src` points at
+ * pixel (meter->source_bounds.x1, .y1). Writes the float exposure scale 2^-log2(Y) to
+ * the device address `device_scale`; pass that address to
+ * fjb_recipe_set_exposure_scale_device so later stages of the frame read it. Uses
+ * scratch memory owned by the recipe, so calls on one recipe must not overlap.
+ * FJ_METER_MEDIAN is rejected (FJ_STATUS_UNSUPPORTED_INPUT), as in the reference. */
+FjStatus fjb_auto_exposure(FjbRecipe* recipe, const float* src, ptrdiff_t src_row_bytes, uint32_t components,
+                           const FjAutoExposure* meter, float* device_scale, void* stream, FjErrorBuffer* error);
+
 /* Scanner LUT input record (reference native/juicer_cuda_frame_values.h FjScannerLutInput). */
 typedef struct FjbScannerLutInput {
     FjFloatSpan eps_c, eps_m, eps_y;

@@ -830,3 +830,131 @@ int oracle_render(const FjPreparedHostData* h, int stage, const float* src, long
     if (flags_out) *flags_out = flags;
     return 0;
 }
+
+/* ---------------- auto exposure (src/Cuda/JuicerCudaAutoExposure.cu:63-141, :266-520) ---------------- */
+
+static int preview_coord(int i, int preview, int source) {
+    if (preview <= 0 || source <= 0) return 0;
+    long long num = (2LL * i + 1LL) * (long long)source;
+    int c = (int)(num / (2LL * preview));
+    return c < 0 ? 0 : (c > source - 1 ? source - 1 : c);
+}
+
+static void meter_w(int method, int x, int y, int w, int h, float lum, float* out) {
+    for (int l = 0; l < 4; ++l) out[l] = 0.0f;
+    if (method == FJ_METER_AVERAGE || method == FJ_METER_MEDIAN) {
+        out[0] = 1.0f;
+        return;
+    }
+    int maxDim = w > h ? w : h;
+    float invMax = maxDim > 0 ? 1.0f / (float)maxDim : 0.0f;
+    if (method == FJ_METER_CENTER_WEIGHTED) {
+        const float sg = 0.2f;
+        float nx = ((float)x / (float)w) - 0.5f, normX = nx * (float)w * invMax;
+        float ny = ((float)y / (float)h) - 0.5f, normY = ny * (float)h * invMax;
+        out[0] = expf(-(normX * normX) / (2.0f * sg * sg)) * expf(-(normY * normY) / (2.0f * sg * sg));
+        return;
+    }
+    float nx = (((float)x / (float)w) - 0.5f) * (float)w * invMax;
+    float ny = (((float)y / (float)h) - 0.5f) * (float)h * invMax;
+    float radius = sqrtf(nx * nx + ny * ny);
+    if (method == FJ_METER_PARTIAL) {
+        out[0] = radius < 0.15f ? 1.0f : 0.0f;
+        out[3] = 1.0f;
+    } else if (method == FJ_METER_MATRIX) {
+        int ch = h / 5, cw = w / 5;
+        if (ch <= 0 || cw <= 0) return;
+        int row = y / ch, col = x / cw;
+        if (row >= 5 || col >= 5) return;
+        float dy = ((float)row - 2.0f) / 2.0f, dx = ((float)col - 2.0f) / 2.0f;
+        float dist = sqrtf(dx * dx + dy * dy) / sqrtf(2.0f);
+        out[0] = 0.5f * (1.0f + cosf(3.14159265358979323846f * dist));
+    } else if (method == FJ_METER_MULTI_ZONE) {
+        if (radius >= 0.0f && radius < 0.05f) out[0] = 1.0f;
+        else if (radius >= 0.05f && radius < 0.25f) out[1] = 1.0f;
+        else if (radius >= 0.25f && radius < 0.50f) out[2] = 1.0f;
+        out[3] = 1.0f;
+    } else if (method == FJ_METER_HIGHLIGHT_WEIGHTED) {
+        out[0] = lum * lum;
+        out[3] = 1.0f;
+    }
+}
+
+/* Returns the exposure scale; *ok = 0 for rejected records (median, empty windows). */
+float oracle_auto_exposure(const FjPreparedHostData* h, const FjAutoExposure* m, const float* src, long src_row_floats,
+                           int comps, int* ok) {
+    *ok = 0;
+    if (m->method == FJ_METER_MEDIAN || m->preview_width <= 0 || m->preview_height <= 0) return 1.0f;
+    Packed pk;
+    if (pack(h, &pk)) {
+        free(pk.lut_store);
+        return 1.0f;
+    }
+    const Pack* p = &pk.p;
+    double Y[4] = {0, 0, 0, 0}, W[4] = {0, 0, 0, 0};
+    int pw = m->preview_width, ph = m->preview_height;
+    int sw = m->meter_bounds.x2 - m->meter_bounds.x1, sh = m->meter_bounds.y2 - m->meter_bounds.y1;
+    for (int y = 0; y < ph; ++y) {
+        int py = m->meter_bounds.y1 + preview_coord(y, ph, sh);
+        if (py < m->source_bounds.y1 || py >= m->source_bounds.y2) continue;
+        for (int x = 0; x < pw; ++x) {
+            int px = m->meter_bounds.x1 + preview_coord(x, pw, sw);
+            if (px < m->source_bounds.x1 || px >= m->source_bounds.x2) continue;
+            const float* s = src + (size_t)(py - m->source_bounds.y1) * src_row_floats +
+                             (size_t)(px - m->source_bounds.x1) * comps;
+            float raw[3];
+            if (p->method == FJ_RAW_MALLETT_2019) mallett_exposure(p, s, raw);
+            else tc_exposure(p, s, raw);
+            float mean = (raw[0] + raw[1] + raw[2]) * (1.0f / 3.0f);
+            if (!isfinite(mean)) continue;
+            float w[4];
+            meter_w((int)m->method, x, y, pw, ph, mean, w);
+            for (int l = 0; l < 4; ++l) {
+                float wl = (isfinite(w[l]) && w[l] > 0.0f) ? w[l] : 0.0f;
+                Y[l] += (double)mean * (double)wl;
+                W[l] += (double)wl;
+            }
+        }
+    }
+    free(pk.lut_store);
+    double yexp = 0.0;
+    int has = 0;
+    if (m->method == FJ_METER_PARTIAL) {
+        int l = W[0] > 0.0 ? 0 : 3;
+        if (W[l] > 0.0) {
+            yexp = Y[l] / W[l];
+            has = 1;
+        }
+    } else if (m->method == FJ_METER_MULTI_ZONE) {
+        const double ring[3] = {0.50, 0.30, 0.20};
+        double ws = 0.0, wt = 0.0;
+        for (int l = 0; l < 3; ++l)
+            if (W[l] > 0.0) {
+                ws += ring[l] * Y[l] / W[l];
+                wt += ring[l];
+            }
+        if (wt > 0.0) {
+            yexp = ws / wt;
+            has = 1;
+        } else if (W[3] > 0.0) {
+            yexp = Y[3] / W[3];
+            has = 1;
+        }
+    } else if (m->method == FJ_METER_HIGHLIGHT_WEIGHTED && W[0] < 1e-12) {
+        if (W[3] > 0.0) {
+            yexp = Y[3] / W[3];
+            has = 1;
+        }
+    } else if (W[0] > 0.0) {
+        yexp = Y[0] / W[0];
+        has = 1;
+    }
+    double ev = 0.0;
+    if (has && isfinite(yexp) && yexp > 0.0) {
+        double c = -log(yexp / 1.0) / log(2.0);
+        if (isfinite(c)) ev = c;
+    }
+    double s64 = exp2(ev);
+    *ok = 1;
+    return (isfinite(s64) && s64 > 0.0) ? (float)s64 : 1.0f;
+}

@@ -88,3 +88,69 @@ def scanner_lut(inp):
                                                                     for _ in range(2)]
     rc = lib.oracle_scanner_lut(C.byref(inp), *[C.c_void_p(o.ctypes.data) for o in outs])
     return rc, outs
+
+
+REF_LIB = os.path.join(HERE, "_ref", "libjuicer_ref.so")
+_ref = None
+
+
+def load_reference():
+    """The reference's own CUDA render kernels (oracle/_ref/libjuicer_ref.so) or None."""
+    global _ref
+    if _ref is not None:
+        return _ref
+    if not os.path.exists(REF_LIB):
+        return None
+    abi = _abi()
+    lib = C.CDLL(REF_LIB)
+    lib.ref_render.restype = C.c_int
+    lib.ref_render.argtypes = [C.POINTER(abi.FjPreparedHostData), C.POINTER(C.c_void_p), C.c_void_p, C.c_long,
+                               C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint32)]
+    lib.ref_capture_density.restype = C.c_int
+    lib.ref_capture_density.argtypes = [C.POINTER(abi.FjPreparedHostData), C.POINTER(C.c_void_p), C.c_void_p,
+                                        C.c_long, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    _ref = lib
+    return lib
+
+
+def scanner_lut_for(record):
+    """The record's scanner LUT built by the oracle (word-exact to the reference)."""
+    import numpy as np
+
+    abi = _abi()
+    h = record.h
+    sp = h.scanner_spectra
+    inp = abi.FjbScannerLutInput()
+    inp.eps_c, inp.eps_m, inp.eps_y = sp.dye_c, sp.dye_m, sp.dye_y
+    inp.weighted_x, inp.weighted_y, inp.weighted_z = sp.weighted_x, sp.weighted_y, sp.weighted_z
+    inp.baseline_min = sp.base_density
+    inp.has_baseline = 1 if sp.base_density.count else 0
+    inp.sample_count = sp.dye_c.count
+    inp.inv_yn = sp.inverse_y_normalization
+    prt = h.route in (1, 3)
+    for c in range(3):
+        inp.range_min_cmy[c] = h.scanner_bounds.min_cmy[c] if prt else -h.scanner_bounds.min_cmy[c]
+        inp.inverse_span_cmy[c] = h.scanner_bounds.inv_span_cmy[c]
+    inp.medium = 1 if prt else 0
+    inp.resolution = h.scanner_lut.resolution
+    rc, outs = scanner_lut(inp)
+    if rc != 0:
+        raise RuntimeError("oracle scanner LUT failed")
+    return [np.ascontiguousarray(o) for o in outs]
+
+
+def auto_exposure(record, meter, src):
+    """Exposure scale metered by the oracle (None when the record is rejected)."""
+    import numpy as np
+
+    lib = load()
+    abi = _abi()
+    fn = lib.oracle_auto_exposure
+    fn.restype = C.c_float
+    fn.argtypes = [C.POINTER(abi.FjPreparedHostData), C.POINTER(abi.FjAutoExposure), C.c_void_p, C.c_long, C.c_int,
+                   C.POINTER(C.c_int)]
+    src = np.ascontiguousarray(src, dtype=np.float32)
+    ok = C.c_int()
+    v = fn(record.pointer(), C.byref(meter), C.c_void_p(src.ctypes.data), src.shape[1] * src.shape[2], src.shape[2],
+           C.byref(ok))
+    return float(v) if ok.value else None
