@@ -53,6 +53,10 @@ _EXPORTS = {
                                                C.c_uint32, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
     "fjb_auto_exposure": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.c_ssize_t, C.c_uint32, C.POINTER(abi.FjAutoExposure),
                                          C.c_void_p, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_scatter_halation_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
+    "fjb_scatter_halation": (abi.FjStatus, [C.POINTER(abi.FjScatterHalation), C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_ssize_t, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, C.c_void_p,
+                                            C.POINTER(abi.FjErrorBuffer)]),
     "fjb_scanner_lut_build_host": (abi.FjStatus, [C.POINTER(abi.FjbScannerLutInput)] + [C.c_void_p] * 6 +
                                    [C.POINTER(abi.FjErrorBuffer)]),
 }

@@ -21,6 +21,7 @@
 #include "../../include/juicer_cuda_api.h"
 #include "fjb_internal.h"
 #include "fjb_recipe.h"
+#include "fjb_optics.h"
 #include "fjb_schedule.h"
 
 struct FjbRecipe {
@@ -258,6 +259,38 @@ FjStatus fjb_auto_exposure(FjbRecipe* recipe, const float* src, ptrdiff_t src_ro
     if (e != cudaSuccess) return cuda_status(e, error, "auto exposure launch");
     write_error(error, "");
     return ok_status();
+}
+
+size_t fjb_scatter_halation_scratch_bytes(int32_t width, int32_t height) {
+    if (width <= 0 || height <= 0) return 0;
+    return fjb::halation_scratch_floats(width, height) * sizeof(float);
+}
+
+FjStatus fjb_scatter_halation(const FjScatterHalation* halation, float* carrier_r, float* carrier_g,
+                              float* carrier_b, ptrdiff_t stride, int32_t width, int32_t height, float* scratch,
+                              size_t scratch_bytes, void* stream, FjErrorBuffer* error) {
+    try {
+        if (!halation || !carrier_r || !carrier_g || !carrier_b)
+            return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+        if (width <= 0 || height <= 0) {
+            write_error(error, "");
+            return ok_status();
+        }
+        if (stride < width) return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "carrier stride below width");
+        if (!scratch || scratch_bytes < fjb_scatter_halation_scratch_bytes(width, height))
+            return fail_status(FJ_STATUS_ALLOCATION_FAILURE, error, "scatter/halation scratch is too small");
+        float* planes[3] = {carrier_r, carrier_g, carrier_b};
+        std::string why;
+        cudaError_t e = cudaSuccess;
+        if (!fjb::scatter_halation(*halation, planes, stride, width, height, scratch, as_stream(stream), why, e)) {
+            if (e != cudaSuccess) return cuda_status(e, error, why.c_str());
+            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, why);
+        }
+        write_error(error, "");
+        return ok_status();
+    } catch (...) {
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "unexpected exception in fjb_scatter_halation");
+    }
 }
 
 FjStatus fjb_scanner_lut_build_host(const FjbScannerLutInput* in, float* log2_xyz, float* slope_c, float* slope_m,

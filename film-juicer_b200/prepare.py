@@ -458,3 +458,100 @@ def synthetic_frame(width: int, height: int, seed: int, frame_index: int = 0) ->
     mod = 1.0 + chroma[..., None] * (np.cos(hue)[..., None] * a_ax + np.sin(hue)[..., None] * b_ax)
     rgb = lum[..., None] * mod
     return np.ascontiguousarray(np.maximum(rgb, 0.0).astype(np.float32))
+
+
+# ---------------------------------------------------------------------------
+# Scatter / halation descriptor (rust/film-juicer-core/src/optics/halation_frame.rs)
+# ---------------------------------------------------------------------------
+HALATION_TAIL_RATIOS = (0.5360, 1.5236, 2.7684)
+HALATION_BOUNCE_MULTIPLIERS = (1.0, 1.4142135623730950488, 1.7320508075688772935, 2.0, 2.23606797749979)
+
+
+def _yvv_coefficients(sigma: float):
+    """Young-van Vliet third-order coefficients [B, b1/b0, b2/b0, b3/b0] (halation_frame.rs:221-229)."""
+    q = 0.98711 * sigma - 0.96330
+    q2, q3 = q * q, q * q * q
+    b0 = 1.57825 + 2.44413 * q + 1.4281 * q2 + 0.422205 * q3
+    b1 = 2.44413 * q + 2.85619 * q2 + 1.26661 * q3
+    b2 = -(1.4281 * q2 + 1.26661 * q3)
+    b3 = 0.422205 * q3
+    return [1.0 - (b1 + b2 + b3) / b0, b1 / b0, b2 / b0, b3 / b0]
+
+
+def _factored(coeffs):
+    """Real pole + second-order section factors [h, g, t, 0] (halation_frame.rs:88-146)."""
+    b, a1, a2, a3 = coeffs
+    c1 = 3.0 - 2.0 * a1 - a2
+    c2 = 3.0 - a1
+    poly = lambda h: ((-h + c2) * h - c1) * h + b
+    lo, hi = 0.0, 1.0
+    for _ in range(64):
+        mid = (lo + hi) * 0.5
+        if poly(mid) > 0.0:
+            lo = mid
+        else:
+            hi = mid
+    h = (lo + hi) * 0.5
+    t = a3 / (1.0 - h)
+    g = b / h
+    return [np.float32(h), np.float32(g), np.float32(t), np.float32(0.0)]
+
+
+def halation_gaussian(out: "abi.FjHalationGaussian", sigma_px: float, legacy: bool = True) -> None:
+    """Fills one FjHalationGaussian the way halation_frame.rs:157-236 builds it."""
+    C.memset(C.addressof(out), 0, C.sizeof(out))
+    if not (sigma_px > 0.0):
+        out.kind = abi.FJ_HALATION_IDENTITY
+        return
+    if sigma_px < 3.0:
+        radius = int(3.0 * sigma_px + 0.5)
+        if radius == 0:
+            out.kind = abi.FJ_HALATION_IDENTITY
+            return
+        x = np.arange(-radius, radius + 1, dtype=np.float64)
+        w = np.exp(-(x * x) / (2.0 * sigma_px * sigma_px))
+        w = (w / w.sum()).astype(np.float32)
+        out.kind = abi.FJ_HALATION_FIR_REFLECT
+        out.radius = radius
+        for i, v in enumerate(w):
+            out.fir_weights[i] = float(v)
+        return
+    co = _yvv_coefficients(sigma_px)
+    if legacy:
+        out.kind = abi.FJ_HALATION_YVV_REPLICATE
+        vals = [np.float32(v) for v in co]
+    else:
+        out.kind = abi.FJ_HALATION_YVV_REPLICATE_FACTORED
+        vals = _factored(co)
+    for i, v in enumerate(vals):
+        out.yvv[i] = float(v)
+
+
+def scatter_halation_record(pixel_size_um: float, *, scatter_amount: float = 0.35,
+                            core_um=(14.0, 11.0, 8.0), tail_um=(60.0, 45.0, 30.0), tail_weight=(0.25, 0.2, 0.15),
+                            halation_first_sigma_um=(90.0, 70.0, 50.0), strength=(0.08, 0.03, 0.0),
+                            bounce_weights=(0.6, 0.25, 0.15), renormalize: bool = True,
+                            legacy: bool = True) -> "abi.FjScatterHalation":
+    """An FjScatterHalation for the given pixel size with plausible still-film settings
+    (sigmas in micrometres; channels R, G, B)."""
+    d = abi.FjScatterHalation()
+    d.recipe_hash = 1
+    d.scatter_amount = scatter_amount
+    d.bounce_count = len(bounce_weights)
+    for i, w in enumerate(bounce_weights):
+        d.bounce_weights[i] = w
+    d.renormalize = 1 if renormalize else 0
+    for c in range(3):
+        ch = d.channels[c]
+        ch.tail_weight = tail_weight[c]
+        ch.total_strength = strength[c]
+        if ch.tail_weight != 1.0:
+            halation_gaussian(ch.core, max(core_um[c] / pixel_size_um, 1e-6), legacy)
+        if ch.tail_weight != 0.0:
+            for i in range(3):
+                halation_gaussian(ch.tail[i], max(tail_um[c] * HALATION_TAIL_RATIOS[i] / pixel_size_um, 1e-6), legacy)
+        if ch.total_strength != 0.0:
+            for b in range(d.bounce_count):
+                halation_gaussian(ch.bounce[b], halation_first_sigma_um[c] * HALATION_BOUNCE_MULTIPLIERS[b]
+                                  / pixel_size_um, legacy)
+    return d

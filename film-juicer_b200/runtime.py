@@ -187,3 +187,20 @@ def auto_exposure(recipe: "DeviceRecipe", src, meter: "abi.FjAutoExposure", scal
                                       C.byref(meter), C.c_void_p(_ptr(scale_out)), C.c_void_p(_stream_handle(stream)),
                                       C.byref(err.buf))
     _check("fjb_auto_exposure", st, err)
+
+
+def scatter_halation(descriptor: "abi.FjScatterHalation", planes_rgb, stream=None, scratch=None):
+    """In-place scatter/halation on three CUDA planes (R, G, B), each (H, W) float32."""
+    torch = _torch()
+    lib = load_library()
+    r, g, b = planes_rgb
+    h, w = r.shape
+    need = int(lib.fjb_scatter_halation_scratch_bytes(w, h))
+    if scratch is None:
+        scratch = torch.empty(need // 4, dtype=torch.float32, device=r.device)
+    err = abi.ErrorText()
+    st = lib.fjb_scatter_halation(C.byref(descriptor), C.c_void_p(_ptr(r)), C.c_void_p(_ptr(g)), C.c_void_p(_ptr(b)),
+                                  r.stride(0), w, h, C.c_void_p(_ptr(scratch)), scratch.numel() * 4,
+                                  C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+    _check("fjb_scatter_halation", st, err)
+    return scratch

@@ -86,6 +86,18 @@ FjStatus fjb_render_from_density(FjbRecipe* recipe, const float* density_c, cons
 FjStatus fjb_auto_exposure(FjbRecipe* recipe, const float* src, ptrdiff_t src_row_bytes, uint32_t components,
                            const FjAutoExposure* meter, float* device_scale, void* stream, FjErrorBuffer* error);
 
+/* Bytes of device scratch fjb_scatter_halation needs for a width x height frame. */
+size_t fjb_scatter_halation_scratch_bytes(int32_t width, int32_t height);
+
+/* Emulsion scatter then halation back-reflection on the three carrier planes, in
+ * place (reference src/Cuda/Film/JuicerCudaScatterHalation.cu:690
+ * JuicerCuda::launch_scatter_halation). The descriptor's channels are R, G, B;
+ * `stride` is in floats. `scratch` is caller-owned device memory of at least
+ * fjb_scatter_halation_scratch_bytes(width, height) bytes. */
+FjStatus fjb_scatter_halation(const FjScatterHalation* halation, float* carrier_r, float* carrier_g,
+                              float* carrier_b, ptrdiff_t stride, int32_t width, int32_t height, float* scratch,
+                              size_t scratch_bytes, void* stream, FjErrorBuffer* error);
+
 /* Scanner LUT input record (reference native/juicer_cuda_frame_values.h FjScannerLutInput). */
 typedef struct FjbScannerLutInput {
     FjFloatSpan eps_c, eps_m, eps_y;

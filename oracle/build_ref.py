@@ -16,7 +16,8 @@ REPO = os.path.dirname(HERE)
 REF = os.environ.get("FJ_REFERENCE_ROOT", "/root/reference")
 OUT = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT, "libjuicer_ref.so")
-TUS = ["src/Cuda/Scan/JuicerCudaScanPipeline.cu", "src/Cuda/Film/JuicerCudaFilmPipeline.cu"]
+TUS = ["src/Cuda/Scan/JuicerCudaScanPipeline.cu", "src/Cuda/Film/JuicerCudaFilmPipeline.cu",
+       "src/Cuda/Film/JuicerCudaScatterHalation.cu"]
 
 
 def main() -> int:

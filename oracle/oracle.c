@@ -958,3 +958,136 @@ float oracle_auto_exposure(const FjPreparedHostData* h, const FjAutoExposure* m,
     *ok = 1;
     return (isfinite(s64) && s64 > 0.0) ? (float)s64 : 1.0f;
 }
+
+/* ---------------- scatter / halation (src/Cuda/Film/JuicerCudaScatterHalation.cu) ----------------
+ * Literal per-channel schedule of launch_scatter_halation (:690-852): accumulation
+ * buffer cleared, each tail Gaussian accumulated with its amplitude, the core pass
+ * combined with the source, then the bounces accumulated and added. FIR Gaussians
+ * filter columns first then rows (:483-526); YVV Gaussians rows first (forward then
+ * backward) then columns (bottom-up then top-down) (:201-345). */
+
+static int reflect_half(int i, int n) {
+    if (i >= 0 && i < n) return i;
+    if (i >= -n && i < 0) return -i - 1;
+    if (i >= n && i < 2 * n) return 2 * n - 1 - i;
+    int period = 2 * n;
+    i %= period;
+    if (i < 0) i += period;
+    return i >= n ? period - 1 - i : i;
+}
+
+typedef struct {
+    float s1, s2, s3;
+} Yvv;
+
+static void yvv_init(const FjHalationGaussian* g, float first, Yvv* s) {
+    s->s1 = first;
+    s->s2 = first;
+    s->s3 = g->kind == FJ_HALATION_YVV_REPLICATE_FACTORED ? 0.0f : first;
+}
+
+static float yvv_step(const FjHalationGaussian* g, float x, Yvv* s) {
+    if (g->kind == FJ_HALATION_YVV_REPLICATE_FACTORED) {
+        s->s1 += g->yvv[0] * (x - s->s1);
+        s->s3 = g->yvv[2] * s->s3 + g->yvv[1] * (s->s1 - s->s2);
+        s->s2 += s->s3;
+        return s->s2;
+    }
+    float v = g->yvv[0] * x + g->yvv[1] * s->s1 + g->yvv[2] * s->s2 + g->yvv[3] * s->s3;
+    s->s3 = s->s2;
+    s->s2 = s->s1;
+    s->s1 = v;
+    return v;
+}
+
+/* Gaussian of `src` (stride sstride) into `out` (width stride); tmp is scratch. */
+static void gauss(const FjHalationGaussian* g, const float* src, long sstride, float* out, float* tmp, int W, int H) {
+    if (g->kind == FJ_HALATION_IDENTITY) {
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x) out[(size_t)y * W + x] = src[(size_t)y * sstride + x];
+        return;
+    }
+    if (g->kind == FJ_HALATION_FIR_REFLECT) {
+        int r = g->radius;
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x) {
+                float s = 0.0f;
+                for (int o = -r; o <= r; ++o) s += src[(size_t)reflect_half(y - o, H) * sstride + x] * g->fir_weights[o + r];
+                tmp[(size_t)y * W + x] = s;
+            }
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x) {
+                float s = 0.0f;
+                for (int o = -r; o <= r; ++o) s += tmp[(size_t)y * W + reflect_half(x + o, W)] * g->fir_weights[o + r];
+                out[(size_t)y * W + x] = s;
+            }
+        return;
+    }
+    for (int y = 0; y < H; ++y) {
+        Yvv s;
+        yvv_init(g, src[(size_t)y * sstride], &s);
+        for (int x = 0; x < W; ++x) tmp[(size_t)y * W + x] = yvv_step(g, src[(size_t)y * sstride + x], &s);
+        yvv_init(g, tmp[(size_t)y * W + W - 1], &s);
+        for (int x = W - 1; x >= 0; --x) tmp[(size_t)y * W + x] = yvv_step(g, tmp[(size_t)y * W + x], &s);
+    }
+    for (int x = 0; x < W; ++x) {
+        Yvv s;
+        yvv_init(g, tmp[(size_t)(H - 1) * W + x], &s);
+        for (int y = H - 1; y >= 0; --y) tmp[(size_t)y * W + x] = yvv_step(g, tmp[(size_t)y * W + x], &s);
+        yvv_init(g, tmp[x], &s);
+        for (int y = 0; y < H; ++y) out[(size_t)y * W + x] = yvv_step(g, tmp[(size_t)y * W + x], &s);
+    }
+}
+
+/* planes: R, G, B planes of width W, row stride `stride` floats, modified in place. */
+int oracle_scatter_halation(const FjScatterHalation* d, float* r, float* g, float* b, long stride, int W, int H) {
+    static const float amp[3] = {0.1633f, 0.6496f, 0.1870f};
+    size_t n = (size_t)W * H;
+    float* acc = (float*)calloc(n, sizeof(float));
+    float* val = (float*)malloc(n * sizeof(float));
+    float* tmp = (float*)malloc(n * sizeof(float));
+    float* planes[3] = {r, g, b};
+    if (!acc || !val || !tmp) return 1;
+    for (int c = 0; c < 3; ++c) {
+        float* P = planes[c];
+        const FjHalationChannel* ch = &d->channels[c];
+        if (d->scatter_amount != 0.0f) {
+            int tails = ch->tail_weight > 0.0f;
+            if (tails) {
+                for (int i = 0; i < 3; ++i) {
+                    gauss(&ch->tail[i], P, stride, val, tmp, W, H);
+                    for (size_t k = 0; k < n; ++k) acc[k] = i == 0 ? amp[i] * val[k] : acc[k] + amp[i] * val[k];
+                }
+            }
+            gauss(&ch->core, P, stride, val, tmp, W, H);
+            for (int y = 0; y < H; ++y)
+                for (int x = 0; x < W; ++x) {
+                    size_t k = (size_t)y * W + x;
+                    float source = P[(size_t)y * stride + x];
+                    float tail = tails ? acc[k] : 0.0f;
+                    float coreTerm = (1.0f - ch->tail_weight) * val[k];
+                    float tailTerm = ch->tail_weight * tail;
+                    float scattered = coreTerm + tailTerm;
+                    float sourceTerm = (1.0f - d->scatter_amount) * source;
+                    float scatteredTerm = d->scatter_amount * scattered;
+                    P[(size_t)y * stride + x] = sourceTerm + scatteredTerm;
+                }
+        }
+        if (ch->total_strength == 0.0f) continue;
+        memset(acc, 0, n * sizeof(float));
+        for (unsigned i = 0; i < d->bounce_count; ++i) {
+            gauss(&ch->bounce[i], P, stride, val, tmp, W, H);
+            for (size_t k = 0; k < n; ++k) acc[k] = i == 0 ? d->bounce_weights[i] * val[k] : acc[k] + d->bounce_weights[i] * val[k];
+        }
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x) {
+                float source = P[(size_t)y * stride + x];
+                float added = source + ch->total_strength * acc[(size_t)y * W + x];
+                P[(size_t)y * stride + x] = d->renormalize ? added / (1.0f + ch->total_strength) : added;
+            }
+    }
+    free(acc);
+    free(val);
+    free(tmp);
+    return 0;
+}

@@ -252,3 +252,59 @@ extern "C" int ref_capture_density(const FjPreparedHostData* h, const float* con
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return (int)e;
 }
+
+#include "Cuda/Film/JuicerCudaScatterHalation.h"
+#include "ScatterHalation.h"
+
+// Scatter/halation with the reference's own kernels
+// (src/Cuda/Film/JuicerCudaScatterHalation.cu:690 launch_scatter_halation). planes are
+// device pointers (R, G, B) with `stride` floats per row; modified in place.
+extern "C" int ref_scatter_halation(const FjScatterHalation* d, float* r, float* g, float* b, long stride, int width,
+                                    int height) {
+    ScatterHalationFrameDescriptor desc{};
+    desc.recipeHash = d->recipe_hash ? d->recipe_hash : 1;
+    desc.scatterAmount = d->scatter_amount;
+    desc.bounceCount = d->bounce_count;
+    for (int i = 0; i < 5; ++i) desc.bounceWeights[i] = d->bounce_weights[i];
+    desc.renormalize = d->renormalize != 0;
+    auto conv = [](const FjHalationGaussian& s) {
+        ScatterHalationGaussianDescriptor o{};
+        o.kind = static_cast<ScatterHalationGaussianKind>(s.kind);
+        o.radius = s.radius;
+        for (int i = 0; i < 19; ++i) o.firWeights[i] = s.fir_weights[i];
+        for (int i = 0; i < 4; ++i) o.yvv[i] = s.yvv[i];
+        return o;
+    };
+    for (int c = 0; c < 3; ++c) {
+        const FjHalationChannel& ch = d->channels[c];
+        desc.channels[c].core = conv(ch.core);
+        for (int i = 0; i < 3; ++i) desc.channels[c].tail[i] = conv(ch.tail[i]);
+        for (int i = 0; i < 5; ++i) desc.channels[c].bounce[i] = conv(ch.bounce[i]);
+        desc.channels[c].totalStrength = ch.total_strength;
+        desc.channels[c].tailWeight = ch.tail_weight;
+    }
+    float* temp = nullptr;
+    float* acc = nullptr;
+    const size_t bytes = (size_t)width * height * sizeof(float);
+    if (cudaMalloc(&temp, bytes) != cudaSuccess) return 2;
+    if (cudaMalloc(&acc, bytes) != cudaSuccess) {
+        cudaFree(temp);
+        return 2;
+    }
+    JuicerCuda::ScatterHalationPreparedView view{};
+    view.descriptor = &desc;
+    view.fullFrameWidth = width;
+    view.fullFrameHeight = height;
+    view.currentCarrier.redSensitive = r;
+    view.currentCarrier.greenSensitive = g;
+    view.currentCarrier.blueSensitive = b;
+    view.currentCarrier.rowStrideFloats = (size_t)stride;
+    view.filterTemp = temp;
+    view.weightedAccumulation = acc;
+    const JuicerCuda::ScatterHalationLaunchResult res = JuicerCuda::launch_scatter_halation(view, nullptr);
+    cudaError_t e = res.status;
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(temp);
+    cudaFree(acc);
+    return (int)e;
+}
