@@ -57,6 +57,16 @@ _EXPORTS = {
     "fjb_scatter_halation": (abi.FjStatus, [C.POINTER(abi.FjScatterHalation), C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_ssize_t, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, C.c_void_p,
                                             C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_spatial_dir_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
+    "fjb_spatial_dir_build": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjSpatialDir), C.c_void_p, C.c_ssize_t,
+                                             C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_ssize_t, C.c_int32,
+                                             C.c_int32] + [C.c_void_p] * 7 + [C.c_size_t, C.c_void_p,
+                                                                                C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_recipe_set_spatial_dir_planes": (abi.FjStatus, [C.c_void_p] + [C.c_void_p] * 6 +
+                                          [C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_dir_boundary_host": (abi.FjStatus, [C.POINTER(abi.FjDirGaussian), C.c_int32, C.POINTER(C.c_double),
+                                             C.c_size_t, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                             C.POINTER(C.c_double), C.POINTER(abi.FjErrorBuffer)]),
     "fjb_scanner_lut_build_host": (abi.FjStatus, [C.POINTER(abi.FjbScannerLutInput)] + [C.c_void_p] * 6 +
                                    [C.POINTER(abi.FjErrorBuffer)]),
 }

@@ -37,7 +37,7 @@ def _compile(src: str, verbose: bool) -> str:
     deps += [os.path.join(REPO, "include", f) for f in os.listdir(os.path.join(REPO, "include"))]
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj
-    cmd = [nvcc(), "-std=c++17", *ARCH, "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I",
+    cmd = [nvcc(), "-std=c++17", *ARCH, "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3,-ffp-contract=off", "-I",
            os.path.join(REPO, "include"), "-c", src, "-o", obj]
     if src.endswith(".cpp"):
         cmd[1:1] = ["-x", "cu"]

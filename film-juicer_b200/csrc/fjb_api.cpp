@@ -24,11 +24,6 @@
 #include "fjb_optics.h"
 #include "fjb_schedule.h"
 
-struct FjbRecipe {
-    fjb::Recipe r;
-    int device = 0;
-};
-
 namespace fjb {
 
 void write_error(FjErrorBuffer* error, const std::string& text) {

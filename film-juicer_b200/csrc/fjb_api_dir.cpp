@@ -1,0 +1,146 @@
+// fjb_api_dir.cpp -- extern "C" entry points of the spatial-DIR stage.
+//
+// The stage order restates src/Cuda/Film/JuicerCudaFilmPipeline.cu:799-1060
+// (build_spatial_dir_impl): raw donor corrections and raw log exposure per pixel,
+// then the weighted Gaussian components on each correction plane; the filtered
+// planes and the cached log exposure are then consumed by capture development
+// (src/Cuda/JuicerCudaDeviceHelpers.cuh:1267-1328).
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/juicer_b200.h"
+#include "fjb_dir.h"
+#include "fjb_internal.h"
+#include "fjb_recipe.h"
+#include "fjb_schedule.h"
+
+using fjb::cuda_status;
+using fjb::fail_status;
+using fjb::ok_status;
+using fjb::write_error;
+
+extern "C" {
+
+size_t fjb_spatial_dir_scratch_bytes(int32_t width, int32_t height) {
+    if (width <= 0 || height <= 0) return 0;
+    return (size_t)(3 + 3 * fjb::kDirMaxComponents) * (size_t)width * (size_t)height * sizeof(float);
+}
+
+FjStatus fjb_spatial_dir_build(FjbRecipe* recipe, const FjSpatialDir* spatial_dir, const float* src,
+                               ptrdiff_t src_row_bytes, uint32_t components, const float* carrier_b,
+                               const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                               int32_t width, int32_t height, float* filtered_y, float* filtered_m,
+                               float* filtered_c, float* log_raw_b, float* log_raw_g, float* log_raw_r,
+                               float* scratch, size_t scratch_bytes, void* stream, FjErrorBuffer* error) {
+    try {
+        if (!recipe || !spatial_dir || !filtered_y || !filtered_m || !filtered_c || !log_raw_b || !log_raw_g ||
+            !log_raw_r)
+            return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+        if (width <= 0 || height <= 0) {
+            write_error(error, "");
+            return ok_status();
+        }
+        const bool carrier = carrier_b && carrier_g && carrier_r;
+        if (!carrier && (!src || !(components == 3 || components == 4)))
+            return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "spatial DIR needs a source image or carrier planes");
+        if (recipe->r.params.dir_mode == fjb::kDirInactive)
+            return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "spatial DIR needs active DIR couplers");
+        if (!scratch || scratch_bytes < fjb_spatial_dir_scratch_bytes(width, height))
+            return fail_status(FJ_STATUS_ALLOCATION_FAILURE, error, "spatial DIR scratch is too small");
+        cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+        fjb::DirPlan plan;
+        std::string why;
+        cudaError_t e = cudaSuccess;
+        if (!fjb::dir_plan_create(*spatial_dir, width, height, s, plan, why, e)) {
+            plan.release();
+            if (e != cudaSuccess) return cuda_status(e, error, "spatial DIR plan");
+            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, why);
+        }
+        const size_t plane = (size_t)width * (size_t)height;
+        float* raw[3] = {scratch, scratch + plane, scratch + 2 * plane};
+        fjb::PixelParams p = recipe->r.params;
+        p.src = reinterpret_cast<const char*>(src);
+        p.src_row_bytes = src_row_bytes;
+        p.components = (int)components;
+        p.width = width;
+        p.height = height;
+        p.carrier_b = carrier_b;
+        p.carrier_g = carrier_g;
+        p.carrier_r = carrier_r;
+        p.carrier_stride = carrier_stride;
+        p.dir_src_y = raw[0];
+        p.dir_src_m = raw[1];
+        p.dir_src_c = raw[2];
+        p.dir_src_log_b = log_raw_b;
+        p.dir_src_log_g = log_raw_g;
+        p.dir_src_log_r = log_raw_r;
+        e = fjb::launch_pixel_chain(
+            p, carrier ? fjb::PixelStage::CarrierToDirSource : fjb::PixelStage::SourceToDirSource, s);
+        if (e == cudaSuccess) {
+            fjb::DirBlurParams bp{};
+            bp.width = width;
+            bp.height = height;
+            bp.count = plan.count;
+            for (int k = 0; k < plan.count; ++k) bp.comp[k] = plan.comp[k];
+            float* out[3] = {filtered_y, filtered_m, filtered_c};
+            for (int c = 0; c < 3; ++c) {
+                bp.raw[c] = raw[c];
+                bp.filtered[c] = out[c];
+                for (int k = 0; k < fjb::kDirMaxComponents; ++k)
+                    bp.temp[c][k] = scratch + (3 + (size_t)c * fjb::kDirMaxComponents + k) * plane;
+            }
+            e = fjb::launch_dir_blur(bp, s);
+        }
+        // the plan's device tables must outlive the kernels that read them
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        plan.release();
+        if (e != cudaSuccess) return cuda_status(e, error, "spatial DIR");
+        write_error(error, "");
+        return ok_status();
+    } catch (...) {
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "unexpected exception in fjb_spatial_dir_build");
+    }
+}
+
+FjStatus fjb_recipe_set_spatial_dir_planes(FjbRecipe* recipe, const float* filtered_y, const float* filtered_m,
+                                           const float* filtered_c, const float* log_raw_b, const float* log_raw_g,
+                                           const float* log_raw_r, FjErrorBuffer* error) {
+    if (!recipe) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null recipe");
+    fjb::PixelParams& p = recipe->r.params;
+    const bool on = filtered_y && filtered_m && filtered_c && log_raw_b && log_raw_g && log_raw_r;
+    p.dir_spatial = on ? 1 : 0;
+    p.dir_filtered_y = on ? filtered_y : nullptr;
+    p.dir_filtered_m = on ? filtered_m : nullptr;
+    p.dir_filtered_c = on ? filtered_c : nullptr;
+    p.dir_log_raw_b = on ? log_raw_b : nullptr;
+    p.dir_log_raw_g = on ? log_raw_g : nullptr;
+    p.dir_log_raw_r = on ? log_raw_r : nullptr;
+    write_error(error, "");
+    return ok_status();
+}
+
+FjStatus fjb_dir_boundary_host(const FjDirGaussian* component, int32_t axis_length, double* weights,
+                               size_t weights_capacity, int32_t* out_length, int32_t* out_terminal_size,
+                               double* terminal, FjErrorBuffer* error) {
+    try {
+        if (!component || !weights || !out_length || !out_terminal_size || !terminal)
+            return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+        fjb::DirAxisBoundary b;
+        std::string why;
+        if (!fjb::dir_axis_boundary(*component, axis_length, b, why))
+            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, why);
+        if (b.weights.size() > weights_capacity)
+            return fail_status(FJ_STATUS_ALLOCATION_FAILURE, error, "boundary weights exceed the buffer");
+        for (size_t i = 0; i < b.weights.size(); ++i) weights[i] = b.weights[i];
+        for (int i = 0; i < 9; ++i) terminal[i] = b.terminal[i];
+        *out_length = b.length;
+        *out_terminal_size = b.terminal_size;
+        write_error(error, "");
+        return ok_status();
+    } catch (...) {
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "unexpected exception in fjb_dir_boundary_host");
+    }
+}
+
+} // extern "C"

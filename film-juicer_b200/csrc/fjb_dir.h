@@ -1,0 +1,73 @@
+// fjb_dir.h -- spatial DIR (development-inhibitor-releasing coupler) diffusion (a7).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/juicer_cuda_api.h"
+
+namespace fjb {
+
+enum DirOperator : int { kDirOpNone = 0, kDirOpIdentity = 1, kDirOpFir = 2, kDirOpYvv = 3 };
+constexpr int kDirMaxComponents = 4;
+constexpr int kDirMaxFirRadius = 64;
+
+// Reflected-boundary start weights and end matrix of one axis of a recursive
+// Gaussian (restatement of rust/film-juicer-core/src/film/dir/boundary.rs:362-490).
+struct DirAxisBoundary {
+    std::vector<double> weights; // 3 rows x length, row-major (state history 0, 1, 2)
+    int length = 0;
+    int terminal_size = 0;
+    double terminal[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+// Returns false with `why` when the boundary system is singular or the weights fail
+// the record's certification tolerance.
+bool dir_axis_boundary(const FjDirGaussian& g, int axis_length, DirAxisBoundary& out, std::string& why);
+
+// Normalized Gaussian taps for radius r (restatement of
+// rust/film-juicer-core/src/optics/gaussian.rs:16-52): f64 exponentials narrowed to f32,
+// then scaled by the f64 reciprocal of their f64 sum.
+std::vector<float> gaussian_taps(int radius, float sigma_px);
+
+struct DirComponentDev {
+    int op;
+    float weight;
+    int radius;
+    const float* taps; // device, 2r+1
+    double ff;
+    double fb[3];
+    const double* h_init;
+    int h_len, h_tsize;
+    double h_term[9];
+    const double* v_init;
+    int v_len, v_tsize;
+    double v_term[9];
+};
+
+struct DirBlurParams {
+    int width, height, count;
+    DirComponentDev comp[kDirMaxComponents];
+    const float* raw[3]; // correction planes Y, M, C (width floats per row)
+    float* filtered[3];  // outputs Y, M, C
+    float* temp[3][kDirMaxComponents];
+};
+
+cudaError_t launch_dir_blur(const DirBlurParams& p, cudaStream_t stream);
+
+// Device-resident operator tables for one frame geometry.
+struct DirPlan {
+    int width = 0, height = 0, count = 0;
+    DirComponentDev comp[kDirMaxComponents] = {};
+    std::vector<void*> owned;
+    void release();
+};
+
+bool dir_plan_create(const FjSpatialDir& sd, int width, int height, cudaStream_t stream, DirPlan& plan,
+                     std::string& why, cudaError_t& err);
+
+size_t dir_scratch_floats(int width, int height);
+
+} // namespace fjb

@@ -19,6 +19,8 @@ enum class PixelStage : int {
     SourceToDensity = 2,  // source RGB -> capture density planes
     CarrierToDensity = 3, // optics carrier planes -> capture density planes
     DensityToOutput = 4,  // (grained) capture density planes -> encoded output
+    SourceToDirSource = 5,  // source RGB -> spatial-DIR raw corrections + log exposure
+    CarrierToDirSource = 6, // carrier planes -> spatial-DIR raw corrections + log exposure
 };
 
 cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStream_t stream);

@@ -108,6 +108,15 @@ struct PixelParams {
     const float* dir_log_raw_g;
     const float* dir_log_raw_r;
 
+    // Spatial-DIR source outputs: raw donor corrections (Y, M, C receivers) and raw
+    // log exposure (B, G, R).
+    float* dir_src_y;
+    float* dir_src_m;
+    float* dir_src_c;
+    float* dir_src_log_b;
+    float* dir_src_log_g;
+    float* dir_src_log_r;
+
     // Optional density-plane input for the scan stage (after grain): C, M, Y planes.
     const float* scan_density_c;
     const float* scan_density_m;

@@ -19,7 +19,29 @@
 namespace fjb {
 
 enum InputKind : int { kInSource = 0, kInCarrier = 1, kInDensity = 2 };
-enum OutputKind : int { kOutEncoded = 0, kOutDensity = 1 };
+enum OutputKind : int { kOutEncoded = 0, kOutDensity = 1, kOutDirSource = 2 };
+
+// Spatial-DIR source (src/Cuda/Film/JuicerCudaFilmPipeline.cu:124-214): raw log
+// exposure, pre-DIR layer densities and the donor corrections they release.
+__device__ __forceinline__ void dir_source(const PixelParams& p, const float* __restrict__ blob, const float e[3],
+                                           long long idx) {
+    float logE[3], layer[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        logE[c] = log_exposure(e[c]);
+        const float s = clamp_infinite_log(blob, p.film_curve[c], logE[c]);
+        layer[c] = curve_sample(blob, p.film_curve[c], s, p.gamma_bgr[c]);
+    }
+    float corr[3];
+    const unsigned fail = dir_donor_corrections(p, layer, corr);
+    flag_dir_failure(p, fail);
+    p.dir_src_y[idx] = corr[0];
+    p.dir_src_m[idx] = corr[1];
+    p.dir_src_c[idx] = corr[2];
+    p.dir_src_log_b[idx] = logE[0];
+    p.dir_src_log_g[idx] = logE[1];
+    p.dir_src_log_r[idx] = logE[2];
+}
 
 template <int In, int Out, bool Print, bool SpatialDir>
 __global__ void __launch_bounds__(kPixelThreads) pixel_chain_kernel(const __grid_constant__ PixelParams p) {
@@ -40,6 +62,22 @@ __global__ void __launch_bounds__(kPixelThreads) pixel_chain_kernel(const __grid
         const float* srcPix = nullptr;
         if (p.src) {
             srcPix = reinterpret_cast<const float*>(p.src + (long long)y * p.src_row_bytes) + (long long)x * p.components;
+        }
+
+        if constexpr (Out == kOutDirSource) {
+            float e[3];
+            if constexpr (In == kInCarrier) {
+                const long long ci = (long long)y * p.carrier_stride + x;
+                e[0] = p.carrier_b[ci];
+                e[1] = p.carrier_g[ci];
+                e[2] = p.carrier_r[ci];
+                for (int c = 0; c < 3; ++c) e[c] = fmaxf(0.0f, e[c] * p.route_correction_scale);
+            } else {
+                const float in[3] = {srcPix[0], srcPix[1], srcPix[2]};
+                camera_linear_exposure(p, in, true, e);
+            }
+            dir_source(p, blob, e, idx);
+            continue;
         }
 
         float d[3];
@@ -188,6 +226,10 @@ cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStrea
         case PixelStage::CarrierToDensity:
             return sdir ? launch_variant<kInCarrier, kOutDensity, false, true>(p, grid, smem, stream)
                         : launch_variant<kInCarrier, kOutDensity, false, false>(p, grid, smem, stream);
+        case PixelStage::SourceToDirSource:
+            return launch_variant<kInSource, kOutDirSource, false, false>(p, grid, smem, stream);
+        case PixelStage::CarrierToDirSource:
+            return launch_variant<kInCarrier, kOutDirSource, false, false>(p, grid, smem, stream);
         case PixelStage::DensityToOutput:
             return print ? launch_variant<kInDensity, kOutEncoded, true, false>(p, grid, smem, stream)
                          : launch_variant<kInDensity, kOutEncoded, false, false>(p, grid, smem, stream);

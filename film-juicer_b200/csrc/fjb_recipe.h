@@ -46,6 +46,16 @@ struct Recipe {
 
 bool create_recipe(const FjPreparedHostData& h, cudaStream_t stream, Recipe& r, std::string& why, FjStatus& status);
 
+} // namespace fjb
+
+// The C-ABI's opaque recipe handle.
+struct FjbRecipe {
+    fjb::Recipe r;
+    int device = 0;
+};
+
+namespace fjb {
+
 // FjAutoExposure -> metering grid; false (with a reason) for rejected records:
 // median metering, empty preview or meter window, meter window outside the source.
 inline bool meter_spec_from(const FjAutoExposure& a, MeterSpec& m, std::string& why) {

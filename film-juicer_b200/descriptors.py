@@ -1,0 +1,82 @@
+"""Frame descriptors of the spatial stages (host side), filled the way the reference's
+Rust host builds them.
+
+* spatial_dir_record: rust/film-juicer-core/src/film/dir/frame.rs:185-280 -- a core
+  Gaussian (diffusion size / pixel size, weight 1 - tail weight) and, when the tail
+  weight is positive, three tail Gaussians (tail size x {0.5360, 1.5236, 2.7684},
+  amplitudes {0.1633, 0.6496, 0.1870} normalised, times the tail weight); operator
+  identity for radius 0, FIR below sigma 3, the reflected recursive Gaussian from
+  sigma 3 with Young-van Vliet coefficients (frame.rs:70-99), boundary accuracy 1e-11,
+  tolerance 5e-7, derivation version 1 (frame.rs:60-68).
+* gaussian_taps: rust/film-juicer-core/src/optics/gaussian.rs:16-52.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import abi
+
+DIR_TAIL_AMPLITUDES = (0.1633, 0.6496, 0.1870)
+DIR_TAIL_RATIOS = (0.5360, 1.5236, 2.7684)
+
+
+def gaussian_taps(radius: int, sigma_px: float) -> np.ndarray:
+    sigma = float(np.float32(sigma_px))
+    s2 = sigma * sigma * 2.0
+    x = np.arange(-radius, radius + 1, dtype=np.float64)
+    w64 = np.exp(-(x * x) / s2)
+    w32 = w64.astype(np.float32)
+    total = float(np.sum(w64))
+    rec = 1.0 / total if total != 0.0 else 0.0
+    return (w32.astype(np.float64) * rec).astype(np.float32)
+
+
+def _dir_component(g: "abi.FjDirGaussian", sigma_px: np.float32, weight: np.float32) -> None:
+    g.sigma_px = float(sigma_px)
+    g.weight = float(weight)
+    radius = 3.0 * float(sigma_px) + 0.5
+    g.radius = int(radius)
+    g.boundary_truncation_accuracy = 1.0e-11
+    g.boundary_certification_tolerance = 5.0e-7
+    g.boundary_derivation_version = 1
+    if sigma_px <= 0.0 or g.radius == 0:
+        g.reference_operator = abi.FJ_DIR_OPERATOR_IDENTITY
+        g.radius = 0
+        return
+    if sigma_px >= 3.0:
+        g.reference_operator = abi.FJ_DIR_OPERATOR_YVV_REFLECT
+        g.radius = int(radius)
+        q = 0.98711 * float(sigma_px) - 0.96330
+        q2, q3 = q * q, q * q * q
+        den = 1.57825 + 2.44413 * q + 1.4281 * q2 + 0.422205 * q3
+        g.normalization_denominator = den
+        g.feedforward_numerator = 1.57825
+        g.feedback_numerators[0] = 2.44413 * q + 2.0 * 1.4281 * q2 + 3.0 * 0.422205 * q3
+        g.feedback_numerators[1] = -(1.4281 * q2 + 3.0 * 0.422205 * q3)
+        g.feedback_numerators[2] = 0.422205 * q3
+        g.feedforward = g.feedforward_numerator / den
+        for i in range(3):
+            g.feedback[i] = g.feedback_numerators[i] / den
+        return
+    g.reference_operator = abi.FJ_DIR_OPERATOR_FIR_REFLECT
+
+
+def spatial_dir_record(pixel_size_um: float, width: int, height: int, *, diffusion_size_um: float = 20.0,
+                       tail_um: float = 200.0, tail_weight: float = 0.03) -> "abi.FjSpatialDir":
+    sd = abi.FjSpatialDir()
+    for ext in (sd.render_extent, sd.full_frame_extent, sd.filter_domain_extent):
+        ext.x, ext.y, ext.width, ext.height = 0, 0, width, height
+    px = np.float32(pixel_size_um)
+    tw = np.float32(tail_weight)
+    comps = [(np.float32(np.float32(diffusion_size_um) / px), np.float32(np.float32(1.0) - tw))]
+    if tw > 0:
+        total = np.float32(np.float32(DIR_TAIL_AMPLITUDES[0]) + np.float32(DIR_TAIL_AMPLITUDES[1])
+                           + np.float32(DIR_TAIL_AMPLITUDES[2]))
+        tail_sigma = np.float32(np.float32(tail_um) / px)
+        for a, r in zip(DIR_TAIL_AMPLITUDES, DIR_TAIL_RATIOS):
+            comps.append((np.float32(tail_sigma * np.float32(r)), np.float32(tw * np.float32(np.float32(a) / total))))
+    sd.component_count = len(comps)
+    for i, (s, w) in enumerate(comps):
+        _dir_component(sd.components[i], s, w)
+    sd.recipe_hash = sd.hash = 1
+    return sd

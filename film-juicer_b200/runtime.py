@@ -138,6 +138,35 @@ class DeviceRecipe:
         _check("fjb_render_from_density", st, err)
 
 
+    def set_spatial_dir_planes(self, filtered=None, log_raw=None):
+        """Capture development reads these planes (filtered Y, M, C; log raw B, G, R)
+        from now on; None returns to runtime DIR."""
+        ptrs = [C.c_void_p(_ptr(t)) for t in (*filtered, *log_raw)] if filtered is not None else [C.c_void_p(0)] * 6
+        err = abi.ErrorText()
+        _check("fjb_recipe_set_spatial_dir_planes",
+               self.lib.fjb_recipe_set_spatial_dir_planes(self.handle, *ptrs, C.byref(err.buf)), err)
+
+    def spatial_dir_build(self, spatial_dir, filtered, log_raw, *, src=None, carrier=None, scratch=None,
+                          stream=None):
+        """Spatial-DIR source + diffusion into `filtered` (Y, M, C) and `log_raw` (B, G, R)."""
+        torch = _torch()
+        h, w = filtered[0].shape
+        need = int(self.lib.fjb_spatial_dir_scratch_bytes(w, h))
+        if scratch is None:
+            scratch = torch.empty(need // 4, dtype=torch.float32, device=filtered[0].device)
+        cb, cg, cr = carrier if carrier is not None else (None, None, None)
+        err = abi.ErrorText()
+        st = self.lib.fjb_spatial_dir_build(
+            self.handle, C.byref(spatial_dir), C.c_void_p(_ptr(src) if src is not None else 0),
+            (src.stride(0) * 4) if src is not None else 0, src.shape[2] if src is not None else 3,
+            C.c_void_p(_ptr(cb) if cb is not None else 0), C.c_void_p(_ptr(cg) if cg is not None else 0),
+            C.c_void_p(_ptr(cr) if cr is not None else 0), cb.stride(0) if cb is not None else 0, w, h,
+            *[C.c_void_p(_ptr(t)) for t in (*filtered, *log_raw)], C.c_void_p(_ptr(scratch)), scratch.numel() * 4,
+            C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+        _check("fjb_spatial_dir_build", st, err)
+        return scratch
+
+
 def render_pixels_numpy(record, src: np.ndarray) -> np.ndarray:
     """One fused per-pixel render of a host image (H, W, 3|4) through the C-ABI."""
     torch = _torch()

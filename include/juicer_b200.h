@@ -98,6 +98,38 @@ FjStatus fjb_scatter_halation(const FjScatterHalation* halation, float* carrier_
                               float* carrier_b, ptrdiff_t stride, int32_t width, int32_t height, float* scratch,
                               size_t scratch_bytes, void* stream, FjErrorBuffer* error);
 
+/* Bytes of device scratch fjb_spatial_dir_build needs for a width x height frame. */
+size_t fjb_spatial_dir_scratch_bytes(int32_t width, int32_t height);
+
+/* Spatial DIR source + diffusion (reference src/Cuda/Film/JuicerCudaFilmPipeline.cu:1479
+ * juicer_cuda_build_print_spatial_dir -> build_spatial_dir_impl :799). From the
+ * carrier planes (when all three are given) or the source image it writes the
+ * filtered donor-correction planes (Y, M, C receivers) and the raw log exposure (B,
+ * G, R), all width x height floats. Operators: identity, reflect FIR (sigma < 3) and
+ * the reflected-boundary recursive Gaussian (sigma >= 3), whose boundary weights are
+ * derived on the host (see fjb_dir_boundary_host). Synchronises `stream`. */
+FjStatus fjb_spatial_dir_build(FjbRecipe* recipe, const FjSpatialDir* spatial_dir, const float* src,
+                               ptrdiff_t src_row_bytes, uint32_t components, const float* carrier_b,
+                               const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                               int32_t width, int32_t height, float* filtered_y, float* filtered_m,
+                               float* filtered_c, float* log_raw_b, float* log_raw_g, float* log_raw_r,
+                               float* scratch, size_t scratch_bytes, void* stream, FjErrorBuffer* error);
+
+/* Makes later capture-development calls on `recipe` use spatially filtered DIR
+ * corrections and cached log exposure (all six device planes, or all NULL to return
+ * to runtime DIR). */
+FjStatus fjb_recipe_set_spatial_dir_planes(FjbRecipe* recipe, const float* filtered_y, const float* filtered_m,
+                                           const float* filtered_c, const float* log_raw_b, const float* log_raw_g,
+                                           const float* log_raw_r, FjErrorBuffer* error);
+
+/* Reflected-boundary start weights (3 rows x *out_length, row-major) and end matrix
+ * (*out_terminal_size squared, row-major) of one axis of a recursive DIR component;
+ * the construction the reference obtains from its host through
+ * native/juicer_dir_boundary_api.h:58-61 (fj_dir_boundary_acquire/view). */
+FjStatus fjb_dir_boundary_host(const FjDirGaussian* component, int32_t axis_length, double* weights,
+                               size_t weights_capacity, int32_t* out_length, int32_t* out_terminal_size,
+                               double* terminal, FjErrorBuffer* error);
+
 /* Scanner LUT input record (reference native/juicer_cuda_frame_values.h FjScannerLutInput). */
 typedef struct FjbScannerLutInput {
     FjFloatSpan eps_c, eps_m, eps_y;

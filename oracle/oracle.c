@@ -1091,3 +1091,234 @@ int oracle_scatter_halation(const FjScatterHalation* d, float* r, float* g, floa
     free(tmp);
     return 0;
 }
+
+/* ---------------- spatial DIR (src/Cuda/Film/JuicerCudaFilmPipeline.cu:124-1060) ---------------- */
+
+typedef struct {
+    int op; /* 1 identity, 2 FIR, 3 recursive */
+    float weight;
+    int radius;
+    const float* taps;
+    double ff, fb[3];
+    const double* h_init;
+    int h_len, h_ts;
+    double h_term[9];
+    const double* v_init;
+    int v_len, v_ts;
+    double v_term[9];
+} OracleDirComp;
+
+static int reflect_dir(int i, int n) {
+    if (n <= 1) return 0;
+    int period = 2 * n;
+    i %= period;
+    if (i < 0) i += period;
+    return i >= n ? period - 1 - i : i;
+}
+
+static double iir(const OracleDirComp* c, double x, double* s) {
+    double v = c->ff * x + c->fb[0] * s[0] + c->fb[1] * s[1] + c->fb[2] * s[2];
+    s[2] = s[1];
+    s[1] = s[0];
+    s[0] = v;
+    return v;
+}
+
+/* Raw donor corrections (Y, M, C) and raw log exposure (B, G, R) per pixel, from the
+ * source image (carrier == NULL) or carrier planes B, G, R (:124-214). */
+int oracle_dir_source(const FjPreparedHostData* h, const float* src, long src_row_floats, int comps,
+                      const float* cb, const float* cg, const float* cr, int W, int H, float* y_out, float* m_out,
+                      float* c_out, float* lb, float* lg, float* lr, unsigned* flags_out) {
+    Packed pk;
+    if (pack(h, &pk)) {
+        free(pk.lut_store);
+        return 1;
+    }
+    const Pack* p = &pk.p;
+    unsigned flags = 0;
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            size_t i = (size_t)y * W + x;
+            float e[3];
+            if (cb) {
+                e[0] = fmaxf(0.0f, cb[i] * p->route);
+                e[1] = fmaxf(0.0f, cg[i] * p->route);
+                e[2] = fmaxf(0.0f, cr[i] * p->route);
+            } else {
+                film_exposure(p, src + (size_t)y * src_row_floats + (size_t)x * comps, 1.0f, 1, e);
+            }
+            float logE[3], layer[3];
+            for (int c = 0; c < 3; ++c) {
+                logE[c] = log10f(fmaxf(e[c], 0.0f) + 1e-10f);
+                layer[c] = curve_at(&p->dens[c], inf_clamp(&p->dens[c], logE[c]), p->gamma_bgr[c]);
+            }
+            float donor[3] = {p->dmax[0] - layer[0], p->dmax[1] - layer[1], p->dmax[2] - layer[2]};
+            unsigned fail = 0;
+            if (p->dir_mode == FJ_DIR_NEGATIVE_DONOR_LANGMUIR)
+                for (int c = 0; c < 3; ++c)
+                    if (!langmuir(layer[c], p->dk[c], p->dref[c], &donor[c])) fail |= 1u << c;
+            float corr[3];
+            corr[0] = p->M[0] * donor[0] + p->M[3] * donor[1] + p->M[6] * donor[2];
+            corr[1] = p->M[1] * donor[0] + p->M[4] * donor[1] + p->M[7] * donor[2];
+            corr[2] = p->M[2] * donor[0] + p->M[5] * donor[1] + p->M[8] * donor[2];
+            for (int c = 0; c < 3; ++c)
+                if (!isfinite(corr[c])) fail |= 1u << c;
+            if (fail) flags |= (1u << 8) | ((fail & 7u) << 9);
+            y_out[i] = corr[0];
+            m_out[i] = corr[1];
+            c_out[i] = corr[2];
+            lb[i] = logE[0];
+            lg[i] = logE[1];
+            lr[i] = logE[2];
+        }
+    free(pk.lut_store);
+    if (flags_out) *flags_out = flags;
+    return 0;
+}
+
+/* filtered = sum over components in order of weight * G(raw), the reference's
+ * per-component schedule (:940-1060) with its FP64 accumulations. */
+int oracle_dir_blur(const OracleDirComp* comps, int n, const float* raw, int W, int H, float* filtered) {
+    size_t N = (size_t)W * H;
+    float* tmp = (float*)malloc(N * sizeof(float));
+    float* fwd = (float*)malloc(N * sizeof(float));
+    if (!tmp || !fwd) return 1;
+    int first = 1;
+    for (int k = 0; k < n; ++k) {
+        const OracleDirComp* c = &comps[k];
+        if (!(c->weight > 0.0f)) continue;
+        if (c->op == 1) {
+            for (size_t i = 0; i < N; ++i) {
+                float wv = raw[i] * c->weight;
+                filtered[i] = first ? wv : filtered[i] + wv;
+            }
+        } else if (c->op == 2) {
+            int r = c->radius;
+            for (int y = 0; y < H; ++y)
+                for (int x = 0; x < W; ++x) {
+                    double s = 0.0;
+                    for (int o = -r; o <= r; ++o)
+                        s += (double)raw[(size_t)y * W + reflect_dir(x + o, W)] * (double)c->taps[o + r];
+                    tmp[(size_t)y * W + x] = isfinite(s) ? (float)s : 0.0f;
+                }
+            for (int y = 0; y < H; ++y)
+                for (int x = 0; x < W; ++x) {
+                    double s = 0.0;
+                    for (int o = -r; o <= r; ++o)
+                        s += (double)tmp[(size_t)reflect_dir(y + o, H) * W + x] * (double)c->taps[o + r];
+                    float b = isfinite(s) ? (float)s : 0.0f;
+                    float wv = b * c->weight;
+                    size_t i = (size_t)y * W + x;
+                    filtered[i] = first ? wv : filtered[i] + wv;
+                }
+        } else {
+            for (int y = 0; y < H; ++y) {
+                const float* in = raw + (size_t)y * W;
+                float* out = tmp + (size_t)y * W;
+                double anchor = (double)in[0];
+                double s[3] = {anchor, anchor, anchor};
+                for (int i = 0; i < c->h_len; ++i) {
+                    double d = (double)in[i] - anchor;
+                    for (int hh = 0; hh < 3; ++hh) s[hh] += c->h_init[hh * c->h_len + i] * d;
+                }
+                for (int x = 0; x < W; ++x) out[x] = (float)iir(c, (double)in[x], s);
+                int ts = c->h_ts;
+                double term[3] = {0, 0, 0}, last = s[0];
+                for (int rr = 0; rr < ts; ++rr) {
+                    double v = last;
+                    for (int q = 0; q < ts; ++q) v += c->h_term[rr * ts + q] * (s[ts - 1 - q] - last);
+                    term[rr] = v;
+                    out[W - ts + rr] = (float)v;
+                }
+                for (int hh = 0; hh < ts; ++hh) s[hh] = term[hh];
+                for (int x = W - ts - 1; x >= 0; --x) out[x] = (float)iir(c, (double)out[x], s);
+            }
+            for (int x = 0; x < W; ++x) {
+                double anchor = (double)tmp[(size_t)(H - 1) * W + x];
+                double s[3] = {anchor, anchor, anchor};
+                for (int i = 0; i < c->v_len; ++i) {
+                    double d = (double)tmp[(size_t)(H - 1 - i) * W + x] - anchor;
+                    for (int hh = 0; hh < 3; ++hh) s[hh] += c->v_init[hh * c->v_len + i] * d;
+                }
+                for (int vy = 0; vy < H; ++vy) {
+                    size_t i = (size_t)(H - 1 - vy) * W + x;
+                    fwd[i] = (float)iir(c, (double)tmp[i], s);
+                }
+                int ts = c->v_ts;
+                double term[3] = {0, 0, 0}, last = s[0];
+                for (int rr = 0; rr < ts; ++rr) {
+                    double v = last;
+                    for (int q = 0; q < ts; ++q) v += c->v_term[rr * ts + q] * (s[ts - 1 - q] - last);
+                    term[rr] = v;
+                    int vy = H - ts + rr;
+                    size_t i = (size_t)(H - 1 - vy) * W + x;
+                    float wv = (float)v * c->weight;
+                    filtered[i] = first ? wv : filtered[i] + wv;
+                }
+                for (int hh = 0; hh < ts; ++hh) s[hh] = term[hh];
+                for (int vy = H - ts - 1; vy >= 0; --vy) {
+                    size_t i = (size_t)(H - 1 - vy) * W + x;
+                    double v = iir(c, (double)fwd[i], s);
+                    float wv = (float)v * c->weight;
+                    filtered[i] = first ? wv : filtered[i] + wv;
+                }
+            }
+        }
+        first = 0;
+    }
+    free(tmp);
+    free(fwd);
+    return 0;
+}
+
+/* Capture density from filtered corrections + cached log exposure
+ * (src/Cuda/JuicerCudaDeviceHelpers.cuh:1267-1328); planes C, M, Y out. */
+int oracle_develop_spatial(const FjPreparedHostData* h, const float* fy, const float* fm, const float* fc,
+                           const float* lb, const float* lg, const float* lr, int W, int H, float* oc, float* om,
+                           float* oy, unsigned* flags_out) {
+    Packed pk;
+    if (pack(h, &pk)) {
+        free(pk.lut_store);
+        return 1;
+    }
+    const Pack* p = &pk.p;
+    unsigned flags = 0;
+    for (size_t i = 0; i < (size_t)W * H; ++i) {
+        float corr[3] = {fy[i], fm[i], fc[i]};
+        unsigned fail = 0;
+        if (p->dir_mode == FJ_DIR_POSITIVE_RECEIVER_LANGMUIR)
+            for (int c = 0; c < 3; ++c) {
+                if (p->rcref[c] == 0.0f) {
+                    corr[c] = 0.0f;
+                    continue;
+                }
+                float v = corr[c];
+                if (!langmuir(v, p->rkr[c], p->rcref[c], &corr[c])) fail |= 1u << c;
+            }
+        float lc[3];
+        const float lraw[3] = {lb[i], lg[i], lr[i]};
+        if (!fail)
+            for (int c = 0; c < 3; ++c) {
+                float o = lraw[c];
+                if (isnan(o)) {
+                    fail |= 1u << c;
+                    continue;
+                }
+                lc[c] = o - corr[c];
+                if ((!isinf(o) && !isfinite(lc[c])) || (isinf(o) && (!isinf(lc[c]) || signbit(o) != signbit(lc[c]))))
+                    fail |= 1u << c;
+            }
+        if (fail) {
+            flags |= (1u << 8) | ((fail & 7u) << 9);
+            oc[i] = om[i] = oy[i] = nanf("");
+            continue;
+        }
+        for (int c = 0; c < 3; ++c) lc[c] = inf_clamp(&p->dens[c], lc[c]);
+        oy[i] = curve_at(&p->dirc[0], lc[0], p->gamma_bgr[0]);
+        om[i] = curve_at(&p->dirc[1], lc[1], p->gamma_bgr[1]);
+        oc[i] = curve_at(&p->dirc[2], lc[2], p->gamma_bgr[2]);
+    }
+    free(pk.lut_store);
+    if (flags_out) *flags_out = flags;
+    return 0;
+}

@@ -308,3 +308,99 @@ extern "C" int ref_scatter_halation(const FjScatterHalation* d, float* r, float*
     cudaFree(acc);
     return (int)e;
 }
+
+// Spatial DIR with the reference's own kernels (src/Cuda/Film/JuicerCudaFilmPipeline.cu:1479
+// juicer_cuda_build_print_spatial_dir). `comps` lists the frame's components in order
+// (core first), with boundary weights and FIR taps computed on the host; outputs are
+// device planes.
+struct RefDirComp {
+    int op;
+    float weight;
+    int radius;
+    const float* taps;
+    double ff, fb[3];
+    const double* h_init;
+    int h_len, h_ts;
+    double h_term[9];
+    const double* v_init;
+    int v_len, v_ts;
+    double v_term[9];
+};
+
+extern "C" cudaError_t juicer_cuda_build_print_spatial_dir(const JuicerCuda::PrintPipelineRunParams*,
+                                                          JuicerCuda::SpatialDirBuildRequest);
+
+extern "C" int ref_spatial_dir(const FjPreparedHostData* h, const float* const* lut, const float* src,
+                               long src_row_bytes, int width, int height, int comps_n, const RefDirComp* comps,
+                               int count, float* fy, float* fm, float* fc, float* lb, float* lg, float* lr) {
+    Arena a;
+    unsigned* d_flags = nullptr;
+    if (cudaMalloc(&d_flags, sizeof(unsigned)) != cudaSuccess) return 2;
+    cudaMemset(d_flags, 0, sizeof(unsigned));
+    a.ptrs.push_back(d_flags);
+    JuicerCuda::PipelineRunParams p;
+    if (!pack(*h, lut, a, p, d_flags)) return 1;
+    JuicerCuda::PrintPipelineRunParams q{};
+    q.src = src;
+    q.srcRowBytes = (size_t)src_row_bytes;
+    q.dst = fy;
+    q.dstRowBytes = (size_t)src_row_bytes;
+    q.width = width;
+    q.height = height;
+    q.nComponents = comps_n;
+    q.filmExpose = p.filmExpose;
+    q.filmDevelop = p.filmDevelop;
+    q.printExpose = p.printExpose;
+    q.printDevelop = p.printDevelop;
+    q.scanStage = p.scanStage;
+    q.filmRaw = p.filmRaw;
+    const size_t plane = (size_t)width * height;
+    float* work = nullptr;
+    if (cudaMalloc(&work, 6 * plane * sizeof(float)) != cudaSuccess) return 2;
+    a.ptrs.push_back(work);
+    JuicerCuda::SpatialDirBuildRequest req{};
+    req.planes.rawCorrectionY = work;
+    req.planes.rawCorrectionM = work + plane;
+    req.planes.rawCorrectionC = work + 2 * plane;
+    req.planes.filterTemp = work + 3 * plane;
+    req.planes.filterTempM = work + 4 * plane;
+    req.planes.filterTempC = work + 5 * plane;
+    req.planes.filteredCorrectionY = fy;
+    req.planes.filteredCorrectionM = fm;
+    req.planes.filteredCorrectionC = fc;
+    req.planes.logRawB = lb;
+    req.planes.logRawG = lg;
+    req.planes.logRawR = lr;
+    JuicerCuda::SpatialDirFilterSpec* specs[4] = {&req.gaussian, &req.tails[0], &req.tails[1], &req.tails[2]};
+    for (int k = 0; k < count && k < 4; ++k) {
+        const RefDirComp& c = comps[k];
+        JuicerCuda::SpatialDirFilterSpec& s = *specs[k];
+        s.weight = c.weight;
+        s.radius = c.radius;
+        s.sigma = 0.0f;
+        if (c.op == 1) {
+            s.filterOperator = JuicerCuda::SpatialDirFilterOperator::Identity;
+        } else if (c.op == 2) {
+            s.filterOperator = JuicerCuda::SpatialDirFilterOperator::FirReflect;
+            s.kernel = a.put(c.taps, (size_t)(2 * c.radius + 1));
+            s.sigma = 1.0f; // eligibility only: FIR requires 0 < sigma < 3
+        } else if (c.op == 3) {
+            s.filterOperator = JuicerCuda::SpatialDirFilterOperator::YvvReflect;
+            s.radius = 0;
+            s.sigma = 3.0f; // eligibility only: recursion requires sigma >= 3
+            s.iir.feedforward = c.ff;
+            for (int i = 0; i < 3; ++i) s.iir.feedback[i] = c.fb[i];
+            s.horizontalBoundary.initialWeights = a.put(c.h_init, (size_t)3 * c.h_len);
+            s.horizontalBoundary.initialWeightLength = c.h_len;
+            s.horizontalBoundary.terminalSize = c.h_ts;
+            for (int i = 0; i < 9; ++i) s.horizontalBoundary.terminalMatrix[i] = c.h_term[i];
+            s.verticalBoundary.initialWeights = a.put(c.v_init, (size_t)3 * c.v_len);
+            s.verticalBoundary.initialWeightLength = c.v_len;
+            s.verticalBoundary.terminalSize = c.v_ts;
+            for (int i = 0; i < 9; ++i) s.verticalBoundary.terminalMatrix[i] = c.v_term[i];
+        }
+    }
+    cudaError_t e = juicer_cuda_build_print_spatial_dir(&q, req);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return (int)e;
+}

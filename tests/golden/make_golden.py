@@ -46,6 +46,40 @@ def scanner_cases():
     print("scanner cases:", len(names))
 
 
+def dir_boundary_cases():
+    """Reflected-YVV boundary characterization (tests/dir/boundary-fixtures): inputs and
+    the exact binary64 words of both axes' weights and terminal matrices."""
+    base = os.path.join(REF, "tests", "dir", "boundary-fixtures")
+    with open(os.path.join(base, "inputs.json")) as fh:
+        inputs = json.load(fh)["cases"]
+    with open(os.path.join(base, "linux-release.json")) as fh:
+        outputs = {c["input"]["name"] if "name" in c.get("input", {}) else i: c
+                   for i, c in enumerate(json.load(fh)["cases"])}
+    out = {}
+    names = []
+    for i, case in enumerate(inputs):
+        res = outputs.get(case["name"], outputs.get(i))
+        if res is None or not res.get("success"):
+            continue
+        cid = f"c{i:03d}"
+        names.append(cid)
+        comp = case["component"]
+        out[f"{cid}__u32"] = np.array([comp["sigma"], comp["weight"]], dtype=np.uint32)
+        out[f"{cid}__i32"] = np.array([comp["radius"], comp["operator"], comp["version"], case["width"],
+                                       case["height"]], dtype=np.int64)
+        out[f"{cid}__f64"] = np.array([comp["feedforward"], *comp["feedback"], comp["denominator"],
+                                       comp["numerator"], *comp["numerators"], comp["accuracy"],
+                                       comp["tolerance"]], dtype=np.uint64)
+        for axis in ("horizontal", "vertical"):
+            ax = res[axis]
+            out[f"{cid}__{axis}_meta"] = np.array([ax["length"], ax["terminal_size"]], dtype=np.int64)
+            out[f"{cid}__{axis}_weights"] = np.array(ax["weights"], dtype=np.uint64)
+            out[f"{cid}__{axis}_terminal"] = np.array(ax["terminal"], dtype=np.uint64)
+    out["names"] = np.array(names)
+    np.savez_compressed(os.path.join(HERE, "dir_boundary_cases.npz"), **out)
+    print("dir boundary cases:", len(names))
+
+
 def recipes():
     sys.path.insert(0, ROOT)
     import __graft_entry__
@@ -61,4 +95,5 @@ def recipes():
 
 if __name__ == "__main__":
     scanner_cases()
+    dir_boundary_cases()
     recipes()
