@@ -67,6 +67,11 @@ _EXPORTS = {
     "fjb_dir_boundary_host": (abi.FjStatus, [C.POINTER(abi.FjDirGaussian), C.c_int32, C.POINTER(C.c_double),
                                              C.c_size_t, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                              C.POINTER(C.c_double), C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_diffusion_components_host": (abi.FjStatus, [C.POINTER(abi.FjDiffusion), C.POINTER(abi.FjDiffusionComponents),
+                                                     C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_diffusion": (abi.FjStatus, [C.POINTER(abi.FjDiffusionComponents), C.c_int32, C.c_double] +
+                      [C.c_void_p] * 6 + [C.c_ssize_t, C.c_int32, C.c_int32, C.c_void_p,
+                                          C.POINTER(abi.FjErrorBuffer)]),
     "fjb_scanner_lut_build_host": (abi.FjStatus, [C.POINTER(abi.FjbScannerLutInput)] + [C.c_void_p] * 6 +
                                    [C.POINTER(abi.FjErrorBuffer)]),
 }

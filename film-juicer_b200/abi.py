@@ -245,6 +245,8 @@ FjPreparedHostData = _s("FjPreparedHostData", [
     ("scanner_correction", FjScannerCorrection), ("scanner_post", FjScannerPostEffects),
     ("output_color", FjOutputColor), ("print", FjPrint), ("optics", FjOptics), ("spatial_dir", FjSpatialDir),
     ("grain", FjVisualGrain), ("effects", FjFilmEffects), ("noise", FjStaticNoise)])
+FjDiffusionComponents = _s("FjDiffusionComponents", [("lambda_px", f64 * 9), ("red_weights", f64 * 9),
+                                                     ("green_weights", f64 * 9), ("blue_weights", f64 * 9)])
 FjbScannerLutInput = _s("FjbScannerLutInput", [
     ("eps_c", FjFloatSpan), ("eps_m", FjFloatSpan), ("eps_y", FjFloatSpan), ("weighted_x", FjFloatSpan),
     ("weighted_y", FjFloatSpan), ("weighted_z", FjFloatSpan), ("baseline_min", FjFloatSpan),
@@ -259,7 +261,7 @@ ALL_RECORDS = [
     FjScannerCorrection, FjScannerPostEffects, FjOutputEncoding, FjOutputColor, FjPrint, FjDiffusion,
     FjHalationGaussian, FjHalationChannel, FjScatterHalation, FjHighlightBoost, FjOptics, FjDirGaussian,
     FjSpatialDir, FjGrainGaussian, FjVisualGrain, FjDust, FjScratch, FjDefectOrigin, FjFilmEffects,
-    FjStaticNoise, FjPreparedHostData, FjbScannerLutInput,
+    FjStaticNoise, FjPreparedHostData, FjbScannerLutInput, FjDiffusionComponents,
 ]
 
 

@@ -80,3 +80,23 @@ def spatial_dir_record(pixel_size_um: float, width: int, height: int, *, diffusi
         _dir_component(sd.components[i], s, w)
     sd.recipe_hash = sd.hash = 1
     return sd
+
+
+def diffusion_record(pixel_size_um: float, width: int, *, family: int = 2, scatter_fraction: float = 0.12,
+                     group_weights=(0.55, 0.30, 0.15), group_lambda_um=(8.0, 40.0, 150.0), warmth: float = 0.3,
+                     spatial_scale: float = 1.0, radius_fraction_of_width: float = 0.005) -> "abi.FjDiffusion":
+    """A camera diffusion filter record; the radius is the given fraction of the frame
+    width (0.5 % -> 10 px at 1920, 20 px at 3840, the configuration of the 1080p/4K
+    benchmarks)."""
+    d = abi.FjDiffusion()
+    d.family = family
+    d.scatter_fraction = scatter_fraction
+    for i in range(3):
+        d.group_weights[i] = group_weights[i]
+        d.group_lambda_um[i] = group_lambda_um[i]
+    d.warmth = warmth
+    d.spatial_scale = spatial_scale
+    d.pixel_size_um = pixel_size_um
+    d.radius_px = max(1, int(round(radius_fraction_of_width * width)))
+    d.sample_hash = d.hash = 1
+    return d

@@ -233,3 +233,24 @@ def scatter_halation(descriptor: "abi.FjScatterHalation", planes_rgb, stream=Non
                                   C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
     _check("fjb_scatter_halation", st, err)
     return scratch
+
+
+def diffusion_components(diffusion: "abi.FjDiffusion") -> "abi.FjDiffusionComponents":
+    """The nine PSF components of a diffusion record (host computation in the library)."""
+    lib = load_library()
+    out = abi.FjDiffusionComponents()
+    err = abi.ErrorText()
+    _check("fjb_diffusion_components_host", lib.fjb_diffusion_components_host(C.byref(diffusion), C.byref(out),
+                                                                              C.byref(err.buf)), err)
+    return out
+
+
+def diffusion(components, radius: int, fraction: float, src_rgb, dst_rgb, stream=None):
+    """dst = (1 - f) src + f (PSF * src) for three CUDA planes (R, G, B)."""
+    lib = load_library()
+    err = abi.ErrorText()
+    h, w = src_rgb[0].shape
+    st = lib.fjb_diffusion(C.byref(components), radius, fraction, *[C.c_void_p(_ptr(t)) for t in src_rgb],
+                           *[C.c_void_p(_ptr(t)) for t in dst_rgb], src_rgb[0].stride(0), w, h,
+                           C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+    _check("fjb_diffusion", st, err)

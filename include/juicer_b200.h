@@ -130,6 +130,32 @@ FjStatus fjb_dir_boundary_host(const FjDirGaussian* component, int32_t axis_leng
                                size_t weights_capacity, int32_t* out_length, int32_t* out_terminal_size,
                                double* terminal, FjErrorBuffer* error);
 
+/* Nine exponential PSF components and their per-channel weights, as the host's
+ * diffusion preparation produces them (reference native/juicer_diffusion_api.h:18-20,
+ * fj_diffusion_components_prepare). */
+typedef struct FjDiffusionComponents {
+    double lambda_px[9];
+    double red_weights[9];
+    double green_weights[9];
+    double blue_weights[9];
+} FjDiffusionComponents;
+
+/* Expands a diffusion filter record into its nine PSF components on the host (the
+ * preparation the reference obtains from fj_diffusion_components_prepare,
+ * native/juicer_diffusion_api.h:63). */
+FjStatus fjb_diffusion_components_host(const FjDiffusion* diffusion, FjDiffusionComponents* out,
+                                       FjErrorBuffer* error);
+
+/* Camera or enlarger diffusion (reference src/Cuda/Diffusion/JuicerCudaDiffusion.cu:779
+ * JuicerCuda::Diffusion::launch_stage): dst_c = (1 - f) src_c + f (PSF_c * src_c) with
+ * PSF_c = sum_k w_ck exp(-rho / lambda_k) / (2 pi lambda_k^2) on the (2r+1)^2 grid,
+ * normalised, and whole-sample reflection at the frame border. Planes R, G, B with
+ * `stride` floats per row; dst must not alias src. radius_px <= 80. */
+FjStatus fjb_diffusion(const FjDiffusionComponents* components, int32_t radius_px, double scatter_fraction,
+                       const float* src_r, const float* src_g, const float* src_b, float* dst_r, float* dst_g,
+                       float* dst_b, ptrdiff_t stride, int32_t width, int32_t height, void* stream,
+                       FjErrorBuffer* error);
+
 /* Scanner LUT input record (reference native/juicer_cuda_frame_values.h FjScannerLutInput). */
 typedef struct FjbScannerLutInput {
     FjFloatSpan eps_c, eps_m, eps_y;

@@ -39,3 +39,73 @@ def reference_scatter_halation(torch, descriptor, planes_rgb):
     if rc != 0:
         raise RuntimeError(f"reference scatter/halation returned cudaError {rc}")
     return [t.cpu().numpy() for t in dev]
+
+
+def diffusion(components, radius, fraction, planes_rgb):
+    """CPU oracle of the diffusion stage; returns new planes (R, G, B)."""
+    lib = _o.load()
+    fn = lib.oracle_diffusion
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, C.c_double,
+                   C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int, C.c_int]
+    lam = (C.c_double * 9)(*components.lambda_px)
+    w = (C.c_double * 27)(*components.red_weights, *components.green_weights, *components.blue_weights)
+    src = [np.ascontiguousarray(p, dtype=np.float32) for p in planes_rgb]
+    out = [np.zeros_like(p) for p in src]
+    h, wd = src[0].shape
+    sp = (C.c_void_p * 3)(*[p.ctypes.data for p in src])
+    dp = (C.c_void_p * 3)(*[p.ctypes.data for p in out])
+    if fn(lam, w, radius, fraction, sp, dp, wd, h) != 0:
+        raise RuntimeError("oracle_diffusion failed")
+    return out
+
+
+def diffusion_components(family, group_weights, group_lambda_um, warmth, spatial_scale, pixel_size_um):
+    """Pure-Python restatement of the reference's diffusion component expansion
+    (rust/film-juicer-core/src/optics/diffusion_frame.rs:285-421: expand_group,
+    halo_weights, Components::new). Returns (lambda_px[9], weights[3][9]) as lists."""
+    import math
+
+    def expand(center, spread, count, alpha):
+        lo, hi = math.log(center / spread), math.log(center * spread)
+        lam, w = [], []
+        for i in range(count):
+            if i + 1 == count:
+                ll = hi
+            elif i != 0:
+                ll = lo + (hi - lo) * (i / (count - 1))
+            else:
+                ll = lo
+            lam.append(math.exp(ll))
+            w.append(lam[-1] ** (2.0 - alpha) if alpha is not None else 1.0)
+        t = 0.0
+        for v in w:
+            t += v
+        return lam, [v / t for v in w]
+
+    core = expand(group_lambda_um[0], 1.5, 2, None)
+    halo = expand(group_lambda_um[1], 2.0, 3, None)
+    bloom = expand(group_lambda_um[2], 2.5, 4, (3.2, 3.5, 2.9, 2.5)[family])
+    grad = [-1.0 + 2.0 * i / 2 for i in range(3)]
+    target = 0.0
+    wg = 0.0
+    for i in range(3):
+        target += halo[1][i]
+        wg += halo[1][i] * grad[i]
+    wg /= target
+    grad = [g - wg for g in grad]
+    halo_rgb = []
+    for axis in (1.30, 0.15, -1.45):
+        row = [max(halo[1][i] * (1.0 + warmth * axis * grad[i]), 0.0) for i in range(3)]
+        t = 0.0
+        for v in row:
+            t += v
+        halo_rgb.append([v * (target / t) for v in row] if t > 0.0 else list(halo[1]))
+    scale = max(spatial_scale, 1e-6)
+    lam_px, weights = [], [[], [], []]
+    for gi, (lam, w) in enumerate((core, halo, bloom)):
+        for i, l in enumerate(lam):
+            lam_px.append(max(l * scale / pixel_size_um, 1e-6))
+            for c in range(3):
+                weights[c].append(group_weights[1] * halo_rgb[c][i] if gi == 1 else group_weights[gi] * w[i])
+    return lam_px, weights

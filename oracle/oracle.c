@@ -1322,3 +1322,55 @@ int oracle_develop_spatial(const FjPreparedHostData* h, const float* fy, const f
     if (flags_out) *flags_out = flags;
     return 0;
 }
+
+/* ---------------- diffusion (src/Cuda/Diffusion/JuicerCudaDiffusion.cu:294-487) ----------------
+ * PSF in FP64, stored as float, normalised by the FP64 sum of the stored floats; the
+ * convolution is evaluated directly in FP64 over the whole-sample-reflected frame
+ * (the reference's reflect-padded FFT tiles compute the same linear convolution). */
+static long reflect_whole(long i, long n) {
+    if (n <= 1) return 0;
+    long period = 2 * (n - 1);
+    long v = i % period;
+    if (v < 0) v += period;
+    return v < n ? v : period - v;
+}
+
+int oracle_diffusion(const double* lambda_px, const double* weights /* [3][9] R,G,B */, int radius, double fraction,
+                     const float* const* src, float* const* dst, int W, int H) {
+    int d = 2 * radius + 1;
+    float* psf = (float*)malloc((size_t)d * d * sizeof(float));
+    if (!psf) return 1;
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int c = 0; c < 3; ++c) {
+        double sum = 0.0;
+        for (int iy = 0; iy < d; ++iy)
+            for (int ix = 0; ix < d; ++ix) {
+                int dx = ix - radius, dy = iy - radius;
+                double rho = sqrt((double)dx * dx + (double)dy * dy);
+                double v = 0.0;
+                for (int k = 0; k < 9; ++k) {
+                    double l = lambda_px[k];
+                    v += weights[c * 9 + k] * exp(-rho / l) / (two_pi * l * l);
+                }
+                psf[(size_t)iy * d + ix] = (float)v;
+                sum += (double)(float)v;
+            }
+        for (size_t i = 0; i < (size_t)d * d; ++i) psf[i] = (float)((double)psf[i] / sum);
+        const float f = (float)fraction;
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x) {
+                double acc = 0.0;
+                for (int iy = 0; iy < d; ++iy) {
+                    long sy = reflect_whole(y + iy - radius, H);
+                    for (int ix = 0; ix < d; ++ix) {
+                        long sx = reflect_whole(x + ix - radius, W);
+                        acc += (double)psf[(size_t)iy * d + ix] * (double)src[c][sy * W + sx];
+                    }
+                }
+                float cur = src[c][(size_t)y * W + x];
+                dst[c][(size_t)y * W + x] = (1.0f - f) * cur + f * (float)acc;
+            }
+    }
+    free(psf);
+    return 0;
+}

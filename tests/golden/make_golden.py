@@ -4,6 +4,18 @@ container, where the reference is mounted read-only).
 * scanner_lut_cases.npz: the reference's scanner LUT characterization
   (tests/scanner/lut-fixtures/native.json): every case's input words and the exact
   f32 words of the six arrays the native builder produced.
+* diffusion_component_cases.npz: the reference's diffusion component
+  characterization (tests/diffusion/frame-fixtures/manifest.json, production cases
+  "diffusion/components/*"): input words (family, 3 group weights, 3 group centers,
+  warmth, spatial scale, pixel size, radius, hash) and the 36 binary64 output words
+  (lambda_px, red, green, blue weights), or the failure flag.
+* diffusion_images.npz: the reference's external diffusion cohort
+  (tests/diffusion/fixtures/diffusion_reference_v1.{json,npz}, produced by the
+  upstream model the reference ports): 17x19, 16x18, 23x11, 11x23 RGB inputs, the
+  filter parameters of each case mapped onto the diffusion record (group weights =
+  family weights x intensities, group centres = family centres x sizes, warmth =
+  family base + halo warmth clamped to [-1.5, 1.5], scatter fraction from the
+  strength table) and the float32 outputs.
 * recipe_direct.npz / recipe_print.npz: prepared recipes (film_juicer_b200.prepare)
   for kodak_portra_400 direct and kodak_portra_400 -> kodak_portra_endura print,
   built from the reference's Resources/ profiles and spectral tables.
@@ -80,6 +92,58 @@ def dir_boundary_cases():
     print("dir boundary cases:", len(names))
 
 
+def diffusion_component_cases():
+    with open(os.path.join(REF, "tests", "diffusion", "frame-fixtures", "manifest.json")) as fh:
+        m = json.load(fh)
+    inputs = m["production_inputs"]
+    names, words, outputs, failed = [], [], [], []
+    for case in m["production_cases"]:
+        if not case["case"].startswith("diffusion/components/"):
+            continue
+        names.append(case["case"])
+        words.append(np.array(inputs[case["case"]]["words"], dtype=np.uint64))
+        outputs.append(np.array(case["output"], dtype=np.uint64))
+        failed.append(case["envelope"][0] != 0)
+    np.savez_compressed(os.path.join(HERE, "diffusion_component_cases.npz"), names=np.array(names),
+                        words=np.stack(words), outputs=np.stack(outputs), failed=np.array(failed))
+    print("diffusion component cases:", len(names))
+
+
+def diffusion_images():
+    base = os.path.join(REF, "tests", "diffusion", "fixtures")
+    with open(os.path.join(base, "diffusion_reference_v1.json")) as fh:
+        j = json.load(fh)
+    z = np.load(os.path.join(base, "diffusion_reference_v1.npz"))
+    families = {c["family"]: c for c in j["family_cases"]}
+    order = j["family_order"]
+    fractions = {(c["family"], c["strength"]): c["scatter_fraction"] for c in j["strength_cases"]}
+    inputs, input_names = [], []
+    out = {"names": [], "input_index": [], "family": [], "params": [], "radius": [], "outputs": []}
+    for case in j["image_cases"] + j["radius_cases"] + j["hdr_cases"]:
+        p, f = case["params"], families[case["family"]]
+        weights = (f["w_c"] * p["core_intensity"], f["w_h"] * p["halo_intensity"], f["w_b"] * p["bloom_intensity"])
+        centers = (f["core"]["lambda_um"] * p["core_size"], f["halo"]["lambda_um"] * p["halo_size"],
+                   f["bloom"]["lambda_um"] * p["bloom_size"])
+        warmth = max(-1.5, min(1.5, f["halo_warmth_base"] + p["halo_warmth"]))
+        if case["input_array"] not in input_names:
+            input_names.append(case["input_array"])
+            inputs.append(z[case["input_array"]])
+        out["names"].append(case["output_array"])
+        out["input_index"].append(input_names.index(case["input_array"]))
+        out["family"].append(order.index(case["family"]))
+        out["params"].append([*weights, *centers, warmth, p["spatial_scale"], case["pixel_size_um"],
+                              fractions[(case["family"], p["strength"])]])
+        out["radius"].append(case["psf_radius"])
+        out["outputs"].append(z[case["output_array"]])
+    arrays = {k: np.array(v) for k, v in out.items() if k != "outputs"}
+    for i, a in enumerate(inputs):
+        arrays[f"input_{i}"] = a
+    for i, a in enumerate(out["outputs"]):
+        arrays[f"output_{i}"] = a
+    np.savez_compressed(os.path.join(HERE, "diffusion_images.npz"), **arrays)
+    print("diffusion image cases:", len(out["names"]))
+
+
 def recipes():
     sys.path.insert(0, ROOT)
     import __graft_entry__
@@ -96,4 +160,6 @@ def recipes():
 if __name__ == "__main__":
     scanner_cases()
     dir_boundary_cases()
+    diffusion_component_cases()
+    diffusion_images()
     recipes()
