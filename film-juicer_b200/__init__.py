@@ -72,6 +72,9 @@ _EXPORTS = {
     "fjb_diffusion": (abi.FjStatus, [C.POINTER(abi.FjDiffusionComponents), C.c_int32, C.c_double] +
                       [C.c_void_p] * 6 + [C.c_ssize_t, C.c_int32, C.c_int32, C.c_void_p,
                                           C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_diffusion_no_alloc": (abi.FjStatus, [C.POINTER(abi.FjDiffusionComponents), C.c_int32, C.c_double] +
+                               [C.c_void_p] * 6 + [C.c_ssize_t, C.c_int32, C.c_int32, C.c_void_p,
+                                                   C.POINTER(abi.FjErrorBuffer)]),
     "fjb_scanner_lut_build_host": (abi.FjStatus, [C.POINTER(abi.FjbScannerLutInput)] + [C.c_void_p] * 6 +
                                    [C.POINTER(abi.FjErrorBuffer)]),
 }

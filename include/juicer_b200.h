@@ -156,6 +156,22 @@ FjStatus fjb_diffusion(const FjDiffusionComponents* components, int32_t radius_p
                        float* dst_b, ptrdiff_t stride, int32_t width, int32_t height, void* stream,
                        FjErrorBuffer* error);
 
+/* Same result as fjb_diffusion (to FP32 rounding of the PSF tables), for hosts that
+ * cannot allocate device memory while rendering. No counterpart in the reference.
+ * It allocates nothing: the PSF tables are built on the device into one static
+ * device array of 3 x 81 x 176 floats (167 KiB) per device, and the call only
+ * enqueues two kernels on `stream`, without synchronising. Limits: radius_px <= 80
+ * (larger is rejected with FJ_STATUS_UNSUPPORTED_INPUT); weights finite and
+ * non-negative, as fjb_diffusion_components_host produces them; the array is shared
+ * by all calls on a device, so calls that may overlap (other streams or host threads)
+ * race and must be ordered by the caller. The first call on each device looks up the
+ * array's device address with that device current; make it before any stream
+ * capture begins. */
+FjStatus fjb_diffusion_no_alloc(const FjDiffusionComponents* components, int32_t radius_px, double scatter_fraction,
+                                const float* src_r, const float* src_g, const float* src_b, float* dst_r,
+                                float* dst_g, float* dst_b, ptrdiff_t stride, int32_t width, int32_t height,
+                                void* stream, FjErrorBuffer* error);
+
 /* Scanner LUT input record (reference native/juicer_cuda_frame_values.h FjScannerLutInput). */
 typedef struct FjbScannerLutInput {
     FjFloatSpan eps_c, eps_m, eps_y;
