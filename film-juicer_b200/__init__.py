@@ -75,6 +75,13 @@ _EXPORTS = {
     "fjb_diffusion_no_alloc": (abi.FjStatus, [C.POINTER(abi.FjDiffusionComponents), C.c_int32, C.c_double] +
                                [C.c_void_p] * 6 + [C.c_ssize_t, C.c_int32, C.c_int32, C.c_void_p,
                                                    C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_noise_create": (abi.FjStatus, [C.POINTER(abi.FjStaticNoise), C.c_void_p, C.POINTER(C.c_void_p),
+                                        C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_noise_destroy": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_visual_grain_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
+    "fjb_visual_grain": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjVisualGrain), C.c_void_p] + [C.c_void_p] * 3 +
+                         [C.c_ssize_t, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, C.c_void_p,
+                          C.POINTER(abi.FjErrorBuffer)]),
     "fjb_scanner_lut_build_host": (abi.FjStatus, [C.POINTER(abi.FjbScannerLutInput)] + [C.c_void_p] * 6 +
                                    [C.POINTER(abi.FjErrorBuffer)]),
 }

@@ -87,6 +87,11 @@ FJ_DIR_OPERATOR_IDENTITY = 1
 FJ_DIR_OPERATOR_FIR_REFLECT = 2
 FJ_DIR_OPERATOR_YVV_REFLECT = 3
 FJ_GRAIN_ACTIVE = 1
+FJ_GRAIN_SUBLAYERS = 2
+FJ_GRAIN_FULL_FRAME = 4
+FJ_GRAIN_AXIS_FINITE_C = 8
+FJ_GRAIN_DEBUG_OFF = 0
+FJ_GRAIN_DEBUG_MEAN_DENSITY = 6
 
 
 def _s(name, fields):

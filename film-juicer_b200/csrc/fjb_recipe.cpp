@@ -18,6 +18,7 @@
 // nodes as float4 vectors.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -67,7 +68,7 @@ void set_curve_guess(const std::vector<float>& blob, CurveRef& c) {
 void Recipe::release() noexcept {
     void* ptrs[] = {curves, tc_lut, mallett_basis, mallett_illum, film_sens_bgr, gamut_cmax, flags,
                     lut.nodes, lut.log2_xyz, lut.slope_c, lut.slope_m, lut.slope_y, lut.cell_min, lut.cell_max,
-                    lut.packed_nodes, lut.packed_cells, lut.failure, lut_spectra, meter_scratch};
+                    lut.packed_nodes, lut.packed_cells, lut.failure, lut_spectra, meter_scratch, layer_curves};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     curves = nullptr;
@@ -76,6 +77,9 @@ void Recipe::release() noexcept {
     flags = nullptr;
     lut = ScannerLutDevice{};
     lut_spectra = nullptr;
+    meter_scratch = nullptr;
+    layer_curves = nullptr;
+    layer_n = 0;
 }
 
 cudaError_t alloc_scanner_lut(int r, ScannerLutDevice& lut) {
@@ -159,6 +163,7 @@ bool create_recipe(const FjPreparedHostData& h, cudaStream_t stream, Recipe& r, 
     const bool print = h.route == FJ_ROUTE_NEGATIVE_PRINT || h.route == FJ_ROUTE_POSITIVE_PRINT;
     p.route = print ? kRoutePrint : kRouteDirect;
     r.print = print;
+    r.positive_film = h.capture_polarity == FJ_POLARITY_POSITIVE;
 
     // ---- exposure ----
     const FjFilmExposure& ex = h.film_exposure;
@@ -236,6 +241,21 @@ bool create_recipe(const FjPreparedHostData& h, cudaStream_t stream, Recipe& r, 
             for (size_t i = 0; i < n; ++i) blob.push_back(dv.density_rgb.data[i * 3 + rgb]);
             p.film_curve[bgr] = CurveRef{xoff, yoff[bgr], (int)n};
             p.gamma_bgr[bgr] = dv.gamma_rgb[rgb];
+        }
+        // Sublayer density curves [layer][CMY] for the grain's layer model, kept
+        // when all nine are present with the development's sample count.
+        bool layers = true;
+        for (int l = 0; l < 3; ++l)
+            for (int c = 0; c < 3; ++c) layers = layers && dv.density_layers[l][c].data && dv.density_layers[l][c].count == n;
+        if (layers) {
+            std::vector<float> lc(9 * n);
+            for (int l = 0; l < 3; ++l)
+                for (int c = 0; c < 3; ++c)
+                    std::copy(dv.density_layers[l][c].data, dv.density_layers[l][c].data + n, lc.begin() + (l * 3 + c) * n);
+            if ((e = upload(&r.layer_curves, lc.data(), lc.size() * 4, stream)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(stream)) != cudaSuccess)
+                goto cuda_fail;
+            r.layer_n = (int)n;
         }
         const FjDirCouplers& dir = h.dir_couplers;
         if (dir.mode > FJ_DIR_POSITIVE_RECEIVER_LANGMUIR) {

@@ -40,6 +40,9 @@ struct Recipe {
     unsigned* flags = nullptr;
     double* lut_spectra = nullptr;
     void* meter_scratch = nullptr; // auto-exposure partial sums + ticket
+    float* layer_curves = nullptr; // [layer][CMY] x layer_n sublayer density curves (grain), or null
+    int layer_n = 0;
+    bool positive_film = false;
     ScannerLutDevice lut{};
     void release() noexcept;
 };

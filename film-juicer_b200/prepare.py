@@ -68,6 +68,8 @@ def load_profile(path: str) -> dict:
     for key in ("log_sensitivity", "channel_density", "base_density", "midscale_neutral_density",
                 "log_exposure", "density_curves"):
         out[key] = _nan_array(data[key])
+    if "density_curves_layers" in data:
+        out["density_curves_layers"] = _nan_array(data["density_curves_layers"])
     return out
 
 
@@ -202,6 +204,9 @@ def prepare_recipe(resources: str, film: str, paper: str | None = None, *, dir_a
     a["tc_lut"] = f32(tc)
     a["log_exposure"] = f32(log_e)
     a["density_rgb"] = f32(curves)
+    if "density_curves_layers" in prof:
+        # sublayer curves [sample][layer][channel] as authored (the grain's layer model)
+        a["density_layers"] = f32(prof["density_curves_layers"])
     s["route_correction_scale"] = route_scale
     s["manual_exposure_ev"] = exposure_ev
     s["input_rgb_to_xyz"] = SRGB_TO_XYZ.ravel().tolist()
@@ -341,6 +346,10 @@ class HostRecord:
         dv = h.film_development
         dv.log_exposure = span(a["log_exposure"])
         dv.density_rgb = span(a["density_rgb"])
+        if "density_layers" in a:
+            for layer in range(3):
+                for ch in range(3):
+                    dv.density_layers[layer][ch] = span(a["density_layers"][:, layer, ch])
         abi.set_floats(dv.gamma_rgb, [1.0, 1.0, 1.0])
         dv.density_curves_hash = dv.hash = 1
 

@@ -254,3 +254,43 @@ def diffusion(components, radius: int, fraction: float, src_rgb, dst_rgb, stream
                            *[C.c_void_p(_ptr(t)) for t in dst_rgb], src_rgb[0].stride(0), w, h,
                            C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
     _check("fjb_diffusion", st, err)
+
+
+class DeviceNoise:
+    """Device copy of the static grain noise (fjb_noise_create / fjb_noise_destroy)."""
+
+    def __init__(self, noise_record, stream=None):
+        self.lib = load_library()
+        self.handle = C.c_void_p()
+        err = abi.ErrorText()
+        _check("fjb_noise_create", self.lib.fjb_noise_create(C.byref(noise_record), C.c_void_p(_stream_handle(stream)),
+                                                             C.byref(self.handle), C.byref(err.buf)), err)
+
+    def close(self):
+        if self.handle:
+            err = abi.ErrorText()
+            self.lib.fjb_noise_destroy(self.handle, C.byref(err.buf))
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def visual_grain(recipe: "DeviceRecipe", grain, density_cmy, noise: "DeviceNoise | None" = None, scratch=None,
+                 stream=None):
+    """Grain on three CUDA density planes (C, M, Y) in place."""
+    torch = _torch()
+    lib = load_library()
+    h, w = density_cmy[0].shape
+    need = int(lib.fjb_visual_grain_scratch_bytes(w, h))
+    if scratch is None:
+        scratch = torch.empty((need + 3) // 4, dtype=torch.float32, device=density_cmy[0].device)
+    err = abi.ErrorText()
+    st = lib.fjb_visual_grain(recipe.handle, C.byref(grain), noise.handle if noise is not None else None,
+                              *[C.c_void_p(_ptr(t)) for t in density_cmy], density_cmy[0].stride(0), w, h,
+                              C.c_void_p(_ptr(scratch)), scratch.numel() * 4, C.c_void_p(_stream_handle(stream)),
+                              C.byref(err.buf))
+    _check("fjb_visual_grain", st, err)

@@ -172,6 +172,29 @@ FjStatus fjb_diffusion_no_alloc(const FjDiffusionComponents* components, int32_t
                                 float* dst_g, float* dst_b, ptrdiff_t stride, int32_t width, int32_t height,
                                 void* stream, FjErrorBuffer* error);
 
+/* Device copy of the static grain noise (blue-noise volume, Wang tiles and their
+ * colour table), uploaded once and shared by every frame (the reference keeps the
+ * same bytes resident, src/Cuda/JuicerCudaFilmPayloads.cpp:400-422). Synchronises
+ * `stream`. */
+typedef struct FjbNoise FjbNoise;
+FjStatus fjb_noise_create(const FjStaticNoise* noise, void* stream, FjbNoise** out_noise, FjErrorBuffer* error);
+FjStatus fjb_noise_destroy(FjbNoise* noise, FjErrorBuffer* error);
+
+/* Bytes of device scratch fjb_visual_grain needs for a width x height frame. */
+size_t fjb_visual_grain_scratch_bytes(int32_t width, int32_t height);
+
+/* Density-space visual grain on the capture density planes C, M, Y in place
+ * (reference src/Cuda/Scan/JuicerCudaScanPipeline.cu:3141 juicer_cuda_apply_visual_grain):
+ * per channel up to three particle-size scales of Poisson particle samples (one layer
+ * or three sublayers with dye-cloud blurs), correlation blurs, size-mix gain, shared
+ * chroma mix, debug views. `noise` NULL draws from the Philox counter stream instead of
+ * the blue noise. Sublayers read the recipe's density-layer curves. `scratch` is
+ * caller-owned, 16-byte aligned, at least fjb_visual_grain_scratch_bytes bytes; calls
+ * sharing a scratch buffer must not overlap. Does not synchronise. */
+FjStatus fjb_visual_grain(FjbRecipe* recipe, const FjVisualGrain* grain, const FjbNoise* noise, float* density_c,
+                          float* density_m, float* density_y, ptrdiff_t stride, int32_t width, int32_t height,
+                          float* scratch, size_t scratch_bytes, void* stream, FjErrorBuffer* error);
+
 /* Scanner LUT input record (reference native/juicer_cuda_frame_values.h FjScannerLutInput). */
 typedef struct FjbScannerLutInput {
     FjFloatSpan eps_c, eps_m, eps_y;

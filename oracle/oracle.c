@@ -1374,3 +1374,783 @@ int oracle_diffusion(const double* lambda_px, const double* weights /* [3][9] R,
     free(psf);
     return 0;
 }
+
+/* ------------------------------------------------------------------------------ *
+ * Visual grain (a15). Restates src/Cuda/Film/JuicerCudaFilmPipeline.cu:1580-2986  *
+ * (random draws, particle model, Wang offsets, value noise, breathing, clump,     *
+ * frame uniforms, layer lookup, sample kernels) and the schedule of               *
+ * src/Cuda/Scan/JuicerCudaScanPipeline.cu:3141-3740 with its blurs (:317-380,     *
+ * :454-578). The reference's compiler contracts a + b * c into one fused          *
+ * multiply-add; those places use fmaf() here. expf/logf/cosf/sinf/sqrtf/rsqrtf    *
+ * come from libm (rsqrtf as 1/sqrtf), so the oracle agrees with a GPU to the      *
+ * last bits of those functions: the random streams themselves (blue-noise         *
+ * lookups, Philox words, hashes) are exact.                                        *
+ * ------------------------------------------------------------------------------ */
+
+typedef struct {
+    int breathing_active;
+    float breathing_t;
+    uint64_t seed_a, seed_b;
+    float cell_small, cell_large, drift_x, drift_y, roll_y, mix;
+    int clump_active;
+    float clump_cell, clump_roll;
+    uint64_t clump_seed;
+    float clump_rms, clump_mu, clump_sigma;
+} OGrainUniforms;
+
+typedef struct {
+    const FjVisualGrain* g;
+    const uint8_t* stbn;
+    int stbn_w, stbn_h, stbn_frames, stbn_off_x, stbn_off_y, stbn_frame;
+    const uint8_t* wang;
+    const uint8_t* wang_lut;
+    int wang_w, wang_h, wang_count, wang_colors;
+    const float* base[3];
+    const float* layer[3][3];
+    int n;
+    int positive;
+    /* per-scale overrides */
+    uint64_t seed, seed_next;
+    float n_particles[3], od_particle[3], n_layers[3][3], od_layers[3][3];
+    OGrainUniforms u;
+} OGrain;
+
+static inline uint64_t og_splitmix(uint64_t v) {
+    v += 0x9E3779B97F4A7C15ULL;
+    v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    v = (v ^ (v >> 27)) * 0x94D049BB133111EBULL;
+    return v ^ (v >> 31);
+}
+static inline int og_wrap(int64_t c, int size) {
+    if (size <= 0) return 0;
+    if ((size & (size - 1)) == 0) return (int)((uint64_t)c & (uint64_t)(size - 1));
+    c %= (int64_t)size;
+    if (c < 0) c += size;
+    return (int)c;
+}
+static inline float og_clamp(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
+static inline float og_san(float v) { return isfinite(v) ? v : 0.0f; }
+static inline float og_smooth(float t) { return (t * t) * fmaf(-2.0f, t, 3.0f); }
+static inline float og_hash01(int x, int y, uint64_t seed) {
+    uint64_t h = og_splitmix(seed ^ ((uint64_t)(int64_t)x * 0x9E3779B97F4A7C15ULL) ^
+                             ((uint64_t)(int64_t)y * 0xBF58476D1CE4E5B9ULL));
+    return (float)(uint32_t)(h & 0xFFFFFFFFu) * (1.0f / 4294967296.0f);
+}
+static inline float og_spatial(int x, int y, uint64_t seed) {
+    uint32_t lo = (uint32_t)seed, hi = (uint32_t)(seed >> 32);
+    uint32_t h = lo ^ ((hi << 16) | (hi >> 16));
+    h ^= (uint32_t)x * 0x9E3779B9u;
+    h ^= (uint32_t)y * 0x85EBCA6Bu;
+    h ^= h >> 16;
+    h *= 0x7FEB352Du;
+    h ^= h >> 15;
+    h *= 0x846CA68Bu;
+    h ^= h >> 16;
+    return (float)h * (1.0f / 4294967296.0f);
+}
+static inline float og_noise(float cx, float cy, uint64_t seed) {
+    int ix = (int)floorf(cx), iy = (int)floorf(cy);
+    float sx = og_smooth(cx - (float)ix), sy = og_smooth(cy - (float)iy);
+    float v00 = og_spatial(ix, iy, seed), v10 = og_spatial(ix + 1, iy, seed);
+    float v01 = og_spatial(ix, iy + 1, seed), v11 = og_spatial(ix + 1, iy + 1, seed);
+    float v0 = fmaf(v10 - v00, sx, v00), v1 = fmaf(v11 - v01, sx, v01);
+    return fmaf(v1 - v0, sy, v0);
+}
+
+/* Philox4x32-10, openrand arrangement (third_party/openrand/philox.h:60-150). */
+typedef struct {
+    uint32_t k0, k1, c0, c1, c2, n;
+} OPhilox;
+static uint32_t og_philox(OPhilox* p) {
+    uint32_t x0 = p->c0, x1 = p->c1, x2 = p->c2, x3 = p->n, a = p->k0, b = p->k1;
+    for (int r = 0; r < 10; ++r) {
+        if (r > 0) {
+            a += 0x9E3779B9u;
+            b += 0xBB67AE85u;
+        }
+        uint64_t p0 = (uint64_t)0xD2511F53u * x0, p1 = (uint64_t)0xCD9E8D57u * x2;
+        uint32_t y0 = (uint32_t)(p1 >> 32) ^ x1 ^ a, y2 = (uint32_t)(p0 >> 32) ^ x3 ^ b;
+        x0 = y0;
+        x1 = (uint32_t)p1;
+        x2 = y2;
+        x3 = (uint32_t)p0;
+    }
+    p->n++;
+    return x0;
+}
+
+typedef struct {
+    OPhilox ph;
+    const OGrain* o;
+    uint64_t ax, ay, seed;
+    uint32_t draw;
+    int stbn, wx, wy, mask_w, mask_h;
+    int64_t pitch;
+    size_t row_base;
+} ORng;
+
+static void og_rng_init(ORng* r, const OGrain* o, uint64_t seed, uint64_t ax, uint64_t ay, int stbn, int frame_off,
+                        int wx, int wy) {
+    memset(r, 0, sizeof(*r));
+    r->ph.k0 = (uint32_t)(seed >> 32);
+    r->ph.k1 = (uint32_t)seed;
+    r->ph.c0 = (uint32_t)ax;
+    r->ph.c1 = (uint32_t)ay;
+    r->ph.c2 = 0xAAAAAAAAu;
+    r->o = o;
+    r->ax = ax;
+    r->ay = ay;
+    r->seed = seed;
+    r->stbn = stbn;
+    r->wx = wx;
+    r->wy = wy;
+    r->mask_w = r->mask_h = -1;
+    if (!stbn) return;
+    if ((o->stbn_w & (o->stbn_w - 1)) == 0 && (o->stbn_h & (o->stbn_h - 1)) == 0) {
+        r->mask_w = o->stbn_w - 1;
+        r->mask_h = o->stbn_h - 1;
+    }
+    if (o->g->pitch_px > 0) r->pitch = (int64_t)o->g->pitch_px * (o->g->frame0 + (int64_t)frame_off);
+    r->row_base = (size_t)og_wrap((int64_t)o->stbn_frame + frame_off, o->stbn_frames) * (size_t)o->stbn_h;
+}
+
+static float og_uniform(ORng* r) {
+    if (r->stbn) {
+        uint32_t d = r->draw++;
+        uint64_t h = og_splitmix(r->seed + (uint64_t)d * 0x9E3779B97F4A7C15ULL);
+        int ox = (int)(h & 0xFFFFu) + r->wx, oy = (int)((h >> 16) & 0xFFFFu) + r->wy;
+        int64_t xc = (int64_t)r->ax + ox + r->o->stbn_off_x;
+        int64_t yc = (int64_t)r->ay + oy + r->o->stbn_off_y + r->pitch;
+        int x, y;
+        if (r->mask_w >= 0) {
+            x = (int)((uint64_t)xc & (uint64_t)r->mask_w);
+            y = (int)((uint64_t)yc & (uint64_t)r->mask_h);
+        } else {
+            x = og_wrap(xc, r->o->stbn_w);
+            y = og_wrap(yc, r->o->stbn_h);
+        }
+        uint8_t v = r->o->stbn[(r->row_base + (size_t)y) * (size_t)r->o->stbn_w + (size_t)x];
+        return ((float)v + 0.5f) * (1.0f / 256.0f);
+    }
+    return fmaf((float)og_philox(&r->ph), 1.0f / 4294967296.0f, 0.5f / 4294967296.0f);
+}
+
+static float og_normal(ORng* r) {
+    float u1 = og_clamp(og_uniform(r), 1e-7f, 1.0f);
+    float u2 = og_uniform(r);
+    return sqrtf(-2.0f * logf(u1)) * cosf(6.28318530717958647692f * u2);
+}
+
+static int og_poisson(float lambda, ORng* r) {
+    if (!isfinite(lambda) || !(lambda > 0.0f)) return 0;
+    if (lambda < 10.0f) {
+        float L = expf(-lambda), p = 1.0f;
+        int k = 0;
+        while (p > L && k < 1024) {
+            ++k;
+            p *= og_clamp(og_uniform(r), 1e-7f, 1.0f);
+        }
+        return k - 1;
+    }
+    float z = og_normal(r);
+    float s = fmaf(sqrtf(lambda), z, lambda);
+    if (!isfinite(s)) s = 0.0f;
+    int k = (int)floorf(s + 0.5f);
+    return k < 0 ? 0 : k;
+}
+
+static float og_particle(const OGrain* o, float density, float dmax, float np, float od, float unif, uint64_t seed,
+                         int frame_off, uint64_t ax, uint64_t ay, int stbn, int wx, int wy) {
+    if (!isfinite(density) || density < 0.0f) density = 0.0f;
+    float p = og_clamp(density / dmax, 1e-6f, 1.0f - 1e-6f);
+    float u = isfinite(unif) ? og_clamp(unif, 0.0f, 1.0f) : 0.0f;
+    float sat = fmaf(-(p * u), 1.0f - 1e-6f, 1.0f);
+    if (!isfinite(sat) || sat <= 0.0f) sat = 1e-6f;
+    ORng r;
+    og_rng_init(&r, o, seed, ax, ay, stbn, frame_off, wx, wy);
+    float lambda = np / sat;
+    int count = og_poisson(lambda * p, &r);
+    return og_san((float)count * od * sat);
+}
+
+static void og_wang(const OGrain* o, uint64_t ax, uint64_t ay, int* ox, int* oy) {
+    const FjVisualGrain* g = o->g;
+    *ox = *oy = 0;
+    if (!o->wang || !o->wang_lut || o->wang_w <= 0 || o->wang_h <= 0 || o->wang_count <= 0) return;
+    if (!(g->pixel_size_um > 0.0f) || !(g->wang_cell_mm > 0.0f) || o->wang_colors <= 0) return;
+    float xmm = (float)ax * (g->pixel_size_um * 0.001f), ymm = (float)ay * (g->pixel_size_um * 0.001f);
+    float inv = 1.0f / g->wang_cell_mm;
+    float cx = xmm * inv, cy = ymm * inv;
+    float fx = cx - floorf(cx), fy = cy - floorf(cy);
+    int64_t mx = (int64_t)floorf(cx), my = (int64_t)floorf(cy);
+    uint64_t s0 = g->clip_token != 0 ? g->clip_token : g->session_seed;
+    uint64_t base = s0 != 0 ? s0 : 1ULL;
+#define OG_HU32(X, Y, SALT)                                                                                        \
+    ((uint32_t)(og_splitmix(base ^ (SALT) ^ ((uint64_t)(int64_t)(X) * 0x9E3779B97F4A7C15ULL) ^                    \
+                            ((uint64_t)(int64_t)(Y) * 0xBF58476D1CE4E5B9ULL)) &                                    \
+                0xFFFFFFFFu))
+    uint32_t colors = (uint32_t)o->wang_colors;
+    uint32_t l = OG_HU32((int)mx, (int)my, 0xA5A5A5A5ULL) % colors;
+    uint32_t rr = OG_HU32((int)(mx + 1), (int)my, 0x5A5A5A5AULL) % colors;
+    uint32_t t = OG_HU32((int)mx, (int)my, 0xC3C3C3C3ULL) % colors;
+    uint32_t b = OG_HU32((int)mx, (int)(my + 1), 0x3C3C3C3CULL) % colors;
+#undef OG_HU32
+    size_t c = colors;
+    int tile = (int)o->wang_lut[(((size_t)l * c + rr) * c + t) * c + b];
+    int w = o->wang_w, h = o->wang_h;
+    int tx = (int)floorf(fx * (float)w), ty = (int)floorf(fy * (float)h);
+    if (tx >= w) tx = w - 1;
+    if (ty >= h) ty = h - 1;
+    float v[2];
+    int xs[2] = {tx, (tx + (w >> 1)) % w}, ys[2] = {ty, (ty + (h >> 1)) % h};
+    for (int i = 0; i < 2; ++i) {
+        if (tile < 0 || tile >= o->wang_count) {
+            v[i] = 0.0f;
+            continue;
+        }
+        int x = xs[i] < 0 ? 0 : (xs[i] >= w ? w - 1 : xs[i]);
+        int y = ys[i] < 0 ? 0 : (ys[i] >= h ? h - 1 : ys[i]);
+        v[i] = ((float)o->wang[((size_t)tile * h + y) * w + x] + 0.5f) * (1.0f / 256.0f);
+    }
+    int warp_x = o->stbn_w > 0 ? ((o->stbn_w / 8) > 4 ? o->stbn_w / 8 : 4) : 0;
+    int warp_y = o->stbn_h > 0 ? ((o->stbn_h / 8) > 4 ? o->stbn_h / 8 : 4) : 0;
+    if (warp_x == 0 || warp_y == 0) return;
+    *ox = (int)floorf((v[0] - 0.5f) * 2.0f * (float)warp_x);
+    *oy = (int)floorf((v[1] - 0.5f) * 2.0f * (float)warp_y);
+}
+
+static float og_breathing(const OGrain* o, uint64_t ax, uint64_t ay) {
+    const OGrainUniforms* u = &o->u;
+    if (!u->breathing_active) return 1.0f;
+    float bx = (float)ax + u->drift_x, by = (float)ay + u->drift_y + u->roll_y;
+    float xs = bx / u->cell_small, ys = by / u->cell_small, xl = bx / u->cell_large, yl = by / u->cell_large;
+    float sa = og_noise(xs, ys, u->seed_a ^ 0x9E3779B97F4A7C15ULL), sb = og_noise(xs, ys, u->seed_b ^ 0x9E3779B97F4A7C15ULL);
+    float la = og_noise(xl, yl, u->seed_a ^ 0xBF58476D1CE4E5B9ULL), lb = og_noise(xl, yl, u->seed_b ^ 0xBF58476D1CE4E5B9ULL);
+    float ns = fmaf(sb - sa, u->breathing_t, sa), nl = fmaf(lb - la, u->breathing_t, la);
+    float noise = fmaf(u->mix, ns, (1.0f - u->mix) * nl);
+    float f = fmaf(o->g->breathing_amplitude, fmaf(noise, 2.0f, -1.0f), 1.0f);
+    return f > 0.0f ? f : 0.0f;
+}
+
+static float og_clump(const OGrain* o, uint64_t ax, uint64_t ay) {
+    const OGrainUniforms* u = &o->u;
+    if (!u->clump_active) return 1.0f;
+    float xs = (float)ax / u->clump_cell, ys = ((float)ay + u->clump_roll) / u->clump_cell;
+    float a = og_noise(xs, ys, u->clump_seed ^ 0x9E3779B97F4A7C15ULL);
+    float b = og_noise(xs + 19.19f, ys + 7.23f, u->clump_seed ^ 0xBF58476D1CE4E5B9ULL);
+    float u1 = og_clamp(a, 1e-6f, 1.0f - 1e-6f), u2 = og_clamp(b, 0.0f, 1.0f);
+    float n = sqrtf(-2.0f * logf(u1)) * cosf(6.28318530717958647692f * u2);
+    float v = expf(fmaf(u->clump_sigma, n, u->clump_mu));
+    if (!isfinite(v)) v = 1.0f;
+    return v * u->clump_rms;
+}
+
+static void og_lognormal(float mean, float sd, float* mu, float* sigma) {
+    float m2 = mean * mean, s2 = sd * sd;
+    float sq = logf(1.0f + s2 / m2);
+    *sigma = sqrtf(fmaxf(0.0f, sq));
+    *mu = fmaf(-0.5f, sq, logf(fmaxf(1e-12f, mean)));
+}
+
+static void og_uniforms(OGrain* o) {
+    const FjVisualGrain* g = o->g;
+    OGrainUniforms u;
+    memset(&u, 0, sizeof(u));
+    float time = (float)g->frame0 + g->frame_alpha;
+    if (g->breathing_amplitude > 0.0f && g->breathing_period_frames > 0 && g->pixel_size_um > 0.0f &&
+        g->breathing_cell_um_small > 0.0f && g->breathing_cell_um_large > 0.0f) {
+        float period = (float)g->breathing_period_frames;
+        float step_f = floorf(time / period);
+        int64_t step = (int64_t)step_f;
+        float frac = fmaf(-step_f, period, time) / period;
+        u.breathing_t = og_smooth(og_clamp(frac, 0.0f, 1.0f));
+        uint64_t seed = g->session_seed != 0 ? g->session_seed : 1ULL;
+        u.seed_a = og_splitmix(seed ^ ((uint64_t)step * 0x8EBC6AF09C88C6E3ULL));
+        u.seed_b = og_splitmix(seed ^ ((uint64_t)(step + 1) * 0x8EBC6AF09C88C6E3ULL));
+        float inv = 1.0f / g->pixel_size_um;
+        u.cell_small = fmaxf(4.0f, g->breathing_cell_um_small * inv);
+        u.cell_large = fmaxf(4.0f, g->breathing_cell_um_large * inv);
+        float drift = g->breathing_drift_um_per_frame > 0.0f ? g->breathing_drift_um_per_frame * inv : 0.0f;
+        float dx = 0.0f, dy = 0.0f;
+        if (drift > 0.0f) {
+            uint64_t h = og_splitmix(seed ^ 0x6A09E667F3BCC909ULL);
+            float angle = (float)(uint32_t)(h & 0xFFFFFFFFu) * (1.0f / 4294967296.0f) * 6.28318530717958647692f;
+            dx = cosf(angle) * drift;
+            dy = sinf(angle) * drift;
+        }
+        float roll = g->pitch_px > 0 ? (float)g->pitch_px : 0.0f;
+        u.drift_x = dx * time;
+        u.drift_y = dy * time;
+        u.roll_y = roll * time;
+        u.mix = og_clamp(g->breathing_mix, 0.0f, 1.0f);
+        u.breathing_active = 1;
+    }
+    float sds = g->micro_structure[1] * 0.001f;
+    if (sds > 0.0f && g->pixel_size_um > 0.0f) {
+        float cell = g->micro_structure[0];
+        if (!(cell > 0.0f)) cell = 0.0f;
+        float inv = 1.0f / g->pixel_size_um;
+        u.clump_cell = cell * inv;
+        if (!(u.clump_cell > 4.0f)) u.clump_cell = 4.0f;
+        float roll = g->pitch_px > 0 ? (float)g->pitch_px : 0.0f;
+        u.clump_roll = roll * time;
+        u.clump_seed = g->clip_token != 0 ? g->clip_token : g->session_seed;
+        if (u.clump_seed == 0) u.clump_seed = 1ULL;
+        float sd = sds;
+        u.clump_rms = 1.0f;
+        float mix = og_clamp(g->clump_temporal_mix, 0.0f, 1.0f);
+        if (mix > 0.0f) {
+            int per = g->clump_morph_period_frames;
+            if (per <= 0) per = 1;
+            float period = (float)per;
+            float step_f = floorf(time / period);
+            int64_t step = (int64_t)step_f;
+            float frac = fmaf(-step_f, period, time) / period;
+            float t = og_smooth(og_clamp(frac, 0.0f, 1.0f));
+            uint64_t ts = g->session_seed != 0 ? g->session_seed : 1ULL;
+            uint64_t sa = og_splitmix(ts ^ ((uint64_t)step * 0xD2B74407B1CE6E93ULL));
+            uint64_t sb = og_splitmix(ts ^ ((uint64_t)(step + 1) * 0xD2B74407B1CE6E93ULL));
+            float u1a = og_hash01(0, 0, sa ^ 0x9E3779B97F4A7C15ULL), u2a = og_hash01(1, 0, sa ^ 0xBF58476D1CE4E5B9ULL);
+            float u1b = og_hash01(0, 0, sb ^ 0x9E3779B97F4A7C15ULL), u2b = og_hash01(1, 0, sb ^ 0xBF58476D1CE4E5B9ULL);
+            float u1 = og_clamp(fmaf(u1b - u1a, t, u1a), 1e-6f, 1.0f - 1e-6f);
+            float u2 = og_clamp(fmaf(u2b - u2a, t, u2a), 0.0f, 1.0f);
+            float nt = sqrtf(-2.0f * logf(u1)) * cosf(6.28318530717958647692f * u2);
+            float ssd = mix * 0.23597824f, mu, sigma;
+            og_lognormal(1.0f, ssd, &mu, &sigma);
+            float strength = expf(fmaf(sigma, nt, mu));
+            strength *= 1.0f / sqrtf(fmaf(ssd, ssd, 1.0f));
+            sd = sds * strength;
+            float den = fmaf(sd, sd, 1.0f), num = fmaf(sds, sds, 1.0f);
+            u.clump_rms = den > 0.0f ? sqrtf(num / den) : 1.0f;
+        }
+        og_lognormal(1.0f, sd, &u.clump_mu, &u.clump_sigma);
+        u.clump_active = 1;
+    }
+    o->u = u;
+}
+
+static float og_layer_density(const OGrain* o, int ch, int layer, float density) {
+    const float* x = o->base[ch];
+    const float* y = o->layer[layer][ch];
+    int n = o->n;
+    if (!x || !y || n <= 0) return density;
+    if (!isfinite(density)) return y[0];
+    int pos = o->positive;
+    float q = pos ? -density : density;
+#define OG_AX(i) (pos ? -x[(i)] : x[(i)])
+    int bounded = (o->g->flags & (FJ_GRAIN_AXIS_FINITE_C << ch)) != 0 && n == 256;
+    int b0 = 0, b1 = n - 1;
+    if (!bounded) {
+        while (b0 < n && !isfinite(OG_AX(b0))) ++b0;
+        if (b0 >= n) return density;
+        while (b1 > b0 && !isfinite(OG_AX(b1))) --b1;
+    }
+    float xmin = OG_AX(b0), xmax = OG_AX(b1);
+    if (!isfinite(xmin) || !isfinite(xmax) || !(xmax >= xmin)) return y[b0];
+    if (q <= xmin) return y[b0];
+    if (q >= xmax) return y[b1];
+    int i1 = b0 + 1;
+    if (bounded) {
+        const float* prefix = o->g->layer_axis_block_prefix_max[ch];
+        int lo = 0, hi = 15;
+        for (int s = 0; s < 4; ++s) {
+            int mid = lo + (hi - lo) / 2;
+            if (prefix[mid] < q)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        i1 = lo * 16 > 1 ? lo * 16 : 1;
+        int end = (lo + 1) * 16 - 1 < b1 ? (lo + 1) * 16 - 1 : b1;
+        while (i1 <= end && OG_AX(i1) < q) ++i1;
+    } else {
+        while (i1 <= b1 && OG_AX(i1) < q) ++i1;
+    }
+    if (i1 > b1) return y[b1];
+    int i0 = i1 - 1;
+    float x0 = OG_AX(i0), x1 = OG_AX(i1), den = x1 - x0;
+#undef OG_AX
+    if (!(den > 0.0f) || !isfinite(den)) return y[i0];
+    return fmaf((q - x0) / den, y[i1] - y[i0], y[i0]);
+}
+
+static float og_modulate(float g, float density, float br, float cl) { return fmaf((g - density) * br, cl, density); }
+
+static float og_retime(float g, float gn, float density, float alpha) {
+    float d0 = g - density, d1 = gn - density;
+    float blend = fmaf(d1 - d0, alpha, d0);
+    float w0 = 1.0f - alpha;
+    float den = fmaf(w0, w0, alpha * alpha) + 1e-6f;
+    return fmaf(blend, 1.0f / sqrtf(den), density);
+}
+
+/* mode 0 simple, 1 layer, 2 triplet: the sanitised sample of one pixel. */
+static float og_sample(const OGrain* o, int mode, int ch, int layer, float in_density, uint64_t ax, uint64_t ay) {
+    const FjVisualGrain* g = o->g;
+    int stbn = (o->stbn && o->stbn_w > 0 && o->stbn_h > 0 && o->stbn_frames > 0) ? 1 : 0;
+    float alpha = g->frame_alpha;
+    int retime = alpha > 1e-6f && alpha < 0.999999f;
+    int wx = 0, wy = 0;
+    float cl = og_clump(o, ax, ay);
+    if (stbn) og_wang(o, ax, ay, &wx, &wy);
+    float br = og_breathing(o, ax, ay);
+    if (mode == 0) {
+        float density = in_density + g->particle_density_min_cmy[ch];
+        int nsub = g->sublayer_count > 0 ? (int)g->sublayer_count : 1;
+        float acc = 0.0f, accn = 0.0f;
+        for (int sl = 0; sl < nsub; ++sl) {
+            uint64_t salt = (uint64_t)ch + (uint64_t)sl * 10ULL;
+            acc += og_particle(o, density, g->density_max_cmy[ch], o->n_particles[ch], o->od_particle[ch],
+                               g->uniformity_cmy[ch], o->seed ^ salt, 0, ax, ay, stbn, wx, wy);
+            if (retime)
+                accn += og_particle(o, density, g->density_max_cmy[ch], o->n_particles[ch], o->od_particle[ch],
+                                    g->uniformity_cmy[ch], o->seed_next ^ salt, 1, ax, ay, stbn, wx, wy);
+        }
+        acc /= (float)nsub;
+        if (retime) accn /= (float)nsub;
+        acc = og_modulate(acc, density, br, cl);
+        if (retime) acc = og_retime(acc, og_modulate(accn, density, br, cl), density, alpha);
+        return og_san(acc);
+    }
+    float sum = 0.0f;
+    for (int l = (mode == 1 ? layer : 0); l < (mode == 1 ? layer + 1 : 3); ++l) {
+        float density = og_layer_density(o, ch, l, in_density) + g->density_min_layers[l][ch];
+        uint64_t salt = (uint64_t)ch + (uint64_t)l * 10ULL;
+        float v = og_particle(o, density, g->density_max_layers[l][ch], o->n_layers[l][ch], o->od_layers[l][ch],
+                              g->uniformity_cmy[ch], o->seed ^ salt, 0, ax, ay, stbn, wx, wy);
+        v = og_modulate(v, density, br, cl);
+        if (retime) {
+            float vn = og_particle(o, density, g->density_max_layers[l][ch], o->n_layers[l][ch], o->od_layers[l][ch],
+                                   g->uniformity_cmy[ch], o->seed_next ^ salt, 1, ax, ay, stbn, wx, wy);
+            v = og_retime(v, og_modulate(vn, density, br, cl), density, alpha);
+        }
+        if (mode == 1) return og_san(v);
+        sum += og_san(v);
+    }
+    return og_san(sum);
+}
+
+static int og_reflect_half(long i, int n) {
+    if (n <= 1) return 0;
+    long p = 2L * n, m = i % p;
+    if (m < 0) m += p;
+    return (int)(m < n ? m : p - 1 - m);
+}
+
+/* Normalised Gaussian taps (rust/film-juicer-core/src/optics/gaussian.rs:16-52). */
+static void og_taps(int radius, float sigma, float* w) {
+    double s = (double)sigma, s2 = s * s * 2.0, sum = 0.0;
+    for (int i = -radius; i <= radius; ++i) {
+        double v = exp(-((double)i * (double)i) / s2);
+        w[i + radius] = (float)v;
+        sum += v;
+    }
+    double rec = sum != 0.0 ? 1.0 / sum : 0.0;
+    for (int i = 0; i <= 2 * radius; ++i) w[i] = (float)((double)w[i] * rec);
+}
+
+static void og_blur_rows(const float* in, float* out, const float* w, int r, int W, int H) {
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            float acc = 0.0f;
+            for (int k = 0; k <= 2 * r; ++k) acc = fmaf(in[(size_t)y * W + og_reflect_half((long)x - r + k, W)], w[k], acc);
+            out[(size_t)y * W + x] = og_san(acc);
+        }
+}
+
+static float og_blur_col(const float* in, const float* w, int r, int W, int H, int x, int y) {
+    float acc = 0.0f;
+    for (int k = 0; k <= 2 * r; ++k) acc = fmaf(in[(size_t)og_reflect_half((long)y - r + k, H) * W + x], w[k], acc);
+    return og_san(acc);
+}
+
+typedef struct {
+    float w[151];
+    int r;
+    uint64_t hash;
+} OTaps;
+
+typedef struct {
+    OGrain o;
+    OTaps corr[3], dye[3][3];
+    int W, H;
+    float *temp, *scale, *layer;
+} OSched;
+
+/* One scale of one channel, accumulated into `target` (generate_scale). */
+static int og_scale_pass(OSched* s, const float* dens, int ch, uint64_t salt, float factor, const OTaps* corr,
+                         int apply, float weight, int init, float* target) {
+    OGrain* o = &s->o;
+    const FjVisualGrain* g = o->g;
+    int W = s->W, H = s->H;
+    size_t N = (size_t)W * H;
+    o->seed = g->seed_base ^ salt;
+    o->seed_next = g->seed_base_next ^ salt;
+    for (int c = 0; c < 3; ++c) {
+        o->n_particles[c] = g->n_particles_cmy[c] / factor;
+        o->od_particle[c] = g->od_particle_cmy[c] * factor;
+        for (int l = 0; l < 3; ++l) {
+            o->n_layers[l][c] = g->n_particles_layers[l][c] / factor;
+            o->od_layers[l][c] = g->od_particle_layers[l][c] * factor;
+        }
+    }
+    float bias = -g->particle_density_min_cmy[ch];
+    int sub = (g->flags & FJ_GRAIN_SUBLAYERS) != 0;
+    int delta_formed = 0;
+#define OG_DELTA(v, i)                                                                                             \
+    do {                                                                                                            \
+        if (bias != 0.0f) (v) = og_san((v) + bias);                                                               \
+        (v) = og_san((v) - dens[(i)]);                                                                              \
+    } while (0)
+    if (sub) {
+        const OTaps *d0 = &s->dye[0][ch], *d1 = &s->dye[1][ch], *d2 = &s->dye[2][ch];
+        int zero = d0->r <= 0 && d1->r <= 0 && d2->r <= 0;
+        int same = d0->r == d1->r && d0->r == d2->r && (zero || (d0->hash == d1->hash && d0->hash == d2->hash));
+        if (same) {
+#pragma omp parallel for schedule(dynamic, 4)
+            for (int y = 0; y < H; ++y)
+                for (int x = 0; x < W; ++x) {
+                    size_t i = (size_t)y * W + x;
+                    float v = og_sample(o, 2, ch, 0, dens[i], (uint64_t)((int64_t)g->render_extent.x + x),
+                                        (uint64_t)((int64_t)g->render_extent.y + y));
+                    if (zero) {
+                        v = og_san(0.0f + v);
+                        OG_DELTA(v, i);
+                        s->scale[i] = v;
+                    } else {
+                        s->layer[i] = v;
+                    }
+                }
+            if (!zero) {
+                og_blur_rows(s->layer, s->temp, d0->w, d0->r, W, H);
+#pragma omp parallel for schedule(static)
+                for (int y = 0; y < H; ++y)
+                    for (int x = 0; x < W; ++x) {
+                        size_t i = (size_t)y * W + x;
+                        float v = og_san(0.0f + og_blur_col(s->temp, d0->w, d0->r, W, H, x, y));
+                        OG_DELTA(v, i);
+                        s->scale[i] = v;
+                    }
+            }
+            delta_formed = 1;
+        } else {
+            for (int l = 0; l < 3; ++l) {
+                const OTaps* d = &s->dye[l][ch];
+#pragma omp parallel for schedule(dynamic, 4)
+                for (int y = 0; y < H; ++y)
+                    for (int x = 0; x < W; ++x) {
+                        size_t i = (size_t)y * W + x;
+                        float v = og_sample(o, 1, ch, l, dens[i], (uint64_t)((int64_t)g->render_extent.x + x),
+                                            (uint64_t)((int64_t)g->render_extent.y + y));
+                        if (d->r > 0) {
+                            s->layer[i] = v;
+                        } else {
+                            v = og_san((l == 0 ? 0.0f : s->scale[i]) + v);
+                            if (l == 2) OG_DELTA(v, i);
+                            s->scale[i] = v;
+                        }
+                    }
+                if (d->r > 0) {
+                    og_blur_rows(s->layer, s->temp, d->w, d->r, W, H);
+#pragma omp parallel for schedule(static)
+                    for (int y = 0; y < H; ++y)
+                        for (int x = 0; x < W; ++x) {
+                            size_t i = (size_t)y * W + x;
+                            float v = og_san((l == 0 ? 0.0f : s->scale[i]) + og_blur_col(s->temp, d->w, d->r, W, H, x, y));
+                            if (l == 2) OG_DELTA(v, i);
+                            s->scale[i] = v;
+                        }
+                }
+            }
+            delta_formed = 1;
+        }
+    } else {
+#pragma omp parallel for schedule(dynamic, 4)
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x) {
+                size_t i = (size_t)y * W + x;
+                float v = og_sample(o, 0, ch, 0, dens[i], (uint64_t)((int64_t)g->render_extent.x + x),
+                                    (uint64_t)((int64_t)g->render_extent.y + y));
+                OG_DELTA(v, i);
+                s->scale[i] = v;
+            }
+        delta_formed = 1;
+    }
+#undef OG_DELTA
+    if (!delta_formed) return 1;
+    float wgt = isfinite(weight) ? weight : 0.0f;
+    if (apply && corr->r > 0) {
+        og_blur_rows(s->scale, s->temp, corr->w, corr->r, W, H);
+#pragma omp parallel for schedule(static)
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x) {
+                size_t i = (size_t)y * W + x;
+                target[i] = og_san(fmaf(wgt, og_blur_col(s->temp, corr->w, corr->r, W, H, x, y), init ? 0.0f : target[i]));
+            }
+    } else {
+        for (size_t i = 0; i < N; ++i) target[i] = og_san(fmaf(wgt, s->scale[i], init ? 0.0f : target[i]));
+    }
+    return 0;
+}
+
+static int og_mix(OSched* s, const float* dens, int ch, float* target) {
+    const FjVisualGrain* g = s->o.g;
+    float wf = g->size_mix_weights[0], wm = g->size_mix_weights[1], wc = g->size_mix_weights[2];
+    float sms = g->size_mix_scale;
+    float ws[3] = {wf, wm, wc}, fac[3] = {1.0f, sqrtf(sms), sms};
+    uint64_t salts[3] = {0xA24BAED4963EE407ULL, 0x9F6C1E6B2C4D7A13ULL, 0x3C79AC492BA7B653ULL};
+    int init = 1;
+    for (int i = 0; i < 3; ++i) {
+        if (!(ws[i] > 0.0f)) continue;
+        int apply = i == 0 ? s->corr[0].r > 0 : 1;
+        if (og_scale_pass(s, dens, ch, salts[i], fac[i], &s->corr[i], apply, ws[i], init, target)) return 1;
+        init = 0;
+    }
+    float gain = isfinite(g->size_mix_gain) ? g->size_mix_gain : 0.0f;
+    size_t N = (size_t)s->W * s->H;
+    for (size_t i = 0; i < N; ++i) target[i] = og_san(target[i] * gain);
+    return 0;
+}
+
+static uint64_t og_fnv(uint64_t a, uint64_t b) {
+    uint64_t h = 0xcbf29ce484222325ULL, v[2] = {a, b};
+    for (int k = 0; k < 2; ++k)
+        for (int i = 0; i < 8; ++i) {
+            h ^= (v[k] >> (8 * i)) & 0xFFu;
+            h *= 0x100000001b3ULL;
+        }
+    return h;
+}
+
+/* Visual grain on the three density planes in place. `noise` may be NULL (Philox
+ * stream); base curves are the capture density curves of C, M, Y (n samples), layer
+ * curves [layer][CMY]. Returns 0 on success. */
+int oracle_visual_grain(const FjVisualGrain* g, const FjStaticNoise* noise, const float* const* base_cmy,
+                        const float* const* layers, int n, int positive, float* dc, float* dm, float* dy, int W, int H) {
+    if (!(g->flags & FJ_GRAIN_ACTIVE)) return 0;
+    OSched s;
+    memset(&s, 0, sizeof(s));
+    OGrain* o = &s.o;
+    o->g = g;
+    if (noise) {
+        o->stbn = noise->stbn.data;
+        o->stbn_w = noise->stbn_width;
+        o->stbn_h = noise->stbn_height;
+        o->stbn_frames = noise->stbn_frames;
+        o->wang = noise->wang_tiles.data;
+        o->wang_lut = noise->wang_lut.data;
+        o->wang_w = noise->wang_width;
+        o->wang_h = noise->wang_height;
+        o->wang_count = (int)noise->wang_tile_count;
+        o->wang_colors = noise->wang_colors;
+    }
+    o->stbn_off_x = o->stbn_w > 0 ? (int)(og_fnv(g->session_seed, 0xA5u) % (uint64_t)o->stbn_w) : 0;
+    o->stbn_off_y = o->stbn_h > 0 ? (int)(og_fnv(g->session_seed, 0x5Au) % (uint64_t)o->stbn_h) : 0;
+    if (o->stbn_frames > 0) {
+        int64_t ph = (int64_t)(g->session_seed % (uint64_t)o->stbn_frames);
+        int f = (int)((g->frame0 + ph) % o->stbn_frames);
+        o->stbn_frame = f < 0 ? f + o->stbn_frames : f;
+    }
+    int sub = (g->flags & FJ_GRAIN_SUBLAYERS) != 0;
+    if (sub) {
+        for (int c = 0; c < 3; ++c) {
+            o->base[c] = base_cmy[c];
+            for (int l = 0; l < 3; ++l) o->layer[l][c] = layers[l * 3 + c];
+        }
+        o->n = n;
+    }
+    o->positive = positive;
+    for (int i = 0; i < 3; ++i)
+        if (g->correlation[i].radius > 0) {
+            s.corr[i].r = g->correlation[i].radius;
+            s.corr[i].hash = g->correlation[i].hash;
+            og_taps(s.corr[i].r, g->correlation[i].sigma_px, s.corr[i].w);
+        }
+    for (int l = 0; l < 3; ++l)
+        for (int c = 0; c < 3; ++c)
+            if (sub && g->dye_cloud[l][c].radius > 0) {
+                s.dye[l][c].r = g->dye_cloud[l][c].radius;
+                s.dye[l][c].hash = g->dye_cloud[l][c].hash;
+                og_taps(s.dye[l][c].r, g->dye_cloud[l][c].sigma_px, s.dye[l][c].w);
+            }
+    s.W = W;
+    s.H = H;
+    size_t N = (size_t)W * H;
+    float* buf = (float*)calloc(5 * N, sizeof(float));
+    if (!buf) return 1;
+    s.temp = buf;
+    s.scale = buf + N;
+    s.layer = buf + 2 * N;
+    float* accum = buf + 3 * N;
+    float* shared = buf + 4 * N;
+    float* dens[3] = {dc, dm, dy};
+    int rc = 0;
+    unsigned debug = g->debug_view;
+    if (debug == FJ_GRAIN_DEBUG_MEAN_DENSITY) {
+        float sc = g->debug_scale * 4.0f;
+        sc = isfinite(sc) ? sc : 1.0f;
+        for (size_t i = 0; i < N; ++i) {
+            float a = (dc[i] + dm[i] + dy[i]) * (1.0f / 3.0f);
+            if (!isfinite(a)) a = 0.0f;
+            dc[i] = dm[i] = dy[i] = fmaf(a, sc, 0.0f);
+        }
+        free(buf);
+        return 0;
+    }
+    og_uniforms(o);
+    if (debug >= FJ_GRAIN_DEBUG_DELTA_FINE && debug <= FJ_GRAIN_DEBUG_DELTA_COARSE_RAW) {
+        int coarse = debug == FJ_GRAIN_DEBUG_DELTA_COARSE || debug == FJ_GRAIN_DEBUG_DELTA_COARSE_RAW;
+        int raw = debug == FJ_GRAIN_DEBUG_DELTA_FINE_RAW || debug == FJ_GRAIN_DEBUG_DELTA_COARSE_RAW;
+        for (int c = 0; c < 3 && !rc; ++c) {
+            if (!coarse || g->size_mix_weights[2] > 0.0f) {
+                const OTaps* corr = coarse ? &s.corr[2] : &s.corr[0];
+                rc = og_scale_pass(&s, dens[c], c, coarse ? 0x3C79AC492BA7B653ULL : 0xA24BAED4963EE407ULL,
+                                   coarse ? g->size_mix_scale : 1.0f, corr, !raw && corr->r > 0, 1.0f, 1, accum);
+            } else {
+                memset(accum, 0, N * sizeof(float));
+            }
+            float a = isfinite(g->amplitude) ? g->amplitude : 0.0f;
+            for (size_t i = 0; i < N; ++i) dens[c][i] = og_san(fmaf(a, accum[i], 0.0f));
+        }
+    } else {
+        int shared_chroma = (debug == FJ_GRAIN_DEBUG_OFF || debug == FJ_GRAIN_DEBUG_DELTA_MIX) && g->chroma_mix < 0.999f &&
+                            g->chroma_shared_weight > 0.0f;
+        if (shared_chroma) {
+            FjVisualGrain sg = *g;
+            sg.seed_base ^= 0x7E8A1B9D3F2C65A1ULL;
+            sg.seed_base_next ^= 0x7E8A1B9D3F2C65A1ULL;
+            o->g = &sg;
+            rc = og_mix(&s, dm, 1, shared);
+            o->g = g;
+        }
+        for (int c = 0; c < 3 && !rc; ++c) {
+            int independent = g->chroma_independent_weight > 0.0f || !shared_chroma;
+            if (independent) rc = og_mix(&s, dens[c], c, accum);
+            if (rc) break;
+            float sw = og_clamp(g->chroma_shared_weight, 0.0f, 1.0f), iw = og_clamp(g->chroma_independent_weight, 0.0f, 1.0f);
+            float amp = g->amplitude;
+            float scale = shared_chroma ? 1.0f : amp;
+            scale = isfinite(scale) ? scale : 0.0f;
+            for (size_t i = 0; i < N; ++i) {
+                float d = accum[i];
+                if (shared_chroma) {
+                    float sv = sw > 0.0f ? shared[i] : 0.0f, iv = iw > 0.0f ? accum[i] : 0.0f;
+                    d = og_san(amp * fmaf(sw, sv, iw * iv));
+                }
+                float mean = debug == FJ_GRAIN_DEBUG_OFF ? dens[c][i] : 0.0f;
+                dens[c][i] = og_san(fmaf(scale, d, mean));
+            }
+        }
+    }
+    if (!rc && debug != FJ_GRAIN_DEBUG_OFF) {
+        float sc = isfinite(g->debug_scale) ? g->debug_scale : 1.0f;
+        for (size_t i = 0; i < N; ++i) {
+            float a = (dc[i] + dm[i] + dy[i]) * (1.0f / 3.0f);
+            if (!isfinite(a)) a = 0.0f;
+            dc[i] = dm[i] = dy[i] = fmaf(a, sc, 0.5f);
+        }
+    }
+    free(buf);
+    return rc;
+}

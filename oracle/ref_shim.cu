@@ -404,3 +404,158 @@ extern "C" int ref_spatial_dir(const FjPreparedHostData* h, const float* const* 
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return (int)e;
 }
+
+// ---- visual grain: src/Cuda/Scan/JuicerCudaScanPipeline.cu:3141 with the payload
+// packing of src/Cuda/JuicerCudaFilmPayloads.cpp:384-495 (stbn offsets :212-240).
+extern "C" cudaError_t juicer_cuda_apply_visual_grain(const JuicerCuda::GrainPayload*,
+                                                      const JuicerCuda::GrainKernelPayload*, int, int, float*, float*,
+                                                      float*, float*, float*, float*, float*, float*, void*);
+
+namespace {
+
+uint64_t fnv_pair(uint64_t a, uint64_t b) {
+    uint64_t h = 0xcbf29ce484222325ULL, v[2] = {a, b};
+    for (int k = 0; k < 2; ++k)
+        for (int i = 0; i < 8; ++i) {
+            h ^= (v[k] >> (8 * i)) & 0xFFu;
+            h *= 0x100000001b3ULL;
+        }
+    return h;
+}
+
+// Host Gaussian taps as the reference's host preparation callback produces them
+// (rust/film-juicer-core/src/optics/gaussian.rs:16-52).
+std::vector<float> host_taps(int radius, float sigma) {
+    std::vector<float> w((size_t)(2 * radius + 1));
+    const double s = (double)sigma, s2 = s * s * 2.0;
+    double sum = 0.0;
+    for (int i = -radius; i <= radius; ++i) {
+        const double v = std::exp(-((double)i * (double)i) / s2);
+        w[(size_t)(i + radius)] = (float)v;
+        sum += v;
+    }
+    const double rec = sum != 0.0 ? 1.0 / sum : 0.0;
+    for (float& v : w) v = (float)((double)v * rec);
+    return w;
+}
+
+} // namespace
+
+// Density planes (device, width x height, contiguous) in place. base_cmy: capture
+// density curve values (host, n each); layers: 9 host curves [layer][CMY].
+extern "C" int ref_visual_grain(const FjVisualGrain* g, const FjStaticNoise* noise, const float* const* base_cmy,
+                                const float* const* layers, int n, int positive, float* dc, float* dm, float* dy,
+                                int width, int height) {
+    Arena a;
+    JuicerCuda::GrainPayload p{};
+    JuicerCuda::GrainKernelPayload k{};
+    const bool sub = (g->flags & FJ_GRAIN_SUBLAYERS) != 0;
+    p.active = (g->flags & FJ_GRAIN_ACTIVE) ? 1 : 0;
+    p.sublayersActive = sub ? 1 : 0;
+    p.positiveFilm = positive;
+    p.nSubLayers = (int)g->sublayer_count;
+    p.originX = g->render_extent.x;
+    p.originY = g->render_extent.y;
+    p.seedBase = g->seed_base;
+    p.seedBaseNext = g->seed_base_next;
+    if (noise) {
+        p.stbn = a.put(noise->stbn.data, noise->stbn.count);
+        p.stbnWidth = noise->stbn_width;
+        p.stbnHeight = noise->stbn_height;
+        p.stbnFrames = noise->stbn_frames;
+        p.wangTiles = a.put(noise->wang_tiles.data, noise->wang_tiles.count);
+        p.wangLut = a.put(noise->wang_lut.data, noise->wang_lut.count);
+        p.wangWidth = noise->wang_width;
+        p.wangHeight = noise->wang_height;
+        p.wangCount = (int)noise->wang_tile_count;
+        p.wangColors = noise->wang_colors;
+    }
+    p.stbnOffsetX = p.stbnWidth > 0 ? (int)(fnv_pair(g->session_seed, 0xA5u) % (uint64_t)p.stbnWidth) : 0;
+    p.stbnOffsetY = p.stbnHeight > 0 ? (int)(fnv_pair(g->session_seed, 0x5Au) % (uint64_t)p.stbnHeight) : 0;
+    if (p.stbnFrames > 0) {
+        const int64_t ph = (int64_t)(g->session_seed % (uint64_t)p.stbnFrames);
+        int f = (int)((g->frame0 + ph) % p.stbnFrames);
+        p.stbnFrame = f < 0 ? f + p.stbnFrames : f;
+    }
+    p.frameIndex = g->frame0;
+    p.timeAlpha = g->frame_alpha;
+    p.stbnSessionSeed = g->session_seed;
+    p.clipToken = g->clip_token;
+    p.wangCellMm = g->wang_cell_mm;
+    p.breathingPeriodFrames = g->breathing_period_frames;
+    p.breathingAmplitude = g->breathing_amplitude;
+    p.breathingCellUmSmall = g->breathing_cell_um_small;
+    p.breathingCellUmLarge = g->breathing_cell_um_large;
+    p.breathingMix = g->breathing_mix;
+    p.breathingDriftUmPerFrame = g->breathing_drift_um_per_frame;
+    p.debugView = (int)g->debug_view;
+    p.pixelSizeUm = g->pixel_size_um;
+    p.pitchPx = g->pitch_px;
+    p.microStructure[0] = g->micro_structure[0];
+    p.microStructure[1] = g->micro_structure[1];
+    p.clumpTemporalMix = g->clump_temporal_mix;
+    p.clumpMorphPeriodFrames = g->clump_morph_period_frames;
+    p.sizeMixWeightFine = g->size_mix_weights[0];
+    p.sizeMixWeightMid = g->size_mix_weights[1];
+    p.sizeMixWeight = g->size_mix_weights[2];
+    p.sizeMixScale = g->size_mix_scale;
+    p.sizeMixGain = g->size_mix_gain;
+    p.amplitude = g->amplitude;
+    p.chromaMix = g->chroma_mix;
+    p.chromaSharedWeight = g->chroma_shared_weight;
+    p.chromaIndWeight = g->chroma_independent_weight;
+    p.debugScale = g->debug_scale;
+    for (int c = 0; c < 3; ++c) {
+        p.densityMin[c] = g->particle_density_min_cmy[c];
+        p.uniformity[c] = g->uniformity_cmy[c];
+        p.densityMax[c] = g->density_max_cmy[c];
+        p.nParticles[c] = g->n_particles_cmy[c];
+        p.odParticle[c] = g->od_particle_cmy[c];
+        if (sub) {
+            const float* y = a.put(base_cmy[c], (size_t)n);
+            p.densityCurveCmy[c] = curve(y, y, n);
+            p.densityLayerAxisFinite[c] = (g->flags & (FJ_GRAIN_AXIS_FINITE_C << c)) ? 1 : 0;
+            for (int b = 0; b < 16; ++b) p.densityLayerAxisBlockPrefixMax[c][b] = g->layer_axis_block_prefix_max[c][b];
+        }
+    }
+    // identical Gaussians (same descriptor hash) share one prepared kernel, as the
+    // reference's preparation dedupes them (src/ProcessRoot.cpp:3441-3490)
+    std::vector<std::pair<uint64_t, const float*>> prepared;
+    auto prep = [&](const FjGrainGaussian& gg) -> const float* {
+        if (gg.radius <= 0) return nullptr;
+        for (auto& e : prepared)
+            if (e.first == gg.hash) return e.second;
+        const std::vector<float> w = host_taps(gg.radius, gg.sigma_px);
+        const float* d = a.put(w.data(), w.size());
+        prepared.push_back({gg.hash, d});
+        return d;
+    };
+    k.blurKernel = prep(g->correlation[0]);
+    k.blurRadius = g->correlation[0].radius;
+    k.blurKernelMid = prep(g->correlation[1]);
+    k.blurRadiusMid = g->correlation[1].radius;
+    k.blurKernelCoarse = prep(g->correlation[2]);
+    k.blurRadiusCoarse = g->correlation[2].radius;
+    for (int l = 0; l < 3; ++l)
+        for (int c = 0; c < 3; ++c) {
+            p.densityMinLayers[l][c] = g->density_min_layers[l][c];
+            p.densityMaxLayers[l][c] = g->density_max_layers[l][c];
+            p.nParticlesLayers[l][c] = g->n_particles_layers[l][c];
+            p.odParticleLayers[l][c] = g->od_particle_layers[l][c];
+            p.densityCurvesLayers[l][c] = sub ? a.put(layers[l * 3 + c], (size_t)n) : nullptr;
+            k.dyeKernel[l][c] = sub ? prep(g->dye_cloud[l][c]) : nullptr;
+            k.dyeRadius[l][c] = sub ? g->dye_cloud[l][c].radius : 0;
+        }
+    void* uniforms = nullptr;
+    if (cudaMalloc(&uniforms, sizeof(JuicerCuda::GrainFrameUniforms)) != cudaSuccess) return 2;
+    a.ptrs.push_back(uniforms);
+    p.frameUniforms = static_cast<JuicerCuda::GrainFrameUniforms*>(uniforms);
+    float* work = nullptr;
+    const size_t plane = (size_t)width * (size_t)height;
+    if (cudaMalloc(&work, 5 * plane * sizeof(float)) != cudaSuccess) return 2;
+    a.ptrs.push_back(work);
+    cudaError_t e = juicer_cuda_apply_visual_grain(&p, &k, width, height, dc, dm, dy, work, work + plane,
+                                                   work + 2 * plane, work + 3 * plane, work + 4 * plane, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return (int)e;
+}

@@ -16,6 +16,10 @@ container, where the reference is mounted read-only).
   family weights x intensities, group centres = family centres x sizes, warmth =
   family base + halo warmth clamped to [-1.5, 1.5], scatter fraction from the
   strength table) and the float32 outputs.
+* grain_plan_cases.json: the reference's visual-grain frame characterization
+  (tests/grain/frame-fixtures/linux-release.json): inputs and exact native output
+  fields of every successful case, and the gaussian / energy / period primitives.
+* wang_lut.json: the Wang tile index table of Resources/Noise/Wang/tiles.json.
 * recipe_direct.npz / recipe_print.npz: prepared recipes (film_juicer_b200.prepare)
   for kodak_portra_400 direct and kodak_portra_400 -> kodak_portra_endura print,
   built from the reference's Resources/ profiles and spectral tables.
@@ -144,6 +148,31 @@ def diffusion_images():
     print("diffusion image cases:", len(out["names"]))
 
 
+def grain_plan_cases():
+    with open(os.path.join(REF, "tests", "grain", "frame-fixtures", "linux-release.json")) as fh:
+        j = json.load(fh)
+    keep = ["frame0", "frame_alpha", "seed_base", "seed_base_next", "pitch_px", "breathing_period_frames",
+            "clump_morph_period_frames", "wang_cell_mm", "breathing_amplitude", "breathing_cell_um_small",
+            "breathing_cell_um_large", "breathing_mix", "breathing_drift_um_per_frame", "debug_scale",
+            "density_max_cmy", "n_particles_cmy", "od_particle_cmy", "density_min_layers", "density_max_layers",
+            "n_particles_layers", "od_particle_layers", "correlation", "dye_cloud", "size_mix_weights",
+            "size_mix_gain", "requires_full_frame", "density_layers_hash"]
+    cases = [{"input": c["input"], "expected": {k: c["native"][k] for k in keep}}
+             for c in j["cases"] if c["success"] and c["native"]["active"]]
+    prims = [p for p in j["primitives"] if p["input"]["op"] in ("gaussian", "energy", "period")]
+    with open(os.path.join(HERE, "grain_plan_cases.json"), "w") as fh:
+        json.dump({"cases": cases, "primitives": prims}, fh, separators=(",", ":"))
+    with open(os.path.join(REF, "Resources", "Noise", "Wang", "tiles.json")) as fh:
+        tiles = json.load(fh)
+    lut = [0] * 16
+    for e in tiles["mapping"]:
+        lab = e["labels"]
+        lut[((lab["L"] * 2 + lab["R"]) * 2 + lab["T"]) * 2 + lab["B"]] = e["index"]
+    with open(os.path.join(HERE, "wang_lut.json"), "w") as fh:
+        json.dump(lut, fh)
+    print("grain plan cases:", len(cases), "primitives:", len(prims))
+
+
 def recipes():
     sys.path.insert(0, ROOT)
     import __graft_entry__
@@ -162,4 +191,5 @@ if __name__ == "__main__":
     dir_boundary_cases()
     diffusion_component_cases()
     diffusion_images()
+    grain_plan_cases()
     recipes()
