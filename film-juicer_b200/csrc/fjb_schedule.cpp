@@ -9,12 +9,15 @@
 // src/Cuda/Scan/JuicerCudaScanPipeline.cu:3771).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 
+#include "../../include/juicer_b200.h"
 #include "../../include/juicer_cuda_api.h"
 #include "fjb_internal.h"
 #include "fjb_recipe.h"
@@ -24,7 +27,12 @@ struct FjCuda {
     std::mutex gate;
     bool closed = false;
     int device = -1;
-    std::map<uint64_t, fjb::Recipe*> recipes; // keyed by recipe_hash (non-zero only)
+    std::map<uint64_t, FjbRecipe*> recipes; // keyed by recipe_hash (non-zero only)
+    void* work = nullptr;                    // frame workspace: planes + stage scratch
+    size_t work_bytes = 0;
+    float* ae_scale = nullptr;               // device auto-exposure scale
+    FjbNoise* noise = nullptr;               // device copy of the static grain noise
+    uintptr_t noise_key[3] = {0, 0, 0};
 };
 
 namespace {
@@ -50,10 +58,157 @@ bool aborted(const FjAbortCallback& cb) { return cb.query && cb.query(cb.user) =
 
 void release_all(FjCuda* cuda) {
     for (auto& kv : cuda->recipes) {
-        kv.second->release();
+        kv.second->r.release();
         delete kv.second;
     }
     cuda->recipes.clear();
+    if (cuda->work) cudaFree(cuda->work);
+    cuda->work = nullptr;
+    cuda->work_bytes = 0;
+    if (cuda->ae_scale) cudaFree(cuda->ae_scale);
+    cuda->ae_scale = nullptr;
+    if (cuda->noise) fjb_noise_destroy(cuda->noise, nullptr);
+    cuda->noise = nullptr;
+}
+
+bool same_rect(const FjRect& a, const FjRect& b) { return a.x1 == b.x1 && a.y1 == b.y1 && a.x2 == b.x2 && a.y2 == b.y2; }
+
+// Stages this build schedules; the others are rejected by name rather than skipped.
+bool stages_supported(const FjPreparedHostData& h, std::string& why) {
+    if (h.optics.flags & FJ_OPTICS_ENLARGER_DIFFUSION) {
+        why = "enlarger diffusion is not supported by this build";
+        return false;
+    }
+    if (h.optics.flags & FJ_OPTICS_HIGHLIGHT_BOOST) {
+        why = "highlight boost is not supported by this build";
+        return false;
+    }
+    if (h.scanner_post.flags != 0) {
+        why = "scanner post effects (glare, lens blur, unsharp) are not supported by this build";
+        return false;
+    }
+    if (h.effects.flags & (FJ_EFFECTS_FILM | FJ_EFFECTS_GATE_OUTPUT)) {
+        why = "film and gate defects are not supported by this build";
+        return false;
+    }
+    return true;
+}
+
+cudaError_t ensure_scalar(FjCuda* cuda) {
+    if (cuda->ae_scale) return cudaSuccess;
+    return cudaMalloc(&cuda->ae_scale, 256);
+}
+
+cudaError_t ensure_work(FjCuda* cuda, size_t bytes) {
+    if (cuda->work_bytes >= bytes) return cudaSuccess;
+    if (cuda->work) cudaFree(cuda->work);
+    cuda->work = nullptr;
+    cuda->work_bytes = 0;
+    cudaError_t e = cudaMalloc(&cuda->work, bytes);
+    if (e == cudaSuccess) cuda->work_bytes = bytes;
+    return e;
+}
+
+// Device copy of the static grain noise, uploaded once per distinct host buffer.
+FjStatus ensure_noise(FjCuda* cuda, const FjStaticNoise& n, void* stream, const FjbNoise** out, FjErrorBuffer* error) {
+    *out = nullptr;
+    if (!n.stbn.data || n.stbn.count == 0) return fjb::ok_status();
+    const uintptr_t k0 = reinterpret_cast<uintptr_t>(n.stbn.data), k1 = reinterpret_cast<uintptr_t>(n.wang_tiles.data);
+    if (cuda->noise && cuda->noise_key[0] == k0 && cuda->noise_key[1] == k1 && cuda->noise_key[2] == n.stbn.count) {
+        *out = cuda->noise;
+        return fjb::ok_status();
+    }
+    if (cuda->noise) {
+        fjb_noise_destroy(cuda->noise, nullptr);
+        cuda->noise = nullptr;
+    }
+    FjbNoise* fresh = nullptr;
+    FjStatus st = fjb_noise_create(&n, stream, &fresh, error);
+    if (st.category != FJ_STATUS_SUCCESS) return st;
+    cuda->noise = fresh;
+    cuda->noise_key[0] = k0;
+    cuda->noise_key[1] = k1;
+    cuda->noise_key[2] = n.stbn.count;
+    *out = fresh;
+    return fjb::ok_status();
+}
+
+// The staged schedule of src/Cuda/JuicerCudaExecutor.cpp:1874-2400: camera exposure
+// to carrier planes, camera diffusion, scatter/halation, spatial DIR, capture
+// density, grain, then print/scan/output from the density planes.
+FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData& h, const float* src, ptrdiff_t srb,
+                       float* dst, ptrdiff_t drb, int width, int height, uint32_t comps, void* vs,
+                       const FjAbortCallback& abort_cb, bool camera_diffusion, bool halation, bool spatial_dir,
+                       bool grain, FjErrorBuffer* error) {
+    const size_t plane = (size_t)width * (size_t)height;
+    const size_t plane_bytes = (plane * sizeof(float) + 255) / 256 * 256;
+    size_t scratch = 0;
+    if (halation) scratch = std::max(scratch, fjb_scatter_halation_scratch_bytes(width, height));
+    if (spatial_dir) scratch = std::max(scratch, fjb_spatial_dir_scratch_bytes(width, height));
+    if (grain) scratch = std::max(scratch, fjb_visual_grain_scratch_bytes(width, height));
+    const int planes = 3 + 3 + (spatial_dir ? 6 : 0);
+    cudaError_t e = ensure_work(cuda, planes * plane_bytes + scratch + 256);
+    if (e != cudaSuccess) return fjb::cuda_status(e, error, "frame workspace");
+    char* base = static_cast<char*>(cuda->work);
+    auto P = [&](int i) { return reinterpret_cast<float*>(base + (size_t)i * plane_bytes); };
+    float* carrier[3] = {P(0), P(1), P(2)}; // B, G, R
+    float* density[3] = {P(3), P(4), P(5)}; // C, M, Y (also the diffusion target)
+    float* dirp[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (spatial_dir)
+        for (int i = 0; i < 6; ++i) dirp[i] = P(6 + i);
+    float* scratch_p = reinterpret_cast<float*>(base + (size_t)planes * plane_bytes);
+    const ptrdiff_t stride = width;
+    const FjOptics& o = h.optics;
+
+    FjStatus st = fjb_camera_exposure(recipe, src, srb, comps, width, height, carrier[0], carrier[1], carrier[2],
+                                      stride, vs, error);
+    if (st.category != FJ_STATUS_SUCCESS) return st;
+    if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
+    if (camera_diffusion) {
+        FjDiffusionComponents dc{};
+        st = fjb_diffusion_components_host(&o.camera, &dc, error);
+        if (st.category != FJ_STATUS_SUCCESS) return st;
+        // R, G, B planes into the density planes, which then carry the exposure
+        st = fjb_diffusion(&dc, o.camera.radius_px, o.camera.scatter_fraction, carrier[2], carrier[1], carrier[0],
+                           density[2], density[1], density[0], stride, width, height, vs, error);
+        if (st.category != FJ_STATUS_SUCCESS) return st;
+        std::swap(carrier[0], density[0]);
+        std::swap(carrier[1], density[1]);
+        std::swap(carrier[2], density[2]);
+        if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
+    }
+    if (halation) {
+        st = fjb_scatter_halation(&o.scatter_halation, carrier[2], carrier[1], carrier[0], stride, width, height,
+                                  scratch_p, scratch, vs, error);
+        if (st.category != FJ_STATUS_SUCCESS) return st;
+        if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
+    }
+    if (spatial_dir) {
+        st = fjb_spatial_dir_build(recipe, &h.spatial_dir, nullptr, 0, 3, carrier[0], carrier[1], carrier[2], stride,
+                                   width, height, dirp[0], dirp[1], dirp[2], dirp[3], dirp[4], dirp[5], scratch_p,
+                                   scratch, vs, error);
+        if (st.category == FJ_STATUS_SUCCESS)
+            st = fjb_recipe_set_spatial_dir_planes(recipe, dirp[0], dirp[1], dirp[2], dirp[3], dirp[4], dirp[5], error);
+        if (st.category != FJ_STATUS_SUCCESS) return st;
+        if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
+    }
+    st = fjb_capture_density(recipe, nullptr, 0, 3, carrier[0], carrier[1], carrier[2], stride, width, height,
+                             density[0], density[1], density[2], vs, error);
+    if (st.category != FJ_STATUS_SUCCESS) return st;
+    if (grain) {
+        const FjVisualGrain& g = h.grain;
+        if (g.render_extent.width != width || g.render_extent.height != height)
+            return fjb::fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "grain render extent differs from the render window");
+        const FjbNoise* noise = nullptr;
+        st = ensure_noise(cuda, h.noise, vs, &noise, error);
+        if (st.category != FJ_STATUS_SUCCESS) return st;
+        st = fjb_visual_grain(recipe, &g, noise, density[0], density[1], density[2], stride, width, height, scratch_p,
+                              scratch, vs, error);
+        if (st.category != FJ_STATUS_SUCCESS) return st;
+        if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
+    }
+    return fjb_render_from_density(recipe, density[0], density[1], density[2], comps == 4 ? src : nullptr, srb, dst,
+                                   drb, width, height, comps, vs, error);
 }
 
 } // namespace
@@ -140,71 +295,118 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
             out.status = fjb::fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "frame images or render window rejected");
             return out;
         }
+        const uint32_t optics = prepared->optics.flags;
+        if (optics != 0 && (!same_rect(frame->source.bounds, frame->full_frame_extent) ||
+                            !same_rect(frame->destination.bounds, frame->full_frame_extent) ||
+                            !same_rect(frame->render_window, frame->full_frame_extent))) {
+            out.status = fjb::fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "CUDA optics require the complete frame domain");
+            return out;
+        }
+        std::string unsupported;
+        if (!stages_supported(*prepared, unsupported)) {
+            out.status = fjb::fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, unsupported);
+            return out;
+        }
         if (aborted(abort_callback)) {
             out.status = fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
             return out;
         }
         const bool hostStream = (frame->flags & FJ_FRAME_STREAM_PRESENT) != 0;
         cudaStream_t stream = hostStream ? reinterpret_cast<cudaStream_t>(frame->stream) : nullptr;
+        void* vs = reinterpret_cast<void*>(stream);
 
-        const uint32_t spatialOptics = prepared->optics.flags;
-        const bool grain = (prepared->grain.flags & FJ_GRAIN_ACTIVE) != 0;
-        const bool spatialDir = prepared->spatial_dir.component_count > 0;
-        if (spatialOptics != 0 || grain || spatialDir) {
-            out.status = fjb::fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error,
-                                          "spatial stages are not enabled in this fj_cuda_render build");
-            return out;
-        }
-        if (prepared->film_exposure.flags & FJ_FILM_AUTO_EXPOSURE) {
-            out.status = fjb::fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error,
-                                          "auto exposure is not enabled in this fj_cuda_render build");
-            return out;
-        }
-
-        // ---- recipe tables (cached by recipe_hash) ----
-        fjb::Recipe* recipe = nullptr;
-        fjb::Recipe transient;
+        // ---- recipe tables (cached by recipe_hash; hash 0 = this frame only) ----
+        FjbRecipe* recipe = nullptr;
+        std::unique_ptr<FjbRecipe> transient;
         const uint64_t key = prepared->recipe_hash;
         if (key != 0) {
             auto it = cuda->recipes.find(key);
             if (it != cuda->recipes.end()) recipe = it->second;
         }
         if (!recipe) {
-            auto* fresh = key != 0 ? new fjb::Recipe() : &transient;
+            std::unique_ptr<FjbRecipe> fresh(new FjbRecipe());
+            fresh->device = dev;
             std::string why;
             FjStatus st{};
-            if (!fjb::create_recipe(*prepared, stream, *fresh, why, st)) {
-                if (fresh != &transient) delete fresh;
+            if (!fjb::create_recipe(*prepared, stream, fresh->r, why, st)) {
                 fjb::write_error(error, why);
                 out.status = st;
                 return out;
             }
-            if (key != 0) cuda->recipes[key] = fresh;
-            recipe = fresh;
+            recipe = fresh.get();
+            if (key != 0)
+                cuda->recipes[key] = fresh.release();
+            else
+                transient = std::move(fresh);
         }
-        if (aborted(abort_callback)) {
-            if (recipe == &transient) transient.release();
-            out.status = fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
+        // frame-scoped recipe state is cleared on every exit path
+        struct FrameState {
+            FjbRecipe* r;
+            ~FrameState() {
+                r->r.params.auto_exposure_scale = nullptr;
+                fjb_recipe_set_spatial_dir_planes(r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+            }
+        } frame_state{recipe};
+        struct TransientRelease {
+            std::unique_ptr<FjbRecipe>& t;
+            ~TransientRelease() {
+                if (t) t->r.release();
+            }
+        } transient_release{transient};
+
+        const FjRect& w = frame->render_window;
+        const int width = w.x2 - w.x1, height = w.y2 - w.y1;
+        const uint32_t comps = frame->source.components;
+        const float* src = reinterpret_cast<const float*>(pixel_address(frame->source, w.x1, w.y1));
+        float* dst = const_cast<float*>(reinterpret_cast<const float*>(pixel_address(frame->destination, w.x1, w.y1)));
+        const ptrdiff_t srb = frame->source.row_bytes, drb = frame->destination.row_bytes;
+        FjStatus st = fjb_recipe_clear_flags(recipe, vs, error);
+        if (st.category != FJ_STATUS_SUCCESS) {
+            out.status = st;
             return out;
         }
 
-        const FjRect& w = frame->render_window;
-        fjb::PixelParams p = recipe->params;
-        p.src = pixel_address(frame->source, w.x1, w.y1);
-        p.dst = const_cast<char*>(pixel_address(frame->destination, w.x1, w.y1));
-        p.src_row_bytes = frame->source.row_bytes;
-        p.dst_row_bytes = frame->destination.row_bytes;
-        p.width = w.x2 - w.x1;
-        p.height = w.y2 - w.y1;
-        p.components = (int)frame->source.components;
-        cudaError_t e = cudaMemsetAsync(recipe->flags, 0, sizeof(unsigned), stream);
-        if (e == cudaSuccess) e = fjb::launch_pixel_chain(p, fjb::PixelStage::SourceToOutput, stream);
-        unsigned flags = 0;
-        if (e == cudaSuccess) e = cudaMemcpyAsync(&flags, recipe->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        if (recipe == &transient) transient.release();
-        if (e != cudaSuccess) {
-            out.status = fjb::cuda_status(e, error, "render");
+        // ---- camera auto exposure (src/Cuda/JuicerCudaExecutor.cpp:1013) ----
+        if (prepared->film_exposure.flags & FJ_FILM_AUTO_EXPOSURE) {
+            const FjAutoExposure& ae = prepared->auto_exposure;
+            if (!rect_inside(ae.source_bounds, frame->source.bounds)) {
+                out.status = fjb::fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "auto exposure source bounds outside the source image");
+                return out;
+            }
+            cudaError_t e = ensure_scalar(cuda);
+            if (e != cudaSuccess) {
+                out.status = fjb::cuda_status(e, error, "auto exposure scale");
+                return out;
+            }
+            const float* msrc = reinterpret_cast<const float*>(pixel_address(frame->source, ae.source_bounds.x1, ae.source_bounds.y1));
+            st = fjb_auto_exposure(recipe, msrc, srb, comps, &ae, cuda->ae_scale, vs, error);
+            if (st.category == FJ_STATUS_SUCCESS) st = fjb_recipe_set_exposure_scale_device(recipe, cuda->ae_scale, error);
+            if (st.category != FJ_STATUS_SUCCESS) {
+                out.status = st;
+                return out;
+            }
+        }
+
+        const bool camera_diffusion = (optics & FJ_OPTICS_CAMERA_DIFFUSION) != 0;
+        const bool halation = (optics & FJ_OPTICS_SCATTER_HALATION) != 0;
+        const bool spatial_dir = prepared->spatial_dir.component_count > 0;
+        const bool grain = (prepared->grain.flags & FJ_GRAIN_ACTIVE) != 0;
+        if (!camera_diffusion && !halation && !spatial_dir && !grain) {
+            // Monolithic: one fused pass source -> output
+            st = fjb_render_pixels(recipe, src, srb, dst, drb, width, height, comps, vs, error);
+        } else {
+            st = render_staged(cuda, recipe, *prepared, src, srb, dst, drb, width, height, comps, vs, abort_callback,
+                               camera_diffusion, halation, spatial_dir, grain, error);
+        }
+        if (st.category != FJ_STATUS_SUCCESS) {
+            cudaStreamSynchronize(stream);
+            out.status = st;
+            return out;
+        }
+        uint32_t flags = 0;
+        st = fjb_recipe_read_flags(recipe, vs, &flags, error);
+        if (st.category != FJ_STATUS_SUCCESS) {
+            out.status = st;
             return out;
         }
         if (flags & (1u << 8)) out.flags |= FJ_RENDER_DEFERRED_DIR_ERROR;

@@ -294,3 +294,52 @@ def visual_grain(recipe: "DeviceRecipe", grain, density_cmy, noise: "DeviceNoise
                               C.c_void_p(_ptr(scratch)), scratch.numel() * 4, C.c_void_p(_stream_handle(stream)),
                               C.byref(err.buf))
     _check("fjb_visual_grain", st, err)
+
+
+class Owner:
+    """The drop-in boundary: fj_cuda_create / inspect / render / destroy over CUDA tensors."""
+
+    def __init__(self):
+        self.lib = load_library()
+        self.handle = C.c_void_p()
+        err = abi.ErrorText()
+        _check("fj_cuda_create", self.lib.fj_cuda_create(C.byref(self.handle), C.byref(err.buf)), err)
+
+    def close(self):
+        if self.handle:
+            err = abi.ErrorText()
+            self.lib.fj_cuda_destroy(self.handle, C.byref(err.buf))
+            self.handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def render(self, prepared, src, dst, window=None, stream=None, abort=None):
+        """src/dst: (H, W, comps) float32 CUDA tensors covering the full frame; returns
+        the FjRenderOutcome (raises on a failed status)."""
+        h, w, comps = src.shape
+        fr = abi.FjFrame()
+        for im, t in ((fr.source, src), (fr.destination, dst)):
+            im.address = _ptr(t)
+            im.bounds = abi.FjRect(0, 0, w, h)
+            im.row_bytes = t.stride(0) * 4
+            im.components = comps
+            im.depth = abi.FJ_DEPTH_FLOAT32
+        fr.render_window = abi.FjRect(*(window or (0, 0, w, h)))
+        fr.full_frame_extent = abi.FjRect(0, 0, w, h)
+        if stream is not None:
+            fr.stream = _stream_handle(stream)
+            fr.flags |= abi.FJ_FRAME_STREAM_PRESENT
+        err = abi.ErrorText()
+        ctx = abi.FjCudaContext()
+        _check("fj_cuda_inspect", self.lib.fj_cuda_inspect(self.handle, C.byref(fr), C.byref(ctx), C.byref(err.buf)), err)
+        sub = abi.FjSubmission()
+        query = abi.FjAbortQuery(abort or (lambda user: abi.FJ_ABORT_CONTINUE))
+        cb = abi.FjAbortCallback(query, None)
+        out = self.lib.fj_cuda_render(self.handle, C.byref(ctx), C.byref(fr), C.byref(sub), prepared.pointer(), cb,
+                                      C.byref(err.buf))
+        _check("fj_cuda_render", out.status, err)
+        return out

@@ -1,0 +1,53 @@
+"""The oracle's whole-frame chain for the staged schedule (test infrastructure only):
+camera exposure -> camera diffusion -> scatter/halation -> spatial DIR -> capture
+density -> grain -> print/scan/output, each stage the CPU restatement in oracle/."""
+from __future__ import annotations
+
+import numpy as np
+
+from . import dir as odir
+from . import grain as ograin
+from . import optics as ooptics
+from . import oracle as orc
+
+
+class _Components:
+    def __init__(self, lam, w):
+        self.lambda_px, self.red_weights, self.green_weights, self.blue_weights = lam, w[0], w[1], w[2]
+
+
+def render_frame(frame_record, recipe, src):
+    """frame_record: film_juicer_b200.frame_records.FrameRecord; recipe: the
+    PreparedRecipe it was built from; src: (H, W, comps) float32. Returns the encoded
+    output (H, W, comps) and the error flags."""
+    abi = orc._abi()
+    host = frame_record.host
+    h = host.h
+    scale = 1.0
+    if h.film_exposure.flags & abi.FJ_FILM_AUTO_EXPOSURE:
+        scale = orc.auto_exposure(host, h.auto_exposure, src)
+    carrier, _ = orc.render(host, src, stage=3, auto_scale=scale)  # B, G, R
+    flags = h.optics.flags
+    if flags & abi.FJ_OPTICS_CAMERA_DIFFUSION:
+        d = h.optics.camera
+        lam, w = ooptics.diffusion_components(d.family, list(d.group_weights), list(d.group_lambda_um), d.warmth,
+                                              d.spatial_scale, d.pixel_size_um)
+        r, g, b = ooptics.diffusion(_Components(lam, w), d.radius_px, d.scatter_fraction,
+                                    [carrier[2], carrier[1], carrier[0]])
+        carrier = [b, g, r]
+    if flags & abi.FJ_OPTICS_SCATTER_HALATION:
+        r, g, b = ooptics.scatter_halation(h.optics.scatter_halation, [carrier[2], carrier[1], carrier[0]])
+        carrier = [b, g, r]
+    if h.spatial_dir.component_count > 0:
+        filtered, log_raw, _ = odir.spatial_dir(host, h.spatial_dir, carrier=carrier, width=src.shape[1],
+                                               height=src.shape[0])
+        density, _ = odir.develop_spatial(host, filtered, log_raw)
+    else:
+        density, _ = orc.render(host, None, stage=5, planes=carrier)
+    if h.grain.flags & abi.FJ_GRAIN_ACTIVE:
+        a = recipe.arrays
+        layers = [[a["density_layers"][:, l, c] for c in range(3)] for l in range(3)]
+        base = [a["density_rgb"][:, c] for c in range(3)]
+        noise = frame_record.noise.record if frame_record.noise is not None else None
+        density = ograin.visual_grain(h.grain, noise, base, layers, h.capture_polarity == 1, density)
+    return orc.render(host, src, stage=2, planes=density)

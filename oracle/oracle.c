@@ -789,11 +789,17 @@ int oracle_render(const FjPreparedHostData* h, int stage, const float* src, long
                 D[0] = p0[i];
                 D[1] = p1[i];
                 D[2] = p2[i];
-            } else if (stage == 4) {
+            } else if (stage == 4 || stage == 5) {
                 float e[3] = {p0[i], p1[i], p2[i]};
                 for (int c = 0; c < 3; ++c) e[c] = fmaxf(0.0f, e[c] * p->route);
                 unsigned f = capture_density(p, e, D);
                 if (f) flags |= (1u << 8) | ((f & 7u) << 9);
+                if (stage == 5) { /* carrier B, G, R -> density C, M, Y in the same planes */
+                    p0[i] = D[0];
+                    p1[i] = D[1];
+                    p2[i] = D[2];
+                    continue;
+                }
             } else {
                 float e[3];
                 film_exposure(p, s, auto_scale, stage == 3 ? 0 : 1, e);
