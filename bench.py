@@ -1,20 +1,23 @@
 #!/usr/bin/env python
 """Throughput of the B200 film-process render path (one JSON line on rank 0).
 
-Workload (one step = one frame): 3840x2160 float32 linear Rec.709 RGB synthetic frame
-(seeded smooth fields, see prepare.synthetic_frame), kodak_portra_400 ->
-kodak_portra_endura print route rendered through the fused per-pixel chain
-(exposure, capture development with runtime DIR couplers, 81-wavelength print
-exposure and development, scanner PCHIP LUT, OkLch gamut compression, sRGB
-encoding). Frames are independent, so N GPUs run N replicas (weak scaling, no
-collective on the data path).
+Workload (one step = one frame): the full optical print at 3840x2160 -- a float32
+linear Rec.709 RGB synthetic frame (seeded smooth fields, prepare.synthetic_frame),
+kodak_portra_400 -> kodak_portra_endura print route with every spatial stage on
+(camera diffusion radius 0.5 % of the width, emulsion scatter/halation, spatial DIR
+tail 200 um weight 0.03, density-space grain 35 mm format with fixed seeds over
+synthetic noise of the production shapes), then capture development, 81-wavelength
+print, scanner LUT, OkLch gamut and sRGB output -- rendered by fj_cuda_render, the
+drop-in entry point. Frames are independent, so N GPUs run N replicas (weak scaling,
+no collective on the data path).
 
-  value   Mpix/s with the frame resident in HBM (device-timed with CUDA events on the
-          launching stream, max over ranks);
+  value   Mpix/s with the frame resident in HBM (CUDA events on the render stream
+          around the timed frames, max over ranks);
+  stages  device time per stage from the owner's stage events in the timed region;
   e2e     Mpix/s through the C-ABI with host buffers: pinned host frame -> H2D, render,
           D2H of the rendered frame, every step;
   --impl reference  times the CPU restatement of the reference's render path (the
-          reference has no CPU renderer) on all host threads.
+          reference has no CPU renderer) on all host threads, on crops of the frame.
 """
 from __future__ import annotations
 
@@ -34,14 +37,15 @@ import __graft_entry__  # noqa: E402
 
 WIDTH, HEIGHT = 3840, 2160
 SEED = 20261203 + 2  # seed of the 4K precision-form configuration
-METRIC = "4K print-route render throughput (Mpix/s)"
+METRIC = "4K full optical print render throughput (Mpix/s)"
+CROP = (384, 216)  # CPU sample: a crop of the frame with the 4K frame's descriptors
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="0 skips the CPU baseline leg")
@@ -139,67 +143,88 @@ def dist_setup(n):
     return rank, world, dist
 
 
+def _crop_workload(threads, crop=CROP):
+    """The CPU sample: a crop of the 4K frame rendered by the oracle's chain with the 4K
+    frame's descriptors (same pixel size, diffusion radius, grain)."""
+    __graft_entry__.package()
+    from film_juicer_b200 import frame_records, prepare
+    from oracle import frame as oframe
+
+    recipe = prepare.PreparedRecipe.load(os.path.join(ROOT, "tests", "golden", "recipe_print.npz"))
+    w, h = crop
+    rec = frame_records.FrameRecord(recipe, w, h, descriptor_width=WIDTH)
+    src = prepare.synthetic_frame(WIDTH, HEIGHT, seed=SEED)[:h, :w].copy()
+    return lambda: oframe.render_frame(rec, recipe, src, threads=threads)
+
+
 def run_reference(args):
     """CPU restatement of the reference render path on all host threads."""
-    import numpy as np
-
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    __graft_entry__.package()
-    from film_juicer_b200 import prepare
-    from oracle import oracle as orc
-
-    recipe = prepare.PreparedRecipe.load(os.path.join(ROOT, "tests", "golden", "recipe_print.npz"))
-    rec = prepare.HostRecord(recipe)
     threads = os.cpu_count() or 1
-    rows = 216  # one tenth of the 4K frame per sample
-    strip = prepare.synthetic_frame(WIDTH, HEIGHT, seed=SEED)[:rows]
+    # crops shrink with the step count so that the whole run stays within minutes
+    scale = min(1.0, (100.0 / max(args.steps, 1)) ** 0.5)
+    crop = (max(96, int(CROP[0] * scale) // 8 * 8), max(54, int(CROP[1] * scale) // 2 * 2))
+    step = _crop_workload(threads, crop)
     for _ in range(max(args.warmup, 1)):
-        orc.render(rec, strip, threads=threads)
+        step()
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        orc.render(rec, strip, threads=threads)
+        step()
         times.append(time.perf_counter() - t0)
     per_step = statistics.median(times)
-    mpix = WIDTH * rows / per_step / 1e6
-    sample = f"{WIDTH}x{rows} strip of the 4K frame per step (1/10 frame), median of {args.steps}"
+    mpix = crop[0] * crop[1] / per_step / 1e6
+    sample = (f"{crop[0]}x{crop[1]} crop of the 4K frame per step with the 4K descriptors, "
+              f"median of {args.steps}")
     line = {
-        "impl": "reference", "metric": METRIC, "value": round(mpix, 3), "unit": "Mpix/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": round(mpix, 4), "unit": "Mpix/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "print route per-pixel chain, 3840x2160 frame, sampled as 3840x216 strips",
+        "config": {"workload": "full optical print, 3840x2160 frame, sampled as crops",
                    "recipe": "kodak_portra_400 -> kodak_portra_endura", "threads": threads},
-        "cpu_baseline": {"value": round(mpix, 3), "unit": "Mpix/s", "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": round(mpix, 4), "unit": "Mpix/s", "cores": threads, "kind": "port",
                          "sample": sample},
-        "e2e": {"value": round(mpix, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": round(mpix, 4), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
 def cpu_baseline(seconds: float):
-    """Oracle on a bounded sample of the same frame (all host threads)."""
-    __graft_entry__.package()
-    from film_juicer_b200 import prepare
-    from oracle import oracle as orc
-
-    recipe = prepare.PreparedRecipe.load(os.path.join(ROOT, "tests", "golden", "recipe_print.npz"))
-    rec = prepare.HostRecord(recipe)
+    """The oracle's whole-frame chain on crops of the frame, all host threads."""
     threads = os.cpu_count() or 1
-    rows = 216
-    strip = prepare.synthetic_frame(WIDTH, HEIGHT, seed=SEED)[:rows]
-    orc.render(rec, strip, threads=threads)
+    step = _crop_workload(threads)
+    step()
     n, t0 = 0, time.perf_counter()
     while time.perf_counter() - t0 < seconds:
-        orc.render(rec, strip, threads=threads)
+        step()
         n += 1
     dt = time.perf_counter() - t0
-    return {"value": round(WIDTH * rows * n / dt / 1e6, 3), "unit": "Mpix/s", "cores": threads, "kind": "port",
-            "sample": f"{n} x ({WIDTH}x{rows} strip of the 4K frame) in {dt:.1f} s"}
+    return {"value": round(CROP[0] * CROP[1] * n / dt / 1e6, 4), "unit": "Mpix/s", "cores": threads,
+            "kind": "port",
+            "sample": f"{n} x ({CROP[0]}x{CROP[1]} crop of the 4K frame, 4K descriptors) in {dt:.1f} s"}
+
+
+# Algorithmic work per stage per pixel of the frame (the roofline numerators):
+# compulsory HBM bytes of a fused schedule (4 B per plane read or written), or FLOPs.
+def stage_models(record):
+    h = record.host.h
+    r = h.optics.camera.radius_px
+    return {
+        "camera_exposure": ("hbm", 12 + 12),          # RGB in, 3 planes out
+        "camera_diffusion": ("fp32", 3 * (2 * r + 1) ** 2 * 2.0),  # dense (2r+1)^2 PSF per channel
+        "scatter_halation": ("hbm", 24 + 24),         # 3 planes in + out, in place, plus one temp round trip
+        "spatial_dir": ("hbm", 12 + 36),              # carrier in; raw, filtered and log-raw planes out
+        "capture_density": ("hbm", 12 + 24 + 12),     # carrier + spatial DIR planes in, density out
+        "grain": ("hbm", 12 + 12),                    # density in, density out
+        "print_scan_output": ("hbm", 12 + 12),        # density in, RGB out
+    }
 
 
 def run_b200(args):
+    import ctypes as C
+
     import numpy as np
     import torch
 
@@ -207,18 +232,19 @@ def run_b200(args):
     if world == 1 and torch.cuda.is_available():
         torch.cuda.set_device(0)
     pkg = __graft_entry__.package()
-    pkg.load_library()
-    from film_juicer_b200 import prepare, runtime
+    lib = pkg.load_library()
+    from film_juicer_b200 import abi, frame_records, prepare, runtime
 
     dev = torch.cuda.current_device()
-    recipe = prepare.PreparedRecipe.load(os.path.join(ROOT, "tests", "golden", "recipe_print.npz"))
-    rec = prepare.HostRecord(recipe)
-    stream = torch.cuda.Stream()
-    dr = runtime.DeviceRecipe(rec, stream)
     W, H = args.width, args.height
+    recipe = prepare.PreparedRecipe.load(os.path.join(ROOT, "tests", "golden", "recipe_print.npz"))
+    record = frame_records.FrameRecord(recipe, W, H)
     host = prepare.synthetic_frame(W, H, seed=SEED + rank)
     src = torch.from_numpy(host).to("cuda")
     dst = torch.empty_like(src)
+    stream = torch.cuda.Stream()
+    owner = runtime.Owner()
+    err = abi.ErrorText()
     torch.cuda.synchronize()
 
     def barrier():
@@ -233,88 +259,111 @@ def run_b200(args):
         return float(t.item())
 
     # ---- device-resident throughput ----
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            dr.render(src, dst, stream)
+    for _ in range(args.warmup):
+        owner.render(record, src, dst, stream=stream)
     stream.synchronize()
+    lib.fjb_owner_stage_timing(owner.handle, 1, C.byref(err.buf))
+    launches0 = int(lib.fjb_kernel_launches())
     barrier()
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev) as clocks:
-        with torch.cuda.stream(stream):
-            start.record(stream)
-            for _ in range(args.steps):
-                dr.render(src, dst, stream)
-            end.record(stream)
+        start.record(stream)
+        for _ in range(args.steps):
+            owner.render(record, src, dst, stream=stream)
+        end.record(stream)
         end.synchronize()
     torch.cuda.synchronize()
+    launches = int(lib.fjb_kernel_launches()) - launches0
+    times = abi.FjbStageTimes()
+    lib.fjb_owner_stage_times(owner.handle, C.byref(times), C.byref(err.buf))
+    lib.fjb_owner_stage_timing(owner.handle, 0, C.byref(err.buf))
     barrier()
-    ms = start.elapsed_time(end) / args.steps
-    ms = max_over_ranks(ms)
+    ms = max_over_ranks(start.elapsed_time(end) / args.steps)
     px = W * H
     value = world * px / (ms * 1e-3) / 1e6
+    stages = {}
+    for i, name in enumerate(abi.FJB_STAGE_NAMES):
+        if times.frames[i]:
+            stages[name] = round(times.total_ms[i] / times.frames[i], 4)
 
     # ---- end to end through the C-ABI with host buffers ----
     h_src = torch.from_numpy(host).pin_memory()
     h_dst = torch.empty_like(h_src).pin_memory()
-    with torch.cuda.stream(stream):
-        for _ in range(max(2, args.warmup // 2)):
+    e_steps = max(3, min(args.steps, 30))
+    for _ in range(2):
+        with torch.cuda.stream(stream):
             src.copy_(h_src, non_blocking=True)
-            dr.render(src, dst, stream)
+        owner.render(record, src, dst, stream=stream)
+        with torch.cuda.stream(stream):
             h_dst.copy_(dst, non_blocking=True)
     stream.synchronize()
     barrier()
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        e_start.record(stream)
-        for _ in range(args.steps):
+    e_start.record(stream)
+    for _ in range(e_steps):
+        with torch.cuda.stream(stream):
             src.copy_(h_src, non_blocking=True)
-            dr.render(src, dst, stream)
+        owner.render(record, src, dst, stream=stream)
+        with torch.cuda.stream(stream):
             h_dst.copy_(dst, non_blocking=True)
-        e_end.record(stream)
+    e_end.record(stream)
     e_end.synchronize()
     barrier()
-    e_ms = max_over_ranks(e_start.elapsed_time(e_end) / args.steps)
+    e_ms = max_over_ranks(e_start.elapsed_time(e_end) / e_steps)
     e2e = world * px / (e_ms * 1e-3) / 1e6
     ok = bool(np.isfinite(h_dst.numpy()).all())
 
     if rank == 0:
         pk, pk_kind = peaks()
-        bytes_per_px = 24  # 12 B RGB in + 12 B RGB out, the compulsory HBM traffic
-        achieved = px * bytes_per_px / (ms * 1e-3) / 1e9
+        clk = clocks.summary()
+        models = stage_models(record)
+        # roofline of the stage that takes the most device time
+        dominant = max((k for k in stages if k in models), key=lambda k: stages[k])
+        kind, per_px = models[dominant]
+        stage_s = stages[dominant] * 1e-3
+        if kind == "hbm":
+            achieved = px * per_px / stage_s / 1e9
+            roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                    "frac": round(achieved / pk["hbm_gbs"], 4), "peak_source": pk_kind}
+        else:
+            # FP32 FMA pipe: 148 SMs x 128 lanes x 2 FLOP per clock at the sampled SM clock
+            sm_mhz = clk.get("sm_mhz") or 1965.0
+            peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+            achieved = px * per_px / stage_s / 1e12
+            roof = {"bound": "fp32", "achieved": round(achieved, 2), "peak": round(peak, 1), "unit": "TFLOP/s",
+                    "frac": round(achieved / peak, 4),
+                    "peak_source": "nominal FP32 FMA rate at the sampled SM clock (no tensor or HBM bound applies)"}
+        roof["kernel_stage"] = dominant
+        roof["stage_ms"] = stages[dominant]
         traffic = None
-        prof = os.path.join(ROOT, "profiles", "pixel_chain_print_4k.json")
+        prof = os.path.join(ROOT, "profiles", "frame_stages_4k.json")
         if os.path.exists(prof):
             with open(prof) as fh:
-                traffic = json.load(fh).get("dram_bytes_per_launch")
-        flops_per_px = 1053.0
-        ex2_per_px = 81.0
-        clk = clocks.summary()
+                traffic = json.load(fh).get(dominant, {}).get("dram_bytes_per_launch")
+        roof["traffic"] = traffic
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{W}x{H} print route, fused per-pixel chain (no spatial stages)",
-                       "recipe": "kodak_portra_400 -> kodak_portra_endura, Hanatos TC LUT, runtime DIR, "
-                                 "scanner LUT r=17, OkLch gamut, sRGB",
-                       "frame_bytes": px * 12, "l2_policy": "inputs larger than L2 (2 x 99.5 MB per step)",
+            "config": {"workload": f"{W}x{H} full optical print through fj_cuda_render",
+                       "recipe": "kodak_portra_400 -> kodak_portra_endura, Hanatos TC LUT, spatial DIR tail 200 um "
+                                 "w 0.03, camera diffusion r=0.5% W, scatter/halation, grain 35 mm, scanner LUT r=17, "
+                                 "OkLch gamut, sRGB",
+                       "frame_bytes": px * 12, "l2_policy": "inputs larger than L2 (99.5 MB frame in and out, "
+                                                           "~0.7 GB of stage planes per frame)",
                        "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
-                         "frac": round(achieved / pk["hbm_gbs"], 4), "traffic": traffic,
-                         "peak_source": pk_kind,
-                         "note": "per-pixel chain is MUFU/FMA bound; HBM fraction shown per contract"},
-            "compute": {"flop_per_px": flops_per_px, "ex2_per_px": ex2_per_px,
-                        "fp32_tflops": round(px * flops_per_px / (ms * 1e-3) / 1e12, 2),
-                        "ex2_tera_per_s": round(px * ex2_per_px / (ms * 1e-3) / 1e12, 3)},
+            "stages_ms": stages,
+            "roofline": roof,
             "cpu_baseline": cpu_baseline(args.cpu_seconds) if world == 1 and args.cpu_seconds > 0 else None,
             "e2e": {"value": round(e2e, 2), "unit": "Mpix/s", "h2d_bytes_per_step": int(h_src.numel() * 4),
-                    "d2h_bytes_per_step": int(h_dst.numel() * 4)},
-            "gpu_launches": args.steps,
+                    "d2h_bytes_per_step": int(h_dst.numel() * 4), "steps": e_steps},
+            "gpu_launches": launches,
             "clocks": clk,
             "output_finite": ok,
         }
         print(json.dumps(line), flush=True)
-    dr.close()
+    owner.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

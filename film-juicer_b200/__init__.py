@@ -82,6 +82,9 @@ _EXPORTS = {
     "fjb_visual_grain": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjVisualGrain), C.c_void_p] + [C.c_void_p] * 3 +
                          [C.c_ssize_t, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, C.c_void_p,
                           C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_owner_stage_timing": (abi.FjStatus, [C.c_void_p, C.c_int32, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_owner_stage_times": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbStageTimes), C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_kernel_launches": (C.c_uint64, []),
     "fjb_scanner_lut_build_host": (abi.FjStatus, [C.POINTER(abi.FjbScannerLutInput)] + [C.c_void_p] * 6 +
                                    [C.POINTER(abi.FjErrorBuffer)]),
 }

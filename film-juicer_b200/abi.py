@@ -252,6 +252,9 @@ FjPreparedHostData = _s("FjPreparedHostData", [
     ("grain", FjVisualGrain), ("effects", FjFilmEffects), ("noise", FjStaticNoise)])
 FjDiffusionComponents = _s("FjDiffusionComponents", [("lambda_px", f64 * 9), ("red_weights", f64 * 9),
                                                      ("green_weights", f64 * 9), ("blue_weights", f64 * 9)])
+FJB_STAGE_NAMES = ["auto_exposure", "camera_exposure", "camera_diffusion", "scatter_halation", "spatial_dir",
+                   "capture_density", "grain", "print_scan_output", "monolithic"]
+FjbStageTimes = _s("FjbStageTimes", [("total_ms", f64 * 9), ("frames", u64 * 9)])
 FjbScannerLutInput = _s("FjbScannerLutInput", [
     ("eps_c", FjFloatSpan), ("eps_m", FjFloatSpan), ("eps_y", FjFloatSpan), ("weighted_x", FjFloatSpan),
     ("weighted_y", FjFloatSpan), ("weighted_z", FjFloatSpan), ("baseline_min", FjFloatSpan),
@@ -266,7 +269,7 @@ ALL_RECORDS = [
     FjScannerCorrection, FjScannerPostEffects, FjOutputEncoding, FjOutputColor, FjPrint, FjDiffusion,
     FjHalationGaussian, FjHalationChannel, FjScatterHalation, FjHighlightBoost, FjOptics, FjDirGaussian,
     FjSpatialDir, FjGrainGaussian, FjVisualGrain, FjDust, FjScratch, FjDefectOrigin, FjFilmEffects,
-    FjStaticNoise, FjPreparedHostData, FjbScannerLutInput, FjDiffusionComponents,
+    FjStaticNoise, FjPreparedHostData, FjbScannerLutInput, FjDiffusionComponents, FjbStageTimes,
 ]
 
 

@@ -9,6 +9,8 @@
 // The stage schedule of fj_cuda_render lives in fjb_schedule.cpp.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <cstdio>
 #include <cstring>
 #include <exception>
@@ -22,9 +24,16 @@
 #include "fjb_internal.h"
 #include "fjb_recipe.h"
 #include "fjb_optics.h"
+#include "fjb_launches.h"
 #include "fjb_schedule.h"
 
 namespace fjb {
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void write_error(FjErrorBuffer* error, const std::string& text) {
     if (!error) return;
@@ -66,6 +75,8 @@ cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 } // namespace
 
 extern "C" {
+
+uint64_t fjb_kernel_launches(void) { return (uint64_t)fjb::g_launches.load(std::memory_order_relaxed); }
 
 FjStatus fjb_recipe_create(const FjPreparedHostData* prepared, void* stream, FjbRecipe** out_recipe,
                            FjErrorBuffer* error) {

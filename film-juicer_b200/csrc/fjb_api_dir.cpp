@@ -20,11 +20,83 @@ using fjb::fail_status;
 using fjb::ok_status;
 using fjb::write_error;
 
+namespace fjb {
+
+FjStatus spatial_dir_apply(FjbRecipe* recipe, const DirPlan& plan, const float* src, ptrdiff_t src_row_bytes,
+                           uint32_t components, const float* carrier_b, const float* carrier_g, const float* carrier_r,
+                           ptrdiff_t carrier_stride, int width, int height, float* filtered_y, float* filtered_m,
+                           float* filtered_c, float* log_raw_b, float* log_raw_g, float* log_raw_r, float* scratch,
+                           size_t scratch_bytes, void* stream, FjErrorBuffer* error) {
+    if (!filtered_y || !filtered_m || !filtered_c || !log_raw_b || !log_raw_g || !log_raw_r)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    const bool carrier = carrier_b && carrier_g && carrier_r;
+    if (!carrier && (!src || !(components == 3 || components == 4)))
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "spatial DIR needs a source image or carrier planes");
+    if (recipe->r.params.dir_mode == kDirInactive)
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "spatial DIR needs active DIR couplers");
+    if (!scratch || scratch_bytes < fjb_spatial_dir_scratch_bytes(width, height))
+        return fail_status(FJ_STATUS_ALLOCATION_FAILURE, error, "spatial DIR scratch is too small");
+    if (reinterpret_cast<uintptr_t>(scratch) % 16 != 0)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "spatial DIR scratch must be 16-byte aligned");
+    if (plan.width != width || plan.height != height)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "spatial DIR plan built for another frame size");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const size_t plane = (size_t)width * (size_t)height;
+    float* raw[3] = {scratch, scratch + plane, scratch + 2 * plane};
+    PixelParams p = recipe->r.params;
+    p.src = reinterpret_cast<const char*>(src);
+    p.src_row_bytes = src_row_bytes;
+    p.components = (int)components;
+    p.width = width;
+    p.height = height;
+    p.carrier_b = carrier_b;
+    p.carrier_g = carrier_g;
+    p.carrier_r = carrier_r;
+    p.carrier_stride = carrier_stride;
+    p.dir_src_y = raw[0];
+    p.dir_src_m = raw[1];
+    p.dir_src_c = raw[2];
+    p.dir_src_log_b = log_raw_b;
+    p.dir_src_log_g = log_raw_g;
+    p.dir_src_log_r = log_raw_r;
+    cudaError_t e = launch_pixel_chain(p, carrier ? PixelStage::CarrierToDirSource : PixelStage::SourceToDirSource, s);
+    if (e == cudaSuccess) {
+        DirBlurParams bp{};
+        bp.width = width;
+        bp.height = height;
+        {
+            const size_t planes_bytes =
+                ((size_t)(3 + 3 * kDirMaxComponents) * plane * sizeof(float) + 255) / 256 * 256;
+            char* rec = reinterpret_cast<char*>(scratch) + planes_bytes;
+            bp.lines_max = width > height ? width : height;
+            const int sw = width / kDirSeg > 1 ? width / kDirSeg : 1, sh = height / kDirSeg > 1 ? height / kDirSeg : 1;
+            bp.segs_max = sw > sh ? sw : sh;
+            bp.carry = reinterpret_cast<double*>(rec);
+            bp.start = bp.carry + (size_t)3 * kDirMaxComponents * bp.lines_max * bp.segs_max * 3;
+        }
+        bp.count = plan.count;
+        for (int k = 0; k < plan.count; ++k) bp.comp[k] = plan.comp[k];
+        float* out[3] = {filtered_y, filtered_m, filtered_c};
+        for (int c = 0; c < 3; ++c) {
+            bp.raw[c] = raw[c];
+            bp.filtered[c] = out[c];
+            for (int k = 0; k < kDirMaxComponents; ++k)
+                bp.temp[c][k] = scratch + (3 + (size_t)c * kDirMaxComponents + k) * plane;
+        }
+        e = launch_dir_blur(bp, s);
+    }
+    if (e != cudaSuccess) return cuda_status(e, error, "spatial DIR");
+    return ok_status();
+}
+
+} // namespace fjb
+
 extern "C" {
 
 size_t fjb_spatial_dir_scratch_bytes(int32_t width, int32_t height) {
     if (width <= 0 || height <= 0) return 0;
-    return (size_t)(3 + 3 * fjb::kDirMaxComponents) * (size_t)width * (size_t)height * sizeof(float);
+    const size_t planes = (size_t)(3 + 3 * fjb::kDirMaxComponents) * (size_t)width * (size_t)height * sizeof(float);
+    return (planes + 255) / 256 * 256 + fjb::dir_recursion_bytes(width, height);
 }
 
 FjStatus fjb_spatial_dir_build(FjbRecipe* recipe, const FjSpatialDir* spatial_dir, const float* src,
@@ -34,20 +106,11 @@ FjStatus fjb_spatial_dir_build(FjbRecipe* recipe, const FjSpatialDir* spatial_di
                                float* filtered_c, float* log_raw_b, float* log_raw_g, float* log_raw_r,
                                float* scratch, size_t scratch_bytes, void* stream, FjErrorBuffer* error) {
     try {
-        if (!recipe || !spatial_dir || !filtered_y || !filtered_m || !filtered_c || !log_raw_b || !log_raw_g ||
-            !log_raw_r)
-            return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+        if (!recipe || !spatial_dir) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
         if (width <= 0 || height <= 0) {
             write_error(error, "");
             return ok_status();
         }
-        const bool carrier = carrier_b && carrier_g && carrier_r;
-        if (!carrier && (!src || !(components == 3 || components == 4)))
-            return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "spatial DIR needs a source image or carrier planes");
-        if (recipe->r.params.dir_mode == fjb::kDirInactive)
-            return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "spatial DIR needs active DIR couplers");
-        if (!scratch || scratch_bytes < fjb_spatial_dir_scratch_bytes(width, height))
-            return fail_status(FJ_STATUS_ALLOCATION_FAILURE, error, "spatial DIR scratch is too small");
         cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
         fjb::DirPlan plan;
         std::string why;
@@ -57,44 +120,14 @@ FjStatus fjb_spatial_dir_build(FjbRecipe* recipe, const FjSpatialDir* spatial_di
             if (e != cudaSuccess) return cuda_status(e, error, "spatial DIR plan");
             return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, why);
         }
-        const size_t plane = (size_t)width * (size_t)height;
-        float* raw[3] = {scratch, scratch + plane, scratch + 2 * plane};
-        fjb::PixelParams p = recipe->r.params;
-        p.src = reinterpret_cast<const char*>(src);
-        p.src_row_bytes = src_row_bytes;
-        p.components = (int)components;
-        p.width = width;
-        p.height = height;
-        p.carrier_b = carrier_b;
-        p.carrier_g = carrier_g;
-        p.carrier_r = carrier_r;
-        p.carrier_stride = carrier_stride;
-        p.dir_src_y = raw[0];
-        p.dir_src_m = raw[1];
-        p.dir_src_c = raw[2];
-        p.dir_src_log_b = log_raw_b;
-        p.dir_src_log_g = log_raw_g;
-        p.dir_src_log_r = log_raw_r;
-        e = fjb::launch_pixel_chain(
-            p, carrier ? fjb::PixelStage::CarrierToDirSource : fjb::PixelStage::SourceToDirSource, s);
-        if (e == cudaSuccess) {
-            fjb::DirBlurParams bp{};
-            bp.width = width;
-            bp.height = height;
-            bp.count = plan.count;
-            for (int k = 0; k < plan.count; ++k) bp.comp[k] = plan.comp[k];
-            float* out[3] = {filtered_y, filtered_m, filtered_c};
-            for (int c = 0; c < 3; ++c) {
-                bp.raw[c] = raw[c];
-                bp.filtered[c] = out[c];
-                for (int k = 0; k < fjb::kDirMaxComponents; ++k)
-                    bp.temp[c][k] = scratch + (3 + (size_t)c * fjb::kDirMaxComponents + k) * plane;
-            }
-            e = fjb::launch_dir_blur(bp, s);
-        }
+        FjStatus st = fjb::spatial_dir_apply(recipe, plan, src, src_row_bytes, components, carrier_b, carrier_g,
+                                             carrier_r, carrier_stride, width, height, filtered_y, filtered_m,
+                                             filtered_c, log_raw_b, log_raw_g, log_raw_r, scratch, scratch_bytes,
+                                             stream, error);
         // the plan's device tables must outlive the kernels that read them
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        e = cudaStreamSynchronize(s);
         plan.release();
+        if (st.category != FJ_STATUS_SUCCESS) return st;
         if (e != cudaSuccess) return cuda_status(e, error, "spatial DIR");
         write_error(error, "");
         return ok_status();

@@ -15,6 +15,7 @@
 
 #include "fjb_internal.h"
 #include "fjb_pixel_math.cuh"
+#include "fjb_launches.h"
 
 namespace fjb {
 
@@ -202,6 +203,7 @@ cudaError_t launch_auto_exposure(const PixelParams& p, const MeterSpec& m, void*
     double* partials = static_cast<double*>(scratch);
     unsigned* ticket = reinterpret_cast<unsigned*>(static_cast<char*>(scratch) + (size_t)kMeterBlocks * 2 * kLanes *
                                                                                       sizeof(double));
+    fjb::count_launch();
     meter_kernel<<<grid, kMeterThreads, 0, stream>>>(p, m, partials, ticket, scale);
     return cudaGetLastError();
 }

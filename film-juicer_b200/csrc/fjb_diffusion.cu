@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "fjb_diffusion.h"
+#include "fjb_launches.h"
 
 namespace fjb {
 
@@ -172,6 +173,7 @@ cudaError_t launch_diffusion(const float* const psf_rows[3], int radius, int tap
     cudaError_t e = cudaFuncSetAttribute(diffusion_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const dim3 grid((width + kTileW - 1) / kTileW, (height + kTileH - 1) / kTileH, 3);
+    fjb::count_launch();
     diffusion_kernel<<<grid, kThreads, smem, stream>>>(P);
     return cudaGetLastError();
 }

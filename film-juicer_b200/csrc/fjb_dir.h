@@ -45,7 +45,10 @@ struct DirComponentDev {
     const double* v_init;
     int v_len, v_tsize;
     double v_term[9];
+    double seg[9]; // recursion state map over kDirSeg zero-input steps (row-major 3x3)
 };
+
+constexpr int kDirSeg = 64; // segment length of the block-parallel recursions
 
 struct DirBlurParams {
     int width, height, count;
@@ -53,7 +56,16 @@ struct DirBlurParams {
     const float* raw[3]; // correction planes Y, M, C (width floats per row)
     float* filtered[3];  // outputs Y, M, C
     float* temp[3][kDirMaxComponents];
+    // block-parallel recursion buffers: 3 doubles of segment state per (channel,
+    // component, line, segment); 9 doubles of start states and end block per
+    // (channel, component, line)
+    double* carry;
+    double* start;
+    int lines_max, segs_max;
 };
+
+// Bytes of the recursion buffers for a width x height frame.
+size_t dir_recursion_bytes(int width, int height);
 
 cudaError_t launch_dir_blur(const DirBlurParams& p, cudaStream_t stream);
 
@@ -69,5 +81,19 @@ bool dir_plan_create(const FjSpatialDir& sd, int width, int height, cudaStream_t
                      std::string& why, cudaError_t& err);
 
 size_t dir_scratch_floats(int width, int height);
+
+} // namespace fjb
+
+struct FjbRecipe;
+
+namespace fjb {
+
+// Spatial-DIR source + blur with a prepared plan (enqueues only; the plan must stay
+// alive until the work has run).
+FjStatus spatial_dir_apply(FjbRecipe* recipe, const DirPlan& plan, const float* src, ptrdiff_t src_row_bytes,
+                           uint32_t components, const float* carrier_b, const float* carrier_g, const float* carrier_r,
+                           ptrdiff_t carrier_stride, int width, int height, float* filtered_y, float* filtered_m,
+                           float* filtered_c, float* log_raw_b, float* log_raw_g, float* log_raw_r, float* scratch,
+                           size_t scratch_bytes, void* stream, FjErrorBuffer* error);
 
 } // namespace fjb

@@ -260,6 +260,14 @@ void DirPlan::release() {
     count = 0;
 }
 
+size_t dir_recursion_bytes(int width, int height) {
+    const size_t lines = (size_t)(width > height ? width : height);
+    const int sw = width / kDirSeg > 1 ? width / kDirSeg : 1, sh = height / kDirSeg > 1 ? height / kDirSeg : 1;
+    const size_t segs = (size_t)(sw > sh ? sw : sh);
+    return ((size_t)3 * kDirMaxComponents * lines * segs * 3 + (size_t)3 * kDirMaxComponents * lines * 9) *
+           sizeof(double);
+}
+
 size_t dir_scratch_floats(int width, int height) {
     // raw corrections (3) + log raw (3) + filtered (3) + one temp per channel/component
     return (size_t)(9 + 3 * kDirMaxComponents) * (size_t)width * (size_t)height;
@@ -328,6 +336,19 @@ bool dir_plan_create(const FjSpatialDir& sd, int width, int height, cudaStream_t
                 c.op = kDirOpYvv;
                 c.ff = g.feedforward;
                 for (int k = 0; k < 3; ++k) c.fb[k] = g.feedback[k];
+                {
+                    // companion map (s0, s1, s2) -> (fb0 s0 + fb1 s1 + fb2 s2, s0, s1), kDirSeg steps
+                    const double m[9] = {c.fb[0], c.fb[1], c.fb[2], 1, 0, 0, 0, 1, 0};
+                    double r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+                    for (int step = 0; step < kDirSeg; ++step) {
+                        double t[9];
+                        for (int i = 0; i < 3; ++i)
+                            for (int j = 0; j < 3; ++j)
+                                t[i * 3 + j] = m[i * 3] * r[j] + m[i * 3 + 1] * r[3 + j] + m[i * 3 + 2] * r[6 + j];
+                        std::memcpy(r, t, sizeof(r));
+                    }
+                    std::memcpy(c.seg, r, sizeof(r));
+                }
                 DirAxisBoundary hb, vb;
                 if (!dir_axis_boundary(g, width, hb, why) || !dir_axis_boundary(g, height, vb, why)) return false;
                 void* d = nullptr;

@@ -30,6 +30,7 @@
 #include <cstdint>
 
 #include "fjb_grain.h"
+#include "fjb_launches.h"
 
 namespace fjb {
 
@@ -705,6 +706,7 @@ dim3 plane_grid(int width, int height) { return dim3((width + 31) / 32, (height 
 } // namespace
 
 cudaError_t launch_grain_uniforms(const GrainFrame& f, cudaStream_t s) {
+    fjb::count_launch();
     grain_uniforms_kernel<<<1, 32, 0, s>>>(f);
     return cudaGetLastError();
 }
@@ -716,14 +718,17 @@ cudaError_t launch_grain_sample(const GrainFrame& f, int mode, int channel, int 
     const dim3 block(32, 8), grid = plane_grid(width, height);
     switch (mode) {
     case kGrainSimple:
+        fjb::count_launch();
         grain_sample_kernel<kGrainSimple><<<grid, block, 0, s>>>(f, channel, layer, density, density_stride, out, ep,
                                                                  width, height);
         break;
     case kGrainLayer:
+        fjb::count_launch();
         grain_sample_kernel<kGrainLayer><<<grid, block, 0, s>>>(f, channel, layer, density, density_stride, out, ep,
                                                                 width, height);
         break;
     default:
+        fjb::count_launch();
         grain_sample_kernel<kGrainTriplet><<<grid, block, 0, s>>>(f, channel, layer, density, density_stride, out,
                                                                   ep, width, height);
         break;
@@ -737,6 +742,7 @@ cudaError_t launch_grain_blur_rows(const float* in, long long in_stride, float* 
     if (taps.radius <= 0 || taps.radius > kGrainMaxRadius) return cudaErrorInvalidValue;
     const size_t smem = (size_t)kRowLines * (kRowTile + 2 * taps.radius) * sizeof(float);
     const dim3 grid((width + kRowTile - 1) / kRowTile, (height + kRowLines - 1) / kRowLines);
+    fjb::count_launch();
     grain_rows_kernel<<<grid, dim3(kRowTile, kRowLines), smem, s>>>(in, in_stride, out, out_stride, taps, width,
                                                                     height);
     return cudaGetLastError();
@@ -749,6 +755,7 @@ cudaError_t launch_grain_blur_columns(const float* in, long long in_stride, Grai
     if (taps.radius <= 0 || taps.radius > kGrainMaxRadius) return cudaErrorInvalidValue;
     const size_t smem = (size_t)(kColTileY + 2 * taps.radius) * kColTileX * sizeof(float);
     const dim3 grid((width + kColTileX - 1) / kColTileX, (height + kColTileY - 1) / kColTileY);
+    fjb::count_launch();
     grain_columns_kernel<<<grid, dim3(kColTileX, kColThreadsY), smem, s>>>(in, in_stride, out, taps, ep, width,
                                                                            height);
     return cudaGetLastError();
@@ -758,6 +765,7 @@ cudaError_t launch_grain_accumulate_weighted(GrainPlane dst, const float* src, l
                                              int init, int apply_gain, float gain, int width, int height,
                                              cudaStream_t s) {
     if (width <= 0 || height <= 0) return cudaSuccess;
+    fjb::count_launch();
     grain_accumulate_weighted_kernel<<<plane_grid(width, height), dim3(32, 8), 0, s>>>(
         dst, src, src_stride, weight, init, apply_gain, gain, width, height);
     return cudaGetLastError();
@@ -765,6 +773,7 @@ cudaError_t launch_grain_accumulate_weighted(GrainPlane dst, const float* src, l
 
 cudaError_t launch_grain_clear(GrainPlane dst, int width, int height, cudaStream_t s) {
     if (width <= 0 || height <= 0) return cudaSuccess;
+    fjb::count_launch();
     grain_clear_kernel<<<plane_grid(width, height), dim3(32, 8), 0, s>>>(dst, width, height);
     return cudaGetLastError();
 }
@@ -773,6 +782,7 @@ cudaError_t launch_grain_finish(float* density, long long density_stride, const 
                                 const float* shared, float shared_weight, float independent_weight, float amplitude,
                                 float scale, int add_mean, int width, int height, cudaStream_t s) {
     if (width <= 0 || height <= 0) return cudaSuccess;
+    fjb::count_launch();
     grain_finish_kernel<<<plane_grid(width, height), dim3(32, 8), 0, s>>>(
         density, density_stride, delta, delta_stride, shared, shared_weight, independent_weight, amplitude, scale,
         add_mean, width, height);
@@ -782,6 +792,7 @@ cudaError_t launch_grain_finish(float* density, long long density_stride, const 
 cudaError_t launch_grain_debug_average(float* c, float* m, float* y, long long stride, float offset, float scale,
                                        int width, int height, cudaStream_t s) {
     if (width <= 0 || height <= 0) return cudaSuccess;
+    fjb::count_launch();
     grain_debug_average_kernel<<<plane_grid(width, height), dim3(32, 8), 0, s>>>(c, m, y, stride, offset, scale,
                                                                                 width, height);
     return cudaGetLastError();

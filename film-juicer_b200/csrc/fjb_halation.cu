@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include "fjb_optics.h"
+#include "fjb_launches.h"
 
 namespace fjb {
 
@@ -67,57 +68,176 @@ __device__ __forceinline__ float yvv_step(const OpticGauss& g, float x, YvvState
 __host__ __device__ __forceinline__ bool is_yvv(int kind) { return kind == kGaussYvv || kind == kGaussYvvFactored; }
 
 // ---------------------------------------------------------------------------
-// Row pass, recursive Gaussians: one warp owns 32 rows; 32x32 tiles are staged in
-// shared memory so every global access is a coalesced 128-byte row segment, then each
-// lane walks its own row through the tile (forward, then backward).
+// Recursive Gaussians, block-parallel. A line is cut into segments of kOpticSeg
+// samples (the segment processed last in a direction absorbs the remainder). A
+// partial kernel runs every segment from a zero state and keeps its exit state Z;
+// the final kernel rebuilds each segment's true entry state from the line's start
+// state and the exit states of the segments before it (x_{k+1} = M x_k + Z_k with
+// M the recursion's state map over one segment, in FP64), then runs the segment
+// again and writes it. In exact arithmetic this is the sequential recursion; in
+// FP32 it differs from it by rounding. Row kernels stage 32 rows x one segment in
+// shared memory so global accesses stay coalesced; column kernels give each lane one
+// column, so a warp reads 32 consecutive floats per step.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kTile) rows_yvv_kernel(const __grid_constant__ OpticPass P) {
-    const OpticJob& J = P.job[blockIdx.y];
-    __shared__ float tile[kTile][kTile + 1];
-    const int lane = threadIdx.x;
-    const int row0 = blockIdx.x * kTile;
-    if (row0 >= P.height) return;
-    const int y = row0 + lane;
+constexpr int kSeg = kOpticSeg;
+constexpr int kTileCols = 2 * kSeg; // longest segment < 2 * kSeg
+
+__device__ __forceinline__ int seg_count(int n) { return n / kSeg > 1 ? n / kSeg : 1; }
+
+// forward segment b: [b*kSeg, (b+1)*kSeg), the last one running to n
+__device__ __forceinline__ void fwd_seg(int n, int b, int& lo, int& hi) {
+    lo = b * kSeg;
+    hi = b == seg_count(n) - 1 ? n : lo + kSeg;
+}
+
+// backward segment b (b-th from the end): [n-(b+1)*kSeg, n-b*kSeg), the last one from 0
+__device__ __forceinline__ void bwd_seg(int n, int b, int& lo, int& hi) {
+    hi = n - b * kSeg;
+    lo = b == seg_count(n) - 1 ? 0 : hi - kSeg;
+}
+
+__device__ __forceinline__ float* carry_at(const OpticPass& P, int job, int g, int line, int seg) {
+    return P.carry + ((((size_t)job * kOpticMaxGauss + g) * P.lines_max + line) * P.segs_max + seg) * 3;
+}
+
+__device__ __forceinline__ size_t edge_at(const OpticPass& P, int job, int g, int line) {
+    return ((size_t)job * kOpticMaxGauss + g) * P.lines_max + line;
+}
+
+__device__ __forceinline__ void store_exit(float* c, const YvvState& s) {
+    c[0] = s.s1;
+    c[1] = s.s2;
+    c[2] = s.s3;
+}
+
+// Entry state of segment `seg` (processing order) from the replicate start `first`.
+__device__ __forceinline__ YvvState entry_state(const OpticGauss& g, const OpticPass& P, int job, int gi, int line,
+                                                int seg, float first) {
+    YvvState s0;
+    yvv_init(g, first, s0);
+    double a = s0.s1, b = s0.s2, c = s0.s3;
+    for (int i = 0; i < seg; ++i) {
+        const float* z = carry_at(P, job, gi, line, i);
+        const double na = g.seg[0] * a + g.seg[1] * b + g.seg[2] * c + (double)z[0];
+        const double nb = g.seg[3] * a + g.seg[4] * b + g.seg[5] * c + (double)z[1];
+        const double nc = g.seg[6] * a + g.seg[7] * b + g.seg[8] * c + (double)z[2];
+        a = na;
+        b = nb;
+        c = nc;
+    }
+    return YvvState{(float)a, (float)b, (float)c};
+}
+
+__device__ __forceinline__ void load_rows(float (*tile)[kTileCols + 1], const float* src, long long stride, int row0,
+                                          int H, int lo, int len) {
+    for (int r = 0; r < 32; ++r) {
+        const int y = row0 + r;
+        for (int c = threadIdx.x; c < len; c += 32) tile[r][c] = y < H ? src[(long long)y * stride + lo + c] : 0.0f;
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void store_rows(float (*tile)[kTileCols + 1], float* dst, long long stride, int row0, int H,
+                                           int lo, int len) {
+    __syncwarp();
+    for (int r = 0; r < 32; ++r) {
+        const int y = row0 + r;
+        if (y >= H) break;
+        for (int c = threadIdx.x; c < len; c += 32) dst[(long long)y * stride + lo + c] = tile[r][c];
+    }
+    __syncwarp();
+}
+
+// Rows, forward, zero-state exit states.
+__global__ void __launch_bounds__(32) rows_partial_fwd_kernel(const __grid_constant__ OpticPass P) {
+    const int job = blockIdx.z, seg = blockIdx.y;
+    const OpticJob& J = P.job[job];
     const int W = P.width, H = P.height;
+    if (seg >= seg_count(W) - 1) return; // the last segment's exit state is never used
+    __shared__ float tile[32][kTileCols + 1];
+    int lo, hi;
+    fwd_seg(W, seg, lo, hi);
+    const int row0 = blockIdx.x * 32, y = row0 + threadIdx.x;
+    load_rows(tile, J.src, J.stride, row0, H, lo, hi - lo);
+    if (y >= H) return;
     for (int gi = 0; gi < J.count; ++gi) {
         const OpticGauss& g = J.g[gi];
         if (!is_yvv(g.kind)) continue;
-        float* T = J.temp[gi];
-        YvvState st;
-        yvv_init(g, y < H ? J.src[(long long)y * J.stride] : 0.0f, st);
-        for (int c0 = 0; c0 < W; c0 += kTile) {
-            const int x = c0 + lane;
-            for (int r = 0; r < kTile; ++r) {
-                const int yy = row0 + r;
-                tile[r][lane] = (yy < H && x < W) ? J.src[(long long)yy * J.stride + x] : 0.0f;
-            }
-            __syncwarp();
-            const int cols = min(kTile, W - c0);
-            for (int c = 0; c < cols; ++c) tile[lane][c] = yvv_step(g, tile[lane][c], st);
-            __syncwarp();
-            for (int r = 0; r < kTile; ++r) {
-                const int yy = row0 + r;
-                if (yy < H && x < W) T[(long long)yy * W + x] = tile[r][lane];
-            }
-            __syncwarp();
+        YvvState st{0.0f, 0.0f, 0.0f};
+        for (int c = 0; c < hi - lo; ++c) yvv_step(g, tile[threadIdx.x][c], st);
+        store_exit(carry_at(P, job, gi, y, seg), st);
+    }
+}
+
+// Rows, forward, final values into the Gaussian's row-filtered plane.
+__global__ void __launch_bounds__(32) rows_final_fwd_kernel(const __grid_constant__ OpticPass P) {
+    const int job = blockIdx.z, seg = blockIdx.y;
+    const OpticJob& J = P.job[job];
+    const int W = P.width, H = P.height;
+    if (seg >= seg_count(W)) return;
+    __shared__ float in[32][kTileCols + 1];
+    __shared__ float out[32][kTileCols + 1];
+    int lo, hi;
+    fwd_seg(W, seg, lo, hi);
+    const int len = hi - lo;
+    const int row0 = blockIdx.x * 32, y = row0 + threadIdx.x;
+    load_rows(in, J.src, J.stride, row0, H, lo, len);
+    for (int gi = 0; gi < J.count; ++gi) {
+        const OpticGauss& g = J.g[gi];
+        if (!is_yvv(g.kind)) continue;
+        if (y < H) {
+            YvvState st = entry_state(g, P, job, gi, y, seg, J.src[(long long)y * J.stride]);
+            for (int c = 0; c < len; ++c) out[threadIdx.x][c] = yvv_step(g, in[threadIdx.x][c], st);
+            if (seg == seg_count(W) - 1) P.edge_a[edge_at(P, job, gi, y)] = out[threadIdx.x][len - 1];
         }
-        yvv_init(g, y < H ? T[(long long)y * W + W - 1] : 0.0f, st);
-        for (int c0 = ((W - 1) / kTile) * kTile; c0 >= 0; c0 -= kTile) {
-            const int x = c0 + lane;
-            for (int r = 0; r < kTile; ++r) {
-                const int yy = row0 + r;
-                tile[r][lane] = (yy < H && x < W) ? T[(long long)yy * W + x] : 0.0f;
-            }
-            __syncwarp();
-            const int cols = min(kTile, W - c0);
-            for (int c = cols - 1; c >= 0; --c) tile[lane][c] = yvv_step(g, tile[lane][c], st);
-            __syncwarp();
-            for (int r = 0; r < kTile; ++r) {
-                const int yy = row0 + r;
-                if (yy < H && x < W) T[(long long)yy * W + x] = tile[r][lane];
-            }
-            __syncwarp();
+        store_rows(out, J.temp[gi], W, row0, H, lo, len);
+    }
+}
+
+// Rows, backward, zero-state exit states over the forward result.
+__global__ void __launch_bounds__(32) rows_partial_bwd_kernel(const __grid_constant__ OpticPass P) {
+    const int job = blockIdx.z, seg = blockIdx.y;
+    const OpticJob& J = P.job[job];
+    const int W = P.width, H = P.height;
+    if (seg >= seg_count(W) - 1) return;
+    __shared__ float tile[32][kTileCols + 1];
+    int lo, hi;
+    bwd_seg(W, seg, lo, hi);
+    const int len = hi - lo;
+    const int row0 = blockIdx.x * 32, y = row0 + threadIdx.x;
+    for (int gi = 0; gi < J.count; ++gi) {
+        const OpticGauss& g = J.g[gi];
+        if (!is_yvv(g.kind)) continue;
+        load_rows(tile, J.temp[gi], W, row0, H, lo, len);
+        if (y < H) {
+            YvvState st{0.0f, 0.0f, 0.0f};
+            for (int c = len - 1; c >= 0; --c) yvv_step(g, tile[threadIdx.x][c], st);
+            store_exit(carry_at(P, job, gi, y, seg), st);
         }
+        __syncwarp();
+    }
+}
+
+// Rows, backward, final values in place.
+__global__ void __launch_bounds__(32) rows_final_bwd_kernel(const __grid_constant__ OpticPass P) {
+    const int job = blockIdx.z, seg = blockIdx.y;
+    const OpticJob& J = P.job[job];
+    const int W = P.width, H = P.height;
+    if (seg >= seg_count(W)) return;
+    __shared__ float tile[32][kTileCols + 1];
+    int lo, hi;
+    bwd_seg(W, seg, lo, hi);
+    const int len = hi - lo;
+    const int row0 = blockIdx.x * 32, y = row0 + threadIdx.x;
+    for (int gi = 0; gi < J.count; ++gi) {
+        const OpticGauss& g = J.g[gi];
+        if (!is_yvv(g.kind)) continue;
+        load_rows(tile, J.temp[gi], W, row0, H, lo, len);
+        if (y < H) {
+            YvvState st = entry_state(g, P, job, gi, y, seg, P.edge_a[edge_at(P, job, gi, y)]);
+            for (int c = len - 1; c >= 0; --c) tile[threadIdx.x][c] = yvv_step(g, tile[threadIdx.x][c], st);
+        }
+        store_rows(tile, J.temp[gi], W, row0, H, lo, len);
     }
 }
 
@@ -138,54 +258,96 @@ __global__ void rows_fir_kernel(const __grid_constant__ OpticPass P) {
 }
 
 // ---------------------------------------------------------------------------
-// Column pass + combination. One thread per column: the recursive Gaussians first
-// run bottom-up in place (the reference's anticausal-first column order), then a
-// single top-down sweep produces every Gaussian's final value at (x, y) and the
-// epilogue combines them with the source plane.
+// Columns: the recursive Gaussians run bottom-up first (the reference's
+// anticausal-first column order) in place over the row-filtered planes, then top-down
+// fused with the combination: each thread owns one column segment and evaluates every
+// Gaussian at each of its pixels, then applies the scatter/bounce combination.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float column_value(const OpticJob& J, int gi, const OpticPass& P, int x, int y,
-                                              YvvState& st, float tval) {
-    const OpticGauss& g = J.g[gi];
-    if (g.kind == kGaussIdentity) return J.src[(long long)y * J.stride + x];
-    if (g.kind == kGaussFir) {
+__global__ void __launch_bounds__(kColThreads) cols_partial_up_kernel(const __grid_constant__ OpticPass P) {
+    const int job = blockIdx.z, seg = blockIdx.y;
+    const OpticJob& J = P.job[job];
+    const int W = P.width, H = P.height;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= W || seg >= seg_count(H)) return;
+    int lo, hi;
+    bwd_seg(H, seg, lo, hi);
+    for (int gi = 0; gi < J.count; ++gi) {
+        const OpticGauss& g = J.g[gi];
+        if (!is_yvv(g.kind)) continue;
         const float* T = J.temp[gi];
-        float sum = 0.0f;
-        for (int o = -g.radius; o <= g.radius; ++o)
-            sum += T[(long long)reflect_half(y - o, P.height) * P.width + x] * g.w[o + g.radius];
-        return sum;
+        if (seg == 0) P.edge_a[edge_at(P, job, gi, x)] = T[(long long)(H - 1) * W + x];
+        if (seg == seg_count(H) - 1) continue;
+        YvvState st{0.0f, 0.0f, 0.0f};
+        for (int y = hi - 1; y >= lo; --y) yvv_step(g, T[(long long)y * W + x], st);
+        store_exit(carry_at(P, job, gi, x, seg), st);
     }
-    return yvv_step(g, tval, st);
 }
 
-__global__ void __launch_bounds__(kColThreads) columns_combine_kernel(const __grid_constant__ OpticPass P) {
-    const OpticJob& J = P.job[blockIdx.y];
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kColThreads) cols_final_up_kernel(const __grid_constant__ OpticPass P) {
+    const int job = blockIdx.z, seg = blockIdx.y;
+    const OpticJob& J = P.job[job];
     const int W = P.width, H = P.height;
-    if (x >= W) return;
-    // bottom-up pass of every recursive Gaussian, in place
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= W || seg >= seg_count(H)) return;
+    int lo, hi;
+    bwd_seg(H, seg, lo, hi);
     for (int gi = 0; gi < J.count; ++gi) {
         const OpticGauss& g = J.g[gi];
         if (!is_yvv(g.kind)) continue;
         float* T = J.temp[gi];
-        YvvState st;
-        yvv_init(g, T[(long long)(H - 1) * W + x], st);
-        for (int r0 = H - 1; r0 >= 0; r0 -= kPrefetch) {
-            float v[kPrefetch];
-#pragma unroll
-            for (int r = 0; r < kPrefetch; ++r) v[r] = (r0 - r >= 0) ? T[(long long)(r0 - r) * W + x] : 0.0f;
-#pragma unroll
-            for (int r = 0; r < kPrefetch; ++r)
-                if (r0 - r >= 0) T[(long long)(r0 - r) * W + x] = yvv_step(g, v[r], st);
+        YvvState st = entry_state(g, P, job, gi, x, seg, P.edge_a[edge_at(P, job, gi, x)]);
+        for (int y = hi - 1; y >= lo; --y) {
+            const long long i = (long long)y * W + x;
+            T[i] = yvv_step(g, T[i], st);
         }
+        if (lo == 0) P.edge_b[edge_at(P, job, gi, x)] = T[x];
     }
+}
+
+__global__ void __launch_bounds__(kColThreads) cols_partial_down_kernel(const __grid_constant__ OpticPass P) {
+    const int job = blockIdx.z, seg = blockIdx.y;
+    const OpticJob& J = P.job[job];
+    const int W = P.width, H = P.height;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= W || seg >= seg_count(H) - 1) return;
+    int lo, hi;
+    fwd_seg(H, seg, lo, hi);
+    for (int gi = 0; gi < J.count; ++gi) {
+        const OpticGauss& g = J.g[gi];
+        if (!is_yvv(g.kind)) continue;
+        const float* T = J.temp[gi];
+        YvvState st{0.0f, 0.0f, 0.0f};
+        for (int y = lo; y < hi; ++y) yvv_step(g, T[(long long)y * W + x], st);
+        store_exit(carry_at(P, job, gi, x, seg), st);
+    }
+}
+
+__global__ void __launch_bounds__(kColThreads) cols_final_combine_kernel(const __grid_constant__ OpticPass P) {
+    const int job = blockIdx.z, seg = blockIdx.y;
+    const OpticJob& J = P.job[job];
+    const int W = P.width, H = P.height;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= W || seg >= seg_count(H)) return;
+    int lo, hi;
+    fwd_seg(H, seg, lo, hi);
     YvvState st[kOpticMaxGauss];
     for (int gi = 0; gi < J.count; ++gi)
-        if (is_yvv(J.g[gi].kind)) yvv_init(J.g[gi], J.temp[gi][x], st[gi]);
-    for (int y = 0; y < H; ++y) {
+        if (is_yvv(J.g[gi].kind)) st[gi] = entry_state(J.g[gi], P, job, gi, x, seg, P.edge_b[edge_at(P, job, gi, x)]);
+    for (int y = lo; y < hi; ++y) {
         float v[kOpticMaxGauss];
         for (int gi = 0; gi < J.count; ++gi) {
-            const float t = is_yvv(J.g[gi].kind) ? J.temp[gi][(long long)y * W + x] : 0.0f;
-            v[gi] = column_value(J, gi, P, x, y, st[gi], t);
+            const OpticGauss& g = J.g[gi];
+            if (g.kind == kGaussIdentity) {
+                v[gi] = J.src[(long long)y * J.stride + x];
+            } else if (g.kind == kGaussFir) {
+                const float* T = J.temp[gi];
+                float sum = 0.0f;
+                for (int o = -g.radius; o <= g.radius; ++o)
+                    sum += T[(long long)reflect_half(y - o, H) * W + x] * g.w[o + g.radius];
+                v[gi] = sum;
+            } else {
+                v[gi] = yvv_step(g, J.temp[gi][(long long)y * W + x], st[gi]);
+            }
         }
         float* dst = J.src + (long long)y * J.stride + x;
         const float source = *dst;
@@ -221,18 +383,39 @@ cudaError_t launch_optic_pass(const OpticPass& P, cudaStream_t stream) {
             anyYvv |= is_yvv(P.job[j].g[g].kind);
             anyFir |= P.job[j].g[g].kind == kGaussFir;
         }
+    const int W = P.width, H = P.height;
+    const int sw = W / kSeg > 1 ? W / kSeg : 1, sh = H / kSeg > 1 ? H / kSeg : 1;
+    const dim3 rows_grid((H + 31) / 32, sw, P.jobs);
+    const dim3 cols_grid((W + kColThreads - 1) / kColThreads, sh, P.jobs);
+    cudaError_t e = cudaSuccess;
     if (anyYvv) {
-        rows_yvv_kernel<<<dim3((P.height + kTile - 1) / kTile, P.jobs), kTile, 0, stream>>>(P);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
+        fjb::count_launch();
+        rows_partial_fwd_kernel<<<rows_grid, 32, 0, stream>>>(P);
+        fjb::count_launch();
+        rows_final_fwd_kernel<<<rows_grid, 32, 0, stream>>>(P);
+        fjb::count_launch();
+        rows_partial_bwd_kernel<<<rows_grid, 32, 0, stream>>>(P);
+        fjb::count_launch();
+        rows_final_bwd_kernel<<<rows_grid, 32, 0, stream>>>(P);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (anyFir) {
         const dim3 block(32, 8);
-        rows_fir_kernel<<<dim3((P.width + 31) / 32, (P.height + 7) / 8, P.jobs), block, 0, stream>>>(P);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
+        fjb::count_launch();
+        rows_fir_kernel<<<dim3((W + 31) / 32, (H + 7) / 8, P.jobs), block, 0, stream>>>(P);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    columns_combine_kernel<<<dim3((P.width + kColThreads - 1) / kColThreads, P.jobs), kColThreads, 0, stream>>>(P);
+    if (anyYvv) {
+        fjb::count_launch();
+        cols_partial_up_kernel<<<cols_grid, kColThreads, 0, stream>>>(P);
+        fjb::count_launch();
+        cols_final_up_kernel<<<cols_grid, kColThreads, 0, stream>>>(P);
+        fjb::count_launch();
+        cols_partial_down_kernel<<<cols_grid, kColThreads, 0, stream>>>(P);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    fjb::count_launch();
+    cols_final_combine_kernel<<<cols_grid, kColThreads, 0, stream>>>(P);
     return cudaGetLastError();
 }
 

@@ -16,11 +16,14 @@ enum GaussKind : int { kGaussIdentity = 0, kGaussFir = 1, kGaussYvv = 2, kGaussY
 constexpr int kOpticMaxGauss = 5;
 constexpr int kOpticMaxFirRadius = 9;
 
+constexpr int kOpticSeg = 64; // segment length of the block-parallel recursions
+
 struct OpticGauss {
     int kind;
     int radius;   // FIR only
     float w[19];  // FIR weights, w[radius] is the centre tap
     float yvv[4]; // legacy: B, B1, B2, B3; factored: h, g, t, 0
+    double seg[9]; // recursive kinds: the state map over kOpticSeg zero-input steps (row-major 3x3)
 };
 
 enum OpticMode : int { kOpticScatter = 0, kOpticBounce = 1 };
@@ -43,6 +46,12 @@ struct OpticJob {
 struct OpticPass {
     int width, height, jobs;
     OpticJob job[3];
+    // block-parallel recursion buffers: 3 floats of segment state per (job, Gaussian,
+    // line, segment) and two per-line edge values per (job, Gaussian, line)
+    float* carry;
+    float* edge_a;
+    float* edge_b;
+    int lines_max, segs_max;
 };
 
 cudaError_t launch_optic_pass(const OpticPass& P, cudaStream_t stream);

@@ -16,6 +16,8 @@ namespace fjb {
 
 namespace {
 
+void segment_map(OpticGauss& g);
+
 const float kTailAmplitudes[3] = {0.1633f, 0.6496f, 0.1870f};
 
 bool decode_gauss(const FjHalationGaussian& s, OpticGauss& g) {
@@ -44,13 +46,50 @@ bool decode_gauss(const FjHalationGaussian& s, OpticGauss& g) {
     g.radius = s.radius;
     std::memcpy(g.w, s.fir_weights, sizeof(g.w));
     std::memcpy(g.yvv, s.yvv, sizeof(g.yvv));
+    segment_map(g);
     return true;
 }
 
 } // namespace
 
+namespace {
+
+int segments(int n) { return n / kOpticSeg > 1 ? n / kOpticSeg : 1; }
+
+// The recursion's state map over kOpticSeg steps with zero input, in FP64: the
+// operator that carries a segment's entry state to its exit state.
+void segment_map(OpticGauss& g) {
+    double m[9] = {0};
+    if (g.kind == kGaussYvv) {
+        // (s1, s2, s3) -> (B1 s1 + B2 s2 + B3 s3, s1, s2)
+        const double m0[9] = {g.yvv[1], g.yvv[2], g.yvv[3], 1, 0, 0, 0, 1, 0};
+        std::memcpy(m, m0, sizeof(m));
+    } else if (g.kind == kGaussYvvFactored) {
+        // s1' = (1-h) s1; s3' = t s3 + g (s1' - s2); s2' = s2 + s3'
+        const double h = g.yvv[0], gg = g.yvv[1], t = g.yvv[2];
+        const double m0[9] = {1 - h, 0, 0, gg * (1 - h), 1 - gg, t, gg * (1 - h), -gg, t};
+        std::memcpy(m, m0, sizeof(m));
+    } else {
+        return;
+    }
+    double r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    for (int step = 0; step < kOpticSeg; ++step) {
+        double t[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) t[i * 3 + j] = m[i * 3] * r[j] + m[i * 3 + 1] * r[3 + j] + m[i * 3 + 2] * r[6 + j];
+        std::memcpy(r, t, sizeof(r));
+    }
+    std::memcpy(g.seg, r, sizeof(r));
+}
+
+} // namespace
+
 size_t halation_scratch_floats(int width, int height) {
-    return (size_t)3 * kOpticMaxGauss * (size_t)width * (size_t)height;
+    const size_t lines = (size_t)(width > height ? width : height);
+    const size_t segs = (size_t)(segments(width) > segments(height) ? segments(width) : segments(height));
+    return (size_t)3 * kOpticMaxGauss * (size_t)width * (size_t)height // row-filtered planes
+           + (size_t)3 * kOpticMaxGauss * lines * segs * 3               // segment states
+           + (size_t)2 * 3 * kOpticMaxGauss * lines;                     // edge values
 }
 
 bool scatter_halation(const FjScatterHalation& d, float* planes_rgb[3], long long stride, int width, int height,
@@ -65,6 +104,18 @@ bool scatter_halation(const FjScatterHalation& d, float* planes_rgb[3], long lon
     OpticPass bounce{};
     scatter.width = bounce.width = width;
     scatter.height = bounce.height = height;
+    {
+        const int lines = width > height ? width : height;
+        const int segs = segments(width) > segments(height) ? segments(width) : segments(height);
+        float* tail = scratch + (size_t)3 * kOpticMaxGauss * plane;
+        for (OpticPass* P : {&scatter, &bounce}) {
+            P->lines_max = lines;
+            P->segs_max = segs;
+            P->carry = tail;
+            P->edge_a = tail + (size_t)3 * kOpticMaxGauss * lines * segs * 3;
+            P->edge_b = P->edge_a + (size_t)3 * kOpticMaxGauss * lines;
+        }
+    }
     for (int c = 0; c < 3; ++c) {
         const FjHalationChannel& ch = d.channels[c];
         float* temps[kOpticMaxGauss];

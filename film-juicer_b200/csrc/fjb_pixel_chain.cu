@@ -15,6 +15,7 @@
 
 #include "fjb_internal.h"
 #include "fjb_pixel_math.cuh"
+#include "fjb_launches.h"
 
 namespace fjb {
 
@@ -158,6 +159,7 @@ static cudaError_t launch_variant(const PixelParams& p, int grid, size_t smem, c
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
+    fjb::count_launch();
     k<<<grid, kPixelThreads, smem, stream>>>(p);
     return cudaGetLastError();
 }
@@ -197,6 +199,7 @@ cudaError_t launch_camera_exposure(const PixelParams& p, float* b, float* g, flo
                                    cudaStream_t stream) {
     const long long total = (long long)p.width * (long long)p.height;
     if (total <= 0) return cudaSuccess;
+    fjb::count_launch();
     camera_exposure_kernel<<<persistent_grid(total), kPixelThreads, 0, stream>>>(p, b, g, r, stride);
     return cudaGetLastError();
 }

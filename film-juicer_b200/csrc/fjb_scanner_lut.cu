@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "fjb_internal.h"
+#include "fjb_launches.h"
 
 namespace fjb {
 
@@ -164,14 +165,18 @@ cudaError_t launch_scanner_lut_build(const ScannerLutSpec& spec, const ScannerLu
     const int r = spec.resolution;
     if (r < 2 || r > 64 || spec.k <= 0) return cudaErrorInvalidValue;
     const int nodes = r * r * r;
+    fjb::count_launch();
     scanner_nodes_kernel<<<(nodes + kLutThreads - 1) / kLutThreads, kLutThreads, 0, stream>>>(spec, out);
     const int lines = 3 * r * r * 3;
+    fjb::count_launch();
     scanner_slopes_kernel<<<(lines + kLutThreads - 1) / kLutThreads, kLutThreads, 0, stream>>>(
         r, out.nodes, out.slope_c, out.slope_m, out.slope_y);
     const int cells = (r - 1) * (r - 1) * (r - 1) * 3;
+    fjb::count_launch();
     scanner_cells_kernel<<<(cells + kLutThreads - 1) / kLutThreads, kLutThreads, 0, stream>>>(r, out.nodes,
                                                                                              out.cell_min, out.cell_max);
     const int packs = nodes * 3;
+    fjb::count_launch();
     scanner_pack_kernel<<<(packs + kLutThreads - 1) / kLutThreads, kLutThreads, 0, stream>>>(out, r);
     return cudaGetLastError();
 }

@@ -16,9 +16,12 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/juicer_b200.h"
 #include "../../include/juicer_cuda_api.h"
+#include "fjb_diffusion.h"
+#include "fjb_dir.h"
 #include "fjb_internal.h"
 #include "fjb_recipe.h"
 #include "fjb_schedule.h"
@@ -33,6 +36,19 @@ struct FjCuda {
     float* ae_scale = nullptr;               // device auto-exposure scale
     FjbNoise* noise = nullptr;               // device copy of the static grain noise
     uintptr_t noise_key[3] = {0, 0, 0};
+    fjb::DirPlan dir_plan;                   // spatial-DIR operator tables of the last frame geometry
+    uint64_t dir_key = 0;
+    float* diffusion_psf = nullptr;          // camera-diffusion PSF rows of the last descriptor
+    size_t diffusion_psf_bytes = 0;
+    uint64_t diffusion_key = 0;
+    int diffusion_taps = 0;
+    // optional per-stage device timing (CUDA events on the render stream)
+    bool timing = false;
+    bool timing_events = false;
+    cudaEvent_t stage_ev[2 * FJB_STAGE_COUNT] = {};
+    bool stage_open[FJB_STAGE_COUNT] = {};
+    double stage_ms[FJB_STAGE_COUNT] = {};
+    uint64_t stage_frames[FJB_STAGE_COUNT] = {};
 };
 
 namespace {
@@ -56,6 +72,8 @@ const char* pixel_address(const FjImage& im, int x, int y) {
 
 bool aborted(const FjAbortCallback& cb) { return cb.query && cb.query(cb.user) == FJ_ABORT_REQUESTED; }
 
+void stage_events_release(FjCuda* cuda);
+
 void release_all(FjCuda* cuda) {
     for (auto& kv : cuda->recipes) {
         kv.second->r.release();
@@ -69,6 +87,83 @@ void release_all(FjCuda* cuda) {
     cuda->ae_scale = nullptr;
     if (cuda->noise) fjb_noise_destroy(cuda->noise, nullptr);
     cuda->noise = nullptr;
+    cuda->dir_plan.release();
+    cuda->dir_key = 0;
+    if (cuda->diffusion_psf) cudaFree(cuda->diffusion_psf);
+    cuda->diffusion_psf = nullptr;
+    cuda->diffusion_psf_bytes = 0;
+    cuda->diffusion_key = 0;
+    stage_events_release(cuda);
+}
+
+void stage_begin(FjCuda* cuda, int stage, void* vs) {
+    if (!cuda->timing || !cuda->timing_events) return;
+    cudaEventRecord(cuda->stage_ev[2 * stage], reinterpret_cast<cudaStream_t>(vs));
+    cuda->stage_open[stage] = true;
+}
+
+void stage_end(FjCuda* cuda, int stage, void* vs) {
+    if (!cuda->timing || !cuda->timing_events || !cuda->stage_open[stage]) return;
+    cudaEventRecord(cuda->stage_ev[2 * stage + 1], reinterpret_cast<cudaStream_t>(vs));
+}
+
+// After the frame's stream has drained: fold the recorded stage intervals into the totals.
+void stage_collect(FjCuda* cuda) {
+    for (int s = 0; s < FJB_STAGE_COUNT; ++s) {
+        if (!cuda->stage_open[s]) continue;
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, cuda->stage_ev[2 * s], cuda->stage_ev[2 * s + 1]) == cudaSuccess) {
+            cuda->stage_ms[s] += ms;
+            cuda->stage_frames[s] += 1;
+        }
+        cuda->stage_open[s] = false;
+    }
+}
+
+void stage_events_release(FjCuda* cuda) {
+    if (!cuda->timing_events) return;
+    for (cudaEvent_t& e : cuda->stage_ev) {
+        if (e) cudaEventDestroy(e);
+        e = nullptr;
+    }
+    cuda->timing_events = false;
+}
+
+// FNV-1a over the bytes of individual fields: identities of descriptor contents for
+// the owner's caches (never of padding).
+struct Fnv {
+    uint64_t h = 0xcbf29ce484222325ULL;
+    template <typename T>
+    Fnv& add(const T& v) {
+        const unsigned char* b = reinterpret_cast<const unsigned char*>(&v);
+        for (size_t i = 0; i < sizeof(T); ++i) {
+            h ^= b[i];
+            h *= 0x100000001b3ULL;
+        }
+        return *this;
+    }
+};
+
+uint64_t diffusion_identity(const FjDiffusion& d) {
+    Fnv f;
+    f.add(d.family).add(d.scatter_fraction).add(d.warmth).add(d.spatial_scale).add(d.pixel_size_um).add(d.radius_px);
+    for (int i = 0; i < 3; ++i) f.add(d.group_weights[i]).add(d.group_lambda_um[i]);
+    return f.h | 1;
+}
+
+uint64_t spatial_dir_identity(const FjSpatialDir& sd, int width, int height) {
+    Fnv f;
+    f.add(width).add(height).add(sd.component_count);
+    for (const FjExtent* e : {&sd.render_extent, &sd.full_frame_extent, &sd.filter_domain_extent})
+        f.add(e->x).add(e->y).add(e->width).add(e->height);
+    for (size_t k = 0; k < sd.component_count && k < 4; ++k) {
+        const FjDirGaussian& g = sd.components[k];
+        f.add(g.sigma_px).add(g.weight).add(g.radius).add(g.reference_operator).add(g.feedforward);
+        for (int i = 0; i < 3; ++i) f.add(g.feedback[i]).add(g.feedback_numerators[i]);
+        f.add(g.normalization_denominator).add(g.feedforward_numerator).add(g.boundary_truncation_accuracy);
+        f.add(g.boundary_certification_tolerance).add(g.boundary_derivation_version);
+    }
+    return f.h | 1;
 }
 
 bool same_rect(const FjRect& a, const FjRect& b) { return a.x1 == b.x1 && a.y1 == b.y1 && a.x2 == b.x2 && a.y2 == b.y2; }
@@ -148,6 +243,7 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
     if (grain) scratch = std::max(scratch, fjb_visual_grain_scratch_bytes(width, height));
     const int planes = 3 + 3 + (spatial_dir ? 6 : 0);
     cudaError_t e = ensure_work(cuda, planes * plane_bytes + scratch + 256);
+    FjStatus st{};
     if (e != cudaSuccess) return fjb::cuda_status(e, error, "frame workspace");
     char* base = static_cast<char*>(cuda->work);
     auto P = [&](int i) { return reinterpret_cast<float*>(base + (size_t)i * plane_bytes); };
@@ -160,40 +256,99 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
     const ptrdiff_t stride = width;
     const FjOptics& o = h.optics;
 
-    FjStatus st = fjb_camera_exposure(recipe, src, srb, comps, width, height, carrier[0], carrier[1], carrier[2],
-                                      stride, vs, error);
+    stage_begin(cuda, FJB_STAGE_CAMERA_EXPOSURE, vs);
+    st = fjb_camera_exposure(recipe, src, srb, comps, width, height, carrier[0], carrier[1], carrier[2], stride, vs,
+                             error);
+    stage_end(cuda, FJB_STAGE_CAMERA_EXPOSURE, vs);
     if (st.category != FJ_STATUS_SUCCESS) return st;
     if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
     if (camera_diffusion) {
-        FjDiffusionComponents dc{};
-        st = fjb_diffusion_components_host(&o.camera, &dc, error);
-        if (st.category != FJ_STATUS_SUCCESS) return st;
+        const FjDiffusion& d = o.camera;
+        if (!(d.scatter_fraction >= 0.0 && d.scatter_fraction <= 1.0))
+            return fjb::fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "diffusion scatter fraction outside [0, 1]");
+        const uint64_t key = diffusion_identity(d);
+        if (key != cuda->diffusion_key || !cuda->diffusion_psf) {
+            // PSF rows are built once per distinct descriptor and kept on the device
+            FjDiffusionComponents dc{};
+            st = fjb_diffusion_components_host(&d, &dc, error);
+            if (st.category != FJ_STATUS_SUCCESS) return st;
+            const double* wts[3] = {dc.red_weights, dc.green_weights, dc.blue_weights};
+            std::vector<float> rows[3];
+            int taps = 0;
+            std::string why;
+            for (int c = 0; c < 3; ++c)
+                if (!fjb::diffusion_psf_rows(dc.lambda_px, wts[c], d.radius_px, rows[c], taps, why))
+                    return fjb::fail_status(FJ_STATUS_PREPARATION_FAILURE, error, why);
+            const size_t bytes = 3 * rows[0].size() * sizeof(float);
+            cuda->diffusion_key = 0;
+            if (cuda->diffusion_psf_bytes < bytes) {
+                if (cuda->diffusion_psf) cudaFree(cuda->diffusion_psf);
+                cuda->diffusion_psf = nullptr;
+                cuda->diffusion_psf_bytes = 0;
+                e = cudaMalloc(&cuda->diffusion_psf, bytes);
+                if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion PSF");
+                cuda->diffusion_psf_bytes = bytes;
+            }
+            for (int c = 0; c < 3 && e == cudaSuccess; ++c)
+                e = cudaMemcpy(cuda->diffusion_psf + c * rows[0].size(), rows[c].data(), rows[c].size() * sizeof(float),
+                               cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion PSF upload");
+            cuda->diffusion_key = key;
+            cuda->diffusion_taps = taps;
+        }
+        const size_t n = (size_t)(d.radius_px + 1) * (size_t)cuda->diffusion_taps;
+        const float* psf[3] = {cuda->diffusion_psf, cuda->diffusion_psf + n, cuda->diffusion_psf + 2 * n};
         // R, G, B planes into the density planes, which then carry the exposure
-        st = fjb_diffusion(&dc, o.camera.radius_px, o.camera.scatter_fraction, carrier[2], carrier[1], carrier[0],
-                           density[2], density[1], density[0], stride, width, height, vs, error);
-        if (st.category != FJ_STATUS_SUCCESS) return st;
+        float* ddst[3] = {density[2], density[1], density[0]};
+        const float* dsrc[3] = {carrier[2], carrier[1], carrier[0]};
+        stage_begin(cuda, FJB_STAGE_CAMERA_DIFFUSION, vs);
+        e = fjb::launch_diffusion(psf, d.radius_px, cuda->diffusion_taps, (float)d.scatter_fraction, ddst, dsrc, stride,
+                                  width, height, reinterpret_cast<cudaStream_t>(vs));
+        stage_end(cuda, FJB_STAGE_CAMERA_DIFFUSION, vs);
+        if (e != cudaSuccess) return fjb::cuda_status(e, error, "camera diffusion");
         std::swap(carrier[0], density[0]);
         std::swap(carrier[1], density[1]);
         std::swap(carrier[2], density[2]);
         if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
     }
     if (halation) {
+        stage_begin(cuda, FJB_STAGE_SCATTER_HALATION, vs);
         st = fjb_scatter_halation(&o.scatter_halation, carrier[2], carrier[1], carrier[0], stride, width, height,
                                   scratch_p, scratch, vs, error);
+        stage_end(cuda, FJB_STAGE_SCATTER_HALATION, vs);
         if (st.category != FJ_STATUS_SUCCESS) return st;
         if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
     }
     if (spatial_dir) {
-        st = fjb_spatial_dir_build(recipe, &h.spatial_dir, nullptr, 0, 3, carrier[0], carrier[1], carrier[2], stride,
-                                   width, height, dirp[0], dirp[1], dirp[2], dirp[3], dirp[4], dirp[5], scratch_p,
-                                   scratch, vs, error);
+        const uint64_t key = spatial_dir_identity(h.spatial_dir, width, height);
+        if (key != cuda->dir_key) {
+            // operator tables (taps, reflected boundaries) are built once per geometry
+            cuda->dir_plan.release();
+            cuda->dir_key = 0;
+            std::string why;
+            e = cudaSuccess;
+            if (!fjb::dir_plan_create(h.spatial_dir, width, height, reinterpret_cast<cudaStream_t>(vs), cuda->dir_plan,
+                                      why, e)) {
+                cuda->dir_plan.release();
+                if (e != cudaSuccess) return fjb::cuda_status(e, error, "spatial DIR plan");
+                return fjb::fail_status(FJ_STATUS_PREPARATION_FAILURE, error, why);
+            }
+            cuda->dir_key = key;
+        }
+        stage_begin(cuda, FJB_STAGE_SPATIAL_DIR, vs);
+        st = fjb::spatial_dir_apply(recipe, cuda->dir_plan, nullptr, 0, 3, carrier[0], carrier[1], carrier[2], stride,
+                                    width, height, dirp[0], dirp[1], dirp[2], dirp[3], dirp[4], dirp[5], scratch_p,
+                                    scratch, vs, error);
+        stage_end(cuda, FJB_STAGE_SPATIAL_DIR, vs);
         if (st.category == FJ_STATUS_SUCCESS)
             st = fjb_recipe_set_spatial_dir_planes(recipe, dirp[0], dirp[1], dirp[2], dirp[3], dirp[4], dirp[5], error);
         if (st.category != FJ_STATUS_SUCCESS) return st;
         if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
     }
+    stage_begin(cuda, FJB_STAGE_CAPTURE_DENSITY, vs);
     st = fjb_capture_density(recipe, nullptr, 0, 3, carrier[0], carrier[1], carrier[2], stride, width, height,
                              density[0], density[1], density[2], vs, error);
+    stage_end(cuda, FJB_STAGE_CAPTURE_DENSITY, vs);
     if (st.category != FJ_STATUS_SUCCESS) return st;
     if (grain) {
         const FjVisualGrain& g = h.grain;
@@ -202,13 +357,18 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
         const FjbNoise* noise = nullptr;
         st = ensure_noise(cuda, h.noise, vs, &noise, error);
         if (st.category != FJ_STATUS_SUCCESS) return st;
+        stage_begin(cuda, FJB_STAGE_GRAIN, vs);
         st = fjb_visual_grain(recipe, &g, noise, density[0], density[1], density[2], stride, width, height, scratch_p,
                               scratch, vs, error);
+        stage_end(cuda, FJB_STAGE_GRAIN, vs);
         if (st.category != FJ_STATUS_SUCCESS) return st;
         if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
     }
-    return fjb_render_from_density(recipe, density[0], density[1], density[2], comps == 4 ? src : nullptr, srb, dst,
-                                   drb, width, height, comps, vs, error);
+    stage_begin(cuda, FJB_STAGE_PRINT_SCAN_OUTPUT, vs);
+    st = fjb_render_from_density(recipe, density[0], density[1], density[2], comps == 4 ? src : nullptr, srb, dst, drb,
+                                 width, height, comps, vs, error);
+    stage_end(cuda, FJB_STAGE_PRINT_SCAN_OUTPUT, vs);
+    return st;
 }
 
 } // namespace
@@ -379,7 +539,9 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
                 return out;
             }
             const float* msrc = reinterpret_cast<const float*>(pixel_address(frame->source, ae.source_bounds.x1, ae.source_bounds.y1));
+            stage_begin(cuda, FJB_STAGE_AUTO_EXPOSURE, vs);
             st = fjb_auto_exposure(recipe, msrc, srb, comps, &ae, cuda->ae_scale, vs, error);
+            stage_end(cuda, FJB_STAGE_AUTO_EXPOSURE, vs);
             if (st.category == FJ_STATUS_SUCCESS) st = fjb_recipe_set_exposure_scale_device(recipe, cuda->ae_scale, error);
             if (st.category != FJ_STATUS_SUCCESS) {
                 out.status = st;
@@ -393,13 +555,16 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
         const bool grain = (prepared->grain.flags & FJ_GRAIN_ACTIVE) != 0;
         if (!camera_diffusion && !halation && !spatial_dir && !grain) {
             // Monolithic: one fused pass source -> output
+            stage_begin(cuda, FJB_STAGE_MONOLITHIC, vs);
             st = fjb_render_pixels(recipe, src, srb, dst, drb, width, height, comps, vs, error);
+            stage_end(cuda, FJB_STAGE_MONOLITHIC, vs);
         } else {
             st = render_staged(cuda, recipe, *prepared, src, srb, dst, drb, width, height, comps, vs, abort_callback,
                                camera_diffusion, halation, spatial_dir, grain, error);
         }
         if (st.category != FJ_STATUS_SUCCESS) {
             cudaStreamSynchronize(stream);
+            for (bool& o : cuda->stage_open) o = false;
             out.status = st;
             return out;
         }
@@ -409,6 +574,7 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
             out.status = st;
             return out;
         }
+        stage_collect(cuda);
         if (flags & (1u << 8)) out.flags |= FJ_RENDER_DEFERRED_DIR_ERROR;
         out.status = fjb::ok_status();
         fjb::write_error(error, (flags & 1u) ? "scanner stage reported non-finite pixels" : "");
@@ -434,6 +600,41 @@ FjStatus fj_cuda_shutdown(FjCuda* cuda, FjErrorBuffer* error) {
     if (!cuda->closed) {
         release_all(cuda);
         cuda->closed = true;
+    }
+    fjb::write_error(error, "");
+    return fjb::ok_status();
+}
+
+FjStatus fjb_owner_stage_timing(FjCuda* cuda, int32_t enable, FjErrorBuffer* error) {
+    if (!cuda) return fjb::fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null owner");
+    std::lock_guard<std::mutex> lock(cuda->gate);
+    if (cuda->closed) return fjb::fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "owner is shut down");
+    if (enable && !cuda->timing_events) {
+        for (cudaEvent_t& e : cuda->stage_ev) {
+            cudaError_t err = cudaEventCreate(&e);
+            if (err != cudaSuccess) {
+                stage_events_release(cuda);
+                return fjb::cuda_status(err, error, "stage timing events");
+            }
+        }
+        cuda->timing_events = true;
+    }
+    cuda->timing = enable != 0;
+    for (int s = 0; s < FJB_STAGE_COUNT; ++s) {
+        cuda->stage_ms[s] = 0.0;
+        cuda->stage_frames[s] = 0;
+        cuda->stage_open[s] = false;
+    }
+    fjb::write_error(error, "");
+    return fjb::ok_status();
+}
+
+FjStatus fjb_owner_stage_times(FjCuda* cuda, FjbStageTimes* out, FjErrorBuffer* error) {
+    if (!cuda || !out) return fjb::fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    std::lock_guard<std::mutex> lock(cuda->gate);
+    for (int s = 0; s < FJB_STAGE_COUNT; ++s) {
+        out->total_ms[s] = cuda->stage_ms[s];
+        out->frames[s] = cuda->stage_frames[s];
     }
     fjb::write_error(error, "");
     return fjb::ok_status();

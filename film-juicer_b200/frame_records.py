@@ -19,9 +19,12 @@ class FrameRecord:
     def __init__(self, recipe: "prepare.PreparedRecipe", width: int, height: int, *, recipe_hash: int = 0x5EED,
                  diffusion: bool = True, halation: bool = True, spatial_dir: bool = True, grain: bool = True,
                  auto_exposure: bool = False, noise: "grain_plan.Noise | None" = None,
-                 pixel_size_um: float | None = None, frame_time: float = 0.0):
+                 pixel_size_um: float | None = None, frame_time: float = 0.0, descriptor_width: int | None = None):
+        """descriptor_width: the frame width the pixel size and diffusion radius are
+        derived for (defaults to `width`; a crop of a larger frame passes the full width)."""
         self.width, self.height = width, height
-        self.pixel_size_um = pixel_size_um or 35000.0 / width
+        dw = descriptor_width or width
+        self.pixel_size_um = pixel_size_um or 35000.0 / dw
         self.host = prepare.HostRecord(recipe, recipe_hash=recipe_hash, auto_exposure=auto_exposure)
         h = self.host.h
         px = self.pixel_size_um
@@ -33,7 +36,7 @@ class FrameRecord:
         h.optics.full_frame.x, h.optics.full_frame.y = 0, 0
         h.optics.full_frame.width, h.optics.full_frame.height = width, height
         if diffusion:
-            h.optics.camera = descriptors.diffusion_record(px, width)
+            h.optics.camera = descriptors.diffusion_record(px, dw)
             flags |= abi.FJ_OPTICS_CAMERA_DIFFUSION
         if halation:
             h.optics.scatter_halation = prepare.scatter_halation_record(px)

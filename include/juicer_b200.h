@@ -195,6 +195,31 @@ FjStatus fjb_visual_grain(FjbRecipe* recipe, const FjVisualGrain* grain, const F
                           float* density_m, float* density_y, ptrdiff_t stride, int32_t width, int32_t height,
                           float* scratch, size_t scratch_bytes, void* stream, FjErrorBuffer* error);
 
+/* Per-stage device time of fj_cuda_render frames (CUDA events recorded on the render
+ * stream around each stage, read after the frame completes). Tracing aid; no
+ * counterpart in the reference. */
+#define FJB_STAGE_AUTO_EXPOSURE 0
+#define FJB_STAGE_CAMERA_EXPOSURE 1
+#define FJB_STAGE_CAMERA_DIFFUSION 2
+#define FJB_STAGE_SCATTER_HALATION 3
+#define FJB_STAGE_SPATIAL_DIR 4
+#define FJB_STAGE_CAPTURE_DENSITY 5
+#define FJB_STAGE_GRAIN 6
+#define FJB_STAGE_PRINT_SCAN_OUTPUT 7
+#define FJB_STAGE_MONOLITHIC 8
+#define FJB_STAGE_COUNT 9
+typedef struct FjbStageTimes {
+    double total_ms[FJB_STAGE_COUNT];
+    uint64_t frames[FJB_STAGE_COUNT];
+} FjbStageTimes;
+/* Turns stage timing on (enable != 0) or off and resets the totals. */
+FjStatus fjb_owner_stage_timing(FjCuda* cuda, int32_t enable, FjErrorBuffer* error);
+/* Totals since the last fjb_owner_stage_timing call. */
+FjStatus fjb_owner_stage_times(FjCuda* cuda, FjbStageTimes* out, FjErrorBuffer* error);
+
+/* Kernel launches this library has made in the process so far (all entry points). */
+uint64_t fjb_kernel_launches(void);
+
 /* Scanner LUT input record (reference native/juicer_cuda_frame_values.h FjScannerLutInput). */
 typedef struct FjbScannerLutInput {
     FjFloatSpan eps_c, eps_m, eps_y;

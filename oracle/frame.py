@@ -16,17 +16,18 @@ class _Components:
         self.lambda_px, self.red_weights, self.green_weights, self.blue_weights = lam, w[0], w[1], w[2]
 
 
-def render_frame(frame_record, recipe, src):
+def render_frame(frame_record, recipe, src, threads: int = 1):
     """frame_record: film_juicer_b200.frame_records.FrameRecord; recipe: the
     PreparedRecipe it was built from; src: (H, W, comps) float32. Returns the encoded
-    output (H, W, comps) and the error flags."""
+    output (H, W, comps) and the error flags. `threads` parallelises the per-pixel
+    stages (the spatial stages use the oracle's OpenMP default)."""
     abi = orc._abi()
     host = frame_record.host
     h = host.h
     scale = 1.0
     if h.film_exposure.flags & abi.FJ_FILM_AUTO_EXPOSURE:
         scale = orc.auto_exposure(host, h.auto_exposure, src)
-    carrier, _ = orc.render(host, src, stage=3, auto_scale=scale)  # B, G, R
+    carrier, _ = orc.render(host, src, stage=3, auto_scale=scale, threads=threads)  # B, G, R
     flags = h.optics.flags
     if flags & abi.FJ_OPTICS_CAMERA_DIFFUSION:
         d = h.optics.camera
@@ -43,11 +44,11 @@ def render_frame(frame_record, recipe, src):
                                                height=src.shape[0])
         density, _ = odir.develop_spatial(host, filtered, log_raw)
     else:
-        density, _ = orc.render(host, None, stage=5, planes=carrier)
+        density, _ = orc.render(host, None, stage=5, planes=carrier, threads=threads)
     if h.grain.flags & abi.FJ_GRAIN_ACTIVE:
         a = recipe.arrays
         layers = [[a["density_layers"][:, l, c] for c in range(3)] for l in range(3)]
         base = [a["density_rgb"][:, c] for c in range(3)]
         noise = frame_record.noise.record if frame_record.noise is not None else None
         density = ograin.visual_grain(h.grain, noise, base, layers, h.capture_polarity == 1, density)
-    return orc.render(host, src, stage=2, planes=density)
+    return orc.render(host, src, stage=2, planes=density, threads=threads)

@@ -1363,6 +1363,7 @@ int oracle_diffusion(const double* lambda_px, const double* weights /* [3][9] R,
             }
         for (size_t i = 0; i < (size_t)d * d; ++i) psf[i] = (float)((double)psf[i] / sum);
         const float f = (float)fraction;
+#pragma omp parallel for schedule(static)
         for (int y = 0; y < H; ++y)
             for (int x = 0; x < W; ++x) {
                 double acc = 0.0;
