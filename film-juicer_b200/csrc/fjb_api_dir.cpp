@@ -69,7 +69,7 @@ FjStatus spatial_dir_apply(FjbRecipe* recipe, const DirPlan& plan, const float* 
                 ((size_t)(3 + 3 * kDirMaxComponents) * plane * sizeof(float) + 255) / 256 * 256;
             char* rec = reinterpret_cast<char*>(scratch) + planes_bytes;
             bp.lines_max = width > height ? width : height;
-            const int sw = width / kDirSeg > 1 ? width / kDirSeg : 1, sh = height / kDirSeg > 1 ? height / kDirSeg : 1;
+            const int sw = dir_segments(width), sh = dir_segments(height);
             bp.segs_max = sw > sh ? sw : sh;
             bp.carry = reinterpret_cast<double*>(rec);
             bp.start = bp.carry + (size_t)3 * kDirMaxComponents * bp.lines_max * bp.segs_max * 3;

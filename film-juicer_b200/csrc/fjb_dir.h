@@ -67,6 +67,9 @@ struct DirBlurParams {
 // Bytes of the recursion buffers for a width x height frame.
 size_t dir_recursion_bytes(int width, int height);
 
+// Segments of the block-parallel recursions along a line of n samples.
+int dir_segments(int n);
+
 cudaError_t launch_dir_blur(const DirBlurParams& p, cudaStream_t stream);
 
 // Device-resident operator tables for one frame geometry.

@@ -6,12 +6,18 @@
 // end-block matrix (:478-780), rows left to right then right to left, columns from
 // the visual top (last memory row) down, then back up.
 //
-// B200 schedule: all components of all three correction planes are computed in two
-// launches plus one fused column launch: row FIR (thread per pixel, grid.z =
-// channel), row recursion (thread per row, grid.y = channel), and a column kernel
-// (thread per column, grid.y = channel) that runs every recursive component's
-// first column pass in place and then one final sweep that evaluates all components
-// at each pixel and writes the weighted sum once, so the reference's per-component
+// B200 schedule. The recursions are block-parallel: a line is cut into segments of
+// kDirSeg samples (the segment processed last in a direction is shorter, or absorbs
+// a remainder of fewer than 8 samples). A start kernel forms each line's reflected
+// start state with parallel dot products; a partial kernel runs every segment (the
+// first from the true start state, the others from a zero state) and keeps its exit
+// state; a scan kernel turns those into every segment's entry state (x_{j+1} =
+// M x_j + Z_j, M the recursion's state map over one segment); the final kernel runs
+// each segment again from its entry state. In exact arithmetic this is the sequential recursion; in FP64 it differs
+// from it by rounding. Row kernels stage 32 rows x one segment in shared memory so
+// global accesses stay coalesced; column kernels give each lane one column and load
+// rows ahead of the recursion. The last column pass evaluates every component at each
+// pixel and writes the weighted sum once, so the reference's per-component
 // read-modify-write accumulation never reaches HBM.
 #include <cuda_runtime.h>
 
@@ -23,6 +29,9 @@ namespace fjb {
 namespace {
 
 constexpr int kLineThreads = 128;
+constexpr int kSeg = kDirSeg;
+constexpr int kSegMax = kSeg + 8;  // longest segment: a remainder below 8 joins the last one
+constexpr int kAhead = 8;          // column kernels: rows loaded ahead of the recursion
 
 __device__ __forceinline__ int reflect_dir(int i, int n) {
     if (n <= 1) return 0;
@@ -32,53 +41,30 @@ __device__ __forceinline__ int reflect_dir(int i, int n) {
     return i >= n ? period - 1 - i : i;
 }
 
+// One step of the recursion; the newest state enters last so that the loop-carried
+// dependency is a single fused multiply-add.
 __device__ __forceinline__ double iir_step(const DirComponentDev& c, double x, double s[3]) {
-    const double v = c.ff * x + c.fb[0] * s[0] + c.fb[1] * s[1] + c.fb[2] * s[2];
+    const double v = fma(c.fb[0], s[0], fma(c.fb[1], s[1], fma(c.fb[2], s[2], c.ff * x)));
     s[2] = s[1];
     s[1] = s[0];
     s[0] = v;
     return v;
 }
 
-// Row FIR, FP64 accumulation, one thread per pixel.
-__global__ void dir_rows_fir_kernel(const __grid_constant__ DirBlurParams p) {
-    const int ch = blockIdx.z;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= p.width || y >= p.height) return;
-    const float* row = p.raw[ch] + (size_t)y * p.width;
-    for (int k = 0; k < p.count; ++k) {
-        const DirComponentDev& c = p.comp[k];
-        if (c.op != kDirOpFir) continue;
-        double sum = 0.0;
-        for (int o = -c.radius; o <= c.radius; ++o)
-            sum += (double)row[reflect_dir(x + o, p.width)] * (double)c.taps[o + c.radius];
-        p.temp[ch][k][(size_t)y * p.width + x] = isfinite(sum) ? (float)sum : 0.0f;
-    }
+__host__ __device__ __forceinline__ int seg_count(int n) {
+    if (n <= 0) return 0;
+    const int full = n / kSeg, rem = n % kSeg;
+    const int ns = full + (rem >= 8 ? 1 : 0);
+    return ns > 0 ? ns : 1;
 }
 
-// ---------------------------------------------------------------------------
-// Recursive components, block-parallel in FP64. Lines are cut into segments of
-// kDirSeg samples (the segment processed last in a direction absorbs the remainder).
-// The partial kernels run every segment but the first from a zero state and keep its
-// exit state; the first segment starts from the line's true start state (reflected
-// start weights, or the end block) and keeps its true exit state. The final kernels
-// rebuild each segment's entry state from those (x_{j+1} = M x_j + Z_j, M the
-// recursion's state map over one segment) and run the segment again. In exact
-// arithmetic this is the sequential recursion; in FP64 it differs from it by
-// rounding. Row kernels stage 32 rows x one segment in shared memory for coalesced
-// access; column kernels give each lane one column.
-// ---------------------------------------------------------------------------
-constexpr int kSeg = kDirSeg;
-constexpr int kTileCols = 2 * kSeg;
-
-__device__ __forceinline__ int seg_count(int n) { return n / kSeg > 1 ? n / kSeg : 1; }
-
+// forward segment b: [b*kSeg, ...), the last one running to n
 __device__ __forceinline__ void fwd_seg(int n, int b, int& lo, int& hi) {
     lo = b * kSeg;
     hi = b == seg_count(n) - 1 ? n : lo + kSeg;
 }
 
+// backward segment b (b-th from the end), the last one starting at 0
 __device__ __forceinline__ void bwd_seg(int n, int b, int& lo, int& hi) {
     hi = n - b * kSeg;
     lo = b == seg_count(n) - 1 ? 0 : hi - kSeg;
@@ -88,37 +74,86 @@ __device__ __forceinline__ double* carry_at(const DirBlurParams& p, int ch, int 
     return p.carry + ((((size_t)ch * kDirMaxComponents + k) * p.lines_max + line) * p.segs_max + seg) * 3;
 }
 
+// Start record per (channel, component, line): [0..2] the second pass's start state,
+// [3..5] the first pass's reflected start state, [6..8] the column end block.
 __device__ __forceinline__ double* start_at(const DirBlurParams& p, int ch, int k, int line) {
     return p.start + (((size_t)ch * kDirMaxComponents + k) * p.lines_max + line) * 9;
 }
 
-// Entry state of segment seg >= 1: the first segment's true exit, then the map.
-__device__ __forceinline__ void scan_entry(const DirComponentDev& c, const DirBlurParams& p, int ch, int k, int line,
-                                           int seg, double s[3]) {
-    const double* z0 = carry_at(p, ch, k, line, 0);
-    s[0] = z0[0];
-    s[1] = z0[1];
-    s[2] = z0[2];
-    for (int i = 1; i < seg; ++i) {
-        const double* z = carry_at(p, ch, k, line, i);
-        const double a = c.seg[0] * s[0] + c.seg[1] * s[1] + c.seg[2] * s[2] + z[0];
-        const double b = c.seg[3] * s[0] + c.seg[4] * s[1] + c.seg[5] * s[2] + z[1];
-        const double d = c.seg[6] * s[0] + c.seg[7] * s[1] + c.seg[8] * s[2] + z[2];
-        s[0] = a;
-        s[1] = b;
-        s[2] = d;
-    }
+__device__ __forceinline__ void put3(double* d, const double s[3]) {
+    d[0] = s[0];
+    d[1] = s[1];
+    d[2] = s[2];
 }
 
-// Reflected start state from the first `len` samples (the line reads forward from
-// `at(0)`): anchor + sum_i w_h[i] (x_i - anchor).
-template <typename At>
-__device__ __forceinline__ void reflected_start(const double* w, int len, At at, double s[3]) {
-    const double anchor = (double)at(0);
-    s[0] = s[1] = s[2] = anchor;
-    for (int i = 0; i < len; ++i) {
-        const double d = (double)at(i) - anchor;
-        for (int h = 0; h < 3; ++h) s[h] += w[h * len + i] * d;
+__device__ __forceinline__ void get3(const double* d, double s[3]) {
+    s[0] = d[0];
+    s[1] = d[1];
+    s[2] = d[2];
+}
+
+// Entry state of segment seg >= 1, left in the carry slot by the scan kernel.
+__device__ __forceinline__ void scan_entry(const DirComponentDev&, const DirBlurParams& p, int ch, int k, int line,
+                                           int seg, double s[3]) {
+    get3(carry_at(p, ch, k, line, seg), s);
+}
+
+enum DirPassKind : int { kRowsFwd = 0, kRowsBwd = 1, kColsA = 2, kColsB = 3 };
+
+// Carry scan of one pass: turns the exit states (segment 0's true, the others from a
+// zero state) into every segment's entry state, in place: entry_1 = exit_0,
+// entry_{j+1} = M entry_j + Z_j. One thread per (line, component).
+__global__ void __launch_bounds__(kLineThreads) dir_scan_kernel(const __grid_constant__ DirBlurParams p, int pass) {
+    const int ch = blockIdx.y;
+    const int line = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool rows = pass == kRowsFwd || pass == kRowsBwd;
+    if (line >= (rows ? p.height : p.width)) return;
+    for (int k = 0; k < p.count; ++k) {
+        const DirComponentDev& c = p.comp[k];
+        if (c.op != kDirOpYvv) continue;
+        const int n = pass == kRowsFwd ? p.width : pass == kRowsBwd ? p.width - c.h_tsize : p.height;
+        const int ns = seg_count(n);
+        if (ns < 2) continue;
+        double s[3];
+        get3(carry_at(p, ch, k, line, 0), s);
+        // exit states are loaded a batch ahead of the dependent chain and the entry
+        // stores (the loads cannot pass the stores to the same buffer otherwise)
+        constexpr int B = 8;
+        double nz[B][3];
+        auto load_batch = [&](int j0) {
+#pragma unroll
+            for (int t = 0; t < B; ++t) {
+                const int j = j0 + t;
+                if (j < ns - 1) {
+                    get3(carry_at(p, ch, k, line, j), nz[t]);
+                } else {
+                    nz[t][0] = nz[t][1] = nz[t][2] = 0.0; // the last segment keeps no exit state
+                }
+            }
+        };
+        load_batch(1);
+        for (int j0 = 1; j0 < ns; j0 += B) {
+            double z[B][3];
+#pragma unroll
+            for (int t = 0; t < B; ++t) {
+                z[t][0] = nz[t][0];
+                z[t][1] = nz[t][1];
+                z[t][2] = nz[t][2];
+            }
+            if (j0 + B < ns) load_batch(j0 + B);
+#pragma unroll
+            for (int t = 0; t < B; ++t) {
+                const int j = j0 + t;
+                if (j >= ns) break;
+                put3(carry_at(p, ch, k, line, j), s);
+                const double a = c.seg[0] * s[0] + c.seg[1] * s[1] + c.seg[2] * s[2] + z[t][0];
+                const double b = c.seg[3] * s[0] + c.seg[4] * s[1] + c.seg[5] * s[2] + z[t][1];
+                const double d = c.seg[6] * s[0] + c.seg[7] * s[1] + c.seg[8] * s[2] + z[t][2];
+                s[0] = a;
+                s[1] = b;
+                s[2] = d;
+            }
+        }
     }
 }
 
@@ -132,7 +167,7 @@ __device__ __forceinline__ void end_block(const double* T, int ts, const double 
     }
 }
 
-__device__ __forceinline__ void load_rows(float (*tile)[kTileCols + 1], const float* src, int W, int row0, int H,
+__device__ __forceinline__ void load_rows(float (*tile)[kSegMax + 1], const float* src, int W, int row0, int H,
                                           int lo, int len) {
     for (int r = 0; r < 32; ++r) {
         const int y = row0 + r;
@@ -141,7 +176,7 @@ __device__ __forceinline__ void load_rows(float (*tile)[kTileCols + 1], const fl
     __syncwarp();
 }
 
-__device__ __forceinline__ void store_rows(float (*tile)[kTileCols + 1], float* dst, int W, int row0, int H, int lo,
+__device__ __forceinline__ void store_rows(float (*tile)[kSegMax + 1], float* dst, int W, int row0, int H, int lo,
                                            int len) {
     __syncwarp();
     for (int r = 0; r < 32; ++r) {
@@ -152,29 +187,78 @@ __device__ __forceinline__ void store_rows(float (*tile)[kTileCols + 1], float* 
     __syncwarp();
 }
 
+// Row FIR, FP64 accumulation, one thread per pixel.
+__global__ void dir_rows_fir_kernel(const __grid_constant__ DirBlurParams p) {
+    const int ch = blockIdx.z;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= p.width || y >= p.height) return;
+    const float* row = p.raw[ch] + (size_t)y * p.width;
+    for (int k = 0; k < p.count; ++k) {
+        const DirComponentDev& c = p.comp[k];
+        if (c.op != kDirOpFir) continue;
+        double sum = 0.0;
+        if (x - c.radius >= 0 && x + c.radius < p.width) {
+            for (int o = -c.radius; o <= c.radius; ++o) sum += (double)row[x + o] * (double)c.taps[o + c.radius];
+        } else {
+            for (int o = -c.radius; o <= c.radius; ++o)
+                sum += (double)row[reflect_dir(x + o, p.width)] * (double)c.taps[o + c.radius];
+        }
+        p.temp[ch][k][(size_t)y * p.width + x] = isfinite(sum) ? (float)sum : 0.0f;
+    }
+}
+
+// Reflected start states of the rows: anchor + sum_i w_h[i] (x_i - anchor), one warp
+// per row, lanes striding the row, FP64 warp reduction.
+__global__ void __launch_bounds__(256) dir_row_starts_kernel(const __grid_constant__ DirBlurParams p) {
+    const int ch = blockIdx.y;
+    const int y = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (y >= p.height) return;
+    const float* line = p.raw[ch] + (size_t)y * p.width;
+    const double anchor = (double)line[0];
+    for (int k = 0; k < p.count; ++k) {
+        const DirComponentDev& c = p.comp[k];
+        if (c.op != kDirOpYvv) continue;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int i = lane; i < c.h_len; i += 32) {
+            const double d = (double)line[i] - anchor;
+            a0 += c.h_init[i] * d;
+            a1 += c.h_init[c.h_len + i] * d;
+            a2 += c.h_init[2 * c.h_len + i] * d;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+        if (lane == 0) {
+            double* st = start_at(p, ch, k, y) + 3;
+            st[0] = anchor + a0;
+            st[1] = anchor + a1;
+            st[2] = anchor + a2;
+        }
+    }
+}
+
 // Rows, left to right: exit states (segment 0 from the reflected start).
 __global__ void __launch_bounds__(32) dir_rows_partial_fwd_kernel(const __grid_constant__ DirBlurParams p) {
     const int ch = blockIdx.z, seg = blockIdx.y;
     const int W = p.width, H = p.height;
-    if (seg >= seg_count(W) - 1) return;
-    __shared__ float tile[32][kTileCols + 1];
+    if (seg >= seg_count(W) - 1) return; // the last segment's exit state is never used
+    __shared__ float tile[32][kSegMax + 1];
     int lo, hi;
     fwd_seg(W, seg, lo, hi);
     const int row0 = blockIdx.x * 32, y = row0 + threadIdx.x;
-    const float* raw = p.raw[ch];
-    load_rows(tile, raw, W, row0, H, lo, hi - lo);
+    load_rows(tile, p.raw[ch], W, row0, H, lo, hi - lo);
     if (y >= H) return;
-    const float* line = raw + (size_t)y * W;
     for (int k = 0; k < p.count; ++k) {
         const DirComponentDev& c = p.comp[k];
         if (c.op != kDirOpYvv) continue;
         double s[3] = {0.0, 0.0, 0.0};
-        if (seg == 0) reflected_start(c.h_init, c.h_len, [&](int i) { return line[i]; }, s);
+        if (seg == 0) get3(start_at(p, ch, k, y) + 3, s);
         for (int x = 0; x < hi - lo; ++x) iir_step(c, (double)tile[threadIdx.x][x], s);
-        double* z = carry_at(p, ch, k, y, seg);
-        z[0] = s[0];
-        z[1] = s[1];
-        z[2] = s[2];
+        put3(carry_at(p, ch, k, y, seg), s);
     }
 }
 
@@ -183,36 +267,33 @@ __global__ void __launch_bounds__(32) dir_rows_partial_fwd_kernel(const __grid_c
 __global__ void __launch_bounds__(32) dir_rows_final_fwd_kernel(const __grid_constant__ DirBlurParams p) {
     const int ch = blockIdx.z, seg = blockIdx.y;
     const int W = p.width, H = p.height;
-    __shared__ float in[32][kTileCols + 1];
-    __shared__ float out[32][kTileCols + 1];
+    __shared__ float tile[32][kSegMax + 1];
     int lo, hi;
     fwd_seg(W, seg, lo, hi);
     const int len = hi - lo;
     const int row0 = blockIdx.x * 32, y = row0 + threadIdx.x;
-    const float* raw = p.raw[ch];
-    load_rows(in, raw, W, row0, H, lo, len);
     for (int k = 0; k < p.count; ++k) {
         const DirComponentDev& c = p.comp[k];
         if (c.op != kDirOpYvv) continue;
+        load_rows(tile, p.raw[ch], W, row0, H, lo, len);
         if (y < H) {
-            const float* line = raw + (size_t)y * W;
             double s[3];
             if (seg == 0)
-                reflected_start(c.h_init, c.h_len, [&](int i) { return line[i]; }, s);
+                get3(start_at(p, ch, k, y) + 3, s);
             else
                 scan_entry(c, p, ch, k, y, seg, s);
-            for (int x = 0; x < len; ++x) out[threadIdx.x][x] = (float)iir_step(c, (double)in[threadIdx.x][x], s);
+            for (int x = 0; x < len; ++x) tile[threadIdx.x][x] = (float)iir_step(c, (double)tile[threadIdx.x][x], s);
             if (seg == seg_count(W) - 1) {
                 const int ts = c.h_tsize;
                 double term[3] = {0.0, 0.0, 0.0};
                 end_block(c.h_term, ts, s, term);
                 for (int r = 0; r < ts; ++r)
-                    if (len - ts + r >= 0) out[threadIdx.x][len - ts + r] = (float)term[r];
+                    if (len - ts + r >= 0) tile[threadIdx.x][len - ts + r] = (float)term[r];
                 double* st = start_at(p, ch, k, y);
                 for (int h = 0; h < 3; ++h) st[h] = h < ts ? term[h] : s[h];
             }
         }
-        store_rows(out, p.temp[ch][k], W, row0, H, lo, len);
+        store_rows(tile, p.temp[ch][k], W, row0, H, lo, len);
     }
 }
 
@@ -220,7 +301,7 @@ __global__ void __launch_bounds__(32) dir_rows_final_fwd_kernel(const __grid_con
 __global__ void __launch_bounds__(32) dir_rows_partial_bwd_kernel(const __grid_constant__ DirBlurParams p) {
     const int ch = blockIdx.z, seg = blockIdx.y;
     const int W = p.width, H = p.height;
-    __shared__ float tile[32][kTileCols + 1];
+    __shared__ float tile[32][kSegMax + 1];
     const int row0 = blockIdx.x * 32, y = row0 + threadIdx.x;
     for (int k = 0; k < p.count; ++k) {
         const DirComponentDev& c = p.comp[k];
@@ -232,17 +313,9 @@ __global__ void __launch_bounds__(32) dir_rows_partial_bwd_kernel(const __grid_c
         load_rows(tile, p.temp[ch][k], W, row0, H, lo, hi - lo);
         if (y < H) {
             double s[3] = {0.0, 0.0, 0.0};
-            if (seg == 0) {
-                const double* st = start_at(p, ch, k, y);
-                s[0] = st[0];
-                s[1] = st[1];
-                s[2] = st[2];
-            }
+            if (seg == 0) get3(start_at(p, ch, k, y), s);
             for (int x = hi - lo - 1; x >= 0; --x) iir_step(c, (double)tile[threadIdx.x][x], s);
-            double* z = carry_at(p, ch, k, y, seg);
-            z[0] = s[0];
-            z[1] = s[1];
-            z[2] = s[2];
+            put3(carry_at(p, ch, k, y, seg), s);
         }
         __syncwarp();
     }
@@ -252,7 +325,7 @@ __global__ void __launch_bounds__(32) dir_rows_partial_bwd_kernel(const __grid_c
 __global__ void __launch_bounds__(32) dir_rows_final_bwd_kernel(const __grid_constant__ DirBlurParams p) {
     const int ch = blockIdx.z, seg = blockIdx.y;
     const int W = p.width, H = p.height;
-    __shared__ float tile[32][kTileCols + 1];
+    __shared__ float tile[32][kSegMax + 1];
     const int row0 = blockIdx.x * 32, y = row0 + threadIdx.x;
     for (int k = 0; k < p.count; ++k) {
         const DirComponentDev& c = p.comp[k];
@@ -264,14 +337,10 @@ __global__ void __launch_bounds__(32) dir_rows_final_bwd_kernel(const __grid_con
         load_rows(tile, p.temp[ch][k], W, row0, H, lo, hi - lo);
         if (y < H) {
             double s[3];
-            if (seg == 0) {
-                const double* st = start_at(p, ch, k, y);
-                s[0] = st[0];
-                s[1] = st[1];
-                s[2] = st[2];
-            } else {
+            if (seg == 0)
+                get3(start_at(p, ch, k, y), s);
+            else
                 scan_entry(c, p, ch, k, y, seg, s);
-            }
             for (int x = hi - lo - 1; x >= 0; --x)
                 tile[threadIdx.x][x] = (float)iir_step(c, (double)tile[threadIdx.x][x], s);
         }
@@ -279,15 +348,55 @@ __global__ void __launch_bounds__(32) dir_rows_final_bwd_kernel(const __grid_con
     }
 }
 
-// Columns, first pass from the visual top (memory row H-1) to memory row 0, in place
-// over the row-filtered planes: exit states, and the reflected start state (start
-// record slots 3..5). Start record: [0..2] the next pass's start state, [3..5] this
-// pass's start state, [6..8] the end block.
+// Reflected start states of the columns' first pass (from memory row H-1 upward in
+// the visual sense): a block of 32 columns x kStartSlices slices of the start window;
+// lanes read consecutive columns, slices split the window, shared-memory reduction.
+constexpr int kStartSlices = 8;
+
+__global__ void __launch_bounds__(32 * kStartSlices) dir_col_starts_kernel(const __grid_constant__ DirBlurParams p) {
+    __shared__ double part[kStartSlices][3][32];
+    const int ch = blockIdx.y;
+    const int lane = threadIdx.x & 31, slice = threadIdx.x >> 5;
+    const int x = blockIdx.x * 32 + lane;
+    const int W = p.width, H = p.height;
+    for (int k = 0; k < p.count; ++k) {
+        const DirComponentDev& c = p.comp[k];
+        if (c.op != kDirOpYvv) continue;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        double anchor = 0.0;
+        if (x < W) {
+            const float* T = p.temp[ch][k];
+            anchor = (double)T[(size_t)(H - 1) * W + x];
+            for (int i = slice; i < c.v_len; i += kStartSlices) {
+                const double d = (double)T[(size_t)(H - 1 - i) * W + x] - anchor;
+                a0 += c.v_init[i] * d;
+                a1 += c.v_init[c.v_len + i] * d;
+                a2 += c.v_init[2 * c.v_len + i] * d;
+            }
+        }
+        part[slice][0][lane] = a0;
+        part[slice][1][lane] = a1;
+        part[slice][2][lane] = a2;
+        __syncthreads();
+        if (slice == 0 && x < W) {
+            double* st = start_at(p, ch, k, x) + 3;
+            for (int h = 0; h < 3; ++h) {
+                double t = 0.0;
+                for (int q = 0; q < kStartSlices; ++q) t += part[q][h][lane];
+                st[h] = anchor + t;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Columns, first pass from memory row H-1 down to row 0 over the row-filtered planes:
+// exit states (segment 0 from the reflected start).
 __global__ void __launch_bounds__(kLineThreads) dir_cols_partial_a_kernel(const __grid_constant__ DirBlurParams p) {
     const int ch = blockIdx.z, seg = blockIdx.y;
     const int W = p.width, H = p.height;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= W || seg >= seg_count(H)) return;
+    if (x >= W || seg >= seg_count(H) - 1) return;
     int lo, hi;
     bwd_seg(H, seg, lo, hi);
     for (int k = 0; k < p.count; ++k) {
@@ -295,21 +404,16 @@ __global__ void __launch_bounds__(kLineThreads) dir_cols_partial_a_kernel(const 
         if (c.op != kDirOpYvv) continue;
         const float* T = p.temp[ch][k];
         double s[3] = {0.0, 0.0, 0.0};
-        if (seg == 0) {
-            // the start reads up to v_len rows above the bottom; they are read here,
-            // before the in-place pass rewrites them, and kept for that pass
-            reflected_start(c.v_init, c.v_len, [&](int i) { return T[(size_t)(H - 1 - i) * W + x]; }, s);
-            double* st = start_at(p, ch, k, x) + 3;
-            st[0] = s[0];
-            st[1] = s[1];
-            st[2] = s[2];
+        if (seg == 0) get3(start_at(p, ch, k, x) + 3, s);
+        for (int y0 = hi - 1; y0 >= lo; y0 -= kAhead) {
+            float v[kAhead];
+#pragma unroll
+            for (int r = 0; r < kAhead; ++r) v[r] = y0 - r >= lo ? T[(size_t)(y0 - r) * W + x] : 0.0f;
+#pragma unroll
+            for (int r = 0; r < kAhead; ++r)
+                if (y0 - r >= lo) iir_step(c, (double)v[r], s);
         }
-        if (seg >= seg_count(H) - 1) continue;
-        for (int y = hi - 1; y >= lo; --y) iir_step(c, (double)T[(size_t)y * W + x], s);
-        double* z = carry_at(p, ch, k, x, seg);
-        z[0] = s[0];
-        z[1] = s[1];
-        z[2] = s[2];
+        put3(carry_at(p, ch, k, x, seg), s);
     }
 }
 
@@ -327,17 +431,17 @@ __global__ void __launch_bounds__(kLineThreads) dir_cols_final_a_kernel(const __
         if (c.op != kDirOpYvv) continue;
         float* T = p.temp[ch][k];
         double s[3];
-        if (seg == 0) {
-            const double* st = start_at(p, ch, k, x) + 3;
-            s[0] = st[0];
-            s[1] = st[1];
-            s[2] = st[2];
-        } else {
+        if (seg == 0)
+            get3(start_at(p, ch, k, x) + 3, s);
+        else
             scan_entry(c, p, ch, k, x, seg, s);
-        }
-        for (int y = hi - 1; y >= lo; --y) {
-            const size_t i = (size_t)y * W + x;
-            T[i] = (float)iir_step(c, (double)T[i], s);
+        for (int y0 = hi - 1; y0 >= lo; y0 -= kAhead) {
+            float v[kAhead];
+#pragma unroll
+            for (int r = 0; r < kAhead; ++r) v[r] = y0 - r >= lo ? T[(size_t)(y0 - r) * W + x] : 0.0f;
+#pragma unroll
+            for (int r = 0; r < kAhead; ++r)
+                if (y0 - r >= lo) T[(size_t)(y0 - r) * W + x] = (float)iir_step(c, (double)v[r], s);
         }
         if (lo == 0) {
             const int ts = c.v_tsize;
@@ -368,17 +472,18 @@ __global__ void __launch_bounds__(kLineThreads) dir_cols_partial_b_kernel(const 
         double s[3] = {0.0, 0.0, 0.0};
         int from = lo;
         if (seg == 0) {
-            const double* st = start_at(p, ch, k, x);
-            s[0] = st[0];
-            s[1] = st[1];
-            s[2] = st[2];
+            get3(start_at(p, ch, k, x), s);
             from = c.v_tsize;
         }
-        for (int y = from; y < hi; ++y) iir_step(c, (double)T[(size_t)y * W + x], s);
-        double* z = carry_at(p, ch, k, x, seg);
-        z[0] = s[0];
-        z[1] = s[1];
-        z[2] = s[2];
+        for (int y0 = from; y0 < hi; y0 += kAhead) {
+            float v[kAhead];
+#pragma unroll
+            for (int r = 0; r < kAhead; ++r) v[r] = y0 + r < hi ? T[(size_t)(y0 + r) * W + x] : 0.0f;
+#pragma unroll
+            for (int r = 0; r < kAhead; ++r)
+                if (y0 + r < hi) iir_step(c, (double)v[r], s);
+        }
+        put3(carry_at(p, ch, k, x, seg), s);
     }
 }
 
@@ -397,11 +502,10 @@ __global__ void __launch_bounds__(kLineThreads) dir_cols_final_kernel(const __gr
         if (c.op != kDirOpYvv) continue;
         const double* start = start_at(p, ch, k, x);
         for (int h = 0; h < 3; ++h) term[k][h] = start[6 + h];
-        if (seg == 0) {
-            for (int h = 0; h < 3; ++h) st[k][h] = start[h];
-        } else {
+        if (seg == 0)
+            get3(start, st[k]);
+        else
             scan_entry(c, p, ch, k, x, seg, st[k]);
-        }
     }
     const float* raw = p.raw[ch];
     float* dst = p.filtered[ch];
@@ -416,8 +520,13 @@ __global__ void __launch_bounds__(kLineThreads) dir_cols_final_kernel(const __gr
             } else if (c.op == kDirOpFir) {
                 const float* T = p.temp[ch][k];
                 double sum = 0.0;
-                for (int o = -c.radius; o <= c.radius; ++o)
-                    sum += (double)T[(size_t)reflect_dir(y + o, H) * W + x] * (double)c.taps[o + c.radius];
+                if (y - c.radius >= 0 && y + c.radius < H) {
+                    for (int o = -c.radius; o <= c.radius; ++o)
+                        sum += (double)T[(size_t)(y + o) * W + x] * (double)c.taps[o + c.radius];
+                } else {
+                    for (int o = -c.radius; o <= c.radius; ++o)
+                        sum += (double)T[(size_t)reflect_dir(y + o, H) * W + x] * (double)c.taps[o + c.radius];
+                }
                 blurred = isfinite(sum) ? (float)sum : 0.0f;
             } else {
                 // memory row y is visual row H-1-y; the end block covers memory rows [0, ts)
@@ -436,6 +545,8 @@ __global__ void __launch_bounds__(kLineThreads) dir_cols_final_kernel(const __gr
 
 } // namespace
 
+int dir_segments(int n) { return seg_count(n); }
+
 cudaError_t launch_dir_blur(const DirBlurParams& p, cudaStream_t stream) {
     if (p.width <= 0 || p.height <= 0 || p.count <= 0) return cudaSuccess;
     bool fir = false, iir = false;
@@ -444,9 +555,8 @@ cudaError_t launch_dir_blur(const DirBlurParams& p, cudaStream_t stream) {
         iir |= p.comp[k].op == kDirOpYvv;
     }
     const int W = p.width, H = p.height;
-    const int sw = W / kSeg > 1 ? W / kSeg : 1, sh = H / kSeg > 1 ? H / kSeg : 1;
-    const dim3 rows_grid((H + 31) / 32, sw, 3);
-    const dim3 cols_grid((W + kLineThreads - 1) / kLineThreads, sh, 3);
+    const dim3 rows_grid((H + 31) / 32, seg_count(W), 3);
+    const dim3 cols_grid((W + kLineThreads - 1) / kLineThreads, seg_count(H), 3);
     cudaError_t e = cudaSuccess;
     if (fir) {
         const dim3 block(32, 8);
@@ -456,19 +566,32 @@ cudaError_t launch_dir_blur(const DirBlurParams& p, cudaStream_t stream) {
     }
     if (iir) {
         fjb::count_launch();
+        dir_row_starts_kernel<<<dim3((H + 7) / 8, 3), 256, 0, stream>>>(p);
+        const dim3 row_lines((H + kLineThreads - 1) / kLineThreads, 3), col_lines((W + kLineThreads - 1) / kLineThreads, 3);
+        fjb::count_launch();
         dir_rows_partial_fwd_kernel<<<rows_grid, 32, 0, stream>>>(p);
+        fjb::count_launch();
+        dir_scan_kernel<<<row_lines, kLineThreads, 0, stream>>>(p, kRowsFwd);
         fjb::count_launch();
         dir_rows_final_fwd_kernel<<<rows_grid, 32, 0, stream>>>(p);
         fjb::count_launch();
         dir_rows_partial_bwd_kernel<<<rows_grid, 32, 0, stream>>>(p);
         fjb::count_launch();
+        dir_scan_kernel<<<row_lines, kLineThreads, 0, stream>>>(p, kRowsBwd);
+        fjb::count_launch();
         dir_rows_final_bwd_kernel<<<rows_grid, 32, 0, stream>>>(p);
         fjb::count_launch();
+        dir_col_starts_kernel<<<dim3((W + 31) / 32, 3), 32 * kStartSlices, 0, stream>>>(p);
+        fjb::count_launch();
         dir_cols_partial_a_kernel<<<cols_grid, kLineThreads, 0, stream>>>(p);
+        fjb::count_launch();
+        dir_scan_kernel<<<col_lines, kLineThreads, 0, stream>>>(p, kColsA);
         fjb::count_launch();
         dir_cols_final_a_kernel<<<cols_grid, kLineThreads, 0, stream>>>(p);
         fjb::count_launch();
         dir_cols_partial_b_kernel<<<cols_grid, kLineThreads, 0, stream>>>(p);
+        fjb::count_launch();
+        dir_scan_kernel<<<col_lines, kLineThreads, 0, stream>>>(p, kColsB);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     fjb::count_launch();

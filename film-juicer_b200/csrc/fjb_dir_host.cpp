@@ -262,7 +262,7 @@ void DirPlan::release() {
 
 size_t dir_recursion_bytes(int width, int height) {
     const size_t lines = (size_t)(width > height ? width : height);
-    const int sw = width / kDirSeg > 1 ? width / kDirSeg : 1, sh = height / kDirSeg > 1 ? height / kDirSeg : 1;
+    const int sw = dir_segments(width), sh = dir_segments(height);
     const size_t segs = (size_t)(sw > sh ? sw : sh);
     return ((size_t)3 * kDirMaxComponents * lines * segs * 3 + (size_t)3 * kDirMaxComponents * lines * 9) *
            sizeof(double);

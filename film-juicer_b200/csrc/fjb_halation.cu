@@ -12,12 +12,12 @@
 //
 // B200 schedule: the reference runs one read-modify-write accumulation pass per
 // Gaussian per channel (up to ~14 full-plane passes per channel). Here every
-// Gaussian that reads the same source plane is evaluated in the same sweep: a row
-// kernel writes one row-filtered plane per Gaussian, and a column kernel runs all
-// column filters of a channel together and applies the scatter/bounce combination
-// in its epilogue, so the tail accumulator never touches HBM. All three channels run
-// in one launch (grid.y = channel). Four launches per frame: scatter rows, scatter
-// columns + combine, bounce rows, bounce columns + combine.
+// Gaussian that reads the same source plane is evaluated in the same sweep: the row
+// kernels write one row-filtered plane per Gaussian, and the last column kernel runs
+// all column filters of a channel together and applies the scatter/bounce
+// combination in its epilogue, so the tail accumulator never touches HBM. All three
+// channels run in each launch (grid.z = channel); the recursions are block-parallel
+// (below).
 #include <cuda_runtime.h>
 
 #include "fjb_optics.h"
@@ -27,9 +27,7 @@ namespace fjb {
 
 namespace {
 
-constexpr int kTile = 32;     // row kernel: one warp filters 32 rows through 32x32 tiles
 constexpr int kColThreads = 128;
-constexpr int kPrefetch = 8;  // column kernel: rows loaded ahead of the recursion
 
 __device__ __forceinline__ int reflect_half(int i, int n) {
     if (i >= 0 && i < n) return i;
@@ -58,7 +56,8 @@ __device__ __forceinline__ float yvv_step(const OpticGauss& g, float x, YvvState
         s.s2 += s.s3;
         return s.s2;
     }
-    const float v = g.yvv[0] * x + g.yvv[1] * s.s1 + g.yvv[2] * s.s2 + g.yvv[3] * s.s3;
+    // the newest state enters last: the loop-carried dependency is one fused multiply-add
+    const float v = __fmaf_rn(g.yvv[1], s.s1, __fmaf_rn(g.yvv[2], s.s2, __fmaf_rn(g.yvv[3], s.s3, g.yvv[0] * x)));
     s.s3 = s.s2;
     s.s2 = s.s1;
     s.s1 = v;
@@ -69,28 +68,34 @@ __host__ __device__ __forceinline__ bool is_yvv(int kind) { return kind == kGaus
 
 // ---------------------------------------------------------------------------
 // Recursive Gaussians, block-parallel. A line is cut into segments of kOpticSeg
-// samples (the segment processed last in a direction absorbs the remainder). A
-// partial kernel runs every segment from a zero state and keeps its exit state Z;
-// the final kernel rebuilds each segment's true entry state from the line's start
-// state and the exit states of the segments before it (x_{k+1} = M x_k + Z_k with
-// M the recursion's state map over one segment, in FP64), then runs the segment
-// again and writes it. In exact arithmetic this is the sequential recursion; in
-// FP32 it differs from it by rounding. Row kernels stage 32 rows x one segment in
+// samples (the segment processed last in a direction is shorter, or absorbs a
+// remainder of fewer than 8 samples). A partial kernel runs every segment -- the
+// first from the line's replicate start, the others from a zero state -- and keeps
+// its exit state; a scan kernel turns those into each segment's entry state
+// (x_{k+1} = M x_k + Z_k with M the recursion's state map over one segment, in
+// FP64); the final kernel runs each segment again from its entry state and writes
+// it. In exact arithmetic this is the sequential recursion; in FP32 it differs from
+// it by rounding. Row kernels stage 32 rows x one segment in
 // shared memory so global accesses stay coalesced; column kernels give each lane one
 // column, so a warp reads 32 consecutive floats per step.
 // ---------------------------------------------------------------------------
 constexpr int kSeg = kOpticSeg;
-constexpr int kTileCols = 2 * kSeg; // longest segment < 2 * kSeg
+constexpr int kTileCols = kSeg + 8; // longest segment: a remainder below 8 joins the last one
+constexpr int kAhead = 8;           // column kernels: rows loaded ahead of the recursion
 
-__device__ __forceinline__ int seg_count(int n) { return n / kSeg > 1 ? n / kSeg : 1; }
+__host__ __device__ __forceinline__ int seg_count(int n) {
+    if (n <= 0) return 0;
+    const int ns = n / kSeg + (n % kSeg >= 8 ? 1 : 0);
+    return ns > 0 ? ns : 1;
+}
 
-// forward segment b: [b*kSeg, (b+1)*kSeg), the last one running to n
+// forward segment b: [b*kSeg, ...), the last one running to n
 __device__ __forceinline__ void fwd_seg(int n, int b, int& lo, int& hi) {
     lo = b * kSeg;
     hi = b == seg_count(n) - 1 ? n : lo + kSeg;
 }
 
-// backward segment b (b-th from the end): [n-(b+1)*kSeg, n-b*kSeg), the last one from 0
+// backward segment b (b-th from the end), the last one starting at 0
 __device__ __forceinline__ void bwd_seg(int n, int b, int& lo, int& hi) {
     hi = n - b * kSeg;
     lo = b == seg_count(n) - 1 ? 0 : hi - kSeg;
@@ -110,22 +115,83 @@ __device__ __forceinline__ void store_exit(float* c, const YvvState& s) {
     c[2] = s.s3;
 }
 
-// Entry state of segment `seg` (processing order) from the replicate start `first`.
+// Entry state of segment `seg` (processing order): the replicate start from `first`
+// for segment 0, else the state the scan kernel left in the carry slot.
 __device__ __forceinline__ YvvState entry_state(const OpticGauss& g, const OpticPass& P, int job, int gi, int line,
                                                 int seg, float first) {
-    YvvState s0;
-    yvv_init(g, first, s0);
-    double a = s0.s1, b = s0.s2, c = s0.s3;
-    for (int i = 0; i < seg; ++i) {
-        const float* z = carry_at(P, job, gi, line, i);
-        const double na = g.seg[0] * a + g.seg[1] * b + g.seg[2] * c + (double)z[0];
-        const double nb = g.seg[3] * a + g.seg[4] * b + g.seg[5] * c + (double)z[1];
-        const double nc = g.seg[6] * a + g.seg[7] * b + g.seg[8] * c + (double)z[2];
-        a = na;
-        b = nb;
-        c = nc;
+    YvvState s;
+    if (seg == 0) {
+        yvv_init(g, first, s);
+    } else {
+        const float* z = carry_at(P, job, gi, line, seg);
+        s = YvvState{z[0], z[1], z[2]};
     }
-    return YvvState{(float)a, (float)b, (float)c};
+    return s;
+}
+
+enum OpticPassKind : int { kRowsFwd = 0, kRowsBwd = 1, kColsUp = 2, kColsDown = 3 };
+
+// Carry scan of one pass: exit states (segment 0's true, the others from a zero
+// state) -> every segment's entry state, in place, in FP64: entry_1 = exit_0,
+// entry_{j+1} = M entry_j + Z_j. One thread per (line, job, Gaussian).
+__global__ void __launch_bounds__(128) optic_scan_kernel(const __grid_constant__ OpticPass P, int pass) {
+    const int job = blockIdx.y;
+    const OpticJob& J = P.job[job];
+    const int line = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool rows = pass == kRowsFwd || pass == kRowsBwd;
+    if (line >= (rows ? P.height : P.width)) return;
+    const int ns = seg_count(rows ? P.width : P.height);
+    if (ns < 2) return;
+    for (int gi = 0; gi < J.count; ++gi) {
+        const OpticGauss& g = J.g[gi];
+        if (!is_yvv(g.kind)) continue;
+        const float* z0 = carry_at(P, job, gi, line, 0);
+        double a = z0[0], b = z0[1], c = z0[2];
+        // exit states are loaded a batch ahead of the dependent chain and the entry
+        // stores (the loads cannot pass the stores to the same buffer otherwise)
+        constexpr int B = 8;
+        float nz[B][3];
+        auto load_batch = [&](int j0) {
+#pragma unroll
+            for (int t = 0; t < B; ++t) {
+                const int j = j0 + t;
+                if (j < ns - 1) {
+                    const float* z = carry_at(P, job, gi, line, j);
+                    nz[t][0] = z[0];
+                    nz[t][1] = z[1];
+                    nz[t][2] = z[2];
+                } else {
+                    nz[t][0] = nz[t][1] = nz[t][2] = 0.0f; // the last segment keeps no exit state
+                }
+            }
+        };
+        load_batch(1);
+        for (int j0 = 1; j0 < ns; j0 += B) {
+            float z[B][3];
+#pragma unroll
+            for (int t = 0; t < B; ++t) {
+                z[t][0] = nz[t][0];
+                z[t][1] = nz[t][1];
+                z[t][2] = nz[t][2];
+            }
+            if (j0 + B < ns) load_batch(j0 + B);
+#pragma unroll
+            for (int t = 0; t < B; ++t) {
+                const int j = j0 + t;
+                if (j >= ns) break;
+                float* slot = carry_at(P, job, gi, line, j);
+                slot[0] = (float)a;
+                slot[1] = (float)b;
+                slot[2] = (float)c;
+                const double na = g.seg[0] * a + g.seg[1] * b + g.seg[2] * c + (double)z[t][0];
+                const double nb = g.seg[3] * a + g.seg[4] * b + g.seg[5] * c + (double)z[t][1];
+                const double nc = g.seg[6] * a + g.seg[7] * b + g.seg[8] * c + (double)z[t][2];
+                a = na;
+                b = nb;
+                c = nc;
+            }
+        }
+    }
 }
 
 __device__ __forceinline__ void load_rows(float (*tile)[kTileCols + 1], const float* src, long long stride, int row0,
@@ -164,6 +230,7 @@ __global__ void __launch_bounds__(32) rows_partial_fwd_kernel(const __grid_const
         const OpticGauss& g = J.g[gi];
         if (!is_yvv(g.kind)) continue;
         YvvState st{0.0f, 0.0f, 0.0f};
+        if (seg == 0) yvv_init(g, J.src[(long long)y * J.stride], st);
         for (int c = 0; c < hi - lo; ++c) yvv_step(g, tile[threadIdx.x][c], st);
         store_exit(carry_at(P, job, gi, y, seg), st);
     }
@@ -175,22 +242,21 @@ __global__ void __launch_bounds__(32) rows_final_fwd_kernel(const __grid_constan
     const OpticJob& J = P.job[job];
     const int W = P.width, H = P.height;
     if (seg >= seg_count(W)) return;
-    __shared__ float in[32][kTileCols + 1];
-    __shared__ float out[32][kTileCols + 1];
+    __shared__ float tile[32][kTileCols + 1];
     int lo, hi;
     fwd_seg(W, seg, lo, hi);
     const int len = hi - lo;
     const int row0 = blockIdx.x * 32, y = row0 + threadIdx.x;
-    load_rows(in, J.src, J.stride, row0, H, lo, len);
     for (int gi = 0; gi < J.count; ++gi) {
         const OpticGauss& g = J.g[gi];
         if (!is_yvv(g.kind)) continue;
+        load_rows(tile, J.src, J.stride, row0, H, lo, len);
         if (y < H) {
             YvvState st = entry_state(g, P, job, gi, y, seg, J.src[(long long)y * J.stride]);
-            for (int c = 0; c < len; ++c) out[threadIdx.x][c] = yvv_step(g, in[threadIdx.x][c], st);
-            if (seg == seg_count(W) - 1) P.edge_a[edge_at(P, job, gi, y)] = out[threadIdx.x][len - 1];
+            for (int c = 0; c < len; ++c) tile[threadIdx.x][c] = yvv_step(g, tile[threadIdx.x][c], st);
+            if (seg == seg_count(W) - 1) P.edge_a[edge_at(P, job, gi, y)] = tile[threadIdx.x][len - 1];
         }
-        store_rows(out, J.temp[gi], W, row0, H, lo, len);
+        store_rows(tile, J.temp[gi], W, row0, H, lo, len);
     }
 }
 
@@ -211,6 +277,7 @@ __global__ void __launch_bounds__(32) rows_partial_bwd_kernel(const __grid_const
         load_rows(tile, J.temp[gi], W, row0, H, lo, len);
         if (y < H) {
             YvvState st{0.0f, 0.0f, 0.0f};
+            if (seg == 0) yvv_init(g, P.edge_a[edge_at(P, job, gi, y)], st);
             for (int c = len - 1; c >= 0; --c) yvv_step(g, tile[threadIdx.x][c], st);
             store_exit(carry_at(P, job, gi, y, seg), st);
         }
@@ -252,7 +319,10 @@ __global__ void rows_fir_kernel(const __grid_constant__ OpticPass P) {
         const OpticGauss& g = J.g[gi];
         if (g.kind != kGaussFir) continue;
         float sum = 0.0f;
-        for (int o = -g.radius; o <= g.radius; ++o) sum += row[reflect_half(x + o, P.width)] * g.w[o + g.radius];
+        if (x - g.radius >= 0 && x + g.radius < P.width)
+            for (int o = -g.radius; o <= g.radius; ++o) sum += row[x + o] * g.w[o + g.radius];
+        else
+            for (int o = -g.radius; o <= g.radius; ++o) sum += row[reflect_half(x + o, P.width)] * g.w[o + g.radius];
         J.temp[gi][(long long)y * P.width + x] = sum;
     }
 }
@@ -275,10 +345,21 @@ __global__ void __launch_bounds__(kColThreads) cols_partial_up_kernel(const __gr
         const OpticGauss& g = J.g[gi];
         if (!is_yvv(g.kind)) continue;
         const float* T = J.temp[gi];
-        if (seg == 0) P.edge_a[edge_at(P, job, gi, x)] = T[(long long)(H - 1) * W + x];
-        if (seg == seg_count(H) - 1) continue;
         YvvState st{0.0f, 0.0f, 0.0f};
-        for (int y = hi - 1; y >= lo; --y) yvv_step(g, T[(long long)y * W + x], st);
+        if (seg == 0) {
+            const float bottom = T[(long long)(H - 1) * W + x];
+            P.edge_a[edge_at(P, job, gi, x)] = bottom;
+            yvv_init(g, bottom, st);
+        }
+        if (seg == seg_count(H) - 1) continue;
+        for (int y0 = hi - 1; y0 >= lo; y0 -= kAhead) {
+            float v[kAhead];
+#pragma unroll
+            for (int r = 0; r < kAhead; ++r) v[r] = y0 - r >= lo ? T[(long long)(y0 - r) * W + x] : 0.0f;
+#pragma unroll
+            for (int r = 0; r < kAhead; ++r)
+                if (y0 - r >= lo) yvv_step(g, v[r], st);
+        }
         store_exit(carry_at(P, job, gi, x, seg), st);
     }
 }
@@ -296,9 +377,13 @@ __global__ void __launch_bounds__(kColThreads) cols_final_up_kernel(const __grid
         if (!is_yvv(g.kind)) continue;
         float* T = J.temp[gi];
         YvvState st = entry_state(g, P, job, gi, x, seg, P.edge_a[edge_at(P, job, gi, x)]);
-        for (int y = hi - 1; y >= lo; --y) {
-            const long long i = (long long)y * W + x;
-            T[i] = yvv_step(g, T[i], st);
+        for (int y0 = hi - 1; y0 >= lo; y0 -= kAhead) {
+            float v[kAhead];
+#pragma unroll
+            for (int r = 0; r < kAhead; ++r) v[r] = y0 - r >= lo ? T[(long long)(y0 - r) * W + x] : 0.0f;
+#pragma unroll
+            for (int r = 0; r < kAhead; ++r)
+                if (y0 - r >= lo) T[(long long)(y0 - r) * W + x] = yvv_step(g, v[r], st);
         }
         if (lo == 0) P.edge_b[edge_at(P, job, gi, x)] = T[x];
     }
@@ -317,7 +402,15 @@ __global__ void __launch_bounds__(kColThreads) cols_partial_down_kernel(const __
         if (!is_yvv(g.kind)) continue;
         const float* T = J.temp[gi];
         YvvState st{0.0f, 0.0f, 0.0f};
-        for (int y = lo; y < hi; ++y) yvv_step(g, T[(long long)y * W + x], st);
+        if (seg == 0) yvv_init(g, P.edge_b[edge_at(P, job, gi, x)], st);
+        for (int y0 = lo; y0 < hi; y0 += kAhead) {
+            float v[kAhead];
+#pragma unroll
+            for (int r = 0; r < kAhead; ++r) v[r] = y0 + r < hi ? T[(long long)(y0 + r) * W + x] : 0.0f;
+#pragma unroll
+            for (int r = 0; r < kAhead; ++r)
+                if (y0 + r < hi) yvv_step(g, v[r], st);
+        }
         store_exit(carry_at(P, job, gi, x, seg), st);
     }
 }
@@ -375,6 +468,8 @@ __global__ void __launch_bounds__(kColThreads) cols_final_combine_kernel(const _
 
 } // namespace
 
+int optic_segments(int n) { return seg_count(n); }
+
 cudaError_t launch_optic_pass(const OpticPass& P, cudaStream_t stream) {
     if (P.jobs <= 0 || P.width <= 0 || P.height <= 0) return cudaSuccess;
     bool anyYvv = false, anyFir = false;
@@ -384,17 +479,22 @@ cudaError_t launch_optic_pass(const OpticPass& P, cudaStream_t stream) {
             anyFir |= P.job[j].g[g].kind == kGaussFir;
         }
     const int W = P.width, H = P.height;
-    const int sw = W / kSeg > 1 ? W / kSeg : 1, sh = H / kSeg > 1 ? H / kSeg : 1;
+    const int sw = seg_count(W), sh = seg_count(H);
     const dim3 rows_grid((H + 31) / 32, sw, P.jobs);
     const dim3 cols_grid((W + kColThreads - 1) / kColThreads, sh, P.jobs);
     cudaError_t e = cudaSuccess;
     if (anyYvv) {
+        const dim3 row_lines((H + 127) / 128, P.jobs);
         fjb::count_launch();
         rows_partial_fwd_kernel<<<rows_grid, 32, 0, stream>>>(P);
+        fjb::count_launch();
+        optic_scan_kernel<<<row_lines, 128, 0, stream>>>(P, kRowsFwd);
         fjb::count_launch();
         rows_final_fwd_kernel<<<rows_grid, 32, 0, stream>>>(P);
         fjb::count_launch();
         rows_partial_bwd_kernel<<<rows_grid, 32, 0, stream>>>(P);
+        fjb::count_launch();
+        optic_scan_kernel<<<row_lines, 128, 0, stream>>>(P, kRowsBwd);
         fjb::count_launch();
         rows_final_bwd_kernel<<<rows_grid, 32, 0, stream>>>(P);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -406,12 +506,17 @@ cudaError_t launch_optic_pass(const OpticPass& P, cudaStream_t stream) {
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (anyYvv) {
+        const dim3 col_lines((W + 127) / 128, P.jobs);
         fjb::count_launch();
         cols_partial_up_kernel<<<cols_grid, kColThreads, 0, stream>>>(P);
+        fjb::count_launch();
+        optic_scan_kernel<<<col_lines, 128, 0, stream>>>(P, kColsUp);
         fjb::count_launch();
         cols_final_up_kernel<<<cols_grid, kColThreads, 0, stream>>>(P);
         fjb::count_launch();
         cols_partial_down_kernel<<<cols_grid, kColThreads, 0, stream>>>(P);
+        fjb::count_launch();
+        optic_scan_kernel<<<col_lines, 128, 0, stream>>>(P, kColsDown);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     fjb::count_launch();

@@ -56,6 +56,9 @@ struct OpticPass {
 
 cudaError_t launch_optic_pass(const OpticPass& P, cudaStream_t stream);
 
+// Segments of the block-parallel recursions along a line of n samples.
+int optic_segments(int n);
+
 // Scratch floats needed by scatter_halation for a width x height frame.
 size_t halation_scratch_floats(int width, int height);
 

@@ -54,7 +54,7 @@ bool decode_gauss(const FjHalationGaussian& s, OpticGauss& g) {
 
 namespace {
 
-int segments(int n) { return n / kOpticSeg > 1 ? n / kOpticSeg : 1; }
+int segments(int n) { return optic_segments(n); }
 
 // The recursion's state map over kOpticSeg steps with zero input, in FP64: the
 // operator that carries a segment's entry state to its exit state.
