@@ -48,6 +48,29 @@ struct Arena {
     }
 };
 
+// Device time of the last reference launcher call (CUDA events around the launcher
+// only, after every upload), for the speed comparisons of the GPU tests.
+float g_last_ms = 0.0f;
+
+struct LaunchTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    LaunchTimer() {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaDeviceSynchronize();
+        cudaEventRecord(a, nullptr);
+    }
+    void stop() {
+        cudaEventRecord(b, nullptr);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&g_last_ms, a, b);
+    }
+    ~LaunchTimer() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+};
+
 JuicerCuda::DeviceCurveView curve(const float* x, const float* y, int n) {
     JuicerCuda::DeviceCurveView c{};
     c.x = x;
@@ -214,8 +237,10 @@ extern "C" int ref_render(const FjPreparedHostData* h, const float* const* lut, 
     p.width = width;
     p.height = height;
     p.nComponents = comps;
+    LaunchTimer timer;
     cudaError_t e = p.printExpose.active ? juicer_cuda_print_pipeline(&p, nullptr)
                                          : juicer_cuda_negative_pipeline(&p, nullptr);
+    timer.stop();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     unsigned f = 0;
     cudaMemcpy(&f, d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost);
@@ -248,7 +273,9 @@ extern "C" int ref_capture_density(const FjPreparedHostData* h, const float* con
     q.printDevelop = p.printDevelop;
     q.scanStage = p.scanStage;
     q.filmRaw = p.filmRaw;
+    LaunchTimer timer;
     cudaError_t e = juicer_cuda_print_focused_capture_density(&q, c, m, y, nullptr);
+    timer.stop();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return (int)e;
 }
@@ -301,7 +328,9 @@ extern "C" int ref_scatter_halation(const FjScatterHalation* d, float* r, float*
     view.currentCarrier.rowStrideFloats = (size_t)stride;
     view.filterTemp = temp;
     view.weightedAccumulation = acc;
+    LaunchTimer timer;
     const JuicerCuda::ScatterHalationLaunchResult res = JuicerCuda::launch_scatter_halation(view, nullptr);
+    timer.stop();
     cudaError_t e = res.status;
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     cudaFree(temp);
@@ -400,10 +429,14 @@ extern "C" int ref_spatial_dir(const FjPreparedHostData* h, const float* const* 
             for (int i = 0; i < 9; ++i) s.verticalBoundary.terminalMatrix[i] = c.v_term[i];
         }
     }
+    LaunchTimer timer;
     cudaError_t e = juicer_cuda_build_print_spatial_dir(&q, req);
+    timer.stop();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return (int)e;
 }
+
+extern "C" float ref_last_ms() { return g_last_ms; }
 
 // ---- visual grain: src/Cuda/Scan/JuicerCudaScanPipeline.cu:3141 with the payload
 // packing of src/Cuda/JuicerCudaFilmPayloads.cpp:384-495 (stbn offsets :212-240).
@@ -554,8 +587,10 @@ extern "C" int ref_visual_grain(const FjVisualGrain* g, const FjStaticNoise* noi
     const size_t plane = (size_t)width * (size_t)height;
     if (cudaMalloc(&work, 5 * plane * sizeof(float)) != cudaSuccess) return 2;
     a.ptrs.push_back(work);
+    LaunchTimer timer;
     cudaError_t e = juicer_cuda_apply_visual_grain(&p, &k, width, height, dc, dm, dy, work, work + plane,
                                                    work + 2 * plane, work + 3 * plane, work + 4 * plane, nullptr);
+    timer.stop();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return (int)e;
 }

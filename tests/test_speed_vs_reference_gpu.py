@@ -1,0 +1,92 @@
+"""Device time of each stage against the reference's own CUDA kernels on the same 4K
+frame (the reference compiled for sm_100a into the test harness; its launchers timed
+with CUDA events after every upload). Guards against regressions: no stage may be
+more than 1.5x slower than the reference's. Set FJB_SPEED_REPORT to a path to keep
+the table as JSON."""
+import ctypes as C
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+W, H = 3840, 2160
+
+
+def test_stage_times_against_reference_cuda(torch_cuda, recipes, prepare, oracle):
+    torch = torch_cuda
+    from film_juicer_b200 import abi, frame_records, load_library, runtime
+    from oracle import dir as odir
+    from oracle import grain as ograin
+    from oracle import optics as ooptics
+
+    ref = oracle.load_reference()
+    if ref is None:
+        pytest.skip("reference CUDA harness not built")
+    ref.ref_last_ms.restype = C.c_float
+    lib = load_library()
+    recipe = recipes["print"]
+    rec = frame_records.FrameRecord(recipe, W, H)
+    src = np.ascontiguousarray(prepare.synthetic_frame(W, H, seed=20261205))
+    s = torch.from_numpy(src).cuda()
+    d = torch.empty_like(s)
+    err = abi.ErrorText()
+    ours = {}
+    with runtime.Owner() as owner:
+        owner.render(rec, s, d)
+        lib.fjb_owner_stage_timing(owner.handle, 1, C.byref(err.buf))
+        for _ in range(5):
+            owner.render(rec, s, d)
+        t = abi.FjbStageTimes()
+        lib.fjb_owner_stage_times(owner.handle, C.byref(t), C.byref(err.buf))
+        for i, name in enumerate(abi.FJB_STAGE_NAMES):
+            if t.frames[i]:
+                ours[name] = t.total_ms[i] / t.frames[i]
+    # the fused per-pixel chain alone (no spatial stages)
+    host = prepare.HostRecord(recipe)
+    dr = runtime.DeviceRecipe(host)
+    for _ in range(3):
+        dr.render(s, d)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        dr.render(s, d)
+    e1.record()
+    e1.synchronize()
+    ours["monolithic"] = e0.elapsed_time(e1) / 10
+    dr.close()
+
+    theirs = {}
+    lut = oracle.scanner_lut_for(host)
+    ptrs = (C.c_void_p * 6)(*[o.ctypes.data for o in lut])
+    flags = C.c_uint32()
+    for _ in range(2):
+        assert ref.ref_render(host.pointer(), ptrs, C.c_void_p(s.data_ptr()), W * 12, C.c_void_p(d.data_ptr()),
+                              W * 12, W, H, 3, C.byref(flags)) == 0
+    theirs["monolithic"] = ref.ref_last_ms()
+    planes = [np.ascontiguousarray(prepare.synthetic_frame(W, H, seed=c)[..., 0]) for c in range(3)]
+    for _ in range(2):
+        ooptics.reference_scatter_halation(torch, rec.host.h.optics.scatter_halation, planes)
+    theirs["scatter_halation"] = ref.ref_last_ms()
+    for _ in range(2):
+        odir.reference_spatial_dir(torch, rec.host, rec.host.h.spatial_dir, src)
+    theirs["spatial_dir"] = ref.ref_last_ms()
+    a = recipe.arrays
+    layers = [[a["density_layers"][:, l, c] for c in range(3)] for l in range(3)]
+    base = [a["density_rgb"][:, c] for c in range(3)]
+    dens = [np.ascontiguousarray(np.clip(p * 2.0, 0.05, 2.5)) for p in planes]
+    for _ in range(2):
+        ograin.reference_visual_grain(torch, rec.host.h.grain, rec.noise.record, base, layers, False, dens)
+    theirs["grain"] = ref.ref_last_ms()
+
+    table = {k: {"ours_ms": round(ours[k], 4), "reference_ms": round(theirs[k], 4),
+                 "speedup": round(theirs[k] / ours[k], 2)} for k in theirs}
+    print(json.dumps(table, indent=1))
+    path = os.environ.get("FJB_SPEED_REPORT")
+    if path:
+        with open(path, "w") as fh:
+            json.dump(table, fh, indent=1)
+    for k, v in table.items():
+        assert v["ours_ms"] <= 1.5 * v["reference_ms"], (k, v)
