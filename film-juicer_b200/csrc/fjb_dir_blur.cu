@@ -23,6 +23,7 @@
 
 #include "fjb_dir.h"
 #include "fjb_launches.h"
+#include "fjb_lines.cuh"
 
 namespace fjb {
 
@@ -543,6 +544,212 @@ __global__ void __launch_bounds__(kLineThreads) dir_cols_final_kernel(const __gr
     }
 }
 
+// ---------------------------------------------------------------------------
+// Shared-memory form, used when whole lines fit on chip (the usual case): a CTA
+// holds kRowsPerCta full rows, or a kStripCols-wide strip of full columns, and runs
+// the block-parallel recursion of fjb_lines.cuh on them (reflected starts as
+// segment-wise partial dot products summed in segment order, the end block from the
+// last state), so each component costs one read and one write of the plane per pass.
+// ---------------------------------------------------------------------------
+constexpr int kRowsPerCta = 4;
+constexpr int kStripCols = 8;
+constexpr size_t kSmemLimit = 200 * 1024;
+static_assert(kDirSeg == lines::kLineSeg, "segment maps are built for the line segment length");
+
+// One recursive component with its coefficients held in registers.
+struct DirStep {
+    using Real = double;
+    double ff, fb0, fb1, fb2;
+    const double* seg;
+    __device__ explicit DirStep(const DirComponentDev& c)
+        : ff(c.ff), fb0(c.fb[0]), fb1(c.fb[1]), fb2(c.fb[2]), seg(c.seg) {}
+    __device__ __forceinline__ double step(float x, double s[3]) const {
+        const double v = fma(fb0, s[0], fma(fb1, s[1], fma(fb2, s[2], ff * (double)x)));
+        s[2] = s[1];
+        s[1] = s[0];
+        s[0] = v;
+        return v;
+    }
+    __device__ __forceinline__ const double* map() const { return seg; }
+};
+
+size_t rows_smem_bytes(int W) {
+    return (size_t)kRowsPerCta * lines::padded(W) * sizeof(float) +
+           ((size_t)kRowsPerCta * lines::segs(W) * 3 + (size_t)kRowsPerCta * 6) * sizeof(double);
+}
+
+size_t cols_smem_bytes(int H) {
+    return (size_t)kStripCols * lines::padded(H) * sizeof(float) +
+           ((size_t)kStripCols * lines::segs(H) * 3 + (size_t)kStripCols * 6) * sizeof(double);
+}
+
+// Reflected start of each line: anchor + sum_i w_h[i] (x_i - anchor) over the first
+// `len` samples in processing order, as partial sums per segment (tasks) then summed
+// in segment order by one thread per line.
+template <typename Buf>
+__device__ void reflected_starts(Buf buf, int es, int L, int n, bool forward, const double* w, int len,
+                                 double* partial, double* entry, bool line_fastest) {
+    const int ns = lines::segs(n);
+    for (int task = threadIdx.x; task < L * ns; task += blockDim.x) {
+        const int line = line_fastest ? task % L : task / ns;
+        const int j = line_fastest ? task / L : task - line * ns;
+        const float* b = buf(line);
+        const double anchor = (double)b[lines::at(lines::seg_pos(n, 0, 0, forward)) * es];
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        const int hi = min(lines::seg_len(n, j), len - j * lines::kLineSeg);
+        for (int t = 0; t < hi; ++t) {
+            const int i = j * lines::kLineSeg + t;
+            const double d = (double)b[lines::at(lines::seg_pos(n, j, t, forward)) * es] - anchor;
+            a0 += w[i] * d;
+            a1 += w[len + i] * d;
+            a2 += w[2 * len + i] * d;
+        }
+        double* q = partial + ((size_t)line * ns + j) * 3;
+        q[0] = a0;
+        q[1] = a1;
+        q[2] = a2;
+    }
+    __syncthreads();
+    for (int line = threadIdx.x; line < L; line += blockDim.x) {
+        const float* b = buf(line);
+        const double anchor = (double)b[lines::at(lines::seg_pos(n, 0, 0, forward)) * es];
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int j = 0; j < ns; ++j) {
+            const double* q = partial + ((size_t)line * ns + j) * 3;
+            a0 += q[0];
+            a1 += q[1];
+            a2 += q[2];
+        }
+        entry[line * 3] = anchor + a0;
+        entry[line * 3 + 1] = anchor + a1;
+        entry[line * 3 + 2] = anchor + a2;
+    }
+    __syncthreads();
+}
+
+// Rows: every recursive component, left to right, end block, right to left, into its
+// row-filtered plane.
+__global__ void __launch_bounds__(lines::kMaxLineThreads) dir_rows_smem_kernel(const __grid_constant__ DirBlurParams p) {
+    extern __shared__ __align__(16) unsigned char dsm[];
+    const int ch = blockIdx.y;
+    const int W = p.width, H = p.height;
+    const int row0 = blockIdx.x * kRowsPerCta;
+    const int L = min(kRowsPerCta, H - row0);
+    const int pw = lines::padded(W);
+    double* exits = reinterpret_cast<double*>(dsm);
+    double* entry = exits + (size_t)kRowsPerCta * lines::segs(W) * 3;
+    double* last = entry + (size_t)kRowsPerCta * 3;
+    float* buf = reinterpret_cast<float*>(last + (size_t)kRowsPerCta * 3);
+    auto line = [&](int r) { return buf + (size_t)r * pw; };
+    const float* raw = p.raw[ch];
+    for (int k = 0; k < p.count; ++k) {
+        const DirComponentDev& c = p.comp[k];
+        if (c.op != kDirOpYvv) continue;
+        lines::load_rows(buf, raw, W, row0, L, W);
+        reflected_starts(line, 1, L, W, true, c.h_init, c.h_len, exits, entry, false);
+        const DirStep op(c);
+        lines::run_direction(op, line, 1, L, W, true, entry, exits, last, true, false);
+        const int ts = c.h_tsize;
+        for (int r = threadIdx.x; r < L; r += blockDim.x) {
+            double term[3] = {0.0, 0.0, 0.0};
+            end_block(c.h_term, ts, last + r * 3, term);
+            for (int q = 0; q < ts; ++q)
+                if (W - ts + q >= 0) line(r)[lines::at(W - ts + q)] = (float)term[q];
+            for (int h = 0; h < 3; ++h) entry[r * 3 + h] = h < ts ? term[h] : last[r * 3 + h];
+        }
+        __syncthreads();
+        if (W - ts > 0)
+            lines::run_direction(op, line, 1, L, W - ts, false, entry, exits, (double*)nullptr, true, false);
+        float* T = p.temp[ch][k];
+        for (int i = threadIdx.x; i < L * W; i += blockDim.x) {
+            const int r = i / W, x = i - r * W;
+            T[(size_t)(row0 + r) * W + x] = line(r)[lines::at(x)];
+        }
+        __syncthreads();
+    }
+}
+
+// Columns of a kStripCols-wide strip: every component in order (recursive: from the
+// visual top, memory row H-1, down to row 0 with the reflected start, end block at
+// rows [0, ts), back up from row ts; FIR: reflect taps in FP64; identity), weighted
+// and summed as the reference accumulates them, into the filtered plane. The running
+// sum is parked in the strip of the row-filtered plane this CTA has just consumed (it
+// stays in L2), which keeps shared memory to one strip.
+__global__ void __launch_bounds__(lines::kMaxLineThreads) dir_cols_smem_kernel(const __grid_constant__ DirBlurParams p) {
+    extern __shared__ __align__(16) unsigned char dsm[];
+    const int ch = blockIdx.y;
+    const int W = p.width, H = p.height;
+    const int x0 = blockIdx.x * kStripCols;
+    const int C = min(kStripCols, W - x0);
+    double* exits = reinterpret_cast<double*>(dsm);
+    double* entry = exits + (size_t)kStripCols * lines::segs(H) * 3;
+    double* last = entry + (size_t)kStripCols * 3;
+    float* work = reinterpret_cast<float*>(last + (size_t)kStripCols * 3);
+    auto column = [&](int cc) { return work + cc; };
+    const float* raw = p.raw[ch];
+    __shared__ double terms[kStripCols][3];
+    for (int k = 0; k < p.count; ++k) {
+        const DirComponentDev& c = p.comp[k];
+        if (c.op != kDirOpIdentity) lines::load_strip8(work, p.temp[ch][k], W, H, x0, C);
+        const int ts = c.v_tsize;
+        if (c.op == kDirOpYvv) {
+            reflected_starts(column, kStripCols, kStripCols, H, false, c.v_init, c.v_len, exits, entry, true);
+            const DirStep op(c);
+            lines::run_direction(op, column, kStripCols, kStripCols, H, false, entry, exits, last, true, true);
+            for (int cc = threadIdx.x; cc < kStripCols; cc += blockDim.x) {
+                double term[3] = {0.0, 0.0, 0.0};
+                end_block(c.v_term, ts, last + cc * 3, term);
+                for (int h = 0; h < 3; ++h) {
+                    terms[cc][h] = term[h];
+                    entry[cc * 3 + h] = h < ts ? term[h] : last[cc * 3 + h];
+                }
+            }
+            __syncthreads();
+            if (H - ts > 0)
+                lines::run_direction(op, column, kStripCols, kStripCols, H - ts, true, entry, exits, (double*)nullptr,
+                                     true, true, ts);
+        }
+        const bool final_comp = k == p.count - 1;
+        const float* acc_in = k > 0 ? p.temp[ch][k - 1] : nullptr;
+        float* acc_out = final_comp ? p.filtered[ch] : p.temp[ch][k];
+        // global reads (raw plane, running sum) go kBatch per thread at a time so they overlap
+        constexpr int kBatch = 8;
+        const bool reads_raw = c.op == kDirOpIdentity;
+        for (int base = 0; base < H * kStripCols; base += kBatch * blockDim.x) {
+            float rawv[kBatch], accv[kBatch];
+#pragma unroll
+            for (int b = 0; b < kBatch; ++b) {
+                const int i = base + b * blockDim.x + threadIdx.x;
+                const int y = i / kStripCols, cc = i - y * kStripCols;
+                const bool in = i < H * kStripCols && cc < C;
+                rawv[b] = reads_raw && in ? raw[(size_t)y * W + x0 + cc] : 0.0f;
+                accv[b] = acc_in && in ? acc_in[(size_t)y * W + x0 + cc] : 0.0f;
+            }
+#pragma unroll
+            for (int b = 0; b < kBatch; ++b) {
+                const int i = base + b * blockDim.x + threadIdx.x;
+                const int y = i / kStripCols, cc = i - y * kStripCols;
+                if (i >= H * kStripCols || cc >= C) continue;
+                float blurred;
+                if (c.op == kDirOpIdentity) {
+                    blurred = rawv[b];
+                } else if (c.op == kDirOpFir) {
+                    double sum = 0.0;
+                    for (int o = -c.radius; o <= c.radius; ++o)
+                        sum += (double)work[lines::at(reflect_dir(y + o, H)) * kStripCols + cc] *
+                               (double)c.taps[o + c.radius];
+                    blurred = isfinite(sum) ? (float)sum : 0.0f;
+                } else {
+                    blurred = y < ts ? (float)terms[cc][ts - 1 - y] : work[lines::at(y) * kStripCols + cc];
+                }
+                const float weighted = blurred * c.weight;
+                acc_out[(size_t)y * W + x0 + cc] = k == 0 ? weighted : accv[b] + weighted;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 } // namespace
 
 int dir_segments(int n) { return seg_count(n); }
@@ -564,10 +771,21 @@ cudaError_t launch_dir_blur(const DirBlurParams& p, cudaStream_t stream) {
         dir_rows_fir_kernel<<<dim3((W + 31) / 32, (H + 7) / 8, 3), block, 0, stream>>>(p);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    if (iir) {
+    // whole rows / column strips in shared memory when they fit, else the global form
+    const size_t rs = rows_smem_bytes(W), cs = cols_smem_bytes(H);
+    const bool rows_on_chip = rs <= kSmemLimit, cols_on_chip = cs <= kSmemLimit;
+    if (iir && rows_on_chip) {
+        if ((e = cudaFuncSetAttribute(dir_rows_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rs)) !=
+            cudaSuccess)
+            return e;
+        fjb::count_launch();
+        dir_rows_smem_kernel<<<dim3((H + kRowsPerCta - 1) / kRowsPerCta, 3), lines::line_threads(kRowsPerCta, W), rs,
+                               stream>>>(p);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    } else if (iir) {
         fjb::count_launch();
         dir_row_starts_kernel<<<dim3((H + 7) / 8, 3), 256, 0, stream>>>(p);
-        const dim3 row_lines((H + kLineThreads - 1) / kLineThreads, 3), col_lines((W + kLineThreads - 1) / kLineThreads, 3);
+        const dim3 row_lines((H + kLineThreads - 1) / kLineThreads, 3);
         fjb::count_launch();
         dir_rows_partial_fwd_kernel<<<rows_grid, 32, 0, stream>>>(p);
         fjb::count_launch();
@@ -580,6 +798,19 @@ cudaError_t launch_dir_blur(const DirBlurParams& p, cudaStream_t stream) {
         dir_scan_kernel<<<row_lines, kLineThreads, 0, stream>>>(p, kRowsBwd);
         fjb::count_launch();
         dir_rows_final_bwd_kernel<<<rows_grid, 32, 0, stream>>>(p);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (cols_on_chip) {
+        if ((e = cudaFuncSetAttribute(dir_cols_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cs)) !=
+            cudaSuccess)
+            return e;
+        fjb::count_launch();
+        dir_cols_smem_kernel<<<dim3((W + kStripCols - 1) / kStripCols, 3), lines::line_threads(kStripCols, H), cs,
+                               stream>>>(p);
+        return cudaGetLastError();
+    }
+    if (iir) {
+        const dim3 col_lines((W + kLineThreads - 1) / kLineThreads, 3);
         fjb::count_launch();
         dir_col_starts_kernel<<<dim3((W + 31) / 32, 3), 32 * kStartSlices, 0, stream>>>(p);
         fjb::count_launch();

@@ -20,8 +20,9 @@
 // (below).
 #include <cuda_runtime.h>
 
-#include "fjb_optics.h"
 #include "fjb_launches.h"
+#include "fjb_lines.cuh"
+#include "fjb_optics.h"
 
 namespace fjb {
 
@@ -466,6 +467,210 @@ __global__ void __launch_bounds__(kColThreads) cols_final_combine_kernel(const _
     }
 }
 
+// ---------------------------------------------------------------------------
+// Shared-memory form, used when whole lines fit on chip (the usual case): a CTA
+// holds kRowsPerCta full rows, or a kStripCols-wide strip of full columns, and runs
+// the block-parallel recursion of fjb_lines.cuh on them, so each Gaussian costs one
+// read and one write of the plane per direction pair.
+// ---------------------------------------------------------------------------
+constexpr int kRowsPerCta = 4;
+constexpr int kStripCols = 8;
+constexpr size_t kSmemLimit = 200 * 1024;
+static_assert(kOpticSeg == lines::kLineSeg, "segment maps are built for the line segment length");
+
+// One recursive Gaussian with its coefficients held in registers (read once per CTA,
+// not once per sample through the parameter block).
+struct HalStep {
+    using Real = float;
+    bool factored;
+    float c0, c1, c2, c3;
+    const double* seg;
+    __device__ explicit HalStep(const OpticGauss& g)
+        : factored(g.kind == kGaussYvvFactored), c0(g.yvv[0]), c1(g.yvv[1]), c2(g.yvv[2]), c3(g.yvv[3]),
+          seg(g.seg) {}
+    __device__ __forceinline__ float step(float x, float s[3]) const {
+        if (factored) {
+            s[0] += c0 * (x - s[0]);
+            s[2] = c2 * s[2] + c1 * (s[0] - s[1]);
+            s[1] += s[2];
+            return s[1];
+        }
+        const float v = __fmaf_rn(c1, s[0], __fmaf_rn(c2, s[1], __fmaf_rn(c3, s[2], c0 * x)));
+        s[2] = s[1];
+        s[1] = s[0];
+        s[0] = v;
+        return v;
+    }
+    __device__ __forceinline__ const double* map() const { return seg; }
+};
+
+size_t rows_smem_bytes(int W) {
+    return ((size_t)kRowsPerCta * lines::padded(W) + (size_t)kRowsPerCta * lines::segs(W) * 3 +
+            (size_t)kRowsPerCta * 3) *
+           sizeof(float);
+}
+
+size_t cols_smem_bytes(int H) {
+    return ((size_t)kStripCols * lines::padded(H) + (size_t)kStripCols * lines::segs(H) * 3 +
+            (size_t)kStripCols * 3) *
+           sizeof(float);
+}
+
+// Rows: every recursive Gaussian of the job, left to right then right to left, into
+// its row-filtered plane.
+__global__ void __launch_bounds__(lines::kMaxLineThreads) rows_smem_kernel(const __grid_constant__ OpticPass P) {
+    extern __shared__ __align__(16) float sm[];
+    const int job = blockIdx.y;
+    const OpticJob& J = P.job[job];
+    const int W = P.width, H = P.height;
+    const int row0 = blockIdx.x * kRowsPerCta;
+    const int L = min(kRowsPerCta, H - row0);
+    const int pw = lines::padded(W);
+    float* buf = sm;
+    float* exits = buf + (size_t)kRowsPerCta * pw;
+    float* entry = exits + (size_t)kRowsPerCta * lines::segs(W) * 3;
+    auto line = [&](int r) { return buf + (size_t)r * pw; };
+    for (int gi = 0; gi < J.count; ++gi) {
+        const OpticGauss& g = J.g[gi];
+        if (!is_yvv(g.kind)) continue;
+        lines::load_rows(buf, J.src, J.stride, row0, L, W);
+        for (int r = threadIdx.x; r < L; r += blockDim.x) {
+            YvvState st;
+            yvv_init(g, line(r)[0], st);
+            entry[r * 3] = st.s1;
+            entry[r * 3 + 1] = st.s2;
+            entry[r * 3 + 2] = st.s3;
+        }
+        __syncthreads();
+        const HalStep op(g);
+        lines::run_direction(op, line, 1, L, W, true, entry, exits, (float*)nullptr, true, false);
+        for (int r = threadIdx.x; r < L; r += blockDim.x) {
+            YvvState st;
+            yvv_init(g, line(r)[lines::at(W - 1)], st);
+            entry[r * 3] = st.s1;
+            entry[r * 3 + 1] = st.s2;
+            entry[r * 3 + 2] = st.s3;
+        }
+        __syncthreads();
+        lines::run_direction(op, line, 1, L, W, false, entry, exits, (float*)nullptr, true, false);
+        float* T = J.temp[gi];
+        for (int i = threadIdx.x; i < L * W; i += blockDim.x) {
+            const int r = i / W, x = i - r * W;
+            T[(long long)(row0 + r) * W + x] = line(r)[lines::at(x)];
+        }
+        __syncthreads();
+    }
+}
+
+// Columns of a kStripCols-wide strip: every Gaussian (recursive: bottom-up then
+// top-down; FIR: reflect taps; identity) in order, accumulated as the reference
+// combines them, then the scatter/bounce combination into the carrier plane. The
+// running sum of the Gaussians so far is parked in the strip of the row-filtered plane
+// this CTA has just consumed (it stays in L2), which keeps shared memory to one strip.
+__global__ void __launch_bounds__(lines::kMaxLineThreads) cols_smem_kernel(const __grid_constant__ OpticPass P) {
+    extern __shared__ __align__(16) float sm[];
+    const int job = blockIdx.y;
+    const OpticJob& J = P.job[job];
+    const int W = P.width, H = P.height;
+    const int x0 = blockIdx.x * kStripCols;
+    const int C = min(kStripCols, W - x0);
+    const int ph = lines::padded(H);
+    float* work = sm; // [padded(H)][kStripCols]
+    float* exits = work + (size_t)ph * kStripCols;
+    float* entry = exits + (size_t)kStripCols * lines::segs(H) * 3;
+    auto column = [&](int c) { return work + c; };
+    const int count = J.count;
+    for (int gi = 0; gi < count; ++gi) {
+        const OpticGauss& g = J.g[gi];
+        if (g.kind != kGaussIdentity) lines::load_strip8(work, J.temp[gi], W, H, x0, C);
+        if (is_yvv(g.kind)) {
+            const HalStep op(g);
+            for (int c = threadIdx.x; c < kStripCols; c += blockDim.x) {
+                YvvState st;
+                yvv_init(g, work[lines::at(H - 1) * kStripCols + c], st);
+                entry[c * 3] = st.s1;
+                entry[c * 3 + 1] = st.s2;
+                entry[c * 3 + 2] = st.s3;
+            }
+            __syncthreads();
+            lines::run_direction(op, column, kStripCols, kStripCols, H, false, entry, exits, (float*)nullptr, true,
+                                 true);
+            for (int c = threadIdx.x; c < kStripCols; c += blockDim.x) {
+                YvvState st;
+                yvv_init(g, work[c], st);
+                entry[c * 3] = st.s1;
+                entry[c * 3 + 1] = st.s2;
+                entry[c * 3 + 2] = st.s3;
+            }
+            __syncthreads();
+            lines::run_direction(op, column, kStripCols, kStripCols, H, true, entry, exits, (float*)nullptr, true,
+                                 true);
+        }
+        // roles of this Gaussian in the combination
+        const bool scatter = J.mode == kOpticScatter;
+        const bool finishes = scatter ? gi >= J.tail_count : gi == count - 1; // writes the carrier plane
+        const bool reads_acc = gi > 0 && (!scatter || J.tail_count > 0);    // a running sum exists
+        const bool reads_src = g.kind == kGaussIdentity || finishes;
+        const float* acc_in = reads_acc ? J.temp[scatter && finishes ? J.tail_count - 1 : gi - 1] : nullptr;
+        float* acc_out = J.temp[gi];
+        // global reads (source, running sum) go kBatch per thread at a time so they overlap
+        constexpr int kBatch = 8;
+        for (int base = 0; base < H * kStripCols; base += kBatch * blockDim.x) {
+            float srcv[kBatch], accv[kBatch];
+#pragma unroll
+            for (int b = 0; b < kBatch; ++b) {
+                const int i = base + b * blockDim.x + threadIdx.x;
+                const int y = i / kStripCols, c = i - y * kStripCols;
+                const bool in = i < H * kStripCols && c < C;
+                srcv[b] = reads_src && in ? J.src[(long long)y * J.stride + x0 + c] : 0.0f;
+                accv[b] = reads_acc && in ? acc_in[(long long)y * W + x0 + c] : 0.0f;
+            }
+#pragma unroll
+            for (int b = 0; b < kBatch; ++b) {
+                const int i = base + b * blockDim.x + threadIdx.x;
+                const int y = i / kStripCols, c = i - y * kStripCols;
+                if (i >= H * kStripCols || c >= C) continue;
+                float v;
+                if (g.kind == kGaussIdentity) {
+                    v = srcv[b];
+                } else if (g.kind == kGaussFir) {
+                    float sum = 0.0f;
+                    for (int o = -g.radius; o <= g.radius; ++o)
+                        sum += work[lines::at(reflect_half(y - o, H)) * kStripCols + c] * g.w[o + g.radius];
+                    v = sum;
+                } else {
+                    v = work[lines::at(y) * kStripCols + c];
+                }
+                const long long si = (long long)y * J.stride + x0 + c;
+                const long long ti = (long long)y * W + x0 + c;
+                if (scatter) {
+                    if (!finishes) {
+                        acc_out[ti] = gi == 0 ? J.coef[0] * v : accv[b] + J.coef[gi] * v;
+                    } else {
+                        // the core is the job's last Gaussian
+                        const float tail = J.tail_count > 0 ? accv[b] : 0.0f;
+                        const float coreTerm = (1.0f - J.tail_weight) * v;
+                        const float tailTerm = J.tail_weight * tail;
+                        const float scattered = coreTerm + tailTerm;
+                        const float sourceTerm = (1.0f - J.amount) * srcv[b];
+                        const float scatteredTerm = J.amount * scattered;
+                        J.src[si] = sourceTerm + scatteredTerm;
+                    }
+                } else {
+                    const float a = gi == 0 ? J.coef[0] * v : accv[b] + J.coef[gi] * v;
+                    if (!finishes) {
+                        acc_out[ti] = a;
+                    } else {
+                        const float added = srcv[b] + J.amount * a;
+                        J.src[si] = J.renormalize ? added / (1.0f + J.amount) : added;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 } // namespace
 
 int optic_segments(int n) { return seg_count(n); }
@@ -483,7 +688,18 @@ cudaError_t launch_optic_pass(const OpticPass& P, cudaStream_t stream) {
     const dim3 rows_grid((H + 31) / 32, sw, P.jobs);
     const dim3 cols_grid((W + kColThreads - 1) / kColThreads, sh, P.jobs);
     cudaError_t e = cudaSuccess;
-    if (anyYvv) {
+    // whole rows / column strips in shared memory when they fit, else the global form
+    const size_t rs = rows_smem_bytes(W), cs = cols_smem_bytes(H);
+    const bool rows_on_chip = rs <= kSmemLimit, cols_on_chip = cs <= kSmemLimit;
+    if (anyYvv && rows_on_chip) {
+        if ((e = cudaFuncSetAttribute(rows_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rs)) !=
+            cudaSuccess)
+            return e;
+        fjb::count_launch();
+        rows_smem_kernel<<<dim3((H + kRowsPerCta - 1) / kRowsPerCta, P.jobs), lines::line_threads(kRowsPerCta, W), rs,
+                           stream>>>(P);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    } else if (anyYvv) {
         const dim3 row_lines((H + 127) / 128, P.jobs);
         fjb::count_launch();
         rows_partial_fwd_kernel<<<rows_grid, 32, 0, stream>>>(P);
@@ -504,6 +720,15 @@ cudaError_t launch_optic_pass(const OpticPass& P, cudaStream_t stream) {
         fjb::count_launch();
         rows_fir_kernel<<<dim3((W + 31) / 32, (H + 7) / 8, P.jobs), block, 0, stream>>>(P);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (cols_on_chip) {
+        if ((e = cudaFuncSetAttribute(cols_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cs)) !=
+            cudaSuccess)
+            return e;
+        fjb::count_launch();
+        cols_smem_kernel<<<dim3((W + kStripCols - 1) / kStripCols, P.jobs), lines::line_threads(kStripCols, H), cs,
+                           stream>>>(P);
+        return cudaGetLastError();
     }
     if (anyYvv) {
         const dim3 col_lines((W + 127) / 128, P.jobs);
