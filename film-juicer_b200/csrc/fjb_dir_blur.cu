@@ -553,6 +553,10 @@ __global__ void __launch_bounds__(kLineThreads) dir_cols_final_kernel(const __gr
 // ---------------------------------------------------------------------------
 constexpr int kRowsPerCta = 4;
 constexpr int kStripCols = 8;
+// CTA sizes (threads, resident CTAs per SM) that bound registers so shared memory,
+// not registers, sets the occupancy
+constexpr int kRowsThreads = 256, kRowsBlocks = 3;
+constexpr int kColsThreads = 320, kColsBlocks = 2;
 constexpr size_t kSmemLimit = 200 * 1024;
 static_assert(kDirSeg == lines::kLineSeg, "segment maps are built for the line segment length");
 
@@ -584,22 +588,26 @@ size_t cols_smem_bytes(int H) {
 }
 
 // Reflected start of each line: anchor + sum_i w_h[i] (x_i - anchor) over the first
-// `len` samples in processing order, as partial sums per segment (tasks) then summed
-// in segment order by one thread per line.
-template <typename Buf>
-__device__ void reflected_starts(Buf buf, int es, int L, int n, bool forward, const double* w, int len,
-                                 double* partial, double* entry, bool line_fastest) {
-    const int ns = lines::segs(n);
+// `len` samples in processing order (i counts from the first sample processed), as
+// partial sums per piece (tasks, in processing order) then summed in piece order by
+// one thread per line.
+template <int ES, bool kForward, typename Buf>
+__device__ void reflected_starts(Buf buf, int L, int n, const double* w, int len, double* partial, double* entry,
+                                 bool line_fastest) {
+    const int ns = lines::range_pieces(0, n);
     for (int task = threadIdx.x; task < L * ns; task += blockDim.x) {
         const int line = line_fastest ? task % L : task / ns;
         const int j = line_fastest ? task / L : task - line * ns;
         const float* b = buf(line);
-        const double anchor = (double)b[lines::at(lines::seg_pos(n, 0, 0, forward)) * es];
+        const double anchor = (double)b[lines::at(kForward ? 0 : n - 1) * ES];
+        const lines::Piece pc = lines::piece<kForward>(0, n, j);
+        const int base = pc.q * lines::kLineSeg;
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        const int hi = min(lines::seg_len(n, j), len - j * lines::kLineSeg);
-        for (int t = 0; t < hi; ++t) {
-            const int i = j * lines::kLineSeg + t;
-            const double d = (double)b[lines::at(lines::seg_pos(n, j, t, forward)) * es] - anchor;
+        for (int t = 0; t < pc.hi - pc.lo; ++t) {
+            const int l = kForward ? pc.lo + t : pc.hi - 1 - t;
+            const int i = kForward ? base + l : n - 1 - (base + l);
+            if (i >= len) break;
+            const double d = (double)b[(pc.q * lines::kSegStride + l) * ES] - anchor;
             a0 += w[i] * d;
             a1 += w[len + i] * d;
             a2 += w[2 * len + i] * d;
@@ -612,7 +620,7 @@ __device__ void reflected_starts(Buf buf, int es, int L, int n, bool forward, co
     __syncthreads();
     for (int line = threadIdx.x; line < L; line += blockDim.x) {
         const float* b = buf(line);
-        const double anchor = (double)b[lines::at(lines::seg_pos(n, 0, 0, forward)) * es];
+        const double anchor = (double)b[lines::at(kForward ? 0 : n - 1) * ES];
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
         for (int j = 0; j < ns; ++j) {
             const double* q = partial + ((size_t)line * ns + j) * 3;
@@ -629,7 +637,7 @@ __device__ void reflected_starts(Buf buf, int es, int L, int n, bool forward, co
 
 // Rows: every recursive component, left to right, end block, right to left, into its
 // row-filtered plane.
-__global__ void __launch_bounds__(lines::kMaxLineThreads) dir_rows_smem_kernel(const __grid_constant__ DirBlurParams p) {
+__global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) dir_rows_smem_kernel(const __grid_constant__ DirBlurParams p) {
     extern __shared__ __align__(16) unsigned char dsm[];
     const int ch = blockIdx.y;
     const int W = p.width, H = p.height;
@@ -646,9 +654,9 @@ __global__ void __launch_bounds__(lines::kMaxLineThreads) dir_rows_smem_kernel(c
         const DirComponentDev& c = p.comp[k];
         if (c.op != kDirOpYvv) continue;
         lines::load_rows(buf, raw, W, row0, L, W);
-        reflected_starts(line, 1, L, W, true, c.h_init, c.h_len, exits, entry, false);
+        reflected_starts<1, true>(line, L, W, c.h_init, c.h_len, exits, entry, false);
         const DirStep op(c);
-        lines::run_direction(op, line, 1, L, W, true, entry, exits, last, true, false);
+        lines::run_direction<1, true>(op, line, L, 0, W, entry, exits, last, false);
         const int ts = c.h_tsize;
         for (int r = threadIdx.x; r < L; r += blockDim.x) {
             double term[3] = {0.0, 0.0, 0.0};
@@ -659,13 +667,8 @@ __global__ void __launch_bounds__(lines::kMaxLineThreads) dir_rows_smem_kernel(c
         }
         __syncthreads();
         if (W - ts > 0)
-            lines::run_direction(op, line, 1, L, W - ts, false, entry, exits, (double*)nullptr, true, false);
-        float* T = p.temp[ch][k];
-        for (int i = threadIdx.x; i < L * W; i += blockDim.x) {
-            const int r = i / W, x = i - r * W;
-            T[(size_t)(row0 + r) * W + x] = line(r)[lines::at(x)];
-        }
-        __syncthreads();
+            lines::run_direction<1, false>(op, line, L, 0, W - ts, entry, exits, (double*)nullptr, false);
+        lines::store_rows(buf, p.temp[ch][k], row0, L, W);
     }
 }
 
@@ -675,7 +678,7 @@ __global__ void __launch_bounds__(lines::kMaxLineThreads) dir_rows_smem_kernel(c
 // and summed as the reference accumulates them, into the filtered plane. The running
 // sum is parked in the strip of the row-filtered plane this CTA has just consumed (it
 // stays in L2), which keeps shared memory to one strip.
-__global__ void __launch_bounds__(lines::kMaxLineThreads) dir_cols_smem_kernel(const __grid_constant__ DirBlurParams p) {
+__global__ void __launch_bounds__(kColsThreads, kColsBlocks) dir_cols_smem_kernel(const __grid_constant__ DirBlurParams p) {
     extern __shared__ __align__(16) unsigned char dsm[];
     const int ch = blockIdx.y;
     const int W = p.width, H = p.height;
@@ -693,9 +696,9 @@ __global__ void __launch_bounds__(lines::kMaxLineThreads) dir_cols_smem_kernel(c
         if (c.op != kDirOpIdentity) lines::load_strip8(work, p.temp[ch][k], W, H, x0, C);
         const int ts = c.v_tsize;
         if (c.op == kDirOpYvv) {
-            reflected_starts(column, kStripCols, kStripCols, H, false, c.v_init, c.v_len, exits, entry, true);
+            reflected_starts<kStripCols, false>(column, kStripCols, H, c.v_init, c.v_len, exits, entry, true);
             const DirStep op(c);
-            lines::run_direction(op, column, kStripCols, kStripCols, H, false, entry, exits, last, true, true);
+            lines::run_direction<kStripCols, false>(op, column, kStripCols, 0, H, entry, exits, last, true);
             for (int cc = threadIdx.x; cc < kStripCols; cc += blockDim.x) {
                 double term[3] = {0.0, 0.0, 0.0};
                 end_block(c.v_term, ts, last + cc * 3, term);
@@ -706,8 +709,8 @@ __global__ void __launch_bounds__(lines::kMaxLineThreads) dir_cols_smem_kernel(c
             }
             __syncthreads();
             if (H - ts > 0)
-                lines::run_direction(op, column, kStripCols, kStripCols, H - ts, true, entry, exits, (double*)nullptr,
-                                     true, true, ts);
+                lines::run_direction<kStripCols, true>(op, column, kStripCols, ts, H - ts, entry, exits,
+                                                       (double*)nullptr, true);
         }
         const bool final_comp = k == p.count - 1;
         const float* acc_in = k > 0 ? p.temp[ch][k - 1] : nullptr;
@@ -715,21 +718,21 @@ __global__ void __launch_bounds__(lines::kMaxLineThreads) dir_cols_smem_kernel(c
         // global reads (raw plane, running sum) go kBatch per thread at a time so they overlap
         constexpr int kBatch = 8;
         const bool reads_raw = c.op == kDirOpIdentity;
-        for (int base = 0; base < H * kStripCols; base += kBatch * blockDim.x) {
+        // (the block size is a multiple of kStripCols: a thread keeps its column)
+        const int cc = threadIdx.x % kStripCols, ystep = blockDim.x / kStripCols;
+        for (int y0 = threadIdx.x / kStripCols; y0 < H; y0 += kBatch * ystep) {
             float rawv[kBatch], accv[kBatch];
 #pragma unroll
             for (int b = 0; b < kBatch; ++b) {
-                const int i = base + b * blockDim.x + threadIdx.x;
-                const int y = i / kStripCols, cc = i - y * kStripCols;
-                const bool in = i < H * kStripCols && cc < C;
+                const int y = y0 + b * ystep;
+                const bool in = y < H && cc < C;
                 rawv[b] = reads_raw && in ? raw[(size_t)y * W + x0 + cc] : 0.0f;
                 accv[b] = acc_in && in ? acc_in[(size_t)y * W + x0 + cc] : 0.0f;
             }
 #pragma unroll
             for (int b = 0; b < kBatch; ++b) {
-                const int i = base + b * blockDim.x + threadIdx.x;
-                const int y = i / kStripCols, cc = i - y * kStripCols;
-                if (i >= H * kStripCols || cc >= C) continue;
+                const int y = y0 + b * ystep;
+                if (y >= H || cc >= C) continue;
                 float blurred;
                 if (c.op == kDirOpIdentity) {
                     blurred = rawv[b];
@@ -779,7 +782,7 @@ cudaError_t launch_dir_blur(const DirBlurParams& p, cudaStream_t stream) {
             cudaSuccess)
             return e;
         fjb::count_launch();
-        dir_rows_smem_kernel<<<dim3((H + kRowsPerCta - 1) / kRowsPerCta, 3), lines::line_threads(kRowsPerCta, W), rs,
+        dir_rows_smem_kernel<<<dim3((H + kRowsPerCta - 1) / kRowsPerCta, 3), lines::line_threads(kRowsPerCta, W, kRowsThreads), rs,
                                stream>>>(p);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     } else if (iir) {
@@ -805,7 +808,7 @@ cudaError_t launch_dir_blur(const DirBlurParams& p, cudaStream_t stream) {
             cudaSuccess)
             return e;
         fjb::count_launch();
-        dir_cols_smem_kernel<<<dim3((W + kStripCols - 1) / kStripCols, 3), lines::line_threads(kStripCols, H), cs,
+        dir_cols_smem_kernel<<<dim3((W + kStripCols - 1) / kStripCols, 3), lines::line_threads(kStripCols, H, kColsThreads), cs,
                                stream>>>(p);
         return cudaGetLastError();
     }

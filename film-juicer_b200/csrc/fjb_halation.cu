@@ -475,21 +475,25 @@ __global__ void __launch_bounds__(kColThreads) cols_final_combine_kernel(const _
 // ---------------------------------------------------------------------------
 constexpr int kRowsPerCta = 4;
 constexpr int kStripCols = 8;
+// CTA sizes (threads, resident CTAs per SM) that bound registers so shared memory,
+// not registers, sets the occupancy
+constexpr int kRowsThreads = 256, kRowsBlocks = 3;
+constexpr int kColsThreads = 288, kColsBlocks = 3;
 constexpr size_t kSmemLimit = 200 * 1024;
 static_assert(kOpticSeg == lines::kLineSeg, "segment maps are built for the line segment length");
 
-// One recursive Gaussian with its coefficients held in registers (read once per CTA,
-// not once per sample through the parameter block).
+// One recursive Gaussian (kFactored: h, g, t form; else legacy B, B1, B2, B3) with its
+// coefficients held in registers (read once per CTA, not once per sample through the
+// parameter block).
+template <bool kFactored>
 struct HalStep {
     using Real = float;
-    bool factored;
     float c0, c1, c2, c3;
     const double* seg;
     __device__ explicit HalStep(const OpticGauss& g)
-        : factored(g.kind == kGaussYvvFactored), c0(g.yvv[0]), c1(g.yvv[1]), c2(g.yvv[2]), c3(g.yvv[3]),
-          seg(g.seg) {}
+        : c0(g.yvv[0]), c1(g.yvv[1]), c2(g.yvv[2]), c3(g.yvv[3]), seg(g.seg) {}
     __device__ __forceinline__ float step(float x, float s[3]) const {
-        if (factored) {
+        if (kFactored) {
             s[0] += c0 * (x - s[0]);
             s[2] = c2 * s[2] + c1 * (s[0] - s[1]);
             s[1] += s[2];
@@ -503,6 +507,32 @@ struct HalStep {
     }
     __device__ __forceinline__ const double* map() const { return seg; }
 };
+
+// Replicate start of each line from its first sample in processing order (position
+// `first`), into entry (L x 3).
+template <int ES, typename Buf>
+__device__ __forceinline__ void replicate_starts(const OpticGauss& g, Buf buf, int L, int first, float* entry) {
+    for (int r = threadIdx.x; r < L; r += blockDim.x) {
+        YvvState st;
+        yvv_init(g, buf(r)[lines::at(first) * ES], st);
+        entry[r * 3] = st.s1;
+        entry[r * 3 + 1] = st.s2;
+        entry[r * 3 + 2] = st.s3;
+    }
+    __syncthreads();
+}
+
+// Both passes of one recursive Gaussian over L lines of n samples held in shared
+// memory: kFirstForward runs ascending positions first (rows: left to right, then
+// back), else descending first (columns: bottom-up, then top-down).
+template <int ES, bool kFirstForward, bool kFactored, typename Buf>
+__device__ __forceinline__ void yvv_lines(const OpticGauss& g, Buf buf, int L, int n, float* exits, float* entry) {
+    const HalStep<kFactored> op(g);
+    replicate_starts<ES>(g, buf, L, kFirstForward ? 0 : n - 1, entry);
+    lines::run_direction<ES, kFirstForward>(op, buf, L, 0, n, entry, exits, (float*)nullptr, ES != 1);
+    replicate_starts<ES>(g, buf, L, kFirstForward ? n - 1 : 0, entry);
+    lines::run_direction<ES, !kFirstForward>(op, buf, L, 0, n, entry, exits, (float*)nullptr, ES != 1);
+}
 
 size_t rows_smem_bytes(int W) {
     return ((size_t)kRowsPerCta * lines::padded(W) + (size_t)kRowsPerCta * lines::segs(W) * 3 +
@@ -518,7 +548,7 @@ size_t cols_smem_bytes(int H) {
 
 // Rows: every recursive Gaussian of the job, left to right then right to left, into
 // its row-filtered plane.
-__global__ void __launch_bounds__(lines::kMaxLineThreads) rows_smem_kernel(const __grid_constant__ OpticPass P) {
+__global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) rows_smem_kernel(const __grid_constant__ OpticPass P) {
     extern __shared__ __align__(16) float sm[];
     const int job = blockIdx.y;
     const OpticJob& J = P.job[job];
@@ -534,31 +564,11 @@ __global__ void __launch_bounds__(lines::kMaxLineThreads) rows_smem_kernel(const
         const OpticGauss& g = J.g[gi];
         if (!is_yvv(g.kind)) continue;
         lines::load_rows(buf, J.src, J.stride, row0, L, W);
-        for (int r = threadIdx.x; r < L; r += blockDim.x) {
-            YvvState st;
-            yvv_init(g, line(r)[0], st);
-            entry[r * 3] = st.s1;
-            entry[r * 3 + 1] = st.s2;
-            entry[r * 3 + 2] = st.s3;
-        }
-        __syncthreads();
-        const HalStep op(g);
-        lines::run_direction(op, line, 1, L, W, true, entry, exits, (float*)nullptr, true, false);
-        for (int r = threadIdx.x; r < L; r += blockDim.x) {
-            YvvState st;
-            yvv_init(g, line(r)[lines::at(W - 1)], st);
-            entry[r * 3] = st.s1;
-            entry[r * 3 + 1] = st.s2;
-            entry[r * 3 + 2] = st.s3;
-        }
-        __syncthreads();
-        lines::run_direction(op, line, 1, L, W, false, entry, exits, (float*)nullptr, true, false);
-        float* T = J.temp[gi];
-        for (int i = threadIdx.x; i < L * W; i += blockDim.x) {
-            const int r = i / W, x = i - r * W;
-            T[(long long)(row0 + r) * W + x] = line(r)[lines::at(x)];
-        }
-        __syncthreads();
+        if (g.kind == kGaussYvvFactored)
+            yvv_lines<1, true, true>(g, line, L, W, exits, entry);
+        else
+            yvv_lines<1, true, false>(g, line, L, W, exits, entry);
+        lines::store_rows(buf, J.temp[gi], row0, L, W);
     }
 }
 
@@ -567,7 +577,7 @@ __global__ void __launch_bounds__(lines::kMaxLineThreads) rows_smem_kernel(const
 // combines them, then the scatter/bounce combination into the carrier plane. The
 // running sum of the Gaussians so far is parked in the strip of the row-filtered plane
 // this CTA has just consumed (it stays in L2), which keeps shared memory to one strip.
-__global__ void __launch_bounds__(lines::kMaxLineThreads) cols_smem_kernel(const __grid_constant__ OpticPass P) {
+__global__ void __launch_bounds__(kColsThreads, kColsBlocks) cols_smem_kernel(const __grid_constant__ OpticPass P) {
     extern __shared__ __align__(16) float sm[];
     const int job = blockIdx.y;
     const OpticJob& J = P.job[job];
@@ -583,29 +593,10 @@ __global__ void __launch_bounds__(lines::kMaxLineThreads) cols_smem_kernel(const
     for (int gi = 0; gi < count; ++gi) {
         const OpticGauss& g = J.g[gi];
         if (g.kind != kGaussIdentity) lines::load_strip8(work, J.temp[gi], W, H, x0, C);
-        if (is_yvv(g.kind)) {
-            const HalStep op(g);
-            for (int c = threadIdx.x; c < kStripCols; c += blockDim.x) {
-                YvvState st;
-                yvv_init(g, work[lines::at(H - 1) * kStripCols + c], st);
-                entry[c * 3] = st.s1;
-                entry[c * 3 + 1] = st.s2;
-                entry[c * 3 + 2] = st.s3;
-            }
-            __syncthreads();
-            lines::run_direction(op, column, kStripCols, kStripCols, H, false, entry, exits, (float*)nullptr, true,
-                                 true);
-            for (int c = threadIdx.x; c < kStripCols; c += blockDim.x) {
-                YvvState st;
-                yvv_init(g, work[c], st);
-                entry[c * 3] = st.s1;
-                entry[c * 3 + 1] = st.s2;
-                entry[c * 3 + 2] = st.s3;
-            }
-            __syncthreads();
-            lines::run_direction(op, column, kStripCols, kStripCols, H, true, entry, exits, (float*)nullptr, true,
-                                 true);
-        }
+        if (g.kind == kGaussYvvFactored)
+            yvv_lines<kStripCols, false, true>(g, column, kStripCols, H, exits, entry);
+        else if (g.kind == kGaussYvv)
+            yvv_lines<kStripCols, false, false>(g, column, kStripCols, H, exits, entry);
         // roles of this Gaussian in the combination
         const bool scatter = J.mode == kOpticScatter;
         const bool finishes = scatter ? gi >= J.tail_count : gi == count - 1; // writes the carrier plane
@@ -615,21 +606,21 @@ __global__ void __launch_bounds__(lines::kMaxLineThreads) cols_smem_kernel(const
         float* acc_out = J.temp[gi];
         // global reads (source, running sum) go kBatch per thread at a time so they overlap
         constexpr int kBatch = 8;
-        for (int base = 0; base < H * kStripCols; base += kBatch * blockDim.x) {
+        // (the block size is a multiple of kStripCols: a thread keeps its column)
+        const int c = threadIdx.x % kStripCols, ystep = blockDim.x / kStripCols;
+        for (int y0 = threadIdx.x / kStripCols; y0 < H; y0 += kBatch * ystep) {
             float srcv[kBatch], accv[kBatch];
 #pragma unroll
             for (int b = 0; b < kBatch; ++b) {
-                const int i = base + b * blockDim.x + threadIdx.x;
-                const int y = i / kStripCols, c = i - y * kStripCols;
-                const bool in = i < H * kStripCols && c < C;
+                const int y = y0 + b * ystep;
+                const bool in = y < H && c < C;
                 srcv[b] = reads_src && in ? J.src[(long long)y * J.stride + x0 + c] : 0.0f;
                 accv[b] = reads_acc && in ? acc_in[(long long)y * W + x0 + c] : 0.0f;
             }
 #pragma unroll
             for (int b = 0; b < kBatch; ++b) {
-                const int i = base + b * blockDim.x + threadIdx.x;
-                const int y = i / kStripCols, c = i - y * kStripCols;
-                if (i >= H * kStripCols || c >= C) continue;
+                const int y = y0 + b * ystep;
+                if (y >= H || c >= C) continue;
                 float v;
                 if (g.kind == kGaussIdentity) {
                     v = srcv[b];
@@ -696,7 +687,7 @@ cudaError_t launch_optic_pass(const OpticPass& P, cudaStream_t stream) {
             cudaSuccess)
             return e;
         fjb::count_launch();
-        rows_smem_kernel<<<dim3((H + kRowsPerCta - 1) / kRowsPerCta, P.jobs), lines::line_threads(kRowsPerCta, W), rs,
+        rows_smem_kernel<<<dim3((H + kRowsPerCta - 1) / kRowsPerCta, P.jobs), lines::line_threads(kRowsPerCta, W, kRowsThreads), rs,
                            stream>>>(P);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     } else if (anyYvv) {
@@ -726,7 +717,7 @@ cudaError_t launch_optic_pass(const OpticPass& P, cudaStream_t stream) {
             cudaSuccess)
             return e;
         fjb::count_launch();
-        cols_smem_kernel<<<dim3((W + kStripCols - 1) / kStripCols, P.jobs), lines::line_threads(kStripCols, H), cs,
+        cols_smem_kernel<<<dim3((W + kStripCols - 1) / kStripCols, P.jobs), lines::line_threads(kStripCols, H, kColsThreads), cs,
                            stream>>>(P);
         return cudaGetLastError();
     }

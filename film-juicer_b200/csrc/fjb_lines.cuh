@@ -1,18 +1,22 @@
 // fjb_lines.cuh -- third-order linear recursions over whole lines held in shared memory.
 //
 // A CTA stages L lines (rows of a plane, or the columns of a narrow strip) in shared
-// memory and runs a recursion along each of them block-parallel: each line is cut
-// into segments of kLineSeg samples; thread tasks are (line, segment) pairs.
-//   partial : each segment runs from a zero state (segment 0 from the line's entry
+// memory and runs a recursion along each of them block-parallel. Lines are stored in
+// blocks of kLineSeg samples, each followed by one pad word: sample p of a line sits at
+// (p / kLineSeg) * (kLineSeg + 1) + p % kLineSeg (times the element stride), so the
+// threads of a warp, which walk different blocks in step, hit different banks. A
+// recursion over line positions [off, off + n) is cut along those storage blocks
+// (only the first and last piece can be shorter than kLineSeg); thread tasks are
+// (line, piece) pairs:
+//   partial : each piece runs from a zero state (the first from the line's entry
 //             state) and leaves its exit state;
-//   scan    : one thread per line turns the exit states into every segment's entry
+//   scan    : one thread per line turns the exit states into every piece's entry
 //             state: entry_1 = exit_0, entry_{j+1} = M entry_j + exit_j, with M the
-//             recursion's state map over one segment (FP64);
-//   final   : each segment runs again from its entry state, writing in place.
+//             recursion's state map over kLineSeg steps (FP64), which is exact
+//             because every piece between the first and the last is full;
+//   final   : each piece runs again from its entry state, writing in place.
 // In exact arithmetic this equals the sequential recursion; in floating point it
-// differs from it by rounding. Layout: element i of a line sits at
-// (i / kLineSeg) * (kLineSeg + 1) + i % kLineSeg (times the element stride), so that
-// the threads of a warp, which walk different segments in step, hit different banks.
+// differs from it by rounding.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -27,41 +31,53 @@ constexpr int kSegStride = kLineSeg + 1;
 
 __host__ __device__ __forceinline__ int segs(int n) { return (n + kLineSeg - 1) / kLineSeg; }
 __host__ __device__ __forceinline__ int padded(int n) { return segs(n) * kSegStride; }
-__device__ __forceinline__ int at(int i) { return (i / kLineSeg) * kSegStride + i % kLineSeg; }
-
-// Length of segment j of an n-sample line, and the line position of its t-th sample
-// (forward: ascending from 64 j; backward: descending from n-1-64 j).
-__device__ __forceinline__ int seg_len(int n, int j) {
-    const int rest = n - j * kLineSeg;
-    return rest < kLineSeg ? rest : kLineSeg;
-}
-__device__ __forceinline__ int seg_pos(int n, int j, int t, bool forward) {
-    return forward ? j * kLineSeg + t : n - 1 - j * kLineSeg - t;
+__device__ __forceinline__ int at(int p) {
+    const unsigned u = (unsigned)p;
+    return (int)((u / kLineSeg) * kSegStride + u % kLineSeg);
 }
 
-// Runs segment j of a line (positions [off, off + n), forward or backward) from state
-// s. Samples are read kChunk at a time into registers, so each chunk pays the shared
-// memory latency once, then stepped (and written back in place when kWrite).
-template <bool kWrite, typename Step>
-__device__ __forceinline__ void run_segment(const Step& op, float* b, int es, int n, int j, bool forward, int off,
-                                            typename Step::Real s[3]) {
-    constexpr int kChunk = 8;
-    const int len = seg_len(n, j);
-    for (int t0 = 0; t0 < len; t0 += kChunk) {
-        float x[kChunk];
-        int idx[kChunk];
+// Pieces of the range [off, off + n) (n >= 1), and piece j in processing order:
+// storage block q and the block-local sample range [lo, hi).
+__device__ __forceinline__ int range_pieces(int off, int n) { return (off + n - 1) / kLineSeg - off / kLineSeg + 1; }
+struct Piece {
+    int q, lo, hi;
+};
+template <bool kForward>
+__device__ __forceinline__ Piece piece(int off, int n, int j) {
+    const int q = kForward ? off / kLineSeg + j : (off + n - 1) / kLineSeg - j;
+    const int base = q * kLineSeg;
+    const int lo = off > base ? off - base : 0;
+    const int end = off + n - base;
+    return {q, lo, end < kLineSeg ? end : kLineSeg};
+}
+
+// Runs one piece of a line from state s (kForward: ascending positions), writing
+// outputs back in place when kWrite. Full pieces read their samples eight at a time
+// into registers, so each group pays the shared-memory latency once. ES is the
+// element stride of the line in shared memory.
+template <bool kWrite, int ES, bool kForward, typename Step>
+__device__ __forceinline__ void run_piece(const Step& op, float* line, Piece pc, typename Step::Real s[3]) {
+    constexpr int D = kForward ? ES : -ES;
+    float* p = line + (pc.q * kSegStride + (kForward ? pc.lo : pc.hi - 1)) * ES;
+    const int len = pc.hi - pc.lo;
+    if (len == kLineSeg) {
+#pragma unroll 1
+        for (int c = 0; c < kLineSeg / 8; ++c, p += 8 * D) {
+            float x[8];
 #pragma unroll
-        for (int k = 0; k < kChunk; ++k) {
-            const int t = t0 + k < len ? t0 + k : len - 1; // past the end: re-read the last sample
-            idx[k] = at(off + seg_pos(n, j, t, forward)) * es;
-            x[k] = b[idx[k]];
-        }
+            for (int k = 0; k < 8; ++k) x[k] = p[k * D];
 #pragma unroll
-        for (int k = 0; k < kChunk; ++k) {
-            if (t0 + k < len) {
+            for (int k = 0; k < 8; ++k) {
                 const auto v = op.step(x[k], s);
-                if (kWrite) b[idx[k]] = (float)v;
+                if (kWrite) p[k * D] = (float)v;
             }
+        }
+    } else {
+        // a short first or last piece: one sample at a time
+#pragma unroll 1
+        for (int t = 0; t < len; ++t, p += D) {
+            const auto v = op.step(*p, s);
+            if (kWrite) *p = (float)v;
         }
     }
 }
@@ -70,20 +86,19 @@ __device__ __forceinline__ void run_segment(const Step& op, float* b, int es, in
 //   using Real;                               // state precision
 //   Real step(float x, Real s[3]) const;      // one sample, returns the output
 //   const double* map() const;                // 3x3 state map over kLineSeg steps
-// `buf(line)` returns the line's base pointer (float, element stride `es`), `entry`
-// holds each line's entry state (L x 3), `exits` is scratch of L x segs(n) x 3 Real,
-// `last` receives each line's final state (may be null). Outputs are written in place
-// when `write`. `line_fastest` orders the tasks line-first (column strips, whose lines
-// interleave element by element) instead of segment-first (rows), which keeps the
-// threads of a warp on different shared-memory banks in both layouts. The recursion
-// covers line positions [off, off + n). Caller synchronises before (the line data and
-// entry states must be visible) and this function ends with a barrier.
-template <typename Step, typename Buf>
-__device__ void run_direction(const Step& op, Buf buf, int es, int L, int n, bool forward,
-                              const typename Step::Real* entry, typename Step::Real* exits,
-                              typename Step::Real* last, bool write, bool line_fastest, int off = 0) {
+// `buf(line)` returns the line's base pointer (element stride ES), `entry` holds each
+// line's entry state (L x 3), `exits` is scratch of L x segs(off + n) x 3 Real,
+// `last` receives each line's final state (may be null). The final pass writes the
+// outputs in place. `line_fastest` orders the tasks line-first (column strips, whose lines
+// interleave element by element) instead of piece-first (rows), which keeps the
+// threads of a warp on different shared-memory banks in both layouts. Caller
+// synchronises before (the line data and entry states must be visible) and this
+// function ends with a barrier.
+template <int ES, bool kForward, typename Step, typename Buf>
+__device__ void run_direction(const Step& op, Buf buf, int L, int off, int n, const typename Step::Real* entry,
+                              typename Step::Real* exits, typename Step::Real* last, bool line_fastest) {
     using Real = typename Step::Real;
-    const int ns = segs(n);
+    const int ns = range_pieces(off, n);
     const int tasks = L * ns;
     // partial
     for (int task = threadIdx.x; task < tasks; task += blockDim.x) {
@@ -98,7 +113,7 @@ __device__ void run_direction(const Step& op, Buf buf, int es, int L, int n, boo
         } else {
             s[0] = s[1] = s[2] = Real(0);
         }
-        run_segment<false>(op, buf(line), es, n, j, forward, off, s);
+        run_piece<false, ES, kForward>(op, buf(line), piece<kForward>(off, n, j), s);
         Real* e = exits + ((size_t)line * ns + j) * 3;
         e[0] = s[0];
         e[1] = s[1];
@@ -139,10 +154,7 @@ __device__ void run_direction(const Step& op, Buf buf, int es, int L, int n, boo
         s[0] = e[0];
         s[1] = e[1];
         s[2] = e[2];
-        if (write)
-            run_segment<true>(op, buf(line), es, n, j, forward, off, s);
-        else
-            run_segment<false>(op, buf(line), es, n, j, forward, off, s);
+        run_piece<true, ES, kForward>(op, buf(line), piece<kForward>(off, n, j), s);
         if (last && j == ns - 1) {
             last[line * 3] = s[0];
             last[line * 3 + 1] = s[1];
@@ -152,26 +164,38 @@ __device__ void run_direction(const Step& op, Buf buf, int es, int L, int n, boo
     __syncthreads();
 }
 
-// Threads for a CTA that runs L lines of n samples: one per (line, segment) task,
-// rounded to whole warps, within [128, kMaxLineThreads].
-constexpr int kMaxLineThreads = 512;
-inline int line_threads(int L, int n) {
+// Threads for a CTA that runs L lines of n samples: one per (line, piece) task,
+// rounded to whole warps, within [128, cap] (more tasks loop).
+inline int line_threads(int L, int n, int cap) {
     const int t = (L * segs(n) + 31) / 32 * 32;
-    return t < 128 ? 128 : (t > kMaxLineThreads ? kMaxLineThreads : t);
+    return t < 128 ? 128 : (t > cap ? cap : t);
 }
 
 // Stages rows [row0, row0 + L) of a row-major plane (`stride` floats per row, W
-// columns) into the padded line layout at dst + r * padded(W): 4-byte cp.async copies,
-// all in flight at once. Ends with a barrier.
+// columns) into the line layout at dst + r * padded(W): 4-byte cp.async copies, all in
+// flight at once. Ends with a barrier.
 __device__ __forceinline__ void load_rows(float* dst, const float* src, long long stride, int row0, int L, int W) {
     const int pw = padded(W);
-    for (int i = threadIdx.x; i < L * W; i += blockDim.x) {
-        const int r = i / W, x = i - r * W;
-        const unsigned d = (unsigned)__cvta_generic_to_shared(dst + (size_t)r * pw + at(x));
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src + (long long)(row0 + r) * stride + x));
+    for (int r = 0; r < L; ++r) {
+        const float* row = src + (long long)(row0 + r) * stride;
+        const unsigned base = (unsigned)__cvta_generic_to_shared(dst + (size_t)r * pw);
+        for (int x = threadIdx.x; x < W; x += blockDim.x)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(base + 4u * (unsigned)at(x)), "l"(row + x));
     }
     asm volatile("cp.async.commit_group;\n" ::);
     asm volatile("cp.async.wait_group 0;\n" ::);
+    __syncthreads();
+}
+
+// Writes rows [row0, row0 + L) back from the line layout (W floats per row of dst).
+// Ends with a barrier.
+__device__ __forceinline__ void store_rows(const float* buf, float* dst, int row0, int L, int W) {
+    const int pw = padded(W);
+    for (int r = 0; r < L; ++r) {
+        float* row = dst + (long long)(row0 + r) * W;
+        const float* line = buf + (size_t)r * pw;
+        for (int x = threadIdx.x; x < W; x += blockDim.x) row[x] = line[at(x)];
+    }
     __syncthreads();
 }
 
