@@ -693,7 +693,18 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) dir_cols_smem_kerne
     __shared__ double terms[kStripCols][3];
     for (int k = 0; k < p.count; ++k) {
         const DirComponentDev& c = p.comp[k];
-        if (c.op != kDirOpIdentity) lines::load_strip8(work, p.temp[ch][k], W, H, x0, C);
+        const bool final_comp = k == p.count - 1;
+        const float* acc_in = k > 0 ? p.temp[ch][k - 1] : nullptr;
+        float* acc_out = final_comp ? p.filtered[ch] : p.temp[ch][k];
+        const bool reads_raw = c.op == kDirOpIdentity;
+        // full strips on 16-byte aligned planes move four columns per access
+        const bool vec = C == kStripCols && W % 4 == 0 && lines::aligned16(raw) && lines::aligned16(acc_out) &&
+                         (reads_raw || lines::aligned16(p.temp[ch][k])) && (!acc_in || lines::aligned16(acc_in));
+        const bool dense_fir = vec && c.op == kDirOpFir;
+        if (dense_fir)
+            lines::load_strip8_dense(work, p.temp[ch][k], W, H, x0);
+        else if (!reads_raw)
+            lines::load_strip8(work, p.temp[ch][k], W, H, x0, C);
         const int ts = c.v_tsize;
         if (c.op == kDirOpYvv) {
             reflected_starts<kStripCols, false>(column, kStripCols, H, c.v_init, c.v_len, exits, entry, true);
@@ -712,41 +723,83 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) dir_cols_smem_kerne
                 lines::run_direction<kStripCols, true>(op, column, kStripCols, ts, H - ts, entry, exits,
                                                        (double*)nullptr, true);
         }
-        const bool final_comp = k == p.count - 1;
-        const float* acc_in = k > 0 ? p.temp[ch][k - 1] : nullptr;
-        float* acc_out = final_comp ? p.filtered[ch] : p.temp[ch][k];
-        // global reads (raw plane, running sum) go kBatch per thread at a time so they overlap
-        constexpr int kBatch = 8;
-        const bool reads_raw = c.op == kDirOpIdentity;
-        // (the block size is a multiple of kStripCols: a thread keeps its column)
-        const int cc = threadIdx.x % kStripCols, ystep = blockDim.x / kStripCols;
-        for (int y0 = threadIdx.x / kStripCols; y0 < H; y0 += kBatch * ystep) {
-            float rawv[kBatch], accv[kBatch];
+        auto fir = [&](const float* col, int stride, int y) {
+            double sum = 0.0;
+            for (int o = -c.radius; o <= c.radius; ++o)
+                sum += (double)col[reflect_dir(y + o, H) * stride] * (double)c.taps[o + c.radius];
+            return isfinite(sum) ? (float)sum : 0.0f;
+        };
+        auto accumulate = [&](float blurred, float a) {
+            const float weighted = blurred * c.weight;
+            return k == 0 ? weighted : a + weighted;
+        };
+        if (vec) {
+            // thread -> (row, half strip); global reads go kBatch rows at a time
+            constexpr int kBatch = 4;
+            const int h = threadIdx.x & 1, ys = blockDim.x >> 1;
+            for (int y0 = threadIdx.x >> 1; y0 < H; y0 += kBatch * ys) {
+                float4 rawv[kBatch], accv[kBatch];
 #pragma unroll
-            for (int b = 0; b < kBatch; ++b) {
-                const int y = y0 + b * ystep;
-                const bool in = y < H && cc < C;
-                rawv[b] = reads_raw && in ? raw[(size_t)y * W + x0 + cc] : 0.0f;
-                accv[b] = acc_in && in ? acc_in[(size_t)y * W + x0 + cc] : 0.0f;
-            }
-#pragma unroll
-            for (int b = 0; b < kBatch; ++b) {
-                const int y = y0 + b * ystep;
-                if (y >= H || cc >= C) continue;
-                float blurred;
-                if (c.op == kDirOpIdentity) {
-                    blurred = rawv[b];
-                } else if (c.op == kDirOpFir) {
-                    double sum = 0.0;
-                    for (int o = -c.radius; o <= c.radius; ++o)
-                        sum += (double)work[lines::at(reflect_dir(y + o, H)) * kStripCols + cc] *
-                               (double)c.taps[o + c.radius];
-                    blurred = isfinite(sum) ? (float)sum : 0.0f;
-                } else {
-                    blurred = y < ts ? (float)terms[cc][ts - 1 - y] : work[lines::at(y) * kStripCols + cc];
+                for (int b = 0; b < kBatch; ++b) {
+                    const int y = y0 + b * ys;
+                    const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    rawv[b] = reads_raw && y < H ? *reinterpret_cast<const float4*>(raw + (size_t)y * W + x0 + 4 * h) : z;
+                    accv[b] = acc_in && y < H ? *reinterpret_cast<const float4*>(acc_in + (size_t)y * W + x0 + 4 * h) : z;
                 }
-                const float weighted = blurred * c.weight;
-                acc_out[(size_t)y * W + x0 + cc] = k == 0 ? weighted : accv[b] + weighted;
+#pragma unroll
+                for (int b = 0; b < kBatch; ++b) {
+                    const int y = y0 + b * ys;
+                    if (y >= H) continue;
+                    float4 v;
+                    if (reads_raw) {
+                        v = rawv[b];
+                    } else if (c.op == kDirOpFir) {
+                        const float* col = work + 4 * h;
+                        v = make_float4(fir(col, 8, y), fir(col + 1, 8, y), fir(col + 2, 8, y), fir(col + 3, 8, y));
+                    } else if (y < ts) {
+                        const int cc = 4 * h;
+                        v = make_float4((float)terms[cc][ts - 1 - y], (float)terms[cc + 1][ts - 1 - y],
+                                        (float)terms[cc + 2][ts - 1 - y], (float)terms[cc + 3][ts - 1 - y]);
+                    } else {
+                        v = *reinterpret_cast<const float4*>(work + lines::at(y) * 8 + 4 * h);
+                    }
+                    const float4 a = accv[b];
+                    *reinterpret_cast<float4*>(acc_out + (size_t)y * W + x0 + 4 * h) =
+                        make_float4(accumulate(v.x, a.x), accumulate(v.y, a.y), accumulate(v.z, a.z),
+                                    accumulate(v.w, a.w));
+                }
+            }
+        } else {
+            // one column per thread (the block size is a multiple of kStripCols)
+            constexpr int kBatch = 8;
+            const int cc = threadIdx.x % kStripCols, ystep = blockDim.x / kStripCols;
+            for (int y0 = threadIdx.x / kStripCols; y0 < H; y0 += kBatch * ystep) {
+                float rawv[kBatch], accv[kBatch];
+#pragma unroll
+                for (int b = 0; b < kBatch; ++b) {
+                    const int y = y0 + b * ystep;
+                    const bool in = y < H && cc < C;
+                    rawv[b] = reads_raw && in ? raw[(size_t)y * W + x0 + cc] : 0.0f;
+                    accv[b] = acc_in && in ? acc_in[(size_t)y * W + x0 + cc] : 0.0f;
+                }
+#pragma unroll
+                for (int b = 0; b < kBatch; ++b) {
+                    const int y = y0 + b * ystep;
+                    if (y >= H || cc >= C) continue;
+                    float blurred;
+                    if (reads_raw) {
+                        blurred = rawv[b];
+                    } else if (c.op == kDirOpFir) {
+                        double sum = 0.0;
+                        for (int o = -c.radius; o <= c.radius; ++o)
+                            sum += (double)work[lines::at(reflect_dir(y + o, H)) * kStripCols + cc] *
+                                   (double)c.taps[o + c.radius];
+                        blurred = isfinite(sum) ? (float)sum : 0.0f;
+                    } else {
+                        blurred = y < ts ? (float)terms[cc][ts - 1 - y] : work[lines::at(y) * kStripCols + cc];
+                    }
+                    acc_out[(size_t)y * W + x0 + cc] = accumulate(blurred, accv[b]);
+                }
             }
         }
         __syncthreads();

@@ -590,71 +590,127 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) cols_smem_kernel(co
     float* entry = exits + (size_t)kStripCols * lines::segs(H) * 3;
     auto column = [&](int c) { return work + c; };
     const int count = J.count;
+    const bool scatter = J.mode == kOpticScatter;
     for (int gi = 0; gi < count; ++gi) {
         const OpticGauss& g = J.g[gi];
-        if (g.kind != kGaussIdentity) lines::load_strip8(work, J.temp[gi], W, H, x0, C);
-        if (g.kind == kGaussYvvFactored)
-            yvv_lines<kStripCols, false, true>(g, column, kStripCols, H, exits, entry);
-        else if (g.kind == kGaussYvv)
-            yvv_lines<kStripCols, false, false>(g, column, kStripCols, H, exits, entry);
         // roles of this Gaussian in the combination
-        const bool scatter = J.mode == kOpticScatter;
         const bool finishes = scatter ? gi >= J.tail_count : gi == count - 1; // writes the carrier plane
         const bool reads_acc = gi > 0 && (!scatter || J.tail_count > 0);    // a running sum exists
         const bool reads_src = g.kind == kGaussIdentity || finishes;
         const float* acc_in = reads_acc ? J.temp[scatter && finishes ? J.tail_count - 1 : gi - 1] : nullptr;
-        float* acc_out = J.temp[gi];
-        // global reads (source, running sum) go kBatch per thread at a time so they overlap
-        constexpr int kBatch = 8;
-        // (the block size is a multiple of kStripCols: a thread keeps its column)
-        const int c = threadIdx.x % kStripCols, ystep = blockDim.x / kStripCols;
-        for (int y0 = threadIdx.x / kStripCols; y0 < H; y0 += kBatch * ystep) {
-            float srcv[kBatch], accv[kBatch];
-#pragma unroll
-            for (int b = 0; b < kBatch; ++b) {
-                const int y = y0 + b * ystep;
-                const bool in = y < H && c < C;
-                srcv[b] = reads_src && in ? J.src[(long long)y * J.stride + x0 + c] : 0.0f;
-                accv[b] = reads_acc && in ? acc_in[(long long)y * W + x0 + c] : 0.0f;
+        float* acc_out = finishes ? nullptr : J.temp[gi];
+        // full strips on 16-byte aligned planes move four columns per access
+        const bool vec = C == kStripCols && W % 4 == 0 && J.stride % 4 == 0 && lines::aligned16(J.src) &&
+                         (g.kind == kGaussIdentity || lines::aligned16(J.temp[gi])) &&
+                         (!acc_in || lines::aligned16(acc_in)) && (!acc_out || lines::aligned16(acc_out));
+        const bool dense_fir = vec && g.kind == kGaussFir;
+        if (dense_fir)
+            lines::load_strip8_dense(work, J.temp[gi], W, H, x0);
+        else if (g.kind != kGaussIdentity)
+            lines::load_strip8(work, J.temp[gi], W, H, x0, C);
+        if (g.kind == kGaussYvvFactored)
+            yvv_lines<kStripCols, false, true>(g, column, kStripCols, H, exits, entry);
+        else if (g.kind == kGaussYvv)
+            yvv_lines<kStripCols, false, false>(g, column, kStripCols, H, exits, entry);
+        const float coef = J.coef[gi];
+        // running sum after this Gaussian, and the carrier value when it finishes the job
+        auto running = [&](float v, float a) { return gi == 0 ? coef * v : a + coef * v; };
+        auto finish = [&](float v, float a, float source) {
+            if (scatter) {
+                // the core is the job's last Gaussian
+                const float tail = J.tail_count > 0 ? a : 0.0f;
+                const float coreTerm = (1.0f - J.tail_weight) * v;
+                const float tailTerm = J.tail_weight * tail;
+                const float scattered = coreTerm + tailTerm;
+                const float sourceTerm = (1.0f - J.amount) * source;
+                const float scatteredTerm = J.amount * scattered;
+                return sourceTerm + scatteredTerm;
             }
+            const float added = source + J.amount * running(v, a);
+            return J.renormalize ? added / (1.0f + J.amount) : added;
+        };
+        if (vec) {
+            // thread -> (row, half strip); global reads go kBatch rows at a time
+            constexpr int kBatch = 4;
+            const int h = threadIdx.x & 1, ys = blockDim.x >> 1;
+            for (int y0 = threadIdx.x >> 1; y0 < H; y0 += kBatch * ys) {
+                float4 srcv[kBatch], accv[kBatch];
 #pragma unroll
-            for (int b = 0; b < kBatch; ++b) {
-                const int y = y0 + b * ystep;
-                if (y >= H || c >= C) continue;
-                float v;
-                if (g.kind == kGaussIdentity) {
-                    v = srcv[b];
-                } else if (g.kind == kGaussFir) {
-                    float sum = 0.0f;
-                    for (int o = -g.radius; o <= g.radius; ++o)
-                        sum += work[lines::at(reflect_half(y - o, H)) * kStripCols + c] * g.w[o + g.radius];
-                    v = sum;
-                } else {
-                    v = work[lines::at(y) * kStripCols + c];
+                for (int b = 0; b < kBatch; ++b) {
+                    const int y = y0 + b * ys;
+                    const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    srcv[b] = reads_src && y < H
+                                  ? *reinterpret_cast<const float4*>(J.src + (long long)y * J.stride + x0 + 4 * h)
+                                  : z;
+                    accv[b] = reads_acc && y < H
+                                  ? *reinterpret_cast<const float4*>(acc_in + (long long)y * W + x0 + 4 * h)
+                                  : z;
                 }
-                const long long si = (long long)y * J.stride + x0 + c;
-                const long long ti = (long long)y * W + x0 + c;
-                if (scatter) {
-                    if (!finishes) {
-                        acc_out[ti] = gi == 0 ? J.coef[0] * v : accv[b] + J.coef[gi] * v;
+#pragma unroll
+                for (int b = 0; b < kBatch; ++b) {
+                    const int y = y0 + b * ys;
+                    if (y >= H) continue;
+                    float4 v;
+                    if (g.kind == kGaussIdentity) {
+                        v = srcv[b];
+                    } else if (g.kind == kGaussFir) {
+                        float4 sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        for (int o = -g.radius; o <= g.radius; ++o) {
+                            const float4 t = *reinterpret_cast<const float4*>(work + reflect_half(y - o, H) * 8 + 4 * h);
+                            const float wt = g.w[o + g.radius];
+                            sum.x += t.x * wt;
+                            sum.y += t.y * wt;
+                            sum.z += t.z * wt;
+                            sum.w += t.w * wt;
+                        }
+                        v = sum;
                     } else {
-                        // the core is the job's last Gaussian
-                        const float tail = J.tail_count > 0 ? accv[b] : 0.0f;
-                        const float coreTerm = (1.0f - J.tail_weight) * v;
-                        const float tailTerm = J.tail_weight * tail;
-                        const float scattered = coreTerm + tailTerm;
-                        const float sourceTerm = (1.0f - J.amount) * srcv[b];
-                        const float scatteredTerm = J.amount * scattered;
-                        J.src[si] = sourceTerm + scatteredTerm;
+                        v = *reinterpret_cast<const float4*>(work + lines::at(y) * 8 + 4 * h);
                     }
-                } else {
-                    const float a = gi == 0 ? J.coef[0] * v : accv[b] + J.coef[gi] * v;
-                    if (!finishes) {
-                        acc_out[ti] = a;
+                    const float4 a = accv[b];
+                    if (finishes) {
+                        const float4 o4 = make_float4(finish(v.x, a.x, srcv[b].x), finish(v.y, a.y, srcv[b].y),
+                                                      finish(v.z, a.z, srcv[b].z), finish(v.w, a.w, srcv[b].w));
+                        *reinterpret_cast<float4*>(J.src + (long long)y * J.stride + x0 + 4 * h) = o4;
                     } else {
-                        const float added = srcv[b] + J.amount * a;
-                        J.src[si] = J.renormalize ? added / (1.0f + J.amount) : added;
+                        const float4 o4 = make_float4(running(v.x, a.x), running(v.y, a.y), running(v.z, a.z),
+                                                      running(v.w, a.w));
+                        *reinterpret_cast<float4*>(acc_out + (long long)y * W + x0 + 4 * h) = o4;
                     }
+                }
+            }
+        } else {
+            // one column per thread (the block size is a multiple of kStripCols)
+            constexpr int kBatch = 8;
+            const int c = threadIdx.x % kStripCols, ystep = blockDim.x / kStripCols;
+            for (int y0 = threadIdx.x / kStripCols; y0 < H; y0 += kBatch * ystep) {
+                float srcv[kBatch], accv[kBatch];
+#pragma unroll
+                for (int b = 0; b < kBatch; ++b) {
+                    const int y = y0 + b * ystep;
+                    const bool in = y < H && c < C;
+                    srcv[b] = reads_src && in ? J.src[(long long)y * J.stride + x0 + c] : 0.0f;
+                    accv[b] = reads_acc && in ? acc_in[(long long)y * W + x0 + c] : 0.0f;
+                }
+#pragma unroll
+                for (int b = 0; b < kBatch; ++b) {
+                    const int y = y0 + b * ystep;
+                    if (y >= H || c >= C) continue;
+                    float v;
+                    if (g.kind == kGaussIdentity) {
+                        v = srcv[b];
+                    } else if (g.kind == kGaussFir) {
+                        float sum = 0.0f;
+                        for (int o = -g.radius; o <= g.radius; ++o)
+                            sum += work[lines::at(reflect_half(y - o, H)) * kStripCols + c] * g.w[o + g.radius];
+                        v = sum;
+                    } else {
+                        v = work[lines::at(y) * kStripCols + c];
+                    }
+                    if (finishes)
+                        J.src[(long long)y * J.stride + x0 + c] = finish(v, accv[b], srcv[b]);
+                    else
+                        acc_out[(long long)y * W + x0 + c] = running(v, accv[b]);
                 }
             }
         }

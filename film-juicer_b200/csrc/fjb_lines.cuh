@@ -223,5 +223,20 @@ __device__ __forceinline__ void load_strip8(float* work, const float* T, long lo
     __syncthreads();
 }
 
+// Stages a full, 16-byte aligned strip of 8 columns densely (element (y, c) at
+// y * 8 + c), for stencils that step across rows by a constant offset.
+__device__ __forceinline__ void load_strip8_dense(float* work, const float* T, long long W, int H, int x0) {
+    for (int i = threadIdx.x; i < H * 2; i += blockDim.x) {
+        const int y = i >> 1, h = i & 1;
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(work + y * 8 + 4 * h);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(T + (long long)y * W + x0 + 4 * h));
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    __syncthreads();
+}
+
+__device__ __forceinline__ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 } // namespace lines
 } // namespace fjb
