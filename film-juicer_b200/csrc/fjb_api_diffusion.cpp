@@ -173,15 +173,28 @@ extern "C" FjStatus fjb_diffusion(const FjDiffusionComponents* components, int32
         cudaError_t e = cudaMalloc(&d_psf, 3 * n * sizeof(float));
         for (int c = 0; c < 3 && e == cudaSuccess; ++c)
             e = cudaMemcpyAsync(d_psf + c * n, rows[c].data(), n * sizeof(float), cudaMemcpyHostToDevice, s);
+        float* d_fft = nullptr; // FFT form: PSF spectrum, then the row-spectrum workspace
         if (e == cudaSuccess) {
             const float* psf[3] = {d_psf, d_psf + n, d_psf + 2 * n};
             float* dst[3] = {dst_r, dst_g, dst_b};
             const float* src[3] = {src_r, src_g, src_b};
-            e = fjb::launch_diffusion(psf, radius_px, taps, (float)scatter_fraction, dst, src, stride, width, height, s);
+            fjb::DiffusionFftPlan plan;
+            if (fjb::diffusion_prefers_fft(width, height, radius_px) &&
+                fjb::diffusion_fft_plan(width, height, radius_px, plan)) {
+                e = cudaMalloc(&d_fft, (plan.spectrum_floats + plan.work_floats) * sizeof(float));
+                float* work = d_fft + plan.spectrum_floats;
+                if (e == cudaSuccess) e = fjb::launch_diffusion_fft_spectrum(plan, psf, taps, d_fft, work, s);
+                if (e == cudaSuccess)
+                    e = fjb::launch_diffusion_fft(plan, d_fft, (float)scatter_fraction, dst, src, stride, work, s);
+            } else {
+                e = fjb::launch_diffusion(psf, radius_px, taps, (float)scatter_fraction, dst, src, stride, width,
+                                          height, s);
+            }
         }
-        // the host rows and the device PSF must outlive the copies and the kernel
+        // the host rows and the device buffers must outlive the copies and the kernels
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (d_psf) cudaFree(d_psf);
+        if (d_fft) cudaFree(d_fft);
         if (e != cudaSuccess) return cuda_status(e, error, "diffusion");
         write_error(error, "");
         return ok_status();

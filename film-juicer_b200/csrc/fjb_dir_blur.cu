@@ -723,12 +723,6 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) dir_cols_smem_kerne
                 lines::run_direction<kStripCols, true>(op, column, kStripCols, ts, H - ts, entry, exits,
                                                        (double*)nullptr, true);
         }
-        auto fir = [&](const float* col, int stride, int y) {
-            double sum = 0.0;
-            for (int o = -c.radius; o <= c.radius; ++o)
-                sum += (double)col[reflect_dir(y + o, H) * stride] * (double)c.taps[o + c.radius];
-            return isfinite(sum) ? (float)sum : 0.0f;
-        };
         auto accumulate = [&](float blurred, float a) {
             const float weighted = blurred * c.weight;
             return k == 0 ? weighted : a + weighted;
@@ -754,8 +748,18 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) dir_cols_smem_kerne
                     if (reads_raw) {
                         v = rawv[b];
                     } else if (c.op == kDirOpFir) {
-                        const float* col = work + 4 * h;
-                        v = make_float4(fir(col, 8, y), fir(col + 1, 8, y), fir(col + 2, 8, y), fir(col + 3, 8, y));
+                        // four columns per tap from the dense strip, each summed in FP64
+                        double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;
+                        for (int o = -c.radius; o <= c.radius; ++o) {
+                            const float4 t = *reinterpret_cast<const float4*>(work + reflect_dir(y + o, H) * 8 + 4 * h);
+                            const double wt = (double)c.taps[o + c.radius];
+                            sx += (double)t.x * wt;
+                            sy += (double)t.y * wt;
+                            sz += (double)t.z * wt;
+                            sw += (double)t.w * wt;
+                        }
+                        v = make_float4(isfinite(sx) ? (float)sx : 0.0f, isfinite(sy) ? (float)sy : 0.0f,
+                                        isfinite(sz) ? (float)sz : 0.0f, isfinite(sw) ? (float)sw : 0.0f);
                     } else if (y < ts) {
                         const int cc = 4 * h;
                         v = make_float4((float)terms[cc][ts - 1 - y], (float)terms[cc + 1][ts - 1 - y],

@@ -42,6 +42,11 @@ struct FjCuda {
     size_t diffusion_psf_bytes = 0;
     uint64_t diffusion_key = 0;
     int diffusion_taps = 0;
+    float* diffusion_spectrum = nullptr;     // FFT form: PSF spectrum of the last descriptor and frame size
+    size_t diffusion_spectrum_bytes = 0;
+    uint64_t diffusion_spectrum_key = 0;
+    float* diffusion_fft_work = nullptr;     // FFT form: transposed row spectra of the frame
+    size_t diffusion_fft_work_bytes = 0;
     // optional per-stage device timing (CUDA events on the render stream)
     bool timing = false;
     bool timing_events = false;
@@ -93,7 +98,25 @@ void release_all(FjCuda* cuda) {
     cuda->diffusion_psf = nullptr;
     cuda->diffusion_psf_bytes = 0;
     cuda->diffusion_key = 0;
+    if (cuda->diffusion_spectrum) cudaFree(cuda->diffusion_spectrum);
+    cuda->diffusion_spectrum = nullptr;
+    cuda->diffusion_spectrum_bytes = 0;
+    cuda->diffusion_spectrum_key = 0;
+    if (cuda->diffusion_fft_work) cudaFree(cuda->diffusion_fft_work);
+    cuda->diffusion_fft_work = nullptr;
+    cuda->diffusion_fft_work_bytes = 0;
     stage_events_release(cuda);
+}
+
+// Grows an owner buffer to at least `bytes` (contents are not kept).
+cudaError_t ensure_buffer(float*& buf, size_t& have, size_t bytes) {
+    if (have >= bytes && buf) return cudaSuccess;
+    if (buf) cudaFree(buf);
+    buf = nullptr;
+    have = 0;
+    cudaError_t e = cudaMalloc(&buf, bytes);
+    if (e == cudaSuccess) have = bytes;
+    return e;
 }
 
 void stage_begin(FjCuda* cuda, int stage, void* vs) {
@@ -301,9 +324,33 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
         // R, G, B planes into the density planes, which then carry the exposure
         float* ddst[3] = {density[2], density[1], density[0]};
         const float* dsrc[3] = {carrier[2], carrier[1], carrier[0]};
+        const cudaStream_t cs = reinterpret_cast<cudaStream_t>(vs);
+        fjb::DiffusionFftPlan plan;
+        const bool fft = fjb::diffusion_prefers_fft(width, height, d.radius_px) &&
+                         fjb::diffusion_fft_plan(width, height, d.radius_px, plan);
+        if (fft) {
+            // the PSF spectrum depends on the descriptor and the transform sizes
+            const uint64_t skey = (cuda->diffusion_key * 0x100000001b3ULL) ^ ((uint64_t)width << 32) ^ (uint64_t)height;
+            e = ensure_buffer(cuda->diffusion_fft_work, cuda->diffusion_fft_work_bytes, plan.work_floats * sizeof(float));
+            if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion FFT workspace");
+            if (skey != cuda->diffusion_spectrum_key || !cuda->diffusion_spectrum) {
+                cuda->diffusion_spectrum_key = 0;
+                e = ensure_buffer(cuda->diffusion_spectrum, cuda->diffusion_spectrum_bytes,
+                                  plan.spectrum_floats * sizeof(float));
+                if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion PSF spectrum");
+                e = fjb::launch_diffusion_fft_spectrum(plan, psf, cuda->diffusion_taps, cuda->diffusion_spectrum,
+                                                       cuda->diffusion_fft_work, cs);
+                if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion PSF spectrum");
+                cuda->diffusion_spectrum_key = skey;
+            }
+        }
         stage_begin(cuda, FJB_STAGE_CAMERA_DIFFUSION, vs);
-        e = fjb::launch_diffusion(psf, d.radius_px, cuda->diffusion_taps, (float)d.scatter_fraction, ddst, dsrc, stride,
-                                  width, height, reinterpret_cast<cudaStream_t>(vs));
+        if (fft)
+            e = fjb::launch_diffusion_fft(plan, cuda->diffusion_spectrum, (float)d.scatter_fraction, ddst, dsrc, stride,
+                                          cuda->diffusion_fft_work, cs);
+        else
+            e = fjb::launch_diffusion(psf, d.radius_px, cuda->diffusion_taps, (float)d.scatter_fraction, ddst, dsrc,
+                                      stride, width, height, cs);
         stage_end(cuda, FJB_STAGE_CAMERA_DIFFUSION, vs);
         if (e != cudaSuccess) return fjb::cuda_status(e, error, "camera diffusion");
         std::swap(carrier[0], density[0]);

@@ -1,8 +1,9 @@
 """Diffusion (a17) on the GPU through fjb_diffusion, against the reference's external
 diffusion cohort and the CPU oracle.
 
-The kernel convolves directly with FP32 accumulation (the PSF rows folded by
-vertical symmetry); the oracle accumulates in FP64. Bound: |d| <= 2e-6 max(1,
+Radii below 8 convolve directly with FP32 accumulation (the PSF rows folded by
+vertical symmetry); larger radii go through the FP32 FFT convolution; the oracle
+accumulates the direct sum in FP64. Bound: |d| <= 2e-6 max(1,
 max |input|) -- a few float32 roundings of a sum whose weights add to one."""
 import numpy as np
 import pytest
@@ -61,6 +62,9 @@ SHAPES = {
     "one_row": (64, 1, 4, None),
     "one_col": (1, 40, 4, None),
     "radius_beyond_frame": (9, 6, 12, None),
+    # FFT form (radius >= 8): odd log2 transform lengths (128 x 128), and a larger frame
+    "fft_odd_lengths": (200, 100, 9, 224),
+    "fft_frame": (640, 360, 16, None),
 }
 
 
