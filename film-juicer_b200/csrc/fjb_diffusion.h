@@ -32,7 +32,8 @@ struct DiffusionFftPlan {
     int ntw, log2ntw; // twiddle table length (max(nx, ny))
     int ey;           // extended rows H + 2r
     int sy;           // rows per spectrum column in the work buffer (ey rounded up to 4)
-    int rows_per_cta, cols_per_cta;
+    int rows_per_cta, cols_per_cta; // powers of two
+    int log2_rows_per_cta;
     size_t work_floats;     // 3 channels x (m + 1) x sy complex
     size_t spectrum_floats; // twiddles (2 ntw) + 3 channels x (m + 1) x ny reals
 };

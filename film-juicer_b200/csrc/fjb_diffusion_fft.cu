@@ -22,8 +22,8 @@
 // The PSF spectrum is built once per descriptor and frame size by the same row and
 // column transforms over the PSF placed around the origin.
 //
-// Transforms: radix-4 Stockham stages (one radix-2 stage first when log2 n is odd)
-// in shared memory, natural order in and out. Each thread keeps the values of its
+// Transforms: radix-8 Stockham stages (after one radix-2 or radix-4 stage for the
+// remainder) in shared memory, natural order in and out. Each thread keeps the values of its
 // butterflies in registers across the stage barrier, so one buffer per line is
 // enough. Twiddles come from a table exp(-2 pi i k / N) built in FP64 and rounded.
 #include <cuda_runtime.h>
@@ -38,7 +38,7 @@ namespace {
 constexpr int kFftThreads = 512;
 constexpr int kFftMaxValues = 16; // complex values a thread holds across a stage barrier
 constexpr int kFftMaxLen = 8192;  // longest transform (nx / 2 and ny)
-constexpr int kC2rPairs = kFftMaxValues / 2 + 1; // (k, m - k) pairs a thread holds in the inverse split
+constexpr int kC2rPairs = kFftMaxValues / 2; // (k, m - k) pairs a thread holds in the inverse split
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -61,51 +61,94 @@ __global__ void twiddle_kernel(float2* tw, int n) {
     tw[k] = make_float2((float)c, (float)s);
 }
 
-// One Stockham stage of radix R over `count` lines of length n (line stride `ls`)
-// already in shared memory. Butterfly b of a line takes elements j + r n/R, applies
-// the twiddles exp(-+2 pi i r (j mod Ns) / (Ns R)), a size-R DFT, and writes elements
-// (j - j mod Ns) R + j mod Ns + r Ns.
+// Size-R DFT in registers (R = 2, 4, 8); kInverse uses the conjugate roots.
 template <int R, bool kInverse>
-__device__ __forceinline__ void fft_stage(float2* data, int n, int ls, int count, int Ns, const float2* tw,
+__device__ __forceinline__ void dft(float2 (&v)[R]) {
+    auto add = [](float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); };
+    auto sub = [](float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); };
+    // multiply by -i (forward) or +i (inverse)
+    auto rot = [](float2 a) { return kInverse ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x); };
+    if constexpr (R == 2) {
+        const float2 a = v[0], b = v[1];
+        v[0] = add(a, b);
+        v[1] = sub(a, b);
+    } else if constexpr (R == 4) {
+        const float2 a = add(v[0], v[2]), b = sub(v[0], v[2]);
+        const float2 c = add(v[1], v[3]), d = rot(sub(v[1], v[3]));
+        v[0] = add(a, c);
+        v[1] = add(b, d);
+        v[2] = sub(a, c);
+        v[3] = sub(b, d);
+    } else {
+        // even / odd halves, each a size-4 DFT, then the W8^k combination
+        float2 e[4] = {v[0], v[2], v[4], v[6]};
+        float2 o[4] = {v[1], v[3], v[5], v[7]};
+        dft<4, kInverse>(e);
+        dft<4, kInverse>(o);
+        constexpr float h = 0.70710678118654752440f;
+        const float2 o1 = kInverse ? make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
+                                   : make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+        const float2 o2 = rot(o[2]);
+        const float2 o3 = kInverse ? make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
+                                   : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+        v[0] = add(e[0], o[0]);
+        v[4] = sub(e[0], o[0]);
+        v[1] = add(e[1], o1);
+        v[5] = sub(e[1], o1);
+        v[2] = add(e[2], o2);
+        v[6] = sub(e[2], o2);
+        v[3] = add(e[3], o3);
+        v[7] = sub(e[3], o3);
+    }
+}
+
+// One Stockham stage of radix R over `count` lines of length n = 2^log2n (line
+// stride `ls`) already in shared memory, Ns = 2^log2ns. Butterfly j of a line takes
+// elements j + r n/R, applies the twiddles w^r with w = exp(-+2 pi i (j mod Ns) /
+// (Ns R)) (w, w^2 and w^4 from the table, the other powers by products), a size-R
+// DFT, and writes elements (j - j mod Ns) R + j mod Ns + r Ns.
+template <int R, bool kInverse>
+__device__ __forceinline__ void fft_stage(float2* data, int log2n, int ls, int count, int log2ns, const float2* tw,
                                           int tw_shift) {
     constexpr int kMaxB = kFftMaxValues / R;
-    const int nb = n / R;
-    const int total = count * nb;
-    const int step = n / (Ns * R); // twiddle index step, in units of 2 pi / n
+    constexpr int kLog2R = R == 2 ? 1 : (R == 4 ? 2 : 3);
+    const int log2nb = log2n - kLog2R;
+    const int nb = 1 << log2nb;
+    const int Ns = 1 << log2ns;
+    const int total = count << log2nb;
+    const int step_shift = log2n - log2ns - kLog2R + tw_shift; // twiddle index step n / (Ns R), in table units
     float2 v[kMaxB][R];
 #pragma unroll
     for (int i = 0; i < kMaxB; ++i) {
         const int b = threadIdx.x + i * blockDim.x;
         if (b < total) {
-            const int line = b / nb, j = b - line * nb;
+            const int line = b >> log2nb, j = b & (nb - 1);
             const float2* d = data + (size_t)line * ls;
             const int jm = j & (Ns - 1);
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                float2 x = d[j + r * nb];
-                if (r > 0) {
-                    float2 w = tw[(r * jm * step) << tw_shift];
+            for (int r = 0; r < R; ++r) v[i][r] = d[j + r * nb];
+            if (jm != 0) {
+                auto fetch = [&](int k) {
+                    float2 w = tw[(k * jm) << step_shift];
                     if (kInverse) w.y = -w.y;
-                    x = cmul(x, w);
+                    return w;
+                };
+                float2 w[R];
+                w[1] = fetch(1);
+                if constexpr (R >= 4) {
+                    w[2] = fetch(2);
+                    w[3] = cmul(w[1], w[2]);
                 }
-                v[i][r] = x;
+                if constexpr (R == 8) {
+                    w[4] = fetch(4);
+                    w[5] = cmul(w[1], w[4]);
+                    w[6] = cmul(w[2], w[4]);
+                    w[7] = cmul(w[3], w[4]);
+                }
+#pragma unroll
+                for (int r = 1; r < R; ++r) v[i][r] = cmul(v[i][r], w[r]);
             }
-            if (R == 2) {
-                const float2 a = v[i][0], b2 = v[i][1];
-                v[i][0] = make_float2(a.x + b2.x, a.y + b2.y);
-                v[i][1] = make_float2(a.x - b2.x, a.y - b2.y);
-            } else {
-                const float2 a = make_float2(v[i][0].x + v[i][2].x, v[i][0].y + v[i][2].y);
-                const float2 bb = make_float2(v[i][0].x - v[i][2].x, v[i][0].y - v[i][2].y);
-                const float2 c = make_float2(v[i][1].x + v[i][3].x, v[i][1].y + v[i][3].y);
-                const float2 dd = make_float2(v[i][1].x - v[i][3].x, v[i][1].y - v[i][3].y);
-                // forward: -i d; inverse: +i d
-                const float2 md = kInverse ? make_float2(-dd.y, dd.x) : make_float2(dd.y, -dd.x);
-                v[i][0] = make_float2(a.x + c.x, a.y + c.y);
-                v[i][1] = make_float2(bb.x + md.x, bb.y + md.y);
-                v[i][2] = make_float2(a.x - c.x, a.y - c.y);
-                v[i][3] = make_float2(bb.x - md.x, bb.y - md.y);
-            }
+            dft<R, kInverse>(v[i]);
         }
     }
     __syncthreads();
@@ -113,10 +156,10 @@ __device__ __forceinline__ void fft_stage(float2* data, int n, int ls, int count
     for (int i = 0; i < kMaxB; ++i) {
         const int b = threadIdx.x + i * blockDim.x;
         if (b < total) {
-            const int line = b / nb, j = b - line * nb;
+            const int line = b >> log2nb, j = b & (nb - 1);
             float2* d = data + (size_t)line * ls;
             const int jm = j & (Ns - 1);
-            const int base = (j - jm) * R + jm;
+            const int base = ((j - jm) << kLog2R) + jm;
 #pragma unroll
             for (int r = 0; r < R; ++r) d[base + r * Ns] = v[i][r];
         }
@@ -125,16 +168,20 @@ __device__ __forceinline__ void fft_stage(float2* data, int n, int ls, int count
 }
 
 // Unnormalised DFT (kInverse: conjugate twiddles) of `count` lines of length n = 2^log2n
-// in shared memory. Caller synchronises before; ends with a barrier.
+// in shared memory: radix-8 stages, after one radix-2 or radix-4 stage for the
+// remainder of log2n / 3. Caller synchronises before; ends with a barrier.
 template <bool kInverse>
 __device__ void fft_lines(float2* data, int n, int log2n, int ls, int count, const float2* tw, int log2tw) {
     const int tw_shift = log2tw - log2n;
-    int Ns = 1;
-    if (log2n & 1) {
-        fft_stage<2, kInverse>(data, n, ls, count, Ns, tw, tw_shift);
-        Ns = 2;
+    int log2ns = 0;
+    if (log2n % 3 == 1) {
+        fft_stage<2, kInverse>(data, log2n, ls, count, log2ns, tw, tw_shift);
+        log2ns = 1;
+    } else if (log2n % 3 == 2) {
+        fft_stage<4, kInverse>(data, log2n, ls, count, log2ns, tw, tw_shift);
+        log2ns = 2;
     }
-    for (; Ns < n; Ns *= 4) fft_stage<4, kInverse>(data, n, ls, count, Ns, tw, tw_shift);
+    for (; log2ns < log2n; log2ns += 3) fft_stage<8, kInverse>(data, log2n, ls, count, log2ns, tw, tw_shift);
 }
 
 struct FftPass {
@@ -164,8 +211,9 @@ __global__ void __launch_bounds__(kFftThreads) rows_r2c_kernel(const __grid_cons
     if (L <= 0) return;
     const int W = p.width, H = p.height;
     // load: complex sample n of line l = (e[2n], e[2n+1]) of the extended row
+    #pragma unroll 4
     for (int i = threadIdx.x; i < L * m; i += blockDim.x) {
-        const int l = i / m, n = i - l * m;
+        const int l = i >> p.log2m, n = i & (m - 1);
         const int ey = row0 + l;
         float e[2];
 #pragma unroll
@@ -191,8 +239,10 @@ __global__ void __launch_bounds__(kFftThreads) rows_r2c_kernel(const __grid_cons
     // split into the real transform's bins k = 0..m, written transposed
     float2* out = F.work[ch];
     const int shift_nx = p.log2ntw - (p.log2m + 1);
-    for (int i = threadIdx.x; i < L * (m + 1); i += blockDim.x) {
-        const int k = i / L, l = i - k * L;
+    const int lg = p.log2_rows_per_cta;
+    for (int i = threadIdx.x; i < (m + 1) << lg; i += blockDim.x) {
+        const int k = i >> lg, l = i & ((1 << lg) - 1);
+        if (l >= L) continue;
         const float2* z = fsm + (size_t)l * m;
         const float2 zk = z[k == m ? 0 : k];
         const float2 zr = z[k == 0 ? 0 : m - k];
@@ -220,8 +270,9 @@ __global__ void __launch_bounds__(kFftThreads) columns_kernel(const __grid_const
     if (KC <= 0) return;
     const float2* in = F.work[ch];
     const int rows = kBuild ? 2 * r + 1 : p.ey;
+    #pragma unroll 4
     for (int i = threadIdx.x; i < KC * ny; i += blockDim.x) {
-        const int c = i / ny, ey = i - c * ny;
+        const int c = i >> p.log2ny, ey = i & (ny - 1);
         float2 v = make_float2(0.0f, 0.0f);
         if (kBuild) {
             // compact PSF row j holds dy = j - r, placed at dy mod ny
@@ -240,6 +291,7 @@ __global__ void __launch_bounds__(kFftThreads) columns_kernel(const __grid_const
         for (int i = threadIdx.x; i < KC * ny; i += blockDim.x) spec[(size_t)k0 * ny + i] = fsm[i].x * scale;
         return;
     }
+    #pragma unroll 4
     for (int i = threadIdx.x; i < KC * ny; i += blockDim.x) {
         const float s = spec[(size_t)k0 * ny + i];
         fsm[i] = make_float2(fsm[i].x * s, fsm[i].y * s);
@@ -248,10 +300,8 @@ __global__ void __launch_bounds__(kFftThreads) columns_kernel(const __grid_const
     fft_lines<true>(fsm, ny, p.log2ny, ny, KC, F.tw, p.log2ntw);
     float2* out = F.work[ch];
     const int H = p.height;
-    for (int i = threadIdx.x; i < KC * H; i += blockDim.x) {
-        const int c = i / H, y = i - c * H;
-        out[(size_t)(k0 + c) * p.sy + r + y] = fsm[(size_t)c * ny + r + y];
-    }
+    for (int c = 0; c < KC; ++c)
+        for (int y = threadIdx.x; y < H; y += blockDim.x) out[(size_t)(k0 + c) * p.sy + r + y] = fsm[(size_t)c * ny + r + y];
 }
 
 // Output rows: inverse real transform of spectrum rows r + y, crop, mix.
@@ -265,15 +315,18 @@ __global__ void __launch_bounds__(kFftThreads) rows_c2r_kernel(const __grid_cons
     const int L = min(p.rows_per_cta, H - y0);
     if (L <= 0) return;
     const float2* in = F.work[ch];
-    for (int i = threadIdx.x; i < L * (m + 1); i += blockDim.x) {
-        const int k = i / L, l = i - k * L;
-        fsm[(size_t)l * ls + k] = in[(size_t)k * p.sy + r + y0 + l];
+    const int lg = p.log2_rows_per_cta;
+    #pragma unroll 4
+    for (int i = threadIdx.x; i < (m + 1) << lg; i += blockDim.x) {
+        const int k = i >> lg, l = i & ((1 << lg) - 1);
+        if (l < L) fsm[(size_t)l * ls + k] = in[(size_t)k * p.sy + r + y0 + l];
     }
     __syncthreads();
-    // Z[k] = E[k] + i O[k], E = (X[k] + conj X[m-k]) / 2, O = (X[k] - conj X[m-k]) conj(w^k) / 2;
-    // each thread takes the pair (k, m - k), reads both, then writes both after the barrier
+    // Z[k] = E[k] + i O[k], E = (X[k] + conj X[m-k]) / 2, O = (X[k] - conj X[m-k]) conj(w^k) / 2.
+    // A thread takes pairs (k, m - k), 0 <= k < m/2, reads both bins, and writes Z[k] and
+    // Z[m - k] (k > 0) after the barrier; the middle bin m/2 of line l goes to thread l.
     const int shift_nx = p.log2ntw - (p.log2m + 1);
-    const int half = m / 2;
+    const int half = m / 2, log2half = p.log2m - 1;
     constexpr int kMaxPairs = kC2rPairs;
     float2 zk[kMaxPairs], zm[kMaxPairs];
     auto z_of = [&](float2 xk, float2 xm, int k) {
@@ -287,37 +340,44 @@ __global__ void __launch_bounds__(kFftThreads) rows_c2r_kernel(const __grid_cons
 #pragma unroll
     for (int q = 0; q < kMaxPairs; ++q) {
         const int i = threadIdx.x + q * blockDim.x;
-        if (i < L * (half + 1)) {
-            const int l = i / (half + 1), k = i - l * (half + 1);
+        if (i < L << log2half) {
+            const int l = i >> log2half, k = i & (half - 1);
             const float2* x = fsm + (size_t)l * ls;
             const float2 a = x[k], b = x[m - k];
             zk[q] = z_of(a, b, k);
-            zm[q] = z_of(b, a, m - k); // used when 0 < k < m/2
+            zm[q] = z_of(b, a, m - k);
         }
+    }
+    float2 zmid = make_float2(0.0f, 0.0f);
+    if ((int)threadIdx.x < L) {
+        const float2 a = fsm[(size_t)threadIdx.x * ls + half];
+        zmid = z_of(a, a, half);
     }
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < kMaxPairs; ++q) {
         const int i = threadIdx.x + q * blockDim.x;
-        if (i < L * (half + 1)) {
-            const int l = i / (half + 1), k = i - l * (half + 1);
+        if (i < L << log2half) {
+            const int l = i >> log2half, k = i & (half - 1);
             float2* x = fsm + (size_t)l * ls;
             x[k] = zk[q];
-            if (k > 0 && k < half) x[m - k] = zm[q];
+            if (k > 0) x[m - k] = zm[q];
         }
     }
+    if ((int)threadIdx.x < L) fsm[(size_t)threadIdx.x * ls + half] = zmid;
     __syncthreads();
     fft_lines<true>(fsm, m, p.log2m, ls, L, F.tw, p.log2ntw);
     const float f = F.fraction;
-    for (int i = threadIdx.x; i < L * W; i += blockDim.x) {
-        const int l = i / W, x = i - l * W;
-        const int ex = x + r;
-        const float2 z = fsm[(size_t)l * ls + (ex >> 1)];
-        const float conv = (ex & 1) ? z.y : z.x;
-        const long long o = (long long)(y0 + l) * F.stride + x;
-        const float cur = F.src[ch][o];
-        F.dst[ch][o] = (1.0f - f) * cur + f * conv;
-    }
+    for (int l = 0; l < L; ++l)
+        #pragma unroll 4
+        for (int x = threadIdx.x; x < W; x += blockDim.x) {
+            const int ex = x + r;
+            const float2 z = fsm[(size_t)l * ls + (ex >> 1)];
+            const float conv = (ex & 1) ? z.y : z.x;
+            const long long o = (long long)(y0 + l) * F.stride + x;
+            const float cur = F.src[ch][o];
+            F.dst[ch][o] = (1.0f - f) * cur + f * conv;
+        }
 }
 
 int log2_exact(int n) {
@@ -362,7 +422,8 @@ bool diffusion_fft_plan(int width, int height, int radius, DiffusionFftPlan& p) 
     if (p.cols_per_cta > 2) p.cols_per_cta = 2;
     if (p.rows_per_cta < 1 || p.cols_per_cta < 1) return false;
     // the inverse split holds 2 values per (k, m - k) pair: (m/2 + 1) pairs per row
-    if ((long long)p.rows_per_cta * (p.m / 2 + 1) > (long long)kFftThreads * kC2rPairs) return false;
+    if ((long long)p.rows_per_cta * (p.m / 2) > (long long)kFftThreads * kC2rPairs) return false;
+    p.log2_rows_per_cta = log2_exact(p.rows_per_cta);
     p.work_floats = (size_t)3 * (p.m + 1) * p.sy * 2;
     p.spectrum_floats = (size_t)2 * p.ntw + (size_t)3 * (p.m + 1) * ny;
     return true;
