@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="0 skips the CPU baseline leg")
     ap.add_argument("--width", type=int, default=WIDTH, help="frame width (profiling runs use small frames)")
     ap.add_argument("--height", type=int, default=HEIGHT)
+    ap.add_argument("--precision", action="store_true",
+                    help="instead of timing: one frame against the oracle's stage chain (CIEDE2000 of the output)")
     args = ap.parse_args()
     return args
 
@@ -369,9 +371,44 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def run_precision(args):
+    """One frame through fj_cuda_render against the oracle's chain of the same stages
+    (FP32/FP64 CPU restatement, all host threads): CIEDE2000 of the encoded output
+    (p50 / p99 / max) and the largest absolute difference per encoded channel."""
+    import numpy as np
+    import torch
+
+    __graft_entry__.package()
+    from film_juicer_b200 import frame_records, prepare, runtime
+    from oracle import color
+    from oracle import frame as oframe
+
+    W, H = args.width, args.height
+    recipe = prepare.PreparedRecipe.load(os.path.join(ROOT, "tests", "golden", "recipe_print.npz"))
+    record = frame_records.FrameRecord(recipe, W, H)
+    host = np.ascontiguousarray(prepare.synthetic_frame(W, H, seed=SEED))
+    src = torch.from_numpy(host).to("cuda")
+    dst = torch.empty_like(src)
+    with runtime.Owner() as owner:
+        owner.render(record, src, dst)
+    got = dst.cpu().numpy()
+    t0 = time.perf_counter()
+    want, _ = oframe.render_frame(record, recipe, host, threads=os.cpu_count() or 1)
+    t_oracle = time.perf_counter() - t0
+    stats = color.delta_e_stats(got, want)
+    line = {"precision": {"workload": f"{W}x{H} full optical print through fj_cuda_render", "dtype": "f32",
+                          "delta_e00_vs_oracle": {k: round(v, 6) for k, v in stats.items()},
+                          "max_abs_encoded": float(np.abs(got - want).max()),
+                          "mean_abs_encoded": float(np.abs(got - want).mean()),
+                          "oracle_seconds": round(t_oracle, 1), "oracle_threads": os.cpu_count()}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.precision:
+        run_precision(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)
