@@ -46,6 +46,7 @@ struct DirComponentDev {
     int v_len, v_tsize;
     double v_term[9];
     double seg[9]; // recursion state map over kDirSeg zero-input steps (row-major 3x3)
+    double seg4[9]; // the same over 4 kDirSeg steps
 };
 
 constexpr int kDirSeg = 64; // segment length of the block-parallel recursions

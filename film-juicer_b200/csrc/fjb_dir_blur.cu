@@ -565,8 +565,9 @@ struct DirStep {
     using Real = double;
     double ff, fb0, fb1, fb2;
     const double* seg;
+    const double* seg4;
     __device__ explicit DirStep(const DirComponentDev& c)
-        : ff(c.ff), fb0(c.fb[0]), fb1(c.fb[1]), fb2(c.fb[2]), seg(c.seg) {}
+        : ff(c.ff), fb0(c.fb[0]), fb1(c.fb[1]), fb2(c.fb[2]), seg(c.seg), seg4(c.seg4) {}
     __device__ __forceinline__ double step(float x, double s[3]) const {
         const double v = fma(fb0, s[0], fma(fb1, s[1], fma(fb2, s[2], ff * (double)x)));
         s[2] = s[1];
@@ -575,47 +576,67 @@ struct DirStep {
         return v;
     }
     __device__ __forceinline__ const double* map() const { return seg; }
+    __device__ __forceinline__ const double* map4() const { return seg4; }
 };
+
+__host__ __device__ inline size_t carry_doubles(int L, int n) { return (size_t)L * lines::scan_chunks(lines::segs(n)) * 3; }
 
 size_t rows_smem_bytes(int W) {
     return (size_t)kRowsPerCta * lines::padded(W) * sizeof(float) +
-           ((size_t)kRowsPerCta * lines::segs(W) * 3 + (size_t)kRowsPerCta * 6) * sizeof(double);
+           ((size_t)kRowsPerCta * lines::segs(W) * 3 + (size_t)kRowsPerCta * 6 + carry_doubles(kRowsPerCta, W)) *
+               sizeof(double);
 }
 
 size_t cols_smem_bytes(int H) {
     return (size_t)kStripCols * lines::padded(H) * sizeof(float) +
-           ((size_t)kStripCols * lines::segs(H) * 3 + (size_t)kStripCols * 6) * sizeof(double);
+           ((size_t)kStripCols * lines::segs(H) * 3 + (size_t)kStripCols * 6 + carry_doubles(kStripCols, H)) *
+               sizeof(double);
 }
 
 // Reflected start of each line: anchor + sum_i w_h[i] (x_i - anchor) over the first
-// `len` samples in processing order (i counts from the first sample processed), as
-// partial sums per piece (tasks, in processing order) then summed in piece order by
-// one thread per line.
+// `len` samples in processing order (i counts from the first sample processed). One
+// warp per (line, piece) task sums the piece's samples (lanes striding the piece, a
+// fixed-order FP64 butterfly across lanes); then one thread per line adds the pieces in
+// order. Pieces past the window hold zero.
 template <int ES, bool kForward, typename Buf>
 __device__ void reflected_starts(Buf buf, int L, int n, const double* w, int len, double* partial, double* entry,
                                  bool line_fastest) {
     const int ns = lines::range_pieces(0, n);
-    for (int task = threadIdx.x; task < L * ns; task += blockDim.x) {
+    const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int task = threadIdx.x >> 5; task < L * ns; task += nwarps) {
         const int line = line_fastest ? task % L : task / ns;
         const int j = line_fastest ? task / L : task - line * ns;
-        const float* b = buf(line);
-        const double anchor = (double)b[lines::at(kForward ? 0 : n - 1) * ES];
         const lines::Piece pc = lines::piece<kForward>(0, n, j);
         const int base = pc.q * lines::kLineSeg;
+        // processing-order index of the piece's first sample
+        const int i0 = kForward ? base + pc.lo : n - 1 - (base + pc.hi - 1);
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        for (int t = 0; t < pc.hi - pc.lo; ++t) {
-            const int l = kForward ? pc.lo + t : pc.hi - 1 - t;
-            const int i = kForward ? base + l : n - 1 - (base + l);
-            if (i >= len) break;
-            const double d = (double)b[(pc.q * lines::kSegStride + l) * ES] - anchor;
-            a0 += w[i] * d;
-            a1 += w[len + i] * d;
-            a2 += w[2 * len + i] * d;
+        if (i0 < len) {
+            const float* b = buf(line);
+            const double anchor = (double)b[lines::at(kForward ? 0 : n - 1) * ES];
+            for (int t = lane; t < pc.hi - pc.lo; t += 32) {
+                const int l = kForward ? pc.lo + t : pc.hi - 1 - t;
+                const int i = i0 + t;
+                if (i < len) {
+                    const double d = (double)b[(pc.q * lines::kSegStride + l) * ES] - anchor;
+                    a0 += w[i] * d;
+                    a1 += w[len + i] * d;
+                    a2 += w[2 * len + i] * d;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+                a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+                a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+            }
         }
-        double* q = partial + ((size_t)line * ns + j) * 3;
-        q[0] = a0;
-        q[1] = a1;
-        q[2] = a2;
+        if (lane == 0) {
+            double* q = partial + ((size_t)line * ns + j) * 3;
+            q[0] = a0;
+            q[1] = a1;
+            q[2] = a2;
+        }
     }
     __syncthreads();
     for (int line = threadIdx.x; line < L; line += blockDim.x) {
@@ -635,8 +656,8 @@ __device__ void reflected_starts(Buf buf, int L, int n, const double* w, int len
     __syncthreads();
 }
 
-// Rows: every recursive component, left to right, end block, right to left, into its
-// row-filtered plane.
+// Rows: every component into its row-filtered plane (recursive: left to right, end
+// block, right to left; FIR: reflect taps in FP64).
 __global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) dir_rows_smem_kernel(const __grid_constant__ DirBlurParams p) {
     extern __shared__ __align__(16) unsigned char dsm[];
     const int ch = blockIdx.y;
@@ -647,16 +668,37 @@ __global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) dir_rows_smem_kerne
     double* exits = reinterpret_cast<double*>(dsm);
     double* entry = exits + (size_t)kRowsPerCta * lines::segs(W) * 3;
     double* last = entry + (size_t)kRowsPerCta * 3;
-    float* buf = reinterpret_cast<float*>(last + (size_t)kRowsPerCta * 3);
+    double* carry = last + (size_t)kRowsPerCta * 3;
+    float* buf = reinterpret_cast<float*>(carry + carry_doubles(kRowsPerCta, W));
     auto line = [&](int r) { return buf + (size_t)r * pw; };
     const float* raw = p.raw[ch];
     for (int k = 0; k < p.count; ++k) {
         const DirComponentDev& c = p.comp[k];
+        if (c.op == kDirOpFir) {
+            // reflect-boundary taps in FP64 over the densely staged rows
+            lines::load_rows_dense(buf, raw, W, row0, L, W);
+            const int rad = c.radius;
+            for (int r = 0; r < L; ++r) {
+                const float* row = buf + (size_t)r * W;
+                float* out = p.temp[ch][k] + (size_t)(row0 + r) * W;
+                for (int x = threadIdx.x; x < W; x += blockDim.x) {
+                    double sum = 0.0;
+                    if (x - rad >= 0 && x + rad < W)
+                        for (int o = -rad; o <= rad; ++o) sum += (double)row[x + o] * (double)c.taps[o + rad];
+                    else
+                        for (int o = -rad; o <= rad; ++o)
+                            sum += (double)row[reflect_dir(x + o, W)] * (double)c.taps[o + rad];
+                    out[x] = isfinite(sum) ? (float)sum : 0.0f;
+                }
+            }
+            __syncthreads();
+            continue;
+        }
         if (c.op != kDirOpYvv) continue;
         lines::load_rows(buf, raw, W, row0, L, W);
         reflected_starts<1, true>(line, L, W, c.h_init, c.h_len, exits, entry, false);
         const DirStep op(c);
-        lines::run_direction<1, true>(op, line, L, 0, W, entry, exits, last, false);
+        lines::run_direction<1, true>(op, line, L, 0, W, entry, exits, carry, last, false);
         const int ts = c.h_tsize;
         for (int r = threadIdx.x; r < L; r += blockDim.x) {
             double term[3] = {0.0, 0.0, 0.0};
@@ -667,7 +709,7 @@ __global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) dir_rows_smem_kerne
         }
         __syncthreads();
         if (W - ts > 0)
-            lines::run_direction<1, false>(op, line, L, 0, W - ts, entry, exits, (double*)nullptr, false);
+            lines::run_direction<1, false>(op, line, L, 0, W - ts, entry, exits, carry, (double*)nullptr, false);
         lines::store_rows(buf, p.temp[ch][k], row0, L, W);
     }
 }
@@ -687,7 +729,8 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) dir_cols_smem_kerne
     double* exits = reinterpret_cast<double*>(dsm);
     double* entry = exits + (size_t)kStripCols * lines::segs(H) * 3;
     double* last = entry + (size_t)kStripCols * 3;
-    float* work = reinterpret_cast<float*>(last + (size_t)kStripCols * 3);
+    double* carry = last + (size_t)kStripCols * 3;
+    float* work = reinterpret_cast<float*>(carry + carry_doubles(kStripCols, H));
     auto column = [&](int cc) { return work + cc; };
     const float* raw = p.raw[ch];
     __shared__ double terms[kStripCols][3];
@@ -709,7 +752,7 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) dir_cols_smem_kerne
         if (c.op == kDirOpYvv) {
             reflected_starts<kStripCols, false>(column, kStripCols, H, c.v_init, c.v_len, exits, entry, true);
             const DirStep op(c);
-            lines::run_direction<kStripCols, false>(op, column, kStripCols, 0, H, entry, exits, last, true);
+            lines::run_direction<kStripCols, false>(op, column, kStripCols, 0, H, entry, exits, carry, last, true);
             for (int cc = threadIdx.x; cc < kStripCols; cc += blockDim.x) {
                 double term[3] = {0.0, 0.0, 0.0};
                 end_block(c.v_term, ts, last + cc * 3, term);
@@ -720,7 +763,7 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) dir_cols_smem_kerne
             }
             __syncthreads();
             if (H - ts > 0)
-                lines::run_direction<kStripCols, true>(op, column, kStripCols, ts, H - ts, entry, exits,
+                lines::run_direction<kStripCols, true>(op, column, kStripCols, ts, H - ts, entry, exits, carry,
                                                        (double*)nullptr, true);
         }
         auto accumulate = [&](float blurred, float a) {
@@ -825,16 +868,16 @@ cudaError_t launch_dir_blur(const DirBlurParams& p, cudaStream_t stream) {
     const dim3 rows_grid((H + 31) / 32, seg_count(W), 3);
     const dim3 cols_grid((W + kLineThreads - 1) / kLineThreads, seg_count(H), 3);
     cudaError_t e = cudaSuccess;
-    if (fir) {
+    // whole rows / column strips in shared memory when they fit, else the global form
+    const size_t rs = rows_smem_bytes(W), cs = cols_smem_bytes(H);
+    const bool rows_on_chip = rs <= kSmemLimit, cols_on_chip = cs <= kSmemLimit;
+    if (fir && !rows_on_chip) {
         const dim3 block(32, 8);
         fjb::count_launch();
         dir_rows_fir_kernel<<<dim3((W + 31) / 32, (H + 7) / 8, 3), block, 0, stream>>>(p);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    // whole rows / column strips in shared memory when they fit, else the global form
-    const size_t rs = rows_smem_bytes(W), cs = cols_smem_bytes(H);
-    const bool rows_on_chip = rs <= kSmemLimit, cols_on_chip = cs <= kSmemLimit;
-    if (iir && rows_on_chip) {
+    if ((iir || fir) && rows_on_chip) {
         if ((e = cudaFuncSetAttribute(dir_rows_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rs)) !=
             cudaSuccess)
             return e;

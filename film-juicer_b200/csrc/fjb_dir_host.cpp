@@ -337,17 +337,18 @@ bool dir_plan_create(const FjSpatialDir& sd, int width, int height, cudaStream_t
                 c.ff = g.feedforward;
                 for (int k = 0; k < 3; ++k) c.fb[k] = g.feedback[k];
                 {
-                    // companion map (s0, s1, s2) -> (fb0 s0 + fb1 s1 + fb2 s2, s0, s1), kDirSeg steps
+                    // companion map (s0, s1, s2) -> (fb0 s0 + fb1 s1 + fb2 s2, s0, s1) over kDirSeg and 4 kDirSeg steps
                     const double m[9] = {c.fb[0], c.fb[1], c.fb[2], 1, 0, 0, 0, 1, 0};
                     double r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-                    for (int step = 0; step < kDirSeg; ++step) {
+                    for (int step = 1; step <= 4 * kDirSeg; ++step) {
                         double t[9];
                         for (int i = 0; i < 3; ++i)
                             for (int j = 0; j < 3; ++j)
                                 t[i * 3 + j] = m[i * 3] * r[j] + m[i * 3 + 1] * r[3 + j] + m[i * 3 + 2] * r[6 + j];
                         std::memcpy(r, t, sizeof(r));
+                        if (step == kDirSeg) std::memcpy(c.seg, r, sizeof(r));
                     }
-                    std::memcpy(c.seg, r, sizeof(r));
+                    std::memcpy(c.seg4, r, sizeof(r));
                 }
                 DirAxisBoundary hb, vb;
                 if (!dir_axis_boundary(g, width, hb, why) || !dir_axis_boundary(g, height, vb, why)) return false;

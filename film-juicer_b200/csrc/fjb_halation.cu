@@ -490,8 +490,9 @@ struct HalStep {
     using Real = float;
     float c0, c1, c2, c3;
     const double* seg;
+    const double* seg4;
     __device__ explicit HalStep(const OpticGauss& g)
-        : c0(g.yvv[0]), c1(g.yvv[1]), c2(g.yvv[2]), c3(g.yvv[3]), seg(g.seg) {}
+        : c0(g.yvv[0]), c1(g.yvv[1]), c2(g.yvv[2]), c3(g.yvv[3]), seg(g.seg), seg4(g.seg4) {}
     __device__ __forceinline__ float step(float x, float s[3]) const {
         if (kFactored) {
             s[0] += c0 * (x - s[0]);
@@ -506,6 +507,7 @@ struct HalStep {
         return v;
     }
     __device__ __forceinline__ const double* map() const { return seg; }
+    __device__ __forceinline__ const double* map4() const { return seg4; }
 };
 
 // Replicate start of each line from its first sample in processing order (position
@@ -526,28 +528,35 @@ __device__ __forceinline__ void replicate_starts(const OpticGauss& g, Buf buf, i
 // memory: kFirstForward runs ascending positions first (rows: left to right, then
 // back), else descending first (columns: bottom-up, then top-down).
 template <int ES, bool kFirstForward, bool kFactored, typename Buf>
-__device__ __forceinline__ void yvv_lines(const OpticGauss& g, Buf buf, int L, int n, float* exits, float* entry) {
+__device__ __forceinline__ void yvv_lines(const OpticGauss& g, Buf buf, int L, int n, float* exits, double* carry,
+                                          float* entry) {
     const HalStep<kFactored> op(g);
     replicate_starts<ES>(g, buf, L, kFirstForward ? 0 : n - 1, entry);
-    lines::run_direction<ES, kFirstForward>(op, buf, L, 0, n, entry, exits, (float*)nullptr, ES != 1);
+    lines::run_direction<ES, kFirstForward>(op, buf, L, 0, n, entry, exits, carry, (float*)nullptr, ES != 1);
     replicate_starts<ES>(g, buf, L, kFirstForward ? n - 1 : 0, entry);
-    lines::run_direction<ES, !kFirstForward>(op, buf, L, 0, n, entry, exits, (float*)nullptr, ES != 1);
+    lines::run_direction<ES, !kFirstForward>(op, buf, L, 0, n, entry, exits, carry, (float*)nullptr, ES != 1);
 }
 
+// Dynamic shared memory: scan carries (doubles) first, then the lines, exit states and
+// entry states (floats).
+__host__ __device__ inline size_t carry_doubles(int L, int n) { return (size_t)L * lines::scan_chunks(lines::segs(n)) * 3; }
+
 size_t rows_smem_bytes(int W) {
-    return ((size_t)kRowsPerCta * lines::padded(W) + (size_t)kRowsPerCta * lines::segs(W) * 3 +
+    return carry_doubles(kRowsPerCta, W) * sizeof(double) +
+           ((size_t)kRowsPerCta * lines::padded(W) + (size_t)kRowsPerCta * lines::segs(W) * 3 +
             (size_t)kRowsPerCta * 3) *
-           sizeof(float);
+               sizeof(float);
 }
 
 size_t cols_smem_bytes(int H) {
-    return ((size_t)kStripCols * lines::padded(H) + (size_t)kStripCols * lines::segs(H) * 3 +
+    return carry_doubles(kStripCols, H) * sizeof(double) +
+           ((size_t)kStripCols * lines::padded(H) + (size_t)kStripCols * lines::segs(H) * 3 +
             (size_t)kStripCols * 3) *
-           sizeof(float);
+               sizeof(float);
 }
 
-// Rows: every recursive Gaussian of the job, left to right then right to left, into
-// its row-filtered plane.
+// Rows: every Gaussian of the job into its row-filtered plane (recursive: left to
+// right then right to left; FIR: reflect taps).
 __global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) rows_smem_kernel(const __grid_constant__ OpticPass P) {
     extern __shared__ __align__(16) float sm[];
     const int job = blockIdx.y;
@@ -556,18 +565,38 @@ __global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) rows_smem_kernel(co
     const int row0 = blockIdx.x * kRowsPerCta;
     const int L = min(kRowsPerCta, H - row0);
     const int pw = lines::padded(W);
-    float* buf = sm;
+    double* carry = reinterpret_cast<double*>(sm);
+    float* buf = reinterpret_cast<float*>(carry + carry_doubles(kRowsPerCta, W));
     float* exits = buf + (size_t)kRowsPerCta * pw;
     float* entry = exits + (size_t)kRowsPerCta * lines::segs(W) * 3;
     auto line = [&](int r) { return buf + (size_t)r * pw; };
     for (int gi = 0; gi < J.count; ++gi) {
         const OpticGauss& g = J.g[gi];
+        if (g.kind == kGaussFir) {
+            // reflect-boundary taps over the densely staged rows
+            lines::load_rows_dense(buf, J.src, J.stride, row0, L, W);
+            const int rad = g.radius;
+            for (int r = 0; r < L; ++r) {
+                const float* row = buf + (size_t)r * W;
+                float* out = J.temp[gi] + (long long)(row0 + r) * W;
+                for (int x = threadIdx.x; x < W; x += blockDim.x) {
+                    float sum = 0.0f;
+                    if (x - rad >= 0 && x + rad < W)
+                        for (int o = -rad; o <= rad; ++o) sum += row[x + o] * g.w[o + rad];
+                    else
+                        for (int o = -rad; o <= rad; ++o) sum += row[reflect_half(x + o, W)] * g.w[o + rad];
+                    out[x] = sum;
+                }
+            }
+            __syncthreads();
+            continue;
+        }
         if (!is_yvv(g.kind)) continue;
         lines::load_rows(buf, J.src, J.stride, row0, L, W);
         if (g.kind == kGaussYvvFactored)
-            yvv_lines<1, true, true>(g, line, L, W, exits, entry);
+            yvv_lines<1, true, true>(g, line, L, W, exits, carry, entry);
         else
-            yvv_lines<1, true, false>(g, line, L, W, exits, entry);
+            yvv_lines<1, true, false>(g, line, L, W, exits, carry, entry);
         lines::store_rows(buf, J.temp[gi], row0, L, W);
     }
 }
@@ -585,7 +614,8 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) cols_smem_kernel(co
     const int x0 = blockIdx.x * kStripCols;
     const int C = min(kStripCols, W - x0);
     const int ph = lines::padded(H);
-    float* work = sm; // [padded(H)][kStripCols]
+    double* carry = reinterpret_cast<double*>(sm);
+    float* work = reinterpret_cast<float*>(carry + carry_doubles(kStripCols, H)); // [padded(H)][kStripCols]
     float* exits = work + (size_t)ph * kStripCols;
     float* entry = exits + (size_t)kStripCols * lines::segs(H) * 3;
     auto column = [&](int c) { return work + c; };
@@ -609,9 +639,9 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) cols_smem_kernel(co
         else if (g.kind != kGaussIdentity)
             lines::load_strip8(work, J.temp[gi], W, H, x0, C);
         if (g.kind == kGaussYvvFactored)
-            yvv_lines<kStripCols, false, true>(g, column, kStripCols, H, exits, entry);
+            yvv_lines<kStripCols, false, true>(g, column, kStripCols, H, exits, carry, entry);
         else if (g.kind == kGaussYvv)
-            yvv_lines<kStripCols, false, false>(g, column, kStripCols, H, exits, entry);
+            yvv_lines<kStripCols, false, false>(g, column, kStripCols, H, exits, carry, entry);
         const float coef = J.coef[gi];
         // running sum after this Gaussian, and the carrier value when it finishes the job
         auto running = [&](float v, float a) { return gi == 0 ? coef * v : a + coef * v; };
@@ -738,7 +768,7 @@ cudaError_t launch_optic_pass(const OpticPass& P, cudaStream_t stream) {
     // whole rows / column strips in shared memory when they fit, else the global form
     const size_t rs = rows_smem_bytes(W), cs = cols_smem_bytes(H);
     const bool rows_on_chip = rs <= kSmemLimit, cols_on_chip = cs <= kSmemLimit;
-    if (anyYvv && rows_on_chip) {
+    if ((anyYvv || anyFir) && rows_on_chip) {
         if ((e = cudaFuncSetAttribute(rows_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rs)) !=
             cudaSuccess)
             return e;
@@ -762,7 +792,7 @@ cudaError_t launch_optic_pass(const OpticPass& P, cudaStream_t stream) {
         rows_final_bwd_kernel<<<rows_grid, 32, 0, stream>>>(P);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    if (anyFir) {
+    if (anyFir && !rows_on_chip) {
         const dim3 block(32, 8);
         fjb::count_launch();
         rows_fir_kernel<<<dim3((W + 31) / 32, (H + 7) / 8, P.jobs), block, 0, stream>>>(P);

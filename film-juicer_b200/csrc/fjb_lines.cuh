@@ -10,10 +10,11 @@
 // (line, piece) pairs:
 //   partial : each piece runs from a zero state (the first from the line's entry
 //             state) and leaves its exit state;
-//   scan    : one thread per line turns the exit states into every piece's entry
-//             state: entry_1 = exit_0, entry_{j+1} = M entry_j + exit_j, with M the
-//             recursion's state map over kLineSeg steps (FP64), which is exact
-//             because every piece between the first and the last is full;
+//   scan    : the exit states become every piece's entry state: entry_1 = exit_0,
+//             entry_{j+1} = M entry_j + exit_j, with M the recursion's state map over
+//             kLineSeg steps (FP64), which is exact because every piece between the
+//             first and the last is full; evaluated in chunks of four pieces (local
+//             folds in parallel, a carry over chunks with M^4, then the fill-in);
 //   final   : each piece runs again from its entry state, writing in place.
 // In exact arithmetic this equals the sequential recursion; in floating point it
 // differs from it by rounding.
@@ -82,10 +83,19 @@ __device__ __forceinline__ void run_piece(const Step& op, float* line, Piece pc,
     }
 }
 
+// Entry states are carried in chunks of kScanChunk pieces; a line of ns pieces has
+// scan_chunks(ns) chunks (at least one).
+constexpr int kScanChunk = 4;
+__host__ __device__ __forceinline__ int scan_chunks(int ns) {
+    const int c = (ns - 1 + kScanChunk - 1) / kScanChunk;
+    return c > 0 ? c : 1;
+}
+
 // One direction over all L lines of the CTA. `Step` provides
 //   using Real;                               // state precision
 //   Real step(float x, Real s[3]) const;      // one sample, returns the output
 //   const double* map() const;                // 3x3 state map over kLineSeg steps
+//   const double* map4() const;               // the same over kScanChunk * kLineSeg steps
 // `buf(line)` returns the line's base pointer (element stride ES), `entry` holds each
 // line's entry state (L x 3), `exits` is scratch of L x segs(off + n) x 3 Real,
 // `last` receives each line's final state (may be null). The final pass writes the
@@ -96,7 +106,8 @@ __device__ __forceinline__ void run_piece(const Step& op, float* line, Piece pc,
 // function ends with a barrier.
 template <int ES, bool kForward, typename Step, typename Buf>
 __device__ void run_direction(const Step& op, Buf buf, int L, int off, int n, const typename Step::Real* entry,
-                              typename Step::Real* exits, typename Step::Real* last, bool line_fastest) {
+                              typename Step::Real* exits, double* carry, typename Step::Real* last,
+                              bool line_fastest) {
     using Real = typename Step::Real;
     const int ns = range_pieces(off, n);
     const int tasks = L * ns;
@@ -120,28 +131,76 @@ __device__ void run_direction(const Step& op, Buf buf, int L, int off, int n, co
         e[2] = s[2];
     }
     __syncthreads();
-    // scan
+    // scan, in chunks of kScanChunk entries: (A) each chunk with a successor folds its
+    // exit states from zero, (B) one thread per line carries the chunk entry states
+    // with the kScanChunk-piece map, (C) each chunk writes its entry states
     const double* M = op.map();
+    const double* M4 = op.map4();
+    const int nch = scan_chunks(ns);
+    for (int task = threadIdx.x; task < L * nch; task += blockDim.x) {
+        const int line = task % L, c = task / L;
+        if (c >= nch - 1) continue;
+        const Real* e = exits + (size_t)line * ns * 3;
+        double a = 0.0, b = 0.0, d = 0.0;
+#pragma unroll
+        for (int t = 0; t < kScanChunk; ++t) {
+            const int j = 1 + c * kScanChunk + t; // a full chunk: j <= ns - 2
+            const double na = (M[0] * a + M[1] * b) + (M[2] * d + (double)e[j * 3]);
+            const double nb = (M[3] * a + M[4] * b) + (M[5] * d + (double)e[j * 3 + 1]);
+            const double nd = (M[6] * a + M[7] * b) + (M[8] * d + (double)e[j * 3 + 2]);
+            a = na;
+            b = nb;
+            d = nd;
+        }
+        double* q = carry + ((size_t)line * nch + c) * 3;
+        q[0] = a;
+        q[1] = b;
+        q[2] = d;
+    }
+    __syncthreads();
     for (int line = threadIdx.x; line < L; line += blockDim.x) {
-        if (ns < 2) continue;
+        const Real* e = exits + (size_t)line * ns * 3;
+        double a = e[0], b = e[1], d = e[2]; // entry of piece 1 = exit of piece 0
+        for (int c = 0; c < nch; ++c) {
+            double* q = carry + ((size_t)line * nch + c) * 3;
+            const double la = q[0], lb = q[1], ld = q[2];
+            q[0] = a;
+            q[1] = b;
+            q[2] = d;
+            if (c + 1 < nch) {
+                const double na = (M4[0] * a + M4[1] * b) + (M4[2] * d + la);
+                const double nb = (M4[3] * a + M4[4] * b) + (M4[5] * d + lb);
+                const double nd = (M4[6] * a + M4[7] * b) + (M4[8] * d + ld);
+                a = na;
+                b = nb;
+                d = nd;
+            }
+        }
+    }
+    __syncthreads();
+    for (int task = threadIdx.x; task < L * nch; task += blockDim.x) {
+        const int line = task % L, c = task / L;
         Real* e = exits + (size_t)line * ns * 3;
-        double a = e[0], b = e[1], c = e[2];
-        for (int j = 1; j < ns; ++j) {
-            double za = 0.0, zb = 0.0, zc = 0.0;
+        const double* q = carry + ((size_t)line * nch + c) * 3;
+        double a = q[0], b = q[1], d = q[2];
+        for (int t = 0; t < kScanChunk; ++t) {
+            const int j = 1 + c * kScanChunk + t;
+            if (j >= ns) break;
+            double za = 0.0, zb = 0.0, zd = 0.0;
             if (j < ns - 1) {
                 za = e[j * 3];
                 zb = e[j * 3 + 1];
-                zc = e[j * 3 + 2];
+                zd = e[j * 3 + 2];
             }
             e[j * 3] = (Real)a;
             e[j * 3 + 1] = (Real)b;
-            e[j * 3 + 2] = (Real)c;
-            const double na = M[0] * a + M[1] * b + M[2] * c + za;
-            const double nb = M[3] * a + M[4] * b + M[5] * c + zb;
-            const double nc = M[6] * a + M[7] * b + M[8] * c + zc;
+            e[j * 3 + 2] = (Real)d;
+            const double na = (M[0] * a + M[1] * b) + (M[2] * d + za);
+            const double nb = (M[3] * a + M[4] * b) + (M[5] * d + zb);
+            const double nd = (M[6] * a + M[7] * b) + (M[8] * d + zd);
             a = na;
             b = nb;
-            c = nc;
+            d = nd;
         }
     }
     __syncthreads();
@@ -181,6 +240,28 @@ __device__ __forceinline__ void load_rows(float* dst, const float* src, long lon
         const unsigned base = (unsigned)__cvta_generic_to_shared(dst + (size_t)r * pw);
         for (int x = threadIdx.x; x < W; x += blockDim.x)
             asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(base + 4u * (unsigned)at(x)), "l"(row + x));
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    __syncthreads();
+}
+
+// Stages rows [row0, row0 + L) densely (row r at dst + r * W) for stencils along the
+// rows: 16-byte cp.async copies when rows and the plane are 16-byte aligned, else
+// 4-byte ones. Ends with a barrier.
+__device__ __forceinline__ void load_rows_dense(float* dst, const float* src, long long stride, int row0, int L,
+                                                int W) {
+    const bool vec = W % 4 == 0 && stride % 4 == 0 && (reinterpret_cast<uintptr_t>(src) & 15u) == 0;
+    for (int r = 0; r < L; ++r) {
+        const float* row = src + (long long)(row0 + r) * stride;
+        const unsigned base = (unsigned)__cvta_generic_to_shared(dst + (size_t)r * W);
+        if (vec) {
+            for (int x = 4 * threadIdx.x; x < W; x += 4 * blockDim.x)
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(base + 4u * (unsigned)x), "l"(row + x));
+        } else {
+            for (int x = threadIdx.x; x < W; x += blockDim.x)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(base + 4u * (unsigned)x), "l"(row + x));
+        }
     }
     asm volatile("cp.async.commit_group;\n" ::);
     asm volatile("cp.async.wait_group 0;\n" ::);

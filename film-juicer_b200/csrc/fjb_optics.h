@@ -24,6 +24,7 @@ struct OpticGauss {
     float w[19];  // FIR weights, w[radius] is the centre tap
     float yvv[4]; // legacy: B, B1, B2, B3; factored: h, g, t, 0
     double seg[9]; // recursive kinds: the state map over kOpticSeg zero-input steps (row-major 3x3)
+    double seg4[9]; // the same over 4 kOpticSeg steps
 };
 
 enum OpticMode : int { kOpticScatter = 0, kOpticBounce = 1 };

@@ -73,13 +73,14 @@ void segment_map(OpticGauss& g) {
         return;
     }
     double r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-    for (int step = 0; step < kOpticSeg; ++step) {
+    for (int step = 1; step <= 4 * kOpticSeg; ++step) {
         double t[9];
         for (int i = 0; i < 3; ++i)
             for (int j = 0; j < 3; ++j) t[i * 3 + j] = m[i * 3] * r[j] + m[i * 3 + 1] * r[3 + j] + m[i * 3 + 2] * r[6 + j];
         std::memcpy(r, t, sizeof(r));
+        if (step == kOpticSeg) std::memcpy(g.seg, r, sizeof(r));
     }
-    std::memcpy(g.seg, r, sizeof(r));
+    std::memcpy(g.seg4, r, sizeof(r));
 }
 
 } // namespace
