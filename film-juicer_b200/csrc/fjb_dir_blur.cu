@@ -581,77 +581,80 @@ struct DirStep {
 
 __host__ __device__ inline size_t carry_doubles(int L, int n) { return (size_t)L * lines::scan_chunks(lines::segs(n)) * 3; }
 
+// Exit states of the pieces (L x segs x 3), also the reduction scratch of the
+// reflected starts (warps x ceil(L / 4) x 12) for blocks of up to `threads` threads.
+__host__ __device__ inline size_t exits_doubles(int L, int n, int threads) {
+    const size_t e = (size_t)L * lines::segs(n) * 3, r = (size_t)(threads / 32) * ((L + 3) / 4) * 12;
+    return e > r ? e : r;
+}
+
 size_t rows_smem_bytes(int W) {
     return (size_t)kRowsPerCta * lines::padded(W) * sizeof(float) +
-           ((size_t)kRowsPerCta * lines::segs(W) * 3 + (size_t)kRowsPerCta * 6 + carry_doubles(kRowsPerCta, W)) *
+           (exits_doubles(kRowsPerCta, W, kRowsThreads) + (size_t)kRowsPerCta * 6 + carry_doubles(kRowsPerCta, W)) *
                sizeof(double);
 }
 
 size_t cols_smem_bytes(int H) {
     return (size_t)kStripCols * lines::padded(H) * sizeof(float) +
-           ((size_t)kStripCols * lines::segs(H) * 3 + (size_t)kStripCols * 6 + carry_doubles(kStripCols, H)) *
+           (exits_doubles(kStripCols, H, kColsThreads) + (size_t)kStripCols * 6 + carry_doubles(kStripCols, H)) *
                sizeof(double);
 }
 
 // Reflected start of each line: anchor + sum_i w_h[i] (x_i - anchor) over the first
-// `len` samples in processing order (i counts from the first sample processed). One
-// warp per (line, piece) task sums the piece's samples (lanes striding the piece, a
-// fixed-order FP64 butterfly across lanes); then one thread per line adds the pieces in
-// order. Pieces past the window hold zero.
+// `len` samples in processing order (i counts from the first sample processed). The
+// sums run sample-major: a thread takes samples i (strided by the block) for a group of
+// four lines, so each weight is read once per group; partial sums are reduced across
+// each warp (fixed butterfly order) and then across warps in warp order, in FP64.
+// `red` is scratch of (blockDim / 32) x ceil(L / 4) x 12 doubles.
 template <int ES, bool kForward, typename Buf>
-__device__ void reflected_starts(Buf buf, int L, int n, const double* w, int len, double* partial, double* entry,
-                                 bool line_fastest) {
-    const int ns = lines::range_pieces(0, n);
-    const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    for (int task = threadIdx.x >> 5; task < L * ns; task += nwarps) {
-        const int line = line_fastest ? task % L : task / ns;
-        const int j = line_fastest ? task / L : task - line * ns;
-        const lines::Piece pc = lines::piece<kForward>(0, n, j);
-        const int base = pc.q * lines::kLineSeg;
-        // processing-order index of the piece's first sample
-        const int i0 = kForward ? base + pc.lo : n - 1 - (base + pc.hi - 1);
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        if (i0 < len) {
-            const float* b = buf(line);
-            const double anchor = (double)b[lines::at(kForward ? 0 : n - 1) * ES];
-            for (int t = lane; t < pc.hi - pc.lo; t += 32) {
-                const int l = kForward ? pc.lo + t : pc.hi - 1 - t;
-                const int i = i0 + t;
-                if (i < len) {
-                    const double d = (double)b[(pc.q * lines::kSegStride + l) * ES] - anchor;
-                    a0 += w[i] * d;
-                    a1 += w[len + i] * d;
-                    a2 += w[2 * len + i] * d;
-                }
-            }
+__device__ void reflected_starts(Buf buf, int L, int n, const double* w, int len, double* red, double* entry) {
+    constexpr int G = 4;
+    const int groups = (L + G - 1) / G; // 1 or 2: lanes of equal parity share a group when 2
+    const int grp = threadIdx.x % groups;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int first = kForward ? 0 : n - 1;
+    double anchor[G], acc[G][3];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-                a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-                a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    for (int g = 0; g < G; ++g) {
+        const int line = grp * G + g;
+        anchor[g] = line < L ? (double)buf(line)[lines::at(first) * ES] : 0.0;
+        acc[g][0] = acc[g][1] = acc[g][2] = 0.0;
+    }
+    const int stride = blockDim.x / groups;
+    for (int i = threadIdx.x / groups; i < len; i += stride) {
+        const int idx = lines::at(kForward ? i : n - 1 - i) * ES;
+        const double w0 = w[i], w1 = w[len + i], w2 = w[2 * len + i];
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const int line = grp * G + g;
+            if (line < L) {
+                const double d = (double)buf(line)[idx] - anchor[g];
+                acc[g][0] += w0 * d;
+                acc[g][1] += w1 * d;
+                acc[g][2] += w2 * d;
             }
-        }
-        if (lane == 0) {
-            double* q = partial + ((size_t)line * ns + j) * 3;
-            q[0] = a0;
-            q[1] = a1;
-            q[2] = a2;
         }
     }
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+            for (int o = 16; o >= groups; o >>= 1) acc[g][r] += __shfl_xor_sync(0xffffffffu, acc[g][r], o);
+    if (lane < groups) {
+        double* q = red + ((size_t)warp * groups + lane) * (G * 3);
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) q[g * 3 + r] = acc[g][r];
+    }
     __syncthreads();
-    for (int line = threadIdx.x; line < L; line += blockDim.x) {
-        const float* b = buf(line);
-        const double anchor = (double)b[lines::at(kForward ? 0 : n - 1) * ES];
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        for (int j = 0; j < ns; ++j) {
-            const double* q = partial + ((size_t)line * ns + j) * 3;
-            a0 += q[0];
-            a1 += q[1];
-            a2 += q[2];
-        }
-        entry[line * 3] = anchor + a0;
-        entry[line * 3 + 1] = anchor + a1;
-        entry[line * 3 + 2] = anchor + a2;
+    const int nwarps = blockDim.x >> 5;
+    for (int t = threadIdx.x; t < L * 3; t += blockDim.x) {
+        const int line = t / 3, r = t - line * 3;
+        const int g = line / G, k = line - g * G;
+        double sum = 0.0;
+        for (int wi = 0; wi < nwarps; ++wi) sum += red[((size_t)wi * groups + g) * (G * 3) + k * 3 + r];
+        entry[t] = (double)buf(line)[lines::at(first) * ES] + sum;
     }
     __syncthreads();
 }
@@ -666,7 +669,7 @@ __global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) dir_rows_smem_kerne
     const int L = min(kRowsPerCta, H - row0);
     const int pw = lines::padded(W);
     double* exits = reinterpret_cast<double*>(dsm);
-    double* entry = exits + (size_t)kRowsPerCta * lines::segs(W) * 3;
+    double* entry = exits + exits_doubles(kRowsPerCta, W, kRowsThreads);
     double* last = entry + (size_t)kRowsPerCta * 3;
     double* carry = last + (size_t)kRowsPerCta * 3;
     float* buf = reinterpret_cast<float*>(carry + carry_doubles(kRowsPerCta, W));
@@ -696,7 +699,7 @@ __global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) dir_rows_smem_kerne
         }
         if (c.op != kDirOpYvv) continue;
         lines::load_rows(buf, raw, W, row0, L, W);
-        reflected_starts<1, true>(line, L, W, c.h_init, c.h_len, exits, entry, false);
+        reflected_starts<1, true>(line, L, W, c.h_init, c.h_len, exits, entry);
         const DirStep op(c);
         lines::run_direction<1, true>(op, line, L, 0, W, entry, exits, carry, last, false);
         const int ts = c.h_tsize;
@@ -727,7 +730,7 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) dir_cols_smem_kerne
     const int x0 = blockIdx.x * kStripCols;
     const int C = min(kStripCols, W - x0);
     double* exits = reinterpret_cast<double*>(dsm);
-    double* entry = exits + (size_t)kStripCols * lines::segs(H) * 3;
+    double* entry = exits + exits_doubles(kStripCols, H, kColsThreads);
     double* last = entry + (size_t)kStripCols * 3;
     double* carry = last + (size_t)kStripCols * 3;
     float* work = reinterpret_cast<float*>(carry + carry_doubles(kStripCols, H));
@@ -750,7 +753,7 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) dir_cols_smem_kerne
             lines::load_strip8(work, p.temp[ch][k], W, H, x0, C);
         const int ts = c.v_tsize;
         if (c.op == kDirOpYvv) {
-            reflected_starts<kStripCols, false>(column, kStripCols, H, c.v_init, c.v_len, exits, entry, true);
+            reflected_starts<kStripCols, false>(column, kStripCols, H, c.v_init, c.v_len, exits, entry);
             const DirStep op(c);
             lines::run_direction<kStripCols, false>(op, column, kStripCols, 0, H, entry, exits, carry, last, true);
             for (int cc = threadIdx.x; cc < kStripCols; cc += blockDim.x) {
