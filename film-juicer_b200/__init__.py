@@ -21,6 +21,15 @@ _lib = None
 
 _EXPORTS = {
     "fj_cuda_create": (abi.FjStatus, [C.POINTER(C.c_void_p), C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_scanner_post_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
+    "fjb_render_from_density_post": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjScannerPostEffects), C.c_uint64,
+                                                    C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                    C.c_void_p, C.c_ssize_t, C.c_void_p, C.c_ssize_t, C.c_int32,
+                                                    C.c_int32, C.c_uint32, C.c_void_p, C.c_size_t, C.c_void_p,
+                                                    C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_glare_seed": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_int32, C.c_int32]),
+    "fjb_gaussian_kernel_host": (abi.FjStatus, [C.c_int32, C.c_float, C.POINTER(C.c_float), C.c_size_t,
+                                                C.POINTER(abi.FjErrorBuffer)]),
     "fj_cuda_check_terminal": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
     "fj_cuda_inspect": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjFrame), C.POINTER(abi.FjCudaContext),
                                        C.POINTER(abi.FjErrorBuffer)]),

@@ -60,6 +60,7 @@ FJ_DIR_INACTIVE = 0
 FJ_DIR_NEGATIVE_DONOR_LANGMUIR = 1
 FJ_DIR_POSITIVE_RECEIVER_LANGMUIR = 2
 FJ_CORRECTION_ACTIVE = 1
+FJ_POST_GLARE = 1
 FJ_OUTPUT_SRGB = 0
 FJ_COLOR_ENCODE_CCTF = 1
 FJ_COLOR_INPUT_IS_OUTPUT_SPACE = 2

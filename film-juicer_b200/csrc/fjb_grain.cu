@@ -31,6 +31,7 @@
 
 #include "fjb_grain.h"
 #include "fjb_launches.h"
+#include "fjb_philox.cuh"
 
 namespace fjb {
 
@@ -96,34 +97,6 @@ __device__ __forceinline__ float value_noise(float cx, float cy, uint64_t seed) 
     const float v1 = __fmaf_rn(v11 - v01, sx, v01);
     return __fmaf_rn(v1 - v0, sy, v0);
 }
-
-// Philox4x32-10 (Salmon et al. 2011) in the openrand arrangement: key = seed hi/lo,
-// counter = {ctr0, ctr1, global seed, draw index}, first output word per draw.
-struct Philox {
-    uint32_t k0, k1, c0, c1, c2, n;
-    __device__ Philox(uint64_t seed, uint32_t ctr0, uint32_t global, uint32_t ctr1)
-        : k0((uint32_t)(seed >> 32)), k1((uint32_t)seed), c0(ctr0), c1(ctr1), c2(global), n(0) {}
-    __device__ __forceinline__ uint32_t next() {
-        uint32_t x0 = c0, x1 = c1, x2 = c2, x3 = n;
-        uint32_t a = k0, b = k1;
-#pragma unroll
-        for (int r = 0; r < 10; ++r) {
-            if (r > 0) {
-                a += 0x9E3779B9u;
-                b += 0xBB67AE85u;
-            }
-            const uint32_t hi0 = __umulhi(0xD2511F53u, x0), lo0 = 0xD2511F53u * x0;
-            const uint32_t hi1 = __umulhi(0xCD9E8D57u, x2), lo1 = 0xCD9E8D57u * x2;
-            const uint32_t y0 = hi1 ^ x1 ^ a, y2 = hi0 ^ x3 ^ b;
-            x0 = y0;
-            x1 = lo1;
-            x2 = y2;
-            x3 = lo0;
-        }
-        ++n;
-        return x0;
-    }
-};
 
 constexpr uint32_t kPhiloxGlobalSeed = 0xAAAAAAAAu;
 

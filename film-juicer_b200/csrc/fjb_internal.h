@@ -21,6 +21,8 @@ enum class PixelStage : int {
     DensityToOutput = 4,  // (grained) capture density planes -> encoded output
     SourceToDirSource = 5,  // source RGB -> spatial-DIR raw corrections + log exposure
     CarrierToDirSource = 6, // carrier planes -> spatial-DIR raw corrections + log exposure
+    DensityToLinearRgb = 7, // density planes -> linear output-RGB planes (+ glare), before encoding
+    LinearRgbToOutput = 8,  // linear output-RGB planes -> encoded output
 };
 
 cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStream_t stream);

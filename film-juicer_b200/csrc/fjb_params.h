@@ -140,6 +140,14 @@ struct PixelParams {
     int correction_active;
     float correction_slope;
     float correction_offset;
+    // scanner post effects: glare percent plane added in XYZ (may be null), the scan
+    // illuminant it is scaled by, and linear output-RGB planes written instead of the
+    // encoded pixels when the stage stops before encoding
+    const float* scan_glare;
+    float scan_illuminant_xyz[3];
+    float* lin_r;
+    float* lin_g;
+    float* lin_b;
 
     // ---- output colour ----
     float cat02[9];

@@ -10,7 +10,8 @@
 // :1891 focused_capture_film_density_kernel, :1944 scan_linear_density_rgb_kernel,
 // :1362 develop_print_density_kernel):
 //   Input  = source RGB(A) | carrier planes (B, G, R linear exposure) | density planes
-//   Output = encoded RGB(A) | capture density planes (C, M, Y)
+//   Output = encoded RGB(A) | capture density planes (C, M, Y) | linear output-RGB
+//            planes (for the scanner post effects, then encode_planes_kernel)
 #include <cuda_runtime.h>
 
 #include "fjb_internal.h"
@@ -20,7 +21,7 @@
 namespace fjb {
 
 enum InputKind : int { kInSource = 0, kInCarrier = 1, kInDensity = 2 };
-enum OutputKind : int { kOutEncoded = 0, kOutDensity = 1, kOutDirSource = 2 };
+enum OutputKind : int { kOutEncoded = 0, kOutDensity = 1, kOutDirSource = 2, kOutLinearRgb = 3 };
 
 // Spatial-DIR source (src/Cuda/Film/JuicerCudaFilmPipeline.cu:124-214): raw log
 // exposure, pre-DIR layer densities and the donor corrections they release.
@@ -135,6 +136,18 @@ __global__ void __launch_bounds__(kPixelThreads) pixel_chain_kernel(const __grid
         }
 
         double rgb[3];
+        if constexpr (Out == kOutLinearRgb) {
+            // src/Cuda/Scan/JuicerCudaScanPipeline.cu:1944-2037 scan_linear_density_rgb_kernel
+            const float glare = p.scan_glare ? p.scan_glare[idx] : -1.0f;
+            if (!scan_to_linear(p, d, rgb, glare)) {
+                flag_scan_failure(p);
+                rgb[0] = rgb[1] = rgb[2] = 0.0;
+            }
+            p.lin_r[idx] = (float)rgb[0];
+            p.lin_g[idx] = (float)rgb[1];
+            p.lin_b[idx] = (float)rgb[2];
+            continue;
+        }
         float* dstPix = reinterpret_cast<float*>(p.dst + (long long)y * p.dst_row_bytes) + (long long)x * p.components;
         if (!scan_to_linear(p, d, rgb)) {
             flag_scan_failure(p);
@@ -149,6 +162,28 @@ __global__ void __launch_bounds__(kPixelThreads) pixel_chain_kernel(const __grid
         dstPix[1] = (float)rgb[1];
         dstPix[2] = (float)rgb[2];
         if (p.components == 4) dstPix[3] = srcPix ? srcPix[3] : 1.0f;
+    }
+}
+
+// Encoding of linear output-RGB planes (src/Cuda/Scan/JuicerCudaScanPipeline.cu:2096-2182
+// focused_scan_output_encode_kernel, without gate defects and weave).
+__global__ void __launch_bounds__(kPixelThreads) encode_planes_kernel(const __grid_constant__ PixelParams p) {
+    const long long total = (long long)p.width * (long long)p.height;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
+        const int y = (int)(idx / p.width);
+        const int x = (int)(idx - (long long)y * p.width);
+        double rgb[3] = {(double)p.lin_r[idx], (double)p.lin_g[idx], (double)p.lin_b[idx]};
+        encode_output(p, rgb);
+        float* dstPix = reinterpret_cast<float*>(p.dst + (long long)y * p.dst_row_bytes) + (long long)x * p.components;
+        dstPix[0] = (float)rgb[0];
+        dstPix[1] = (float)rgb[1];
+        dstPix[2] = (float)rgb[2];
+        if (p.components == 4) {
+            const float* srcPix =
+                reinterpret_cast<const float*>(p.src + (long long)y * p.src_row_bytes) + (long long)x * p.components;
+            dstPix[3] = srcPix[3];
+        }
     }
 }
 
@@ -233,6 +268,13 @@ cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStrea
             return launch_variant<kInSource, kOutDirSource, false, false>(p, grid, smem, stream);
         case PixelStage::CarrierToDirSource:
             return launch_variant<kInCarrier, kOutDirSource, false, false>(p, grid, smem, stream);
+        case PixelStage::DensityToLinearRgb:
+            return print ? launch_variant<kInDensity, kOutLinearRgb, true, false>(p, grid, smem, stream)
+                         : launch_variant<kInDensity, kOutLinearRgb, false, false>(p, grid, smem, stream);
+        case PixelStage::LinearRgbToOutput:
+            fjb::count_launch();
+            encode_planes_kernel<<<grid, kPixelThreads, 0, stream>>>(p);
+            return cudaGetLastError();
         case PixelStage::DensityToOutput:
             return print ? launch_variant<kInDensity, kOutEncoded, true, false>(p, grid, smem, stream)
                          : launch_variant<kInDensity, kOutEncoded, false, false>(p, grid, smem, stream);

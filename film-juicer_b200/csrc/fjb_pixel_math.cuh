@@ -769,7 +769,9 @@ __device__ __forceinline__ void encode_output(const PixelParams& p, double rgb[3
 // failure (the pixel is then written as black).
 // (src/Cuda/Scan/JuicerCudaScanPipeline.cu:1757-1858)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool scan_to_linear(const PixelParams& p, const float d[3], double rgb[3]) {
+// glare: the scanner-glare percent of the pixel, or a negative value for none.
+__device__ __forceinline__ bool scan_to_linear(const PixelParams& p, const float d[3], double rgb[3],
+                                               float glare_percent = -1.0f) {
     double nd[3];
     for (int c = 0; c < 3; ++c) {
         if (p.scan_medium_negative) {
@@ -787,6 +789,13 @@ __device__ __forceinline__ bool scan_to_linear(const PixelParams& p, const float
         xyz[0] *= sc;
         xyz[1] *= sc;
         xyz[2] *= sc;
+    }
+    if (glare_percent >= 0.0f) {
+        // src/Cuda/Scan/JuicerCudaScanPipeline.cu:2018-2023
+        const double glare = (double)glare_percent * 0.01;
+        xyz[0] += glare * (double)p.scan_illuminant_xyz[0];
+        xyz[1] += glare * (double)p.scan_illuminant_xyz[1];
+        xyz[2] += glare * (double)p.scan_illuminant_xyz[2];
     }
     double ad[3];
     mat3_apply_d(p.cat02, xyz, ad);

@@ -405,6 +405,7 @@ bool create_recipe(const FjPreparedHostData& h, cudaStream_t stream, Recipe& r, 
             return false;
         }
         std::memcpy(p.cat02, oc.cat02, sizeof(p.cat02));
+        std::memcpy(p.scan_illuminant_xyz, oc.illuminant_xyz, sizeof(p.scan_illuminant_xyz));
         std::memcpy(p.xyz_to_rgb, oc.xyz_to_rgb, sizeof(p.xyz_to_rgb));
         p.gamut_active = (oc.flags & FJ_COLOR_GAMUT_COMPRESSION) ? 1 : 0;
         if (p.gamut_active) {

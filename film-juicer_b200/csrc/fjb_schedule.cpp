@@ -21,6 +21,7 @@
 #include "../../include/juicer_b200.h"
 #include "../../include/juicer_cuda_api.h"
 #include "fjb_diffusion.h"
+#include "fjb_scanner_post.h"
 #include "fjb_dir.h"
 #include "fjb_internal.h"
 #include "fjb_recipe.h"
@@ -47,6 +48,9 @@ struct FjCuda {
     uint64_t diffusion_spectrum_key = 0;
     float* diffusion_fft_work = nullptr;     // FFT form: transposed row spectra of the frame
     size_t diffusion_fft_work_bytes = 0;
+    float* post_taps = nullptr;              // scanner post-effect Gaussian taps of the last descriptor
+    size_t post_taps_bytes = 0;
+    uint64_t post_key = 0;
     // optional per-stage device timing (CUDA events on the render stream)
     bool timing = false;
     bool timing_events = false;
@@ -105,6 +109,10 @@ void release_all(FjCuda* cuda) {
     if (cuda->diffusion_fft_work) cudaFree(cuda->diffusion_fft_work);
     cuda->diffusion_fft_work = nullptr;
     cuda->diffusion_fft_work_bytes = 0;
+    if (cuda->post_taps) cudaFree(cuda->post_taps);
+    cuda->post_taps = nullptr;
+    cuda->post_taps_bytes = 0;
+    cuda->post_key = 0;
     stage_events_release(cuda);
 }
 
@@ -201,10 +209,8 @@ bool stages_supported(const FjPreparedHostData& h, std::string& why) {
         why = "highlight boost is not supported by this build";
         return false;
     }
-    if (h.scanner_post.flags != 0) {
-        why = "scanner post effects (glare, lens blur, unsharp) are not supported by this build";
-        return false;
-    }
+    fjb::PostPlan post;
+    if (!fjb::post_plan_from(h.scanner_post, post, why)) return false;
     if (h.effects.flags & (FJ_EFFECTS_FILM | FJ_EFFECTS_GATE_OUTPUT)) {
         why = "film and gate defects are not supported by this build";
         return false;
@@ -257,10 +263,12 @@ FjStatus ensure_noise(FjCuda* cuda, const FjStaticNoise& n, void* stream, const 
 FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData& h, const float* src, ptrdiff_t srb,
                        float* dst, ptrdiff_t drb, int width, int height, uint32_t comps, void* vs,
                        const FjAbortCallback& abort_cb, bool camera_diffusion, bool halation, bool spatial_dir,
-                       bool grain, FjErrorBuffer* error) {
+                       bool grain, const fjb::PostPlan& post, uint64_t glare_seed, int glare_x, int glare_y,
+                       FjErrorBuffer* error) {
     const size_t plane = (size_t)width * (size_t)height;
     const size_t plane_bytes = (plane * sizeof(float) + 255) / 256 * 256;
     size_t scratch = 0;
+    if (post.active) scratch = std::max(scratch, fjb_scanner_post_scratch_bytes(width, height));
     if (halation) scratch = std::max(scratch, fjb_scatter_halation_scratch_bytes(width, height));
     if (spatial_dir) scratch = std::max(scratch, fjb_spatial_dir_scratch_bytes(width, height));
     if (grain) scratch = std::max(scratch, fjb_visual_grain_scratch_bytes(width, height));
@@ -410,6 +418,28 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
         stage_end(cuda, FJB_STAGE_GRAIN, vs);
         if (st.category != FJ_STATUS_SUCCESS) return st;
         if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
+    }
+    if (post.active) {
+        // scanner post effects: taps kept on the device per descriptor
+        const std::vector<float> taps = fjb::post_taps(post);
+        if (cuda->post_key != h.scanner_post.hash || (!taps.empty() && !cuda->post_taps)) {
+            cuda->post_key = 0;
+            if (!taps.empty()) {
+                e = ensure_buffer(cuda->post_taps, cuda->post_taps_bytes, taps.size() * sizeof(float));
+                // pageable source: the copy is staged before the call returns
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(cuda->post_taps, taps.data(), taps.size() * sizeof(float),
+                                        cudaMemcpyHostToDevice, reinterpret_cast<cudaStream_t>(vs));
+                if (e != cudaSuccess) return fjb::cuda_status(e, error, "scanner post taps");
+            }
+            cuda->post_key = h.scanner_post.hash;
+        }
+        stage_begin(cuda, FJB_STAGE_PRINT_SCAN_OUTPUT, vs);
+        st = fjb::render_from_density_post(recipe, post, glare_seed, glare_x, glare_y, density[0], density[1],
+                                           density[2], comps == 4 ? src : nullptr, srb, dst, drb, width, height, comps,
+                                           scratch_p, cuda->post_taps, reinterpret_cast<cudaStream_t>(vs), error);
+        stage_end(cuda, FJB_STAGE_PRINT_SCAN_OUTPUT, vs);
+        return st;
     }
     stage_begin(cuda, FJB_STAGE_PRINT_SCAN_OUTPUT, vs);
     st = fjb_render_from_density(recipe, density[0], density[1], density[2], comps == 4 ? src : nullptr, srb, dst, drb,
@@ -600,14 +630,27 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
         const bool halation = (optics & FJ_OPTICS_SCATTER_HALATION) != 0;
         const bool spatial_dir = prepared->spatial_dir.component_count > 0;
         const bool grain = (prepared->grain.flags & FJ_GRAIN_ACTIVE) != 0;
-        if (!camera_diffusion && !halation && !spatial_dir && !grain) {
+        fjb::PostPlan post;
+        {
+            std::string why;
+            if (!fjb::post_plan_from(prepared->scanner_post, post, why)) {
+                out.status = fjb::fail_status(FJ_STATUS_PREPARATION_FAILURE, error, why);
+                return out;
+            }
+        }
+        if (!camera_diffusion && !halation && !spatial_dir && !grain && !post.active) {
             // Monolithic: one fused pass source -> output
             stage_begin(cuda, FJB_STAGE_MONOLITHIC, vs);
             st = fjb_render_pixels(recipe, src, srb, dst, drb, width, height, comps, vs, error);
             stage_end(cuda, FJB_STAGE_MONOLITHIC, vs);
         } else {
+            // the glare noise is keyed by the recipe, the frame token and the source origin
+            // (src/Cuda/JuicerCudaExecutor.cpp:2416-2420)
+            const uint64_t seed = fjb::glare_seed(prepared->recipe_hash, submission ? submission->frame_token : 0,
+                                                  frame->source.bounds.x1, frame->source.bounds.y1);
             st = render_staged(cuda, recipe, *prepared, src, srb, dst, drb, width, height, comps, vs, abort_callback,
-                               camera_diffusion, halation, spatial_dir, grain, error);
+                               camera_diffusion, halation, spatial_dir, grain, post, seed, frame->source.bounds.x1,
+                               frame->source.bounds.y1, error);
         }
         if (st.category != FJ_STATUS_SUCCESS) {
             cudaStreamSynchronize(stream);

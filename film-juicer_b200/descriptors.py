@@ -100,3 +100,31 @@ def diffusion_record(pixel_size_um: float, width: int, *, family: int = 2, scatt
     d.radius_px = max(1, int(round(radius_fraction_of_width * width)))
     d.sample_hash = d.hash = 1
     return d
+
+
+def scanner_post_record(*, glare_percent: float = 0.0, glare_roughness: float = 0.4, glare_blur_sigma_px: float = 0.0,
+                        glare_blur_radius: int = 0, lens_blur_sigma_px: float = 0.0, lens_blur_radius: int = 0,
+                        unsharp_sigma_px: float = 0.0, unsharp_radius: int = 0, unsharp_amount: float = 0.0,
+                        hash: int = 0x5C9E7):
+    """FjScannerPostEffects as the host projects it (rust/film-juicer-plugin/src/cuda/
+    projection.rs:336-352): glare on when its percent is positive; each blur on when its
+    sigma is positive; the record is active when its hash is non-zero. Radii default to
+    the 4 sigma + 0.5 rule when not given."""
+    from . import abi
+
+    def radius(sigma, r):
+        return r if r > 0 else (int(4.0 * sigma + 0.5) if sigma > 0 else 0)
+
+    p = abi.FjScannerPostEffects()
+    p.flags = abi.FJ_POST_GLARE if glare_percent > 0 else 0
+    p.glare_percent = glare_percent
+    p.glare_roughness = glare_roughness
+    p.glare_blur_sigma_px = glare_blur_sigma_px
+    p.glare_blur_radius = radius(glare_blur_sigma_px, glare_blur_radius)
+    p.lens_blur_sigma_px = lens_blur_sigma_px
+    p.lens_blur_radius = radius(lens_blur_sigma_px, lens_blur_radius)
+    p.unsharp_sigma_px = unsharp_sigma_px
+    p.unsharp_radius = radius(unsharp_sigma_px, unsharp_radius)
+    p.unsharp_amount = unsharp_amount
+    p.hash = hash
+    return p

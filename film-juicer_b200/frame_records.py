@@ -19,9 +19,11 @@ class FrameRecord:
     def __init__(self, recipe: "prepare.PreparedRecipe", width: int, height: int, *, recipe_hash: int = 0x5EED,
                  diffusion: bool = True, halation: bool = True, spatial_dir: bool = True, grain: bool = True,
                  auto_exposure: bool = False, noise: "grain_plan.Noise | None" = None,
-                 pixel_size_um: float | None = None, frame_time: float = 0.0, descriptor_width: int | None = None):
+                 pixel_size_um: float | None = None, frame_time: float = 0.0, descriptor_width: int | None = None,
+                 post=None):
         """descriptor_width: the frame width the pixel size and diffusion radius are
-        derived for (defaults to `width`; a crop of a larger frame passes the full width)."""
+        derived for (defaults to `width`; a crop of a larger frame passes the full width);
+        post: an FjScannerPostEffects record (descriptors.scanner_post_record)."""
         self.width, self.height = width, height
         dw = descriptor_width or width
         self.pixel_size_um = pixel_size_um or 35000.0 / dw
@@ -44,6 +46,8 @@ class FrameRecord:
         h.optics.flags = flags
         if spatial_dir:
             h.spatial_dir = descriptors.spatial_dir_record(px, width, height)
+        if post is not None:
+            h.scanner_post = post
         self.noise = None
         if grain:
             a = recipe.arrays

@@ -317,7 +317,7 @@ class Owner:
     def __exit__(self, *exc):
         self.close()
 
-    def render(self, prepared, src, dst, window=None, stream=None, abort=None):
+    def render(self, prepared, src, dst, window=None, stream=None, abort=None, frame_token: int = 0):
         """src/dst: (H, W, comps) float32 CUDA tensors covering the full frame; returns
         the FjRenderOutcome (raises on a failed status)."""
         h, w, comps = src.shape
@@ -337,9 +337,31 @@ class Owner:
         ctx = abi.FjCudaContext()
         _check("fj_cuda_inspect", self.lib.fj_cuda_inspect(self.handle, C.byref(fr), C.byref(ctx), C.byref(err.buf)), err)
         sub = abi.FjSubmission()
+        sub.frame_token = frame_token
         query = abi.FjAbortQuery(abort or (lambda user: abi.FJ_ABORT_CONTINUE))
         cb = abi.FjAbortCallback(query, None)
         out = self.lib.fj_cuda_render(self.handle, C.byref(ctx), C.byref(fr), C.byref(sub), prepared.pointer(), cb,
                                       C.byref(err.buf))
         _check("fj_cuda_render", out.status, err)
         return out
+
+
+def render_from_density_post(recipe: "DeviceRecipe", post, seed: int, origin, density_cmy, dst, src=None,
+                             stream=None, scratch=None):
+    """fjb_render_from_density_post on CUDA tensors: density planes (C, M, Y) -> print ->
+    scan with scanner glare -> lens blur -> unsharp -> dst (H, W, comps)."""
+    torch = _torch()
+    lib = recipe.lib
+    h, w = density_cmy[0].shape
+    comps = dst.shape[2]
+    need = int(lib.fjb_scanner_post_scratch_bytes(w, h))
+    if scratch is None:
+        scratch = torch.empty(need // 4, dtype=torch.float32, device=dst.device)
+    err = abi.ErrorText()
+    st = lib.fjb_render_from_density_post(
+        recipe.handle, C.byref(post), seed, origin[0], origin[1], *[C.c_void_p(_ptr(t)) for t in density_cmy],
+        C.c_void_p(_ptr(src) if src is not None else 0), (src.stride(0) * 4) if src is not None else 0,
+        C.c_void_p(_ptr(dst)), dst.stride(0) * 4, w, h, comps, C.c_void_p(_ptr(scratch)), scratch.numel() * 4,
+        C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+    _check("fjb_render_from_density_post", st, err)
+    return scratch

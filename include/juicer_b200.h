@@ -76,6 +76,34 @@ FjStatus fjb_render_from_density(FjbRecipe* recipe, const float* density_c, cons
                                  ptrdiff_t dst_row_bytes, int32_t width, int32_t height, uint32_t components,
                                  void* stream, FjErrorBuffer* error);
 
+/* Scanner post effects (reference src/Cuda/Scan/JuicerCudaScanPipeline.cu:2982
+ * juicer_cuda_print_focused_scan_linear_density_rgb + :2586-2878 launch_focused_scanner_post_output,
+ * scheduled by src/Cuda/JuicerCudaExecutor.cpp:2384-2500): capture density planes ->
+ * (print) -> scan to linear output RGB with the glare percent plane added in XYZ ->
+ * lens blur -> unsharp mask -> encoded output. `post` is the prepared record
+ * (active when its hash is non-zero); `glare_seed` and the glare origin (the frame's
+ * source x1, y1) key the glare noise, see fjb_glare_seed. `scratch` holds
+ * fjb_scanner_post_scratch_bytes(width, height) bytes of device memory. */
+size_t fjb_scanner_post_scratch_bytes(int32_t width, int32_t height);
+FjStatus fjb_render_from_density_post(FjbRecipe* recipe, const FjScannerPostEffects* post, uint64_t glare_seed,
+                                      int32_t glare_origin_x, int32_t glare_origin_y, const float* density_c,
+                                      const float* density_m, const float* density_y, const float* src,
+                                      ptrdiff_t src_row_bytes, float* dst, ptrdiff_t dst_row_bytes, int32_t width,
+                                      int32_t height, uint32_t components, float* scratch, size_t scratch_bytes,
+                                      void* stream, FjErrorBuffer* error);
+
+/* Glare seed of a frame (reference src/Cuda/JuicerCudaExecutor.cpp:2416, src/Hash.h:50):
+ * FNV-1a 64 over the little-endian 8-byte words {recipe hash, frame token, source x1,
+ * source y1}. */
+uint64_t fjb_glare_seed(uint64_t recipe_hash, uint64_t frame_token, int32_t source_x1, int32_t source_y1);
+
+/* Normalised Gaussian taps w[0..2 radius] (replaces the host preparation callback
+ * FjHostPreparation.gaussian, native/juicer_cuda_call_scope.h:15, which the reference
+ * serves from rust/film-juicer-core/src/optics/gaussian.rs:18-59): radius 1..2048,
+ * sigma finite and positive; `count` >= 2 radius + 1. */
+FjStatus fjb_gaussian_kernel_host(int32_t radius, float sigma_px, float* weights, size_t count,
+                                  FjErrorBuffer* error);
+
 /* Camera auto-exposure metering (reference src/Cuda/JuicerCudaAutoExposure.cu:314-520,
  * run by src/Cuda/JuicerCudaExecutor.cpp:1013 meter_camera_exposure). `src` points at
  * pixel (meter->source_bounds.x1, .y1). Writes the float exposure scale 2^-log2(Y) to

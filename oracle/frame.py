@@ -16,7 +16,7 @@ class _Components:
         self.lambda_px, self.red_weights, self.green_weights, self.blue_weights = lam, w[0], w[1], w[2]
 
 
-def render_frame(frame_record, recipe, src, threads: int = 1):
+def render_frame(frame_record, recipe, src, threads: int = 1, frame_token: int = 0):
     """frame_record: film_juicer_b200.frame_records.FrameRecord; recipe: the
     PreparedRecipe it was built from; src: (H, W, comps) float32. Returns the encoded
     output (H, W, comps) and the error flags. `threads` parallelises the per-pixel
@@ -51,4 +51,8 @@ def render_frame(frame_record, recipe, src, threads: int = 1):
         base = [a["density_rgb"][:, c] for c in range(3)]
         noise = frame_record.noise.record if frame_record.noise is not None else None
         density = ograin.visual_grain(h.grain, noise, base, layers, h.capture_polarity == 1, density)
+    if h.scanner_post.hash != 0:
+        # scanner post effects; the source origin of these frames is (0, 0)
+        seed = orc.glare_seed(h.recipe_hash, frame_token, 0, 0)
+        return orc.render_post(host, h.scanner_post, seed, 0, 0, density, src=src, threads=threads)
     return orc.render(host, src, stage=2, planes=density, threads=threads)

@@ -59,7 +59,7 @@ typedef struct {
     float *lut_v, *lut_sc, *lut_sm, *lut_sy, *cell_lo, *cell_hi;
     int corr_active;
     float corr_slope, corr_offset;
-    float cat02[9], xyz_rgb[9];
+    float cat02[9], xyz_rgb[9], illum_xyz[3];
     int gamut;
     const float* cmax;
     float g_to_xyz[9], g_from_xyz[9], lknee[3], cknee[3];
@@ -605,8 +605,9 @@ static float enc(const Pack* p, float v) {
     }
 }
 
-/* :1700-1858: density -> encoded RGB; returns 0 on a scan failure */
-static int scan_out(const Pack* p, const float* D, double* rgb) {
+/* :1700-1840, :1944-2037: density -> linear output RGB (glare percent added in XYZ when
+ * glare >= 0); returns 0 on a scan failure */
+static int scan_lin(const Pack* p, const float* D, double* rgb, float glare) {
     double n[3];
     for (int c = 0; c < 3; ++c)
         n[c] = p->medium_negative ? ((double)D[c] + (double)p->min_cmy[c]) * (double)p->inv_cmy[c]
@@ -619,6 +620,10 @@ static int scan_out(const Pack* p, const float* D, double* rgb) {
         double s = cy / (xyz[1] + 1e-10);
         for (int c = 0; c < 3; ++c) xyz[c] *= s;
     }
+    if (glare >= 0.0f) {
+        double g = (double)glare * 0.01;
+        for (int c = 0; c < 3; ++c) xyz[c] += g * (double)p->illum_xyz[c];
+    }
     double ad[3];
     mat3d(p->cat02, xyz, ad);
     mat3d(p->xyz_rgb, ad, rgb);
@@ -629,11 +634,22 @@ static int scan_out(const Pack* p, const float* D, double* rgb) {
         if (!isfinite(f[0]) || !isfinite(f[1]) || !isfinite(f[2])) return 0;
         for (int c = 0; c < 3; ++c) rgb[c] = f[c];
     }
+    return 1;
+}
+
+/* :152 apply_output_encoding_device: linear output RGB -> encoded, clamped */
+static void encode_lin(const Pack* p, double* rgb) {
     double lin[3];
     if (p->enc_iso) memcpy(lin, rgb, sizeof(lin));
     else mat3d(p->dwg, rgb, lin);
     for (int c = 0; c < 3; ++c) rgb[c] = p->enc_cctf ? (double)enc(p, (float)lin[c]) : lin[c];
     for (int c = 0; c < 3; ++c) rgb[c] = clamp01(rgb[c]);
+}
+
+/* :1700-1858: density -> encoded RGB; returns 0 on a scan failure */
+static int scan_out(const Pack* p, const float* D, double* rgb) {
+    if (!scan_lin(p, D, rgb, -1.0f)) return 0;
+    encode_lin(p, rgb);
     return 1;
 }
 
@@ -741,6 +757,7 @@ static int pack(const FjPreparedHostData* h, Packed* out) {
     p->corr_offset = h->scanner_correction.xyz_offset;
     const FjOutputColor* oc = &h->output_color;
     memcpy(p->cat02, oc->cat02, 36);
+    memcpy(p->illum_xyz, oc->illuminant_xyz, 12);
     memcpy(p->xyz_rgb, oc->xyz_to_rgb, 36);
     p->gamut = (oc->flags & FJ_COLOR_GAMUT_COMPRESSION) != 0;
     p->cmax = oc->gamut_cmax.data;
@@ -2160,4 +2177,130 @@ int oracle_visual_grain(const FjVisualGrain* g, const FjStaticNoise* noise, cons
     }
     free(buf);
     return rc;
+}
+
+
+/* ---------------- scanner post effects (src/Cuda/Scan/JuicerCudaScanPipeline.cu:214-316,
+ * :318-446, :586-655, :1944-2037, :2096-2182, :2586-2878) ---------------- */
+
+/* taps of one blur of the record, or radius 0 when that blur is off */
+static int post_taps(int radius, float sigma, float** w) {
+    *w = NULL;
+    if (!(sigma > 0.0f)) return 0;
+    if (radius < 1 || radius > 2048 || !isfinite(sigma)) return -1;
+    *w = (float*)malloc(sizeof(float) * (size_t)(2 * radius + 1));
+    og_taps(radius, sigma, *w);
+    return radius;
+}
+
+/* separable blur, taps summed in order in FP64; unsharp: plane <- v + a (v - blurred) */
+static void post_blur(float* plane, float* tmp, int W, int H, const float* w, int r, int unsharp, float amount) {
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            double acc = 0.0;
+            for (int k = 0; k <= 2 * r; ++k)
+                acc += (double)plane[(size_t)y * W + og_reflect_half((long)x - r + k, W)] * (double)w[k];
+            tmp[(size_t)y * W + x] = isfinite(acc) ? (float)acc : 0.0f;
+        }
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            double acc = 0.0;
+            for (int k = 0; k <= 2 * r; ++k)
+                acc += (double)tmp[(size_t)og_reflect_half((long)y - r + k, H) * W + x] * (double)w[k];
+            float blurred = isfinite(acc) ? (float)acc : 0.0f;
+            size_t i = (size_t)y * W + x;
+            if (unsharp) {
+                double v0 = (double)plane[i], o = v0 + (double)amount * (v0 - (double)blurred);
+                plane[i] = isfinite(o) ? (float)o : 0.0f;
+            } else {
+                plane[i] = blurred;
+            }
+        }
+}
+
+/* density planes (C, M, Y) -> print -> scan to linear RGB with glare -> lens blur ->
+ * unsharp -> encoded dst. Returns 0, or -1 for a malformed record. */
+int oracle_render_post(const FjPreparedHostData* h, const FjScannerPostEffects* post, uint64_t seed, int ox, int oy,
+                       const float* dc, const float* dm, const float* dy, const float* src, long src_row_floats,
+                       int W, int H, int comps, float* dst, long dst_row_floats, int threads, unsigned* flags_out) {
+    if ((post->flags & ~1u) != 0) return -1;
+    Packed pk;
+    int rc = pack(h, &pk);
+    if (rc) {
+        free(pk.lut_store);
+        return rc;
+    }
+    const Pack* p = &pk.p;
+    size_t plane = (size_t)W * H;
+    float* lin = (float*)malloc(sizeof(float) * plane * 3);
+    float* tmp = (float*)malloc(sizeof(float) * plane);
+    float* glare = NULL;
+    float *gw = NULL, *lw = NULL, *uw = NULL;
+    int gr = 0, lr = 0, ur = 0;
+    int active = post->hash != 0;
+    if (active) {
+        lr = post_taps(post->lens_blur_radius, post->lens_blur_sigma_px, &lw);
+        ur = post_taps(post->unsharp_radius, post->unsharp_sigma_px, &uw);
+        gr = (post->flags & 1u) ? post_taps(post->glare_blur_radius, post->glare_blur_sigma_px, &gw) : 0;
+        if (lr < 0 || ur < 0 || gr < 0) {
+            free(lin), free(tmp), free(gw), free(lw), free(uw), free(pk.lut_store);
+            return -1;
+        }
+        if (!(isfinite(post->unsharp_amount) && post->unsharp_amount > 0.0f)) ur = 0;
+        if (isfinite(post->glare_percent) && post->glare_percent > 0.0f && isfinite(post->glare_roughness)) {
+            glare = (float*)malloc(sizeof(float) * plane);
+            float mean = fmaxf(0.0f, post->glare_percent), sd = fmaxf(0.0f, post->glare_roughness * post->glare_percent);
+            uint32_t medium = p->medium_negative ? 0u : 1u;
+            for (int y = 0; y < H; ++y)
+                for (int x = 0; x < W; ++x) {
+                    uint64_t ax = (uint64_t)((int64_t)ox + x), ay = (uint64_t)((int64_t)oy + y);
+                    OPhilox ph = {(uint32_t)(seed >> 32), (uint32_t)seed, (uint32_t)ax, (uint32_t)ay, medium, 0};
+                    float u1 = fmaf((float)og_philox(&ph), 1.0f / 4294967296.0f, 0.5f / 4294967296.0f);
+                    u1 = fminf(fmaxf(u1, 1e-7f), 1.0f);
+                    float u2 = fmaf((float)og_philox(&ph), 1.0f / 4294967296.0f, 0.5f / 4294967296.0f);
+                    float n = sqrtf(-2.0f * logf(u1)) * cosf(6.28318530717958647692f * u2);
+                    float m2 = mean * mean, s2 = sd * sd;
+                    float sig2 = logf(1.0f + (s2 / m2));
+                    float sig = sqrtf(fmaxf(0.0f, sig2));
+                    float mu = logf(fmaxf(1e-12f, mean)) - 0.5f * sig2;
+                    float g = expf(mu + sig * n);
+                    glare[(size_t)y * W + x] = isfinite(g) ? g : 0.0f;
+                }
+            if (gr > 0) post_blur(glare, tmp, W, H, gw, gr, 0, 0.0f);
+        }
+    }
+    unsigned flags = 0;
+#if defined(_OPENMP)
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threads > 0 ? threads : 1) reduction(| : flags)
+#endif
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            size_t i = (size_t)y * W + x;
+            float D[3] = {dc[i], dm[i], dy[i]};
+            if (p->print) print_stage(p, D);
+            double rgb[3];
+            if (!scan_lin(p, D, rgb, glare ? glare[i] : -1.0f)) {
+                flags |= 1u;
+                rgb[0] = rgb[1] = rgb[2] = 0.0;
+            }
+            for (int c = 0; c < 3; ++c) lin[c * plane + i] = (float)rgb[c];
+        }
+    for (int c = 0; c < 3 && lr > 0; ++c) post_blur(lin + c * plane, tmp, W, H, lw, lr, 0, 0.0f);
+    for (int c = 0; c < 3 && ur > 0; ++c) post_blur(lin + c * plane, tmp, W, H, uw, ur, 1, post->unsharp_amount);
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            size_t i = (size_t)y * W + x;
+            double rgb[3] = {(double)lin[i], (double)lin[plane + i], (double)lin[2 * plane + i]};
+            encode_lin(p, rgb);
+            float* o = dst + (size_t)y * dst_row_floats + (size_t)x * comps;
+            o[0] = (float)rgb[0];
+            o[1] = (float)rgb[1];
+            o[2] = (float)rgb[2];
+            if (comps == 4) o[3] = src ? src[(size_t)y * src_row_floats + (size_t)x * comps + 3] : 1.0f;
+        }
+    free(lin), free(tmp), free(glare), free(gw), free(lw), free(uw), free(pk.lut_store);
+    if (flags_out) *flags_out = flags;
+    return 0;
 }

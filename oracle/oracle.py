@@ -37,6 +37,11 @@ def load():
     lib.oracle_render.argtypes = [C.POINTER(abi.FjPreparedHostData), C.c_int, C.c_void_p, C.c_long, C.c_int,
                                   C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_float, C.c_int, C.POINTER(C.c_uint32)]
+    lib.oracle_render_post.restype = C.c_int
+    lib.oracle_render_post.argtypes = [C.POINTER(abi.FjPreparedHostData), C.POINTER(abi.FjScannerPostEffects),
+                                       C.c_uint64, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_long, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_int,
+                                       C.POINTER(C.c_uint32)]
     _lib = lib
     return lib
 
@@ -110,6 +115,12 @@ def load_reference():
     lib.ref_capture_density.restype = C.c_int
     lib.ref_capture_density.argtypes = [C.POINTER(abi.FjPreparedHostData), C.POINTER(C.c_void_p), C.c_void_p,
                                         C.c_long, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    if hasattr(lib, "ref_scanner_post"):
+        lib.ref_scanner_post.restype = C.c_int
+        lib.ref_scanner_post.argtypes = [C.POINTER(abi.FjPreparedHostData), C.POINTER(C.c_void_p),
+                                         C.POINTER(abi.FjScannerPostEffects), C.c_ulonglong, C.c_int, C.c_int,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p,
+                                         C.c_long, C.c_int, C.c_int, C.c_int]
     _ref = lib
     return lib
 
@@ -155,3 +166,36 @@ def auto_exposure(record, meter, src):
     v = fn(record.pointer(), C.byref(meter), C.c_void_p(src.ctypes.data), src.shape[1] * src.shape[2], src.shape[2],
            C.byref(ok))
     return float(v) if ok.value else None
+
+
+def glare_seed(recipe_hash: int, frame_token: int, x1: int, y1: int) -> int:
+    """FNV-1a 64 over the little-endian 8-byte words {recipe hash, frame token, x1, y1}
+    (src/Cuda/JuicerCudaExecutor.cpp:2416, src/Hash.h:50)."""
+    h = 0xcbf29ce484222325
+    for v in (recipe_hash, frame_token, x1, y1):
+        for b in (v & 0xFFFFFFFFFFFFFFFF).to_bytes(8, "little"):
+            h = ((h ^ b) * 0x100000001b3) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def render_post(record, post, seed: int, origin_x: int, origin_y: int, planes, src=None, threads: int = 1):
+    """Density planes (C, M, Y) -> print -> scan with scanner glare -> lens blur ->
+    unsharp -> encoded output (H, W, comps). Returns (result, flags)."""
+    import numpy as np
+
+    lib = load()
+    p = [np.ascontiguousarray(q, dtype=np.float32) for q in planes]
+    h, w = p[0].shape
+    comps = 3
+    if src is not None:
+        src = np.ascontiguousarray(src, dtype=np.float32)
+        comps = src.shape[2]
+    dst = np.zeros((h, w, comps), np.float32)
+    flags = C.c_uint32()
+    rc = lib.oracle_render_post(record.pointer(), C.byref(post), seed, origin_x, origin_y,
+                                *[C.c_void_p(q.ctypes.data) for q in p],
+                                C.c_void_p(src.ctypes.data if src is not None else 0), w * comps, w, h, comps,
+                                C.c_void_p(dst.ctypes.data), w * comps, threads, C.byref(flags))
+    if rc != 0:
+        raise RuntimeError(f"oracle_render_post failed with code {rc}")
+    return dst, int(flags.value)

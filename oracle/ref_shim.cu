@@ -594,3 +594,112 @@ extern "C" int ref_visual_grain(const FjVisualGrain* g, const FjStaticNoise* noi
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return (int)e;
 }
+
+// ---- scanner post effects with the reference's kernels ----
+extern "C" cudaError_t juicer_cuda_print_focused_scan_linear_density_rgb(
+    const JuicerCuda::PrintPipelineRunParams*, const float*, const float*, const float*, float*, float*, float*,
+    float*, float*, int, int, std::uint64_t, float, float, const float*, int, void*);
+extern "C" cudaError_t juicer_cuda_print_focused_continue_from_capture_density(
+    const JuicerCuda::PrintPipelineRunParams*, float*, float*, float*, const float*, void*);
+extern "C" cudaError_t juicer_cuda_print_focused_scanner_post_output(
+    const JuicerCuda::PrintPipelineRunParams*, float*, float*, float*, float*, const float*, int, const float*, int,
+    float, const JuicerCuda::FilmDefectsPayload*, const JuicerCuda::GateWeavePayload*, const float*, int, int, void*);
+
+namespace {
+// rust/film-juicer-core/src/optics/gaussian.rs:18-59 (the host callback's kernel)
+std::vector<float> ref_gaussian(int radius, float sigma_px) {
+    std::vector<float> w;
+    const double sigma = (double)sigma_px, s2 = sigma * sigma * 2.0;
+    double sum = 0.0;
+    for (int i = -radius; i <= radius; ++i) {
+        const double v = std::exp(-((double)i * (double)i) / s2);
+        w.push_back((float)v);
+        sum += v;
+    }
+    const double rec = sum != 0.0 ? 1.0 / sum : 0.0;
+    for (float& v : w) v = (float)((double)v * rec);
+    return w;
+}
+} // namespace
+
+// Density planes (device) -> print -> scan to linear RGB with glare -> lens blur ->
+// unsharp -> encoded dst (device), through the reference's launchers
+// (src/Cuda/Scan/JuicerCudaScanPipeline.cu:2982, :3106), scheduled as
+// src/Cuda/JuicerCudaExecutor.cpp:2384-2500 does for the materialized-density route.
+extern "C" int ref_scanner_post(const FjPreparedHostData* h, const float* const* lut, const FjScannerPostEffects* post,
+                                unsigned long long seed, int origin_x, int origin_y, const float* dc, const float* dm,
+                                const float* dy, const float* src, long src_row_bytes, float* dst, long dst_row_bytes,
+                                int width, int height, int comps) {
+    Arena a;
+    unsigned* d_flags = nullptr;
+    if (cudaMalloc(&d_flags, sizeof(unsigned)) != cudaSuccess) return 2;
+    cudaMemset(d_flags, 0, sizeof(unsigned));
+    a.ptrs.push_back(d_flags);
+    JuicerCuda::PipelineRunParams p;
+    if (!pack(*h, lut, a, p, d_flags)) return 1;
+    JuicerCuda::PrintPipelineRunParams q{};
+    q.src = src;
+    q.srcRowBytes = (size_t)src_row_bytes;
+    q.dst = dst;
+    q.dstRowBytes = (size_t)dst_row_bytes;
+    q.width = width;
+    q.height = height;
+    q.nComponents = comps;
+    q.filmExpose = p.filmExpose;
+    q.filmDevelop = p.filmDevelop;
+    q.printExpose = p.printExpose;
+    q.printDevelop = p.printDevelop;
+    q.scanStage = p.scanStage;
+    q.filmRaw = p.filmRaw;
+    const size_t plane = (size_t)width * (size_t)height;
+    float* buf = nullptr;
+    if (cudaMalloc(&buf, plane * 8 * sizeof(float)) != cudaSuccess) return 2;
+    a.ptrs.push_back(buf);
+    float *r = buf, *g = buf + plane, *b = buf + 2 * plane, *tmp = buf + 3 * plane, *blurred = buf + 4 * plane;
+    // the materialized-density route scans print densities: develop the print first
+    // (src/Cuda/JuicerCudaExecutor.cpp develop_print_capture -> :2908)
+    float *pc = buf + 5 * plane, *pm = buf + 6 * plane, *py = buf + 7 * plane;
+    cudaMemcpy(pc, dc, plane * sizeof(float), cudaMemcpyDeviceToDevice);
+    cudaMemcpy(pm, dm, plane * sizeof(float), cudaMemcpyDeviceToDevice);
+    cudaMemcpy(py, dy, plane * sizeof(float), cudaMemcpyDeviceToDevice);
+    if (p.printExpose.active) {
+        cudaError_t pe = juicer_cuda_print_focused_continue_from_capture_density(&q, pc, pm, py, nullptr, nullptr);
+        if (pe != cudaSuccess) return (int)pe;
+    }
+    dc = pc;
+    dm = pm;
+    dy = py;
+    const bool active = post->hash != 0;
+    const float* gk = nullptr;
+    const float* lk = nullptr;
+    const float* uk = nullptr;
+    int gr = 0, lr = 0, ur = 0;
+    std::vector<float> gw, lw, uw;
+    if (active && (post->flags & FJ_POST_GLARE) && post->glare_blur_sigma_px > 0.0f) {
+        gw = ref_gaussian(post->glare_blur_radius, post->glare_blur_sigma_px);
+        gk = a.put(gw.data(), gw.size());
+        gr = post->glare_blur_radius;
+    }
+    if (active && post->lens_blur_sigma_px > 0.0f) {
+        lw = ref_gaussian(post->lens_blur_radius, post->lens_blur_sigma_px);
+        lk = a.put(lw.data(), lw.size());
+        lr = post->lens_blur_radius;
+    }
+    if (active && post->unsharp_sigma_px > 0.0f) {
+        uw = ref_gaussian(post->unsharp_radius, post->unsharp_sigma_px);
+        uk = a.put(uw.data(), uw.size());
+        ur = post->unsharp_radius;
+    }
+    LaunchTimer timer;
+    cudaError_t e = juicer_cuda_print_focused_scan_linear_density_rgb(
+        &q, dc, dm, dy, r, g, b, active ? tmp : nullptr, active ? blurred : nullptr, origin_x, origin_y,
+        (std::uint64_t)seed, active ? post->glare_percent : 0.0f, active ? post->glare_roughness : 0.0f, gk, gr,
+        nullptr);
+    if (e == cudaSuccess)
+        e = juicer_cuda_print_focused_scanner_post_output(&q, r, g, b, active ? tmp : nullptr, lk, lr, uk, ur,
+                                                          active ? post->unsharp_amount : 0.0f, nullptr, nullptr,
+                                                          nullptr, 0, 0, nullptr);
+    timer.stop();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return (int)e;
+}

@@ -173,6 +173,19 @@ def grain_plan_cases():
     print("grain plan cases:", len(cases), "primitives:", len(prims))
 
 
+def gaussian_cases():
+    """Normalised Gaussian taps: the reference's native characterization
+    (tests/optics/gaussian-fixtures/linux-payload.json, 188 arrays of exact f32 words;
+    empty arrays are inputs the active API rejects)."""
+    with open(os.path.join(REF, "tests", "optics", "gaussian-fixtures", "linux-payload.json")) as fh:
+        j = json.load(fh)
+    cases = [{"name": c["name"], "radius": c["radius"], "sigma_bits": c["sigma_bits"], "weights": c["weights"]}
+             for c in j["cases"]]
+    with open(os.path.join(HERE, "gaussian_cases.json"), "w") as fh:
+        json.dump(cases, fh, separators=(",", ":"))
+    print("gaussian cases:", len(cases))
+
+
 def recipes():
     sys.path.insert(0, ROOT)
     import __graft_entry__
@@ -192,4 +205,5 @@ if __name__ == "__main__":
     diffusion_component_cases()
     diffusion_images()
     grain_plan_cases()
+    gaussian_cases()
     recipes()

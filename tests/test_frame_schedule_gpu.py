@@ -99,6 +99,13 @@ def test_unsupported_stages_and_partial_windows_are_rejected(torch_cuda, recipes
             owner.render(rec, src, d)
         assert e.value.status.category == abi.FJ_STATUS_UNSUPPORTED_INPUT
         rec.host.h.optics.flags &= ~abi.FJ_OPTICS_ENLARGER_DIFFUSION
-        rec.host.h.scanner_post.flags = 1
+        rec.host.h.scanner_post.flags = 6  # unknown post-effect flags
+        rec.host.h.scanner_post.hash = 1
         with pytest.raises(runtime.FjError, match="post effects"):
             owner.render(rec, src, d)
+        rec.host.h.scanner_post.flags = 0
+        rec.host.h.scanner_post.hash = 0
+        rec.host.h.optics.flags |= abi.FJ_OPTICS_HIGHLIGHT_BOOST
+        with pytest.raises(runtime.FjError, match="highlight boost"):
+            owner.render(rec, src, d)
+        rec.host.h.optics.flags &= ~abi.FJ_OPTICS_HIGHLIGHT_BOOST
