@@ -28,6 +28,12 @@ _EXPORTS = {
                                                     C.c_int32, C.c_uint32, C.c_void_p, C.c_size_t, C.c_void_p,
                                                     C.POINTER(abi.FjErrorBuffer)]),
     "fjb_glare_seed": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_int32, C.c_int32]),
+    "fjb_highlight_boost_state_bytes": (C.c_size_t, []),
+    "fjb_highlight_boost": (abi.FjStatus, [C.POINTER(abi.FjHighlightBoost), C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_ssize_t, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                           C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_highlight_boost_result": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32),
+                                                  C.POINTER(abi.FjErrorBuffer)]),
     "fjb_gaussian_kernel_host": (abi.FjStatus, [C.c_int32, C.c_float, C.POINTER(C.c_float), C.c_size_t,
                                                 C.POINTER(abi.FjErrorBuffer)]),
     "fj_cuda_check_terminal": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),

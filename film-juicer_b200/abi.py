@@ -77,6 +77,11 @@ FJ_OPTICS_CAMERA_DIFFUSION = 1
 FJ_OPTICS_ENLARGER_DIFFUSION = 2
 FJ_OPTICS_SCATTER_HALATION = 4
 FJ_OPTICS_HIGHLIGHT_BOOST = 8
+FJ_EFFECTS_WEAVE = 1
+FJ_EFFECTS_FILM = 2
+FJ_EFFECTS_GATE_TRANSMITTANCE = 4
+FJ_EFFECTS_GATE_OUTPUT = 8
+FJ_EFFECTS_FULL_FRAME = 16
 FJ_HALATION_IDENTITY = 0
 FJ_HALATION_FIR_REFLECT = 1
 FJ_HALATION_YVV_REPLICATE = 2

@@ -21,6 +21,7 @@
 #include "../../include/juicer_b200.h"
 #include "../../include/juicer_cuda_api.h"
 #include "fjb_diffusion.h"
+#include "fjb_highlight_boost.h"
 #include "fjb_scanner_post.h"
 #include "fjb_dir.h"
 #include "fjb_internal.h"
@@ -48,6 +49,7 @@ struct FjCuda {
     uint64_t diffusion_spectrum_key = 0;
     float* diffusion_fft_work = nullptr;     // FFT form: transposed row spectra of the frame
     size_t diffusion_fft_work_bytes = 0;
+    void* boost_state = nullptr;             // highlight reconstruction: frame maximum and disposition
     float* post_taps = nullptr;              // scanner post-effect Gaussian taps of the last descriptor
     size_t post_taps_bytes = 0;
     uint64_t post_key = 0;
@@ -109,6 +111,8 @@ void release_all(FjCuda* cuda) {
     if (cuda->diffusion_fft_work) cudaFree(cuda->diffusion_fft_work);
     cuda->diffusion_fft_work = nullptr;
     cuda->diffusion_fft_work_bytes = 0;
+    if (cuda->boost_state) cudaFree(cuda->boost_state);
+    cuda->boost_state = nullptr;
     if (cuda->post_taps) cudaFree(cuda->post_taps);
     cuda->post_taps = nullptr;
     cuda->post_taps_bytes = 0;
@@ -205,10 +209,6 @@ bool stages_supported(const FjPreparedHostData& h, std::string& why) {
         why = "enlarger diffusion is not supported by this build";
         return false;
     }
-    if (h.optics.flags & FJ_OPTICS_HIGHLIGHT_BOOST) {
-        why = "highlight boost is not supported by this build";
-        return false;
-    }
     fjb::PostPlan post;
     if (!fjb::post_plan_from(h.scanner_post, post, why)) return false;
     if (h.effects.flags & (FJ_EFFECTS_FILM | FJ_EFFECTS_GATE_OUTPUT)) {
@@ -290,9 +290,20 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
     stage_begin(cuda, FJB_STAGE_CAMERA_EXPOSURE, vs);
     st = fjb_camera_exposure(recipe, src, srb, comps, width, height, carrier[0], carrier[1], carrier[2], stride, vs,
                              error);
-    stage_end(cuda, FJB_STAGE_CAMERA_EXPOSURE, vs);
     if (st.category != FJ_STATUS_SUCCESS) return st;
     if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
+    if (o.flags & FJ_OPTICS_HIGHLIGHT_BOOST) {
+        // highlight reconstruction on the carrier, before diffusion; the disposition is
+        // checked when the frame's flags are read
+        if (!cuda->boost_state) {
+            e = cudaMalloc(&cuda->boost_state, fjb_highlight_boost_state_bytes());
+            if (e != cudaSuccess) return fjb::cuda_status(e, error, "highlight boost state");
+        }
+        st = fjb_highlight_boost(&o.highlight_boost, carrier[0], carrier[1], carrier[2], stride, width, height,
+                                 cuda->boost_state, vs, error);
+        if (st.category != FJ_STATUS_SUCCESS) return st;
+    }
+    stage_end(cuda, FJB_STAGE_CAMERA_EXPOSURE, vs);
     if (camera_diffusion) {
         const FjDiffusion& d = o.camera;
         if (!(d.scatter_fraction >= 0.0 && d.scatter_fraction <= 1.0))
@@ -638,7 +649,8 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
                 return out;
             }
         }
-        if (!camera_diffusion && !halation && !spatial_dir && !grain && !post.active) {
+        const bool boost = (optics & FJ_OPTICS_HIGHLIGHT_BOOST) != 0;
+        if (!camera_diffusion && !halation && !spatial_dir && !grain && !post.active && !boost) {
             // Monolithic: one fused pass source -> output
             stage_begin(cuda, FJB_STAGE_MONOLITHIC, vs);
             st = fjb_render_pixels(recipe, src, srb, dst, drb, width, height, comps, vs, error);
@@ -665,6 +677,14 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
             return out;
         }
         stage_collect(cuda);
+        if (boost) {
+            // src/ProcessRoot.cpp:4063-4096: an invalid carrier or peak overflow fails the frame
+            st = fjb_highlight_boost_result(cuda->boost_state, vs, nullptr, error);
+            if (st.category != FJ_STATUS_SUCCESS) {
+                out.status = st;
+                return out;
+            }
+        }
         if (flags & (1u << 8)) out.flags |= FJ_RENDER_DEFERRED_DIR_ERROR;
         out.status = fjb::ok_status();
         fjb::write_error(error, (flags & 1u) ? "scanner stage reported non-finite pixels" : "");

@@ -128,3 +128,17 @@ def scanner_post_record(*, glare_percent: float = 0.0, glare_roughness: float = 
     p.unsharp_amount = unsharp_amount
     p.hash = hash
     return p
+
+
+def highlight_boost_record(protection: float = 1.0, sharpness: float = 4.0, peak_gain: float = 2.0,
+                           recipe_hash: int = 0xB0057):
+    """FjHighlightBoost: samples above `protection` are lifted so that the frame maximum
+    reaches maximum * peak_gain; `sharpness` shapes the curve."""
+    from . import abi
+
+    d = abi.FjHighlightBoost()
+    d.recipe_hash = recipe_hash
+    d.protection = protection
+    d.sharpness = sharpness
+    d.peak_gain = peak_gain
+    return d

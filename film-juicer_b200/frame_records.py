@@ -20,10 +20,11 @@ class FrameRecord:
                  diffusion: bool = True, halation: bool = True, spatial_dir: bool = True, grain: bool = True,
                  auto_exposure: bool = False, noise: "grain_plan.Noise | None" = None,
                  pixel_size_um: float | None = None, frame_time: float = 0.0, descriptor_width: int | None = None,
-                 post=None):
+                 post=None, highlight_boost=None):
         """descriptor_width: the frame width the pixel size and diffusion radius are
         derived for (defaults to `width`; a crop of a larger frame passes the full width);
-        post: an FjScannerPostEffects record (descriptors.scanner_post_record)."""
+        post: an FjScannerPostEffects record (descriptors.scanner_post_record);
+        highlight_boost: an FjHighlightBoost record (descriptors.highlight_boost_record)."""
         self.width, self.height = width, height
         dw = descriptor_width or width
         self.pixel_size_um = pixel_size_um or 35000.0 / dw
@@ -43,6 +44,9 @@ class FrameRecord:
         if halation:
             h.optics.scatter_halation = prepare.scatter_halation_record(px)
             flags |= abi.FJ_OPTICS_SCATTER_HALATION
+        if highlight_boost is not None:
+            h.optics.highlight_boost = highlight_boost
+            flags |= abi.FJ_OPTICS_HIGHLIGHT_BOOST
         h.optics.flags = flags
         if spatial_dir:
             h.spatial_dir = descriptors.spatial_dir_record(px, width, height)

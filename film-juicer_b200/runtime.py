@@ -365,3 +365,25 @@ def render_from_density_post(recipe: "DeviceRecipe", post, seed: int, origin, de
         C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
     _check("fjb_render_from_density_post", st, err)
     return scratch
+
+
+def highlight_boost(descriptor: "abi.FjHighlightBoost", carrier_bgr, stream=None, state=None):
+    """In-place highlight reconstruction on CUDA carrier planes (B, G, R), then the
+    disposition check (raises FjError on an invalid carrier or a peak overflow). Returns
+    the disposition (0 bypass, 1 applied)."""
+    torch = _torch()
+    lib = load_library()
+    b, g, r = carrier_bgr
+    h, w = b.shape
+    if state is None:
+        state = torch.zeros(int(lib.fjb_highlight_boost_state_bytes()) // 4, dtype=torch.int32, device=b.device)
+    err = abi.ErrorText()
+    st = lib.fjb_highlight_boost(C.byref(descriptor), C.c_void_p(_ptr(b)), C.c_void_p(_ptr(g)), C.c_void_p(_ptr(r)),
+                                 b.stride(0), w, h, C.c_void_p(_ptr(state)), C.c_void_p(_stream_handle(stream)),
+                                 C.byref(err.buf))
+    _check("fjb_highlight_boost", st, err)
+    disp = C.c_uint32()
+    st = lib.fjb_highlight_boost_result(C.c_void_p(_ptr(state)), C.c_void_p(_stream_handle(stream)), C.byref(disp),
+                                        C.byref(err.buf))
+    _check("fjb_highlight_boost_result", st, err)
+    return disp.value

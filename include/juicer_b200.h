@@ -104,6 +104,20 @@ uint64_t fjb_glare_seed(uint64_t recipe_hash, uint64_t frame_token, int32_t sour
 FjStatus fjb_gaussian_kernel_host(int32_t radius, float sigma_px, float* weights, size_t count,
                                   FjErrorBuffer* error);
 
+/* Highlight reconstruction on the camera carrier planes B, G, R (reference
+ * src/Cuda/Film/JuicerCudaHighlightBoost.cu:207-258 launch_highlight_boost; scheduled after
+ * the camera exposure and before camera diffusion, src/Cuda/JuicerCudaExecutor.cpp:1155-1185).
+ * `state` is fjb_highlight_boost_state_bytes() of device memory; the call is asynchronous.
+ * fjb_highlight_boost_result synchronises `stream` and maps the disposition as the
+ * reference does (src/ProcessRoot.cpp:4063-4096): applied / bypass succeed, an invalid
+ * (negative or non-finite) carrier or a peak above FLT_MAX is FJ_STATUS_UNSUPPORTED_INPUT.
+ * disposition: 0 bypass, 1 applied, 2 invalid carrier, 3 peak overflow. */
+size_t fjb_highlight_boost_state_bytes(void);
+FjStatus fjb_highlight_boost(const FjHighlightBoost* descriptor, float* carrier_b, float* carrier_g, float* carrier_r,
+                             ptrdiff_t carrier_stride, int32_t width, int32_t height, void* state, void* stream,
+                             FjErrorBuffer* error);
+FjStatus fjb_highlight_boost_result(const void* state, void* stream, uint32_t* disposition, FjErrorBuffer* error);
+
 /* Camera auto-exposure metering (reference src/Cuda/JuicerCudaAutoExposure.cu:314-520,
  * run by src/Cuda/JuicerCudaExecutor.cpp:1013 meter_camera_exposure). `src` points at
  * pixel (meter->source_bounds.x1, .y1). Writes the float exposure scale 2^-log2(Y) to

@@ -1,5 +1,5 @@
 """The oracle's whole-frame chain for the staged schedule (test infrastructure only):
-camera exposure -> camera diffusion -> scatter/halation -> spatial DIR -> capture
+camera exposure -> highlight reconstruction -> camera diffusion -> scatter/halation -> spatial DIR -> capture
 density -> grain -> print/scan/output, each stage the CPU restatement in oracle/."""
 from __future__ import annotations
 
@@ -29,6 +29,10 @@ def render_frame(frame_record, recipe, src, threads: int = 1, frame_token: int =
         scale = orc.auto_exposure(host, h.auto_exposure, src)
     carrier, _ = orc.render(host, src, stage=3, auto_scale=scale, threads=threads)  # B, G, R
     flags = h.optics.flags
+    if flags & abi.FJ_OPTICS_HIGHLIGHT_BOOST:
+        carrier, disp = ooptics.highlight_boost(h.optics.highlight_boost, carrier)
+        if disp not in (0, 1):
+            raise RuntimeError(f"highlight boost disposition {disp}")
     if flags & abi.FJ_OPTICS_CAMERA_DIFFUSION:
         d = h.optics.camera
         lam, w = ooptics.diffusion_components(d.family, list(d.group_weights), list(d.group_lambda_um), d.warmth,

@@ -109,3 +109,39 @@ def diffusion_components(family, group_weights, group_lambda_um, warmth, spatial
             for c in range(3):
                 weights[c].append(group_weights[1] * halo_rgb[c][i] if gi == 1 else group_weights[gi] * w[i])
     return lam_px, weights
+
+
+def highlight_boost(descriptor, carrier_bgr):
+    """CPU oracle of the highlight reconstruction (src/Cuda/Film/JuicerCudaHighlightBoost.cu)
+    on carrier planes B, G, R; returns (new planes B, G, R, disposition)."""
+    import numpy as np
+
+    lib = _o.load()
+    fn = lib.oracle_highlight_boost
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long,
+                   C.c_int, C.c_int]
+    planes = [np.array(p, dtype=np.float32, copy=True, order="C") for p in carrier_bgr]
+    h, w = planes[0].shape
+    disp = fn(descriptor.recipe_hash, descriptor.protection, descriptor.sharpness, descriptor.peak_gain,
+              *[C.c_void_p(p.ctypes.data) for p in planes], w, w, h)
+    return planes, disp
+
+
+def reference_highlight_boost(torch, descriptor, carrier_bgr):
+    """The reference's own CUDA highlight reconstruction on device planes (in place);
+    returns the disposition."""
+    ref = _o.load_reference()
+    fn = ref.ref_highlight_boost
+    fn.restype = C.c_int
+    abi = _o._abi()
+    fn.argtypes = [C.POINTER(abi.FjHighlightBoost), C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_int,
+                   C.POINTER(C.c_int)]
+    b, g, r = carrier_bgr
+    h, w = b.shape
+    disp = C.c_int()
+    rc = fn(C.byref(descriptor), C.c_void_p(b.data_ptr()), C.c_void_p(g.data_ptr()), C.c_void_p(r.data_ptr()),
+            b.stride(0), w, h, C.byref(disp))
+    if rc != 0:
+        raise RuntimeError(f"ref_highlight_boost failed with code {rc}")
+    return disp.value

@@ -2304,3 +2304,103 @@ int oracle_render_post(const FjPreparedHostData* h, const FjScannerPostEffects* 
     if (flags_out) *flags_out = flags;
     return 0;
 }
+
+/* ---------------- highlight reconstruction (src/Cuda/Film/JuicerCudaHighlightBoost.cu) ---------------- */
+
+typedef struct {
+    int disposition;
+    float maximum, protection, protection_res, onset, peak, peak_res, range, range_res, shape, shape_res, tail_exp,
+        tail_lin, delta, inv_norm;
+} OBoost;
+
+static double hb_normexp(double t) {
+    if (t >= 0.03125) return (expm1(t) - t) / (t * t);
+    return 0.5 + t * (1.0 / 6.0 + t * (1.0 / 24.0 + t * (1.0 / 120.0 + t * (1.0 / 720.0 +
+               t * (1.0 / 5040.0 + t * (1.0 / 40320.0 + t * (1.0 / 362880.0 + t / 3628800.0)))))));
+}
+
+static float hb_normf(float t, float res) {
+    if (t < 0.5f)
+        return 0.5f + t * (1.0f / 6.0f + t * (1.0f / 24.0f + t * (1.0f / 120.0f + t * (1.0f / 720.0f +
+                   t * (1.0f / 5040.0f + t * (1.0f / 40320.0f + t * (1.0f / 362880.0f + t / 3628800.0f)))))));
+    float num = fmaf(expf(t), res, expm1f(t) - t) - res;
+    return num / (t * t);
+}
+
+static float hb_sample(float s, const OBoost* w) {
+    if (s < w->onset) return s;
+    if (s == w->maximum) return w->peak;
+    float dist = s - w->protection, vp = dist - s;
+    float dres = ((s - (dist - vp)) + (-w->protection - vp)) - w->protection_res;
+    float q = dist / w->range;
+    float corr = (fmaf(-q, w->range, dist) + dres - q * w->range_res) / w->range;
+    float fr = q + corr, vc = fr - q;
+    float frres = (q - (fr - vc)) + (corr - vc);
+    float t = w->shape * fr;
+    float tres = fmaf(w->shape, fr, -t) + w->shape * frres + w->shape_res * fr;
+    float frsq = fmaf(2.0f * fr, frres, fr * fr);
+    float ratio = frsq * (hb_normf(t, tres) * w->inv_norm);
+    if (w->shape >= 0.5f && ratio >= 0.5f) {
+        float gap = w->maximum - s, gf = gap / w->range;
+        float gres = (fmaf(-gf, w->range, gap) - gf * w->range_res) / w->range;
+        float d = w->shape * gf;
+        float dr = fmaf(w->shape, gf, -d) + w->shape * gres + w->shape_res * gf;
+        float ome = fmaf(expf(-d), dr, -expm1f(-d));
+        float tail = fmaf(ome, w->tail_exp, -(d + dr) * w->tail_lin);
+        float ep = w->peak - gap, vg = w->peak - ep;
+        float epres = (w->peak - (ep + vg)) + (vg - gap);
+        return ep + ((epres + w->peak_res) - w->delta * tail);
+    }
+    return s + w->delta * ratio;
+}
+
+/* carrier planes B, G, R boosted in place; returns the disposition (0 bypass, 1 applied,
+ * 2 invalid carrier, 3 peak overflow) */
+int oracle_highlight_boost(uint64_t recipe_hash, double protection, double sharpness, double peak_gain, float* b,
+                           float* g, float* r, long stride, int W, int H) {
+    if (recipe_hash == 0 || W <= 0 || H <= 0) return 0;
+    float mx = 0.0f;
+    int invalid = 0;
+    float* planes[3] = {r, g, b};
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x)
+            for (int c = 0; c < 3; ++c) {
+                float v = planes[c][(size_t)y * stride + x];
+                if (isfinite(v) && v >= 0.0f) mx = fmaxf(mx, v);
+                else invalid = 1;
+            }
+    OBoost w;
+    memset(&w, 0, sizeof(w));
+    double maximum = mx;
+    w.maximum = mx;
+    if (invalid) return 2;
+    if (maximum <= protection) return 0;
+    double peak = maximum * peak_gain;
+    if (peak > (double)FLT_MAX) return 3;
+    double range = maximum - protection;
+    double shape = sharpness * range / maximum;
+    double norm = hb_normexp(shape);
+    w.protection = (float)protection;
+    w.protection_res = (float)(protection - (double)w.protection);
+    w.onset = (double)w.protection <= protection ? nextafterf(w.protection, INFINITY) : w.protection;
+    w.peak = (float)peak;
+    w.peak_res = (float)(peak - (double)w.peak);
+    w.range = (float)range;
+    w.range_res = (float)(range - (double)w.range);
+    w.shape = (float)shape;
+    w.shape_res = (float)(shape - (double)w.shape);
+    if (w.shape >= 0.5f) {
+        double den = shape * shape * norm;
+        w.tail_exp = (float)(exp(shape) / den);
+        w.tail_lin = (float)(1.0 / den);
+    }
+    w.delta = (float)(maximum * (peak_gain - 1.0));
+    w.inv_norm = (float)(1.0 / norm);
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x)
+            for (int c = 0; c < 3; ++c) {
+                float* v = &planes[c][(size_t)y * stride + x];
+                *v = hb_sample(*v, &w);
+            }
+    return 1;
+}

@@ -703,3 +703,37 @@ extern "C" int ref_scanner_post(const FjPreparedHostData* h, const float* const*
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return (int)e;
 }
+
+// ---- highlight reconstruction with the reference's launcher ----
+#include "Cuda/Film/JuicerCudaHighlightBoost.h"
+
+// Carrier planes B, G, R (device, `stride` floats per row) boosted in place by
+// JuicerCuda::launch_highlight_boost (src/Cuda/Film/JuicerCudaHighlightBoost.cu:207);
+// writes the disposition. Returns a cudaError_t value.
+extern "C" int ref_highlight_boost(const FjHighlightBoost* d, float* b, float* g, float* r, long stride, int width,
+                                   int height, int* disposition) {
+    JuicerCuda::HighlightBoostWorkspace* ws = nullptr;
+    if (cudaMalloc(&ws, sizeof(*ws)) != cudaSuccess) return 2;
+    cudaMemset(ws, 0, sizeof(*ws));
+    JuicerCuda::HighlightBoostDescriptor desc{};
+    desc.recipeHash = d->recipe_hash;
+    desc.protection = d->protection;
+    desc.sharpness = d->sharpness;
+    desc.peakGain = d->peak_gain;
+    JuicerCuda::CameraFilmLinearExposurePlanes carrier{};
+    carrier.blueSensitive = b;
+    carrier.greenSensitive = g;
+    carrier.redSensitive = r;
+    carrier.rowStrideFloats = (size_t)stride;
+    LaunchTimer timer;
+    const auto res = JuicerCuda::launch_highlight_boost(desc, carrier, width, height, ws, nullptr,
+                                                        JuicerCuda::kHighlightBoostMaxBlocks);
+    timer.stop();
+    cudaError_t e = res.status;
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    JuicerCuda::HighlightBoostDisposition disp{};
+    if (e == cudaSuccess) e = cudaMemcpy(&disp, &ws->disposition, sizeof(disp), cudaMemcpyDeviceToHost);
+    if (disposition) *disposition = (int)disp;
+    cudaFree(ws);
+    return (int)e;
+}

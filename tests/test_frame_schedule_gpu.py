@@ -105,7 +105,7 @@ def test_unsupported_stages_and_partial_windows_are_rejected(torch_cuda, recipes
             owner.render(rec, src, d)
         rec.host.h.scanner_post.flags = 0
         rec.host.h.scanner_post.hash = 0
-        rec.host.h.optics.flags |= abi.FJ_OPTICS_HIGHLIGHT_BOOST
-        with pytest.raises(runtime.FjError, match="highlight boost"):
+        rec.host.h.effects.flags |= abi.FJ_EFFECTS_FILM
+        with pytest.raises(runtime.FjError, match="defects"):
             owner.render(rec, src, d)
-        rec.host.h.optics.flags &= ~abi.FJ_OPTICS_HIGHLIGHT_BOOST
+        rec.host.h.effects.flags = 0
