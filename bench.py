@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="0 skips the CPU baseline leg")
     ap.add_argument("--width", type=int, default=WIDTH, help="frame width (profiling runs use small frames)")
     ap.add_argument("--height", type=int, default=HEIGHT)
+    ap.add_argument("--next-rows", action="store_true",
+                    help="workload variant: add highlight reconstruction and scanner post effects (glare, lens blur, "
+                         "the production unsharp 0.7 px / 0.7)")
     ap.add_argument("--precision", action="store_true",
                     help="instead of timing: one frame against the oracle's stage chain (CIEDE2000 of the output)")
     args = ap.parse_args()
@@ -224,6 +227,20 @@ def stage_models(record):
     }
 
 
+def workload_record(frame_records, recipe, W, H, next_rows: bool):
+    """The bench frame; `next_rows` adds highlight reconstruction (protection 4, sharpness
+    3, peak gain 1.5) and scanner post effects (glare 0.3 % blurred 4 px, lens blur 0.8 px,
+    unsharp 0.7 px amount 0.7)."""
+    if not next_rows:
+        return frame_records.FrameRecord(recipe, W, H)
+    from film_juicer_b200 import descriptors
+
+    post = descriptors.scanner_post_record(glare_percent=0.3, glare_roughness=0.4, glare_blur_sigma_px=4.0,
+                                           lens_blur_sigma_px=0.8, unsharp_sigma_px=0.7, unsharp_amount=0.7)
+    boost = descriptors.highlight_boost_record(4.0, 3.0, 1.5)
+    return frame_records.FrameRecord(recipe, W, H, post=post, highlight_boost=boost)
+
+
 def run_b200(args):
     import ctypes as C
 
@@ -240,7 +257,7 @@ def run_b200(args):
     dev = torch.cuda.current_device()
     W, H = args.width, args.height
     recipe = prepare.PreparedRecipe.load(os.path.join(ROOT, "tests", "golden", "recipe_print.npz"))
-    record = frame_records.FrameRecord(recipe, W, H)
+    record = workload_record(frame_records, recipe, W, H, args.next_rows)
     host = prepare.synthetic_frame(W, H, seed=SEED + rank)
     src = torch.from_numpy(host).to("cuda")
     dst = torch.empty_like(src)
@@ -348,7 +365,8 @@ def run_b200(args):
             "metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{W}x{H} full optical print through fj_cuda_render",
+            "config": {"workload": f"{W}x{H} full optical print through fj_cuda_render"
+                                   + (" + highlight reconstruction + scanner post effects" if args.next_rows else ""),
                        "recipe": "kodak_portra_400 -> kodak_portra_endura, Hanatos TC LUT, spatial DIR tail 200 um "
                                  "w 0.03, camera diffusion r=0.5% W, scatter/halation, grain 35 mm, scanner LUT r=17, "
                                  "OkLch gamut, sRGB",
