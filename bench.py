@@ -15,7 +15,7 @@ no collective on the data path).
           around the timed frames, max over ranks);
   stages  device time per stage from the owner's stage events in the timed region;
   e2e     Mpix/s through the C-ABI with host buffers: pinned host frame -> H2D, render,
-          D2H of the rendered frame, every step;
+          D2H of the rendered frame, every step, frames pipelined over two copy streams;
   --impl reference  times the CPU restatement of the reference's render path (the
           reference has no CPU renderer) on all host threads, on crops of the frame.
 """
@@ -307,31 +307,55 @@ def run_b200(args):
             stages[name] = round(times.total_ms[i] / times.frames[i], 4)
 
     # ---- end to end through the C-ABI with host buffers ----
+    # Frames are pipelined as a host would: while frame i renders on the render stream,
+    # frame i+1's pixels go up on a copy stream and frame i-1's result comes down on
+    # another (two device frame buffers, pinned host buffers). Every step still copies
+    # its whole input up and its whole output down inside the timed region.
     h_src = torch.from_numpy(host).pin_memory()
-    h_dst = torch.empty_like(h_src).pin_memory()
+    h_dst = [torch.empty_like(h_src).pin_memory() for _ in range(2)]
+    d_src = [src, torch.empty_like(src)]
+    d_dst = [dst, torch.empty_like(dst)]
+    cin, cout = torch.cuda.Stream(), torch.cuda.Stream()
     e_steps = max(3, min(args.steps, 30))
-    for _ in range(2):
-        with torch.cuda.stream(stream):
-            src.copy_(h_src, non_blocking=True)
-        owner.render(record, src, dst, stream=stream)
-        with torch.cuda.stream(stream):
-            h_dst.copy_(dst, non_blocking=True)
-    stream.synchronize()
+
+    def pipelined(n, t0=None, t1=None):
+        ev = lambda: torch.cuda.Event()  # noqa: E731
+        up, done, down = [ev(), ev()], [ev(), ev()], [ev(), ev()]
+        if t0 is not None:
+            t0.record(cin)
+        with torch.cuda.stream(cin):
+            d_src[0].copy_(h_src, non_blocking=True)
+        up[0].record(cin)
+        for i in range(n):
+            b = i % 2
+            if i + 1 < n:
+                nb = (i + 1) % 2
+                if i >= 1:
+                    cin.wait_event(done[nb])  # frame i-1 has finished reading d_src[nb]
+                with torch.cuda.stream(cin):
+                    d_src[nb].copy_(h_src, non_blocking=True)
+                up[nb].record(cin)
+            stream.wait_event(up[b])
+            if i >= 2:
+                stream.wait_event(down[b])  # frame i-2's result has left d_dst[b]
+            owner.render(record, d_src[b], d_dst[b], stream=stream)
+            done[b].record(stream)
+            cout.wait_event(done[b])
+            with torch.cuda.stream(cout):
+                h_dst[b].copy_(d_dst[b], non_blocking=True)
+            down[b].record(cout)
+        if t1 is not None:
+            t1.record(cout)
+        cout.synchronize()
+
+    pipelined(3)
     barrier()
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e_start.record(stream)
-    for _ in range(e_steps):
-        with torch.cuda.stream(stream):
-            src.copy_(h_src, non_blocking=True)
-        owner.render(record, src, dst, stream=stream)
-        with torch.cuda.stream(stream):
-            h_dst.copy_(dst, non_blocking=True)
-    e_end.record(stream)
-    e_end.synchronize()
+    pipelined(e_steps, e_start, e_end)
     barrier()
     e_ms = max_over_ranks(e_start.elapsed_time(e_end) / e_steps)
     e2e = world * px / (e_ms * 1e-3) / 1e6
-    ok = bool(np.isfinite(h_dst.numpy()).all())
+    ok = bool(np.isfinite(h_dst[0].numpy()).all() and np.isfinite(h_dst[1].numpy()).all())
 
     if rank == 0:
         pk, pk_kind = peaks()
@@ -377,7 +401,9 @@ def run_b200(args):
             "roofline": roof,
             "cpu_baseline": cpu_baseline(args.cpu_seconds) if world == 1 and args.cpu_seconds > 0 else None,
             "e2e": {"value": round(e2e, 2), "unit": "Mpix/s", "h2d_bytes_per_step": int(h_src.numel() * 4),
-                    "d2h_bytes_per_step": int(h_dst.numel() * 4), "steps": e_steps},
+                    "d2h_bytes_per_step": int(h_dst[0].numel() * 4), "steps": e_steps,
+                    "schedule": "frames pipelined: H2D of frame i+1 and D2H of frame i-1 on copy streams "
+                                "while frame i renders"},
             "gpu_launches": launches,
             "clocks": clk,
             "output_finite": ok,
