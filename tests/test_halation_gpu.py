@@ -22,6 +22,9 @@ CASES = {
     "tiny": (18.0, 7, 5, True),
     "one_row": (18.0, 64, 1, True),
     "one_col": (18.0, 1, 40, True),
+    # lines too long for shared memory: the global-memory block-parallel form
+    "long_rows": (9.11, 12800, 2, True),
+    "long_cols": (9.11, 2, 6600, False),
 }
 
 

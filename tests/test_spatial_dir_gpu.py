@@ -12,7 +12,9 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 GEOMS = {"1080p": (18.23, 96, 54), "4k": (9.11, 128, 72), "tiny": (18.23, 7, 5), "row": (18.23, 40, 1),
-         "col": (18.23, 1, 33)}
+         "col": (18.23, 1, 33),
+         # lines too long for shared memory: the global-memory block-parallel form
+         "long_rows": (9.11, 12800, 2), "long_cols": (9.11, 2, 6600)}
 
 
 def close(a, b, atol, rtol):
