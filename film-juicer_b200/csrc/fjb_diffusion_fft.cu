@@ -52,6 +52,19 @@ __device__ __forceinline__ int reflect_whole(int i, int n) {
     return v < n ? v : period - v;
 }
 
+// Shared-memory position of element i of a line: an XOR swizzle inside aligned groups
+// of 16 complex values, which spreads the strided Stockham writes over the banks.
+__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 4) & 15); }
+// The same for a line of n + 1 entries (n a power of two): the extra entry n keeps its place.
+__device__ __forceinline__ int swz_n1(int i, int n) { return i < n ? swz(i) : i; }
+
+// Stages the first `n` entries of exp(-2 pi i k / n) from the global table (ntw entries)
+// into shared memory. Caller synchronises after.
+__device__ __forceinline__ void stage_twiddles(float2* dst, const float2* tw, int log2n, int log2ntw) {
+    const int n = 1 << log2n, shift = log2ntw - log2n;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = tw[(size_t)k << shift];
+}
+
 // Twiddle table tw[k] = exp(-2 pi i k / n), k < n.
 __global__ void twiddle_kernel(float2* tw, int n) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -126,7 +139,7 @@ __device__ __forceinline__ void fft_stage(float2* data, int log2n, int ls, int c
             const float2* d = data + (size_t)line * ls;
             const int jm = j & (Ns - 1);
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[i][r] = d[j + r * nb];
+            for (int r = 0; r < R; ++r) v[i][r] = d[swz(j + r * nb)];
             if (jm != 0) {
                 auto fetch = [&](int k) {
                     float2 w = tw[(k * jm) << step_shift];
@@ -161,7 +174,7 @@ __device__ __forceinline__ void fft_stage(float2* data, int log2n, int ls, int c
             const int jm = j & (Ns - 1);
             const int base = ((j - jm) << kLog2R) + jm;
 #pragma unroll
-            for (int r = 0; r < R; ++r) d[base + r * Ns] = v[i][r];
+            for (int r = 0; r < R; ++r) d[swz(base + r * Ns)] = v[i][r];
         }
     }
     __syncthreads();
@@ -210,8 +223,10 @@ __global__ void __launch_bounds__(kFftThreads) rows_r2c_kernel(const __grid_cons
     const int L = min(p.rows_per_cta, rows - row0);
     if (L <= 0) return;
     const int W = p.width, H = p.height;
+    float2* tws = fsm + (size_t)p.rows_per_cta * (m + 1); // exp(-2 pi i k / nx), k < nx
+    stage_twiddles(tws, F.tw, p.log2m + 1, p.log2ntw);
     // load: complex sample n of line l = (e[2n], e[2n+1]) of the extended row
-    #pragma unroll 4
+    #pragma unroll 8
     for (int i = threadIdx.x; i < L * m; i += blockDim.x) {
         const int l = i >> p.log2m, n = i & (m - 1);
         const int ey = row0 + l;
@@ -232,25 +247,24 @@ __global__ void __launch_bounds__(kFftThreads) rows_r2c_kernel(const __grid_cons
             }
             e[h] = v;
         }
-        fsm[(size_t)l * m + n] = make_float2(e[0], e[1]);
+        fsm[(size_t)l * m + swz(n)] = make_float2(e[0], e[1]);
     }
     __syncthreads();
-    fft_lines<false>(fsm, m, p.log2m, m, L, F.tw, p.log2ntw);
+    fft_lines<false>(fsm, m, p.log2m, m, L, tws, p.log2m + 1);
     // split into the real transform's bins k = 0..m, written transposed
     float2* out = F.work[ch];
-    const int shift_nx = p.log2ntw - (p.log2m + 1);
     const int lg = p.log2_rows_per_cta;
     for (int i = threadIdx.x; i < (m + 1) << lg; i += blockDim.x) {
         const int k = i >> lg, l = i & ((1 << lg) - 1);
         if (l >= L) continue;
         const float2* z = fsm + (size_t)l * m;
-        const float2 zk = z[k == m ? 0 : k];
-        const float2 zr = z[k == 0 ? 0 : m - k];
+        const float2 zk = z[swz(k == m ? 0 : k)];
+        const float2 zr = z[swz(k == 0 ? 0 : m - k)];
         const float2 zc = make_float2(zr.x, -zr.y);
         const float2 E = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
         const float2 D = make_float2(zk.x - zc.x, zk.y - zc.y);
         const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
-        const float2 w = F.tw[(size_t)k << shift_nx];
+        const float2 w = tws[k];
         const float2 wo = cmul(w, O);
         out[(size_t)k * p.sy + row0 + l] = make_float2(E.x + wo.x, E.y + wo.y);
     }
@@ -270,7 +284,9 @@ __global__ void __launch_bounds__(kFftThreads) columns_kernel(const __grid_const
     if (KC <= 0) return;
     const float2* in = F.work[ch];
     const int rows = kBuild ? 2 * r + 1 : p.ey;
-    #pragma unroll 4
+    float2* tws = fsm + (size_t)p.cols_per_cta * ny; // exp(-2 pi i k / ny), k < ny
+    stage_twiddles(tws, F.tw, p.log2ny, p.log2ntw);
+    #pragma unroll 8
     for (int i = threadIdx.x; i < KC * ny; i += blockDim.x) {
         const int c = i >> p.log2ny, ey = i & (ny - 1);
         float2 v = make_float2(0.0f, 0.0f);
@@ -281,27 +297,32 @@ __global__ void __launch_bounds__(kFftThreads) columns_kernel(const __grid_const
         } else if (ey < rows) {
             v = in[(size_t)(k0 + c) * p.sy + ey];
         }
-        fsm[i] = v;
+        fsm[(size_t)c * ny + swz(ey)] = v;
     }
     __syncthreads();
-    fft_lines<false>(fsm, ny, p.log2ny, ny, KC, F.tw, p.log2ntw);
+    fft_lines<false>(fsm, ny, p.log2ny, ny, KC, tws, p.log2ny);
     float* spec = F.spectrum[ch];
     if (kBuild) {
         const float scale = 1.0f / ((float)p.m * (float)ny);
-        for (int i = threadIdx.x; i < KC * ny; i += blockDim.x) spec[(size_t)k0 * ny + i] = fsm[i].x * scale;
+        for (int i = threadIdx.x; i < KC * ny; i += blockDim.x) {
+            const int c = i >> p.log2ny, ky = i & (ny - 1);
+            spec[(size_t)k0 * ny + i] = fsm[(size_t)c * ny + swz(ky)].x * scale;
+        }
         return;
     }
-    #pragma unroll 4
+    #pragma unroll 8
     for (int i = threadIdx.x; i < KC * ny; i += blockDim.x) {
+        const int c = i >> p.log2ny, ky = i & (ny - 1);
         const float s = spec[(size_t)k0 * ny + i];
-        fsm[i] = make_float2(fsm[i].x * s, fsm[i].y * s);
+        float2& v = fsm[(size_t)c * ny + swz(ky)];
+        v = make_float2(v.x * s, v.y * s);
     }
     __syncthreads();
-    fft_lines<true>(fsm, ny, p.log2ny, ny, KC, F.tw, p.log2ntw);
+    fft_lines<true>(fsm, ny, p.log2ny, ny, KC, tws, p.log2ny);
     float2* out = F.work[ch];
     const int H = p.height;
     for (int c = 0; c < KC; ++c)
-        for (int y = threadIdx.x; y < H; y += blockDim.x) out[(size_t)(k0 + c) * p.sy + r + y] = fsm[(size_t)c * ny + r + y];
+        for (int y = threadIdx.x; y < H; y += blockDim.x) out[(size_t)(k0 + c) * p.sy + r + y] = fsm[(size_t)c * ny + swz(r + y)];
 }
 
 // Output rows: inverse real transform of spectrum rows r + y, crop, mix.
@@ -315,17 +336,18 @@ __global__ void __launch_bounds__(kFftThreads) rows_c2r_kernel(const __grid_cons
     const int L = min(p.rows_per_cta, H - y0);
     if (L <= 0) return;
     const float2* in = F.work[ch];
+    float2* tws = fsm + (size_t)p.rows_per_cta * ls; // exp(-2 pi i k / nx), k < nx
+    stage_twiddles(tws, F.tw, p.log2m + 1, p.log2ntw);
     const int lg = p.log2_rows_per_cta;
-    #pragma unroll 4
+    #pragma unroll 8
     for (int i = threadIdx.x; i < (m + 1) << lg; i += blockDim.x) {
         const int k = i >> lg, l = i & ((1 << lg) - 1);
-        if (l < L) fsm[(size_t)l * ls + k] = in[(size_t)k * p.sy + r + y0 + l];
+        if (l < L) fsm[(size_t)l * ls + swz_n1(k, m)] = in[(size_t)k * p.sy + r + y0 + l];
     }
     __syncthreads();
     // Z[k] = E[k] + i O[k], E = (X[k] + conj X[m-k]) / 2, O = (X[k] - conj X[m-k]) conj(w^k) / 2.
     // A thread takes pairs (k, m - k), 0 <= k < m/2, reads both bins, and writes Z[k] and
     // Z[m - k] (k > 0) after the barrier; the middle bin m/2 of line l goes to thread l.
-    const int shift_nx = p.log2ntw - (p.log2m + 1);
     const int half = m / 2, log2half = p.log2m - 1;
     constexpr int kMaxPairs = kC2rPairs;
     float2 zk[kMaxPairs], zm[kMaxPairs];
@@ -333,7 +355,7 @@ __global__ void __launch_bounds__(kFftThreads) rows_c2r_kernel(const __grid_cons
         const float2 xc = make_float2(xm.x, -xm.y);
         const float2 E = make_float2(0.5f * (xk.x + xc.x), 0.5f * (xk.y + xc.y));
         const float2 D = make_float2(0.5f * (xk.x - xc.x), 0.5f * (xk.y - xc.y));
-        const float2 w = F.tw[(size_t)k << shift_nx];
+        const float2 w = tws[k];
         const float2 O = cmul(D, make_float2(w.x, -w.y));
         return make_float2(E.x - O.y, E.y + O.x);
     };
@@ -343,14 +365,14 @@ __global__ void __launch_bounds__(kFftThreads) rows_c2r_kernel(const __grid_cons
         if (i < L << log2half) {
             const int l = i >> log2half, k = i & (half - 1);
             const float2* x = fsm + (size_t)l * ls;
-            const float2 a = x[k], b = x[m - k];
+            const float2 a = x[swz(k)], b = x[swz_n1(m - k, m)];
             zk[q] = z_of(a, b, k);
             zm[q] = z_of(b, a, m - k);
         }
     }
     float2 zmid = make_float2(0.0f, 0.0f);
     if ((int)threadIdx.x < L) {
-        const float2 a = fsm[(size_t)threadIdx.x * ls + half];
+        const float2 a = fsm[(size_t)threadIdx.x * ls + swz(half)];
         zmid = z_of(a, a, half);
     }
     __syncthreads();
@@ -360,19 +382,19 @@ __global__ void __launch_bounds__(kFftThreads) rows_c2r_kernel(const __grid_cons
         if (i < L << log2half) {
             const int l = i >> log2half, k = i & (half - 1);
             float2* x = fsm + (size_t)l * ls;
-            x[k] = zk[q];
-            if (k > 0) x[m - k] = zm[q];
+            x[swz(k)] = zk[q];
+            if (k > 0) x[swz(m - k)] = zm[q]; // 0 < k: m - k < m
         }
     }
-    if ((int)threadIdx.x < L) fsm[(size_t)threadIdx.x * ls + half] = zmid;
+    if ((int)threadIdx.x < L) fsm[(size_t)threadIdx.x * ls + swz(half)] = zmid;
     __syncthreads();
-    fft_lines<true>(fsm, m, p.log2m, ls, L, F.tw, p.log2ntw);
+    fft_lines<true>(fsm, m, p.log2m, ls, L, tws, p.log2m + 1);
     const float f = F.fraction;
     for (int l = 0; l < L; ++l)
         #pragma unroll 4
         for (int x = threadIdx.x; x < W; x += blockDim.x) {
             const int ex = x + r;
-            const float2 z = fsm[(size_t)l * ls + (ex >> 1)];
+            const float2 z = fsm[(size_t)l * ls + swz(ex >> 1)];
             const float conv = (ex & 1) ? z.y : z.x;
             const long long o = (long long)(y0 + l) * F.stride + x;
             const float cur = F.src[ch][o];
@@ -388,8 +410,11 @@ int log2_exact(int n) {
 
 int pow2_at_least(int n) { return 1 << log2_exact(n); }
 
-size_t rows_smem(const DiffusionFftPlan& p) { return (size_t)p.rows_per_cta * (p.m + 1) * sizeof(float2); }
-size_t cols_smem(const DiffusionFftPlan& p) { return (size_t)p.cols_per_cta * p.ny * sizeof(float2); }
+// data lines, then the twiddle table of the transform length
+size_t rows_smem(const DiffusionFftPlan& p) {
+    return ((size_t)p.rows_per_cta * (p.m + 1) + 2 * (size_t)p.m) * sizeof(float2);
+}
+size_t cols_smem(const DiffusionFftPlan& p) { return ((size_t)p.cols_per_cta + 1) * p.ny * sizeof(float2); }
 
 cudaError_t set_smem(const void* fn, size_t bytes) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
