@@ -37,6 +37,7 @@ struct DirComponentDev {
     float weight;
     int radius;
     const float* taps; // device, 2r+1
+    int symmetric_taps; // taps[i] == taps[2r - i] bit for bit
     double ff;
     double fb[3];
     const double* h_init;

@@ -21,6 +21,8 @@
 // read-modify-write accumulation never reaches HBM.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "fjb_dir.h"
 #include "fjb_launches.h"
 #include "fjb_lines.cuh"
@@ -588,16 +590,129 @@ __host__ __device__ inline size_t exits_doubles(int L, int n, int threads) {
     return e > r ? e : r;
 }
 
+// Nine consecutive outputs per thread in the FIR components (odd, so that the warp's
+// threads, nine samples apart, fall in distinct shared-memory banks).
+constexpr int kFirRun = 9;
+constexpr int kFirWindowMaxRadius = 9;
+
+// Doubles ahead of the rows in the rows kernel: the recursion's exits, entry, last and
+// carry arrays, or, for the FIR components, a per-warp staging area of 32 x kFirRun
+// floats through which the outputs go out coalesced.
+__host__ __device__ inline size_t rows_prefix_doubles(int W) {
+    const size_t scan =
+        exits_doubles(kRowsPerCta, W, kRowsThreads) + (size_t)kRowsPerCta * 6 + carry_doubles(kRowsPerCta, W);
+    const size_t stage = (size_t)(kRowsThreads / 32) * 32 * kFirRun / 2;
+    return scan > stage ? scan : stage;
+}
+
 size_t rows_smem_bytes(int W) {
-    return (size_t)kRowsPerCta * lines::padded(W) * sizeof(float) +
-           (exits_doubles(kRowsPerCta, W, kRowsThreads) + (size_t)kRowsPerCta * 6 + carry_doubles(kRowsPerCta, W)) *
-               sizeof(double);
+    return (size_t)kRowsPerCta * lines::padded(W) * sizeof(float) + rows_prefix_doubles(W) * sizeof(double);
 }
 
 size_t cols_smem_bytes(int H) {
     return (size_t)kStripCols * lines::padded(H) * sizeof(float) +
            (exits_doubles(kStripCols, H, kColsThreads) + (size_t)kStripCols * 6 + carry_doubles(kStripCols, H)) *
                sizeof(double);
+}
+
+// ---------------------------------------------------------------------------
+// FIR components on lines staged densely in shared memory: a thread computes nine
+// consecutive outputs from a register window, converting each input to FP64 once
+// (instead of once per tap); the taps are summed in order, as the direct loop does.
+// Gaussian taps are symmetric, so half of them (as doubles) stay in registers.
+// ---------------------------------------------------------------------------
+template <int RAD, typename Get, typename Put>
+__device__ __forceinline__ void fir_run(const double (&t)[RAD + 1], int p0, int n, Get get, Put put) {
+    // streamed over the window: input i adds its term to every output it reaches, in
+    // increasing tap order per output; output j is complete (and handed to `put`) once
+    // input j + 2 RAD is in
+    double sum[kFirRun];
+#pragma unroll
+    for (int j = 0; j < kFirRun; ++j) sum[j] = 0.0;
+#pragma unroll
+    for (int i = 0; i < kFirRun + 2 * RAD; ++i) {
+        int q = p0 - RAD + i;
+        q = (unsigned)q < (unsigned)n ? q : reflect_dir(q, n);
+        const double v = (double)get(q);
+#pragma unroll
+        for (int j = 0; j < kFirRun; ++j) {
+            const int o = i - j;
+            if (o >= 0 && o <= 2 * RAD) sum[j] += v * t[o <= RAD ? o : 2 * RAD - o];
+        }
+        if (i >= 2 * RAD) put(i - 2 * RAD, isfinite(sum[i - 2 * RAD]) ? (float)sum[i - 2 * RAD] : 0.0f);
+    }
+}
+
+template <int RAD>
+__device__ __forceinline__ void fir_load_taps(const float* taps, double (&t)[RAD + 1]) {
+#pragma unroll
+    for (int o = 0; o <= RAD; ++o) t[o] = (double)__ldg(taps + o);
+}
+
+// Rows [row0, row0 + L) of `buf` (dense, W floats per row) into plane T. Each warp
+// takes 32 consecutive runs at a time and writes them out through its staging area.
+template <int RAD>
+__device__ void fir_rows(const DirComponentDev& c, const float* buf, int L, int W, int row0, float* T, float* stage) {
+    double t[RAD + 1];
+    fir_load_taps<RAD>(c.taps, t);
+    const int nb = (W + kFirRun - 1) / kFirRun;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    float* st = stage + warp * 32 * kFirRun;
+    for (int base = warp * 32; base < L * nb; base += warps * 32) {
+        const int task = base + lane;
+        if (task < L * nb) {
+            const int r = task / nb, p0 = (task - r * nb) * kFirRun;
+            const float* row = buf + (size_t)r * W;
+            fir_run<RAD>(t, p0, W, [&](int q) { return row[q]; }, [&](int j, float v) { st[lane * kFirRun + j] = v; });
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < kFirRun; ++i) {
+            const int e = i * 32 + lane;
+            const int tk = base + e / kFirRun;
+            if (tk < L * nb) {
+                const int r = tk / nb, x = (tk - r * nb) * kFirRun + e % kFirRun;
+                if (x < W) T[(size_t)(row0 + r) * W + x] = st[e];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Columns of an 8-wide dense strip (element (y, c) at y * 8 + c): weighted and summed
+// into the running sum as the component epilogue does.
+template <int RAD>
+__device__ void fir_cols(const DirComponentDev& c, const float* work, int H, int W, int x0, int k, const float* acc_in,
+                         float* acc_out) {
+    double t[RAD + 1];
+    fir_load_taps<RAD>(c.taps, t);
+    const int nrb = (H + kFirRun - 1) / kFirRun;
+    for (int task = threadIdx.x; task < 8 * nrb; task += blockDim.x) {
+        const int cc = task & 7, p0 = (task >> 3) * kFirRun;
+        fir_run<RAD>(t, p0, H, [&](int q) { return work[q * 8 + cc]; }, [&](int j, float blurred) {
+            const int y = p0 + j;
+            if (y < H) {
+                const size_t o = (size_t)y * W + x0 + cc;
+                const float weighted = blurred * c.weight;
+                acc_out[o] = k == 0 ? weighted : acc_in[o] + weighted;
+            }
+        });
+    }
+}
+
+template <typename F>
+__device__ __forceinline__ void with_radius(int rad, F f) {
+    switch (rad) {
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        case 2: f(std::integral_constant<int, 2>{}); break;
+        case 3: f(std::integral_constant<int, 3>{}); break;
+        case 4: f(std::integral_constant<int, 4>{}); break;
+        case 5: f(std::integral_constant<int, 5>{}); break;
+        case 6: f(std::integral_constant<int, 6>{}); break;
+        case 7: f(std::integral_constant<int, 7>{}); break;
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        default: f(std::integral_constant<int, 9>{}); break;
+    }
 }
 
 // Reflected start of each line: anchor + sum_i w_h[i] (x_i - anchor) over the first
@@ -672,7 +787,7 @@ __global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) dir_rows_smem_kerne
     double* entry = exits + exits_doubles(kRowsPerCta, W, kRowsThreads);
     double* last = entry + (size_t)kRowsPerCta * 3;
     double* carry = last + (size_t)kRowsPerCta * 3;
-    float* buf = reinterpret_cast<float*>(carry + carry_doubles(kRowsPerCta, W));
+    float* buf = reinterpret_cast<float*>(exits + rows_prefix_doubles(W));
     auto line = [&](int r) { return buf + (size_t)r * pw; };
     const float* raw = p.raw[ch];
     for (int k = 0; k < p.count; ++k) {
@@ -681,6 +796,13 @@ __global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) dir_rows_smem_kerne
             // reflect-boundary taps in FP64 over the densely staged rows
             lines::load_rows_dense(buf, raw, W, row0, L, W);
             const int rad = c.radius;
+            if (c.symmetric_taps && rad >= 1 && rad <= kFirWindowMaxRadius) {
+                float* T = p.temp[ch][k];
+                float* stage = reinterpret_cast<float*>(exits);
+                with_radius(rad, [&](auto R) { fir_rows<decltype(R)::value>(c, buf, L, W, row0, T, stage); });
+                __syncthreads();
+                continue;
+            }
             for (int r = 0; r < L; ++r) {
                 const float* row = buf + (size_t)r * W;
                 float* out = p.temp[ch][k] + (size_t)(row0 + r) * W;
@@ -773,7 +895,10 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) dir_cols_smem_kerne
             const float weighted = blurred * c.weight;
             return k == 0 ? weighted : a + weighted;
         };
-        if (vec) {
+        if (dense_fir && c.symmetric_taps && c.radius >= 1 && c.radius <= kFirWindowMaxRadius) {
+            with_radius(c.radius,
+                        [&](auto R) { fir_cols<decltype(R)::value>(c, work, H, W, x0, k, acc_in, acc_out); });
+        } else if (vec) {
             // thread -> (row, half strip); global reads go kBatch rows at a time
             constexpr int kBatch = 4;
             const int h = threadIdx.x & 1, ys = blockDim.x >> 1;

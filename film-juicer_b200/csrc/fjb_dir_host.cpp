@@ -323,6 +323,9 @@ bool dir_plan_create(const FjSpatialDir& sd, int width, int height, cudaStream_t
                     return false;
                 if ((err = cudaStreamSynchronize(stream)) != cudaSuccess) return false;
                 c.taps = static_cast<const float*>(d);
+                c.symmetric_taps = 1;
+                for (int i = 0; i <= 2 * g.radius; ++i)
+                    if (std::memcmp(&taps[i], &taps[2 * g.radius - i], sizeof(float)) != 0) c.symmetric_taps = 0;
                 break;
             }
             case FJ_DIR_OPERATOR_YVV_REFLECT: {
