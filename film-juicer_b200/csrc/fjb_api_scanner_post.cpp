@@ -88,6 +88,7 @@ size_t post_scratch_floats(int width, int height) {
 }
 
 // Scratch: linear R, G, B planes, blur temp, glare, glare blur temp, then the taps.
+// After the scan, the last three planes serve as the temps of the three-plane blurs.
 // `taps` (device) holds glare, lens and unsharp taps back to back, as in the plan.
 FjStatus render_from_density_post(FjbRecipe* recipe, const PostPlan& plan, uint64_t seed, int32_t origin_x,
                                   int32_t origin_y, const float* density_c, const float* density_m,
@@ -122,14 +123,16 @@ FjStatus render_from_density_post(FjbRecipe* recipe, const PostPlan& plan, uint6
         const uint32_t medium = p.scan_medium_negative ? 0u : 1u;
         e = launch_glare(glare, width, height, seed, medium, origin_x, origin_y, plan.glare_percent,
                          plan.glare_roughness, s);
-        if (e == cudaSuccess && plan.glare_r > 0) e = launch_blur_plane(glare, blurred, width, height, glare_w, plan.glare_r, s);
+        if (e == cudaSuccess && plan.glare_r > 0) e = launch_blur_planes(&glare, &blurred, 1, width, height, glare_w, plan.glare_r, s);
         p.scan_glare = glare;
     }
     if (e == cudaSuccess) e = launch_pixel_chain(p, PixelStage::DensityToLinearRgb, s);
-    for (int c = 0; c < 3 && e == cudaSuccess && plan.lens_r > 0; ++c)
-        e = launch_blur_plane(lin[c], tmp, width, height, lens_w, plan.lens_r, s);
-    for (int c = 0; c < 3 && e == cudaSuccess && plan.unsharp_r > 0; ++c)
-        e = launch_unsharp_plane(lin[c], tmp, width, height, unsharp_w, plan.unsharp_r, plan.unsharp_amount, s);
+    // the glare planes are free once the scan has added the glare: the three planes blur
+    // together through tmp, glare and the glare blur temp
+    float* tmps[3] = {tmp, glare, blurred};
+    if (e == cudaSuccess && plan.lens_r > 0) e = launch_blur_planes(lin, tmps, 3, width, height, lens_w, plan.lens_r, s);
+    if (e == cudaSuccess && plan.unsharp_r > 0)
+        e = launch_unsharp_planes(lin, tmps, 3, width, height, unsharp_w, plan.unsharp_r, plan.unsharp_amount, s);
     if (e == cudaSuccess) e = launch_pixel_chain(p, PixelStage::LinearRgbToOutput, s);
     if (e != cudaSuccess) return cuda_status(e, error, "scanner post effects");
     write_error(error, "");

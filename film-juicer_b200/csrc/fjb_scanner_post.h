@@ -19,13 +19,14 @@ constexpr int kMaxGaussianRadius = 2048; // rust/film-juicer-core/src/optics/gau
 cudaError_t launch_glare(float* out, int width, int height, uint64_t seed, uint32_t medium, int origin_x,
                          int origin_y, float percent, float roughness, cudaStream_t stream);
 
-// Separable Gaussian blur of `plane` in place through `tmp` (taps w[0..2r], device).
-cudaError_t launch_blur_plane(float* plane, float* tmp, int width, int height, const float* w, int radius,
-                              cudaStream_t stream);
+// Separable Gaussian blur of `count` (1..3) planes in place through as many `tmps`
+// (taps w[0..2r], device).
+cudaError_t launch_blur_planes(float* const* planes, float* const* tmps, int count, int width, int height,
+                               const float* w, int radius, cudaStream_t stream);
 
-// plane <- plane + amount (plane - blur(plane)), through `tmp`.
-cudaError_t launch_unsharp_plane(float* plane, float* tmp, int width, int height, const float* w, int radius,
-                                 float amount, cudaStream_t stream);
+// plane <- plane + amount (plane - blur(plane)) for `count` (1..3) planes, through `tmps`.
+cudaError_t launch_unsharp_planes(float* const* planes, float* const* tmps, int count, int width, int height,
+                                  const float* w, int radius, float amount, cudaStream_t stream);
 
 // Which effects a post-effects record turns on, with their Gaussian taps (host).
 struct PostPlan {

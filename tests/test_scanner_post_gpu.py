@@ -77,6 +77,49 @@ def test_post_matches_reference_cuda(torch_cuda, ref_lib, oracle, recipes, prepa
     dr.close()
 
 
+# Frame shapes for the blur kernels: single pixel, frames narrower and shorter than one
+# run of outputs, radii wider than the frame (reflection repeated), and a row too long
+# for a shared-memory tile (the per-output fallback).
+SHAPES = [
+    (1, 1, dict(lens_blur_sigma_px=1.5, unsharp_sigma_px=0.7, unsharp_amount=0.7)),
+    (5, 3, dict(glare_percent=0.4, glare_roughness=0.4, glare_blur_sigma_px=3.0, lens_blur_sigma_px=2.0)),
+    (13, 40, dict(lens_blur_sigma_px=12.0, lens_blur_radius=50, unsharp_sigma_px=1.2, unsharp_amount=0.5)),
+    (257, 11, dict(glare_percent=0.5, glare_roughness=0.3, glare_blur_sigma_px=4.0, lens_blur_sigma_px=0.8)),
+    (24600, 2, dict(lens_blur_sigma_px=0.8, unsharp_sigma_px=0.7, unsharp_amount=0.7)),
+]
+
+
+@pytest.mark.parametrize("w,h,kw", SHAPES, ids=[f"{w}x{h}" for w, h, _ in SHAPES])
+def test_post_shapes_match_reference_cuda(torch_cuda, ref_lib, oracle, recipes, prepare, w, h, kw):
+    torch = torch_cuda
+    from film_juicer_b200 import descriptors, runtime
+
+    if not hasattr(ref_lib, "ref_scanner_post"):
+        pytest.skip("reference harness built without the post-effects entry")
+    rec = prepare.HostRecord(recipes["direct"])
+    post = descriptors.scanner_post_record(**kw)
+    src = np.ascontiguousarray(prepare.synthetic_frame(w, h, seed=29))
+    s = torch.from_numpy(src).cuda()
+    dr = runtime.DeviceRecipe(rec)
+    dens = density_planes(torch, dr, src)
+    seed = oracle.glare_seed(rec.h.recipe_hash, 7, 1, 2)
+    mine = torch.full_like(s, -1.0)
+    runtime.render_from_density_post(dr, post, seed, (1, 2), dens, mine, src=s)
+    lut = oracle.scanner_lut_for(rec)
+    ptrs = (C.c_void_p * 6)(*[o.ctypes.data for o in lut])
+    ref = torch.full_like(s, -1.0)
+    rc = ref_lib.ref_scanner_post(rec.pointer(), ptrs, C.byref(post), seed, 1, 2,
+                                  *[C.c_void_p(p.data_ptr()) for p in dens], C.c_void_p(s.data_ptr()), w * 12,
+                                  C.c_void_p(ref.data_ptr()), w * 12, w, h, 3)
+    assert rc == 0
+    torch.cuda.synchronize()
+    a, b = mine.cpu().numpy(), ref.cpu().numpy()
+    assert np.all(np.isfinite(a))
+    err = np.abs(a - b)
+    assert float(err.max()) <= 1e-6, (w, h, float(err.max()), float((err > 0).mean()))
+    dr.close()
+
+
 @pytest.mark.parametrize("name", list(POSTS))
 def test_post_matches_oracle(torch_cuda, oracle, recipes, prepare, name):
     torch = torch_cuda
