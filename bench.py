@@ -229,8 +229,9 @@ def stage_models(record):
 
 def workload_record(frame_records, recipe, W, H, next_rows: bool):
     """The bench frame; `next_rows` adds highlight reconstruction (protection 4, sharpness
-    3, peak gain 1.5) and scanner post effects (glare 0.3 % blurred 4 px, lens blur 0.8 px,
-    unsharp 0.7 px amount 0.7)."""
+    3, peak gain 1.5), scanner post effects (glare 0.3 % blurred 4 px, lens blur 0.8 px,
+    unsharp 0.7 px amount 0.7) and film / gate defects with weave (the characterization's
+    dust and scratch families at slot probabilities 0.02 / 0.05 / 0.01 / 0.02)."""
     if not next_rows:
         return frame_records.FrameRecord(recipe, W, H)
     from film_juicer_b200 import descriptors
@@ -238,7 +239,8 @@ def workload_record(frame_records, recipe, W, H, next_rows: bool):
     post = descriptors.scanner_post_record(glare_percent=0.3, glare_roughness=0.4, glare_blur_sigma_px=4.0,
                                            lens_blur_sigma_px=0.8, unsharp_sigma_px=0.7, unsharp_amount=0.7)
     boost = descriptors.highlight_boost_record(4.0, 3.0, 1.5)
-    return frame_records.FrameRecord(recipe, W, H, post=post, highlight_boost=boost)
+    effects = descriptors.default_film_effects(W, H)
+    return frame_records.FrameRecord(recipe, W, H, post=post, highlight_boost=boost, effects=effects)
 
 
 def run_b200(args):
@@ -390,7 +392,8 @@ def run_b200(args):
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{W}x{H} full optical print through fj_cuda_render"
-                                   + (" + highlight reconstruction + scanner post effects" if args.next_rows else ""),
+                                   + (" + highlight reconstruction + scanner post effects + film/gate defects and weave"
+                                      if args.next_rows else ""),
                        "recipe": "kodak_portra_400 -> kodak_portra_endura, Hanatos TC LUT, spatial DIR tail 200 um "
                                  "w 0.03, camera diffusion r=0.5% W, scatter/halation, grain 35 mm, scanner LUT r=17, "
                                  "OkLch gamut, sRGB",

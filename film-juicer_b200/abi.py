@@ -259,8 +259,8 @@ FjPreparedHostData = _s("FjPreparedHostData", [
 FjDiffusionComponents = _s("FjDiffusionComponents", [("lambda_px", f64 * 9), ("red_weights", f64 * 9),
                                                      ("green_weights", f64 * 9), ("blue_weights", f64 * 9)])
 FJB_STAGE_NAMES = ["auto_exposure", "camera_exposure", "camera_diffusion", "scatter_halation", "spatial_dir",
-                   "capture_density", "grain", "print_scan_output", "monolithic"]
-FjbStageTimes = _s("FjbStageTimes", [("total_ms", f64 * 9), ("frames", u64 * 9)])
+                   "capture_density", "grain", "print_scan_output", "monolithic", "film_defects"]
+FjbStageTimes = _s("FjbStageTimes", [("total_ms", f64 * 10), ("frames", u64 * 10)])
 FjbScannerLutInput = _s("FjbScannerLutInput", [
     ("eps_c", FjFloatSpan), ("eps_m", FjFloatSpan), ("eps_y", FjFloatSpan), ("weighted_x", FjFloatSpan),
     ("weighted_y", FjFloatSpan), ("weighted_z", FjFloatSpan), ("baseline_min", FjFloatSpan),

@@ -94,7 +94,8 @@ FjStatus render_from_density_post(FjbRecipe* recipe, const PostPlan& plan, uint6
                                   int32_t origin_y, const float* density_c, const float* density_m,
                                   const float* density_y, const float* src, ptrdiff_t src_row_bytes, float* dst,
                                   ptrdiff_t dst_row_bytes, int32_t width, int32_t height, uint32_t components,
-                                  float* scratch, const float* taps, cudaStream_t s, FjErrorBuffer* error) {
+                                  float* scratch, const float* taps, cudaStream_t s, FjErrorBuffer* error,
+                                  const OutputEffects& fx) {
     const size_t plane = ((size_t)width * (size_t)height + 63) / 64 * 64;
     float* lin[3] = {scratch, scratch + plane, scratch + 2 * plane};
     float* tmp = scratch + 3 * plane;
@@ -118,6 +119,7 @@ FjStatus render_from_density_post(FjbRecipe* recipe, const PostPlan& plan, uint6
     p.lin_g = lin[1];
     p.lin_b = lin[2];
     p.scan_glare = nullptr;
+    p.film_dust = fx.dust;
     cudaError_t e = cudaSuccess;
     if (plan.glare) {
         const uint32_t medium = p.scan_medium_negative ? 0u : 1u;
@@ -133,6 +135,16 @@ FjStatus render_from_density_post(FjbRecipe* recipe, const PostPlan& plan, uint6
     if (e == cudaSuccess && plan.lens_r > 0) e = launch_blur_planes(lin, tmps, 3, width, height, lens_w, plan.lens_r, s);
     if (e == cudaSuccess && plan.unsharp_r > 0)
         e = launch_unsharp_planes(lin, tmps, 3, width, height, unsharp_w, plan.unsharp_r, plan.unsharp_amount, s);
+    p.weave_active = fx.weave ? 1 : 0;
+    p.weave_dx = fx.weave_dx;
+    p.weave_dy = fx.weave_dy;
+    p.weave_cos = fx.weave_cos;
+    p.weave_sin = fx.weave_sin;
+    p.gate_mask = fx.gate_mask;
+    p.gate_w = fx.gate_w;
+    p.gate_h = fx.gate_h;
+    p.roi_x = fx.roi_x;
+    p.roi_y = fx.roi_y;
     if (e == cudaSuccess) e = launch_pixel_chain(p, PixelStage::LinearRgbToOutput, s);
     if (e != cudaSuccess) return cuda_status(e, error, "scanner post effects");
     write_error(error, "");

@@ -1,0 +1,493 @@
+// fjb_film_defects.cu -- procedural film and gate defects: dust and scratches.
+//
+// Restates src/Cuda/Scan/JuicerCudaScanPipeline.cu of the reference:
+//   identity / lanes   :803-819, :846-883  splitmix64 hashes of (session seed, clip token
+//                                           for the film families, cell x, cell y, family,
+//                                           slot); attribute lanes remixed per salt;
+//   candidates         :895-1136           compact dust (three ellipses), fibres and
+//                                           scratches (tapered four-vertex strokes);
+//   cross section      :1138-1243          union of the horizontal intervals of a
+//                                           candidate at one height, weighted by depth;
+//   coverage           :1245-1273          3 softness shifts x 8 rows x 3 columns;
+//   family             :1275-1320          candidates of the cells that can reach a
+//                                           pixel; retained *= 1 - strength * coverage;
+//   film defects       :2056-2079          dust transmittance plane, scratches scale the
+//                                           density planes;
+//   gate mask          :2081-2094          gate dust x gate scratch at the half-resolution
+//                                           gate grid (sample step x 2).
+// The hashing constants, the attribute lane numbers and the floating-point expressions
+// are the reference's: they define the defect pattern, which must match it bit for bit.
+//
+// B200 schedule. A CTA covers a 32 x 8 pixel tile. Its threads build the candidates of
+// the tile's cell range 256 at a time, one per thread, and keep -- in candidate order --
+// only the active ones whose bounding box, widened by softness and the pixel footprint,
+// can reach the tile; the tile's pixels then multiply over that short list. A candidate
+// that cannot reach a pixel contributes exactly 1 - strength * 0 = 1 to its product, so
+// the culling changes no result (candidates with a non-finite strength are kept). The
+// reference makes every pixel visit every candidate of its tile.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fjb_film_defects.h"
+#include "fjb_launches.h"
+
+namespace fjb {
+
+namespace {
+
+constexpr int kTileX = 32, kTileY = 8, kTileThreads = kTileX * kTileY;
+
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ULL;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+    return x ^ (x >> 31);
+}
+
+// 24 high bits of a remixed hash as a float in [0, 1).
+__device__ __forceinline__ float lane(uint64_t identity, unsigned k) {
+    const uint64_t h = mix64(identity ^ (0xD6E8FEB86659FD93ULL * ((uint64_t)k + 1ULL)));
+    return (float)((h >> 40) & 0xFFFFFFu) * (1.0f / 16777216.0f);
+}
+
+struct Particle {
+    float cx, cy, xmin, xmax, ymin, ymax, strength, softness;
+    float ex[3], ey[3], ea[3], eb[3], ec[3]; // ellipses: centre and x^2, xy, y^2 coefficients
+    float px[4], py[4], width[4], depth[4];  // stroke vertices (full widths)
+    int stroke, active;
+};
+
+struct Stroke {
+    float length, drift, angle;
+    float t[4], width[4], depth[4];
+};
+
+__device__ uint64_t particle_identity(const FjFilmEffects& e, int family, int64_t cell_x, int64_t cell_y, int slot) {
+    uint64_t h = mix64(e.session_seed);
+    if (family < 2) h = mix64(h ^ mix64(e.clip_token));
+    h = mix64(h ^ (uint64_t)cell_x);
+    h = mix64(h ^ (uint64_t)cell_y);
+    h = mix64(h ^ (0x8EBC6AF09C88C6E3ULL * (uint64_t)(family + 1)));
+    return mix64(h ^ (uint64_t)slot);
+}
+
+// Bulk / tail mixture of a length: t = v^3 spreads over the bulk or the tail range.
+__device__ float mixture(float u, float v, float minimum, float bulk_max, float maximum, float tail_fraction) {
+    const float t = v * v * v;
+    return u < tail_fraction ? bulk_max + (maximum - bulk_max) * t : minimum + (bulk_max - minimum) * t;
+}
+
+__device__ void make_stroke(Particle& q, uint64_t h, const Stroke& s) {
+    float dx[4] = {0.0f, (lane(h, 12) - 0.5f) * s.drift * s.length, (lane(h, 13) - 0.5f) * s.drift * s.length,
+                   (lane(h, 14) - 0.5f) * s.drift * s.length};
+    float total = 0.0f;
+    float widest = 0.0f;
+    for (int i = 1; i < 4; ++i) total += hypotf(dx[i] - dx[i - 1], s.length * (s.t[i] - s.t[i - 1]));
+    for (float w : s.width) widest = fmaxf(widest, w);
+    const float norm = s.length / total;
+    const float c = cosf(s.angle);
+    const float sn = sinf(s.angle);
+    q.stroke = 1;
+    q.xmin = q.ymin = 1.0e30f;
+    q.xmax = q.ymax = -1.0e30f;
+    for (int i = 0; i < 4; ++i) {
+        const float y = (s.t[i] - 0.5f) * s.length * norm;
+        const float x = dx[i] * norm;
+        q.px[i] = x * c - y * sn;
+        q.py[i] = x * sn + y * c;
+        q.width[i] = s.width[i];
+        q.depth[i] = s.depth[i];
+        q.xmin = fminf(q.xmin, q.px[i] - widest * 0.5f);
+        q.xmax = fmaxf(q.xmax, q.px[i] + widest * 0.5f);
+        q.ymin = fminf(q.ymin, q.py[i] - widest * 0.5f);
+        q.ymax = fmaxf(q.ymax, q.py[i] + widest * 0.5f);
+    }
+}
+
+// Piecewise-linear opacity over the faint / intermediate / dense thirds of the draw.
+__device__ float dust_opacity(const FjDust& d, bool fiber, float u) {
+    const float lo = fiber ? d.fiber_opacity_min : d.compact_opacity_min;
+    const float faint = fiber ? d.fiber_opacity_faint_end : d.compact_opacity_faint_end;
+    const float mid = fiber ? d.fiber_opacity_intermediate_end : d.compact_opacity_intermediate_end;
+    const float hi = fiber ? d.fiber_opacity_max : d.compact_opacity_max;
+    const float c1 = d.opacity_faint_cumulative;
+    const float c2 = d.opacity_intermediate_cumulative;
+    if (u < c1) return lo + (faint - lo) * (u / c1);
+    if (u < c2) return faint + (mid - faint) * ((u - c1) / (c2 - c1));
+    return mid + (hi - mid) * ((u - c2) / (1.0f - c2));
+}
+
+__device__ float softness_of(float u, float lo, float hi, float cap_fraction, float size) {
+    return fminf(lo + (hi - lo) * u * u, size * cap_fraction);
+}
+
+__device__ Particle make_particle(const FjFilmEffects& e, int family, int64_t cell_x, int64_t cell_y, int slot,
+                                  int offset_x, int offset_y) {
+    Particle q{};
+    const FjDust& dust = family == 0 ? e.film_dust : e.gate_dust;
+    const FjScratch& scratch = family == 1 ? e.film_scratch : e.gate_scratch;
+    const bool is_dust = family == 0 || family == 2;
+    const uint64_t h = particle_identity(e, family, cell_x, cell_y, slot);
+    if (lane(h, 0) >= (is_dust ? dust.slot_probability : scratch.slot_probability)) return q;
+    const float cw = is_dust ? dust.cell_width_mm : scratch.cell_width_mm;
+    const float ch = is_dust ? dust.cell_height_mm : scratch.cell_height_mm;
+    q.cx = ((float)offset_x + lane(h, 1)) * cw;
+    q.cy = ((float)offset_y + lane(h, 2)) * ch;
+    q.active = 1;
+    if (is_dust) {
+        const float angle = lane(h, 4) * 6.28318530718f;
+        const bool fiber = lane(h, 5) < dust.fiber_fraction;
+        q.strength = dust_opacity(dust, fiber, lane(h, 3));
+        if (fiber) {
+            const float length = dust.fiber_length_min_mm + (dust.fiber_length_max_mm - dust.fiber_length_min_mm) * lane(h, 6);
+            const float width = dust.fiber_width_min_mm + (dust.fiber_width_max_mm - dust.fiber_width_min_mm) * lane(h, 7);
+            q.softness = softness_of(lane(h, 47), dust.softness_min_mm, dust.softness_max_mm,
+                                     dust.softness_size_cap_fraction, width);
+            const float k1 = dust.fiber_first_knot_min + (dust.fiber_first_knot_max - dust.fiber_first_knot_min) * lane(h, 30);
+            const float k2 =
+                dust.fiber_second_knot_min + (dust.fiber_second_knot_max - dust.fiber_second_knot_min) * lane(h, 31);
+            Stroke s{};
+            s.length = length;
+            s.drift = dust.fiber_drift_fraction;
+            s.angle = angle;
+            s.t[0] = 0.0f;
+            s.t[1] = k1;
+            s.t[2] = k2;
+            s.t[3] = 1.0f;
+            const float wspan = dust.fiber_interior_width_max_fraction - dust.fiber_interior_width_min_fraction;
+            s.width[1] = width * (dust.fiber_interior_width_min_fraction + wspan * lane(h, 21));
+            s.width[2] = width * (dust.fiber_interior_width_min_fraction + wspan * lane(h, 22));
+            for (float& d : s.depth) d = 1.0f;
+            make_stroke(q, h, s);
+        } else {
+            const float diameter = mixture(lane(h, 6), lane(h, 7), dust.diameter_min_mm, dust.diameter_bulk_max_mm,
+                                           dust.diameter_max_mm, dust.diameter_tail_fraction);
+            q.softness = softness_of(lane(h, 47), dust.softness_min_mm, dust.softness_max_mm,
+                                     dust.softness_size_cap_fraction, diameter);
+            float ox[3]{}, oy[3]{}, rx[3]{}, ry[3]{}, rot[3]{};
+            rx[0] = 1.0f;
+            ry[0] = dust.compact_dominant_aspect_min +
+                    (dust.compact_dominant_aspect_max - dust.compact_dominant_aspect_min) * lane(h, 32);
+            rot[0] = angle;
+            const float dc = cosf(angle);
+            const float ds = sinf(angle);
+            float enclosing = 1.0f;
+            for (int i = 1; i < 3; ++i) {
+                rx[i] = dust.compact_subsidiary_scale_min +
+                        (dust.compact_subsidiary_scale_max - dust.compact_subsidiary_scale_min) * lane(h, 32 + i * 5);
+                const float aspect =
+                    dust.compact_subsidiary_aspect_min +
+                    (dust.compact_subsidiary_aspect_max - dust.compact_subsidiary_aspect_min) * lane(h, 33 + i * 5);
+                ry[i] = rx[i] * aspect;
+                const float polar = lane(h, 34 + i * 5) * 6.28318530718f;
+                const float radial = dust.compact_subsidiary_offset_max * sqrtf(lane(h, 35 + i * 5));
+                const float lx = radial * cosf(polar);
+                const float ly = radial * ry[0] * sinf(polar);
+                ox[i] = lx * dc - ly * ds;
+                oy[i] = lx * ds + ly * dc;
+                rot[i] = angle + (2.0f * lane(h, 36 + i * 5) - 1.0f) * dust.compact_subsidiary_angle_max_radians;
+                enclosing = fmaxf(enclosing, hypotf(ox[i], oy[i]) + fmaxf(rx[i], ry[i]));
+            }
+            const float scale = diameter * 0.5f / enclosing;
+            q.xmin = q.ymin = 1.0e30f;
+            q.xmax = q.ymax = -1.0e30f;
+            for (int i = 0; i < 3; ++i) {
+                const float a = rx[i] * scale;
+                const float b = ry[i] * scale;
+                const float c = cosf(rot[i]);
+                const float s = sinf(rot[i]);
+                q.ex[i] = ox[i] * scale;
+                q.ey[i] = oy[i] * scale;
+                q.ea[i] = c * c / (a * a) + s * s / (b * b);
+                q.eb[i] = c * s * (1.0f / (a * a) - 1.0f / (b * b));
+                q.ec[i] = s * s / (a * a) + c * c / (b * b);
+                const float hx = sqrtf(a * a * c * c + b * b * s * s);
+                const float hy = sqrtf(a * a * s * s + b * b * c * c);
+                q.xmin = fminf(q.xmin, q.ex[i] - hx);
+                q.xmax = fmaxf(q.xmax, q.ex[i] + hx);
+                q.ymin = fminf(q.ymin, q.ey[i] - hy);
+                q.ymax = fmaxf(q.ymax, q.ey[i] + hy);
+            }
+        }
+    } else {
+        const FjScratch& sp = scratch;
+        q.strength = sp.strength_min + (sp.strength_max - sp.strength_min) * lane(h, 3);
+        const float length =
+            mixture(lane(h, 6), lane(h, 7), sp.length_min_mm, sp.length_bulk_max_mm, sp.length_max_mm, sp.length_tail_fraction);
+        const float width =
+            mixture(lane(h, 8), lane(h, 9), sp.width_min_mm, sp.width_bulk_max_mm, sp.width_max_mm, sp.width_tail_fraction);
+        q.softness = softness_of(lane(h, 47), sp.softness_min_mm, sp.softness_max_mm, sp.softness_size_cap_fraction, width);
+        Stroke s{};
+        s.length = length;
+        s.drift = sp.drift_fraction;
+        const bool interrupted = lane(h, 30) < sp.interruption_probability;
+        if (interrupted) {
+            const float centre = sp.gap_center_min + (sp.gap_center_max - sp.gap_center_min) * lane(h, 31);
+            const float span = sp.gap_span_min + (sp.gap_span_max - sp.gap_span_min) * lane(h, 32);
+            s.t[1] = centre - span * 0.5f;
+            s.t[2] = centre + span * 0.5f;
+        } else {
+            s.t[1] = sp.first_knot_min + (sp.first_knot_max - sp.first_knot_min) * lane(h, 31);
+            s.t[2] = sp.second_knot_min + (sp.second_knot_max - sp.second_knot_min) * lane(h, 32);
+        }
+        s.t[3] = 1.0f;
+        for (int i = 0; i < 4; ++i) {
+            const float wf = sp.interior_width_min_fraction +
+                             (sp.interior_width_max_fraction - sp.interior_width_min_fraction) * lane(h, 33 + i);
+            s.width[i] = (i == 1 || i == 2 || lane(h, 37 + i) < sp.endpoint_abrupt_probability) ? width * wf : 0.0f;
+            s.depth[i] = sp.interior_depth_min_fraction +
+                         (sp.interior_depth_max_fraction - sp.interior_depth_min_fraction) * lane(h, 41 + i);
+        }
+        if (interrupted) s.depth[1] = s.depth[2] = 0.0f;
+        if (length <= sp.scuff_length_max_mm && lane(h, 45) < sp.scuff_probability)
+            s.angle = (2.0f * lane(h, 46) - 1.0f) * sp.scuff_angle_max_radians;
+        make_stroke(q, h, s);
+    }
+    return q;
+}
+
+// Length of the particle's cross section at height y inside [lo_x, hi_x], each piece
+// weighted by its depth (the deepest where pieces overlap).
+__device__ float cross_section(const Particle& q, float y, float lo_x, float hi_x) {
+    float lo[5]{}, hi[5]{}, depth[5]{};
+    int n = 0;
+    for (int i = 0; i < 3; ++i) {
+        float a = 0.0f, b = 0.0f;
+        if (!q.stroke) {
+            const float dy = y - q.ey[i];
+            const float disc = q.ea[i] - (q.ea[i] * q.ec[i] - q.eb[i] * q.eb[i]) * dy * dy;
+            if (disc <= 0.0f) continue;
+            const float centre = q.ex[i] - q.eb[i] * dy / q.ea[i];
+            const float half = sqrtf(disc) / q.ea[i];
+            a = centre - half;
+            b = centre + half;
+        } else {
+            // the tapered quadrilateral of segment i
+            const float dx = q.px[i + 1] - q.px[i];
+            const float dy = q.py[i + 1] - q.py[i];
+            const float inv = rsqrtf(dx * dx + dy * dy);
+            const float nx = -dy * inv * 0.5f;
+            const float ny = dx * inv * 0.5f;
+            const float vx[4] = {q.px[i] + nx * q.width[i], q.px[i + 1] + nx * q.width[i + 1],
+                                 q.px[i + 1] - nx * q.width[i + 1], q.px[i] - nx * q.width[i]};
+            const float vy[4] = {q.py[i] + ny * q.width[i], q.py[i + 1] + ny * q.width[i + 1],
+                                 q.py[i + 1] - ny * q.width[i + 1], q.py[i] - ny * q.width[i]};
+            a = 1.0e30f;
+            b = -1.0e30f;
+            for (int k = 0; k < 4; ++k) {
+                const int k1 = (k + 1) % 4;
+                if (y >= fminf(vy[k], vy[k1]) && y < fmaxf(vy[k], vy[k1])) {
+                    const float x = vx[k] + (y - vy[k]) / (vy[k1] - vy[k]) * (vx[k1] - vx[k]);
+                    a = fminf(a, x);
+                    b = fmaxf(b, x);
+                }
+            }
+        }
+        a = fmaxf(lo_x, a);
+        b = fminf(hi_x, b);
+        if (b > a) {
+            depth[n] = 1.0f;
+            if (q.stroke) {
+                const float dx = q.px[i + 1] - q.px[i];
+                const float dy = q.py[i + 1] - q.py[i];
+                const float mid = 0.5f * (a + b);
+                const float den = dx * dx + dy * dy;
+                const float t = fminf(1.0f, fmaxf(0.0f, ((mid - q.px[i]) * dx + (y - q.py[i]) * dy) / den));
+                depth[n] = q.depth[i] + (q.depth[i + 1] - q.depth[i]) * t;
+            }
+            lo[n] = a;
+            hi[n] = b;
+            ++n;
+        }
+    }
+    if (q.stroke) {
+        // round joints at the two interior vertices
+        for (int i = 1; i < 3; ++i) {
+            const float r = q.width[i] * 0.5f;
+            const float dy = y - q.py[i];
+            if (fabsf(dy) >= r) continue;
+            const float chord = sqrtf(fmaxf(0.0f, r * r - dy * dy));
+            const float a = fmaxf(lo_x, q.px[i] - chord);
+            const float b = fminf(hi_x, q.px[i] + chord);
+            if (b > a) {
+                lo[n] = a;
+                hi[n] = b;
+                depth[n] = q.depth[i];
+                ++n;
+            }
+        }
+    }
+    float ends[10]{};
+    for (int i = 0; i < n; ++i) {
+        ends[2 * i] = lo[i];
+        ends[2 * i + 1] = hi[i];
+    }
+    for (int i = 1; i < 2 * n; ++i)
+        for (int j = i; j > 0 && ends[j] < ends[j - 1]; --j) {
+            const float v = ends[j];
+            ends[j] = ends[j - 1];
+            ends[j - 1] = v;
+        }
+    float length = 0.0f;
+    for (int i = 1; i < 2 * n; ++i) {
+        const float mid = (ends[i - 1] + ends[i]) * 0.5f;
+        float strength = 0.0f;
+        for (int k = 0; k < n; ++k)
+            if (mid >= lo[k] && mid <= hi[k]) strength = fmaxf(strength, depth[k]);
+        length += (ends[i] - ends[i - 1]) * strength;
+    }
+    return length;
+}
+
+// Fraction of the pixel footprint (sx x sy mm at x, y) the particle covers, with its
+// softness as a 3 x 3 box of shifts.
+__device__ float coverage(const Particle& q, float x, float y, float sx, float sy) {
+    x -= q.cx;
+    y -= q.cy;
+    if (x + sx * 0.5f + q.softness < q.xmin || x - sx * 0.5f - q.softness > q.xmax ||
+        y + sy * 0.5f + q.softness < q.ymin || y - sy * 0.5f - q.softness > q.ymax)
+        return 0.0f;
+    float area = 0.0f;
+    for (int soft = 0; soft < 3; ++soft) {
+        const float shift = ((float)soft - 1.0f) * q.softness;
+        const float bottom = fmaxf(q.ymin, y - sy * 0.5f + shift);
+        const float top = fminf(q.ymax, y + sy * 0.5f + shift);
+        if (!(top > bottom)) continue;
+        float sum = 0.0f;
+        for (int row = 0; row < 8; ++row) {
+            const float yy = bottom + ((float)row + 0.5f) * (top - bottom) / 8.0f;
+            for (int col = 0; col < 3; ++col) {
+                const float off = ((float)col - 1.0f) * q.softness;
+                sum += cross_section(q, yy, x - sx * 0.5f + off, x + sx * 0.5f + off);
+            }
+        }
+        area += sum * (top - bottom) / 72.0f;
+    }
+    return fminf(1.0f, fmaxf(0.0f, area / (sx * sy)));
+}
+
+// One family at the pixels of a tile: `tile` is the tile's first pixel in the family's
+// pixel grid, (px, py) this thread's pixel there, `scale` the grid's step in sample
+// steps. Returns the retained fraction (1 when the family is off).
+__device__ float family_retained(const FjFilmEffects& e, int family, int tile_x, int tile_y, int px, int py, float scale,
+                                 Particle* list, int* counts) {
+    const bool is_dust = family == 0 || family == 2;
+    const FjDust& dp = family == 0 ? e.film_dust : e.gate_dust;
+    const FjScratch& sp = family == 1 ? e.film_scratch : e.gate_scratch;
+    const float probability = is_dust ? dp.slot_probability : sp.slot_probability;
+    if (!(probability > 0.0f)) return 1.0f;
+    const float cw = is_dust ? dp.cell_width_mm : sp.cell_width_mm;
+    const float ch = is_dust ? dp.cell_height_mm : sp.cell_height_mm;
+    const float support_x = is_dust ? dp.support_x_mm + dp.softness_max_mm : sp.support_x_mm + sp.softness_max_mm;
+    const float support_y = is_dust ? dp.support_y_mm + dp.softness_max_mm : sp.support_y_mm + sp.softness_max_mm;
+    const FjDefectOrigin& origin = e.origins[family];
+    const float step_x = e.sample_step_x_mm * scale;
+    const float step_y = e.sample_step_y_mm * scale;
+    const float base_x = origin.local_x_mm;
+    const float base_y = origin.local_y_mm;
+    const int x0 = (int)floorf((base_x + (float)tile_x * step_x - support_x) / cw);
+    const int y0 = (int)floorf((base_y + (float)tile_y * step_y - support_y) / ch);
+    const int x1 = (int)floorf((base_x + (float)(tile_x + kTileX) * step_x + support_x) / cw);
+    const int y1 = (int)floorf((base_y + (float)(tile_y + kTileY) * step_y + support_y) / ch);
+    const int columns = x1 - x0 + 1;
+    const int total = columns * (y1 - y0 + 1) * 2;
+    const float x = base_x + ((float)px + 0.5f) * step_x;
+    const float y = base_y + ((float)py + 0.5f) * step_y;
+    // the tile's extreme pixel positions, for the conservative reach test
+    const float tx_lo = base_x + ((float)tile_x + 0.5f) * step_x;
+    const float tx_hi = base_x + ((float)(tile_x + kTileX - 1) + 0.5f) * step_x;
+    const float ty_lo = base_y + ((float)tile_y + 0.5f) * step_y;
+    const float ty_hi = base_y + ((float)(tile_y + kTileY - 1) + 0.5f) * step_y;
+    const int t = threadIdx.y * blockDim.x + threadIdx.x;
+    const int lane_id = t & 31, warp = t >> 5;
+    float retained = 1.0f;
+    for (int first = 0; first < total; first += kTileThreads) {
+        const int ordinal = first + t;
+        bool keep = false;
+        Particle q;
+        if (ordinal < total) {
+            const int dx = x0 + (ordinal / 2) % columns;
+            const int dy = y0 + (ordinal / 2) / columns;
+            q = make_particle(e, family, origin.cell_x + dx, origin.cell_y + dy, ordinal % 2, dx, dy);
+            if (q.active) {
+                // the per-pixel early-out of coverage(), at the tile's extreme pixels: each
+                // side is monotone in the pixel position, so a side that holds there holds
+                // for every pixel of the tile
+                const float xl = tx_lo - q.cx, xh = tx_hi - q.cx, yl = ty_lo - q.cy, yh = ty_hi - q.cy;
+                const bool away = xh + step_x * 0.5f + q.softness < q.xmin || xl - step_x * 0.5f - q.softness > q.xmax ||
+                                  yh + step_y * 0.5f + q.softness < q.ymin || yl - step_y * 0.5f - q.softness > q.ymax;
+                keep = !away || !isfinite(q.strength);
+            }
+        }
+        // order-preserving compaction of the kept candidates
+        const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+        if (lane_id == 0) counts[warp] = __popc(ballot);
+        __syncthreads();
+        int before = 0, kept = 0;
+        for (int w = 0; w < kTileThreads / 32; ++w) {
+            before += w < warp ? counts[w] : 0;
+            kept += counts[w];
+        }
+        if (keep) list[before + __popc(ballot & ((1u << lane_id) - 1u))] = q;
+        __syncthreads();
+        for (int i = 0; i < kept; ++i) retained *= 1.0f - list[i].strength * coverage(list[i], x, y, step_x, step_y);
+        __syncthreads();
+    }
+    return retained;
+}
+
+__global__ void __launch_bounds__(kTileThreads) film_defects_kernel(const __grid_constant__ FjFilmEffects e, int width,
+                                                                    int height, float* c, float* m, float* yp,
+                                                                    float* dust_out) {
+    __shared__ Particle list[kTileThreads];
+    __shared__ int counts[kTileThreads / 32];
+    const int tx = blockIdx.x * kTileX, ty = blockIdx.y * kTileY;
+    const int x = tx + threadIdx.x, y = ty + threadIdx.y;
+    const int fx = x + e.roi_offset_x, fy = y + e.roi_offset_y;
+    const int tfx = tx + e.roi_offset_x, tfy = ty + e.roi_offset_y;
+    const float dust = family_retained(e, 0, tfx, tfy, fx, fy, 1.0f, list, counts);
+    const float retained = family_retained(e, 1, tfx, tfy, fx, fy, 1.0f, list, counts);
+    if (x < width && y < height) {
+        const size_t i = (size_t)y * width + x;
+        if (dust_out) dust_out[i] = dust;
+        if (e.film_scratch.slot_probability > 0.0f) {
+            c[i] *= retained;
+            m[i] *= retained;
+            yp[i] *= retained;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kTileThreads) gate_mask_kernel(const __grid_constant__ FjFilmEffects e, float* mask,
+                                                                 int width, int height) {
+    __shared__ Particle list[kTileThreads];
+    __shared__ int counts[kTileThreads / 32];
+    const int tx = blockIdx.x * kTileX, ty = blockIdx.y * kTileY;
+    const int x = tx + threadIdx.x, y = ty + threadIdx.y;
+    const float dust = family_retained(e, 2, tx, ty, x, y, 2.0f, list, counts);
+    const float scratch = family_retained(e, 3, tx, ty, x, y, 2.0f, list, counts);
+    if (x < width && y < height) mask[(size_t)y * width + x] = dust * scratch;
+}
+
+} // namespace
+
+cudaError_t launch_film_defects(const FjFilmEffects& e, int width, int height, float* c, float* m, float* y,
+                                float* dust_out, cudaStream_t stream) {
+    if (width <= 0 || height <= 0) return cudaSuccess;
+    if (e.film_dust.slot_probability > 0.0f && !dust_out) return cudaErrorInvalidValue;
+    fjb::count_launch();
+    film_defects_kernel<<<dim3((width + kTileX - 1) / kTileX, (height + kTileY - 1) / kTileY), dim3(kTileX, kTileY), 0,
+                          stream>>>(e, width, height, c, m, y, dust_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gate_mask(const FjFilmEffects& e, float* mask, int width, int height, cudaStream_t stream) {
+    if (!mask || width <= 0 || height <= 0) return cudaErrorInvalidValue;
+    fjb::count_launch();
+    gate_mask_kernel<<<dim3((width + kTileX - 1) / kTileX, (height + kTileY - 1) / kTileY), dim3(kTileX, kTileY), 0,
+                       stream>>>(e, mask, width, height);
+    return cudaGetLastError();
+}
+
+} // namespace fjb

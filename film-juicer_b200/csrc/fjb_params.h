@@ -148,6 +148,14 @@ struct PixelParams {
     float* lin_r;
     float* lin_g;
     float* lin_b;
+    // film defects: dust transmittance plane (null when off), applied to the print
+    // exposure on the print route and to the scanned XYZ on the direct route
+    const float* film_dust;
+    // gate output (encoding of linear planes): weave resampling and the gate mask
+    int weave_active;
+    float weave_dx, weave_dy, weave_cos, weave_sin;
+    const float* gate_mask; // gate_w x gate_h, sampled at (roi + pixel) / 2 - 1/4
+    int gate_w, gate_h, roi_x, roi_y;
 
     // ---- output colour ----
     float cat02[9];

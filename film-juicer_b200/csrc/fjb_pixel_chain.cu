@@ -132,14 +132,16 @@ __global__ void __launch_bounds__(kPixelThreads) pixel_chain_kernel(const __grid
         }
 
         if constexpr (Print) {
-            print_develop(p, blob, d);
+            print_develop(p, blob, d, p.film_dust ? p.film_dust[idx] : 1.0f);
         }
+        // the direct route scans the film itself: its dust darkens the scanned XYZ
+        const float* dust = !Print && p.film_dust ? p.film_dust + idx : nullptr;
 
         double rgb[3];
         if constexpr (Out == kOutLinearRgb) {
             // src/Cuda/Scan/JuicerCudaScanPipeline.cu:1944-2037 scan_linear_density_rgb_kernel
             const float glare = p.scan_glare ? p.scan_glare[idx] : -1.0f;
-            if (!scan_to_linear(p, d, rgb, glare)) {
+            if (!scan_to_linear(p, d, rgb, glare, dust)) {
                 flag_scan_failure(p);
                 rgb[0] = rgb[1] = rgb[2] = 0.0;
             }
@@ -149,7 +151,7 @@ __global__ void __launch_bounds__(kPixelThreads) pixel_chain_kernel(const __grid
             continue;
         }
         float* dstPix = reinterpret_cast<float*>(p.dst + (long long)y * p.dst_row_bytes) + (long long)x * p.components;
-        if (!scan_to_linear(p, d, rgb)) {
+        if (!scan_to_linear(p, d, rgb, -1.0f, dust)) {
             flag_scan_failure(p);
             dstPix[0] = 0.0f;
             dstPix[1] = 0.0f;
@@ -165,15 +167,73 @@ __global__ void __launch_bounds__(kPixelThreads) pixel_chain_kernel(const __grid
     }
 }
 
+// Mitchell (B = C = 1/3) sample of a plane at (x, y), clamped to the edge, summed in
+// FP64 (src/Cuda/Scan/JuicerCudaScanPipeline.cu:1514-1556).
+__device__ float plane_mitchell(const float* __restrict__ plane, int width, int height, float x, float y) {
+    x = fminf(fmaxf(x, 0.0f), (float)(width - 1));
+    y = fminf(fmaxf(y, 0.0f), (float)(height - 1));
+    const int ix = (int)floorf(x), iy = (int)floorf(y);
+    const float tx = x - (float)ix, ty = y - (float)iy;
+    const float wx[4] = {mitchell(tx + 1.0f), mitchell(tx), mitchell(tx - 1.0f), mitchell(tx - 2.0f)};
+    const float wy[4] = {mitchell(ty + 1.0f), mitchell(ty), mitchell(ty - 1.0f), mitchell(ty - 2.0f)};
+    double acc = 0.0;
+    for (int j = 0; j < 4; ++j) {
+        const int sy = min(max(iy + j - 1, 0), height - 1);
+        const double wyj = wy[j];
+        const float* row = plane + (size_t)sy * width;
+        for (int i = 0; i < 4; ++i) {
+            const int sx = min(max(ix + i - 1, 0), width - 1);
+            acc += wyj * wx[i] * (double)__ldg(row + sx);
+        }
+    }
+    return (float)acc;
+}
+
+// Bilinear sample of the gate mask, clamped (src/Cuda/Scan/JuicerCudaScanPipeline.cu:1331-1360).
+__device__ float gate_sample(const float* __restrict__ mask, int width, int height, float x, float y) {
+    const float fx = fminf(fmaxf(x, 0.0f), (float)(width - 1));
+    const float fy = fminf(fmaxf(y, 0.0f), (float)(height - 1));
+    const int x0 = (int)floorf(fx), y0 = (int)floorf(fy);
+    const int x1 = x0 + 1 < width ? x0 + 1 : x0;
+    const int y1 = y0 + 1 < height ? y0 + 1 : y0;
+    const float tx = fx - (float)x0, ty = fy - (float)y0;
+    const float m00 = __ldg(mask + y0 * width + x0), m10 = __ldg(mask + y0 * width + x1);
+    const float m01 = __ldg(mask + y1 * width + x0), m11 = __ldg(mask + y1 * width + x1);
+    const float m0 = m00 + (m10 - m00) * tx;
+    const float m1 = m01 + (m11 - m01) * tx;
+    return m0 + (m1 - m0) * ty;
+}
+
 // Encoding of linear output-RGB planes (src/Cuda/Scan/JuicerCudaScanPipeline.cu:2096-2182
-// focused_scan_output_encode_kernel, without gate defects and weave).
+// focused_scan_output_encode_kernel): with gate weave the planes are resampled along the
+// frame's shift and rotation about its centre; the gate mask multiplies the result.
 __global__ void __launch_bounds__(kPixelThreads) encode_planes_kernel(const __grid_constant__ PixelParams p) {
     const long long total = (long long)p.width * (long long)p.height;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
         const int y = (int)(idx / p.width);
         const int x = (int)(idx - (long long)y * p.width);
-        double rgb[3] = {(double)p.lin_r[idx], (double)p.lin_g[idx], (double)p.lin_b[idx]};
+        double rgb[3];
+        if (p.weave_active) {
+            const float cx = 0.5f * (float)(p.width - 1), cy = 0.5f * (float)(p.height - 1);
+            const float ox = (float)x - cx, oy = (float)y - cy;
+            const float sx = p.weave_cos * ox - p.weave_sin * oy + cx + p.weave_dx;
+            const float sy = p.weave_sin * ox + p.weave_cos * oy + cy + p.weave_dy;
+            rgb[0] = plane_mitchell(p.lin_r, p.width, p.height, sx, sy);
+            rgb[1] = plane_mitchell(p.lin_g, p.width, p.height, sx, sy);
+            rgb[2] = plane_mitchell(p.lin_b, p.width, p.height, sx, sy);
+        } else {
+            rgb[0] = (double)p.lin_r[idx];
+            rgb[1] = (double)p.lin_g[idx];
+            rgb[2] = (double)p.lin_b[idx];
+        }
+        if (p.gate_mask && p.gate_w > 0 && p.gate_h > 0) {
+            const double t = (double)gate_sample(p.gate_mask, p.gate_w, p.gate_h, (float)(p.roi_x + x) * 0.5f - 0.25f,
+                                                 (float)(p.roi_y + y) * 0.5f - 0.25f);
+            rgb[0] *= t;
+            rgb[1] *= t;
+            rgb[2] *= t;
+        }
         encode_output(p, rgb);
         float* dstPix = reinterpret_cast<float*>(p.dst + (long long)y * p.dst_row_bytes) + (long long)x * p.components;
         dstPix[0] = (float)rgb[0];

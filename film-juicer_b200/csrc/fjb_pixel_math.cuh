@@ -540,9 +540,13 @@ __device__ __forceinline__ void print_spectral(const PrintSpectral& s, const flo
     }
 }
 
-__device__ __forceinline__ void print_develop(const PixelParams& p, const float* __restrict__ blob, float d[3]) {
+// `dust`: film dust transmittance of the pixel (src/Cuda/JuicerCudaDeviceHelpers.cuh:1062-1066).
+__device__ __forceinline__ void print_develop(const PixelParams& p, const float* __restrict__ blob, float d[3],
+                                              float dust = 1.0f) {
     float raw[3];
     print_spectral(p.spectral, d, raw);
+    if (dust != 1.0f)
+        for (int c = 0; c < 3; ++c) raw[c] *= dust;
     const float k = p.print_midgray;
     for (int c = 0; c < 3; ++c) raw[c] *= k;
     const float pf = p.print_preflash_exposure;
@@ -770,8 +774,10 @@ __device__ __forceinline__ void encode_output(const PixelParams& p, double rgb[3
 // (src/Cuda/Scan/JuicerCudaScanPipeline.cu:1757-1858)
 // ---------------------------------------------------------------------------
 // glare: the scanner-glare percent of the pixel, or a negative value for none.
+// dust: film dust transmittance of the pixel, when the direct route scans a frame with
+// film defects (src/Cuda/Scan/JuicerCudaScanPipeline.cu:2006-2011).
 __device__ __forceinline__ bool scan_to_linear(const PixelParams& p, const float d[3], double rgb[3],
-                                               float glare_percent = -1.0f) {
+                                               float glare_percent = -1.0f, const float* dust = nullptr) {
     double nd[3];
     for (int c = 0; c < 3; ++c) {
         if (p.scan_medium_negative) {
@@ -783,6 +789,12 @@ __device__ __forceinline__ bool scan_to_linear(const PixelParams& p, const float
     float l2[3];
     if (!scan_lut_sample(p, nd, l2)) return false;
     double xyz[3] = {(double)exp2f(l2[0]), (double)exp2f(l2[1]), (double)exp2f(l2[2])};
+    if (dust) {
+        const double t = *dust;
+        xyz[0] *= t;
+        xyz[1] *= t;
+        xyz[2] *= t;
+    }
     if (p.correction_active) {
         const double cy = fmin(fmax((double)p.correction_slope * xyz[1] + (double)p.correction_offset, 0.0), 1.0);
         const double sc = cy / (xyz[1] + 1e-10);

@@ -49,12 +49,23 @@ uint64_t glare_seed(uint64_t recipe_hash, uint64_t frame_token, int32_t x1, int3
 size_t post_scratch_floats(int width, int height);
 std::vector<float> post_taps(const PostPlan& plan);
 
+// Film-defect effects on the way out: the dust transmittance plane, and with the gate
+// output on, weave and gate mask at the encoding.
+struct OutputEffects {
+    const float* dust = nullptr;
+    bool weave = false;
+    float weave_dx = 0.0f, weave_dy = 0.0f, weave_cos = 1.0f, weave_sin = 0.0f;
+    const float* gate_mask = nullptr;
+    int gate_w = 0, gate_h = 0, roi_x = 0, roi_y = 0;
+};
+
 // Density planes -> glare -> linear output RGB -> lens blur -> unsharp -> encoded dst.
 // `taps` (device) holds post_taps(plan).
 FjStatus render_from_density_post(FjbRecipe* recipe, const PostPlan& plan, uint64_t seed, int32_t origin_x,
                                   int32_t origin_y, const float* density_c, const float* density_m,
                                   const float* density_y, const float* src, ptrdiff_t src_row_bytes, float* dst,
                                   ptrdiff_t dst_row_bytes, int32_t width, int32_t height, uint32_t components,
-                                  float* scratch, const float* taps, cudaStream_t s, FjErrorBuffer* error);
+                                  float* scratch, const float* taps, cudaStream_t s, FjErrorBuffer* error,
+                                  const OutputEffects& fx = OutputEffects{});
 
 } // namespace fjb

@@ -22,6 +22,7 @@
 #include "../../include/juicer_cuda_api.h"
 #include "fjb_diffusion.h"
 #include "fjb_highlight_boost.h"
+#include "fjb_film_defects.h"
 #include "fjb_scanner_post.h"
 #include "fjb_dir.h"
 #include "fjb_internal.h"
@@ -211,10 +212,8 @@ bool stages_supported(const FjPreparedHostData& h, std::string& why) {
     }
     fjb::PostPlan post;
     if (!fjb::post_plan_from(h.scanner_post, post, why)) return false;
-    if (h.effects.flags & (FJ_EFFECTS_FILM | FJ_EFFECTS_GATE_OUTPUT)) {
-        why = "film and gate defects are not supported by this build";
-        return false;
-    }
+    fjb::EffectsPlan effects;
+    if (!fjb::effects_plan_from(h.effects, effects, why)) return false;
     return true;
 }
 
@@ -263,17 +262,22 @@ FjStatus ensure_noise(FjCuda* cuda, const FjStaticNoise& n, void* stream, const 
 FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData& h, const float* src, ptrdiff_t srb,
                        float* dst, ptrdiff_t drb, int width, int height, uint32_t comps, void* vs,
                        const FjAbortCallback& abort_cb, bool camera_diffusion, bool halation, bool spatial_dir,
-                       bool grain, const fjb::PostPlan& post, uint64_t glare_seed, int glare_x, int glare_y,
-                       FjErrorBuffer* error) {
+                       bool grain, const fjb::PostPlan& post, const fjb::EffectsPlan& fx, uint64_t glare_seed,
+                       int glare_x, int glare_y, FjErrorBuffer* error) {
     const size_t plane = (size_t)width * (size_t)height;
     const size_t plane_bytes = (plane * sizeof(float) + 255) / 256 * 256;
+    // linear planes before the encoding: scanner post effects or film / gate defects
+    const bool planes_out = post.active || fx.film || fx.gate_output;
     size_t scratch = 0;
-    if (post.active) scratch = std::max(scratch, fjb_scanner_post_scratch_bytes(width, height));
+    if (planes_out) scratch = std::max(scratch, fjb_scanner_post_scratch_bytes(width, height));
     if (halation) scratch = std::max(scratch, fjb_scatter_halation_scratch_bytes(width, height));
     if (spatial_dir) scratch = std::max(scratch, fjb_spatial_dir_scratch_bytes(width, height));
     if (grain) scratch = std::max(scratch, fjb_visual_grain_scratch_bytes(width, height));
-    const int planes = 3 + 3 + (spatial_dir ? 6 : 0);
-    cudaError_t e = ensure_work(cuda, planes * plane_bytes + scratch + 256);
+    const int planes = 3 + 3 + (spatial_dir ? 6 : 0) + (fx.film_dust ? 1 : 0);
+    const size_t mask_bytes =
+        fx.gate_mask ? ((size_t)h.effects.gate_width * (size_t)h.effects.gate_height * sizeof(float) + 255) / 256 * 256
+                     : 0;
+    cudaError_t e = ensure_work(cuda, planes * plane_bytes + scratch + mask_bytes + 256);
     FjStatus st{};
     if (e != cudaSuccess) return fjb::cuda_status(e, error, "frame workspace");
     char* base = static_cast<char*>(cuda->work);
@@ -283,7 +287,9 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
     float* dirp[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     if (spatial_dir)
         for (int i = 0; i < 6; ++i) dirp[i] = P(6 + i);
+    float* dust = fx.film_dust ? P(planes - 1) : nullptr;
     float* scratch_p = reinterpret_cast<float*>(base + (size_t)planes * plane_bytes);
+    float* gate_mask = fx.gate_mask ? reinterpret_cast<float*>(base + (size_t)planes * plane_bytes + scratch) : nullptr;
     const ptrdiff_t stride = width;
     const FjOptics& o = h.optics;
 
@@ -430,7 +436,37 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
         if (st.category != FJ_STATUS_SUCCESS) return st;
         if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
     }
-    if (post.active) {
+    if (fx.film) {
+        // film dust and scratches on the developed capture density, after grain
+        // (src/Cuda/JuicerCudaExecutor.cpp:1674-1690, :2263-2279)
+        stage_begin(cuda, FJB_STAGE_FILM_DEFECTS, vs);
+        e = fjb::launch_film_defects(h.effects, width, height, density[0], density[1], density[2], dust,
+                                     reinterpret_cast<cudaStream_t>(vs));
+        stage_end(cuda, FJB_STAGE_FILM_DEFECTS, vs);
+        if (e != cudaSuccess) return fjb::cuda_status(e, error, "film defects");
+    }
+    if (planes_out) {
+        fjb::OutputEffects out;
+        out.dust = dust;
+        if (fx.gate_output) {
+            const FjFilmEffects& fe = h.effects;
+            out.weave = fx.weave;
+            out.weave_dx = fe.weave_dx_px;
+            out.weave_dy = fe.weave_dy_px;
+            out.weave_cos = fe.weave_cos_rot;
+            out.weave_sin = fe.weave_sin_rot;
+            out.roi_x = fe.roi_offset_x;
+            out.roi_y = fe.roi_offset_y;
+            if (fx.gate_mask) {
+                // gate dust and scratches at the gate grid (src/Cuda/JuicerCudaExecutor.cpp:2788-2790)
+                e = fjb::launch_gate_mask(fe, gate_mask, fe.gate_width, fe.gate_height,
+                                          reinterpret_cast<cudaStream_t>(vs));
+                if (e != cudaSuccess) return fjb::cuda_status(e, error, "gate mask");
+                out.gate_mask = gate_mask;
+                out.gate_w = fe.gate_width;
+                out.gate_h = fe.gate_height;
+            }
+        }
         // scanner post effects: taps kept on the device per descriptor
         const std::vector<float> taps = fjb::post_taps(post);
         if (cuda->post_key != h.scanner_post.hash || (!taps.empty() && !cuda->post_taps)) {
@@ -448,7 +484,8 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
         stage_begin(cuda, FJB_STAGE_PRINT_SCAN_OUTPUT, vs);
         st = fjb::render_from_density_post(recipe, post, glare_seed, glare_x, glare_y, density[0], density[1],
                                            density[2], comps == 4 ? src : nullptr, srb, dst, drb, width, height, comps,
-                                           scratch_p, cuda->post_taps, reinterpret_cast<cudaStream_t>(vs), error);
+                                           scratch_p, cuda->post_taps, reinterpret_cast<cudaStream_t>(vs), error,
+                                           out);
         stage_end(cuda, FJB_STAGE_PRINT_SCAN_OUTPUT, vs);
         return st;
     }
@@ -548,6 +585,16 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
                             !same_rect(frame->destination.bounds, frame->full_frame_extent) ||
                             !same_rect(frame->render_window, frame->full_frame_extent))) {
             out.status = fjb::fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "CUDA optics require the complete frame domain");
+            return out;
+        }
+        // a weave-carrying effects record needs the complete frame domain, as the optics
+        // do (src/Cuda/JuicerCudaExecutor.cpp:752-768)
+        if ((prepared->effects.flags & FJ_EFFECTS_FULL_FRAME) != 0 &&
+            (prepared->effects.flags & (FJ_EFFECTS_FILM | FJ_EFFECTS_GATE_OUTPUT)) != 0 &&
+            (!same_rect(frame->source.bounds, frame->full_frame_extent) ||
+             !same_rect(frame->destination.bounds, frame->full_frame_extent) ||
+             !same_rect(frame->render_window, frame->full_frame_extent))) {
+            out.status = fjb::fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "film effects require the complete frame domain");
             return out;
         }
         std::string unsupported;
@@ -650,7 +697,16 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
             }
         }
         const bool boost = (optics & FJ_OPTICS_HIGHLIGHT_BOOST) != 0;
-        if (!camera_diffusion && !halation && !spatial_dir && !grain && !post.active && !boost) {
+        fjb::EffectsPlan fx;
+        {
+            std::string why;
+            if (!fjb::effects_plan_from(prepared->effects, fx, why)) {
+                out.status = fjb::fail_status(FJ_STATUS_PREPARATION_FAILURE, error, why);
+                return out;
+            }
+        }
+        if (!camera_diffusion && !halation && !spatial_dir && !grain && !post.active && !boost && !fx.film &&
+            !fx.gate_output) {
             // Monolithic: one fused pass source -> output
             stage_begin(cuda, FJB_STAGE_MONOLITHIC, vs);
             st = fjb_render_pixels(recipe, src, srb, dst, drb, width, height, comps, vs, error);
@@ -661,7 +717,7 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
             const uint64_t seed = fjb::glare_seed(prepared->recipe_hash, submission ? submission->frame_token : 0,
                                                   frame->source.bounds.x1, frame->source.bounds.y1);
             st = render_staged(cuda, recipe, *prepared, src, srb, dst, drb, width, height, comps, vs, abort_callback,
-                               camera_diffusion, halation, spatial_dir, grain, post, seed, frame->source.bounds.x1,
+                               camera_diffusion, halation, spatial_dir, grain, post, fx, seed, frame->source.bounds.x1,
                                frame->source.bounds.y1, error);
         }
         if (st.category != FJ_STATUS_SUCCESS) {

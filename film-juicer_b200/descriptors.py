@@ -142,3 +142,77 @@ def highlight_boost_record(protection: float = 1.0, sharpness: float = 4.0, peak
     d.sharpness = sharpness
     d.peak_gain = peak_gain
     return d
+
+
+def film_effects_record(*, film_dust: dict | None = None, film_scratch: dict | None = None,
+                        gate_dust: dict | None = None, gate_scratch: dict | None = None, origins=(), flags: int = 0,
+                        sample_step_mm=(0.0, 0.0), roi_offset=(0, 0), gate_size=(0, 0), session_seed: int = 0,
+                        clip_token: int = 0, weave=(0.0, 0.0, 1.0, 0.0), extent=(0, 0, 0, 0),
+                        recipe_hash: int = 1, hash: int = 1) -> "abi.FjFilmEffects":
+    """An FjFilmEffects record (film / gate dust and scratches, weave) from field values:
+    the family dicts map FjDust / FjScratch field names to floats; origins are up to four
+    (cell_x, cell_y, local_x_mm, local_y_mm); weave is (dx_px, dy_px, cos, sin)."""
+    e = abi.FjFilmEffects()
+    for name, values in (("film_dust", film_dust), ("film_scratch", film_scratch), ("gate_dust", gate_dust),
+                         ("gate_scratch", gate_scratch)):
+        rec = getattr(e, name)
+        for k, v in (values or {}).items():
+            setattr(rec, k, float(v))
+    for i, o in enumerate(origins):
+        e.origins[i].cell_x, e.origins[i].cell_y, e.origins[i].local_x_mm, e.origins[i].local_y_mm = o
+    for ext in (e.render_extent, e.full_frame_extent):
+        ext.x, ext.y, ext.width, ext.height = extent
+    e.sample_step_x_mm, e.sample_step_y_mm = sample_step_mm
+    e.roi_offset_x, e.roi_offset_y = roi_offset
+    e.gate_width, e.gate_height = gate_size
+    e.session_seed, e.clip_token = session_seed, clip_token
+    e.weave_dx_px, e.weave_dy_px, e.weave_cos_rot, e.weave_sin_rot = weave
+    e.flags = flags
+    e.recipe_hash, e.hash = (recipe_hash, hash) if flags & (abi.FJ_EFFECTS_FILM | abi.FJ_EFFECTS_GATE_OUTPUT) else (0, 0)
+    return e
+
+
+# Film dust and scratch families of the reference's effects-frame characterization
+# (tests/film/effects-frame-fixtures/inputs.json, case 0), slot probabilities aside.
+DUST_FAMILY = dict(
+    cell_width_mm=0.5, cell_height_mm=0.5, softness_min_mm=0.00025, softness_max_mm=0.003,
+    softness_size_cap_fraction=0.25, support_x_mm=0.415, support_y_mm=0.415, fiber_fraction=0.25,
+    fiber_drift_fraction=0.1, fiber_first_knot_min=0.08, fiber_first_knot_max=0.35, fiber_second_knot_min=0.65,
+    fiber_second_knot_max=0.92, fiber_interior_width_min_fraction=0.45, fiber_interior_width_max_fraction=1.0,
+    diameter_min_mm=0.008, diameter_bulk_max_mm=0.08, diameter_max_mm=0.25, diameter_tail_fraction=0.2,
+    fiber_length_min_mm=0.04, fiber_length_max_mm=0.65, fiber_width_min_mm=0.003, fiber_width_max_mm=0.025,
+    opacity_faint_cumulative=0.5, opacity_intermediate_cumulative=0.85, compact_opacity_min=0.1,
+    compact_opacity_faint_end=0.45, compact_opacity_intermediate_end=0.85, compact_opacity_max=0.99,
+    fiber_opacity_min=0.08, fiber_opacity_faint_end=0.35, fiber_opacity_intermediate_end=0.75,
+    fiber_opacity_max=0.97, compact_dominant_aspect_min=0.52, compact_dominant_aspect_max=0.95,
+    compact_subsidiary_scale_min=0.3, compact_subsidiary_scale_max=0.75, compact_subsidiary_aspect_min=0.45,
+    compact_subsidiary_aspect_max=1.0, compact_subsidiary_offset_max=0.68,
+    compact_subsidiary_angle_max_radians=3.1415927)
+SCRATCH_FAMILY = dict(
+    cell_width_mm=1.0, cell_height_mm=8.0, softness_min_mm=0.00015, softness_max_mm=0.0015,
+    softness_size_cap_fraction=0.25, support_x_mm=0.68, support_y_mm=12.08, length_min_mm=0.25,
+    length_bulk_max_mm=6.0, length_max_mm=24.0, length_tail_fraction=0.16, width_min_mm=0.002,
+    width_bulk_max_mm=0.025, width_max_mm=0.08, width_tail_fraction=0.18, drift_fraction=0.025,
+    first_knot_min=0.06, first_knot_max=0.28, second_knot_min=0.72, second_knot_max=0.94,
+    interior_width_min_fraction=0.35, interior_width_max_fraction=1.0, interior_depth_min_fraction=0.35,
+    interior_depth_max_fraction=1.0, endpoint_abrupt_probability=0.3, interruption_probability=0.15,
+    gap_center_min=0.25, gap_center_max=0.75, gap_span_min=0.02, gap_span_max=0.12, scuff_probability=0.1,
+    scuff_length_max_mm=0.75, scuff_angle_max_radians=0.61086524, strength_min=0.1425, strength_max=0.95)
+
+
+def default_film_effects(width: int, height: int, *, frame_width_mm: float = 36.0,
+                         slots=(0.02, 0.05, 0.01, 0.02), weave=(-0.35, 0.22, 0.99995, 0.01),
+                         session_seed: int = 0x0123456789ABCDEF, clip_token: int = 0x0FEDCBA987654321):
+    """Film dust and scratches, gate dust and scratches (gate grid at half resolution) and
+    gate weave for a full frame of width x height pixels; `slots` are the slot
+    probabilities of film dust, film scratch, gate dust, gate scratch."""
+    step = frame_width_mm / width
+    fams = [dict(DUST_FAMILY, slot_probability=slots[0]), dict(SCRATCH_FAMILY, slot_probability=slots[1]),
+            dict(DUST_FAMILY, slot_probability=slots[2]), dict(SCRATCH_FAMILY, slot_probability=slots[3])]
+    flags = (abi.FJ_EFFECTS_FILM | abi.FJ_EFFECTS_GATE_TRANSMITTANCE | abi.FJ_EFFECTS_GATE_OUTPUT
+             | abi.FJ_EFFECTS_WEAVE | abi.FJ_EFFECTS_FULL_FRAME)
+    return film_effects_record(film_dust=fams[0], film_scratch=fams[1], gate_dust=fams[2], gate_scratch=fams[3],
+                               origins=[(0, 67, 0.0, 0.25), (0, 4, 0.0, 1.75), (0, 0, 0.0, 0.0), (0, 0, 0.0, 0.0)],
+                               flags=flags, sample_step_mm=(step, step), gate_size=((width + 1) // 2, (height + 1) // 2),
+                               session_seed=session_seed, clip_token=clip_token, weave=weave,
+                               extent=(0, 0, width, height), recipe_hash=0x5EED, hash=0xEFFEC7)

@@ -20,11 +20,12 @@ class FrameRecord:
                  diffusion: bool = True, halation: bool = True, spatial_dir: bool = True, grain: bool = True,
                  auto_exposure: bool = False, noise: "grain_plan.Noise | None" = None,
                  pixel_size_um: float | None = None, frame_time: float = 0.0, descriptor_width: int | None = None,
-                 post=None, highlight_boost=None):
+                 post=None, highlight_boost=None, effects=None):
         """descriptor_width: the frame width the pixel size and diffusion radius are
         derived for (defaults to `width`; a crop of a larger frame passes the full width);
         post: an FjScannerPostEffects record (descriptors.scanner_post_record);
-        highlight_boost: an FjHighlightBoost record (descriptors.highlight_boost_record)."""
+        highlight_boost: an FjHighlightBoost record (descriptors.highlight_boost_record);
+        effects: an FjFilmEffects record (film / gate defects, weave)."""
         self.width, self.height = width, height
         dw = descriptor_width or width
         self.pixel_size_um = pixel_size_um or 35000.0 / dw
@@ -52,6 +53,8 @@ class FrameRecord:
             h.spatial_dir = descriptors.spatial_dir_record(px, width, height)
         if post is not None:
             h.scanner_post = post
+        if effects is not None:
+            h.effects = effects
         self.noise = None
         if grain:
             a = recipe.arrays

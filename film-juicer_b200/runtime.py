@@ -367,6 +367,58 @@ def render_from_density_post(recipe: "DeviceRecipe", post, seed: int, origin, de
     return scratch
 
 
+def film_defects(effects: "abi.FjFilmEffects", density_cmy, dust=None, stream=None):
+    """fjb_film_defects on CUDA density planes (C, M, Y), in place: film scratches scale
+    the densities; the film dust transmittance goes to `dust` (allocated when None and
+    film dust is on). Returns the dust plane (or None)."""
+    torch = _torch()
+    lib = load_library()
+    h, w = density_cmy[0].shape
+    if dust is None and effects.film_dust.slot_probability > 0.0:
+        dust = torch.empty((h, w), dtype=torch.float32, device=density_cmy[0].device)
+    err = abi.ErrorText()
+    st = lib.fjb_film_defects(C.byref(effects), w, h, *[C.c_void_p(_ptr(t)) for t in density_cmy],
+                              C.c_void_p(_ptr(dust) if dust is not None else 0), C.c_void_p(_stream_handle(stream)),
+                              C.byref(err.buf))
+    _check("fjb_film_defects", st, err)
+    return dust
+
+
+def gate_mask(effects: "abi.FjFilmEffects", stream=None):
+    """fjb_gate_mask: the gate transmittance grid (gate_height, gate_width) on the GPU."""
+    torch = _torch()
+    lib = load_library()
+    mask = torch.empty((max(effects.gate_height, 1), max(effects.gate_width, 1)), dtype=torch.float32, device="cuda")
+    err = abi.ErrorText()
+    st = lib.fjb_gate_mask(C.byref(effects), C.c_void_p(_ptr(mask)), effects.gate_width, effects.gate_height,
+                           C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+    _check("fjb_gate_mask", st, err)
+    return mask
+
+
+def render_from_density_effects(recipe: "DeviceRecipe", post, seed: int, origin, effects, dust, mask, density_cmy,
+                                dst, src=None, stream=None, scratch=None):
+    """fjb_render_from_density_effects: render_from_density_post with the film dust plane
+    and, with the gate output on, weave and the gate mask at the encoding."""
+    torch = _torch()
+    lib = recipe.lib
+    h, w = density_cmy[0].shape
+    comps = dst.shape[2]
+    need = int(lib.fjb_scanner_post_scratch_bytes(w, h))
+    if scratch is None:
+        scratch = torch.empty(need // 4, dtype=torch.float32, device=dst.device)
+    err = abi.ErrorText()
+    st = lib.fjb_render_from_density_effects(
+        recipe.handle, C.byref(post), seed, origin[0], origin[1], C.byref(effects) if effects is not None else None,
+        C.c_void_p(_ptr(dust) if dust is not None else 0), C.c_void_p(_ptr(mask) if mask is not None else 0),
+        *[C.c_void_p(_ptr(t)) for t in density_cmy],
+        C.c_void_p(_ptr(src) if src is not None else 0), (src.stride(0) * 4) if src is not None else 0,
+        C.c_void_p(_ptr(dst)), dst.stride(0) * 4, w, h, comps, C.c_void_p(_ptr(scratch)), scratch.numel() * 4,
+        C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+    _check("fjb_render_from_density_effects", st, err)
+    return scratch
+
+
 def highlight_boost(descriptor: "abi.FjHighlightBoost", carrier_bgr, stream=None, state=None):
     """In-place highlight reconstruction on CUDA carrier planes (B, G, R), then the
     disposition check (raises FjError on an invalid carrier or a peak overflow). Returns

@@ -92,6 +92,32 @@ FjStatus fjb_render_from_density_post(FjbRecipe* recipe, const FjScannerPostEffe
                                       int32_t height, uint32_t components, float* scratch, size_t scratch_bytes,
                                       void* stream, FjErrorBuffer* error);
 
+/* Film and gate defects (reference src/Cuda/Scan/JuicerCudaScanPipeline.cu:2186-2242
+ * juicer_cuda_apply_film_defects / juicer_cuda_build_gate_defect_transmittance_focused,
+ * scheduled by src/Cuda/JuicerCudaExecutor.cpp:1674-1690, :2263-2279, :1806-1830).
+ * `effects` is the prepared record; it must pass the reference's descriptor checks
+ * (native/juicer_cuda_descriptors.cpp:467-515).
+ * fjb_film_defects: film dust and scratches on capture density planes of a render
+ *   window (full-frame pixel = pixel + the record's ROI offset): `dust` (width x height,
+ *   required when film dust is on) receives the dust transmittance, and film scratches
+ *   scale the three density planes.
+ * fjb_gate_mask: gate dust x gate scratch transmittance, gate_width x gate_height.
+ * fjb_render_from_density_effects: fjb_render_from_density_post with the defects'
+ *   output effects: `dust` (or null) darkens the print exposure on the print route and
+ *   the scanned XYZ on the direct route; with the gate output on, the weave resamples
+ *   the linear planes and `gate_mask` (or null) multiplies them before encoding. */
+FjStatus fjb_film_defects(const FjFilmEffects* effects, int32_t width, int32_t height, float* density_c,
+                          float* density_m, float* density_y, float* dust, void* stream, FjErrorBuffer* error);
+FjStatus fjb_gate_mask(const FjFilmEffects* effects, float* gate_mask, int32_t gate_width, int32_t gate_height,
+                       void* stream, FjErrorBuffer* error);
+FjStatus fjb_render_from_density_effects(FjbRecipe* recipe, const FjScannerPostEffects* post, uint64_t glare_seed,
+                                         int32_t glare_origin_x, int32_t glare_origin_y,
+                                         const FjFilmEffects* effects, const float* dust, const float* gate_mask,
+                                         const float* density_c, const float* density_m, const float* density_y,
+                                         const float* src, ptrdiff_t src_row_bytes, float* dst,
+                                         ptrdiff_t dst_row_bytes, int32_t width, int32_t height, uint32_t components,
+                                         float* scratch, size_t scratch_bytes, void* stream, FjErrorBuffer* error);
+
 /* Glare seed of a frame (reference src/Cuda/JuicerCudaExecutor.cpp:2416, src/Hash.h:50):
  * FNV-1a 64 over the little-endian 8-byte words {recipe hash, frame token, source x1,
  * source y1}. */
@@ -249,7 +275,8 @@ FjStatus fjb_visual_grain(FjbRecipe* recipe, const FjVisualGrain* grain, const F
 #define FJB_STAGE_GRAIN 6
 #define FJB_STAGE_PRINT_SCAN_OUTPUT 7
 #define FJB_STAGE_MONOLITHIC 8
-#define FJB_STAGE_COUNT 9
+#define FJB_STAGE_FILM_DEFECTS 9
+#define FJB_STAGE_COUNT 10
 typedef struct FjbStageTimes {
     double total_ms[FJB_STAGE_COUNT];
     uint64_t frames[FJB_STAGE_COUNT];

@@ -55,8 +55,18 @@ def render_frame(frame_record, recipe, src, threads: int = 1, frame_token: int =
         base = [a["density_rgb"][:, c] for c in range(3)]
         noise = frame_record.noise.record if frame_record.noise is not None else None
         density = ograin.visual_grain(h.grain, noise, base, layers, h.capture_polarity == 1, density)
-    if h.scanner_post.hash != 0:
-        # scanner post effects; the source origin of these frames is (0, 0)
+    fx = h.effects
+    film = bool(fx.flags & abi.FJ_EFFECTS_FILM)
+    gate_output = bool(fx.flags & abi.FJ_EFFECTS_GATE_OUTPUT)
+    dust = mask = None
+    if film:
+        # film dust / scratches on the developed capture density, after grain
+        density, dust = orc.film_defects(fx, density)
+    if gate_output and (fx.flags & abi.FJ_EFFECTS_GATE_TRANSMITTANCE):
+        mask = orc.gate_mask(fx)
+    if h.scanner_post.hash != 0 or film or gate_output:
+        # linear planes before the encoding; the source origin of these frames is (0, 0)
         seed = orc.glare_seed(h.recipe_hash, frame_token, 0, 0)
-        return orc.render_post(host, h.scanner_post, seed, 0, 0, density, src=src, threads=threads)
+        return orc.render_effects(host, h.scanner_post, seed, 0, 0, fx if (film or gate_output) else None, dust,
+                                  mask, density, src=src, threads=threads)
     return orc.render(host, src, stage=2, planes=density, threads=threads)

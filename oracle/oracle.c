@@ -457,7 +457,12 @@ static unsigned capture_density(const Pack* p, const float* e_in, float* d) {
 }
 
 /* :866-1071 (FP32, same accumulation order as the reference loop) */
-static void print_stage(const Pack* p, float* D) {
+static void print_stage_dust(const Pack* p, float* D, float dust);
+static void print_stage(const Pack* p, float* D) { print_stage_dust(p, D, 1.0f); }
+
+/* src/Cuda/JuicerCudaDeviceHelpers.cuh:1047-1070: `dust` scales the spectral raw print
+ * exposure before the exposure scales */
+static void print_stage_dust(const Pack* p, float* D, float dust) {
     float ac = 0, am = 0, ay = 0;
     for (int i = 0; i < NL; ++i) {
         float sC = p->psens[i * 3], sM = p->psens[i * 3 + 1], sY = p->psens[i * 3 + 2];
@@ -472,6 +477,8 @@ static void print_stage(const Pack* p, float* D) {
         if (aY) ay += e * sY;
     }
     float raw[3] = {ac, am, ay};
+    if (dust != 1.0f)
+        for (int c = 0; c < 3; ++c) raw[c] *= dust;
     for (int c = 0; c < 3; ++c) raw[c] *= p->midgray;
     if (isfinite(p->preflash) && p->preflash > 0.0f)
         for (int c = 0; c < 3; ++c) raw[c] += p->preflash_raw[c] * p->preflash;
@@ -607,7 +614,11 @@ static float enc(const Pack* p, float v) {
 
 /* :1700-1840, :1944-2037: density -> linear output RGB (glare percent added in XYZ when
  * glare >= 0); returns 0 on a scan failure */
-static int scan_lin(const Pack* p, const float* D, double* rgb, float glare) {
+static int scan_lin_dust(const Pack* p, const float* D, double* rgb, float glare, const float* dust);
+static int scan_lin(const Pack* p, const float* D, double* rgb, float glare) { return scan_lin_dust(p, D, rgb, glare, NULL); }
+
+/* `dust`: film dust transmittance scaling the scanned XYZ (direct route, :2006-2011) */
+static int scan_lin_dust(const Pack* p, const float* D, double* rgb, float glare, const float* dust) {
     double n[3];
     for (int c = 0; c < 3; ++c)
         n[c] = p->medium_negative ? ((double)D[c] + (double)p->min_cmy[c]) * (double)p->inv_cmy[c]
@@ -615,6 +626,8 @@ static int scan_lin(const Pack* p, const float* D, double* rgb, float glare) {
     float l2[3];
     if (!scan_lut(p, n, l2)) return 0;
     double xyz[3] = {(double)exp2f(l2[0]), (double)exp2f(l2[1]), (double)exp2f(l2[2])};
+    if (dust)
+        for (int c = 0; c < 3; ++c) xyz[c] *= (double)*dust;
     if (p->corr_active) {
         double cy = fmin(fmax((double)p->corr_slope * xyz[1] + (double)p->corr_offset, 0.0), 1.0);
         double s = cy / (xyz[1] + 1e-10);
@@ -2222,10 +2235,34 @@ static void post_blur(float* plane, float* tmp, int W, int H, const float* w, in
 
 /* density planes (C, M, Y) -> print -> scan to linear RGB with glare -> lens blur ->
  * unsharp -> encoded dst. Returns 0, or -1 for a malformed record. */
+static float weave_mitchell(const float* plane, int W, int H, float x, float y);
+static float gate_bilinear(const float* mask, int W, int H, float x, float y);
+
+int oracle_render_effects(const FjPreparedHostData* h, const FjScannerPostEffects* post, uint64_t seed, int ox,
+                          int oy, const FjFilmEffects* fx, const float* dust, const float* mask, const float* dc,
+                          const float* dm, const float* dy, const float* src, long src_row_floats, int W, int H,
+                          int comps, float* dst, long dst_row_floats, int threads, unsigned* flags_out);
+
 int oracle_render_post(const FjPreparedHostData* h, const FjScannerPostEffects* post, uint64_t seed, int ox, int oy,
                        const float* dc, const float* dm, const float* dy, const float* src, long src_row_floats,
                        int W, int H, int comps, float* dst, long dst_row_floats, int threads, unsigned* flags_out) {
+    return oracle_render_effects(h, post, seed, ox, oy, NULL, NULL, NULL, dc, dm, dy, src, src_row_floats, W, H,
+                                 comps, dst, dst_row_floats, threads, flags_out);
+}
+
+/* Density planes -> (print) -> scan -> post effects -> encoding, with the film defects'
+ * output effects (src/Cuda/JuicerCudaExecutor.cpp:1700-1800, :2384-2500): `dust` (or
+ * NULL) darkens the print exposure (print route) or the scanned XYZ (direct route);
+ * with the gate output on, the weave resamples the linear planes and `mask` (or NULL)
+ * multiplies them before encoding (src/Cuda/Scan/JuicerCudaScanPipeline.cu:2096-2182). */
+int oracle_render_effects(const FjPreparedHostData* h, const FjScannerPostEffects* post, uint64_t seed, int ox,
+                          int oy, const FjFilmEffects* fx, const float* dust, const float* mask, const float* dc,
+                          const float* dm, const float* dy, const float* src, long src_row_floats, int W, int H,
+                          int comps, float* dst, long dst_row_floats, int threads, unsigned* flags_out) {
     if ((post->flags & ~1u) != 0) return -1;
+    const int gate_output = fx && (fx->flags & FJ_EFFECTS_GATE_OUTPUT);
+    const int weave = gate_output && (fx->flags & FJ_EFFECTS_WEAVE);
+    const float* gate = gate_output && (fx->flags & FJ_EFFECTS_GATE_TRANSMITTANCE) ? mask : NULL;
     Packed pk;
     int rc = pack(h, &pk);
     if (rc) {
@@ -2279,9 +2316,9 @@ int oracle_render_post(const FjPreparedHostData* h, const FjScannerPostEffects* 
         for (int x = 0; x < W; ++x) {
             size_t i = (size_t)y * W + x;
             float D[3] = {dc[i], dm[i], dy[i]};
-            if (p->print) print_stage(p, D);
+            if (p->print) print_stage_dust(p, D, dust ? dust[i] : 1.0f);
             double rgb[3];
-            if (!scan_lin(p, D, rgb, glare ? glare[i] : -1.0f)) {
+            if (!scan_lin_dust(p, D, rgb, glare ? glare[i] : -1.0f, dust && !p->print ? dust + i : NULL)) {
                 flags |= 1u;
                 rgb[0] = rgb[1] = rgb[2] = 0.0;
             }
@@ -2293,6 +2330,19 @@ int oracle_render_post(const FjPreparedHostData* h, const FjScannerPostEffects* 
         for (int x = 0; x < W; ++x) {
             size_t i = (size_t)y * W + x;
             double rgb[3] = {(double)lin[i], (double)lin[plane + i], (double)lin[2 * plane + i]};
+            if (weave) {
+                float cx = 0.5f * (float)(W - 1), cy = 0.5f * (float)(H - 1);
+                float px = (float)x - cx, py = (float)y - cy;
+                float sx = fx->weave_cos_rot * px - fx->weave_sin_rot * py + cx + fx->weave_dx_px;
+                float sy = fx->weave_sin_rot * px + fx->weave_cos_rot * py + cy + fx->weave_dy_px;
+                for (int c = 0; c < 3; ++c) rgb[c] = (double)weave_mitchell(lin + c * plane, W, H, sx, sy);
+            }
+            if (gate && fx->gate_width > 0 && fx->gate_height > 0) {
+                double t = (double)gate_bilinear(gate, fx->gate_width, fx->gate_height,
+                                                 (float)(fx->roi_offset_x + x) * 0.5f - 0.25f,
+                                                 (float)(fx->roi_offset_y + y) * 0.5f - 0.25f);
+                for (int c = 0; c < 3; ++c) rgb[c] *= t;
+            }
             encode_lin(p, rgb);
             float* o = dst + (size_t)y * dst_row_floats + (size_t)x * comps;
             o[0] = (float)rgb[0];
@@ -2403,4 +2453,376 @@ int oracle_highlight_boost(uint64_t recipe_hash, double protection, double sharp
                 *v = hb_sample(*v, &w);
             }
     return 1;
+}
+
+/* ---------------- film and gate defects (src/Cuda/Scan/JuicerCudaScanPipeline.cu:801-1360, :2056-2094) ---------------- */
+
+static float weave_mitchell(const float* plane, int W, int H, float x, float y) {
+    x = fminf(fmaxf(x, 0.0f), (float)(W - 1));
+    y = fminf(fmaxf(y, 0.0f), (float)(H - 1));
+    int ix = (int)floorf(x), iy = (int)floorf(y);
+    float tx = x - (float)ix, ty = y - (float)iy;
+    float wx[4] = {mitchell(tx + 1.0f), mitchell(tx), mitchell(tx - 1.0f), mitchell(tx - 2.0f)};
+    float wy[4] = {mitchell(ty + 1.0f), mitchell(ty), mitchell(ty - 1.0f), mitchell(ty - 2.0f)};
+    double acc = 0.0;
+    for (int j = 0; j < 4; ++j) {
+        int sy = iy + j - 1;
+        sy = sy < 0 ? 0 : sy > H - 1 ? H - 1 : sy;
+        for (int i = 0; i < 4; ++i) {
+            int sx = ix + i - 1;
+            sx = sx < 0 ? 0 : sx > W - 1 ? W - 1 : sx;
+            acc += (double)wy[j] * wx[i] * (double)plane[(size_t)sy * W + sx];
+        }
+    }
+    return (float)acc;
+}
+
+static float gate_bilinear(const float* m, int W, int H, float x, float y) {
+    float fx = fminf(fmaxf(x, 0.0f), (float)(W - 1)), fy = fminf(fmaxf(y, 0.0f), (float)(H - 1));
+    int x0 = (int)floorf(fx), y0 = (int)floorf(fy);
+    int x1 = x0 + 1 < W ? x0 + 1 : x0, y1 = y0 + 1 < H ? y0 + 1 : y0;
+    float tx = fx - (float)x0, ty = fy - (float)y0;
+    float m0 = m[y0 * W + x0] + (m[y0 * W + x1] - m[y0 * W + x0]) * tx;
+    float m1 = m[y1 * W + x0] + (m[y1 * W + x1] - m[y1 * W + x0]) * tx;
+    return m0 + (m1 - m0) * ty;
+}
+
+static uint64_t od_mix(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ULL;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+    return x ^ (x >> 31);
+}
+
+static float od_lane(uint64_t id, unsigned k) {
+    uint64_t h = od_mix(id ^ (0xD6E8FEB86659FD93ULL * ((uint64_t)k + 1ULL)));
+    return (float)((h >> 40) & 0xFFFFFFu) * (1.0f / 16777216.0f);
+}
+
+typedef struct {
+    float cx, cy, xmin, xmax, ymin, ymax, strength, softness;
+    float ex[3], ey[3], ea[3], eb[3], ec[3];
+    float px[4], py[4], w[4], d[4];
+    int stroke, active;
+} OParticle;
+
+static float od_mixture(float u, float v, float lo, float bulk, float hi, float tail) {
+    float t = v * v * v;
+    return u < tail ? bulk + (hi - bulk) * t : lo + (bulk - lo) * t;
+}
+
+static void od_stroke(OParticle* q, uint64_t h, float length, float drift, float angle, const float* t,
+                      const float* w, const float* d) {
+    float dx[4] = {0.0f, (od_lane(h, 12) - 0.5f) * drift * length, (od_lane(h, 13) - 0.5f) * drift * length,
+                   (od_lane(h, 14) - 0.5f) * drift * length};
+    float total = 0.0f, widest = 0.0f;
+    for (int i = 1; i < 4; ++i) total += hypotf(dx[i] - dx[i - 1], length * (t[i] - t[i - 1]));
+    for (int i = 0; i < 4; ++i) widest = fmaxf(widest, w[i]);
+    float norm = length / total, c = cosf(angle), s = sinf(angle);
+    q->stroke = 1;
+    q->xmin = q->ymin = 1.0e30f;
+    q->xmax = q->ymax = -1.0e30f;
+    for (int i = 0; i < 4; ++i) {
+        float yy = (t[i] - 0.5f) * length * norm, xx = dx[i] * norm;
+        q->px[i] = xx * c - yy * s;
+        q->py[i] = xx * s + yy * c;
+        q->w[i] = w[i];
+        q->d[i] = d[i];
+        q->xmin = fminf(q->xmin, q->px[i] - widest * 0.5f);
+        q->xmax = fmaxf(q->xmax, q->px[i] + widest * 0.5f);
+        q->ymin = fminf(q->ymin, q->py[i] - widest * 0.5f);
+        q->ymax = fmaxf(q->ymax, q->py[i] + widest * 0.5f);
+    }
+}
+
+static float od_opacity(const FjDust* d, int fiber, float u) {
+    float lo = fiber ? d->fiber_opacity_min : d->compact_opacity_min;
+    float f = fiber ? d->fiber_opacity_faint_end : d->compact_opacity_faint_end;
+    float m = fiber ? d->fiber_opacity_intermediate_end : d->compact_opacity_intermediate_end;
+    float hi = fiber ? d->fiber_opacity_max : d->compact_opacity_max;
+    float c1 = d->opacity_faint_cumulative, c2 = d->opacity_intermediate_cumulative;
+    if (u < c1) return lo + (f - lo) * (u / c1);
+    if (u < c2) return f + (m - f) * ((u - c1) / (c2 - c1));
+    return m + (hi - m) * ((u - c2) / (1.0f - c2));
+}
+
+static OParticle od_particle(const FjFilmEffects* e, int fam, int64_t cxl, int64_t cyl, int slot, int offx, int offy) {
+    OParticle q;
+    memset(&q, 0, sizeof(q));
+    const FjDust* du = fam == 0 ? &e->film_dust : &e->gate_dust;
+    const FjScratch* sc = fam == 1 ? &e->film_scratch : &e->gate_scratch;
+    int dust = fam == 0 || fam == 2;
+    uint64_t h = od_mix(e->session_seed);
+    if (fam < 2) h = od_mix(h ^ od_mix(e->clip_token));
+    h = od_mix(h ^ (uint64_t)cxl);
+    h = od_mix(h ^ (uint64_t)cyl);
+    h = od_mix(h ^ (0x8EBC6AF09C88C6E3ULL * (uint64_t)(fam + 1)));
+    h = od_mix(h ^ (uint64_t)slot);
+    if (od_lane(h, 0) >= (dust ? du->slot_probability : sc->slot_probability)) return q;
+    q.cx = ((float)offx + od_lane(h, 1)) * (dust ? du->cell_width_mm : sc->cell_width_mm);
+    q.cy = ((float)offy + od_lane(h, 2)) * (dust ? du->cell_height_mm : sc->cell_height_mm);
+    q.active = 1;
+    if (dust) {
+        float angle = od_lane(h, 4) * 6.28318530718f;
+        int fiber = od_lane(h, 5) < du->fiber_fraction;
+        q.strength = od_opacity(du, fiber, od_lane(h, 3));
+        if (fiber) {
+            float len = du->fiber_length_min_mm + (du->fiber_length_max_mm - du->fiber_length_min_mm) * od_lane(h, 6);
+            float wid = du->fiber_width_min_mm + (du->fiber_width_max_mm - du->fiber_width_min_mm) * od_lane(h, 7);
+            float u = od_lane(h, 47);
+            q.softness = fminf(du->softness_min_mm + (du->softness_max_mm - du->softness_min_mm) * u * u,
+                               wid * du->softness_size_cap_fraction);
+            float t[4] = {0.0f,
+                          du->fiber_first_knot_min + (du->fiber_first_knot_max - du->fiber_first_knot_min) * od_lane(h, 30),
+                          du->fiber_second_knot_min +
+                              (du->fiber_second_knot_max - du->fiber_second_knot_min) * od_lane(h, 31),
+                          1.0f};
+            float span = du->fiber_interior_width_max_fraction - du->fiber_interior_width_min_fraction;
+            float w[4] = {0.0f, wid * (du->fiber_interior_width_min_fraction + span * od_lane(h, 21)),
+                          wid * (du->fiber_interior_width_min_fraction + span * od_lane(h, 22)), 0.0f};
+            float d[4] = {1.0f, 1.0f, 1.0f, 1.0f};
+            od_stroke(&q, h, len, du->fiber_drift_fraction, angle, t, w, d);
+        } else {
+            float dia = od_mixture(od_lane(h, 6), od_lane(h, 7), du->diameter_min_mm, du->diameter_bulk_max_mm,
+                                   du->diameter_max_mm, du->diameter_tail_fraction);
+            float u = od_lane(h, 47);
+            q.softness = fminf(du->softness_min_mm + (du->softness_max_mm - du->softness_min_mm) * u * u,
+                               dia * du->softness_size_cap_fraction);
+            float ox[3] = {0}, oy[3] = {0}, rx[3] = {0}, ry[3] = {0}, rot[3] = {0};
+            rx[0] = 1.0f;
+            ry[0] = du->compact_dominant_aspect_min +
+                    (du->compact_dominant_aspect_max - du->compact_dominant_aspect_min) * od_lane(h, 32);
+            rot[0] = angle;
+            float dc = cosf(angle), ds = sinf(angle), enc = 1.0f;
+            for (int i = 1; i < 3; ++i) {
+                rx[i] = du->compact_subsidiary_scale_min +
+                        (du->compact_subsidiary_scale_max - du->compact_subsidiary_scale_min) * od_lane(h, 32 + i * 5);
+                float asp = du->compact_subsidiary_aspect_min +
+                            (du->compact_subsidiary_aspect_max - du->compact_subsidiary_aspect_min) * od_lane(h, 33 + i * 5);
+                ry[i] = rx[i] * asp;
+                float polar = od_lane(h, 34 + i * 5) * 6.28318530718f;
+                float radial = du->compact_subsidiary_offset_max * sqrtf(od_lane(h, 35 + i * 5));
+                float lx = radial * cosf(polar), ly = radial * ry[0] * sinf(polar);
+                ox[i] = lx * dc - ly * ds;
+                oy[i] = lx * ds + ly * dc;
+                rot[i] = angle + (2.0f * od_lane(h, 36 + i * 5) - 1.0f) * du->compact_subsidiary_angle_max_radians;
+                enc = fmaxf(enc, hypotf(ox[i], oy[i]) + fmaxf(rx[i], ry[i]));
+            }
+            float scale = dia * 0.5f / enc;
+            q.xmin = q.ymin = 1.0e30f;
+            q.xmax = q.ymax = -1.0e30f;
+            for (int i = 0; i < 3; ++i) {
+                float a = rx[i] * scale, b = ry[i] * scale, c = cosf(rot[i]), s = sinf(rot[i]);
+                q.ex[i] = ox[i] * scale;
+                q.ey[i] = oy[i] * scale;
+                q.ea[i] = c * c / (a * a) + s * s / (b * b);
+                q.eb[i] = c * s * (1.0f / (a * a) - 1.0f / (b * b));
+                q.ec[i] = s * s / (a * a) + c * c / (b * b);
+                float hx = sqrtf(a * a * c * c + b * b * s * s), hy = sqrtf(a * a * s * s + b * b * c * c);
+                q.xmin = fminf(q.xmin, q.ex[i] - hx);
+                q.xmax = fmaxf(q.xmax, q.ex[i] + hx);
+                q.ymin = fminf(q.ymin, q.ey[i] - hy);
+                q.ymax = fmaxf(q.ymax, q.ey[i] + hy);
+            }
+        }
+    } else {
+        q.strength = sc->strength_min + (sc->strength_max - sc->strength_min) * od_lane(h, 3);
+        float len = od_mixture(od_lane(h, 6), od_lane(h, 7), sc->length_min_mm, sc->length_bulk_max_mm,
+                               sc->length_max_mm, sc->length_tail_fraction);
+        float wid = od_mixture(od_lane(h, 8), od_lane(h, 9), sc->width_min_mm, sc->width_bulk_max_mm, sc->width_max_mm,
+                               sc->width_tail_fraction);
+        float u = od_lane(h, 47);
+        q.softness = fminf(sc->softness_min_mm + (sc->softness_max_mm - sc->softness_min_mm) * u * u,
+                           wid * sc->softness_size_cap_fraction);
+        float t[4] = {0.0f, 0.0f, 0.0f, 1.0f}, w[4], d[4], angle = 0.0f;
+        int gap = od_lane(h, 30) < sc->interruption_probability;
+        if (gap) {
+            float c = sc->gap_center_min + (sc->gap_center_max - sc->gap_center_min) * od_lane(h, 31);
+            float sp = sc->gap_span_min + (sc->gap_span_max - sc->gap_span_min) * od_lane(h, 32);
+            t[1] = c - sp * 0.5f;
+            t[2] = c + sp * 0.5f;
+        } else {
+            t[1] = sc->first_knot_min + (sc->first_knot_max - sc->first_knot_min) * od_lane(h, 31);
+            t[2] = sc->second_knot_min + (sc->second_knot_max - sc->second_knot_min) * od_lane(h, 32);
+        }
+        for (int i = 0; i < 4; ++i) {
+            float wf = sc->interior_width_min_fraction +
+                       (sc->interior_width_max_fraction - sc->interior_width_min_fraction) * od_lane(h, 33 + i);
+            w[i] = (i == 1 || i == 2 || od_lane(h, 37 + i) < sc->endpoint_abrupt_probability) ? wid * wf : 0.0f;
+            d[i] = sc->interior_depth_min_fraction +
+                   (sc->interior_depth_max_fraction - sc->interior_depth_min_fraction) * od_lane(h, 41 + i);
+        }
+        if (gap) d[1] = d[2] = 0.0f;
+        if (len <= sc->scuff_length_max_mm && od_lane(h, 45) < sc->scuff_probability)
+            angle = (2.0f * od_lane(h, 46) - 1.0f) * sc->scuff_angle_max_radians;
+        od_stroke(&q, h, len, sc->drift_fraction, angle, t, w, d);
+    }
+    return q;
+}
+
+static float od_section(const OParticle* q, float y, float bx, float by) {
+    float lo[5] = {0}, hi[5] = {0}, dep[5] = {0};
+    int n = 0;
+    for (int i = 0; i < 3; ++i) {
+        float a = 0.0f, b = 0.0f;
+        if (!q->stroke) {
+            float dy = y - q->ey[i];
+            float disc = q->ea[i] - (q->ea[i] * q->ec[i] - q->eb[i] * q->eb[i]) * dy * dy;
+            if (disc <= 0.0f) continue;
+            float c = q->ex[i] - q->eb[i] * dy / q->ea[i], r = sqrtf(disc) / q->ea[i];
+            a = c - r;
+            b = c + r;
+        } else {
+            float dx = q->px[i + 1] - q->px[i], dy = q->py[i + 1] - q->py[i];
+            float inv = 1.0f / sqrtf(dx * dx + dy * dy);
+            float nx = -dy * inv * 0.5f, ny = dx * inv * 0.5f;
+            float vx[4] = {q->px[i] + nx * q->w[i], q->px[i + 1] + nx * q->w[i + 1], q->px[i + 1] - nx * q->w[i + 1],
+                           q->px[i] - nx * q->w[i]};
+            float vy[4] = {q->py[i] + ny * q->w[i], q->py[i + 1] + ny * q->w[i + 1], q->py[i + 1] - ny * q->w[i + 1],
+                           q->py[i] - ny * q->w[i]};
+            a = 1.0e30f;
+            b = -1.0e30f;
+            for (int k = 0; k < 4; ++k) {
+                int k1 = (k + 1) % 4;
+                if (y >= fminf(vy[k], vy[k1]) && y < fmaxf(vy[k], vy[k1])) {
+                    float x = vx[k] + (y - vy[k]) / (vy[k1] - vy[k]) * (vx[k1] - vx[k]);
+                    a = fminf(a, x);
+                    b = fmaxf(b, x);
+                }
+            }
+        }
+        a = fmaxf(bx, a);
+        b = fminf(by, b);
+        if (b > a) {
+            dep[n] = 1.0f;
+            if (q->stroke) {
+                float dx = q->px[i + 1] - q->px[i], dy = q->py[i + 1] - q->py[i];
+                float mid = 0.5f * (a + b), den = dx * dx + dy * dy;
+                float t = fminf(1.0f, fmaxf(0.0f, ((mid - q->px[i]) * dx + (y - q->py[i]) * dy) / den));
+                dep[n] = q->d[i] + (q->d[i + 1] - q->d[i]) * t;
+            }
+            lo[n] = a;
+            hi[n] = b;
+            ++n;
+        }
+    }
+    if (q->stroke)
+        for (int i = 1; i < 3; ++i) {
+            float r = q->w[i] * 0.5f, dy = y - q->py[i];
+            if (fabsf(dy) >= r) continue;
+            float ch = sqrtf(fmaxf(0.0f, r * r - dy * dy));
+            float a = fmaxf(bx, q->px[i] - ch), b = fminf(by, q->px[i] + ch);
+            if (b > a) {
+                lo[n] = a;
+                hi[n] = b;
+                dep[n] = q->d[i];
+                ++n;
+            }
+        }
+    float ends[10] = {0};
+    for (int i = 0; i < n; ++i) {
+        ends[2 * i] = lo[i];
+        ends[2 * i + 1] = hi[i];
+    }
+    for (int i = 1; i < 2 * n; ++i)
+        for (int j = i; j > 0 && ends[j] < ends[j - 1]; --j) {
+            float v = ends[j];
+            ends[j] = ends[j - 1];
+            ends[j - 1] = v;
+        }
+    float len = 0.0f;
+    for (int i = 1; i < 2 * n; ++i) {
+        float mid = (ends[i - 1] + ends[i]) * 0.5f, st = 0.0f;
+        for (int k = 0; k < n; ++k)
+            if (mid >= lo[k] && mid <= hi[k]) st = fmaxf(st, dep[k]);
+        len += (ends[i] - ends[i - 1]) * st;
+    }
+    return len;
+}
+
+static float od_coverage(const OParticle* q, float x, float y, float sx, float sy) {
+    x -= q->cx;
+    y -= q->cy;
+    if (x + sx * 0.5f + q->softness < q->xmin || x - sx * 0.5f - q->softness > q->xmax ||
+        y + sy * 0.5f + q->softness < q->ymin || y - sy * 0.5f - q->softness > q->ymax)
+        return 0.0f;
+    float area = 0.0f;
+    for (int soft = 0; soft < 3; ++soft) {
+        float shift = ((float)soft - 1.0f) * q->softness;
+        float bottom = fmaxf(q->ymin, y - sy * 0.5f + shift), top = fminf(q->ymax, y + sy * 0.5f + shift);
+        if (!(top > bottom)) continue;
+        float sum = 0.0f;
+        for (int row = 0; row < 8; ++row) {
+            float yy = bottom + ((float)row + 0.5f) * (top - bottom) / 8.0f;
+            for (int col = 0; col < 3; ++col) {
+                float off = ((float)col - 1.0f) * q->softness;
+                sum += od_section(q, yy, x - sx * 0.5f + off, x + sx * 0.5f + off);
+            }
+        }
+        area += sum * (top - bottom) / 72.0f;
+    }
+    return fminf(1.0f, fmaxf(0.0f, area / (sx * sy)));
+}
+
+/* Retained fraction of one family over a W x H pixel grid whose first pixel is (gx0, gy0)
+ * in the family's frame; candidates per 32 x 8 tile as the reference enumerates them. */
+static void od_family(const FjFilmEffects* e, int fam, int gx0, int gy0, int W, int H, float scale, float* out) {
+    int dust = fam == 0 || fam == 2;
+    const FjDust* dp = fam == 0 ? &e->film_dust : &e->gate_dust;
+    const FjScratch* sp = fam == 1 ? &e->film_scratch : &e->gate_scratch;
+    for (size_t i = 0; i < (size_t)W * H; ++i) out[i] = 1.0f;
+    if (!((dust ? dp->slot_probability : sp->slot_probability) > 0.0f)) return;
+    float cw = dust ? dp->cell_width_mm : sp->cell_width_mm, ch = dust ? dp->cell_height_mm : sp->cell_height_mm;
+    float sux = dust ? dp->support_x_mm + dp->softness_max_mm : sp->support_x_mm + sp->softness_max_mm;
+    float suy = dust ? dp->support_y_mm + dp->softness_max_mm : sp->support_y_mm + sp->softness_max_mm;
+    const FjDefectOrigin* o = &e->origins[fam];
+    float stx = e->sample_step_x_mm * scale, sty = e->sample_step_y_mm * scale;
+    float bx = o->local_x_mm, by = o->local_y_mm;
+    for (int ty = 0; ty < H; ty += 8)
+        for (int tx = 0; tx < W; tx += 32) {
+            int tfx = gx0 + tx, tfy = gy0 + ty;
+            int x0 = (int)floorf((bx + (float)tfx * stx - sux) / cw), y0 = (int)floorf((by + (float)tfy * sty - suy) / ch);
+            int x1 = (int)floorf((bx + (float)(tfx + 32) * stx + sux) / cw);
+            int y1 = (int)floorf((by + (float)(tfy + 8) * sty + suy) / ch);
+            int cols = x1 - x0 + 1, total = cols * (y1 - y0 + 1) * 2;
+            for (int ord = 0; ord < total; ++ord) {
+                int dx = x0 + (ord / 2) % cols, dy = y0 + (ord / 2) / cols;
+                OParticle q = od_particle(e, fam, o->cell_x + dx, o->cell_y + dy, ord % 2, dx, dy);
+                if (!q.active) continue;
+                for (int yy = ty; yy < ty + 8 && yy < H; ++yy)
+                    for (int xx = tx; xx < tx + 32 && xx < W; ++xx) {
+                        float px = bx + ((float)(gx0 + xx) + 0.5f) * stx, py = by + ((float)(gy0 + yy) + 0.5f) * sty;
+                        out[(size_t)yy * W + xx] *= 1.0f - q.strength * od_coverage(&q, px, py, stx, sty);
+                    }
+            }
+        }
+}
+
+/* film dust -> `dust` (when on), film scratches scale C, M, Y (when on) */
+int oracle_film_defects(const FjFilmEffects* e, int W, int H, float* c, float* m, float* y, float* dust) {
+    float* ret = (float*)malloc(sizeof(float) * (size_t)W * H);
+    if (!ret) return 2;
+    if (e->film_dust.slot_probability > 0.0f && dust)
+        od_family(e, 0, e->roi_offset_x, e->roi_offset_y, W, H, 1.0f, dust);
+    if (e->film_scratch.slot_probability > 0.0f) {
+        od_family(e, 1, e->roi_offset_x, e->roi_offset_y, W, H, 1.0f, ret);
+        for (size_t i = 0; i < (size_t)W * H; ++i) {
+            c[i] *= ret[i];
+            m[i] *= ret[i];
+            y[i] *= ret[i];
+        }
+    }
+    free(ret);
+    return 0;
+}
+
+/* gate dust x gate scratch at the gate grid */
+int oracle_gate_mask(const FjFilmEffects* e, float* mask, int W, int H) {
+    float* s = (float*)malloc(sizeof(float) * (size_t)W * H);
+    if (!s) return 2;
+    od_family(e, 2, 0, 0, W, H, 2.0f, mask);
+    od_family(e, 3, 0, 0, W, H, 2.0f, s);
+    for (size_t i = 0; i < (size_t)W * H; ++i) mask[i] *= s[i];
+    free(s);
+    return 0;
 }

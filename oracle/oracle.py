@@ -42,8 +42,74 @@ def load():
                                        C.c_uint64, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_long, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_int,
                                        C.POINTER(C.c_uint32)]
+    lib.oracle_render_effects.restype = C.c_int
+    lib.oracle_render_effects.argtypes = [C.POINTER(abi.FjPreparedHostData), C.POINTER(abi.FjScannerPostEffects),
+                                          C.c_uint64, C.c_int, C.c_int, C.POINTER(abi.FjFilmEffects), C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long,
+                                          C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_int,
+                                          C.POINTER(C.c_uint32)]
+    lib.oracle_film_defects.restype = C.c_int
+    lib.oracle_film_defects.argtypes = [C.POINTER(abi.FjFilmEffects), C.c_int, C.c_int] + [C.c_void_p] * 4
+    lib.oracle_gate_mask.restype = C.c_int
+    lib.oracle_gate_mask.argtypes = [C.POINTER(abi.FjFilmEffects), C.c_void_p, C.c_int, C.c_int]
     _lib = lib
     return lib
+
+
+def film_defects(effects, planes):
+    """Film dust / scratches on density planes (C, M, Y): returns (scratched planes, dust
+    transmittance plane or None)."""
+    import numpy as np
+
+    lib = load()
+    p = [np.ascontiguousarray(q, dtype=np.float32).copy() for q in planes]
+    h, w = p[0].shape
+    dust = np.ones((h, w), np.float32) if effects.film_dust.slot_probability > 0.0 else None
+    rc = lib.oracle_film_defects(C.byref(effects), w, h, *[C.c_void_p(q.ctypes.data) for q in p],
+                                 C.c_void_p(dust.ctypes.data if dust is not None else 0))
+    if rc != 0:
+        raise RuntimeError(f"oracle_film_defects failed with code {rc}")
+    return p, dust
+
+
+def gate_mask(effects):
+    """Gate dust x gate scratch transmittance on the gate grid (gate_height, gate_width)."""
+    import numpy as np
+
+    lib = load()
+    mask = np.ones((effects.gate_height, effects.gate_width), np.float32)
+    rc = lib.oracle_gate_mask(C.byref(effects), C.c_void_p(mask.ctypes.data), effects.gate_width, effects.gate_height)
+    if rc != 0:
+        raise RuntimeError(f"oracle_gate_mask failed with code {rc}")
+    return mask
+
+
+def render_effects(record, post, seed: int, origin_x: int, origin_y: int, effects, dust, mask, planes, src=None,
+                   threads: int = 1):
+    """render_post with the film defects' output effects (dust plane, weave, gate mask)."""
+    import numpy as np
+
+    lib = load()
+    p = [np.ascontiguousarray(q, dtype=np.float32) for q in planes]
+    h, w = p[0].shape
+    comps = 3
+    if src is not None:
+        src = np.ascontiguousarray(src, dtype=np.float32)
+        comps = src.shape[2]
+    dst = np.zeros((h, w, comps), np.float32)
+    flags = C.c_uint32()
+    dust = np.ascontiguousarray(dust, dtype=np.float32) if dust is not None else None
+    mask = np.ascontiguousarray(mask, dtype=np.float32) if mask is not None else None
+    rc = lib.oracle_render_effects(record.pointer(), C.byref(post), seed, origin_x, origin_y,
+                                   C.byref(effects) if effects is not None else None,
+                                   C.c_void_p(dust.ctypes.data if dust is not None else 0),
+                                   C.c_void_p(mask.ctypes.data if mask is not None else 0),
+                                   *[C.c_void_p(q.ctypes.data) for q in p],
+                                   C.c_void_p(src.ctypes.data if src is not None else 0), w * comps, w, h, comps,
+                                   C.c_void_p(dst.ctypes.data), w * comps, threads, C.byref(flags))
+    if rc != 0:
+        raise RuntimeError(f"oracle_render_effects failed with code {rc}")
+    return dst, int(flags.value)
 
 
 def _abi():
@@ -121,6 +187,12 @@ def load_reference():
                                          C.POINTER(abi.FjScannerPostEffects), C.c_ulonglong, C.c_int, C.c_int,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p,
                                          C.c_long, C.c_int, C.c_int, C.c_int]
+    if hasattr(lib, "ref_effects_render"):
+        lib.ref_effects_render.restype = C.c_int
+        lib.ref_effects_render.argtypes = [C.POINTER(abi.FjPreparedHostData), C.POINTER(C.c_void_p),
+                                           C.POINTER(abi.FjFilmEffects), C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_long, C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_int,
+                                           C.c_void_p, C.c_void_p]
     _ref = lib
     return lib
 

@@ -737,3 +737,127 @@ extern "C" int ref_highlight_boost(const FjHighlightBoost* d, float* b, float* g
     cudaFree(ws);
     return (int)e;
 }
+
+// ---- film and gate defects with the reference's kernels ----
+extern "C" cudaError_t juicer_cuda_apply_film_defects(const JuicerCuda::FilmDefectsPayload*, int, int, float*, float*,
+                                                      float*, float*, void*);
+extern "C" cudaError_t juicer_cuda_build_gate_defect_transmittance_focused(const JuicerCuda::FilmDefectsPayload*,
+                                                                            float*, int, int, void*);
+extern "C" cudaError_t juicer_cuda_direct_focused_scan_linear_density_rgb(const JuicerCuda::DirectPipelineRunParams*,
+                                                                          const float*, const float*, const float*,
+                                                                          float*, float*, float*, const float*, void*);
+extern "C" cudaError_t juicer_cuda_direct_focused_scanner_post_output(
+    const JuicerCuda::DirectPipelineRunParams*, float*, float*, float*, float*, const float*, int, const float*, int,
+    float, const JuicerCuda::FilmDefectsPayload*, const JuicerCuda::GateWeavePayload*, const float*, int, int, void*);
+
+namespace {
+// src/Cuda/JuicerCudaFilmPayloads.cpp:505-688: the record's families, origins and frame
+// fields into the payloads (the dust and scratch records list the same fields in the
+// same order as the payload structs).
+static_assert(sizeof(JuicerCuda::DefectDustPayload) == sizeof(FjDust), "dust layout");
+static_assert(sizeof(JuicerCuda::DefectScratchPayload) == sizeof(FjScratch), "scratch layout");
+void pack_effects(const FjFilmEffects& e, JuicerCuda::FilmDefectsPayload& d, JuicerCuda::GateWeavePayload& w) {
+    d = {};
+    w = {};
+    if (!(e.flags & (FJ_EFFECTS_FILM | FJ_EFFECTS_GATE_OUTPUT))) return;
+    std::memcpy(&d.filmDust, &e.film_dust, sizeof(FjDust));
+    std::memcpy(&d.filmScratch, &e.film_scratch, sizeof(FjScratch));
+    std::memcpy(&d.gateDust, &e.gate_dust, sizeof(FjDust));
+    std::memcpy(&d.gateScratch, &e.gate_scratch, sizeof(FjScratch));
+    for (int i = 0; i < 4; ++i)
+        d.origins[i] = {e.origins[i].cell_x, e.origins[i].cell_y, e.origins[i].local_x_mm, e.origins[i].local_y_mm};
+    d.sampleStepXMm = e.sample_step_x_mm;
+    d.sampleStepYMm = e.sample_step_y_mm;
+    d.roiOffsetX = e.roi_offset_x;
+    d.roiOffsetY = e.roi_offset_y;
+    d.sessionSeed = e.session_seed;
+    d.clipToken = e.clip_token;
+    w.active = (e.flags & FJ_EFFECTS_WEAVE) ? 1 : 0;
+    w.dxPx = e.weave_dx_px;
+    w.dyPx = e.weave_dy_px;
+    w.cosRot = e.weave_cos_rot;
+    w.sinRot = e.weave_sin_rot;
+}
+} // namespace
+
+// Capture density planes (device, modified in place) -> film defects -> print (print
+// route, with the dust) -> scan to linear RGB (direct route: with the dust) -> gate
+// mask -> output with weave and gate mask, through the reference's launchers as
+// src/Cuda/JuicerCudaExecutor.cpp schedules them (:1674-1690 / :2263-2279 film
+// defects, :2788-2790 gate mask, :1700-1800 / :2384-2500 scan and output). `dust`
+// (width x height) and `mask` (gate grid) are device buffers the caller may read back.
+extern "C" int ref_effects_render(const FjPreparedHostData* h, const float* const* lut, const FjFilmEffects* fx,
+                                  float* dc, float* dm, float* dy, const float* src, long src_row_bytes, float* dst,
+                                  long dst_row_bytes, int width, int height, int comps, float* dust, float* mask) {
+    Arena a;
+    unsigned* d_flags = nullptr;
+    if (cudaMalloc(&d_flags, sizeof(unsigned)) != cudaSuccess) return 2;
+    cudaMemset(d_flags, 0, sizeof(unsigned));
+    a.ptrs.push_back(d_flags);
+    JuicerCuda::PipelineRunParams p;
+    if (!pack(*h, lut, a, p, d_flags)) return 1;
+    JuicerCuda::FilmDefectsPayload defects;
+    JuicerCuda::GateWeavePayload weave;
+    pack_effects(*fx, defects, weave);
+    const bool film = (fx->flags & FJ_EFFECTS_FILM) != 0;
+    const bool output = (fx->flags & FJ_EFFECTS_GATE_OUTPUT) != 0;
+    const bool gate = output && (fx->flags & FJ_EFFECTS_GATE_TRANSMITTANCE) != 0;
+    const float* dust_t = film && fx->film_dust.slot_probability > 0.0f ? dust : nullptr;
+    const size_t plane = (size_t)width * (size_t)height;
+    float* buf = nullptr;
+    if (cudaMalloc(&buf, plane * 4 * sizeof(float)) != cudaSuccess) return 2;
+    a.ptrs.push_back(buf);
+    float *r = buf, *g = buf + plane, *b = buf + 2 * plane, *tmp = buf + 3 * plane;
+    cudaError_t e = cudaSuccess;
+    if (film) e = juicer_cuda_apply_film_defects(&defects, width, height, dc, dm, dy, dust, nullptr);
+    if (e == cudaSuccess && gate)
+        e = juicer_cuda_build_gate_defect_transmittance_focused(&defects, mask, fx->gate_width, fx->gate_height,
+                                                                nullptr);
+    if (e != cudaSuccess) return (int)e;
+    if (p.printExpose.active) {
+        JuicerCuda::PrintPipelineRunParams q{};
+        q.src = src;
+        q.srcRowBytes = (size_t)src_row_bytes;
+        q.dst = dst;
+        q.dstRowBytes = (size_t)dst_row_bytes;
+        q.width = width;
+        q.height = height;
+        q.nComponents = comps;
+        q.filmExpose = p.filmExpose;
+        q.filmDevelop = p.filmDevelop;
+        q.printExpose = p.printExpose;
+        q.printDevelop = p.printDevelop;
+        q.scanStage = p.scanStage;
+        q.filmRaw = p.filmRaw;
+        e = juicer_cuda_print_focused_continue_from_capture_density(&q, dc, dm, dy, dust_t, nullptr);
+        if (e == cudaSuccess)
+            e = juicer_cuda_print_focused_scan_linear_density_rgb(&q, dc, dm, dy, r, g, b, nullptr, nullptr, 0, 0, 0,
+                                                                  0.0f, 0.0f, nullptr, 0, nullptr);
+        if (e == cudaSuccess)
+            e = juicer_cuda_print_focused_scanner_post_output(&q, r, g, b, tmp, nullptr, 0, nullptr, 0, 0.0f,
+                                                              output ? &defects : nullptr, output ? &weave : nullptr,
+                                                              gate ? mask : nullptr, gate ? fx->gate_width : 0,
+                                                              gate ? fx->gate_height : 0, nullptr);
+    } else {
+        JuicerCuda::DirectPipelineRunParams q{};
+        q.src = src;
+        q.srcRowBytes = (size_t)src_row_bytes;
+        q.dst = dst;
+        q.dstRowBytes = (size_t)dst_row_bytes;
+        q.width = width;
+        q.height = height;
+        q.nComponents = comps;
+        q.filmExpose = p.filmExpose;
+        q.filmDevelop = p.filmDevelop;
+        q.scanStage = p.scanStage;
+        q.filmRaw = p.filmRaw;
+        e = juicer_cuda_direct_focused_scan_linear_density_rgb(&q, dc, dm, dy, r, g, b, dust_t, nullptr);
+        if (e == cudaSuccess)
+            e = juicer_cuda_direct_focused_scanner_post_output(&q, r, g, b, tmp, nullptr, 0, nullptr, 0, 0.0f,
+                                                               output ? &defects : nullptr, output ? &weave : nullptr,
+                                                               gate ? mask : nullptr, gate ? fx->gate_width : 0,
+                                                               gate ? fx->gate_height : 0, nullptr);
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return (int)e;
+}

@@ -186,6 +186,25 @@ def gaussian_cases():
     print("gaussian cases:", len(cases))
 
 
+def effects_cases():
+    """Composed film-effects records of the reference's effects-frame characterization
+    (tests/film/effects-frame-fixtures/linux-debug-payload.json): the native fields of
+    the active cases (float fields as IEEE bit patterns), for the defects tests."""
+    with open(os.path.join(REF, "tests", "film", "effects-frame-fixtures", "linux-debug-payload.json")) as fh:
+        doc = json.load(fh)
+    keep, per = [], {}
+    for i, case in enumerate(doc["cases"]):
+        n = case.get("native") or {}
+        contract = case["input"].get("contract")
+        if not case.get("success") or not n.get("hash") or per.get(contract, 0) >= 3:
+            continue
+        per[contract] = per.get(contract, 0) + 1
+        keep.append(dict(case=i, contract=contract, native=n))
+    with open(os.path.join(HERE, "effects_cases.json"), "w") as fh:
+        json.dump(keep, fh, separators=(",", ":"), sort_keys=True)
+    print("effects cases:", len(keep))
+
+
 def recipes():
     sys.path.insert(0, ROOT)
     import __graft_entry__
@@ -206,4 +225,5 @@ if __name__ == "__main__":
     diffusion_images()
     grain_plan_cases()
     gaussian_cases()
+    effects_cases()
     recipes()

@@ -105,7 +105,7 @@ def test_unsupported_stages_and_partial_windows_are_rejected(torch_cuda, recipes
             owner.render(rec, src, d)
         rec.host.h.scanner_post.flags = 0
         rec.host.h.scanner_post.hash = 0
-        rec.host.h.effects.flags |= abi.FJ_EFFECTS_FILM
-        with pytest.raises(runtime.FjError, match="defects"):
+        rec.host.h.effects.flags |= abi.FJ_EFFECTS_FILM  # an active effects record without its identity
+        with pytest.raises(runtime.FjError, match="identity"):
             owner.render(rec, src, d)
         rec.host.h.effects.flags = 0
