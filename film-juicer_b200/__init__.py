@@ -28,10 +28,13 @@ _EXPORTS = {
                                                     C.c_int32, C.c_uint32, C.c_void_p, C.c_size_t, C.c_void_p,
                                                     C.POINTER(abi.FjErrorBuffer)]),
     "fjb_glare_seed": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_int32, C.c_int32]),
+    "fjb_film_defects_scratch_bytes": (C.c_size_t, [C.POINTER(abi.FjFilmEffects), C.c_int32, C.c_int32]),
+    "fjb_gate_mask_scratch_bytes": (C.c_size_t, [C.POINTER(abi.FjFilmEffects), C.c_int32, C.c_int32]),
     "fjb_film_defects": (abi.FjStatus, [C.POINTER(abi.FjFilmEffects), C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
-                                        C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                        C.POINTER(abi.FjErrorBuffer)]),
     "fjb_gate_mask": (abi.FjStatus, [C.POINTER(abi.FjFilmEffects), C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
-                                     C.POINTER(abi.FjErrorBuffer)]),
+                                     C.c_size_t, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
     "fjb_render_from_density_effects": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjScannerPostEffects), C.c_uint64,
                                                        C.c_int32, C.c_int32, C.POINTER(abi.FjFilmEffects),
                                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

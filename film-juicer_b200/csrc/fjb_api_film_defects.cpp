@@ -107,8 +107,17 @@ bool effects_plan_from(const FjFilmEffects& e, EffectsPlan& plan, std::string& w
 
 extern "C" {
 
+size_t fjb_film_defects_scratch_bytes(const FjFilmEffects* effects, int32_t width, int32_t height) {
+    return effects ? fjb::film_defects_table_bytes(*effects, width, height) : 0;
+}
+
+size_t fjb_gate_mask_scratch_bytes(const FjFilmEffects* effects, int32_t gate_width, int32_t gate_height) {
+    return effects ? fjb::gate_mask_table_bytes(*effects, gate_width, gate_height) : 0;
+}
+
 FjStatus fjb_film_defects(const FjFilmEffects* effects, int32_t width, int32_t height, float* density_c,
-                          float* density_m, float* density_y, float* dust, void* stream, FjErrorBuffer* error) {
+                          float* density_m, float* density_y, float* dust, void* scratch, size_t scratch_bytes,
+                          void* stream, FjErrorBuffer* error) {
     try {
         if (!effects || !density_c || !density_m || !density_y)
             return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
@@ -120,7 +129,8 @@ FjStatus fjb_film_defects(const FjFilmEffects* effects, int32_t width, int32_t h
             return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "film dust needs a transmittance plane");
         if (width < 0 || height < 0) return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "negative frame size");
         cudaError_t e = fjb::launch_film_defects(*effects, width, height, density_c, density_m, density_y,
-                                                 plan.film_dust ? dust : nullptr, reinterpret_cast<cudaStream_t>(stream));
+                                                 plan.film_dust ? dust : nullptr, reinterpret_cast<cudaStream_t>(stream),
+                                                 scratch, scratch_bytes);
         if (e != cudaSuccess) return cuda_status(e, error, "film defects");
         write_error(error, "");
         return ok_status();
@@ -130,7 +140,7 @@ FjStatus fjb_film_defects(const FjFilmEffects* effects, int32_t width, int32_t h
 }
 
 FjStatus fjb_gate_mask(const FjFilmEffects* effects, float* gate_mask, int32_t gate_width, int32_t gate_height,
-                       void* stream, FjErrorBuffer* error) {
+                       void* scratch, size_t scratch_bytes, void* stream, FjErrorBuffer* error) {
     try {
         if (!effects || !gate_mask) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
         fjb::EffectsPlan plan;
@@ -141,7 +151,7 @@ FjStatus fjb_gate_mask(const FjFilmEffects* effects, float* gate_mask, int32_t g
         if (gate_width <= 0 || gate_height <= 0)
             return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "gate grid must be non-empty");
         cudaError_t e = fjb::launch_gate_mask(*effects, gate_mask, gate_width, gate_height,
-                                              reinterpret_cast<cudaStream_t>(stream));
+                                              reinterpret_cast<cudaStream_t>(stream), scratch, scratch_bytes);
         if (e != cudaSuccess) return cuda_status(e, error, "gate mask");
         write_error(error, "");
         return ok_status();

@@ -18,15 +18,19 @@
 // The hashing constants, the attribute lane numbers and the floating-point expressions
 // are the reference's: they define the defect pattern, which must match it bit for bit.
 //
-// B200 schedule. A CTA covers a 32 x 8 pixel tile. Its threads build the candidates of
-// the tile's cell range 256 at a time, one per thread, and keep -- in candidate order --
-// only the active ones whose bounding box, widened by softness and the pixel footprint,
-// can reach the tile; the tile's pixels then multiply over that short list. A candidate
+// B200 schedule. A pre-pass builds every candidate of the frame's cell range once, one
+// per thread, into a particle table (a candidate depends only on its cell address). A
+// CTA covers a 32 x 8 pixel tile: its threads read the candidates of the tile's cell
+// range 256 at a time from the table (or build them, when no table was given) and keep
+// -- in candidate order -- only the active ones whose bounding box, widened by softness
+// and the pixel footprint, can reach the tile; the tile's pixels then multiply over
+// that short list. A candidate
 // that cannot reach a pixel contributes exactly 1 - strength * 0 = 1 to its product, so
 // the culling changes no result (candidates with a non-finite strength are kept). The
 // reference makes every pixel visit every candidate of its tile.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 
 #include "fjb_film_defects.h"
@@ -367,11 +371,35 @@ __device__ float coverage(const Particle& q, float x, float y, float sx, float s
     return fminf(1.0f, fmaxf(0.0f, area / (sx * sy)));
 }
 
+// Particles of one family built once per frame: the candidates of cells [x0, x0 +
+// columns) x [y0, y0 + rows) (relative to the family's origin), two slots per cell, at
+// index ((y - y0) * columns + (x - x0)) * 2 + slot. A particle depends only on its cell
+// address, so a tile reads it instead of building it again. p == nullptr: tiles build
+// their candidates themselves.
+struct ParticleTable {
+    const Particle* p;
+    int x0, y0, columns, rows;
+};
+
+struct FrameTables {
+    ParticleTable t[2];
+};
+
+__global__ void __launch_bounds__(256) build_particles_kernel(const __grid_constant__ FjFilmEffects e, int family,
+                                                              int x0, int y0, int columns, int rows, Particle* out) {
+    const long long total = (long long)columns * rows * 2;
+    const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= total) return;
+    const int dx = x0 + (int)((o / 2) % columns);
+    const int dy = y0 + (int)((o / 2) / columns);
+    out[o] = make_particle(e, family, e.origins[family].cell_x + dx, e.origins[family].cell_y + dy, (int)(o % 2), dx, dy);
+}
+
 // One family at the pixels of a tile: `tile` is the tile's first pixel in the family's
 // pixel grid, (px, py) this thread's pixel there, `scale` the grid's step in sample
 // steps. Returns the retained fraction (1 when the family is off).
 __device__ float family_retained(const FjFilmEffects& e, int family, int tile_x, int tile_y, int px, int py, float scale,
-                                 Particle* list, int* counts) {
+                                 const ParticleTable& table, Particle* list, int* counts) {
     const bool is_dust = family == 0 || family == 2;
     const FjDust& dp = family == 0 ? e.film_dust : e.gate_dust;
     const FjScratch& sp = family == 1 ? e.film_scratch : e.gate_scratch;
@@ -409,7 +437,14 @@ __device__ float family_retained(const FjFilmEffects& e, int family, int tile_x,
         if (ordinal < total) {
             const int dx = x0 + (ordinal / 2) % columns;
             const int dy = y0 + (ordinal / 2) / columns;
-            q = make_particle(e, family, origin.cell_x + dx, origin.cell_y + dy, ordinal % 2, dx, dy);
+            const int gx = dx - table.x0, gy = dy - table.y0;
+            if (table.p && gx >= 0 && gx < table.columns && gy >= 0 && gy < table.rows) {
+                const Particle* src = table.p + ((size_t)gy * table.columns + gx) * 2 + (ordinal % 2);
+                q.active = src->active;
+                if (q.active) q = *src;
+            } else {
+                q = make_particle(e, family, origin.cell_x + dx, origin.cell_y + dy, ordinal % 2, dx, dy);
+            }
             if (q.active) {
                 // the per-pixel early-out of coverage(), at the tile's extreme pixels: each
                 // side is monotone in the pixel position, so a side that holds there holds
@@ -439,15 +474,15 @@ __device__ float family_retained(const FjFilmEffects& e, int family, int tile_x,
 
 __global__ void __launch_bounds__(kTileThreads) film_defects_kernel(const __grid_constant__ FjFilmEffects e, int width,
                                                                     int height, float* c, float* m, float* yp,
-                                                                    float* dust_out) {
+                                                                    float* dust_out, FrameTables tables) {
     __shared__ Particle list[kTileThreads];
     __shared__ int counts[kTileThreads / 32];
     const int tx = blockIdx.x * kTileX, ty = blockIdx.y * kTileY;
     const int x = tx + threadIdx.x, y = ty + threadIdx.y;
     const int fx = x + e.roi_offset_x, fy = y + e.roi_offset_y;
     const int tfx = tx + e.roi_offset_x, tfy = ty + e.roi_offset_y;
-    const float dust = family_retained(e, 0, tfx, tfy, fx, fy, 1.0f, list, counts);
-    const float retained = family_retained(e, 1, tfx, tfy, fx, fy, 1.0f, list, counts);
+    const float dust = family_retained(e, 0, tfx, tfy, fx, fy, 1.0f, tables.t[0], list, counts);
+    const float retained = family_retained(e, 1, tfx, tfy, fx, fy, 1.0f, tables.t[1], list, counts);
     if (x < width && y < height) {
         const size_t i = (size_t)y * width + x;
         if (dust_out) dust_out[i] = dust;
@@ -460,33 +495,134 @@ __global__ void __launch_bounds__(kTileThreads) film_defects_kernel(const __grid
 }
 
 __global__ void __launch_bounds__(kTileThreads) gate_mask_kernel(const __grid_constant__ FjFilmEffects e, float* mask,
-                                                                 int width, int height) {
+                                                                 int width, int height, FrameTables tables) {
     __shared__ Particle list[kTileThreads];
     __shared__ int counts[kTileThreads / 32];
     const int tx = blockIdx.x * kTileX, ty = blockIdx.y * kTileY;
     const int x = tx + threadIdx.x, y = ty + threadIdx.y;
-    const float dust = family_retained(e, 2, tx, ty, x, y, 2.0f, list, counts);
-    const float scratch = family_retained(e, 3, tx, ty, x, y, 2.0f, list, counts);
+    const float dust = family_retained(e, 2, tx, ty, x, y, 2.0f, tables.t[0], list, counts);
+    const float scratch = family_retained(e, 3, tx, ty, x, y, 2.0f, tables.t[1], list, counts);
     if (x < width && y < height) mask[(size_t)y * width + x] = dust * scratch;
+}
+
+// Cells a family's tiles can visit over a grid of tiles whose first pixels run from
+// (tx0, ty0) to (tx1, ty1), with one cell of margin on each side (the host's rounding
+// may differ from the device's by an ulp); false when the family is off or its table
+// would exceed kMaxTableParticles (its tiles then build their own candidates).
+constexpr long long kMaxTableParticles = 1 << 18;
+
+struct Grid {
+    int x0 = 0, y0 = 0, columns = 0, rows = 0;
+    size_t particles() const { return (size_t)columns * rows * 2; }
+};
+
+bool family_grid(const FjFilmEffects& e, int family, long long tx0, long long ty0, long long tx1, long long ty1,
+                 float scale, Grid& g) {
+    const bool is_dust = family == 0 || family == 2;
+    const FjDust& dp = family == 0 ? e.film_dust : e.gate_dust;
+    const FjScratch& sp = family == 1 ? e.film_scratch : e.gate_scratch;
+    if (!((is_dust ? dp.slot_probability : sp.slot_probability) > 0.0f)) return false;
+    const double cw = is_dust ? dp.cell_width_mm : sp.cell_width_mm;
+    const double ch = is_dust ? dp.cell_height_mm : sp.cell_height_mm;
+    const double sx = is_dust ? (double)dp.support_x_mm + dp.softness_max_mm : (double)sp.support_x_mm + sp.softness_max_mm;
+    const double sy = is_dust ? (double)dp.support_y_mm + dp.softness_max_mm : (double)sp.support_y_mm + sp.softness_max_mm;
+    const double stx = (double)e.sample_step_x_mm * scale, sty = (double)e.sample_step_y_mm * scale;
+    const double bx = e.origins[family].local_x_mm, by = e.origins[family].local_y_mm;
+    const double x0 = std::floor((bx + (double)tx0 * stx - sx) / cw) - 1.0;
+    const double y0 = std::floor((by + (double)ty0 * sty - sy) / ch) - 1.0;
+    const double x1 = std::floor((bx + (double)(tx1 + kTileX) * stx + sx) / cw) + 1.0;
+    const double y1 = std::floor((by + (double)(ty1 + kTileY) * sty + sy) / ch) + 1.0;
+    if (!(x0 > -2.0e9 && y0 > -2.0e9 && x1 < 2.0e9 && y1 < 2.0e9)) return false;
+    const double n = (x1 - x0 + 1.0) * (y1 - y0 + 1.0) * 2.0;
+    if (!(n >= 2.0 && n <= (double)kMaxTableParticles)) return false;
+    g.x0 = (int)x0;
+    g.y0 = (int)y0;
+    g.columns = (int)(x1 - x0 + 1.0);
+    g.rows = (int)(y1 - y0 + 1.0);
+    return true;
+}
+
+// The two families' grids of a launch (film: families 0, 1 at the ROI-offset pixels;
+// gate: families 2, 3 at the gate grid, twice the step).
+void launch_grids(const FjFilmEffects& e, bool gate, int width, int height, Grid g[2], bool on[2]) {
+    const long long ox = gate ? 0 : e.roi_offset_x, oy = gate ? 0 : e.roi_offset_y;
+    const long long tx1 = ox + (long long)((width - 1) / kTileX) * kTileX;
+    const long long ty1 = oy + (long long)((height - 1) / kTileY) * kTileY;
+    for (int k = 0; k < 2; ++k) on[k] = family_grid(e, (gate ? 2 : 0) + k, ox, oy, tx1, ty1, gate ? 2.0f : 1.0f, g[k]);
+}
+
+size_t table_bytes_of(const Grid g[2], const bool on[2]) {
+    size_t n = 0;
+    for (int k = 0; k < 2; ++k)
+        if (on[k]) n += (g[k].particles() * sizeof(Particle) + 255) / 256 * 256;
+    return n;
+}
+
+// Builds the tables that fit `table` (table_bytes bytes, may be null) and returns the
+// kernels' view of them.
+cudaError_t build_tables(const FjFilmEffects& e, bool gate, int width, int height, void* table, size_t table_bytes,
+                         FrameTables& tables, cudaStream_t stream) {
+    tables = FrameTables{};
+    Grid g[2];
+    bool on[2];
+    launch_grids(e, gate, width, height, g, on);
+    if (!table || table_bytes < table_bytes_of(g, on)) return cudaSuccess;
+    char* base = static_cast<char*>(table);
+    for (int k = 0; k < 2; ++k) {
+        if (!on[k]) continue;
+        Particle* out = reinterpret_cast<Particle*>(base);
+        const long long n = (long long)g[k].particles();
+        fjb::count_launch();
+        build_particles_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(e, (gate ? 2 : 0) + k, g[k].x0, g[k].y0,
+                                                                               g[k].columns, g[k].rows, out);
+        cudaError_t err = cudaGetLastError();
+        if (err != cudaSuccess) return err;
+        tables.t[k] = ParticleTable{out, g[k].x0, g[k].y0, g[k].columns, g[k].rows};
+        base += (g[k].particles() * sizeof(Particle) + 255) / 256 * 256;
+    }
+    return cudaSuccess;
 }
 
 } // namespace
 
+size_t film_defects_table_bytes(const FjFilmEffects& e, int width, int height) {
+    if (width <= 0 || height <= 0) return 0;
+    Grid g[2];
+    bool on[2];
+    launch_grids(e, false, width, height, g, on);
+    return table_bytes_of(g, on);
+}
+
+size_t gate_mask_table_bytes(const FjFilmEffects& e, int width, int height) {
+    if (width <= 0 || height <= 0) return 0;
+    Grid g[2];
+    bool on[2];
+    launch_grids(e, true, width, height, g, on);
+    return table_bytes_of(g, on);
+}
+
 cudaError_t launch_film_defects(const FjFilmEffects& e, int width, int height, float* c, float* m, float* y,
-                                float* dust_out, cudaStream_t stream) {
+                                float* dust_out, cudaStream_t stream, void* table, size_t table_bytes) {
     if (width <= 0 || height <= 0) return cudaSuccess;
     if (e.film_dust.slot_probability > 0.0f && !dust_out) return cudaErrorInvalidValue;
+    FrameTables tables;
+    cudaError_t err = build_tables(e, false, width, height, table, table_bytes, tables, stream);
+    if (err != cudaSuccess) return err;
     fjb::count_launch();
     film_defects_kernel<<<dim3((width + kTileX - 1) / kTileX, (height + kTileY - 1) / kTileY), dim3(kTileX, kTileY), 0,
-                          stream>>>(e, width, height, c, m, y, dust_out);
+                          stream>>>(e, width, height, c, m, y, dust_out, tables);
     return cudaGetLastError();
 }
 
-cudaError_t launch_gate_mask(const FjFilmEffects& e, float* mask, int width, int height, cudaStream_t stream) {
+cudaError_t launch_gate_mask(const FjFilmEffects& e, float* mask, int width, int height, cudaStream_t stream,
+                             void* table, size_t table_bytes) {
     if (!mask || width <= 0 || height <= 0) return cudaErrorInvalidValue;
+    FrameTables tables;
+    cudaError_t err = build_tables(e, true, width, height, table, table_bytes, tables, stream);
+    if (err != cudaSuccess) return err;
     fjb::count_launch();
     gate_mask_kernel<<<dim3((width + kTileX - 1) / kTileX, (height + kTileY - 1) / kTileY), dim3(kTileX, kTileY), 0,
-                       stream>>>(e, mask, width, height);
+                       stream>>>(e, mask, width, height, tables);
     return cudaGetLastError();
 }
 

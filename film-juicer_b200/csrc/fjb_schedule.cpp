@@ -277,7 +277,12 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
     const size_t mask_bytes =
         fx.gate_mask ? ((size_t)h.effects.gate_width * (size_t)h.effects.gate_height * sizeof(float) + 255) / 256 * 256
                      : 0;
-    cudaError_t e = ensure_work(cuda, planes * plane_bytes + scratch + mask_bytes + 256);
+    // the defect particle tables (film families, then gate families, in turn)
+    const size_t table_bytes = std::max(fx.film ? fjb::film_defects_table_bytes(h.effects, width, height) : 0,
+                                        fx.gate_mask ? fjb::gate_mask_table_bytes(h.effects, h.effects.gate_width,
+                                                                                  h.effects.gate_height)
+                                                     : 0);
+    cudaError_t e = ensure_work(cuda, planes * plane_bytes + scratch + mask_bytes + table_bytes + 256);
     FjStatus st{};
     if (e != cudaSuccess) return fjb::cuda_status(e, error, "frame workspace");
     char* base = static_cast<char*>(cuda->work);
@@ -290,6 +295,7 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
     float* dust = fx.film_dust ? P(planes - 1) : nullptr;
     float* scratch_p = reinterpret_cast<float*>(base + (size_t)planes * plane_bytes);
     float* gate_mask = fx.gate_mask ? reinterpret_cast<float*>(base + (size_t)planes * plane_bytes + scratch) : nullptr;
+    void* tables = table_bytes ? base + (size_t)planes * plane_bytes + scratch + mask_bytes : nullptr;
     const ptrdiff_t stride = width;
     const FjOptics& o = h.optics;
 
@@ -441,7 +447,7 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
         // (src/Cuda/JuicerCudaExecutor.cpp:1674-1690, :2263-2279)
         stage_begin(cuda, FJB_STAGE_FILM_DEFECTS, vs);
         e = fjb::launch_film_defects(h.effects, width, height, density[0], density[1], density[2], dust,
-                                     reinterpret_cast<cudaStream_t>(vs));
+                                     reinterpret_cast<cudaStream_t>(vs), tables, table_bytes);
         stage_end(cuda, FJB_STAGE_FILM_DEFECTS, vs);
         if (e != cudaSuccess) return fjb::cuda_status(e, error, "film defects");
     }
@@ -460,7 +466,7 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
             if (fx.gate_mask) {
                 // gate dust and scratches at the gate grid (src/Cuda/JuicerCudaExecutor.cpp:2788-2790)
                 e = fjb::launch_gate_mask(fe, gate_mask, fe.gate_width, fe.gate_height,
-                                          reinterpret_cast<cudaStream_t>(vs));
+                                          reinterpret_cast<cudaStream_t>(vs), tables, table_bytes);
                 if (e != cudaSuccess) return fjb::cuda_status(e, error, "gate mask");
                 out.gate_mask = gate_mask;
                 out.gate_w = fe.gate_width;

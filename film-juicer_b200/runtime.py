@@ -367,30 +367,37 @@ def render_from_density_post(recipe: "DeviceRecipe", post, seed: int, origin, de
     return scratch
 
 
-def film_defects(effects: "abi.FjFilmEffects", density_cmy, dust=None, stream=None):
+def film_defects(effects: "abi.FjFilmEffects", density_cmy, dust=None, stream=None, table: bool = True):
     """fjb_film_defects on CUDA density planes (C, M, Y), in place: film scratches scale
     the densities; the film dust transmittance goes to `dust` (allocated when None and
-    film dust is on). Returns the dust plane (or None)."""
+    film dust is on). `table`: pass the particle-table scratch (False: the tiles build
+    their candidates themselves). Returns the dust plane (or None)."""
     torch = _torch()
     lib = load_library()
     h, w = density_cmy[0].shape
     if dust is None and effects.film_dust.slot_probability > 0.0:
         dust = torch.empty((h, w), dtype=torch.float32, device=density_cmy[0].device)
+    need = int(lib.fjb_film_defects_scratch_bytes(C.byref(effects), w, h)) if table else 0
+    scratch = torch.empty(max(need, 4) // 4, dtype=torch.float32, device=density_cmy[0].device) if need else None
     err = abi.ErrorText()
     st = lib.fjb_film_defects(C.byref(effects), w, h, *[C.c_void_p(_ptr(t)) for t in density_cmy],
-                              C.c_void_p(_ptr(dust) if dust is not None else 0), C.c_void_p(_stream_handle(stream)),
-                              C.byref(err.buf))
+                              C.c_void_p(_ptr(dust) if dust is not None else 0),
+                              C.c_void_p(_ptr(scratch) if scratch is not None else 0), need,
+                              C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
     _check("fjb_film_defects", st, err)
     return dust
 
 
-def gate_mask(effects: "abi.FjFilmEffects", stream=None):
+def gate_mask(effects: "abi.FjFilmEffects", stream=None, table: bool = True):
     """fjb_gate_mask: the gate transmittance grid (gate_height, gate_width) on the GPU."""
     torch = _torch()
     lib = load_library()
     mask = torch.empty((max(effects.gate_height, 1), max(effects.gate_width, 1)), dtype=torch.float32, device="cuda")
+    need = int(lib.fjb_gate_mask_scratch_bytes(C.byref(effects), effects.gate_width, effects.gate_height)) if table else 0
+    scratch = torch.empty(max(need, 4) // 4, dtype=torch.float32, device="cuda") if need else None
     err = abi.ErrorText()
     st = lib.fjb_gate_mask(C.byref(effects), C.c_void_p(_ptr(mask)), effects.gate_width, effects.gate_height,
+                           C.c_void_p(_ptr(scratch) if scratch is not None else 0), need,
                            C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
     _check("fjb_gate_mask", st, err)
     return mask

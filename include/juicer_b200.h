@@ -102,14 +102,21 @@ FjStatus fjb_render_from_density_post(FjbRecipe* recipe, const FjScannerPostEffe
  *   required when film dust is on) receives the dust transmittance, and film scratches
  *   scale the three density planes.
  * fjb_gate_mask: gate dust x gate scratch transmittance, gate_width x gate_height.
+ * `scratch` (may be null) holds the frame's particle table, fjb_film_defects_scratch_bytes
+ *   / fjb_gate_mask_scratch_bytes bytes of device memory: every candidate particle is
+ *   built once instead of once per tile that can reach it; without it (null or too
+ *   small) the results are the same, computed more slowly.
  * fjb_render_from_density_effects: fjb_render_from_density_post with the defects'
  *   output effects: `dust` (or null) darkens the print exposure on the print route and
  *   the scanned XYZ on the direct route; with the gate output on, the weave resamples
  *   the linear planes and `gate_mask` (or null) multiplies them before encoding. */
+size_t fjb_film_defects_scratch_bytes(const FjFilmEffects* effects, int32_t width, int32_t height);
+size_t fjb_gate_mask_scratch_bytes(const FjFilmEffects* effects, int32_t gate_width, int32_t gate_height);
 FjStatus fjb_film_defects(const FjFilmEffects* effects, int32_t width, int32_t height, float* density_c,
-                          float* density_m, float* density_y, float* dust, void* stream, FjErrorBuffer* error);
+                          float* density_m, float* density_y, float* dust, void* scratch, size_t scratch_bytes,
+                          void* stream, FjErrorBuffer* error);
 FjStatus fjb_gate_mask(const FjFilmEffects* effects, float* gate_mask, int32_t gate_width, int32_t gate_height,
-                       void* stream, FjErrorBuffer* error);
+                       void* scratch, size_t scratch_bytes, void* stream, FjErrorBuffer* error);
 FjStatus fjb_render_from_density_effects(FjbRecipe* recipe, const FjScannerPostEffects* post, uint64_t glare_seed,
                                          int32_t glare_origin_x, int32_t glare_origin_y,
                                          const FjFilmEffects* effects, const float* dust, const float* gate_mask,

@@ -62,7 +62,7 @@ def _reject(effects):
     lib = pkg.load_library()
     err = abi.ErrorText()
     dummy = C.c_void_p(16)  # never dereferenced: validation fails first
-    st = lib.fjb_film_defects(C.byref(effects), 8, 8, dummy, dummy, dummy, dummy, None, C.byref(err.buf))
+    st = lib.fjb_film_defects(C.byref(effects), 8, 8, dummy, dummy, dummy, dummy, None, 0, None, C.byref(err.buf))
     return st.category, err.text
 
 
@@ -94,5 +94,22 @@ def test_product_rejects_malformed_records(effects_case):
     lib_err = abi.ErrorText()
     import film_juicer_b200 as pkg
 
-    st = pkg.load_library().fjb_gate_mask(C.byref(e), C.c_void_p(16), 0, 0, None, C.byref(lib_err.buf))
+    st = pkg.load_library().fjb_gate_mask(C.byref(e), C.c_void_p(16), 0, 0, None, 0, None, C.byref(lib_err.buf))
     assert st.category == abi.FJ_STATUS_PREPARATION_FAILURE and "grid" in lib_err.text
+
+
+def test_particle_tables_cover_the_frame(effects_case):
+    # the table sizes follow the frame's cell range: non-zero for active families, zero
+    # for a record with every family off
+    import film_juicer_b200 as pkg
+
+    lib = pkg.load_library()
+    e = effects_case(0)
+    film = lib.fjb_film_defects_scratch_bytes(C.byref(e), 64, 48)
+    gate = lib.fjb_gate_mask_scratch_bytes(C.byref(e), e.gate_width, e.gate_height)
+    assert film > 0 and gate > 0 and film % 256 == 0
+    off = effects_case(0, slots=(0.0, 0.0, 0.0, 0.0))
+    assert lib.fjb_film_defects_scratch_bytes(C.byref(off), 64, 48) == 0
+    # this record's 0.56 mm sample step over 3840 x 2160 pixels spans more cells than a
+    # table holds: no table, the tiles build their own candidates
+    assert lib.fjb_film_defects_scratch_bytes(C.byref(e), 3840, 2160) == 0

@@ -182,3 +182,25 @@ def test_effects_change_the_frame_and_inactive_records_do_not(torch_cuda, recipe
     torch.cuda.synchronize()
     assert torch.equal(outs[0], outs[1])
     assert float((outs[2] - outs[0]).abs().max()) > 1e-3
+
+
+@pytest.mark.parametrize("case", [0, 18, 25, 119])
+def test_particle_table_changes_no_result(torch_cuda, effects_case, case):
+    # with the per-frame particle table or with each tile building its own candidates,
+    # the dust plane, the scratched densities and the gate mask are the same bits
+    from film_juicer_b200 import abi, runtime
+
+    torch = torch_cuda
+    e = effects_case(case)
+    w, h = frame_size(e)
+    g = torch.Generator(device="cuda").manual_seed(case)
+    base = [torch.rand((h, w), device="cuda", generator=g) * 2.0 for _ in range(3)]
+    a = [t.clone() for t in base]
+    b = [t.clone() for t in base]
+    da = runtime.film_defects(e, a, table=True)
+    db = runtime.film_defects(e, b, table=False)
+    torch.cuda.synchronize()
+    assert all(torch.equal(x, y) for x, y in zip(a, b))
+    assert (da is None and db is None) or torch.equal(da, db)
+    if e.flags & abi.FJ_EFFECTS_GATE_TRANSMITTANCE:
+        assert torch.equal(runtime.gate_mask(e, table=True), runtime.gate_mask(e, table=False))
