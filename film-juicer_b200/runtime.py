@@ -426,6 +426,32 @@ def render_from_density_effects(recipe: "DeviceRecipe", post, seed: int, origin,
     return scratch
 
 
+def tc_lut_build(spectra, sensitivity_rgb, reference_illuminant, white_xyz, method: int = 0,
+                 spectral_blur: float = 0.0, stream=None):
+    """fjb_tc_lut_build: the film TC LUT (192 * 192 * 4 floats on the GPU) from CUDA
+    spectra (192 * 192 * 81 floats) and host sensitivity (81 x 3) / illuminant (81)."""
+    import numpy as np
+
+    torch = _torch()
+    lib = load_library()
+    sens = np.ascontiguousarray(sensitivity_rgb, np.float32).reshape(-1)
+    ill = np.ascontiguousarray(reference_illuminant, np.float32).reshape(-1)
+    table = torch.empty(192 * 192 * 4, dtype=torch.float32, device=spectra.device)
+    inp = abi.FjbTcLutInput()
+    inp.spectra = _ptr(spectra)
+    inp.sensitivity_rgb = sens.ctypes.data_as(C.POINTER(C.c_float))
+    inp.reference_illuminant = ill.ctypes.data_as(C.POINTER(C.c_float))
+    for i in range(3):
+        inp.projection_white_xyz[i] = float(white_xyz[i])
+    inp.spectral_blur = spectral_blur
+    inp.method = method
+    err = abi.ErrorText()
+    st = lib.fjb_tc_lut_build(C.byref(inp), C.c_void_p(_ptr(table)), C.c_void_p(_stream_handle(stream)),
+                              C.byref(err.buf))
+    _check("fjb_tc_lut_build", st, err)
+    return table
+
+
 def highlight_boost(descriptor: "abi.FjHighlightBoost", carrier_bgr, stream=None, state=None):
     """In-place highlight reconstruction on CUDA carrier planes (B, G, R), then the
     disposition check (raises FjError on an invalid carrier or a peak overflow). Returns

@@ -92,6 +92,28 @@ FjStatus fjb_render_from_density_post(FjbRecipe* recipe, const FjScannerPostEffe
                                       int32_t height, uint32_t components, float* scratch, size_t scratch_bytes,
                                       void* stream, FjErrorBuffer* error);
 
+/* Film TC LUT on the device (reference rust/film-juicer-core/src/reconstruction.rs:594-677
+ * build_tc_lut, which the reference runs on the host when a recipe is prepared): the
+ * 192 x 192 x 81 spectra (`spectra`, device memory, [c][m][wavelength]) contracted with
+ * the sensitivity into the R, G, B, +0 table (`table`, device memory, 192 * 192 * 4
+ * floats, 16-byte aligned), word for word the reference's. method 0: Hanatos
+ * irradiance, with the spectral blur when `spectral_blur` > 0 (radius up to 80
+ * samples); method 2: Arctic reflectance relit by the reference illuminant and
+ * normalised by the neutral response at the projected white. The surface correction
+ * and the input-compression remap are not built here (the call rejects them). The call
+ * allocates 16 bytes of device memory for its own use and synchronises `stream`. */
+typedef struct FjbTcLutInput {
+    const float* spectra;              /* device, 192*192*81 */
+    const float* sensitivity_rgb;      /* host, 81 x 3 */
+    const float* reference_illuminant; /* host, 81 */
+    float projection_white_xyz[3];
+    float spectral_blur;
+    uint32_t method;
+    uint32_t apply_surface;
+    uint32_t input_compression;
+} FjbTcLutInput;
+FjStatus fjb_tc_lut_build(const FjbTcLutInput* input, float* table, void* stream, FjErrorBuffer* error);
+
 /* Film and gate defects (reference src/Cuda/Scan/JuicerCudaScanPipeline.cu:2186-2242
  * juicer_cuda_apply_film_defects / juicer_cuda_build_gate_defect_transmittance_focused,
  * scheduled by src/Cuda/JuicerCudaExecutor.cpp:1674-1690, :2263-2279, :1806-1830).

@@ -205,6 +205,31 @@ def effects_cases():
     print("effects cases:", len(keep))
 
 
+def tc_lut_cases():
+    """TC LUT characterization (tests/ffi/fixtures/tc_lut/records-0.json, built by
+    tests/ffi/tc_lut_test.cpp): the cases whose source is the procedural spectra
+    (word i = 0x3e000123 + (i % 4093) * 173) and that need neither the surface
+    correction nor the input compression: inputs as IEEE bit patterns, the expected
+    status and requirement, and the FNV-1a digest of the complete table."""
+    with open(os.path.join(REF, "tests", "ffi", "fixtures", "tc_lut", "records-0.json")) as fh:
+        doc = json.load(fh)
+    keep = []
+    for c in doc["leaves"]["cases"]:
+        i = c["input"]
+        if i["source"] != "procedural_4093_173" or i["surface"] or i["compression"] or i["id"] in (16, 17):
+            continue
+        row = dict(id=i["id"], built=c["built"], method=i["method"], blur=i["blur"], sensitivity=i["sensitivity"],
+                   spd=i["spd"], white=i["white"],
+                   requirement=c["diagnostic"].split("requirement=")[-1] if not c["built"] else "")
+        if c["built"]:
+            row["digest"] = str(c["table"]["native_byte_digest_fnv1a64"])
+            row["selected"] = c["table"]["selected"]
+        keep.append(row)
+    with open(os.path.join(HERE, "tc_lut_cases.json"), "w") as fh:
+        json.dump(keep, fh, separators=(",", ":"))
+    print("tc lut cases:", [r["id"] for r in keep])
+
+
 def recipes():
     sys.path.insert(0, ROOT)
     import __graft_entry__
@@ -226,4 +251,5 @@ if __name__ == "__main__":
     grain_plan_cases()
     gaussian_cases()
     effects_cases()
+    tc_lut_cases()
     recipes()
