@@ -21,7 +21,7 @@
 // B200 schedule. A pre-pass builds every candidate of the frame's cell range once, one
 // per thread, into a particle table (a candidate depends only on its cell address). A
 // CTA covers a 32 x 8 pixel tile: its threads read the candidates of the tile's cell
-// range 256 at a time from the table (or build them, when no table was given) and keep
+// range kChunk at a time from the table (or build them, when no table was given) and keep
 // -- in candidate order -- only the active ones whose bounding box, widened by softness
 // and the pixel footprint, can reach the tile; the tile's pixels then multiply over
 // that short list. A candidate
@@ -41,6 +41,9 @@ namespace fjb {
 namespace {
 
 constexpr int kTileX = 32, kTileY = 8, kTileThreads = kTileX * kTileY;
+// candidates a tile takes per round (the first kChunk threads read or build one each);
+// the shared list of reachable candidates holds at most one round
+constexpr int kChunk = 64;
 
 __device__ __forceinline__ uint64_t mix64(uint64_t x) {
     x += 0x9E3779B97F4A7C15ULL;
@@ -430,11 +433,11 @@ __device__ float family_retained(const FjFilmEffects& e, int family, int tile_x,
     const int t = threadIdx.y * blockDim.x + threadIdx.x;
     const int lane_id = t & 31, warp = t >> 5;
     float retained = 1.0f;
-    for (int first = 0; first < total; first += kTileThreads) {
+    for (int first = 0; first < total; first += kChunk) {
         const int ordinal = first + t;
         bool keep = false;
         Particle q;
-        if (ordinal < total) {
+        if (t < kChunk && ordinal < total) {
             const int dx = x0 + (ordinal / 2) % columns;
             const int dy = y0 + (ordinal / 2) / columns;
             const int gx = dx - table.x0, gy = dy - table.y0;
@@ -457,10 +460,10 @@ __device__ float family_retained(const FjFilmEffects& e, int family, int tile_x,
         }
         // order-preserving compaction of the kept candidates
         const unsigned ballot = __ballot_sync(0xffffffffu, keep);
-        if (lane_id == 0) counts[warp] = __popc(ballot);
+        if (lane_id == 0 && warp < kChunk / 32) counts[warp] = __popc(ballot);
         __syncthreads();
         int before = 0, kept = 0;
-        for (int w = 0; w < kTileThreads / 32; ++w) {
+        for (int w = 0; w < kChunk / 32; ++w) {
             before += w < warp ? counts[w] : 0;
             kept += counts[w];
         }
@@ -472,11 +475,11 @@ __device__ float family_retained(const FjFilmEffects& e, int family, int tile_x,
     return retained;
 }
 
-__global__ void __launch_bounds__(kTileThreads) film_defects_kernel(const __grid_constant__ FjFilmEffects e, int width,
+__global__ void __launch_bounds__(kTileThreads, 3) film_defects_kernel(const __grid_constant__ FjFilmEffects e, int width,
                                                                     int height, float* c, float* m, float* yp,
                                                                     float* dust_out, FrameTables tables) {
-    __shared__ Particle list[kTileThreads];
-    __shared__ int counts[kTileThreads / 32];
+    __shared__ Particle list[kChunk];
+    __shared__ int counts[kChunk / 32];
     const int tx = blockIdx.x * kTileX, ty = blockIdx.y * kTileY;
     const int x = tx + threadIdx.x, y = ty + threadIdx.y;
     const int fx = x + e.roi_offset_x, fy = y + e.roi_offset_y;
@@ -496,8 +499,8 @@ __global__ void __launch_bounds__(kTileThreads) film_defects_kernel(const __grid
 
 __global__ void __launch_bounds__(kTileThreads) gate_mask_kernel(const __grid_constant__ FjFilmEffects e, float* mask,
                                                                  int width, int height, FrameTables tables) {
-    __shared__ Particle list[kTileThreads];
-    __shared__ int counts[kTileThreads / 32];
+    __shared__ Particle list[kChunk];
+    __shared__ int counts[kChunk / 32];
     const int tx = blockIdx.x * kTileX, ty = blockIdx.y * kTileY;
     const int x = tx + threadIdx.x, y = ty + threadIdx.y;
     const float dust = family_retained(e, 2, tx, ty, x, y, 2.0f, tables.t[0], list, counts);
