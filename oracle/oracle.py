@@ -187,6 +187,10 @@ def load_reference():
                                          C.POINTER(abi.FjScannerPostEffects), C.c_ulonglong, C.c_int, C.c_int,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p,
                                          C.c_long, C.c_int, C.c_int, C.c_int]
+    if hasattr(lib, "ref_defects_timed"):
+        lib.ref_defects_timed.restype = C.c_int
+        lib.ref_defects_timed.argtypes = [C.POINTER(abi.FjFilmEffects), C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p]
     if hasattr(lib, "ref_effects_render"):
         lib.ref_effects_render.restype = C.c_int
         lib.ref_effects_render.argtypes = [C.POINTER(abi.FjPreparedHostData), C.POINTER(C.c_void_p),

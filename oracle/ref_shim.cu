@@ -861,3 +861,20 @@ extern "C" int ref_effects_render(const FjPreparedHostData* h, const float* cons
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return (int)e;
 }
+
+// The reference's film-defect and gate-mask launchers alone, each timed with CUDA
+// events (ref_last_ms after each call): `which` 0 film defects (density planes in
+// place, dust plane), 1 gate mask (gate grid).
+extern "C" int ref_defects_timed(const FjFilmEffects* fx, int which, int width, int height, float* dc, float* dm,
+                                 float* dy, float* out) {
+    JuicerCuda::FilmDefectsPayload defects;
+    JuicerCuda::GateWeavePayload weave;
+    pack_effects(*fx, defects, weave);
+    LaunchTimer timer;
+    cudaError_t e = which == 0
+                        ? juicer_cuda_apply_film_defects(&defects, width, height, dc, dm, dy, out, nullptr)
+                        : juicer_cuda_build_gate_defect_transmittance_focused(&defects, out, width, height, nullptr);
+    timer.stop();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return (int)e;
+}

@@ -81,6 +81,39 @@ def test_stage_times_against_reference_cuda(torch_cuda, recipes, prepare, oracle
         ograin.reference_visual_grain(torch, rec.host.h.grain, rec.noise.record, base, layers, False, dens)
     theirs["grain"] = ref.ref_last_ms()
 
+    # film defects and the gate mask at 4K (the bench's next-rows record)
+    if hasattr(ref, "ref_defects_timed"):
+        from film_juicer_b200 import descriptors
+
+        fx = descriptors.default_film_effects(W, H)
+        fdens = [torch.from_numpy(p).cuda() for p in dens]
+        dust = torch.empty((H, W), device="cuda")
+        mask = torch.empty((fx.gate_height, fx.gate_width), device="cuda")
+        need = max(int(lib.fjb_film_defects_scratch_bytes(C.byref(fx), W, H)),
+                   int(lib.fjb_gate_mask_scratch_bytes(C.byref(fx), fx.gate_width, fx.gate_height)))
+        table = torch.empty(need // 4 + 1, device="cuda")
+        calls = {
+            "film_defects": lambda: lib.fjb_film_defects(C.byref(fx), W, H, *[C.c_void_p(p.data_ptr()) for p in fdens],
+                                                         C.c_void_p(dust.data_ptr()), C.c_void_p(table.data_ptr()),
+                                                         need, None, C.byref(err.buf)),
+            "gate_mask": lambda: lib.fjb_gate_mask(C.byref(fx), C.c_void_p(mask.data_ptr()), fx.gate_width,
+                                                   fx.gate_height, C.c_void_p(table.data_ptr()), need, None,
+                                                   C.byref(err.buf)),
+        }
+        for k, call in calls.items():
+            call()
+            e0.record()
+            for _ in range(5):
+                assert call().category == abi.FJ_STATUS_SUCCESS
+            e1.record()
+            e1.synchronize()
+            ours[k] = e0.elapsed_time(e1) / 5
+        for which, k, w, h in ((0, "film_defects", W, H), (1, "gate_mask", fx.gate_width, fx.gate_height)):
+            for _ in range(2):
+                assert ref.ref_defects_timed(C.byref(fx), which, w, h, *[C.c_void_p(p.data_ptr()) for p in fdens],
+                                             C.c_void_p((dust if which == 0 else mask).data_ptr())) == 0
+            theirs[k] = ref.ref_last_ms()
+
     table = {k: {"ours_ms": round(ours[k], 4), "reference_ms": round(theirs[k], 4),
                  "speedup": round(theirs[k] / ours[k], 2)} for k in theirs}
     print(json.dumps(table, indent=1))
