@@ -7,7 +7,10 @@
 // projected white, projected_white :124-137). The host code rounds every float product
 // and sum on its own (Rust does not fuse), so the kernels spell each one out with
 // __fmul_rn / __fadd_rn / __fdiv_rn: the table is the reference's word for word.
-// The surface correction and the input-compression remap stay on the host.
+// The Hanatos surface correction (eval_hanatos_surface :570-593) is a factor per node
+// and channel: exp2 of a polynomial in the node's offset from the projected white,
+// evaluated on the host with the C library's exp2f (what f32::exp2 calls) and applied
+// on the device. The input-compression remap stays on the host.
 //
 // B200 schedule: one thread per (c, m) node, the 81 wavelengths (blurred on the fly
 // when the blur is on, each tap in the reference's order) contracted with the
@@ -128,8 +131,8 @@ __global__ void tc_neutral_kernel(const float* __restrict__ spectra, const __gri
 }
 
 __global__ void __launch_bounds__(128) tc_lut_kernel(const float* __restrict__ spectra, const __grid_constant__ TcParams p,
-                                                     const float* __restrict__ den, float* __restrict__ table,
-                                                     unsigned* flags) {
+                                                     const float* __restrict__ den, const float* __restrict__ surface,
+                                                     float* __restrict__ table, unsigned* flags) {
     const int node = blockIdx.x * blockDim.x + threadIdx.x;
     if (node >= kNodes) return;
     if (p.arctic && (__ldg(flags) & kNeutralInvalid)) return;
@@ -147,6 +150,7 @@ __global__ void __launch_bounds__(128) tc_lut_kernel(const float* __restrict__ s
     float* o = &out.x;
     for (int c = 0; c < 3; ++c) {
         o[c] = p.arctic ? __fdiv_rn(raw[c], den[c]) : __fdiv_rn(raw[c], 1.0f);
+        if (surface) o[c] = __fmul_rn(o[c], __ldg(surface + (size_t)node * 3 + c));
         bad |= !isfinite(o[c]);
     }
     out.w = 0.0f;
@@ -165,6 +169,41 @@ float add(float a, float b) {
     return r;
 }
 
+// exp2 of the surface polynomial per node and channel (reconstruction.rs:570-593,
+// :626-660): tc = (c / 191, m / 191) about the projected white.
+std::vector<float> surface_factors(const float* params, float center_c, float center_m) {
+    std::vector<float> f((size_t)kNodes * 3);
+    for (int c = 0; c < 192; ++c) {
+        const float tcc = (float)c / 191.0f;
+        for (int m = 0; m < 192; ++m) {
+            const float tcm = (float)m / 191.0f;
+            const float x = add(tcc, -center_c), y = add(tcm, -center_m);
+            const float x2 = mul(x, x), y2 = mul(y, y), x3 = mul(x2, x), y3 = mul(y2, y);
+            for (int ch = 0; ch < 3; ++ch) {
+                const float* q = params + ch * 15;
+                float raw = mul(q[1], x);
+                raw = add(raw, mul(q[2], y));
+                raw = add(raw, mul(q[3], x2));
+                raw = add(raw, mul(q[4], y2));
+                raw = add(raw, mul(mul(q[5], x), y));
+                raw = add(raw, mul(q[6], x3));
+                raw = add(raw, mul(q[7], y3));
+                raw = add(raw, mul(mul(q[8], x2), y));
+                raw = add(raw, mul(mul(q[9], x), y2));
+                raw = add(raw, mul(mul(q[10], x2), x2));
+                raw = add(raw, mul(mul(q[11], y2), y2));
+                raw = add(raw, mul(mul(q[12], x3), y));
+                raw = add(raw, mul(mul(q[13], x2), y2));
+                raw = add(raw, mul(mul(q[14], x), y3));
+                const float n = raw / 2.0f;
+                const float v = raw / std::sqrt(add(1.0f, mul(n, n)));
+                f[((size_t)c * 192 + m) * 3 + ch] = ::exp2f(v);
+            }
+        }
+    }
+    return f;
+}
+
 } // namespace
 
 } // namespace fjb
@@ -176,9 +215,11 @@ extern "C" FjStatus fjb_tc_lut_build(const FjbTcLutInput* in, float* table, void
             return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
         if (in->method != 0 && in->method != 2)
             return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "TC LUT: method must be Hanatos (0) or Arctic (2)");
-        if (in->apply_surface || in->input_compression)
+        if (in->input_compression)
+            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "TC LUT: the input compression is built on the host");
+        if (in->apply_surface && (in->method != 0 || !in->surface_rgb))
             return fail_status(FJ_STATUS_PREPARATION_FAILURE, error,
-                               "TC LUT: the surface correction and the input compression are built on the host");
+                               "TC LUT: the surface correction needs the Hanatos method and its 3 x 15 parameters");
         TcParams p{};
         std::memcpy(p.sens, in->sensitivity_rgb, sizeof(p.sens));
         std::memcpy(p.illum, in->reference_illuminant, sizeof(p.illum));
@@ -222,14 +263,36 @@ extern "C" FjStatus fjb_tc_lut_build(const FjbTcLutInput* in, float* table, void
             if (!std::isfinite(p.tc_c) || !std::isfinite(p.tc_m))
                 return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "TC LUT: requirement=finite_d65_projection_white");
         }
+        std::vector<float> factors;
+        if (in->apply_surface) {
+            const float* w = in->projection_white_xyz;
+            const float sum = add(add(w[0], w[1]), w[2]);
+            if (!std::isfinite(sum) || !(sum > 0.0f))
+                return fail_status(FJ_STATUS_PREPARATION_FAILURE, error,
+                                   "TC LUT: requirement=finite_surface_reference_white");
+            const float tx = w[0] / sum, ty = w[1] / sum;
+            const float x = add(1.0f, -tx);
+            const float den = x < 1e-10f ? 1e-10f : x;
+            const float cc = std::fmin(std::fmax(mul(x, x), 0.0f), 1.0f);
+            const float cm = std::fmin(std::fmax(ty / den, 0.0f), 1.0f);
+            if (!std::isfinite(cc) || !std::isfinite(cm))
+                return fail_status(FJ_STATUS_PREPARATION_FAILURE, error,
+                                   "TC LUT: requirement=finite_surface_reference_white");
+            factors = surface_factors(in->surface_rgb, cc, cm);
+        }
         cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-        // denominators and the failure flags: 16 bytes for the call, freed before it returns
+        // denominators, failure flags and the surface factors: freed before the call returns
+        const size_t bytes = 256 + factors.size() * sizeof(float);
         void* scratch = nullptr;
-        cudaError_t e = cudaMalloc(&scratch, 16);
+        cudaError_t e = cudaMalloc(&scratch, bytes);
         if (e != cudaSuccess) return cuda_status(e, error, "TC LUT scratch");
         float* den = static_cast<float*>(scratch);
         unsigned* flags = reinterpret_cast<unsigned*>(den + 3);
+        float* surface = factors.empty() ? nullptr : reinterpret_cast<float*>(static_cast<char*>(scratch) + 256);
         e = cudaMemsetAsync(scratch, 0, 16, s);
+        // pageable source: the copy completes before cudaMemcpyAsync returns
+        if (e == cudaSuccess && surface)
+            e = cudaMemcpyAsync(surface, factors.data(), factors.size() * sizeof(float), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess && p.arctic) {
             fjb::count_launch();
             tc_neutral_kernel<<<1, 1, 0, s>>>(in->spectra, p, den, flags);
@@ -237,7 +300,7 @@ extern "C" FjStatus fjb_tc_lut_build(const FjbTcLutInput* in, float* table, void
         }
         if (e == cudaSuccess) {
             fjb::count_launch();
-            tc_lut_kernel<<<(kNodes + 127) / 128, 128, 0, s>>>(in->spectra, p, den, table, flags);
+            tc_lut_kernel<<<(kNodes + 127) / 128, 128, 0, s>>>(in->spectra, p, den, surface, table, flags);
             e = cudaGetLastError();
         }
         unsigned f = 0;

@@ -427,7 +427,7 @@ def render_from_density_effects(recipe: "DeviceRecipe", post, seed: int, origin,
 
 
 def tc_lut_build(spectra, sensitivity_rgb, reference_illuminant, white_xyz, method: int = 0,
-                 spectral_blur: float = 0.0, stream=None):
+                 spectral_blur: float = 0.0, surface=None, stream=None):
     """fjb_tc_lut_build: the film TC LUT (192 * 192 * 4 floats on the GPU) from CUDA
     spectra (192 * 192 * 81 floats) and host sensitivity (81 x 3) / illuminant (81)."""
     import numpy as np
@@ -445,6 +445,10 @@ def tc_lut_build(spectra, sensitivity_rgb, reference_illuminant, white_xyz, meth
         inp.projection_white_xyz[i] = float(white_xyz[i])
     inp.spectral_blur = spectral_blur
     inp.method = method
+    if surface is not None:
+        surf = np.ascontiguousarray(surface, np.float32).reshape(-1)
+        inp.apply_surface = 1
+        inp.surface_rgb = surf.ctypes.data_as(C.POINTER(C.c_float))
     err = abi.ErrorText()
     st = lib.fjb_tc_lut_build(C.byref(inp), C.c_void_p(_ptr(table)), C.c_void_p(_stream_handle(stream)),
                               C.byref(err.buf))

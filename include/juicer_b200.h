@@ -99,9 +99,11 @@ FjStatus fjb_render_from_density_post(FjbRecipe* recipe, const FjScannerPostEffe
  * floats, 16-byte aligned), word for word the reference's. method 0: Hanatos
  * irradiance, with the spectral blur when `spectral_blur` > 0 (radius up to 80
  * samples); method 2: Arctic reflectance relit by the reference illuminant and
- * normalised by the neutral response at the projected white. The surface correction
- * and the input-compression remap are not built here (the call rejects them). The call
- * allocates 16 bytes of device memory for its own use and synchronises `stream`. */
+ * normalised by the neutral response at the projected white; `apply_surface` (Hanatos)
+ * multiplies by the surface correction of `surface_rgb` (host, 3 x 15). The
+ * input-compression remap is not built here (the call rejects it). The call allocates
+ * device memory for its own use (256 B, plus 432 KiB with the surface correction),
+ * frees it and synchronises `stream` before returning. */
 typedef struct FjbTcLutInput {
     const float* spectra;              /* device, 192*192*81 */
     const float* sensitivity_rgb;      /* host, 81 x 3 */
@@ -111,6 +113,7 @@ typedef struct FjbTcLutInput {
     uint32_t method;
     uint32_t apply_surface;
     uint32_t input_compression;
+    const float* surface_rgb;          /* host, 3 x 15, with apply_surface */
 } FjbTcLutInput;
 FjStatus fjb_tc_lut_build(const FjbTcLutInput* input, float* table, void* stream, FjErrorBuffer* error);
 

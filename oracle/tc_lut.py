@@ -7,7 +7,8 @@ blur_spectra :540-569, gaussian_kernel :227-268, gaussian_reflect_index :270-279
 sample_mitchell :501-538, mitchell_weight :139-157, mitchell_coordinate :159-169,
 mitchell_reflect_index :171-180, projected_white :124-137, tri2quad :352-356) for the
 Hanatos irradiance method (optionally with spectral blur) and the Arctic reflectance
-method; the surface correction and the input-compression remap are not restated. Every
+method, and the Hanatos surface correction (eval_hanatos_surface :570-593, exp2 from
+the C library as f32::exp2 is); the input-compression remap is not restated. Every
 float32 product and sum is rounded on its own, as the Rust code is (no fused
 multiply-add); reductions run in the reference's order. Raises ValueError with the
 reference's requirement name where it fails.
@@ -23,6 +24,8 @@ F = np.float32
 _libm = C.CDLL("libm.so.6")
 _libm.expf.restype = C.c_float
 _libm.expf.argtypes = [C.c_float]
+_libm.exp2f.restype = C.c_float
+_libm.exp2f.argtypes = [C.c_float]
 CELLS = 192 * 192
 
 
@@ -131,9 +134,43 @@ def sample_mitchell(spectra: np.ndarray, tc, sample: int) -> np.float32:
     return F(value / wsum) if wsum != 0.0 else F(0.0)
 
 
+def surface_factors(params: np.ndarray, center) -> np.ndarray:
+    """exp2 of the Hanatos surface polynomial at every node, (192 * 192, 3) float32."""
+    out = np.empty((CELLS, 3), np.float32)
+    for c in range(192):
+        tcc = F(F(c) / F(191.0))
+        for m in range(192):
+            tcm = F(F(m) / F(191.0))
+            x = F(tcc - center[0])
+            y = F(tcm - center[1])
+            x2, y2 = F(x * x), F(y * y)
+            x3, y3 = F(x2 * x), F(y2 * y)
+            for ch in range(3):
+                p = params[ch]
+                raw = F(p[1] * x)
+                raw = F(raw + F(p[2] * y))
+                raw = F(raw + F(p[3] * x2))
+                raw = F(raw + F(p[4] * y2))
+                raw = F(raw + F(F(p[5] * x) * y))
+                raw = F(raw + F(p[6] * x3))
+                raw = F(raw + F(p[7] * y3))
+                raw = F(raw + F(F(p[8] * x2) * y))
+                raw = F(raw + F(F(p[9] * x) * y2))
+                raw = F(raw + F(F(p[10] * x2) * x2))
+                raw = F(raw + F(F(p[11] * y2) * y2))
+                raw = F(raw + F(F(p[12] * x3) * y))
+                raw = F(raw + F(F(p[13] * x2) * y2))
+                raw = F(raw + F(F(p[14] * x) * y3))
+                n = F(raw / F(2.0))
+                v = F(raw / F(np.sqrt(F(F(1.0) + F(n * n)))))
+                out[c * 192 + m, ch] = F(_libm.exp2f(float(v)))
+    return out
+
+
 def build_tc_lut(spectra: np.ndarray, sensitivity: np.ndarray, illuminant: np.ndarray, white, method: int,
-                 blur_sigma: np.float32) -> np.ndarray:
-    """192 x 192 x 4 (R, G, B, +0) float32 table; method 0 Hanatos, 2 Arctic."""
+                 blur_sigma: np.float32, surface=None) -> np.ndarray:
+    """192 x 192 x 4 (R, G, B, +0) float32 table; method 0 Hanatos, 2 Arctic; `surface`
+    (3 x 15 float32, Hanatos only) applies the surface correction."""
     sens = np.asarray(sensitivity, np.float32).reshape(81, 3)
     ill = np.asarray(illuminant, np.float32)
     if not np.all(np.isfinite(ill) & (ill >= 0.0)):
@@ -153,6 +190,13 @@ def build_tc_lut(spectra: np.ndarray, sensitivity: np.ndarray, illuminant: np.nd
                 den[c] = F(den[c] + F(relit * sens[s, c]))
         if not all(np.isfinite(d) and d > 0.0 for d in den):
             raise ValueError("finite_positive_neutral_response")
+    factors = None
+    if method == 0 and surface is not None:
+        try:
+            center = projected_white(white)
+        except ValueError:
+            raise ValueError("finite_surface_reference_white") from None
+        factors = surface_factors(np.asarray(surface, np.float32).reshape(3, 15), center)
     src = selected.reshape(CELLS, 81)
     raw = np.zeros((CELLS, 3), np.float32)
     for s in range(81):
@@ -163,6 +207,8 @@ def build_tc_lut(spectra: np.ndarray, sensitivity: np.ndarray, illuminant: np.nd
     out = np.zeros((CELLS, 4), np.float32)
     for c in range(3):
         out[:, c] = (raw[:, c] / den[c]).astype(np.float32)
+        if factors is not None:
+            out[:, c] = (out[:, c] * factors[:, c]).astype(np.float32)
     if not np.all(np.isfinite(out[:, :3])):
         raise ValueError("finite_integrated_samples")
     return out.reshape(-1)

@@ -1,7 +1,7 @@
 """The film TC LUT oracle (oracle/tc_lut.py) pinned on the reference's characterization
 (tests/golden/tc_lut_cases.json, from tests/ffi/fixtures/tc_lut/records-0.json): the
 FNV-1a digest of every complete table it builds (Hanatos with and without spectral
-blur, Arctic, negative and NaN blur bypasses) and the requirement of every case the
+blur or surface correction, Arctic, negative and NaN blur bypasses) and the requirement of every case the
 reference rejects."""
 import json
 import os
@@ -30,7 +30,10 @@ def inputs(case):
     sens = np.array([[f32(v) for v in row] for row in case["sensitivity"]], np.float32)
     ill = np.array([f32(v) for v in case["spd"]], np.float32)
     white = [f32(v) for v in case["white"]]
-    return spectra, sens, ill, white, case["method"], f32(case["blur"])
+    surface = None
+    if case.get("surface"):
+        surface = np.array([[f32(v) for v in row] for row in case["surface_params"]], np.float32)
+    return spectra, sens, ill, white, case["method"], f32(case["blur"]), surface
 
 
 @pytest.mark.parametrize("case", CASES, ids=[str(c["id"]) for c in CASES])

@@ -16,16 +16,16 @@ def test_device_tc_lut_matches_reference_words(torch_cuda, case):
     from oracle import tc_lut
 
     torch = torch_cuda
-    spectra, sens, ill, white, method, blur = inputs(case)
+    spectra, sens, ill, white, method, blur, surface = inputs(case)
     dev = torch.from_numpy(spectra).cuda()
     if not case["built"]:
         with pytest.raises(runtime.FjError) as e:
-            runtime.tc_lut_build(dev, sens, ill, white, method, float(blur))
+            runtime.tc_lut_build(dev, sens, ill, white, method, float(blur), surface)
         assert str(e.value).rstrip().endswith("requirement=" + case["requirement"])
         return
-    table = runtime.tc_lut_build(dev, sens, ill, white, method, float(blur)).cpu().numpy()
+    table = runtime.tc_lut_build(dev, sens, ill, white, method, float(blur), surface).cpu().numpy()
     assert tc_lut.digest(table) == int(case["digest"])
-    want = tc_lut.build_tc_lut(spectra, sens, ill, white, method, blur)
+    want = tc_lut.build_tc_lut(spectra, sens, ill, white, method, blur, surface)
     assert np.array_equal(table.view(np.uint32), want.view(np.uint32))
 
 
@@ -42,7 +42,7 @@ def test_device_tc_lut_rejects_host_only_stages(torch_cuda):
     inp.spectra = 16
     inp.sensitivity_rgb = sens.ctypes.data_as(C.POINTER(C.c_float))
     inp.reference_illuminant = ill.ctypes.data_as(C.POINTER(C.c_float))
-    inp.apply_surface = 1
+    inp.input_compression = 1
     err = abi.ErrorText()
     st = lib.fjb_tc_lut_build(C.byref(inp), C.c_void_p(16), None, C.byref(err.buf))
     assert st.category == abi.FJ_STATUS_PREPARATION_FAILURE and "host" in err.text
