@@ -261,7 +261,9 @@ FjDiffusionComponents = _s("FjDiffusionComponents", [("lambda_px", f64 * 9), ("r
 FjbTcLutInput = _s("FjbTcLutInput", [("spectra", C.c_void_p), ("sensitivity_rgb", C.POINTER(C.c_float)),
                                      ("reference_illuminant", C.POINTER(C.c_float)), ("projection_white_xyz", f32 * 3),
                                      ("spectral_blur", f32), ("method", u32), ("apply_surface", u32),
-                                     ("input_compression", u32), ("surface_rgb", C.POINTER(C.c_float))])
+                                     ("input_compression", u32), ("surface_rgb", C.POINTER(C.c_float)),
+                                     ("hull_xy", C.POINTER(C.c_float)), ("hull_center", f32 * 2),
+                                     ("hull_available", u32)])
 FJB_STAGE_NAMES = ["auto_exposure", "camera_exposure", "camera_diffusion", "scatter_halation", "spatial_dir",
                    "capture_density", "grain", "print_scan_output", "monolithic", "film_defects"]
 FjbStageTimes = _s("FjbStageTimes", [("total_ms", f64 * 10), ("frames", u64 * 10)])

@@ -10,7 +10,10 @@
 // The Hanatos surface correction (eval_hanatos_surface :570-593) is a factor per node
 // and channel: exp2 of a polynomial in the node's offset from the projected white,
 // evaluated on the host with the C library's exp2f (what f32::exp2 calls) and applied
-// on the device. The input-compression remap stays on the host.
+// on the device. The input-compression remap (gamut.rs:259-373) moves every node to the
+// coordinates of its compressed chromaticity: those depend only on the input hull, so
+// the host computes them in FP64 with the C library's hypot and pow (as the Rust host
+// does) and the device resamples the table bilinearly, unfused, at them.
 //
 // B200 schedule: one thread per (c, m) node, the 81 wavelengths (blurred on the fly
 // when the blur is on, each tap in the reference's order) contracted with the
@@ -34,7 +37,8 @@ namespace {
 
 constexpr int kNodes = 192 * 192;
 constexpr int kMaxBlurTaps = 161; // radius 80: wider kernels fold onto the 81 samples anyway
-constexpr unsigned kBlurNonFinite = 1u, kIntegratedNonFinite = 2u, kNeutralInvalid = 4u;
+constexpr unsigned kBlurNonFinite = 1u, kIntegratedNonFinite = 2u, kNeutralInvalid = 4u, kSamplingUnusable = 8u,
+                   kRemappedNonFinite = 16u;
 
 struct TcParams {
     float sens[81 * 3];
@@ -159,6 +163,38 @@ __global__ void __launch_bounds__(128) tc_lut_kernel(const float* __restrict__ s
     if (bad) atomicOr(flags, kIntegratedNonFinite);
 }
 
+// Bilinear resampling of the built table at each node's compressed coordinates
+// (gamut.rs:324-341, every product and sum rounded alone).
+__global__ void __launch_bounds__(128) tc_remap_kernel(const float* __restrict__ built, const float2* __restrict__ tc,
+                                                       float* __restrict__ table, unsigned* flags) {
+    const int node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= kNodes) return;
+    const float2 t = tc[node];
+    const float cp = __fmul_rn(fminf(fmaxf(t.x, 0.0f), 1.0f), 191.0f);
+    const float mp = __fmul_rn(fminf(fmaxf(t.y, 0.0f), 1.0f), 191.0f);
+    if (!isfinite(cp) || !isfinite(mp)) {
+        atomicOr(flags, kSamplingUnusable);
+        return;
+    }
+    const int c0 = (int)floorf(cp), m0 = (int)floorf(mp);
+    const int c1 = min(c0 + 1, 191), m1 = min(m0 + 1, 191);
+    const float cf = __fadd_rn(cp, -(float)c0), mf = __fadd_rn(mp, -(float)m0);
+    float4 out;
+    float* o = &out.x;
+    bool bad = false;
+    for (int ch = 0; ch < 3; ++ch) {
+        const float v00 = built[(c0 * 192 + m0) * 4 + ch], v10 = built[(c1 * 192 + m0) * 4 + ch];
+        const float v01 = built[(c0 * 192 + m1) * 4 + ch], v11 = built[(c1 * 192 + m1) * 4 + ch];
+        const float r0 = __fadd_rn(v00, __fmul_rn(cf, __fadd_rn(v10, -v00)));
+        const float r1 = __fadd_rn(v01, __fmul_rn(cf, __fadd_rn(v11, -v01)));
+        o[ch] = __fadd_rn(r0, __fmul_rn(mf, __fadd_rn(r1, -r0)));
+        bad |= !isfinite(o[ch]);
+    }
+    out.w = 0.0f;
+    reinterpret_cast<float4*>(table)[node] = out;
+    if (bad) atomicOr(flags, kRemappedNonFinite);
+}
+
 // f32 arithmetic the compiler may not fuse (host side of the reference's kernel set-up)
 float mul(float a, float b) {
     volatile float r = a * b;
@@ -204,6 +240,57 @@ std::vector<float> surface_factors(const float* params, float center_c, float ce
     return f;
 }
 
+// Compressed TC coordinates of every node (gamut.rs:259-373 compress, knee,
+// ray_polygon_distance; remap_tc_lut's node chromaticities). False when a node's
+// compression is unusable.
+bool remap_coordinates(const float* hull_xy, const float* center, std::vector<float>& out) {
+    out.assign((size_t)kNodes * 2, 0.0f);
+    const double c0 = center[0], c1 = center[1];
+    for (int c = 0; c < 192; ++c) {
+        const float root = std::sqrt((float)c / 191.0f);
+        for (int m = 0; m < 192; ++m) {
+            const float xy0 = add(1.0f, -root), xy1 = mul((float)m / 191.0f, root);
+            const double dx = (double)xy0 - c0, dy = (double)xy1 - c1;
+            const double dist = std::hypot(dx, dy);
+            float rx = xy0, ry = xy1;
+            if (!(dist < 1e-9)) {
+                const double ux = dx / dist, uy = dy / dist;
+                double best = INFINITY;
+                for (int k = 0; k < 1024; ++k) {
+                    const double ax = hull_xy[2 * k], ay = hull_xy[2 * k + 1];
+                    const double ex = (double)hull_xy[2 * k + 2] - ax, ey = (double)hull_xy[2 * k + 3] - ay;
+                    const double den = ux * ey - uy * ex;
+                    if (std::fabs(den) <= 1e-12) continue;
+                    const double ox = c0 - ax, oy = c1 - ay;
+                    const double d = (-ox * ey + oy * ex) / den;
+                    if (d > 1e-9 && d < best) {
+                        const double pos = (-ox * uy + oy * ux) / den;
+                        if (pos >= -1e-9 && pos <= 1.0 + 1e-9) best = d;
+                    }
+                }
+                if (!std::isfinite(best) || best <= 1e-12) return false;
+                double t = dist / best;
+                if (t > 0.815) {
+                    const double scale = 1.0 - 0.815;
+                    const double u = (t - 0.815) / scale;
+                    t = 0.815 + scale * (u / std::pow(1.0 + std::pow(u, 1.2), 1.0 / 1.2));
+                }
+                const double cd = t * best;
+                const double px = c0 + ux * cd, py = c1 + uy * cd;
+                if (!std::isfinite(px) || !std::isfinite(py)) return false;
+                rx = (float)px;
+                ry = (float)py;
+            }
+            // tri2quad (reconstruction.rs:352-356)
+            const float x = add(1.0f, -rx);
+            const float dn = x < 1e-10f ? 1e-10f : x;
+            out[((size_t)c * 192 + m) * 2] = std::fmin(std::fmax(mul(x, x), 0.0f), 1.0f);
+            out[((size_t)c * 192 + m) * 2 + 1] = std::fmin(std::fmax(ry / dn, 0.0f), 1.0f);
+        }
+    }
+    return true;
+}
+
 } // namespace
 
 } // namespace fjb
@@ -215,8 +302,6 @@ extern "C" FjStatus fjb_tc_lut_build(const FjbTcLutInput* in, float* table, void
             return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
         if (in->method != 0 && in->method != 2)
             return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "TC LUT: method must be Hanatos (0) or Arctic (2)");
-        if (in->input_compression)
-            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "TC LUT: the input compression is built on the host");
         if (in->apply_surface && (in->method != 0 || !in->surface_rgb))
             return fail_status(FJ_STATUS_PREPARATION_FAILURE, error,
                                "TC LUT: the surface correction needs the Hanatos method and its 3 x 15 parameters");
@@ -280,19 +365,33 @@ extern "C" FjStatus fjb_tc_lut_build(const FjbTcLutInput* in, float* table, void
                                    "TC LUT: requirement=finite_surface_reference_white");
             factors = surface_factors(in->surface_rgb, cc, cm);
         }
+        // the compression's node coordinates (their failure is reported after the build's)
+        std::vector<float> coords;
+        const bool compress = in->input_compression != 0, hull = in->hull_available && in->hull_xy;
+        const bool coords_ok = compress && hull && remap_coordinates(in->hull_xy, in->hull_center, coords);
         cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-        // denominators, failure flags and the surface factors: freed before the call returns
-        const size_t bytes = 256 + factors.size() * sizeof(float);
+        // denominators, failure flags, surface factors, the table before the remap and the
+        // remap coordinates: freed before the call returns
+        const size_t built_bytes = coords_ok ? (size_t)kNodes * 4 * sizeof(float) : 0;
+        const size_t bytes = 256 + (factors.size() * sizeof(float) + 255) / 256 * 256 + built_bytes +
+                             coords.size() * sizeof(float);
         void* scratch = nullptr;
         cudaError_t e = cudaMalloc(&scratch, bytes);
         if (e != cudaSuccess) return cuda_status(e, error, "TC LUT scratch");
         float* den = static_cast<float*>(scratch);
         unsigned* flags = reinterpret_cast<unsigned*>(den + 3);
-        float* surface = factors.empty() ? nullptr : reinterpret_cast<float*>(static_cast<char*>(scratch) + 256);
+        char* cursor = static_cast<char*>(scratch) + 256;
+        float* surface = factors.empty() ? nullptr : reinterpret_cast<float*>(cursor);
+        cursor += (factors.size() * sizeof(float) + 255) / 256 * 256;
+        float* built = coords_ok ? reinterpret_cast<float*>(cursor) : nullptr;
+        cursor += built_bytes;
+        float2* tc = coords_ok ? reinterpret_cast<float2*>(cursor) : nullptr;
         e = cudaMemsetAsync(scratch, 0, 16, s);
         // pageable source: the copy completes before cudaMemcpyAsync returns
         if (e == cudaSuccess && surface)
             e = cudaMemcpyAsync(surface, factors.data(), factors.size() * sizeof(float), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && tc)
+            e = cudaMemcpyAsync(tc, coords.data(), coords.size() * sizeof(float), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess && p.arctic) {
             fjb::count_launch();
             tc_neutral_kernel<<<1, 1, 0, s>>>(in->spectra, p, den, flags);
@@ -300,7 +399,13 @@ extern "C" FjStatus fjb_tc_lut_build(const FjbTcLutInput* in, float* table, void
         }
         if (e == cudaSuccess) {
             fjb::count_launch();
-            tc_lut_kernel<<<(kNodes + 127) / 128, 128, 0, s>>>(in->spectra, p, den, surface, table, flags);
+            tc_lut_kernel<<<(kNodes + 127) / 128, 128, 0, s>>>(in->spectra, p, den, surface, built ? built : table,
+                                                               flags);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess && built) {
+            fjb::count_launch();
+            tc_remap_kernel<<<(kNodes + 127) / 128, 128, 0, s>>>(built, tc, table, flags);
             e = cudaGetLastError();
         }
         unsigned f = 0;
@@ -316,6 +421,14 @@ extern "C" FjStatus fjb_tc_lut_build(const FjbTcLutInput* in, float* table, void
             return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "TC LUT: requirement=finite_positive_neutral_response");
         if (f & kIntegratedNonFinite)
             return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "TC LUT: requirement=finite_integrated_samples");
+        if (compress && !hull)
+            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "TC LUT: requirement=input_compression_hull");
+        if (compress && !coords_ok)
+            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "TC LUT: requirement=usable_compressed_coordinates");
+        if (f & kSamplingUnusable)
+            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "TC LUT: requirement=usable_sampling_coordinates");
+        if (f & kRemappedNonFinite)
+            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "TC LUT: requirement=finite_remapped_samples");
         write_error(error, "");
         return ok_status();
     } catch (...) {

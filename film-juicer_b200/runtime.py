@@ -427,7 +427,7 @@ def render_from_density_effects(recipe: "DeviceRecipe", post, seed: int, origin,
 
 
 def tc_lut_build(spectra, sensitivity_rgb, reference_illuminant, white_xyz, method: int = 0,
-                 spectral_blur: float = 0.0, surface=None, stream=None):
+                 spectral_blur: float = 0.0, surface=None, compression: bool = False, hull=None, stream=None):
     """fjb_tc_lut_build: the film TC LUT (192 * 192 * 4 floats on the GPU) from CUDA
     spectra (192 * 192 * 81 floats) and host sensitivity (81 x 3) / illuminant (81)."""
     import numpy as np
@@ -449,6 +449,13 @@ def tc_lut_build(spectra, sensitivity_rgb, reference_illuminant, white_xyz, meth
         surf = np.ascontiguousarray(surface, np.float32).reshape(-1)
         inp.apply_surface = 1
         inp.surface_rgb = surf.ctypes.data_as(C.POINTER(C.c_float))
+    if compression:
+        inp.input_compression = 1
+        if hull is not None:
+            xy = np.ascontiguousarray(hull[1], np.float32).reshape(-1)
+            inp.hull_xy = xy.ctypes.data_as(C.POINTER(C.c_float))
+            inp.hull_center[0], inp.hull_center[1] = float(hull[0][0]), float(hull[0][1])
+            inp.hull_available = 1
     err = abi.ErrorText()
     st = lib.fjb_tc_lut_build(C.byref(inp), C.c_void_p(_ptr(table)), C.c_void_p(_stream_handle(stream)),
                               C.byref(err.buf))

@@ -100,10 +100,11 @@ FjStatus fjb_render_from_density_post(FjbRecipe* recipe, const FjScannerPostEffe
  * irradiance, with the spectral blur when `spectral_blur` > 0 (radius up to 80
  * samples); method 2: Arctic reflectance relit by the reference illuminant and
  * normalised by the neutral response at the projected white; `apply_surface` (Hanatos)
- * multiplies by the surface correction of `surface_rgb` (host, 3 x 15). The
- * input-compression remap is not built here (the call rejects it). The call allocates
- * device memory for its own use (256 B, plus 432 KiB with the surface correction),
- * frees it and synchronises `stream` before returning. */
+ * multiplies by the surface correction of `surface_rgb` (host, 3 x 15);
+ * `input_compression` remaps the table through the input gamut hull (`hull_xy`: host,
+ * 1025 closed-polygon points; `hull_center`). The call allocates device memory for its
+ * own use (256 B, plus 432 KiB with the surface correction and 864 KiB with the
+ * compression), frees it and synchronises `stream` before returning. */
 typedef struct FjbTcLutInput {
     const float* spectra;              /* device, 192*192*81 */
     const float* sensitivity_rgb;      /* host, 81 x 3 */
@@ -114,6 +115,9 @@ typedef struct FjbTcLutInput {
     uint32_t apply_surface;
     uint32_t input_compression;
     const float* surface_rgb;          /* host, 3 x 15, with apply_surface */
+    const float* hull_xy;              /* host, 1025 x 2, with input_compression */
+    float hull_center[2];
+    uint32_t hull_available;
 } FjbTcLutInput;
 FjStatus fjb_tc_lut_build(const FjbTcLutInput* input, float* table, void* stream, FjErrorBuffer* error);
 

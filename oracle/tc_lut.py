@@ -8,7 +8,9 @@ sample_mitchell :501-538, mitchell_weight :139-157, mitchell_coordinate :159-169
 mitchell_reflect_index :171-180, projected_white :124-137, tri2quad :352-356) for the
 Hanatos irradiance method (optionally with spectral blur) and the Arctic reflectance
 method, and the Hanatos surface correction (eval_hanatos_surface :570-593, exp2 from
-the C library as f32::exp2 is); the input-compression remap is not restated. Every
+the C library as f32::exp2 is), and the input-compression remap (gamut.rs:259-373:
+ray_polygon_distance, knee, compress, bilinear, remap_tc_lut; FP64 with the C
+library's hypot and pow). Every
 float32 product and sum is rounded on its own, as the Rust code is (no fused
 multiply-add); reductions run in the reference's order. Raises ValueError with the
 reference's requirement name where it fails.
@@ -26,6 +28,9 @@ _libm.expf.restype = C.c_float
 _libm.expf.argtypes = [C.c_float]
 _libm.exp2f.restype = C.c_float
 _libm.exp2f.argtypes = [C.c_float]
+for _fn, _n in (("hypot", 2), ("pow", 2)):
+    getattr(_libm, _fn).restype = C.c_double
+    getattr(_libm, _fn).argtypes = [C.c_double] * _n
 CELLS = 192 * 192
 
 
@@ -168,9 +173,10 @@ def surface_factors(params: np.ndarray, center) -> np.ndarray:
 
 
 def build_tc_lut(spectra: np.ndarray, sensitivity: np.ndarray, illuminant: np.ndarray, white, method: int,
-                 blur_sigma: np.float32, surface=None) -> np.ndarray:
+                 blur_sigma: np.float32, surface=None, compression: bool = False, hull=None) -> np.ndarray:
     """192 x 192 x 4 (R, G, B, +0) float32 table; method 0 Hanatos, 2 Arctic; `surface`
-    (3 x 15 float32, Hanatos only) applies the surface correction."""
+    (3 x 15 float32, Hanatos only) applies the surface correction; `compression` remaps
+    through the input hull (`hull` = (center, 1025 xy points), None when unavailable)."""
     sens = np.asarray(sensitivity, np.float32).reshape(81, 3)
     ill = np.asarray(illuminant, np.float32)
     if not np.all(np.isfinite(ill) & (ill >= 0.0)):
@@ -211,6 +217,10 @@ def build_tc_lut(spectra: np.ndarray, sensitivity: np.ndarray, illuminant: np.nd
             out[:, c] = (out[:, c] * factors[:, c]).astype(np.float32)
     if not np.all(np.isfinite(out[:, :3])):
         raise ValueError("finite_integrated_samples")
+    if compression:
+        if hull is None:
+            raise ValueError("input_compression_hull")
+        return remap(out.reshape(-1), remap_coordinates(*hull))
     return out.reshape(-1)
 
 
@@ -221,3 +231,73 @@ def digest(table: np.ndarray) -> int:
         h ^= b
         h = (h * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
     return h
+
+
+def remap_coordinates(center, hull_xy) -> np.ndarray:
+    """TC coordinates every node reads after the input compression, (192 * 192, 2) float32."""
+    c0, c1 = float(F(center[0])), float(F(center[1]))
+    poly = np.asarray(hull_xy, np.float32).astype(np.float64)
+    cc = np.arange(192, dtype=np.float32)
+    root = np.sqrt((cc / F(191.0)).astype(np.float32)).astype(np.float32)
+    mm = (np.arange(192, dtype=np.float32) / F(191.0)).astype(np.float32)
+    x = np.repeat((F(1.0) - root).astype(np.float32), 192)
+    y = (mm[None, :] * root[:, None]).astype(np.float32).reshape(-1)
+    dx = x.astype(np.float64) - c0
+    dy = y.astype(np.float64) - c1
+    dist = np.array([_libm.hypot(a, b) for a, b in zip(dx, dy)])
+    near = dist < 1e-9
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ux, uy = dx / dist, dy / dist
+        best = np.full(dist.shape, np.inf)
+        for k in range(len(poly) - 1):
+            ax, ay = poly[k]
+            ex, ey = poly[k + 1, 0] - ax, poly[k + 1, 1] - ay
+            den = ux * ey - uy * ex
+            ox, oy = c0 - ax, c1 - ay
+            d = (-ox * ey + oy * ex) / den
+            pos = (-ox * uy + oy * ux) / den
+            ok = (np.abs(den) > 1e-12) & (d > 1e-9) & (d < best) & (pos >= -1e-9) & (pos <= 1.0 + 1e-9)
+            best = np.where(ok, d, best)
+    out = np.empty((CELLS, 2), np.float32)
+    for n in range(CELLS):
+        if near[n]:
+            cx, cy = x[n], y[n]
+        else:
+            b = best[n]
+            if not np.isfinite(b) or b <= 1e-12:
+                raise ValueError("usable_compressed_coordinates")
+            t = dist[n] / b
+            if t > 0.815:
+                s = 1.0 - 0.815
+                u = (t - 0.815) / s
+                t = 0.815 + s * (u / _libm.pow(1.0 + _libm.pow(u, 1.2), 1.0 / 1.2))
+            cd = t * b
+            rx, ry = c0 + ux[n] * cd, c1 + uy[n] * cd
+            if not (np.isfinite(rx) and np.isfinite(ry)):
+                raise ValueError("usable_compressed_coordinates")
+            cx, cy = F(rx), F(ry)
+        out[n] = tri2quad(F(cx), F(cy))
+    return out
+
+
+def remap(table: np.ndarray, coords: np.ndarray) -> np.ndarray:
+    """Bilinear resampling of the table at the compressed coordinates (float32, unfused)."""
+    t = table.reshape(CELLS, 4)
+    cp = (np.clip(coords[:, 0], F(0.0), F(1.0)) * F(191.0)).astype(np.float32)
+    mp = (np.clip(coords[:, 1], F(0.0), F(1.0)) * F(191.0)).astype(np.float32)
+    if not (np.all(np.isfinite(cp)) and np.all(np.isfinite(mp))):
+        raise ValueError("usable_sampling_coordinates")
+    c0 = np.floor(cp).astype(np.int64)
+    m0 = np.floor(mp).astype(np.int64)
+    c1, m1 = np.minimum(c0 + 1, 191), np.minimum(m0 + 1, 191)
+    cf = (cp - c0.astype(np.float32)).astype(np.float32)
+    mf = (mp - m0.astype(np.float32)).astype(np.float32)
+    out = np.zeros((CELLS, 4), np.float32)
+    for ch in range(3):
+        v = lambda c, m: t[c * 192 + m, ch]
+        r0 = (v(c0, m0) + (cf * (v(c1, m0) - v(c0, m0)).astype(np.float32)).astype(np.float32)).astype(np.float32)
+        r1 = (v(c0, m1) + (cf * (v(c1, m1) - v(c0, m1)).astype(np.float32)).astype(np.float32)).astype(np.float32)
+        out[:, ch] = (r0 + (mf * (r1 - r0).astype(np.float32)).astype(np.float32)).astype(np.float32)
+    if not np.all(np.isfinite(out[:, :3])):
+        raise ValueError("finite_remapped_samples")
+    return out.reshape(-1)

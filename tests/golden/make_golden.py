@@ -208,18 +208,19 @@ def effects_cases():
 def tc_lut_cases():
     """TC LUT characterization (tests/ffi/fixtures/tc_lut/records-0.json, built by
     tests/ffi/tc_lut_test.cpp): the cases whose source is the procedural spectra
-    (word i = 0x3e000123 + (i % 4093) * 173) and that do not need the input
-    compression: inputs as IEEE bit patterns, the expected
+    (word i = 0x3e000123 + (i % 4093) * 173), with the input hull of the compression
+    cases in tc_lut_hull.json: inputs as IEEE bit patterns, the expected
     status and requirement, and the FNV-1a digest of the complete table."""
     with open(os.path.join(REF, "tests", "ffi", "fixtures", "tc_lut", "records-0.json")) as fh:
         doc = json.load(fh)
     keep = []
     for c in doc["leaves"]["cases"]:
         i = c["input"]
-        if i["source"] != "procedural_4093_173" or i["compression"] or i["id"] in (16, 17):
+        if i["source"] != "procedural_4093_173" or i["id"] in (16, 17):
             continue
         row = dict(id=i["id"], built=c["built"], method=i["method"], blur=i["blur"], sensitivity=i["sensitivity"],
                    spd=i["spd"], white=i["white"], surface=i["surface"], surface_params=i["surface_params"],
+                   compression=i["compression"], hull_available=i["hull_available"],
                    requirement=c["diagnostic"].split("requirement=")[-1] if not c["built"] else "")
         if c["built"]:
             row["digest"] = str(c["table"]["native_byte_digest_fnv1a64"])
@@ -227,6 +228,9 @@ def tc_lut_cases():
         keep.append(row)
     with open(os.path.join(HERE, "tc_lut_cases.json"), "w") as fh:
         json.dump(keep, fh, separators=(",", ":"))
+    hull = doc["leaves"]["hull"]
+    with open(os.path.join(HERE, "tc_lut_hull.json"), "w") as fh:
+        json.dump(dict(center=hull["center"], xy=hull["xy"]), fh, separators=(",", ":"))
     print("tc lut cases:", [r["id"] for r in keep])
 
 

@@ -1,7 +1,8 @@
 """The film TC LUT oracle (oracle/tc_lut.py) pinned on the reference's characterization
 (tests/golden/tc_lut_cases.json, from tests/ffi/fixtures/tc_lut/records-0.json): the
 FNV-1a digest of every complete table it builds (Hanatos with and without spectral
-blur or surface correction, Arctic, negative and NaN blur bypasses) and the requirement of every case the
+blur, surface correction or input compression, Arctic, negative and NaN blur
+bypasses) and the requirement of every case the
 reference rejects."""
 import json
 import os
@@ -12,6 +13,8 @@ import pytest
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "tc_lut_cases.json")
 with open(GOLDEN) as fh:
     CASES = json.load(fh)
+with open(os.path.join(os.path.dirname(__file__), "golden", "tc_lut_hull.json")) as fh:
+    _HULL = json.load(fh)
 # cases whose first source word the characterization replaces (tests/ffi/tc_lut_test.cpp:101-105)
 PATCH = {21: np.inf, 22: np.nan}
 
@@ -33,7 +36,10 @@ def inputs(case):
     surface = None
     if case.get("surface"):
         surface = np.array([[f32(v) for v in row] for row in case["surface_params"]], np.float32)
-    return spectra, sens, ill, white, case["method"], f32(case["blur"]), surface
+    hull = None
+    if case.get("compression") and case.get("hull_available"):
+        hull = ([f32(v) for v in _HULL["center"]], np.array([[f32(a), f32(b)] for a, b in _HULL["xy"]], np.float32))
+    return spectra, sens, ill, white, case["method"], f32(case["blur"]), surface, bool(case.get("compression")), hull
 
 
 @pytest.mark.parametrize("case", CASES, ids=[str(c["id"]) for c in CASES])

@@ -16,20 +16,20 @@ def test_device_tc_lut_matches_reference_words(torch_cuda, case):
     from oracle import tc_lut
 
     torch = torch_cuda
-    spectra, sens, ill, white, method, blur, surface = inputs(case)
+    spectra, sens, ill, white, method, blur, surface, compression, hull = inputs(case)
     dev = torch.from_numpy(spectra).cuda()
     if not case["built"]:
         with pytest.raises(runtime.FjError) as e:
-            runtime.tc_lut_build(dev, sens, ill, white, method, float(blur), surface)
+            runtime.tc_lut_build(dev, sens, ill, white, method, float(blur), surface, compression, hull)
         assert str(e.value).rstrip().endswith("requirement=" + case["requirement"])
         return
-    table = runtime.tc_lut_build(dev, sens, ill, white, method, float(blur), surface).cpu().numpy()
+    table = runtime.tc_lut_build(dev, sens, ill, white, method, float(blur), surface, compression, hull).cpu().numpy()
     assert tc_lut.digest(table) == int(case["digest"])
-    want = tc_lut.build_tc_lut(spectra, sens, ill, white, method, blur, surface)
+    want = tc_lut.build_tc_lut(spectra, sens, ill, white, method, blur, surface, compression, hull)
     assert np.array_equal(table.view(np.uint32), want.view(np.uint32))
 
 
-def test_device_tc_lut_rejects_host_only_stages(torch_cuda):
+def test_device_tc_lut_rejects_unknown_methods(torch_cuda):
     import ctypes as C
 
     import film_juicer_b200 as pkg
@@ -42,7 +42,7 @@ def test_device_tc_lut_rejects_host_only_stages(torch_cuda):
     inp.spectra = 16
     inp.sensitivity_rgb = sens.ctypes.data_as(C.POINTER(C.c_float))
     inp.reference_illuminant = ill.ctypes.data_as(C.POINTER(C.c_float))
-    inp.input_compression = 1
+    inp.method = 1
     err = abi.ErrorText()
     st = lib.fjb_tc_lut_build(C.byref(inp), C.c_void_p(16), None, C.byref(err.buf))
-    assert st.category == abi.FJ_STATUS_PREPARATION_FAILURE and "host" in err.text
+    assert st.category == abi.FJ_STATUS_PREPARATION_FAILURE and "method" in err.text
