@@ -28,6 +28,8 @@ _EXPORTS = {
                                                     C.c_int32, C.c_uint32, C.c_void_p, C.c_size_t, C.c_void_p,
                                                     C.POINTER(abi.FjErrorBuffer)]),
     "fjb_glare_seed": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_int32, C.c_int32]),
+    "fjb_gamut_boundary_build": (abi.FjStatus, [C.POINTER(C.c_double), C.c_void_p, C.c_void_p,
+                                                C.POINTER(abi.FjErrorBuffer)]),
     "fjb_tc_lut_build": (abi.FjStatus, [C.POINTER(abi.FjbTcLutInput), C.c_void_p, C.c_void_p,
                                         C.POINTER(abi.FjErrorBuffer)]),
     "fjb_film_defects_scratch_bytes": (C.c_size_t, [C.POINTER(abi.FjFilmEffects), C.c_int32, C.c_int32]),

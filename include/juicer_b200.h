@@ -121,6 +121,15 @@ typedef struct FjbTcLutInput {
 } FjbTcLutInput;
 FjStatus fjb_tc_lut_build(const FjbTcLutInput* input, float* table, void* stream, FjErrorBuffer* error);
 
+/* Output gamut boundary table on the device (reference rust/film-juicer-core/src/gamut.rs:760-829
+ * build_output_boundary, run by the reference's host when a recipe is prepared): the
+ * 64 x 720 maximum-chroma table of the OkLch output gamut compression (`cmax`, device
+ * memory, 46 080 floats, lightness-major) for an output space given by its
+ * OkLab-LMS-to-native-RGB matrix (`lms_to_native`, host, 3 x 3 FP64), word for word the
+ * reference's. The call allocates device memory for its own use (12 KiB), frees it and
+ * synchronises `stream` before returning. */
+FjStatus fjb_gamut_boundary_build(const double* lms_to_native, float* cmax, void* stream, FjErrorBuffer* error);
+
 /* Film and gate defects (reference src/Cuda/Scan/JuicerCudaScanPipeline.cu:2186-2242
  * juicer_cuda_apply_film_defects / juicer_cuda_build_gate_defect_transmittance_focused,
  * scheduled by src/Cuda/JuicerCudaExecutor.cpp:1674-1690, :2263-2279, :1806-1830).

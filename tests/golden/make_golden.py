@@ -234,6 +234,34 @@ def tc_lut_cases():
     print("tc lut cases:", [r["id"] for r in keep])
 
 
+def gamut_cases():
+    """Output gamut boundary tables (tests/ffi/fixtures/output_gamut/records-0.json and
+    tables-0.bin): per output space the LMS-to-native matrix (FP64 bits), the FNV-1a
+    digest of its 64 x 720 cmax table, or the builder's rejection; the 720 hue
+    directions (cos, sin as FP64 bits) and the Lab-to-LMS-root matrix (f32 bits)."""
+    base = os.path.join(REF, "tests", "ffi", "fixtures", "output_gamut")
+    with open(os.path.join(base, "records-0.json")) as fh:
+        doc = json.load(fh)
+    tables = np.fromfile(os.path.join(base, "tables-0.bin"), dtype=np.uint8)
+    rows = []
+    for r in doc["rows"]:
+        if not r["transform_ok"]:
+            continue
+        row = dict(tag=r["tag"], variant=r["variant"], lms_to_native=r["lms_to_native"], ok=r["boundary_ok"],
+                   requirement=r["boundary_diagnostic"].split("requirement=")[-1].split(" ")[0])
+        if r["boundary_ok"]:
+            words = tables[r["table_offset"]:r["table_offset"] + 4 * r["table_count"]]
+            h = 0xCBF29CE484222325
+            for b in words.tobytes():
+                h = ((h ^ b) * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+            row["digest"] = str(h)
+        rows.append(row)
+    out = dict(rows=rows, directions=[[d[1], d[2]] for d in doc["directions"]], lab_to_lms_root=doc["oklab"][3])
+    with open(os.path.join(HERE, "gamut_cases.json"), "w") as fh:
+        json.dump(out, fh, separators=(",", ":"))
+    print("gamut cases:", [(r["tag"], r["variant"], r["ok"]) for r in rows])
+
+
 def recipes():
     sys.path.insert(0, ROOT)
     import __graft_entry__
@@ -256,4 +284,5 @@ if __name__ == "__main__":
     gaussian_cases()
     effects_cases()
     tc_lut_cases()
+    gamut_cases()
     recipes()
