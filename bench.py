@@ -17,7 +17,9 @@ no collective on the data path).
   e2e     Mpix/s through the C-ABI with host buffers: pinned host frame -> H2D, render,
           D2H of the rendered frame, every step, frames pipelined over two copy streams;
   --impl reference  times the CPU restatement of the reference's render path (the
-          reference has no CPU renderer) on all host threads, on crops of the frame.
+          reference has no CPU renderer) on all host threads, on the same 3840x2160
+          frame and descriptors, one whole frame per step (diffusion in the
+          reference's FFT form, FP64).
 """
 from __future__ import annotations
 
@@ -38,7 +40,6 @@ import __graft_entry__  # noqa: E402
 WIDTH, HEIGHT = 3840, 2160
 SEED = 20261203 + 2  # seed of the 4K precision-form configuration
 METRIC = "4K full optical print render throughput (Mpix/s)"
-CROP = (384, 216)  # CPU sample: a crop of the frame with the 4K frame's descriptors
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 
@@ -69,7 +70,7 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a region."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms during a region."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -83,7 +84,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -148,31 +149,40 @@ def dist_setup(n):
     return rank, world, dist
 
 
-def _crop_workload(threads, crop=CROP):
-    """The CPU sample: a crop of the 4K frame rendered by the oracle's chain with the 4K
-    frame's descriptors (same pixel size, diffusion radius, grain)."""
+def workload_config(W, H, next_rows: bool):
+    """The `config` of both arms' JSON lines (identical, so the two lines name one workload)."""
+    return {"workload": f"{W}x{H} full optical print (negative -> print -> scan)"
+                        + (" + highlight reconstruction + scanner post effects + film/gate defects and weave"
+                           if next_rows else ""),
+            "recipe": "kodak_portra_400 -> kodak_portra_endura, Hanatos TC LUT, spatial DIR tail 200 um "
+                      "w 0.03, camera diffusion r=0.5% W, scatter/halation, grain 35 mm, scanner LUT r=17, "
+                      "OkLch gamut, sRGB",
+            "frame_bytes": W * H * 12,
+            "l2_policy": "inputs larger than L2 (99.5 MB frame in and out, ~0.7 GB of stage planes per frame)"}
+
+
+def _cpu_frame(threads, W, H, next_rows):
+    """One step of the CPU restatement: the whole frame (same seed and descriptors as
+    the GPU arm) through the oracle's stage chain, diffusion in the FFT form."""
     __graft_entry__.package()
     from film_juicer_b200 import frame_records, prepare
     from oracle import frame as oframe
 
     recipe = prepare.PreparedRecipe.load(os.path.join(ROOT, "tests", "golden", "recipe_print.npz"))
-    w, h = crop
-    rec = frame_records.FrameRecord(recipe, w, h, descriptor_width=WIDTH)
-    src = prepare.synthetic_frame(WIDTH, HEIGHT, seed=SEED)[:h, :w].copy()
-    return lambda: oframe.render_frame(rec, recipe, src, threads=threads)
+    rec = workload_record(frame_records, recipe, W, H, next_rows)
+    src = prepare.synthetic_frame(W, H, seed=SEED)
+    return lambda: oframe.render_frame(rec, recipe, src, threads=threads, diffusion_form="fft")
 
 
 def run_reference(args):
-    """CPU restatement of the reference render path on all host threads."""
+    """CPU restatement of the reference render path on all host threads, whole frames."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    # crops shrink with the step count so that the whole run stays within minutes
-    scale = min(1.0, (100.0 / max(args.steps, 1)) ** 0.5)
-    crop = (max(96, int(CROP[0] * scale) // 8 * 8), max(54, int(CROP[1] * scale) // 2 * 2))
-    step = _crop_workload(threads, crop)
-    for _ in range(max(args.warmup, 1)):
+    W, H = args.width, args.height
+    step = _cpu_frame(threads, W, H, args.next_rows)
+    for _ in range(args.warmup):
         step()
     times = []
     for _ in range(args.steps):
@@ -180,51 +190,72 @@ def run_reference(args):
         step()
         times.append(time.perf_counter() - t0)
     per_step = statistics.median(times)
-    mpix = crop[0] * crop[1] / per_step / 1e6
-    sample = (f"{crop[0]}x{crop[1]} crop of the 4K frame per step with the 4K descriptors, "
-              f"median of {args.steps}")
+    mpix = W * H / per_step / 1e6
+    sample = f"the whole {W}x{H} frame per step, median of {args.steps} steps"
     line = {
         "impl": "reference", "metric": METRIC, "value": round(mpix, 4), "unit": "Mpix/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "full optical print, 3840x2160 frame, sampled as crops",
-                   "recipe": "kodak_portra_400 -> kodak_portra_endura", "threads": threads},
+        "config": workload_config(W, H, args.next_rows),
         "cpu_baseline": {"value": round(mpix, 4), "unit": "Mpix/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": round(mpix, 4), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "threads": threads,
     }
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(seconds: float):
-    """The oracle's whole-frame chain on crops of the frame, all host threads."""
+def cpu_baseline(seconds: float, W, H, next_rows):
+    """The oracle's whole-frame chain on the same frame, all host threads, whole frames
+    until `seconds` have passed (at least one)."""
     threads = os.cpu_count() or 1
-    step = _crop_workload(threads)
-    step()
+    step = _cpu_frame(threads, W, H, next_rows)
     n, t0 = 0, time.perf_counter()
-    while time.perf_counter() - t0 < seconds:
+    while n == 0 or time.perf_counter() - t0 < seconds:
         step()
         n += 1
     dt = time.perf_counter() - t0
-    return {"value": round(CROP[0] * CROP[1] * n / dt / 1e6, 4), "unit": "Mpix/s", "cores": threads,
-            "kind": "port",
-            "sample": f"{n} x ({CROP[0]}x{CROP[1]} crop of the 4K frame, 4K descriptors) in {dt:.1f} s"}
+    return {"value": round(W * H * n / dt / 1e6, 4), "unit": "Mpix/s", "cores": threads, "kind": "port",
+            "sample": f"{n} whole {W}x{H} frame(s) in {dt:.1f} s"}
 
 
-# Algorithmic work per stage per pixel of the frame (the roofline numerators):
-# compulsory HBM bytes of a fused schedule (4 B per plane read or written), or FLOPs.
-def stage_models(record):
-    h = record.host.h
-    r = h.optics.camera.radius_px
+# Algorithmic work per stage per pixel of the frame (the roofline numerators), from the
+# scope table's measurement row: compulsory HBM bytes of a minimal fused schedule (4 B
+# per plane read or written per pixel), and for the print chain its arithmetic
+# (2*81*3 density->spectral + 81 illuminant + 2*81*3 sensitivity FLOP and 81 EX2).
+PRINT_FLOP_PER_PX = 2 * 81 * 3 + 81 + 2 * 81 * 3
+PRINT_EX2_PER_PX = 81
+
+
+def stage_models():
     return {
         "camera_exposure": ("hbm", 12 + 12),          # RGB in, 3 planes out
-        "camera_diffusion": ("fp32", 3 * (2 * r + 1) ** 2 * 2.0),  # dense (2r+1)^2 PSF per channel
-        "scatter_halation": ("hbm", 24 + 24),         # 3 planes in + out, in place, plus one temp round trip
-        "spatial_dir": ("hbm", 12 + 36),              # carrier in; raw, filtered and log-raw planes out
-        "capture_density": ("hbm", 12 + 24 + 12),     # carrier + spatial DIR planes in, density out
-        "grain": ("hbm", 12 + 12),                    # density in, density out
-        "print_scan_output": ("hbm", 12 + 12),        # density in, RGB out
+        "camera_diffusion": ("hbm", 24),              # 3 planes in, 3 planes out
+        "scatter_halation": ("hbm", 24),              # 3 planes in, 3 planes out
+        "spatial_dir": ("hbm", 12 + 24 + 24),         # source: carrier in, corrections + log raw out; blur
+        "capture_density": ("hbm", 24 + 12),         # filtered corrections + log raw in, density out
+        "grain": ("hbm", 24),                         # density in, density out
+        "print_scan_output": ("spectral", 12 + 12),   # density in, RGB out; FMA / MUFU bound
     }
+
+
+def stage_roofline(name, stage_ms, px, pk, sm_mhz):
+    """Achieved work of one stage against its bound (measured HBM peak; FP32 FMA and
+    MUFU EX2 rates at the sampled SM clock for the spectral chain)."""
+    kind, per_px = stage_models()[name]
+    stage_s = stage_ms * 1e-3
+    if kind == "hbm":
+        achieved = px * per_px / stage_s / 1e9
+        return {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": round(achieved / pk["hbm_gbs"], 4), "bytes_per_px": per_px}
+    clk = (sm_mhz or 1965.0) * 1e6
+    fma_peak = 148 * 128 * 2 * clk / 1e12      # TFLOP/s
+    mufu_peak = 148 * 16 * clk / 1e12          # T ex2/s
+    flops = px * PRINT_FLOP_PER_PX / stage_s / 1e12
+    ex2 = px * PRINT_EX2_PER_PX / stage_s / 1e12
+    return {"bound": "fp32+mufu", "achieved": round(flops, 2), "peak": round(fma_peak, 1), "unit": "TFLOP/s",
+            "frac": round(flops / fma_peak, 4), "ex2_per_s_T": round(ex2, 3), "ex2_peak_T": round(mufu_peak, 3),
+            "ex2_frac": round(ex2 / mufu_peak, 4), "flop_per_px": PRINT_FLOP_PER_PX, "ex2_per_px": PRINT_EX2_PER_PX}
 
 
 def workload_record(frame_records, recipe, W, H, next_rows: bool):
@@ -280,27 +311,42 @@ def run_b200(args):
         return float(t.item())
 
     # ---- device-resident throughput ----
+    # Exactly `steps` frames per timed region, bracketed by a barrier and a device
+    # synchronise. The region is repeated so that the clock sampler (50 ms period)
+    # sees at least ~2 s of rendering; ms_per_step is the median region / steps.
     for _ in range(args.warmup):
         owner.render(record, src, dst, stream=stream)
     stream.synchronize()
+    t_est = time.perf_counter()
+    owner.render(record, src, dst, stream=stream)
+    stream.synchronize()
+    est_ms = (time.perf_counter() - t_est) * 1e3
+    regions = max(1, min(50, int(2000.0 / max(est_ms * args.steps, 1e-3)) + 1))
+    if dist is not None:
+        t = torch.tensor([regions], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        regions = int(t.item())
     lib.fjb_owner_stage_timing(owner.handle, 1, C.byref(err.buf))
-    launches0 = int(lib.fjb_kernel_launches())
-    barrier()
-    torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    region_ms, launches = [], 0
     with ClockSampler(dev) as clocks:
-        start.record(stream)
-        for _ in range(args.steps):
-            owner.render(record, src, dst, stream=stream)
-        end.record(stream)
-        end.synchronize()
-    torch.cuda.synchronize()
-    launches = int(lib.fjb_kernel_launches()) - launches0
+        for _ in range(regions):
+            barrier()
+            torch.cuda.synchronize()
+            launches0 = int(lib.fjb_kernel_launches())
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            for _ in range(args.steps):
+                owner.render(record, src, dst, stream=stream)
+            end.record(stream)
+            end.synchronize()
+            torch.cuda.synchronize()
+            launches = int(lib.fjb_kernel_launches()) - launches0
+            region_ms.append(start.elapsed_time(end))
     times = abi.FjbStageTimes()
     lib.fjb_owner_stage_times(owner.handle, C.byref(times), C.byref(err.buf))
     lib.fjb_owner_stage_timing(owner.handle, 0, C.byref(err.buf))
     barrier()
-    ms = max_over_ranks(start.elapsed_time(end) / args.steps)
+    ms = max_over_ranks(statistics.median(region_ms) / args.steps)
     px = W * H
     value = world * px / (ms * 1e-3) / 1e6
     stages = {}
@@ -362,23 +408,12 @@ def run_b200(args):
     if rank == 0:
         pk, pk_kind = peaks()
         clk = clocks.summary()
-        models = stage_models(record)
-        # roofline of the stage that takes the most device time
-        dominant = max((k for k in stages if k in models), key=lambda k: stages[k])
-        kind, per_px = models[dominant]
-        stage_s = stages[dominant] * 1e-3
-        if kind == "hbm":
-            achieved = px * per_px / stage_s / 1e9
-            roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
-                    "frac": round(achieved / pk["hbm_gbs"], 4), "peak_source": pk_kind}
-        else:
-            # FP32 FMA pipe: 148 SMs x 128 lanes x 2 FLOP per clock at the sampled SM clock
-            sm_mhz = clk.get("sm_mhz") or 1965.0
-            peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
-            achieved = px * per_px / stage_s / 1e12
-            roof = {"bound": "fp32", "achieved": round(achieved, 2), "peak": round(peak, 1), "unit": "TFLOP/s",
-                    "frac": round(achieved / peak, 4),
-                    "peak_source": "nominal FP32 FMA rate at the sampled SM clock (no tensor or HBM bound applies)"}
+        models = stage_models()
+        per_stage = {k: stage_roofline(k, stages[k], px, pk, clk.get("sm_mhz")) for k in stages if k in models}
+        # the roofline object: the stage that takes the most device time
+        dominant = max(per_stage, key=lambda k: stages[k])
+        roof = dict(per_stage[dominant])
+        roof["peak_source"] = pk_kind if roof["bound"] == "hbm" else "FP32 FMA / MUFU rates at the sampled SM clock"
         roof["kernel_stage"] = dominant
         roof["stage_ms"] = stages[dominant]
         traffic = None
@@ -391,18 +426,15 @@ def run_b200(args):
             "metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{W}x{H} full optical print through fj_cuda_render"
-                                   + (" + highlight reconstruction + scanner post effects + film/gate defects and weave"
-                                      if args.next_rows else ""),
-                       "recipe": "kodak_portra_400 -> kodak_portra_endura, Hanatos TC LUT, spatial DIR tail 200 um "
-                                 "w 0.03, camera diffusion r=0.5% W, scatter/halation, grain 35 mm, scanner LUT r=17, "
-                                 "OkLch gamut, sRGB",
-                       "frame_bytes": px * 12, "l2_policy": "inputs larger than L2 (99.5 MB frame in and out, "
-                                                           "~0.7 GB of stage planes per frame)",
-                       "parallelism": f"replicas x{world}"},
+            "config": workload_config(W, H, args.next_rows),
+            "entry": "fj_cuda_render (C-ABI)",
+            "replicas": world,
+            "timed_regions": regions,
+            "region_ms": [round(v, 3) for v in region_ms],
             "stages_ms": stages,
             "roofline": roof,
-            "cpu_baseline": cpu_baseline(args.cpu_seconds) if world == 1 and args.cpu_seconds > 0 else None,
+            "stages_roofline": {k: {"frac": v["frac"], "bound": v["bound"]} for k, v in per_stage.items()},
+            "cpu_baseline": cpu_baseline(args.cpu_seconds, W, H, args.next_rows) if world == 1 and args.cpu_seconds > 0 else None,
             "e2e": {"value": round(e2e, 2), "unit": "Mpix/s", "h2d_bytes_per_step": int(h_src.numel() * 4),
                     "d2h_bytes_per_step": int(h_dst[0].numel() * 4), "steps": e_steps,
                     "schedule": "frames pipelined: H2D of frame i+1 and D2H of frame i-1 on copy streams "

@@ -26,6 +26,7 @@
 
 #include "../../include/juicer_b200.h"
 #include "fjb_diffusion.h"
+#include "fjb_launches.h"
 
 namespace {
 
@@ -116,7 +117,10 @@ FjStatus cuda_failure(cudaError_t e, FjErrorBuffer* error, const char* where) {
                     FJ_API_CUDA_RUNTIME, (int32_t)e};
 }
 
-// Device address of the PSF array on the current device, looked up once per device.
+// Device address of the PSF array on the current device, looked up once per device
+// and kept for the life of the process. A cudaDeviceReset (or any other teardown of
+// the device's primary context) invalidates it, so the library must not be called
+// across one.
 cudaError_t psf_scratch_address(float** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
@@ -187,6 +191,7 @@ extern "C" FjStatus fjb_diffusion_no_alloc(const FjDiffusionComponents* componen
         b.taps = ((2 * radius_px + 1 + 15) / 16) * 16;
         b.rows = rows;
         cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+        fjb::count_launch();
         psf_build_kernel<<<3, kBuildThreads, 0, s>>>(b);
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_failure(e, error, "diffusion PSF build");

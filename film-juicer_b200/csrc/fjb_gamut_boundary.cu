@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdio>
 #include <string>
 #include <vector>
 
@@ -24,7 +25,11 @@ namespace fjb {
 namespace {
 
 constexpr int kLightness = 64, kHues = 720;
-constexpr unsigned kEndpointInside = 1u, kExitNotFinite = 2u;
+// Failures are reported as the reference does: the first failing entry in (lightness,
+// hue) order, and within an entry the endpoint test before the first-exit test. Each
+// failing entry offers the key 2 * index + (0 endpoint inside | 1 exit not finite);
+// the smallest key wins.
+constexpr unsigned kNoFailure = 0xFFFFFFFFu;
 
 // OkLab Lab -> LMS^(1/3) (the reference's f32 literals, gamut.rs:493-503)
 __constant__ float kLabToLmsRoot[9] = {1.0f, 0.3963377774f, 0.2158037573f, 1.0f,          -0.1055613458f,
@@ -135,9 +140,11 @@ __global__ void __launch_bounds__(128) boundary_kernel(const BoundaryParams* __r
         const double e = first_exit(c);
         if (e < fe) fe = e;
     }
-    if (!end_out) atomicOr(flags, kEndpointInside);
     if (!neutral_in) fe = 0.0;
-    if (!(isfinite(fe) && fe >= 0.0 && fe <= 2.0)) atomicOr(flags, kExitNotFinite);
+    if (!end_out)
+        atomicMin(flags, 2u * (unsigned)idx);
+    else if (!(isfinite(fe) && fe >= 0.0 && fe <= 2.0))
+        atomicMin(flags, 2u * (unsigned)idx + 1u);
     cmax[idx] = (float)fe;
 }
 
@@ -165,10 +172,10 @@ extern "C" FjStatus fjb_gamut_boundary_build(const double* lms_to_native, float*
         if (e != cudaSuccess) return cuda_status(e, error, "gamut boundary scratch");
         BoundaryParams* dp = static_cast<BoundaryParams*>(scratch);
         unsigned* flags = reinterpret_cast<unsigned*>(static_cast<char*>(scratch) + sizeof(BoundaryParams));
-        unsigned f = 0;
+        unsigned f = kNoFailure;
         // pageable source: the copy completes before cudaMemcpyAsync returns
         e = cudaMemcpyAsync(dp, &h, sizeof(h), cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = cudaMemsetAsync(flags, 0, sizeof(unsigned), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(flags, 0xFF, sizeof(unsigned), s);
         if (e == cudaSuccess) {
             fjb::count_launch();
             boundary_kernel<<<(kLightness * kHues + 127) / 128, 128, 0, s>>>(dp, cmax, flags);
@@ -178,10 +185,16 @@ extern "C" FjStatus fjb_gamut_boundary_build(const double* lms_to_native, float*
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         cudaFree(scratch);
         if (e != cudaSuccess) return cuda_status(e, error, "gamut boundary build");
-        if (f & kEndpointInside)
-            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "gamut boundary: requirement=c2_outside");
-        if (f & kExitNotFinite)
-            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "gamut boundary: requirement=finite_first_exit");
+        if (f != kNoFailure) {
+            if (f & 1u)
+                return fail_status(FJ_STATUS_PREPARATION_FAILURE, error,
+                                   "gamut boundary: requirement=finite_first_exit");
+            char text[128];
+            const unsigned idx = f >> 1;
+            std::snprintf(text, sizeof text, "gamut boundary: requirement=c2_outside lightness_index=%u hue_index=%u",
+                          idx / kHues, idx % kHues);
+            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, text);
+        }
         write_error(error, "");
         return ok_status();
     } catch (...) {

@@ -279,7 +279,8 @@ FjStatus fjb_diffusion(const FjDiffusionComponents* components, int32_t radius_p
  * by all calls on a device, so calls that may overlap (other streams or host threads)
  * race and must be ordered by the caller. The first call on each device looks up the
  * array's device address with that device current; make it before any stream
- * capture begins. */
+ * capture begins. That address is kept for the life of the process: do not reset the
+ * device (cudaDeviceReset) between calls. */
 FjStatus fjb_diffusion_no_alloc(const FjDiffusionComponents* components, int32_t radius_px, double scatter_fraction,
                                 const float* src_r, const float* src_g, const float* src_b, float* dst_r,
                                 float* dst_g, float* dst_b, ptrdiff_t stride, int32_t width, int32_t height,

@@ -1,9 +1,11 @@
 """Oracle wrappers for the spatial-DIR stage (test infrastructure only).
 
-The recursive components' boundary weights are taken from the library's host
-builder, which is pinned word for word against the reference's boundary fixture
-(tests/test_dir_boundary.py); the oracle then restates the reference's per-component
-blur schedule and the source/develop kernels."""
+The recursive components' boundary weights come from the oracle's own double-double
+restatement of the reference's builder (oracle_dir_boundary in oracle.c, following
+rust/film-juicer-core/src/film/dir/boundary.rs:361-489), pinned word for word on the
+reference's boundary fixture (tests/test_dir_boundary.py). The oracle then restates
+the reference's per-component blur schedule and the source/develop kernels. Nothing
+here loads the product library."""
 from __future__ import annotations
 
 import ctypes as C
@@ -20,26 +22,31 @@ class OracleDirComp(C.Structure):
                 ("v_len", C.c_int), ("v_ts", C.c_int), ("v_term", C.c_double * 9)]
 
 
-def boundary(lib, g, length):
-    abi = _o._abi()
-    cap = 3 * max(length, 1)
-    w = (C.c_double * cap)()
+def boundary(g, length):
+    """(weights [3 x retained], retained, terminal size, terminal [9]) of one axis."""
+    lib = _o.load()
+    fn = lib.oracle_dir_boundary
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(C.c_double), C.c_double, C.c_double, C.c_uint, C.c_int, C.POINTER(C.c_double),
+                   C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    coeff = (C.c_double * 9)(g.feedforward, g.feedback[0], g.feedback[1], g.feedback[2], g.normalization_denominator,
+                             g.feedforward_numerator, g.feedback_numerators[0], g.feedback_numerators[1],
+                             g.feedback_numerators[2])
+    w = (C.c_double * (3 * max(length, 1)))()
     t = (C.c_double * 9)()
-    n, ts = C.c_int32(), C.c_int32()
-    err = abi.ErrorText()
-    st = lib.fjb_dir_boundary_host(C.byref(g), length, w, cap, C.byref(n), C.byref(ts), t, C.byref(err.buf))
-    if st.category != 0:
-        raise RuntimeError(err.text)
+    n, ts = C.c_int(), C.c_int()
+    rc = fn(coeff, g.boundary_truncation_accuracy, g.boundary_certification_tolerance,
+            g.boundary_derivation_version, length, w, C.byref(n), C.byref(ts), t)
+    if rc != 0:
+        raise RuntimeError(f"oracle DIR boundary failed with reason {rc}")
     return np.array(w[: 3 * n.value]), n.value, ts.value, np.array(t[:])
 
 
 def components(spatial_dir, width, height, active_only=True):
     """OracleDirComp array (and the arrays it points into) for the active components
     (all components, in order, with active_only=False)."""
-    import film_juicer_b200 as pkg
     from film_juicer_b200 import descriptors
 
-    lib = pkg.load_library()
     keep = []
     out = []
     for i in range(spatial_dir.component_count):
@@ -62,7 +69,7 @@ def components(spatial_dir, width, height, active_only=True):
             for k in range(3):
                 c.fb[k] = g.feedback[k]
             for axis, length in (("h", width), ("v", height)):
-                w, n, ts, t = boundary(lib, g, length)
+                w, n, ts, t = boundary(g, length)
                 w = np.ascontiguousarray(w)
                 keep.append(w)
                 setattr(c, f"{axis}_init", w.ctypes.data_as(C.POINTER(C.c_double)))

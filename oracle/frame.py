@@ -16,11 +16,14 @@ class _Components:
         self.lambda_px, self.red_weights, self.green_weights, self.blue_weights = lam, w[0], w[1], w[2]
 
 
-def render_frame(frame_record, recipe, src, threads: int = 1, frame_token: int = 0):
+def render_frame(frame_record, recipe, src, threads: int = 1, frame_token: int = 0, diffusion_form: str = "direct"):
     """frame_record: film_juicer_b200.frame_records.FrameRecord; recipe: the
     PreparedRecipe it was built from; src: (H, W, comps) float32. Returns the encoded
     output (H, W, comps) and the error flags. `threads` parallelises the per-pixel
-    stages (the spatial stages use the oracle's OpenMP default)."""
+    stages and the FFT (the line stages use the oracle's OpenMP default).
+    diffusion_form: "direct" (FP64 direct sum, the parity form) or "fft" (the
+    reference's FFT convolution in FP64, same results after float rounding; the CPU
+    baseline's form)."""
     abi = orc._abi()
     host = frame_record.host
     h = host.h
@@ -37,8 +40,12 @@ def render_frame(frame_record, recipe, src, threads: int = 1, frame_token: int =
         d = h.optics.camera
         lam, w = ooptics.diffusion_components(d.family, list(d.group_weights), list(d.group_lambda_um), d.warmth,
                                               d.spatial_scale, d.pixel_size_um)
-        r, g, b = ooptics.diffusion(_Components(lam, w), d.radius_px, d.scatter_fraction,
-                                    [carrier[2], carrier[1], carrier[0]])
+        planes = [carrier[2], carrier[1], carrier[0]]
+        if diffusion_form == "fft":
+            r, g, b = ooptics.diffusion_fft(_Components(lam, w), d.radius_px, d.scatter_fraction, planes,
+                                            workers=threads)
+        else:
+            r, g, b = ooptics.diffusion(_Components(lam, w), d.radius_px, d.scatter_fraction, planes)
         carrier = [b, g, r]
     if flags & abi.FJ_OPTICS_SCATTER_HALATION:
         r, g, b = ooptics.scatter_halation(h.optics.scatter_halation, [carrier[2], carrier[1], carrier[0]])

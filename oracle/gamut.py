@@ -119,7 +119,7 @@ def build(lms_to_native, directions, lab) -> np.ndarray:
                 if e < fe:
                     fe = e
             if not end_out:
-                raise ValueError("c2_outside")
+                raise ValueError(f"c2_outside lightness_index={li} hue_index={hi}")
             if not neutral_in:
                 fe = 0.0
             if not (math.isfinite(fe) and 0.0 <= fe <= CMAX):

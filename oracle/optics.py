@@ -60,6 +60,49 @@ def diffusion(components, radius, fraction, planes_rgb):
     return out
 
 
+def diffusion_psf(components, radius):
+    """The three normalised (2r+1)^2 PSFs (R, G, B) as the oracle stores them (float32)."""
+    lib = _o.load()
+    fn = lib.oracle_diffusion_psf
+    fn.restype = None
+    fn.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, C.c_int, C.c_void_p]
+    lam = (C.c_double * 9)(*components.lambda_px)
+    w = (C.c_double * 27)(*components.red_weights, *components.green_weights, *components.blue_weights)
+    out = []
+    for c in range(3):
+        psf = np.zeros((2 * radius + 1, 2 * radius + 1), np.float32)
+        fn(lam, w, radius, c, C.c_void_p(psf.ctypes.data))
+        out.append(psf)
+    return out
+
+
+def diffusion_fft(components, radius, fraction, planes_rgb, workers: int = 1):
+    """The diffusion stage in the reference's own form (src/Cuda/Diffusion/
+    JuicerCudaDiffusion.cu:510-625: reflect-padded frame, real FFT, product with the
+    PSF spectrum, inverse FFT, crop, mix), in FP64 with scipy's FFT over `workers`
+    threads. Same PSF and padding as diffusion(); the results agree with its direct
+    FP64 sum to FP64 transform rounding (checked in tests/test_diffusion_golden.py).
+    The CPU baseline times this form, the parity tests use the direct sum."""
+    import scipy.fft as sfft
+
+    psfs = diffusion_psf(components, radius)
+    out = []
+    f = np.float32(fraction)
+    for p, psf in zip(planes_rgb, psfs):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        h, w = p.shape
+        padded = np.pad(p.astype(np.float64), radius, mode="reflect") if radius > 0 else p.astype(np.float64)
+        ny, nx = sfft.next_fast_len(padded.shape[0], real=True), sfft.next_fast_len(padded.shape[1], real=True)
+        spec = sfft.rfft2(padded, s=(ny, nx), workers=workers)
+        kern = np.zeros((ny, nx))
+        kern[: 2 * radius + 1, : 2 * radius + 1] = psf.astype(np.float64)
+        spec *= sfft.rfft2(kern, workers=workers)
+        conv = sfft.irfft2(spec, s=(ny, nx), workers=workers)
+        acc = conv[2 * radius: 2 * radius + h, 2 * radius: 2 * radius + w].astype(np.float32)
+        out.append(((np.float32(1.0) - f) * p + f * acc).astype(np.float32))
+    return out
+
+
 def diffusion_components(family, group_weights, group_lambda_um, warmth, spatial_scale, pixel_size_um):
     """Pure-Python restatement of the reference's diffusion component expansion
     (rust/film-juicer-core/src/optics/diffusion_frame.rs:285-421: expand_group,

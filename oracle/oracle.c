@@ -1045,12 +1045,14 @@ static void gauss(const FjHalationGaussian* g, const float* src, long sstride, f
     }
     if (g->kind == FJ_HALATION_FIR_REFLECT) {
         int r = g->radius;
+#pragma omp parallel for schedule(static)
         for (int y = 0; y < H; ++y)
             for (int x = 0; x < W; ++x) {
                 float s = 0.0f;
                 for (int o = -r; o <= r; ++o) s += src[(size_t)reflect_half(y - o, H) * sstride + x] * g->fir_weights[o + r];
                 tmp[(size_t)y * W + x] = s;
             }
+#pragma omp parallel for schedule(static)
         for (int y = 0; y < H; ++y)
             for (int x = 0; x < W; ++x) {
                 float s = 0.0f;
@@ -1059,6 +1061,7 @@ static void gauss(const FjHalationGaussian* g, const float* src, long sstride, f
             }
         return;
     }
+#pragma omp parallel for schedule(static)
     for (int y = 0; y < H; ++y) {
         Yvv s;
         yvv_init(g, src[(size_t)y * sstride], &s);
@@ -1066,6 +1069,7 @@ static void gauss(const FjHalationGaussian* g, const float* src, long sstride, f
         yvv_init(g, tmp[(size_t)y * W + W - 1], &s);
         for (int x = W - 1; x >= 0; --x) tmp[(size_t)y * W + x] = yvv_step(g, tmp[(size_t)y * W + x], &s);
     }
+#pragma omp parallel for schedule(static)
     for (int x = 0; x < W; ++x) {
         Yvv s;
         yvv_init(g, tmp[(size_t)(H - 1) * W + x], &s);
@@ -1128,6 +1132,222 @@ int oracle_scatter_halation(const FjScatterHalation* d, float* r, float* g, floa
     return 0;
 }
 
+/* ---------------- spatial DIR boundaries (rust/film-juicer-core/src/film/dir/boundary.rs:207-503) ----------------
+ *
+ * The reflected Young-van Vliet start weights and end matrix of one axis, in the
+ * reference's double-double arithmetic (a value is the unevaluated sum hi + lo; sums
+ * are Knuth two-sums folded into a fast renormalisation, products carry the exact
+ * residual fma(a, b, -a*b)). The operation order follows boundary.rs step by step so
+ * that the binary64 results are the reference's words. */
+
+typedef struct {
+    double h, l;
+} DDv;
+
+static DDv ddv(double v) {
+    DDv r = {v, 0.0};
+    return r;
+}
+static DDv dd_renorm(double h, double l) { /* boundary.rs:215-221 */
+    DDv r;
+    r.h = h + l;
+    r.l = l - (r.h - h);
+    return r;
+}
+static DDv dd_plus(DDv a, DDv b) { /* :222-227 */
+    double s = a.h + b.h;
+    double v = s - a.h;
+    return dd_renorm(s, (a.h - (s - v)) + (b.h - v) + a.l + b.l);
+}
+static DDv dd_minus(DDv a, DDv b) {
+    DDv nb = {-b.h, -b.l};
+    return dd_plus(a, nb);
+}
+static DDv dd_times(DDv a, DDv b) { /* :237-245 */
+    double p = a.h * b.h;
+    return dd_renorm(p, fma(a.h, b.h, -p) + a.h * b.l + a.l * b.h + a.l * b.l);
+}
+static DDv dd_over(DDv a, DDv d) { /* :246-251 */
+    double q1 = a.h / d.h;
+    DDv rem = dd_minus(a, dd_times(d, ddv(q1)));
+    double q2 = (rem.h + rem.l) / d.h;
+    return dd_plus(ddv(q1), ddv(q2));
+}
+static double dd_val(DDv a) { return a.h + a.l; }
+
+/* o = m v for a 3x3 matrix (row-major) and a 3-vector (:276-284) */
+static void dd_matvec(const DDv* m, const DDv* v, DDv* o) {
+    DDv t[3];
+    for (int r = 0; r < 3; ++r) {
+        t[r] = ddv(0.0);
+        for (int c = 0; c < 3; ++c) t[r] = dd_plus(t[r], dd_times(m[r * 3 + c], v[c]));
+    }
+    memcpy(o, t, sizeof t);
+}
+
+/* o = a b (:264-274) */
+static void dd_matmul(const DDv* a, const DDv* b, DDv* o) {
+    DDv t[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            t[r * 3 + c] = ddv(0.0);
+            for (int k = 0; k < 3; ++k) t[r * 3 + c] = dd_plus(t[r * 3 + c], dd_times(a[r * 3 + k], b[k * 3 + c]));
+        }
+    memcpy(o, t, sizeof t);
+}
+
+static void dd_eye(DDv* m) {
+    for (int i = 0; i < 9; ++i) m[i] = ddv(i % 4 == 0 ? 1.0 : 0.0);
+}
+
+/* Gauss-Jordan inverse of the leading n x n block with partial pivoting on the
+ * rounded magnitudes (:286-320). Returns 0 when a pivot is zero or not finite. */
+static int dd_inverse(DDv* m, int n, DDv* inv) {
+    dd_eye(inv);
+    for (int col = 0; col < n; ++col) {
+        int piv = col;
+        double best = fabs(dd_val(m[col * 3 + col]));
+        for (int r = col + 1; r < n; ++r)
+            if (fabs(dd_val(m[r * 3 + col])) > best) {
+                best = fabs(dd_val(m[r * 3 + col]));
+                piv = r;
+            }
+        if (!(best > 0.0 && isfinite(best))) return 0;
+        if (piv != col)
+            for (int j = 0; j < 3; ++j) {
+                DDv t = m[piv * 3 + j];
+                m[piv * 3 + j] = m[col * 3 + j];
+                m[col * 3 + j] = t;
+                t = inv[piv * 3 + j];
+                inv[piv * 3 + j] = inv[col * 3 + j];
+                inv[col * 3 + j] = t;
+            }
+        DDv s = m[col * 3 + col];
+        for (int j = 0; j < n; ++j) {
+            m[col * 3 + j] = dd_over(m[col * 3 + j], s);
+            inv[col * 3 + j] = dd_over(inv[col * 3 + j], s);
+        }
+        for (int r = 0; r < n; ++r) {
+            if (r == col) continue;
+            DDv f = m[r * 3 + col];
+            for (int j = 0; j < n; ++j) {
+                m[r * 3 + j] = dd_minus(m[r * 3 + j], dd_times(f, m[col * 3 + j]));
+                inv[r * 3 + j] = dd_minus(inv[r * 3 + j], dd_times(f, inv[col * 3 + j]));
+            }
+        }
+    }
+    return 1;
+}
+
+static long long reflect_ll(long long i, long long n) { /* boundary.rs:491-502 */
+    long long p = 2 * n, w = i % p;
+    if (w < 0) w += p;
+    return w < n ? w : p - 1 - w;
+}
+
+/* One axis of the boundary (boundary.rs:361-489). coeff: normalised feedforward,
+ * feedback[3], unnormalised denominator, feedforward numerator, feedback
+ * numerators[3]. weights receives 3 x retained start weights (row-major by state
+ * row; capacity 3 L), terminal the ts x ts end matrix. Returns 0, or the reference's
+ * Reason code: 4 policy, 5 causal singular, 6 non-finite weights, 7 causal
+ * certification, 8 tail escape, 9 terminal singular, 10 terminal certification,
+ * 12 allocation. */
+int oracle_dir_boundary(const double* coeff, double accuracy, double tolerance, unsigned version, int L,
+                        double* weights, int* retained_out, int* ts_out, double* terminal) {
+    if (L <= 0 || !(accuracy > 0.0 && tolerance > 0.0) || version != 1) return 4;
+    const long long period = 2LL * L;
+    DDv A[9];
+    for (int i = 0; i < 9; ++i) A[i] = ddv(0.0);
+    A[0] = ddv(coeff[1]);
+    A[1] = ddv(coeff[2]);
+    A[2] = ddv(coeff[3]);
+    A[3] = ddv(1.0);
+    A[7] = ddv(1.0);
+    /* impulse responses b, A b, A^2 b, ... with b = (ff, 0, 0) */
+    DDv* pw = (DDv*)malloc((size_t)period * 3 * sizeof(DDv));
+    double* full = (double*)malloc((size_t)L * 3 * sizeof(double));
+    if (!pw || !full) {
+        free(pw);
+        free(full);
+        return 12;
+    }
+    pw[0] = ddv(coeff[0]);
+    pw[1] = pw[2] = ddv(0.0);
+    for (long long e = 1; e < period; ++e) dd_matvec(A, pw + (e - 1) * 3, pw + e * 3);
+    /* I - A^(2L), A^(2L) accumulated as A (A (... I)) */
+    DDv P[9], S[9], Si[9];
+    dd_eye(P);
+    for (long long e = 0; e < period; ++e) dd_matmul(A, P, P);
+    dd_eye(S);
+    for (int i = 0; i < 9; ++i) S[i] = dd_minus(S[i], P[i]);
+    int rc = 0;
+    if (!dd_inverse(S, 3, Si)) rc = 5;
+    DDv sums[3] = {{0, 0}, {0, 0}, {0, 0}};
+    for (int s = 0; !rc && s < L; ++s) {
+        DDv rhs[3], st[3];
+        for (int r = 0; r < 3; ++r) rhs[r] = dd_plus(pw[s * 3 + r], pw[(period - 1 - s) * 3 + r]);
+        dd_matvec(Si, rhs, st);
+        for (int r = 0; r < 3; ++r) {
+            double v = dd_val(st[r]);
+            if (!isfinite(v)) {
+                rc = 6;
+                break;
+            }
+            full[(size_t)r * L + s] = v;
+            sums[r] = dd_plus(sums[r], ddv(v));
+        }
+    }
+    for (int r = 0; !rc && r < 3; ++r) {
+        double v = dd_val(sums[r]);
+        if (!isfinite(v) || fabs(v - 1.0) > tolerance) rc = 7;
+    }
+    free(pw);
+    if (rc) {
+        free(full);
+        return rc;
+    }
+    /* truncation: drop trailing samples while the tail mass of every row stays below
+     * the accuracy (never below min(L, 3) samples) */
+    int lo = L < 3 ? L : 3, keep = L;
+    double tail[3] = {0.0, 0.0, 0.0};
+    for (int s = L - 1; s >= lo; --s) {
+        for (int r = 0; r < 3; ++r) tail[r] += fabs(full[(size_t)r * L + s]);
+        if (fmax(fmax(tail[0], tail[1]), tail[2]) >= accuracy) {
+            keep = s + 1;
+            break;
+        }
+        keep = s;
+    }
+    for (int r = 0; r < 3; ++r)
+        for (int s = 0; s < keep; ++s) weights[(size_t)r * keep + s] = full[(size_t)r * L + s];
+    free(full);
+    /* end block: denominator on the diagonal minus the reflected feedback numerators */
+    const int n = L < 3 ? L : 3;
+    DDv T[9], Ti[9];
+    for (int i = 0; i < 9; ++i) T[i] = ddv(0.0);
+    for (int d = 0; d < n; ++d) T[d * 3 + d] = ddv(coeff[4]);
+    for (int row = 0; row < n; ++row)
+        for (int k = 0; k < 3; ++k) {
+            long long col = reflect_ll((long long)(L - n + row) + k + 1, L) - (L - n);
+            if (col < 0 || col >= n) return 8;
+            T[row * 3 + col] = dd_minus(T[row * 3 + col], ddv(coeff[6 + k]));
+        }
+    if (!dd_inverse(T, n, Ti)) return 9;
+    for (int i = 0; i < 9; ++i) terminal[i] = 0.0;
+    for (int row = 0; row < n; ++row) {
+        double sum = 0.0;
+        for (int c = 0; c < n; ++c) {
+            double v = dd_val(dd_times(ddv(coeff[5]), Ti[row * 3 + c]));
+            terminal[row * n + c] = v;
+            sum += v;
+        }
+        if (!isfinite(sum) || fabs(sum - 1.0) > tolerance) return 10;
+    }
+    *retained_out = keep;
+    *ts_out = n;
+    return 0;
+}
+
 /* ---------------- spatial DIR (src/Cuda/Film/JuicerCudaFilmPipeline.cu:124-1060) ---------------- */
 
 typedef struct {
@@ -1172,6 +1392,7 @@ int oracle_dir_source(const FjPreparedHostData* h, const float* src, long src_ro
     }
     const Pack* p = &pk.p;
     unsigned flags = 0;
+#pragma omp parallel for schedule(static) reduction(| : flags)
     for (int y = 0; y < H; ++y)
         for (int x = 0; x < W; ++x) {
             size_t i = (size_t)y * W + x;
@@ -1230,6 +1451,7 @@ int oracle_dir_blur(const OracleDirComp* comps, int n, const float* raw, int W, 
             }
         } else if (c->op == 2) {
             int r = c->radius;
+#pragma omp parallel for schedule(static)
             for (int y = 0; y < H; ++y)
                 for (int x = 0; x < W; ++x) {
                     double s = 0.0;
@@ -1237,6 +1459,7 @@ int oracle_dir_blur(const OracleDirComp* comps, int n, const float* raw, int W, 
                         s += (double)raw[(size_t)y * W + reflect_dir(x + o, W)] * (double)c->taps[o + r];
                     tmp[(size_t)y * W + x] = isfinite(s) ? (float)s : 0.0f;
                 }
+#pragma omp parallel for schedule(static)
             for (int y = 0; y < H; ++y)
                 for (int x = 0; x < W; ++x) {
                     double s = 0.0;
@@ -1248,6 +1471,7 @@ int oracle_dir_blur(const OracleDirComp* comps, int n, const float* raw, int W, 
                     filtered[i] = first ? wv : filtered[i] + wv;
                 }
         } else {
+#pragma omp parallel for schedule(static)
             for (int y = 0; y < H; ++y) {
                 const float* in = raw + (size_t)y * W;
                 float* out = tmp + (size_t)y * W;
@@ -1269,6 +1493,7 @@ int oracle_dir_blur(const OracleDirComp* comps, int n, const float* raw, int W, 
                 for (int hh = 0; hh < ts; ++hh) s[hh] = term[hh];
                 for (int x = W - ts - 1; x >= 0; --x) out[x] = (float)iir(c, (double)out[x], s);
             }
+#pragma omp parallel for schedule(static)
             for (int x = 0; x < W; ++x) {
                 double anchor = (double)tmp[(size_t)(H - 1) * W + x];
                 double s[3] = {anchor, anchor, anchor};
@@ -1319,7 +1544,8 @@ int oracle_develop_spatial(const FjPreparedHostData* h, const float* fy, const f
     }
     const Pack* p = &pk.p;
     unsigned flags = 0;
-    for (size_t i = 0; i < (size_t)W * H; ++i) {
+#pragma omp parallel for schedule(static) reduction(| : flags)
+    for (long i = 0; i < (long)W * H; ++i) {
         float corr[3] = {fy[i], fm[i], fc[i]};
         unsigned fail = 0;
         if (p->dir_mode == FJ_DIR_POSITIVE_RECEIVER_LANGMUIR)
@@ -1371,27 +1597,33 @@ static long reflect_whole(long i, long n) {
     return v < n ? v : period - v;
 }
 
+/* The normalised (2r+1)^2 PSF of channel c (0 R, 1 G, 2 B) as stored floats. */
+void oracle_diffusion_psf(const double* lambda_px, const double* weights, int radius, int c, float* psf) {
+    int d = 2 * radius + 1;
+    const double two_pi = 6.283185307179586476925286766559;
+    double sum = 0.0;
+    for (int iy = 0; iy < d; ++iy)
+        for (int ix = 0; ix < d; ++ix) {
+            int dx = ix - radius, dy = iy - radius;
+            double rho = sqrt((double)dx * dx + (double)dy * dy);
+            double v = 0.0;
+            for (int k = 0; k < 9; ++k) {
+                double l = lambda_px[k];
+                v += weights[c * 9 + k] * exp(-rho / l) / (two_pi * l * l);
+            }
+            psf[(size_t)iy * d + ix] = (float)v;
+            sum += (double)(float)v;
+        }
+    for (size_t i = 0; i < (size_t)d * d; ++i) psf[i] = (float)((double)psf[i] / sum);
+}
+
 int oracle_diffusion(const double* lambda_px, const double* weights /* [3][9] R,G,B */, int radius, double fraction,
                      const float* const* src, float* const* dst, int W, int H) {
     int d = 2 * radius + 1;
     float* psf = (float*)malloc((size_t)d * d * sizeof(float));
     if (!psf) return 1;
-    const double two_pi = 6.283185307179586476925286766559;
     for (int c = 0; c < 3; ++c) {
-        double sum = 0.0;
-        for (int iy = 0; iy < d; ++iy)
-            for (int ix = 0; ix < d; ++ix) {
-                int dx = ix - radius, dy = iy - radius;
-                double rho = sqrt((double)dx * dx + (double)dy * dy);
-                double v = 0.0;
-                for (int k = 0; k < 9; ++k) {
-                    double l = lambda_px[k];
-                    v += weights[c * 9 + k] * exp(-rho / l) / (two_pi * l * l);
-                }
-                psf[(size_t)iy * d + ix] = (float)v;
-                sum += (double)(float)v;
-            }
-        for (size_t i = 0; i < (size_t)d * d; ++i) psf[i] = (float)((double)psf[i] / sum);
+        oracle_diffusion_psf(lambda_px, weights, radius, c, psf);
         const float f = (float)fraction;
 #pragma omp parallel for schedule(static)
         for (int y = 0; y < H; ++y)

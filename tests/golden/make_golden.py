@@ -20,6 +20,9 @@ container, where the reference is mounted read-only).
   (tests/grain/frame-fixtures/linux-release.json): inputs and exact native output
   fields of every successful case, and the gaussian / energy / period primitives.
 * wang_lut.json: the Wang tile index table of Resources/Noise/Wang/tiles.json.
+* abi_layout_reference.json: sizeof of every record of the reference's C-ABI header
+  (native/juicer_cuda_api.h) and offsetof of every field, as the system C compiler
+  lays them out; the drop-in boundary test compares the repository's header with it.
 * recipe_direct.npz / recipe_print.npz: prepared recipes (film_juicer_b200.prepare)
   for kodak_portra_400 direct and kodak_portra_400 -> kodak_portra_endura print,
   built from the reference's Resources/ profiles and spectral tables.
@@ -262,6 +265,42 @@ def gamut_cases():
     print("gamut cases:", [(r["tag"], r["variant"], r["ok"]) for r in rows])
 
 
+def abi_layout():
+    import shutil
+    import subprocess
+    import tempfile
+
+    sys.path.insert(0, ROOT)
+    import __graft_entry__
+
+    __graft_entry__.package()
+    from film_juicer_b200 import abi
+
+    header = os.path.join(REF, "native", "juicer_cuda_api.h")
+    with open(header) as fh:
+        text = fh.read()
+    records = [r for r in abi.ALL_RECORDS if f"}} {r.__name__};" in text]
+    lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{header}"', "int main(void) {"]
+    for rec in records:
+        name = rec.__name__
+        lines.append(f'printf("{name} %zu\\n", sizeof({name}));')
+        for fname, _ in rec._fields_:
+            lines.append(f'printf("{name}.{fname} %zu\\n", offsetof({name}, {fname}));')
+    lines.append("return 0; }")
+    cc = shutil.which("gcc") or shutil.which("cc")
+    with tempfile.TemporaryDirectory() as tmp:
+        src, exe = os.path.join(tmp, "layout.c"), os.path.join(tmp, "layout")
+        with open(src, "w") as fh:
+            fh.write("\n".join(lines))
+        subprocess.run([cc, "-std=c11", src, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
+    layout = {k: int(v) for k, v in (line.rsplit(" ", 1) for line in out if line)}
+    with open(os.path.join(HERE, "abi_layout_reference.json"), "w") as fh:
+        json.dump({"header": "native/juicer_cuda_api.h", "records": [r.__name__ for r in records],
+                   "layout": layout}, fh, indent=0, sort_keys=True)
+    print("abi layout:", len(records), "records")
+
+
 def recipes():
     sys.path.insert(0, ROOT)
     import __graft_entry__
@@ -285,4 +324,5 @@ if __name__ == "__main__":
     effects_cases()
     tc_lut_cases()
     gamut_cases()
+    abi_layout()
     recipes()

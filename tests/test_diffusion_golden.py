@@ -35,3 +35,19 @@ def test_oracle_matches_external_cohort():
         assert np.all(err <= 1.5e-7 * max(1.0, float(np.abs(x).max()))), (name, float(err.max()))
         n += 1
     assert n == 72
+
+
+def test_fft_form_matches_external_cohort_and_direct_form():
+    """The oracle's FFT form (the CPU baseline's diffusion) on the same cohort: same
+    bound against the reference's outputs, and within one float32 rounding of the
+    direct FP64 sum (both convolve the same float PSF in FP64)."""
+    n = 0
+    for name, comps, radius, fraction, x, want in cases():
+        planes = [x[..., c] for c in range(3)]
+        got = np.stack(optics.diffusion_fft(comps, radius, fraction, planes), -1)
+        direct = np.stack(optics.diffusion(comps, radius, fraction, planes), -1)
+        scale = max(1.0, float(np.abs(x).max()))
+        assert np.all(np.abs(got - want) <= 1.5e-7 * scale), (name, float(np.abs(got - want).max()))
+        assert np.all(np.abs(got - direct) <= 1.2e-7 * np.maximum(1.0, np.abs(direct))), name
+        n += 1
+    assert n == 72

@@ -16,13 +16,13 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-6
 
 
-def _call(lib, name, comps, radius, fraction, src, dst):
+def _call(lib, name, comps, radius, fraction, src, dst, stream=0):
     from film_juicer_b200 import abi
 
     err = abi.ErrorText()
     h, w = src[0].shape
     st = getattr(lib, name)(C.byref(comps), radius, fraction, *[C.c_void_p(t.data_ptr()) for t in src],
-                            *[C.c_void_p(t.data_ptr()) for t in dst], src[0].stride(0), w, h, C.c_void_p(0),
+                            *[C.c_void_p(t.data_ptr()) for t in dst], src[0].stride(0), w, h, C.c_void_p(stream),
                             C.byref(err.buf))
     return st, err.text
 
@@ -62,3 +62,62 @@ def test_no_alloc_rejects_radius_beyond_static_scratch(torch_cuda):
     st, text = _call(lib, "fjb_diffusion_no_alloc", comps, 81, 0.5, a, b)
     assert st.category == abi.FJ_STATUS_UNSUPPORTED_INPUT
     assert "static PSF scratch" in text
+
+
+def test_no_alloc_leaves_free_device_memory_unchanged_and_runs_on_a_stream(torch_cuda):
+    """The property the entry exists for: after a first call (which sets up the device
+    address of the static array), further calls change the device's free memory by
+    nothing. One call is enqueued on a non-default stream and only that stream is
+    synchronised before the comparison."""
+    torch = torch_cuda
+    from film_juicer_b200 import abi, descriptors, load_library, runtime
+
+    lib = load_library()
+    comps = runtime.diffusion_components(descriptors.diffusion_record(4.0, 1920))
+    rng = np.random.default_rng(5)
+    h, w = 96, 128
+    planes = [torch.from_numpy(rng.uniform(0.0, 1.5, size=(h, w)).astype(np.float32)).cuda() for _ in range(3)]
+    want = [torch.empty_like(p) for p in planes]
+    got = [torch.full_like(p, float("nan")) for p in planes]
+    st, text = _call(lib, "fjb_diffusion", comps, 12, 0.3, planes, want)
+    assert st.category == abi.FJ_STATUS_SUCCESS, text
+    st, text = _call(lib, "fjb_diffusion_no_alloc", comps, 12, 0.3, planes, got)
+    assert st.category == abi.FJ_STATUS_SUCCESS, text
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(4):
+        st, text = _call(lib, "fjb_diffusion_no_alloc", comps, 12, 0.3, planes, got)
+        assert st.category == abi.FJ_STATUS_SUCCESS, text
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    for g in got:
+        g.fill_(float("nan"))
+    torch.cuda.current_stream().synchronize()
+    st, text = _call(lib, "fjb_diffusion_no_alloc", comps, 12, 0.3, planes, got, stream=side.cuda_stream)
+    assert st.category == abi.FJ_STATUS_SUCCESS, text
+    side.synchronize()
+    scale = max(1.0, float(max(p.abs().max() for p in planes)))
+    for g, r in zip(got, want):
+        assert (g - r).abs().max().item() <= TOL * scale
+
+
+def test_no_alloc_rejects_negative_weights_that_the_allocating_entry_accepts(torch_cuda):
+    """The documented difference between the two entries: fjb_diffusion normalises any
+    PSF whose stored sum is finite and positive, the no-allocation entry needs
+    non-negative weights (its device build cannot check the sum before it is used)."""
+    torch = torch_cuda
+    from film_juicer_b200 import abi, descriptors, load_library, runtime
+
+    lib = load_library()
+    comps = runtime.diffusion_components(descriptors.diffusion_record(4.0, 1920))
+    comps.green_weights[8] = -0.01 * abs(comps.green_weights[0]) - 1e-6
+    a = [torch.rand((16, 24), device="cuda") for _ in range(3)]
+    b = [torch.zeros((16, 24), device="cuda") for _ in range(3)]
+    st, text = _call(lib, "fjb_diffusion", comps, 6, 0.5, a, b)
+    assert st.category == abi.FJ_STATUS_SUCCESS, text
+    st, text = _call(lib, "fjb_diffusion_no_alloc", comps, 6, 0.5, a, b)
+    assert st.category == abi.FJ_STATUS_PREPARATION_FAILURE
+    assert "non-negative" in text
