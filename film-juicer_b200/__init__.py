@@ -67,6 +67,9 @@ _EXPORTS = {
     "fjb_recipe_destroy": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
     "fjb_recipe_set_exposure_scale_device": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
     "fjb_recipe_clear_flags": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_recipe_set_print_form": (abi.FjStatus, [C.c_void_p, C.c_int32, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_print_raw": (abi.FjStatus, [C.c_void_p] + [C.c_void_p] * 6 + [C.c_int32, C.c_int32, C.c_void_p,
+                                                                        C.POINTER(abi.FjErrorBuffer)]),
     "fjb_recipe_read_flags": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32),
                                              C.POINTER(abi.FjErrorBuffer)]),
     "fjb_render_pixels": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.c_ssize_t, C.c_void_p, C.c_ssize_t, C.c_int32,
@@ -115,6 +118,7 @@ _EXPORTS = {
                          [C.c_ssize_t, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, C.c_void_p,
                           C.POINTER(abi.FjErrorBuffer)]),
     "fjb_owner_stage_timing": (abi.FjStatus, [C.c_void_p, C.c_int32, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_owner_set_print_form": (abi.FjStatus, [C.c_void_p, C.c_int32, C.POINTER(abi.FjErrorBuffer)]),
     "fjb_owner_stage_times": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbStageTimes), C.POINTER(abi.FjErrorBuffer)]),
     "fjb_kernel_launches": (C.c_uint64, []),
     "fjb_scanner_lut_build_host": (abi.FjStatus, [C.POINTER(abi.FjbScannerLutInput)] + [C.c_void_p] * 6 +

@@ -274,6 +274,9 @@ FjbScannerLutInput = _s("FjbScannerLutInput", [
     ("has_baseline", u32), ("medium", u32), ("resolution", u32)])
 
 # Every record of the public headers, for the layout test.
+# print forms of the 81-wavelength contraction (fjb_recipe_set_print_form)
+FJB_PRINT_FP32, FJB_PRINT_TENSOR, FJB_PRINT_TENSOR_SPLIT = 0, 1, 2
+
 ALL_RECORDS = [
     FjStatus, FjRenderOutcome, FjErrorBuffer, FjStringView, FjFloatSpan, FjByteSpan, FjCudaContext, FjRect,
     FjExtent, FjImage, FjEffectsGeometry, FjFrame, FjSubmission, FjAbortCallback, FjAutoExposure,

@@ -117,6 +117,15 @@ FjStatus fjb_recipe_set_exposure_scale_device(FjbRecipe* recipe, const float* de
     return ok_status();
 }
 
+FjStatus fjb_recipe_set_print_form(FjbRecipe* recipe, int32_t form, FjErrorBuffer* error) {
+    if (!recipe) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null recipe");
+    if (form != FJB_PRINT_FP32 && form != FJB_PRINT_TENSOR && form != FJB_PRINT_TENSOR_SPLIT)
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "unknown print form");
+    recipe->r.params.print_form = form;
+    write_error(error, "");
+    return ok_status();
+}
+
 FjStatus fjb_recipe_clear_flags(FjbRecipe* recipe, void* stream, FjErrorBuffer* error) {
     if (!recipe) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null recipe");
     cudaError_t e = cudaMemsetAsync(recipe->r.flags, 0, sizeof(unsigned), as_stream(stream));
@@ -248,6 +257,27 @@ FjStatus fjb_render_from_density(FjbRecipe* recipe, const float* density_c, cons
     p.scan_density_m = density_m;
     p.scan_density_y = density_y;
     return launch_stage(recipe, p, fjb::PixelStage::DensityToOutput, stream, error);
+}
+
+FjStatus fjb_print_raw(FjbRecipe* recipe, const float* density_c, const float* density_m, const float* density_y,
+                       float* raw_c, float* raw_m, float* raw_y, int32_t width, int32_t height, void* stream,
+                       FjErrorBuffer* error) {
+    if (!recipe || !density_c || !density_m || !density_y || !raw_c || !raw_m || !raw_y)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    if (recipe->r.params.route != fjb::kRoutePrint)
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "the recipe has no print stage");
+    if (width < 0 || height < 0) return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "unsupported image geometry");
+    fjb::PixelParams p = recipe->r.params;
+    p.width = width;
+    p.height = height;
+    p.scan_density_c = density_c;
+    p.scan_density_m = density_m;
+    p.scan_density_y = density_y;
+    p.lin_r = raw_c;
+    p.lin_g = raw_m;
+    p.lin_b = raw_y;
+    p.film_dust = nullptr;
+    return launch_stage(recipe, p, fjb::PixelStage::DensityToPrintRaw, stream, error);
 }
 
 FjStatus fjb_auto_exposure(FjbRecipe* recipe, const float* src, ptrdiff_t src_row_bytes, uint32_t components,

@@ -23,9 +23,15 @@ enum class PixelStage : int {
     CarrierToDirSource = 6, // carrier planes -> spatial-DIR raw corrections + log exposure
     DensityToLinearRgb = 7, // density planes -> linear output-RGB planes (+ glare), before encoding
     LinearRgbToOutput = 8,  // linear output-RGB planes -> encoded output
+    DensityToPrintRaw = 9,  // density planes -> the print's spectral integral (C, M, Y) into lin_r/g/b
 };
 
 cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStream_t stream);
+
+// The print stages from density planes (DensityToOutput, DensityToLinearRgb,
+// DensityToPrintRaw) with the 81-wavelength contraction on the tensor cores
+// (p.print_form kPrintTensor / kPrintTensorSplit, print route).
+cudaError_t launch_print_tensor(const PixelParams& p, PixelStage stage, cudaStream_t stream);
 
 // Camera linear exposure to planar B, G, R carrier planes (reference
 // src/Cuda/Film/JuicerCudaFilmPipeline.cu:3103 camera_film_linear_exposure_kernel).

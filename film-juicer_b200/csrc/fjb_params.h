@@ -20,6 +20,12 @@ constexpr int kGamutHue = 720;         // output gamut boundary columns
 constexpr int kMaxCurveSamples = 1024; // upper bound for staged curves
 
 enum Route : int { kRouteDirect = 0, kRoutePrint = 1 };
+// The print exposure's 81-wavelength contraction: FP32 FMAs (the parity form) or BF16
+// tensor-core tiles with FP32 accumulation (tcgen05), densities and coefficients as
+// hi + lo BF16 pairs, transmittances as one BF16 (kPrintTensor) or a hi + lo pair
+// (kPrintTensorSplit).
+enum PrintForm : int { kPrintFp32 = 0, kPrintTensor = 1, kPrintTensorSplit = 2 };
+constexpr unsigned kErrTensorWait = 1u << 16;
 enum RawMethod : int { kHanatos = 0, kMallett = 1, kArctic = 2 };
 enum DirModeDev : int { kDirInactive = 0, kDirNegativeDonor = 1, kDirPositiveReceiver = 2 };
 
@@ -56,6 +62,7 @@ struct PixelParams {
     int height;
     int components; // 3 or 4, same for source and destination
     int route;      // Route
+    int print_form; // PrintForm: arithmetic of the 81-wavelength print contraction
 
     // Optional carrier input: planar linear exposure (B, G, R) produced by the
     // camera optics stages. When set, exposure reconstruction is skipped.
@@ -175,7 +182,8 @@ struct PixelParams {
     // ---- staged curves + error word ----
     const float* curve_blob;
     int curve_blob_floats;
-    unsigned int* error_flags; // bit 0 scan failure, bit 8 DIR failure, bits 9..11 DIR channels
+    unsigned int* error_flags; // bit 0 scan failure, bit 8 DIR failure, bits 9..11 DIR channels,
+                               // bit 16 a tensor-core wait gave up (print stage, tensor-core form)
 
     PrintSpectral spectral;
 };

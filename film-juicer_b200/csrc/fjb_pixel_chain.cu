@@ -21,7 +21,7 @@
 namespace fjb {
 
 enum InputKind : int { kInSource = 0, kInCarrier = 1, kInDensity = 2 };
-enum OutputKind : int { kOutEncoded = 0, kOutDensity = 1, kOutDirSource = 2, kOutLinearRgb = 3 };
+enum OutputKind : int { kOutEncoded = 0, kOutDensity = 1, kOutDirSource = 2, kOutLinearRgb = 3, kOutPrintRaw = 4 };
 
 // Spatial-DIR source (src/Cuda/Film/JuicerCudaFilmPipeline.cu:124-214): raw log
 // exposure, pre-DIR layer densities and the donor corrections they release.
@@ -131,6 +131,14 @@ __global__ void __launch_bounds__(kPixelThreads) pixel_chain_kernel(const __grid
             continue;
         }
 
+        if constexpr (Out == kOutPrintRaw) {
+            float raw[3];
+            print_spectral(p.spectral, d, raw);
+            p.lin_r[idx] = raw[0];
+            p.lin_g[idx] = raw[1];
+            p.lin_b[idx] = raw[2];
+            continue;
+        }
         if constexpr (Print) {
             print_develop(p, blob, d, p.film_dust ? p.film_dust[idx] : 1.0f);
         }
@@ -302,6 +310,10 @@ cudaError_t launch_camera_exposure(const PixelParams& p, float* b, float* g, flo
 cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStream_t stream) {
     const long long total = (long long)p.width * (long long)p.height;
     if (total <= 0) return cudaSuccess;
+    if (p.route == kRoutePrint && p.print_form != kPrintFp32 &&
+        (stage == PixelStage::DensityToOutput || stage == PixelStage::DensityToLinearRgb ||
+         stage == PixelStage::DensityToPrintRaw))
+        return launch_print_tensor(p, stage, stream);
     if ((p.curve_blob_floats & 3) != 0) return cudaErrorInvalidValue;
     const size_t smem = (size_t)p.curve_blob_floats * sizeof(float);
     const int grid = persistent_grid(total);
@@ -338,6 +350,8 @@ cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStrea
         case PixelStage::DensityToOutput:
             return print ? launch_variant<kInDensity, kOutEncoded, true, false>(p, grid, smem, stream)
                          : launch_variant<kInDensity, kOutEncoded, false, false>(p, grid, smem, stream);
+        case PixelStage::DensityToPrintRaw:
+            return launch_variant<kInDensity, kOutPrintRaw, true, false>(p, grid, smem, stream);
     }
     return cudaErrorInvalidValue;
 }

@@ -540,11 +540,12 @@ __device__ __forceinline__ void print_spectral(const PrintSpectral& s, const flo
     }
 }
 
-// `dust`: film dust transmittance of the pixel (src/Cuda/JuicerCudaDeviceHelpers.cuh:1062-1066).
-__device__ __forceinline__ void print_develop(const PixelParams& p, const float* __restrict__ blob, float d[3],
-                                              float dust = 1.0f) {
-    float raw[3];
-    print_spectral(p.spectral, d, raw);
+// Print exposure from the spectral integral `raw` (C, M, Y) to print density in `d`:
+// dust, mid-grey normaliser, preflash, print exposure, route correction, log10 and
+// the print curves (src/Cuda/JuicerCudaDeviceHelpers.cuh:935-1071). `dust`: film
+// dust transmittance of the pixel (:1062-1066).
+__device__ __forceinline__ void print_finish(const PixelParams& p, const float* __restrict__ blob, float raw[3],
+                                             float d[3], float dust) {
     if (dust != 1.0f)
         for (int c = 0; c < 3; ++c) raw[c] *= dust;
     const float k = p.print_midgray;
@@ -559,6 +560,13 @@ __device__ __forceinline__ void print_develop(const PixelParams& p, const float*
         const float lp = log10f(raw[c] + 1e-10f);
         d[c] = curve_sample(blob, p.print_curve[c], lp, 1.0f);
     }
+}
+
+__device__ __forceinline__ void print_develop(const PixelParams& p, const float* __restrict__ blob, float d[3],
+                                              float dust = 1.0f) {
+    float raw[3];
+    print_spectral(p.spectral, d, raw);
+    print_finish(p, blob, raw, d, dust);
 }
 
 // ---------------------------------------------------------------------------

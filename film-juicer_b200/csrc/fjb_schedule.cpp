@@ -54,6 +54,7 @@ struct FjCuda {
     float* post_taps = nullptr;              // scanner post-effect Gaussian taps of the last descriptor
     size_t post_taps_bytes = 0;
     uint64_t post_key = 0;
+    int32_t print_form = 0;                  // FJB_PRINT_* applied to every recipe rendered
     // optional per-stage device timing (CUDA events on the render stream)
     bool timing = false;
     bool timing_events = false;
@@ -640,6 +641,7 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
             else
                 transient = std::move(fresh);
         }
+        recipe->r.params.print_form = cuda->print_form;
         // frame-scoped recipe state is cleared on every exit path
         struct FrameState {
             FjbRecipe* r;
@@ -747,6 +749,11 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
                 return out;
             }
         }
+        if (flags & fjb::kErrTensorWait) {
+            out.status = fjb::fail_status(FJ_STATUS_CUDA_FAILURE, error,
+                                          "print stage: a tensor-core completion wait ran out of time");
+            return out;
+        }
         if (flags & (1u << 8)) out.flags |= FJ_RENDER_DEFERRED_DIR_ERROR;
         out.status = fjb::ok_status();
         fjb::write_error(error, (flags & 1u) ? "scanner stage reported non-finite pixels" : "");
@@ -773,6 +780,17 @@ FjStatus fj_cuda_shutdown(FjCuda* cuda, FjErrorBuffer* error) {
         release_all(cuda);
         cuda->closed = true;
     }
+    fjb::write_error(error, "");
+    return fjb::ok_status();
+}
+
+FjStatus fjb_owner_set_print_form(FjCuda* cuda, int32_t form, FjErrorBuffer* error) {
+    if (!cuda) return fjb::fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null owner");
+    if (form != FJB_PRINT_FP32 && form != FJB_PRINT_TENSOR && form != FJB_PRINT_TENSOR_SPLIT)
+        return fjb::fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "unknown print form");
+    std::lock_guard<std::mutex> lock(cuda->gate);
+    if (cuda->closed) return fjb::fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "owner is shut down");
+    cuda->print_form = form;
     fjb::write_error(error, "");
     return fjb::ok_status();
 }

@@ -65,6 +65,21 @@ class DeviceRecipe:
         except Exception:
             pass
 
+    def set_print_form(self, form: int):
+        """abi.FJB_PRINT_FP32 | FJB_PRINT_TENSOR | FJB_PRINT_TENSOR_SPLIT."""
+        err = abi.ErrorText()
+        _check("fjb_recipe_set_print_form", self.lib.fjb_recipe_set_print_form(self.handle, form, C.byref(err.buf)),
+               err)
+
+    def print_raw(self, density, raw, stream=None):
+        """The print's spectral integral (C, M, Y planes) of density planes (C, M, Y)."""
+        c, m, y = density
+        h, w = c.shape
+        err = abi.ErrorText()
+        st = self.lib.fjb_print_raw(self.handle, *[C.c_void_p(_ptr(t)) for t in (c, m, y, *raw)], w, h,
+                                    C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+        _check("fjb_print_raw", st, err)
+
     def set_exposure_scale_device(self, tensor):
         err = abi.ErrorText()
         st = self.lib.fjb_recipe_set_exposure_scale_device(self.handle, C.c_void_p(_ptr(tensor) if tensor is not None
@@ -316,6 +331,10 @@ class Owner:
 
     def __exit__(self, *exc):
         self.close()
+
+    def set_print_form(self, form: int):
+        err = abi.ErrorText()
+        _check("fjb_owner_set_print_form", self.lib.fjb_owner_set_print_form(self.handle, form, C.byref(err.buf)), err)
 
     def render(self, prepared, src, dst, window=None, stream=None, abort=None, frame_token: int = 0):
         """src/dst: (H, W, comps) float32 CUDA tensors covering the full frame; returns

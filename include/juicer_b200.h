@@ -35,8 +35,30 @@ FjStatus fjb_recipe_destroy(FjbRecipe* recipe, FjErrorBuffer* error);
 /* Device scalar read by the exposure step as the auto-exposure scale (NULL = 1). */
 FjStatus fjb_recipe_set_exposure_scale_device(FjbRecipe* recipe, const float* device_scale, FjErrorBuffer* error);
 
+/* Arithmetic of the print exposure's 81-wavelength contraction for this recipe's
+ * print stages from density planes (fjb_render_from_density*, fjb_print_raw and the
+ * staged schedule of fj_cuda_render): FJB_PRINT_FP32 (default; FP32 FMAs, the
+ * reference's arithmetic), FJB_PRINT_TENSOR (tcgen05 BF16 tensor-core tiles with FP32
+ * accumulation: densities and spectra as hi + lo BF16 pairs, transmittances as one
+ * BF16) or FJB_PRINT_TENSOR_SPLIT (transmittances as hi + lo pairs too). No
+ * counterpart in the reference, which has the FP32 form only
+ * (src/Cuda/JuicerCudaDeviceHelpers.cuh:866-935). */
+#define FJB_PRINT_FP32 0
+#define FJB_PRINT_TENSOR 1
+#define FJB_PRINT_TENSOR_SPLIT 2
+FjStatus fjb_recipe_set_print_form(FjbRecipe* recipe, int32_t form, FjErrorBuffer* error);
+
+/* The print exposure's spectral integral raw_c = sum_l 10^-D(l) I(l) S_c(l) of
+ * density planes C, M, Y into planes raw C, M, Y (before dust, normaliser, preflash
+ * and exposure), in the recipe's print form: the per-stage precision check of the
+ * tensor-core form (reference print_spectral_integrate_device,
+ * src/Cuda/JuicerCudaDeviceHelpers.cuh:866). Print route only. */
+FjStatus fjb_print_raw(FjbRecipe* recipe, const float* density_c, const float* density_m, const float* density_y,
+                       float* raw_c, float* raw_m, float* raw_y, int32_t width, int32_t height, void* stream,
+                       FjErrorBuffer* error);
+
 /* Device error word (bit 0 scan failure, bit 8 DIR failure, bits 9..11 DIR
- * channels B,G,R). Cleared by fjb_recipe_clear_flags, read by fjb_recipe_read_flags
+ * channels B,G,R, bit 16 a tensor-core wait of the print stage gave up). Cleared by fjb_recipe_clear_flags, read by fjb_recipe_read_flags
  * (which synchronises `stream`). */
 FjStatus fjb_recipe_clear_flags(FjbRecipe* recipe, void* stream, FjErrorBuffer* error);
 FjStatus fjb_recipe_read_flags(FjbRecipe* recipe, void* stream, uint32_t* out_flags, FjErrorBuffer* error);
@@ -328,6 +350,9 @@ typedef struct FjbStageTimes {
     uint64_t frames[FJB_STAGE_COUNT];
 } FjbStageTimes;
 /* Turns stage timing on (enable != 0) or off and resets the totals. */
+/* The print form (FJB_PRINT_*) of every recipe this owner renders, from the next
+ * fj_cuda_render on. No counterpart in the reference. */
+FjStatus fjb_owner_set_print_form(FjCuda* cuda, int32_t form, FjErrorBuffer* error);
 FjStatus fjb_owner_stage_timing(FjCuda* cuda, int32_t enable, FjErrorBuffer* error);
 /* Totals since the last fjb_owner_stage_timing call. */
 FjStatus fjb_owner_stage_times(FjCuda* cuda, FjbStageTimes* out, FjErrorBuffer* error);
