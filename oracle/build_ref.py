@@ -17,7 +17,8 @@ REF = os.environ.get("FJ_REFERENCE_ROOT", "/root/reference")
 OUT = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT, "libjuicer_ref.so")
 TUS = ["src/Cuda/Scan/JuicerCudaScanPipeline.cu", "src/Cuda/Film/JuicerCudaFilmPipeline.cu",
-       "src/Cuda/Film/JuicerCudaScatterHalation.cu", "src/Cuda/Film/JuicerCudaHighlightBoost.cu"]
+       "src/Cuda/Film/JuicerCudaScatterHalation.cu", "src/Cuda/Film/JuicerCudaHighlightBoost.cu",
+       "src/Cuda/JuicerCudaAutoExposure.cu"]
 
 
 def main() -> int:

@@ -244,6 +244,32 @@ def auto_exposure(record, meter, src):
     return float(v) if ok.value else None
 
 
+def reference_auto_exposure(torch, record, meter, src):
+    """Exposure scale metered by the reference's own CUDA launchers
+    (src/Cuda/JuicerCudaAutoExposure.cu:667, :864) on `src` (H, W, comps), or None when
+    the harness is not built."""
+    import numpy as np
+
+    lib = load_reference()
+    if lib is None or not hasattr(lib, "ref_auto_exposure"):
+        return None
+    abi = _abi()
+    fn = lib.ref_auto_exposure
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(abi.FjPreparedHostData), C.POINTER(C.c_void_p), C.POINTER(abi.FjAutoExposure),
+                   C.c_void_p, C.c_long, C.c_int, C.POINTER(C.c_float)]
+    src = np.ascontiguousarray(src, dtype=np.float32)
+    h, w, comps = src.shape
+    lut = scanner_lut_for(record)
+    ptrs = (C.c_void_p * 6)(*[o.ctypes.data for o in lut])
+    s = torch.from_numpy(src).cuda()
+    out = C.c_float()
+    rc = fn(record.pointer(), ptrs, C.byref(meter), C.c_void_p(s.data_ptr()), w * comps * 4, comps, C.byref(out))
+    if rc != 0:
+        raise RuntimeError(f"reference auto exposure returned {rc}")
+    return float(out.value)
+
+
 def glare_seed(recipe_hash: int, frame_token: int, x1: int, y1: int) -> int:
     """FNV-1a 64 over the little-endian 8-byte words {recipe hash, frame token, x1, y1}
     (src/Cuda/JuicerCudaExecutor.cpp:2416, src/Hash.h:50)."""

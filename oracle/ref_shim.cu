@@ -878,3 +878,79 @@ extern "C" int ref_defects_timed(const FjFilmEffects* fx, int which, int width, 
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return (int)e;
 }
+
+// ---------------------------------------------------------------------------
+// Auto-exposure metering with the reference's launchers
+// (src/Cuda/JuicerCudaAutoExposure.cu:667 juicer_cuda_auto_exposure_meter_to_device,
+// :864 juicer_cuda_auto_exposure_build_center_weight_tables), driven as
+// src/Cuda/JuicerCudaExecutor.cpp:1018-1070 meter_camera_exposure does: the film raw
+// and reconstruction payloads of the recipe, the preview descriptor of the record,
+// weight tables for centre-weighted metering. `src` is the device address of the
+// source image's bounds origin. Writes the float scale to *scale_out. Synchronous.
+// Returns 0, or the launcher's non-zero code (+100), or a cudaError_t (+1000).
+// ---------------------------------------------------------------------------
+#include "Cuda/JuicerCudaResources.h"
+
+extern "C" int ref_auto_exposure(const FjPreparedHostData* h, const float* const* lut, const FjAutoExposure* m,
+                                 const float* src, long src_row_bytes, int comps, float* scale_out) {
+    Arena a;
+    unsigned* d_flags = nullptr;
+    if (cudaMalloc(&d_flags, sizeof(unsigned)) != cudaSuccess) return 1002;
+    a.ptrs.push_back(d_flags);
+    JuicerCuda::PipelineRunParams p;
+    if (!pack(*h, lut, a, p, d_flags)) return 1;
+    JuicerCuda::AutoExposurePreviewDescriptor d{};
+    d.sourceX1 = m->source_bounds.x1;
+    d.sourceY1 = m->source_bounds.y1;
+    d.sourceX2 = m->source_bounds.x2;
+    d.sourceY2 = m->source_bounds.y2;
+    d.meterX1 = m->meter_bounds.x1;
+    d.meterY1 = m->meter_bounds.y1;
+    d.meterX2 = m->meter_bounds.x2;
+    d.meterY2 = m->meter_bounds.y2;
+    d.previewWidth = m->preview_width;
+    d.previewHeight = m->preview_height;
+    d.method = static_cast<Spektrafilm::AutoExposureMethod>(m->method);
+    d.hash = m->hash;
+    JuicerCuda::AutoExposureSourceFormat fmt{};
+    fmt.componentCount = comps;
+    fmt.filmRaw = p.filmRaw;
+    fmt.reconstruction = p.filmExpose.reconstruction;
+    const int gx = (d.previewWidth + 15) / 16, gy = (d.previewHeight + 15) / 16;
+    const int blocks = gx > 0 && gy > 0 ? gx * gy : 1;
+    JuicerCudaAutoExposureScratch scratch{};
+    void* mem[6] = {};
+    const size_t sizes[6] = {sizeof(JuicerCudaAutoExposurePartial) * (size_t)blocks,
+                             sizeof(JuicerCudaAutoExposurePartial) * (size_t)blocks, sizeof(unsigned),
+                             sizeof(unsigned) * 2048, sizeof(float) * (size_t)(d.previewWidth > 0 ? d.previewWidth : 1),
+                             sizeof(float) * (size_t)(d.previewHeight > 0 ? d.previewHeight : 1)};
+    for (int i = 0; i < 6; ++i) {
+        if (cudaMalloc(&mem[i], sizes[i]) != cudaSuccess) return 1002;
+        a.ptrs.push_back(mem[i]);
+    }
+    scratch.partialsA = static_cast<JuicerCudaAutoExposurePartial*>(mem[0]);
+    scratch.partialsB = static_cast<JuicerCudaAutoExposurePartial*>(mem[1]);
+    scratch.partialCapacity = blocks;
+    scratch.maxYBits = static_cast<unsigned*>(mem[2]);
+    scratch.histogram = static_cast<unsigned*>(mem[3]);
+    scratch.weightsX = static_cast<float*>(mem[4]);
+    scratch.weightsY = static_cast<float*>(mem[5]);
+    float* d_scale = nullptr;
+    if (cudaMalloc(&d_scale, sizeof(float)) != cudaSuccess) return 1002;
+    a.ptrs.push_back(d_scale);
+    JuicerCudaAutoExposureDeviceState state{};
+    state.exposureScale = d_scale;
+    const char* why = nullptr;
+    if (m->method == FJ_METER_CENTER_WEIGHTED && d.previewWidth > 0 && d.previewHeight > 0) {
+        const int rc = juicer_cuda_auto_exposure_build_center_weight_tables(d.previewWidth, d.previewHeight,
+                                                                            scratch.weightsX, scratch.weightsY,
+                                                                            nullptr, &why);
+        if (rc != 0) return 100 + rc;
+    }
+    const int rc = juicer_cuda_auto_exposure_meter_to_device(src, (size_t)src_row_bytes, d, fmt, scratch, state,
+                                                             nullptr, &why);
+    if (rc != 0) return 100 + rc;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(scale_out, d_scale, sizeof(float), cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? 0 : 1000 + (int)e;
+}

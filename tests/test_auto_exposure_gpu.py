@@ -89,3 +89,42 @@ def test_metered_scale_feeds_the_render(torch_cuda, direct, prepare, oracle):
     dr.set_exposure_scale_device(None)
     ref, _ = oracle.render(rec, src, auto_scale=float(scale.item()))
     assert np.all(np.abs(out.cpu().numpy() - ref) <= 2e-4 + 3e-4 * np.abs(ref))
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("shape", [(640, 360), (333, 517), (1920, 1080), (2, 3)])
+def test_meter_scale_matches_reference_cuda(torch_cuda, direct, prepare, oracle, method, shape):
+    """The reference's own metering launchers (compiled from its sources into the
+    harness) on the same frame and record: the float scale agrees to 1 ulp (both sum
+    FP64 partials, in different orders)."""
+    torch = torch_cuda
+    from film_juicer_b200 import runtime
+
+    rec, dr = direct
+    w, h = shape
+    src = prepare.synthetic_frame(w, h, seed=7 + method)
+    meter = runtime.meter_record(w, h, method=method)
+    ref = oracle.reference_auto_exposure(torch, rec, meter, src)
+    if ref is None:
+        pytest.skip("reference CUDA harness not built")
+    scale = torch.zeros(1, device="cuda")
+    runtime.auto_exposure(dr, torch.from_numpy(src).cuda(), meter, scale)
+    got = float(scale.item())
+    ulp = abs(np.array([got], np.float32).view(np.int32)[0] - np.array([ref], np.float32).view(np.int32)[0])
+    assert ulp <= 1, (got, ref)
+
+
+def test_windowed_meter_matches_reference_cuda(torch_cuda, direct, prepare, oracle):
+    torch = torch_cuda
+    from film_juicer_b200 import runtime
+
+    rec, dr = direct
+    src = prepare.synthetic_frame(1024, 768, seed=5)
+    meter = runtime.meter_record(1024, 768, meter=(100, 50, 900, 700), preview=(200, 162))
+    ref = oracle.reference_auto_exposure(torch, rec, meter, src)
+    if ref is None:
+        pytest.skip("reference CUDA harness not built")
+    scale = torch.zeros(1, device="cuda")
+    runtime.auto_exposure(dr, torch.from_numpy(src).cuda(), meter, scale)
+    got = float(scale.item())
+    assert abs(np.array([got], np.float32).view(np.int32)[0] - np.array([ref], np.float32).view(np.int32)[0]) <= 1
