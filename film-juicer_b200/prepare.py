@@ -46,6 +46,16 @@ SRGB_TO_XYZ = np.array([[0.4123907992659595, 0.3575843393838780, 0.1804807884018
 XYZ_TO_SRGB = np.linalg.inv(SRGB_TO_XYZ)
 CAT02 = np.array([[0.7328, 0.4296, -0.1624], [-0.7036, 1.6975, 0.0061], [0.0030, 0.0136, 0.9834]])
 D65_XYZ = np.array([0.95047, 1.0, 1.08883])
+D60_XYZ = np.array([0.95265, 1.0, 1.00883])
+# RGB -> XYZ of the host's input colour spaces (published primaries; FJ_INPUT_* order)
+INPUT_RGB_TO_XYZ = {
+    0: np.array([[0.70062239, 0.14877482, 0.10105872], [0.27411851, 0.87363190, -0.14775041],
+                 [-0.09896291, -0.13789533, 1.32591599]]),            # DaVinci Wide Gamut
+    1: np.array([[0.6369580, 0.1446169, 0.1688810], [0.2627002, 0.6779981, 0.0593017],
+                 [0.0, 0.0280727, 1.0609851]]),                       # BT.2020
+    2: np.array([[0.9525524, 0.0, 0.0000937], [0.3439664, 0.7281661, -0.0721325],
+                 [0.0, 0.0, 1.0088252]]),                             # ACES2065-1 (AP0, D60)
+}
 
 OK_XYZ_TO_LMS = np.array([[0.8189330101, 0.3618667424, -0.1288597137],
                           [0.0329845436, 0.9293118715, 0.0361456387],
@@ -209,6 +219,17 @@ def prepare_recipe(resources: str, film: str, paper: str | None = None, *, dir_a
         a["density_layers"] = f32(prof["density_curves_layers"])
     s["route_correction_scale"] = route_scale
     s["manual_exposure_ev"] = exposure_ev
+    # Mallett 2019 reconstruction tables (81 x 3 basis, the film's reference
+    # illuminant) and the green mid-grey scale of rust/film-juicer-core/src/exposure.rs:236-249
+    # (1 / sum_l 0.184 I(l) S_green(l), accumulated in FP64, stored as f32).
+    basis_path = os.path.join(resources, "luts", "spectral_upsampling", "mallett2019_basis.npy")
+    if os.path.exists(basis_path):
+        a["mallett_basis"] = f32(np.load(basis_path))
+        a["mallett_illuminant"] = f32(ref_ill)
+        green = 0.0
+        for i in range(a["mallett_illuminant"].size):
+            green += 0.184 * float(a["mallett_illuminant"][i]) * float(a["sensitivity_rgb"][i, 1])
+        s["mallett_green_scale"] = float(np.float32(1.0 / green))
     s["input_rgb_to_xyz"] = SRGB_TO_XYZ.ravel().tolist()
     s["xyz_to_linear_srgb"] = XYZ_TO_SRGB.ravel().tolist()
 
@@ -314,7 +335,15 @@ class HostRecord:
     """An FjPreparedHostData filled from a PreparedRecipe; keeps every array alive."""
 
     def __init__(self, recipe: PreparedRecipe, *, recipe_hash: int = 0, auto_exposure: bool = False,
-                 gamut: bool | None = None, dir_active: bool | None = None, correction=None):
+                 gamut: bool | None = None, dir_active: bool | None = None, correction=None,
+                 method: int = abi.FJ_RAW_HANATOS_2025, input_space: int = abi.FJ_INPUT_SRGB_REC709,
+                 decode: bool = False, adapt: bool = False, encoding: dict | None = None):
+        """method: FJ_RAW_* (Mallett needs the recipe's Mallett tables); input_space,
+        decode, adapt: the input colour space (FJ_INPUT_*), its CCTF decoding and the
+        XYZ adaptation (to D65 for the D60 ACES white); encoding: an output-encoding
+        entry of tests/golden/output_encoding_cases.json (colour space index, CCTF kind,
+        parameters and DWG-to-output matrix as f32 words), encoded from DWG (the
+        input-is-output flag cleared)."""
         self.recipe = recipe
         self._keep = []
         a, s = recipe.arrays, recipe.scalars
@@ -330,14 +359,24 @@ class HostRecord:
             return abi.FjFloatSpan(arr.ctypes.data_as(C.POINTER(C.c_float)), arr.size)
 
         ex = h.film_exposure
-        ex.input_color_space = abi.FJ_INPUT_SRGB_REC709
-        ex.method = abi.FJ_RAW_HANATOS_2025
-        ex.flags = abi.FJ_FILM_AUTO_EXPOSURE if auto_exposure else 0
+        ex.input_color_space = input_space
+        ex.method = method
+        ex.flags = (abi.FJ_FILM_AUTO_EXPOSURE if auto_exposure else 0) | (abi.FJ_FILM_DECODE_CCTF if decode else 0) \
+            | (abi.FJ_FILM_ADAPT_INPUT if adapt else 0)
         ex.manual_exposure_ev = s.get("manual_exposure_ev", 0.0)
         ex.route_correction_scale = s["route_correction_scale"]
         ex.mallett_green_midgray_scale = 1.0
-        abi.set_floats(ex.input_rgb_to_xyz, s["input_rgb_to_xyz"])
-        abi.set_floats(ex.input_xyz_adapt, np.eye(3).ravel())
+        if input_space in INPUT_RGB_TO_XYZ:
+            abi.set_floats(ex.input_rgb_to_xyz, INPUT_RGB_TO_XYZ[input_space].ravel())
+        else:
+            abi.set_floats(ex.input_rgb_to_xyz, s["input_rgb_to_xyz"])
+        abi.set_floats(ex.input_xyz_adapt, (cat02_matrix(D60_XYZ, D65_XYZ) if adapt else np.eye(3)).ravel())
+        if method == abi.FJ_RAW_MALLETT_2019:
+            if "mallett_basis" not in a:
+                raise ValueError("the recipe has no Mallett tables")
+            ex.mallett_basis = span(a["mallett_basis"])
+            ex.mallett_illuminant = span(a["mallett_illuminant"])
+            ex.mallett_green_midgray_scale = s["mallett_green_scale"]
         abi.set_floats(ex.xyz_to_linear_srgb, s["xyz_to_linear_srgb"])
         ex.sensitivity_rgb = span(a["sensitivity_rgb"])
         ex.tc_lut_rgba = span(a["tc_lut"])
@@ -406,6 +445,14 @@ class HostRecord:
         oc.encoding.cctf_kind = abi.FJ_CCTF_SRGB
         oc.encoding.gamma = 1.0 / 2.4
         abi.set_floats(oc.encoding.dwg_to_output, np.eye(3).ravel())
+        if encoding is not None:
+            f = lambda w: float(np.array([w], np.uint32).view(np.float32)[0])  # noqa: E731
+            oc.color_space = encoding["color_space"]
+            oc.flags &= ~abi.FJ_COLOR_INPUT_IS_OUTPUT_SPACE
+            en = oc.encoding
+            en.cctf_kind = encoding["cctf_kind"]
+            en.gamma, en.a, en.b, en.c, en.d, en.linear_cutoff = (f(w) for w in encoding["params"])
+            abi.set_floats(en.dwg_to_output, [f(w) for w in encoding["dwg_to_output"]])
 
         if recipe.route in (abi.FJ_ROUTE_NEGATIVE_PRINT, abi.FJ_ROUTE_POSITIVE_PRINT):
             pr = h.print

@@ -20,6 +20,10 @@ container, where the reference is mounted read-only).
   (tests/grain/frame-fixtures/linux-release.json): inputs and exact native output
   fields of every successful case, and the gaussian / energy / period primitives.
 * wang_lut.json: the Wang tile index table of Resources/Noise/Wang/tiles.json.
+* output_encoding_cases.json: the reference's frozen output-encoding table
+  (tests/scanner/output_encoding_native.inc): per output colour space index, the CCTF
+  kind, its six f32 parameters (gamma, a, b, c, d, linear cutoff) and the DWG-to-output
+  matrix, as f32 words.
 * abi_layout_reference.json: sizeof of every record of the reference's C-ABI header
   (native/juicer_cuda_api.h) and offsetof of every field, as the system C compiler
   lays them out; the drop-in boundary test compares the repository's header with it.
@@ -265,6 +269,24 @@ def gamut_cases():
     print("gamut cases:", [(r["tag"], r["variant"], r["ok"]) for r in rows])
 
 
+def output_encoding_cases():
+    import re
+
+    with open(os.path.join(REF, "tests", "scanner", "output_encoding_native.inc")) as fh:
+        text = fh.read()
+    body = text[text.index("kEntries"):]
+    rows = []
+    for chunk in body.split("{{static_cast<CctfKind>(")[1:]:
+        kind = int(chunk[: chunk.index(")")])
+        words = [int(w, 16) for w in re.findall(r"0x([0-9a-fA-F]+)u", chunk)]
+        assert len(words) == 15, len(words)
+        rows.append({"color_space": len(rows), "cctf_kind": kind, "params": words[:6], "dwg_to_output": words[6:]})
+    assert len(rows) == 9
+    with open(os.path.join(HERE, "output_encoding_cases.json"), "w") as fh:
+        json.dump({"source": "tests/scanner/output_encoding_native.inc", "entries": rows}, fh, indent=0)
+    print("output encodings:", len(rows))
+
+
 def abi_layout():
     import shutil
     import subprocess
@@ -324,5 +346,6 @@ if __name__ == "__main__":
     effects_cases()
     tc_lut_cases()
     gamut_cases()
+    output_encoding_cases()
     abi_layout()
     recipes()
