@@ -147,6 +147,13 @@ FjStatus fjb_recipe_read_flags(FjbRecipe* recipe, void* stream, uint32_t* out_fl
 
 static FjStatus launch_stage(FjbRecipe* recipe, fjb::PixelParams& p, fjb::PixelStage stage, void* stream,
                              FjErrorBuffer* error) {
+    if (p.route == fjb::kRoutePrint && p.print_form != fjb::kPrintFp32 &&
+        (stage == fjb::PixelStage::DensityToOutput || stage == fjb::PixelStage::DensityToLinearRgb)) {
+        // the tensor-core form hands the spectral integral to the FP32 epilogue in planes
+        cudaError_t e = recipe->r.ensure_tc_raw((size_t)p.width * (size_t)p.height);
+        if (e != cudaSuccess) return cuda_status(e, error, "tensor-core print planes");
+        p.tc_raw = recipe->r.tc_raw;
+    }
     cudaError_t e = fjb::launch_pixel_chain(p, stage, as_stream(stream));
     if (e != cudaSuccess) return cuda_status(e, error, "pixel chain launch");
     (void)recipe;

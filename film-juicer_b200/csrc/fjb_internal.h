@@ -24,6 +24,8 @@ enum class PixelStage : int {
     DensityToLinearRgb = 7, // density planes -> linear output-RGB planes (+ glare), before encoding
     LinearRgbToOutput = 8,  // linear output-RGB planes -> encoded output
     DensityToPrintRaw = 9,  // density planes -> the print's spectral integral (C, M, Y) into lin_r/g/b
+    RawToOutput = 10,       // print spectral integral planes (print_raw_*) -> encoded output
+    RawToLinearRgb = 11,    // print spectral integral planes -> linear output-RGB planes
 };
 
 cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStream_t stream);

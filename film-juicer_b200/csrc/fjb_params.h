@@ -158,6 +158,12 @@ struct PixelParams {
     // film defects: dust transmittance plane (null when off), applied to the print
     // exposure on the print route and to the scanned XYZ on the direct route
     const float* film_dust;
+    // print route, tensor-core form: the spectral integral (C, M, Y planes) computed by
+    // the tensor-core kernel, read by the FP32 print / scan / output epilogue
+    const float* print_raw_c;
+    const float* print_raw_m;
+    const float* print_raw_y;
+    float* tc_raw; // scratch for those planes (3 x width x height floats), owned by the recipe
     // gate output (encoding of linear planes): weave resampling and the gate mask
     int weave_active;
     float weave_dx, weave_dy, weave_cos, weave_sin;

@@ -20,7 +20,7 @@
 
 namespace fjb {
 
-enum InputKind : int { kInSource = 0, kInCarrier = 1, kInDensity = 2 };
+enum InputKind : int { kInSource = 0, kInCarrier = 1, kInDensity = 2, kInPrintRaw = 3 };
 enum OutputKind : int { kOutEncoded = 0, kOutDensity = 1, kOutDirSource = 2, kOutLinearRgb = 3, kOutPrintRaw = 4 };
 
 // Spatial-DIR source (src/Cuda/Film/JuicerCudaFilmPipeline.cu:124-214): raw log
@@ -87,6 +87,10 @@ __global__ void __launch_bounds__(kPixelThreads) pixel_chain_kernel(const __grid
             d[0] = p.scan_density_c[idx];
             d[1] = p.scan_density_m[idx];
             d[2] = p.scan_density_y[idx];
+        } else if constexpr (In == kInPrintRaw) {
+            // print development from the spectral integral of the tensor-core form
+            float raw[3] = {p.print_raw_c[idx], p.print_raw_m[idx], p.print_raw_y[idx]};
+            print_finish(p, blob, raw, d, p.film_dust ? p.film_dust[idx] : 1.0f);
         } else if constexpr (SpatialDir) {
             float logRaw[3];
             if (p.dir_log_raw_b) {
@@ -143,7 +147,7 @@ __global__ void __launch_bounds__(kPixelThreads) pixel_chain_kernel(const __grid
             print_develop(p, blob, d, p.film_dust ? p.film_dust[idx] : 1.0f);
         }
         // the direct route scans the film itself: its dust darkens the scanned XYZ
-        const float* dust = !Print && p.film_dust ? p.film_dust + idx : nullptr;
+        const float* dust = !Print && In != kInPrintRaw && p.film_dust ? p.film_dust + idx : nullptr;
 
         double rgb[3];
         if constexpr (Out == kOutLinearRgb) {
@@ -352,6 +356,10 @@ cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStrea
                          : launch_variant<kInDensity, kOutEncoded, false, false>(p, grid, smem, stream);
         case PixelStage::DensityToPrintRaw:
             return launch_variant<kInDensity, kOutPrintRaw, true, false>(p, grid, smem, stream);
+        case PixelStage::RawToOutput:
+            return launch_variant<kInPrintRaw, kOutEncoded, false, false>(p, grid, smem, stream);
+        case PixelStage::RawToLinearRgb:
+            return launch_variant<kInPrintRaw, kOutLinearRgb, false, false>(p, grid, smem, stream);
     }
     return cudaErrorInvalidValue;
 }

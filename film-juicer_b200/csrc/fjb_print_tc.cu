@@ -7,8 +7,8 @@
 // sens(l) = S(l) I_filt(l) (fjb_params.h), so T(l) = 2^(d . nd(l) + nd3(l)) and
 // raw_c = sum_l T(l) sens_c(l).
 //
-// One CTA of 128 threads takes tiles of 128 consecutive pixels (one per thread, one
-// TMEM lane per pixel):
+// One persistent CTA of 128 threads takes tiles of 128 consecutive pixels (one per
+// thread, one TMEM lane per pixel):
 //   GEMM1  D1[128 x 96] = A1[128 x 16] B1[96 x 16]^T  (M = pixels, N = wavelengths
 //          padded 81 -> 96, K = 16). A1 row = (d_hi[3], d_lo[3], d_hi[3], 1, 1, 0...),
 //          B1 row = (nd_hi[3], nd_hi[3], nd_lo[3], nd3_hi, nd3_lo, 0...): BF16 hi + lo
@@ -17,10 +17,16 @@
 //   exp2   per pixel and wavelength in FP32 on the MUFU, read from TMEM with
 //          tcgen05.ld; T rounded to BF16 (kPrintTensor) or to a BF16 pair hi + lo
 //          (kPrintTensorSplit) into shared memory.
-//   GEMM2  D2[128 x 16] = T[128 x 96] [sens_hi; sens_lo][16 x 96]^T (+ T_lo sens_hi),
-//          six K-steps of 16 per product, FP32 accumulate; columns 0..2 are raw C, M, Y.
-//   then   the print development, scan and output encoding of each pixel in FP32,
-//          the same device functions as the FP32 kernel (fjb_pixel_math.cuh).
+//   GEMM2  D2[128 x 16] = T[128 x 96] B2[16 x 96]^T with B2 rows (sens_hi C, M, Y,
+//          sens_lo C, M, Y, 0...): six K-steps of 16 (six more for T_lo), FP32
+//          accumulate; raw_c = D2[c] + D2[3 + c].
+// The tiles are software-pipelined two deep (double-buffered operands and TMEM): in
+// iteration i the CTA turns D1(i) into T(i), issues GEMM2(i) and GEMM1(i + 1) after one
+// barrier, prefetches the densities of tile i + 2, then reads raw(i - 1) from TMEM, so
+// each MMA runs while the CTA works on another tile. The kernel writes the spectral
+// integral planes; the print development, scan and output encoding of each pixel
+// follow in the FP32 pixel-chain kernel at full occupancy (fjb_pixel_chain.cu,
+// kInPrintRaw), the same device functions as the FP32 form.
 // Pixels with a non-finite density (failed DIR) take the FP32 cold path for raw.
 //
 // Operand tiles in shared memory are K-major without swizzle: 8-row x 16-byte core
@@ -43,17 +49,18 @@ namespace {
 constexpr int kTcThreads = 128;     // pixels per tile = MMA M = TMEM lanes
 constexpr int kTcLambda = 96;       // 81 wavelengths padded to six K-steps of 16
 constexpr int kTcK1 = 16;           // GEMM1 K
-constexpr uint32_t kTmemCols = 128; // D1 in columns 0..95, D2 in 96..111
-constexpr uint32_t kD2Col = 96;
 
-// shared-memory map, bytes from the (128-aligned) dynamic base
-constexpr uint32_t kOffA1 = 0;       // 128 x 16 BF16
-constexpr uint32_t kOffB1 = 4096;    // 96 x 16 BF16 (3072 B)
-constexpr uint32_t kOffB2 = 7168;    // 16 x 96 BF16 sens hi (3072 B), then sens lo
-constexpr uint32_t kOffA2 = 13312;   // 128 x 96 BF16 T hi (24576 B)
-constexpr uint32_t kOffA2lo = 37888; // 128 x 96 BF16 T lo (split form only)
-__host__ __device__ constexpr uint32_t off_bar(bool split) { return split ? 62464u : 37888u; }
-__host__ __device__ constexpr uint32_t off_blob(bool split) { return off_bar(split) + 64u; }
+// shared-memory map, bytes from the (128-aligned) dynamic base; buffers [2] alternate
+// between consecutive tiles
+constexpr uint32_t kOffA1 = 0;       // 2 x (128 x 16 BF16, 4096 B)
+constexpr uint32_t kOffB1 = 8192;    // 96 x 16 BF16 (3072 B)
+constexpr uint32_t kOffB2 = 11264;   // 16 x 96 BF16 (3072 B)
+constexpr uint32_t kOffA2 = 14336;   // 2 x (128 x 96 BF16 T hi, 24576 B)
+constexpr uint32_t kOffA2lo = 63488; // 2 x (128 x 96 BF16 T lo), split form only
+__host__ __device__ constexpr uint32_t off_bar(bool split) { return split ? 112640u : 63488u; }
+constexpr uint32_t kA1Bytes = 4096, kA2Bytes = 24576;
+// TMEM columns: D1 of buffer b at 96 b, D2 of buffer b at 192 + 16 b
+constexpr uint32_t kTmemAlloc = 256;
 
 // Byte offset of element (row, k) in a K-major, no-swizzle operand with `kdim` columns.
 __host__ __device__ constexpr uint32_t kmajor(int row, int k, int kdim) {
@@ -126,11 +133,11 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
         : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n\t"
         "tcgen05.wait::ld.sync.aligned;"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
         : "r"(taddr)
         : "memory");
 }
@@ -146,24 +153,53 @@ __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bflo
     lo = __float2bfloat16_rn(isfinite(v) ? v - __bfloat162float(hi) : 0.0f);
 }
 
-template <int Out, bool Split>
-__global__ void __launch_bounds__(kTcThreads) print_tc_kernel(const __grid_constant__ PixelParams p) {
+// A1 row of one pixel (zeros for a dead or non-finite pixel) into buffer `a1`.
+__device__ __forceinline__ void write_a1(unsigned char* a1, int tid, const float d[3], bool finite) {
+    __nv_bfloat16 a[kTcK1];
+    for (int k = 0; k < kTcK1; ++k) a[k] = __float2bfloat16_rn(0.0f);
+    if (finite) {
+        for (int c = 0; c < 3; ++c) {
+            __nv_bfloat16 hi, lo;
+            split_bf16(d[c], hi, lo);
+            a[c] = hi;
+            a[3 + c] = lo;
+            a[6 + c] = hi;
+        }
+        a[9] = a[10] = __float2bfloat16_rn(1.0f);
+    }
+    *reinterpret_cast<uint4*>(a1 + kmajor(tid, 0, kTcK1)) = *reinterpret_cast<const uint4*>(a);
+    *reinterpret_cast<uint4*>(a1 + kmajor(tid, 8, kTcK1)) = *reinterpret_cast<const uint4*>(a + 8);
+}
+
+__device__ __forceinline__ void load_density(const PixelParams& p, long long idx, long long total, float d[3]) {
+    if (idx < total) {
+        d[0] = __ldg(p.scan_density_c + idx);
+        d[1] = __ldg(p.scan_density_m + idx);
+        d[2] = __ldg(p.scan_density_y + idx);
+    } else {
+        d[0] = d[1] = d[2] = 0.0f;
+    }
+}
+
+__device__ __forceinline__ bool all_finite(const float d[3]) {
+    return isfinite(d[0]) && isfinite(d[1]) && isfinite(d[2]);
+}
+
+// Spectral integral planes (raw C, M, Y) of the density planes, tile pipeline above.
+template <bool Split>
+__global__ void __launch_bounds__(kTcThreads, 1) print_raw_tc_kernel(const __grid_constant__ PixelParams p,
+                                                                  float* __restrict__ raw_c,
+                                                                  float* __restrict__ raw_m,
+                                                                  float* __restrict__ raw_y) {
     extern __shared__ __align__(128) unsigned char tc_smem[];
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const uint32_t sbase = smem_addr(tc_smem);
-    float* blob = reinterpret_cast<float*>(tc_smem + off_blob(Split));
-    uint64_t* bars = reinterpret_cast<uint64_t*>(tc_smem + off_bar(Split));
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + off_bar(Split) + 16);
-    const uint32_t bar1 = smem_addr(bars), bar2 = smem_addr(bars + 1);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(tc_smem + off_bar(Split)); // bar1[0..1], bar2[0..1]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + off_bar(Split) + 32);
+    const uint32_t bar1[2] = {smem_addr(bars), smem_addr(bars + 1)};
+    const uint32_t bar2[2] = {smem_addr(bars + 2), smem_addr(bars + 3)};
 
-    // curves into shared memory
-    {
-        const float4* g = reinterpret_cast<const float4*>(p.curve_blob);
-        float4* s4 = reinterpret_cast<float4*>(blob);
-        const int n4 = p.curve_blob_floats >> 2;
-        for (int i = tid; i < n4; i += kTcThreads) s4[i] = __ldg(g + i);
-    }
     // B1: per wavelength (nd_hi[3], nd_hi[3], nd_lo[3], nd3_hi, nd3_lo, 0 x 5)
     const int count = p.spectral.count;
     for (int l = tid; l < kTcLambda; l += kTcThreads) {
@@ -182,84 +218,67 @@ __global__ void __launch_bounds__(kTcThreads) print_tc_kernel(const __grid_const
         for (int k = 0; k < kTcK1; ++k)
             *reinterpret_cast<__nv_bfloat16*>(tc_smem + kOffB1 + kmajor(l, k, kTcK1)) = row[k];
     }
-    // B2: sens hi and lo, rows C, M, Y then zeros, K = wavelength
+    // B2 rows: sens hi C, M, Y, sens lo C, M, Y, zeros; K = wavelength
     for (int e = tid; e < 16 * kTcLambda; e += kTcThreads) {
         const int n = e / kTcLambda, l = e - n * kTcLambda;
-        __nv_bfloat16 hi = __float2bfloat16_rn(0.0f), lo = hi;
-        if (n < 3 && l < count) split_bf16(p.spectral.sens[l][n], hi, lo);
-        *reinterpret_cast<__nv_bfloat16*>(tc_smem + kOffB2 + kmajor(n, l, kTcLambda)) = hi;
-        *reinterpret_cast<__nv_bfloat16*>(tc_smem + kOffB2 + 3072 + kmajor(n, l, kTcLambda)) = lo;
+        __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
+        if (n < 6 && l < count) {
+            __nv_bfloat16 hi, lo;
+            split_bf16(p.spectral.sens[l][n % 3], hi, lo);
+            v = n < 3 ? hi : lo;
+        }
+        *reinterpret_cast<__nv_bfloat16*>(tc_smem + kOffB2 + kmajor(n, l, kTcLambda)) = v;
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar2) : "memory");
+        for (int b = 0; b < 4; ++b)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars + b)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
-                     "r"(kTmemCols)
+                     "r"(kTmemAlloc)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+
+    const long long total = (long long)p.width * (long long)p.height;
+    const long long tiles = (total + kTcThreads - 1) / kTcThreads;
+    const long long n = tiles > blockIdx.x ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0; // tiles of this CTA
+    auto tile_idx = [&](long long j) { return (blockIdx.x + j * (long long)gridDim.x) * kTcThreads + tid; };
+
+    // prologue: A1 of tile 0, densities of tile 1
+    float d_cur[3], d_next[3];
+    load_density(p, n > 0 ? tile_idx(0) : total, total, d_cur);
+    bool fin_cur = tile_idx(0) < total && all_finite(d_cur);
+    write_a1(tc_smem + kOffA1, tid, d_cur, fin_cur);
+    load_density(p, n > 1 ? tile_idx(1) : total, total, d_next);
     fence_proxy_async();
     fence_before();
     __syncthreads();
     fence_after();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-
-    const uint64_t dA1 = smem_desc(sbase + kOffA1, 128, 256);
-    const uint64_t dB1 = smem_desc(sbase + kOffB1, 128, 256);
+    const uint32_t lane = (uint32_t)(warp * 32) << 16;
     const uint32_t i1 = idesc_bf16(128, kTcLambda);
     const uint32_t i2 = idesc_bf16(128, 16);
+    if (tid == 0 && n > 0) {
+        mma_bf16(tmem, smem_desc(sbase + kOffA1, 128, 256), smem_desc(sbase + kOffB1, 128, 256), i1, 0u);
+        mma_commit(bar1[0]);
+    }
 
-    const long long total = (long long)p.width * (long long)p.height;
-    const long long tiles = (total + kTcThreads - 1) / kTcThreads;
-    uint32_t phase = 0;
-    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const long long idx = tile * kTcThreads + tid;
-        const bool live = idx < total;
-        float d[3] = {0.0f, 0.0f, 0.0f};
-        if (live) {
-            d[0] = p.scan_density_c[idx];
-            d[1] = p.scan_density_m[idx];
-            d[2] = p.scan_density_y[idx];
-        }
-        const bool finite = live && isfinite(d[0]) && isfinite(d[1]) && isfinite(d[2]);
-        {
-            __nv_bfloat16 a[kTcK1];
-            for (int k = 0; k < kTcK1; ++k) a[k] = __float2bfloat16_rn(0.0f);
-            if (finite) {
-                for (int c = 0; c < 3; ++c) {
-                    __nv_bfloat16 hi, lo;
-                    split_bf16(d[c], hi, lo);
-                    a[c] = hi;
-                    a[3 + c] = lo;
-                    a[6 + c] = hi;
-                }
-                a[9] = a[10] = __float2bfloat16_rn(1.0f);
-            }
-            *reinterpret_cast<uint4*>(tc_smem + kOffA1 + kmajor(tid, 0, kTcK1)) = *reinterpret_cast<const uint4*>(a);
-            *reinterpret_cast<uint4*>(tc_smem + kOffA1 + kmajor(tid, 8, kTcK1)) =
-                *reinterpret_cast<const uint4*>(a + 8);
-        }
-        fence_proxy_async();
-        fence_before();
-        __syncthreads();
-        if (tid == 0) {
-            fence_after();
-            mma_bf16(tmem, dA1, dB1, i1, 0u);
-            mma_commit(bar1);
-        }
-        // every thread waits; the CTA goes on only if all saw the MMA complete
-        bool ok = __syncthreads_and(mbar_wait(bar1, phase)) != 0;
+    bool ok = true;
+    bool fin_prev = false;
+    float d_prev[3] = {0.0f, 0.0f, 0.0f};
+    for (long long i = 0; i < n; ++i) {
+        const int b = (int)(i & 1);
+        const uint32_t parity = (uint32_t)((i >> 1) & 1);
+        // 1. T(i) from D1(i) into A2[b]; A1[b^1] for tile i + 1; then GEMM2(i) and GEMM1(i + 1)
+        ok = mbar_wait(bar1[b], parity) && ok;
         fence_after();
-        if (ok) {
-            // T = 2^D for the 96 columns of this pixel, as BF16 (and BF16 remainders)
+        if (__all_sync(0xFFFFFFFFu, ok)) {
 #pragma unroll
             for (int chunk = 0; chunk < 3; ++chunk) {
                 uint32_t r[32];
-                tmem_ld32(lane_base + (uint32_t)(chunk * 32), r);
+                tmem_ld32(tmem + lane + (uint32_t)(b * kTcLambda + chunk * 32), r);
                 uint32_t hi[16], lo[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
@@ -274,107 +293,115 @@ __global__ void __launch_bounds__(kTcThreads) print_tc_kernel(const __grid_const
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const uint32_t off = kmajor(tid, chunk * 32 + q * 8, kTcLambda);
-                    *reinterpret_cast<uint4*>(tc_smem + kOffA2 + off) =
+                    *reinterpret_cast<uint4*>(tc_smem + kOffA2 + b * kA2Bytes + off) =
                         make_uint4(hi[4 * q], hi[4 * q + 1], hi[4 * q + 2], hi[4 * q + 3]);
                     if constexpr (Split)
-                        *reinterpret_cast<uint4*>(tc_smem + kOffA2lo + off) =
+                        *reinterpret_cast<uint4*>(tc_smem + kOffA2lo + b * kA2Bytes + off) =
                             make_uint4(lo[4 * q], lo[4 * q + 1], lo[4 * q + 2], lo[4 * q + 3]);
                 }
             }
         }
+        const bool fin_next = i + 1 < n && tile_idx(i + 1) < total && all_finite(d_next);
+        if (i + 1 < n) write_a1(tc_smem + kOffA1 + (b ^ 1) * kA1Bytes, tid, d_next, fin_next);
         fence_proxy_async();
         fence_before();
-        __syncthreads();
-        if (!ok) {
-            if (tid == 0 && p.error_flags) atomicOr(p.error_flags, kErrTensorWait);
-            break;
-        }
+        ok = __syncthreads_and(ok) != 0;
+        if (!ok) break;
         if (tid == 0) {
             fence_after();
+            const uint32_t a2 = sbase + kOffA2 + b * kA2Bytes;
+            const uint32_t d2 = tmem + 2 * kTcLambda + 16 * b;
 #pragma unroll
             for (int j = 0; j < 6; ++j)
-                mma_bf16(tmem + kD2Col, smem_desc(sbase + kOffA2 + 256u * j, 128, 1536),
-                         smem_desc(sbase + kOffB2 + 256u * j, 128, 1536), i2, j > 0 ? 1u : 0u);
-#pragma unroll
-            for (int j = 0; j < 6; ++j)
-                mma_bf16(tmem + kD2Col, smem_desc(sbase + kOffA2 + 256u * j, 128, 1536),
-                         smem_desc(sbase + kOffB2 + 3072u + 256u * j, 128, 1536), i2, 1u);
+                mma_bf16(d2, smem_desc(a2 + 256u * j, 128, 1536), smem_desc(sbase + kOffB2 + 256u * j, 128, 1536), i2,
+                         j > 0 ? 1u : 0u);
             if constexpr (Split) {
+                const uint32_t a2lo = sbase + kOffA2lo + b * kA2Bytes;
 #pragma unroll
                 for (int j = 0; j < 6; ++j)
-                    mma_bf16(tmem + kD2Col, smem_desc(sbase + kOffA2lo + 256u * j, 128, 1536),
-                             smem_desc(sbase + kOffB2 + 256u * j, 128, 1536), i2, 1u);
+                    mma_bf16(d2, smem_desc(a2lo + 256u * j, 128, 1536), smem_desc(sbase + kOffB2 + 256u * j, 128, 1536),
+                             i2, 1u);
             }
-            mma_commit(bar2);
-        }
-        ok = __syncthreads_and(mbar_wait(bar2, phase)) != 0;
-        fence_after();
-        if (!ok) {
-            if (tid == 0 && p.error_flags) atomicOr(p.error_flags, kErrTensorWait);
-            break;
-        }
-        uint32_t r2[4];
-        tmem_ld4(lane_base + kD2Col, r2);
-        phase ^= 1u;
-        if (!live) continue;
-
-        float raw[3] = {__uint_as_float(r2[0]), __uint_as_float(r2[1]), __uint_as_float(r2[2])};
-        if (!finite) print_spectral_nonfinite(p.spectral, d, raw);
-        if constexpr (Out == 2) { // the spectral integral itself
-            p.lin_r[idx] = raw[0];
-            p.lin_g[idx] = raw[1];
-            p.lin_b[idx] = raw[2];
-            continue;
-        }
-        print_finish(p, blob, raw, d, p.film_dust ? p.film_dust[idx] : 1.0f);
-        double rgb[3];
-        if constexpr (Out == 1) { // linear output-RGB planes
-            const float glare = p.scan_glare ? p.scan_glare[idx] : -1.0f;
-            if (!scan_to_linear(p, d, rgb, glare, nullptr)) {
-                flag_scan_failure(p);
-                rgb[0] = rgb[1] = rgb[2] = 0.0;
+            mma_commit(bar2[b]);
+            if (i + 1 < n) {
+                mma_bf16(tmem + (uint32_t)((b ^ 1) * kTcLambda), smem_desc(sbase + kOffA1 + (b ^ 1) * kA1Bytes, 128, 256),
+                         smem_desc(sbase + kOffB1, 128, 256), i1, 0u);
+                mma_commit(bar1[b ^ 1]);
             }
-            p.lin_r[idx] = (float)rgb[0];
-            p.lin_g[idx] = (float)rgb[1];
-            p.lin_b[idx] = (float)rgb[2];
-            continue;
         }
-        const int y = (int)(idx / p.width);
-        const int x = (int)(idx - (long long)y * p.width);
-        float* dstPix = reinterpret_cast<float*>(p.dst + (long long)y * p.dst_row_bytes) + (long long)x * p.components;
-        const float* srcPix =
-            p.src ? reinterpret_cast<const float*>(p.src + (long long)y * p.src_row_bytes) + (long long)x * p.components
-                  : nullptr;
-        if (!scan_to_linear(p, d, rgb, -1.0f, nullptr)) {
-            flag_scan_failure(p);
-            dstPix[0] = dstPix[1] = dstPix[2] = 0.0f;
-            if (p.components == 4) dstPix[3] = srcPix ? srcPix[3] : 1.0f;
-            continue;
+        // 2. densities of tile i + 2 in flight while raw(i - 1) is read out
+        float d_after[3];
+        load_density(p, i + 2 < n ? tile_idx(i + 2) : total, total, d_after);
+        // 3. raw(i - 1) from D2(i - 1)
+        if (i >= 1) {
+            const int pb = b ^ 1;
+            bool got = mbar_wait(bar2[pb], (uint32_t)(((i - 1) >> 1) & 1));
+            fence_after();
+            if (__all_sync(0xFFFFFFFFu, got)) {
+                uint32_t r2[8];
+                tmem_ld8(tmem + lane + (uint32_t)(2 * kTcLambda + 16 * pb), r2);
+                const long long idx = tile_idx(i - 1);
+                if (idx < total) {
+                    float raw[3];
+                    for (int c = 0; c < 3; ++c) raw[c] = __uint_as_float(r2[c]) + __uint_as_float(r2[3 + c]);
+                    if (!fin_prev) print_spectral_nonfinite(p.spectral, d_prev, raw);
+                    raw_c[idx] = raw[0];
+                    raw_m[idx] = raw[1];
+                    raw_y[idx] = raw[2];
+                }
+            } else {
+                got = false;
+            }
+            ok = ok && got;
         }
-        encode_output(p, rgb);
-        dstPix[0] = (float)rgb[0];
-        dstPix[1] = (float)rgb[1];
-        dstPix[2] = (float)rgb[2];
-        if (p.components == 4) dstPix[3] = srcPix ? srcPix[3] : 1.0f;
+        for (int c = 0; c < 3; ++c) {
+            d_prev[c] = d_cur[c];
+            d_cur[c] = d_next[c];
+            d_next[c] = d_after[c];
+        }
+        fin_prev = fin_cur;
+        fin_cur = fin_next;
     }
+    // the last tile's raw
+    if (ok && n > 0) {
+        const long long i = n - 1;
+        const int b = (int)(i & 1);
+        bool got = mbar_wait(bar2[b], (uint32_t)((i >> 1) & 1));
+        fence_after();
+        if (__all_sync(0xFFFFFFFFu, got)) {
+            uint32_t r2[8];
+            tmem_ld8(tmem + lane + (uint32_t)(2 * kTcLambda + 16 * b), r2);
+            const long long idx = tile_idx(i);
+            if (idx < total) {
+                float raw[3];
+                for (int c = 0; c < 3; ++c) raw[c] = __uint_as_float(r2[c]) + __uint_as_float(r2[3 + c]);
+                if (!fin_prev) print_spectral_nonfinite(p.spectral, d_prev, raw); // tile n - 1 after the shift
+                raw_c[idx] = raw[0];
+                raw_m[idx] = raw[1];
+                raw_y[idx] = raw[2];
+            }
+        } else {
+            got = false;
+        }
+        ok = got;
+    }
+    if (!__syncthreads_and(ok) && tid == 0 && p.error_flags) atomicOr(p.error_flags, kErrTensorWait);
 
     fence_before();
     __syncthreads();
     if (warp == 0) {
         fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemAlloc) : "memory");
     }
 }
 
-template <int Out, bool Split>
-cudaError_t launch_tc(const PixelParams& p, cudaStream_t stream) {
-    auto* k = print_tc_kernel<Out, Split>;
-    // Shared memory sized so that at most four (two for the split form) CTAs share an
-    // SM: their TMEM allocations (128 columns each) then always fit the SM's 512.
-    size_t smem = off_blob(Split) + (size_t)p.curve_blob_floats * sizeof(float);
-    const size_t floor_bytes = Split ? 80 * 1024 : 58 * 1024;
-    if (smem < floor_bytes) smem = floor_bytes;
-    const int per_sm = Split ? 2 : 4;
+template <bool Split>
+cudaError_t launch_raw_tc(const PixelParams& p, float* raw_c, float* raw_m, float* raw_y, cudaStream_t stream) {
+    auto* k = print_raw_tc_kernel<Split>;
+    // At least 80 KiB of shared memory per CTA, so that two CTAs at most share an SM:
+    // their TMEM allocations (256 columns each) then always fit the SM's 512.
+    size_t smem = off_bar(Split) + 64;
+    if (smem < 80 * 1024) smem = 80 * 1024;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int device = 0, sms = 0;
@@ -383,10 +410,10 @@ cudaError_t launch_tc(const PixelParams& p, cudaStream_t stream) {
     if (sms <= 0) sms = 148;
     const long long total = (long long)p.width * (long long)p.height;
     const long long tiles = (total + kTcThreads - 1) / kTcThreads;
-    const long long cap = (long long)sms * per_sm;
+    const long long cap = 2LL * sms;
     const int grid = (int)(tiles < cap ? tiles : cap);
     fjb::count_launch();
-    k<<<grid, kTcThreads, smem, stream>>>(p);
+    k<<<grid, kTcThreads, smem, stream>>>(p, raw_c, raw_m, raw_y);
     return cudaGetLastError();
 }
 
@@ -395,19 +422,25 @@ cudaError_t launch_tc(const PixelParams& p, cudaStream_t stream) {
 cudaError_t launch_print_tensor(const PixelParams& p, PixelStage stage, cudaStream_t stream) {
     const long long total = (long long)p.width * (long long)p.height;
     if (total <= 0) return cudaSuccess;
-    if ((p.curve_blob_floats & 3) != 0 || p.spectral.count > kTcLambda || p.spectral.count < 0)
-        return cudaErrorInvalidValue;
+    if (p.spectral.count > kTcLambda || p.spectral.count < 0) return cudaErrorInvalidValue;
     const bool split = p.print_form == kPrintTensorSplit;
-    switch (stage) {
-        case PixelStage::DensityToOutput:
-            return split ? launch_tc<0, true>(p, stream) : launch_tc<0, false>(p, stream);
-        case PixelStage::DensityToLinearRgb:
-            return split ? launch_tc<1, true>(p, stream) : launch_tc<1, false>(p, stream);
-        case PixelStage::DensityToPrintRaw:
-            return split ? launch_tc<2, true>(p, stream) : launch_tc<2, false>(p, stream);
-        default:
-            return cudaErrorInvalidValue;
-    }
+    if (stage == PixelStage::DensityToPrintRaw)
+        return split ? launch_raw_tc<true>(p, p.lin_r, p.lin_g, p.lin_b, stream)
+                     : launch_raw_tc<false>(p, p.lin_r, p.lin_g, p.lin_b, stream);
+    if (stage != PixelStage::DensityToOutput && stage != PixelStage::DensityToLinearRgb) return cudaErrorInvalidValue;
+    if (!p.tc_raw) return cudaErrorInvalidValue;
+    float* rc = p.tc_raw;
+    float* rm = p.tc_raw + total;
+    float* ry = p.tc_raw + 2 * total;
+    cudaError_t e = split ? launch_raw_tc<true>(p, rc, rm, ry, stream) : launch_raw_tc<false>(p, rc, rm, ry, stream);
+    if (e != cudaSuccess) return e;
+    PixelParams q = p;
+    q.print_raw_c = rc;
+    q.print_raw_m = rm;
+    q.print_raw_y = ry;
+    return launch_pixel_chain(q, stage == PixelStage::DensityToOutput ? PixelStage::RawToOutput
+                                                                      : PixelStage::RawToLinearRgb,
+                              stream);
 }
 
 } // namespace fjb

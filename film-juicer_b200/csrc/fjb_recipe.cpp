@@ -65,10 +65,25 @@ void set_curve_guess(const std::vector<float>& blob, CurveRef& c) {
 
 } // namespace
 
+cudaError_t Recipe::ensure_tc_raw(size_t pixels) noexcept {
+    const size_t need = 3 * pixels;
+    if (tc_raw && tc_raw_floats >= need) return cudaSuccess;
+    if (tc_raw) cudaFree(tc_raw);
+    tc_raw = nullptr;
+    tc_raw_floats = 0;
+    void* ptr = nullptr;
+    cudaError_t e = cudaMalloc(&ptr, need * sizeof(float));
+    if (e != cudaSuccess) return e;
+    tc_raw = static_cast<float*>(ptr);
+    tc_raw_floats = need;
+    return cudaSuccess;
+}
+
 void Recipe::release() noexcept {
     void* ptrs[] = {curves, tc_lut, mallett_basis, mallett_illum, film_sens_bgr, gamut_cmax, flags,
                     lut.nodes, lut.log2_xyz, lut.slope_c, lut.slope_m, lut.slope_y, lut.cell_min, lut.cell_max,
-                    lut.packed_nodes, lut.packed_cells, lut.failure, lut_spectra, meter_scratch, layer_curves};
+                    lut.packed_nodes, lut.packed_cells, lut.failure, lut_spectra, meter_scratch, layer_curves,
+                    tc_raw};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     curves = nullptr;
@@ -79,6 +94,8 @@ void Recipe::release() noexcept {
     lut_spectra = nullptr;
     meter_scratch = nullptr;
     layer_curves = nullptr;
+    tc_raw = nullptr;
+    tc_raw_floats = 0;
     layer_n = 0;
 }
 

@@ -40,11 +40,15 @@ struct Recipe {
     unsigned* flags = nullptr;
     double* lut_spectra = nullptr;
     void* meter_scratch = nullptr; // auto-exposure partial sums + ticket
+    float* tc_raw = nullptr;       // tensor-core print form: spectral integral planes of the last frame
+    size_t tc_raw_floats = 0;
     float* layer_curves = nullptr; // [layer][CMY] x layer_n sublayer density curves (grain), or null
     int layer_n = 0;
     bool positive_film = false;
     ScannerLutDevice lut{};
     void release() noexcept;
+    // Grows tc_raw to 3 planes of `pixels` floats (stream-ordered reuse across frames).
+    cudaError_t ensure_tc_raw(size_t pixels) noexcept;
 };
 
 bool create_recipe(const FjPreparedHostData& h, cudaStream_t stream, Recipe& r, std::string& why, FjStatus& status);
