@@ -354,6 +354,50 @@ def run_b200(args):
         if times.frames[i]:
             stages[name] = round(times.total_ms[i] / times.frames[i], 4)
 
+    # ---- the print contraction's tensor-core forms (same frame, same timing rules) ----
+    # The FP32 form above is the parity form and the headline value. The same K-step
+    # regions are timed with the 81-wavelength contraction on the tensor cores (BF16
+    # tiles, FP32 accumulation; transmittances as one BF16 or a hi + lo pair), and each
+    # form's output is compared with the FP32 form's in CIEDE2000 on every 4th pixel of
+    # every 4th row.
+    forms = {}
+    ref_out = dst.cpu().numpy()[::4, ::4] if rank == 0 else None
+    for name, code in (("tensor", abi.FJB_PRINT_TENSOR), ("tensor_split", abi.FJB_PRINT_TENSOR_SPLIT)):
+        owner.set_print_form(code)
+        for _ in range(args.warmup):
+            owner.render(record, src, dst, stream=stream)
+        stream.synchronize()
+        lib.fjb_owner_stage_timing(owner.handle, 1, C.byref(err.buf))
+        f_ms = []
+        for _ in range(regions):
+            barrier()
+            torch.cuda.synchronize()
+            fa, fb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            fa.record(stream)
+            for _ in range(args.steps):
+                owner.render(record, src, dst, stream=stream)
+            fb.record(stream)
+            fb.synchronize()
+            f_ms.append(fa.elapsed_time(fb))
+        ftimes = abi.FjbStageTimes()
+        lib.fjb_owner_stage_times(owner.handle, C.byref(ftimes), C.byref(err.buf))
+        lib.fjb_owner_stage_timing(owner.handle, 0, C.byref(err.buf))
+        barrier()
+        fms = max_over_ranks(statistics.median(f_ms) / args.steps)
+        pso = abi.FJB_STAGE_NAMES.index("print_scan_output")
+        entry = {"value": round(world * W * H / (fms * 1e-3) / 1e6, 2), "ms_per_step": round(fms, 4),
+                 "print_scan_output_ms": round(ftimes.total_ms[pso] / max(ftimes.frames[pso], 1), 4),
+                 "frame_speedup_vs_fp32": round(ms / fms, 4)}
+        if rank == 0:
+            from oracle import color
+
+            entry["delta_e00_vs_fp32"] = {k: round(v, 5) for k, v in
+                                          color.delta_e_stats(dst.cpu().numpy()[::4, ::4], ref_out).items()}
+        forms[name] = entry
+    owner.set_print_form(abi.FJB_PRINT_FP32)
+    owner.render(record, src, dst, stream=stream)
+    stream.synchronize()
+
     # ---- end to end through the C-ABI with host buffers ----
     # Frames are pipelined as a host would: while frame i renders on the render stream,
     # frame i+1's pixels go up on a copy stream and frame i-1's result comes down on
@@ -434,6 +478,8 @@ def run_b200(args):
             "stages_ms": stages,
             "roofline": roof,
             "stages_roofline": {k: {"frac": v["frac"], "bound": v["bound"]} for k, v in per_stage.items()},
+            "print_forms": {"fp32": {"value": round(value, 2), "ms_per_step": round(ms, 4),
+                                     "print_scan_output_ms": stages.get("print_scan_output")}, **forms},
             "cpu_baseline": cpu_baseline(args.cpu_seconds, W, H, args.next_rows) if world == 1 and args.cpu_seconds > 0 else None,
             "e2e": {"value": round(e2e, 2), "unit": "Mpix/s", "h2d_bytes_per_step": int(h_src.numel() * 4),
                     "d2h_bytes_per_step": int(h_dst[0].numel() * 4), "steps": e_steps,

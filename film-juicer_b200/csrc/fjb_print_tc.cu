@@ -20,7 +20,7 @@
 //   GEMM2  D2[128 x 16] = T[128 x 96] B2[16 x 96]^T with B2 rows (sens_hi C, M, Y,
 //          sens_lo C, M, Y, 0...): six K-steps of 16 (six more for T_lo), FP32
 //          accumulate; raw_c = D2[c] + D2[3 + c].
-// The tiles are software-pipelined two deep (double-buffered operands and TMEM): in
+// The tiles are software-pipelined two deep (double-buffered operands and D2): in
 // iteration i the CTA turns D1(i) into T(i), issues GEMM2(i) and GEMM1(i + 1) after one
 // barrier, prefetches the densities of tile i + 2, then reads raw(i - 1) from TMEM, so
 // each MMA runs while the CTA works on another tile. The kernel writes the spectral
@@ -59,8 +59,10 @@ constexpr uint32_t kOffA2 = 14336;   // 2 x (128 x 96 BF16 T hi, 24576 B)
 constexpr uint32_t kOffA2lo = 63488; // 2 x (128 x 96 BF16 T lo), split form only
 __host__ __device__ constexpr uint32_t off_bar(bool split) { return split ? 112640u : 63488u; }
 constexpr uint32_t kA1Bytes = 4096, kA2Bytes = 24576;
-// TMEM columns: D1 of buffer b at 96 b, D2 of buffer b at 192 + 16 b
-constexpr uint32_t kTmemAlloc = 256;
+// TMEM columns: D1 at 0..95 (one buffer: GEMM1(i + 1) is issued only after every thread
+// has read D1(i)), D2 of buffer b at 96 + 16 b
+constexpr uint32_t kTmemAlloc = 128;
+constexpr uint32_t kD2Col = 96;
 
 // Byte offset of element (row, k) in a K-major, no-swizzle operand with `kdim` columns.
 __host__ __device__ constexpr uint32_t kmajor(int row, int k, int kdim) {
@@ -278,12 +280,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) print_raw_tc_kernel(const __gri
 #pragma unroll
             for (int chunk = 0; chunk < 3; ++chunk) {
                 uint32_t r[32];
-                tmem_ld32(tmem + lane + (uint32_t)(b * kTcLambda + chunk * 32), r);
+                tmem_ld32(tmem + lane + (uint32_t)(chunk * 32), r);
                 uint32_t hi[16], lo[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    const float t0 = mufu_exp2(__uint_as_float(r[2 * j]));
-                    const float t1 = mufu_exp2(__uint_as_float(r[2 * j + 1]));
+                    // columns past the 81 wavelengths meet zero spectra: no exponential
+                    const int col = chunk * 32 + 2 * j;
+                    const float t0 = col < kSpectralSamples ? mufu_exp2(__uint_as_float(r[2 * j])) : 0.0f;
+                    const float t1 = col + 1 < kSpectralSamples ? mufu_exp2(__uint_as_float(r[2 * j + 1])) : 0.0f;
                     hi[j] = pack_bf16(t0, t1);
                     if constexpr (Split) {
                         const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&hi[j]);
@@ -310,7 +314,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) print_raw_tc_kernel(const __gri
         if (tid == 0) {
             fence_after();
             const uint32_t a2 = sbase + kOffA2 + b * kA2Bytes;
-            const uint32_t d2 = tmem + 2 * kTcLambda + 16 * b;
+            const uint32_t d2 = tmem + kD2Col + 16 * b;
 #pragma unroll
             for (int j = 0; j < 6; ++j)
                 mma_bf16(d2, smem_desc(a2 + 256u * j, 128, 1536), smem_desc(sbase + kOffB2 + 256u * j, 128, 1536), i2,
@@ -324,7 +328,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) print_raw_tc_kernel(const __gri
             }
             mma_commit(bar2[b]);
             if (i + 1 < n) {
-                mma_bf16(tmem + (uint32_t)((b ^ 1) * kTcLambda), smem_desc(sbase + kOffA1 + (b ^ 1) * kA1Bytes, 128, 256),
+                mma_bf16(tmem, smem_desc(sbase + kOffA1 + (b ^ 1) * kA1Bytes, 128, 256),
                          smem_desc(sbase + kOffB1, 128, 256), i1, 0u);
                 mma_commit(bar1[b ^ 1]);
             }
@@ -339,7 +343,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) print_raw_tc_kernel(const __gri
             fence_after();
             if (__all_sync(0xFFFFFFFFu, got)) {
                 uint32_t r2[8];
-                tmem_ld8(tmem + lane + (uint32_t)(2 * kTcLambda + 16 * pb), r2);
+                tmem_ld8(tmem + lane + (uint32_t)(kD2Col + 16 * pb), r2);
                 const long long idx = tile_idx(i - 1);
                 if (idx < total) {
                     float raw[3];
@@ -370,7 +374,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) print_raw_tc_kernel(const __gri
         fence_after();
         if (__all_sync(0xFFFFFFFFu, got)) {
             uint32_t r2[8];
-            tmem_ld8(tmem + lane + (uint32_t)(2 * kTcLambda + 16 * b), r2);
+            tmem_ld8(tmem + lane + (uint32_t)(kD2Col + 16 * b), r2);
             const long long idx = tile_idx(i);
             if (idx < total) {
                 float raw[3];
@@ -398,10 +402,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) print_raw_tc_kernel(const __gri
 template <bool Split>
 cudaError_t launch_raw_tc(const PixelParams& p, float* raw_c, float* raw_m, float* raw_y, cudaStream_t stream) {
     auto* k = print_raw_tc_kernel<Split>;
-    // At least 80 KiB of shared memory per CTA, so that two CTAs at most share an SM:
-    // their TMEM allocations (256 columns each) then always fit the SM's 512.
-    size_t smem = off_bar(Split) + 64;
-    if (smem < 80 * 1024) smem = 80 * 1024;
+    // 62 KiB (110 KiB split) of shared memory per CTA: three (two) CTAs share an SM at
+    // most, and their TMEM allocations (128 columns each) always fit the SM's 512.
+    const size_t smem = off_bar(Split) + 64;
+    const int per_sm = Split ? 2 : 3;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int device = 0, sms = 0;
@@ -410,7 +414,7 @@ cudaError_t launch_raw_tc(const PixelParams& p, float* raw_c, float* raw_m, floa
     if (sms <= 0) sms = 148;
     const long long total = (long long)p.width * (long long)p.height;
     const long long tiles = (total + kTcThreads - 1) / kTcThreads;
-    const long long cap = 2LL * sms;
+    const long long cap = (long long)per_sm * sms;
     const int grid = (int)(tiles < cap ? tiles : cap);
     fjb::count_launch();
     k<<<grid, kTcThreads, smem, stream>>>(p, raw_c, raw_m, raw_y);
