@@ -515,37 +515,22 @@ static __device__ __noinline__ void print_spectral_nonfinite(const PrintSpectral
     raw[2] = ay;
 }
 
-// One wavelength slot I of the fast path, then the next: the recursion makes every slot
-// index a compile-time constant. Every instruction takes at most one coefficient, so
-// each one is a constant-bank operand: an FMA with two coefficients (d2 nd2 + nd3)
-// would have the compiler fetch them into registers with per-thread constant loads,
-// which measured as the kernel's busiest pipe.
-template <int I>
-__device__ __forceinline__ void print_spectral_slots(const PrintSpectral& s, float d0, float d1, float d2,
-                                                     float (&a0)[3], float (&a1)[3]) {
-    if constexpr (I < kSpectralSamples) {
-        const float dl = fmaf(d0, s.nd[I][0], fmaf(d1, s.nd[I][1], d2 * s.nd[I][2])) + s.nd[I][3];
-        const float t = mufu_exp2(dl);
-        if constexpr ((I & 1) != 0) {
-            a1[0] = fmaf(t, s.sens[I][0], a1[0]);
-            a1[1] = fmaf(t, s.sens[I][1], a1[1]);
-            a1[2] = fmaf(t, s.sens[I][2], a1[2]);
-        } else {
-            a0[0] = fmaf(t, s.sens[I][0], a0[0]);
-            a0[1] = fmaf(t, s.sens[I][1], a0[1]);
-            a0[2] = fmaf(t, s.sens[I][2], a0[2]);
-        }
-        print_spectral_slots<I + 1>(s, d0, d1, d2, a0, a1);
-    }
-}
-
 __device__ __forceinline__ void print_spectral(const PrintSpectral& s, const float d[3], float raw[3]) {
     if (isfinite(d[0]) && isfinite(d[1]) && isfinite(d[2])) {
-        // Fast path: all 81 slots unrolled. Finite densities give finite exponents, so
-        // no NaN guard is needed; padded slots evaluate 2^-inf * 0 = +0. Two partial
-        // sums per channel (even / odd wavelength) halve the dependent FMA chain.
+        // Fast path: all 81 slots unrolled, coefficients are constant-bank operands.
+        // Finite densities give finite exponents, so no NaN guard is needed; padded
+        // slots evaluate 2^-inf * 0 = +0. Two partial sums per channel (even / odd
+        // wavelength) halve the dependent FMA chain.
         float a0[3] = {0.0f, 0.0f, 0.0f}, a1[3] = {0.0f, 0.0f, 0.0f};
-        print_spectral_slots<0>(s, d[0], d[1], d[2], a0, a1);
+#pragma unroll
+        for (int i = 0; i < kSpectralSamples; ++i) {
+            const float dl = fmaf(d[0], s.nd[i][0], fmaf(d[1], s.nd[i][1], fmaf(d[2], s.nd[i][2], s.nd[i][3])));
+            const float t = mufu_exp2(dl);
+            float* a = (i & 1) ? a1 : a0;
+            a[0] = fmaf(t, s.sens[i][0], a[0]);
+            a[1] = fmaf(t, s.sens[i][1], a[1]);
+            a[2] = fmaf(t, s.sens[i][2], a[2]);
+        }
         const float ac = a0[0] + a1[0], am = a0[1] + a1[1], ay = a0[2] + a1[2];
         raw[0] = ac;
         raw[1] = am;
