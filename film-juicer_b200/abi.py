@@ -265,8 +265,9 @@ FjbTcLutInput = _s("FjbTcLutInput", [("spectra", C.c_void_p), ("sensitivity_rgb"
                                      ("hull_xy", C.POINTER(C.c_float)), ("hull_center", f32 * 2),
                                      ("hull_available", u32)])
 FJB_STAGE_NAMES = ["auto_exposure", "camera_exposure", "camera_diffusion", "scatter_halation", "spatial_dir",
-                   "capture_density", "grain", "print_scan_output", "monolithic", "film_defects"]
-FjbStageTimes = _s("FjbStageTimes", [("total_ms", f64 * 10), ("frames", u64 * 10)])
+                   "capture_density", "grain", "print_scan_output", "monolithic", "film_defects",
+                   "enlarger_diffusion"]
+FjbStageTimes = _s("FjbStageTimes", [("total_ms", f64 * 11), ("frames", u64 * 11)])
 FjbScannerLutInput = _s("FjbScannerLutInput", [
     ("eps_c", FjFloatSpan), ("eps_m", FjFloatSpan), ("eps_y", FjFloatSpan), ("weighted_x", FjFloatSpan),
     ("weighted_y", FjFloatSpan), ("weighted_z", FjFloatSpan), ("baseline_min", FjFloatSpan),

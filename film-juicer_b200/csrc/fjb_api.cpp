@@ -147,7 +147,7 @@ FjStatus fjb_recipe_read_flags(FjbRecipe* recipe, void* stream, uint32_t* out_fl
 
 static FjStatus launch_stage(FjbRecipe* recipe, fjb::PixelParams& p, fjb::PixelStage stage, void* stream,
                              FjErrorBuffer* error) {
-    if (p.route == fjb::kRoutePrint && p.print_form != fjb::kPrintFp32 &&
+    if (p.route == fjb::kRoutePrint && p.print_form != fjb::kPrintFp32 && !p.print_done &&
         (stage == fjb::PixelStage::DensityToOutput || stage == fjb::PixelStage::DensityToLinearRgb)) {
         // the tensor-core form hands the spectral integral to the FP32 epilogue in planes
         cudaError_t e = recipe->r.ensure_tc_raw((size_t)p.width * (size_t)p.height);
@@ -285,6 +285,73 @@ FjStatus fjb_print_raw(FjbRecipe* recipe, const float* density_c, const float* d
     p.lin_b = raw_y;
     p.film_dust = nullptr;
     return launch_stage(recipe, p, fjb::PixelStage::DensityToPrintRaw, stream, error);
+}
+
+FjStatus fjb_enlarger_linear_exposure(FjbRecipe* recipe, const float* density_c, const float* density_m,
+                                      const float* density_y, const float* dust, float* linear_c, float* linear_m,
+                                      float* linear_y, int32_t width, int32_t height, void* stream,
+                                      FjErrorBuffer* error) {
+    if (!recipe || !density_c || !density_m || !density_y || !linear_c || !linear_m || !linear_y)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    if (recipe->r.params.route != fjb::kRoutePrint)
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "the recipe has no print stage");
+    if (width < 0 || height < 0) return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "unsupported image geometry");
+    fjb::PixelParams p = recipe->r.params;
+    p.width = width;
+    p.height = height;
+    p.scan_density_c = density_c;
+    p.scan_density_m = density_m;
+    p.scan_density_y = density_y;
+    p.film_dust = dust;
+    p.lin_r = linear_c;
+    p.lin_g = linear_m;
+    p.lin_b = linear_y;
+    return launch_stage(recipe, p, fjb::PixelStage::DensityToEnlargerLinear, stream, error);
+}
+
+FjStatus fjb_enlarger_develop(FjbRecipe* recipe, const float* linear_c, const float* linear_m, const float* linear_y,
+                              float* density_c, float* density_m, float* density_y, int32_t width, int32_t height,
+                              void* stream, FjErrorBuffer* error) {
+    if (!recipe || !density_c || !density_m || !density_y || !linear_c || !linear_m || !linear_y)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    if (recipe->r.params.route != fjb::kRoutePrint)
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "the recipe has no print stage");
+    if (width < 0 || height < 0) return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "unsupported image geometry");
+    fjb::PixelParams p = recipe->r.params;
+    p.width = width;
+    p.height = height;
+    p.scan_density_c = linear_c;
+    p.scan_density_m = linear_m;
+    p.scan_density_y = linear_y;
+    p.density_c = density_c;
+    p.density_m = density_m;
+    p.density_y = density_y;
+    return launch_stage(recipe, p, fjb::PixelStage::EnlargerLinearToPrintDensity, stream, error);
+}
+
+FjStatus fjb_render_from_print_density(FjbRecipe* recipe, const float* density_c, const float* density_m,
+                                       const float* density_y, const float* src, ptrdiff_t src_row_bytes, float* dst,
+                                       ptrdiff_t dst_row_bytes, int32_t width, int32_t height, uint32_t components,
+                                       void* stream, FjErrorBuffer* error) {
+    if (!recipe || !density_c || !density_m || !density_y || !dst)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    if (!valid_components(components)) return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "components");
+    if (recipe->r.params.route != fjb::kRoutePrint)
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "the recipe has no print stage");
+    fjb::PixelParams p = recipe->r.params;
+    p.print_done = 1;
+    p.film_dust = nullptr;
+    p.src = reinterpret_cast<const char*>(src);
+    p.src_row_bytes = src_row_bytes;
+    p.dst = reinterpret_cast<char*>(dst);
+    p.dst_row_bytes = dst_row_bytes;
+    p.width = width;
+    p.height = height;
+    p.components = (int)components;
+    p.scan_density_c = density_c;
+    p.scan_density_m = density_m;
+    p.scan_density_y = density_y;
+    return launch_stage(recipe, p, fjb::PixelStage::DensityToOutput, stream, error);
 }
 
 FjStatus fjb_auto_exposure(FjbRecipe* recipe, const float* src, ptrdiff_t src_row_bytes, uint32_t components,

@@ -128,7 +128,7 @@ FjStatus render_from_density_post(FjbRecipe* recipe, const PostPlan& plan, uint6
         if (e == cudaSuccess && plan.glare_r > 0) e = launch_blur_planes(&glare, &blurred, 1, width, height, glare_w, plan.glare_r, s);
         p.scan_glare = glare;
     }
-    if (e == cudaSuccess && p.route == kRoutePrint && p.print_form != kPrintFp32) {
+    if (e == cudaSuccess && p.route == kRoutePrint && p.print_form != kPrintFp32 && !p.print_done) {
         // the tensor-core form hands the spectral integral to the FP32 epilogue in planes
         e = recipe->r.ensure_tc_raw((size_t)width * (size_t)height);
         p.tc_raw = recipe->r.tc_raw;

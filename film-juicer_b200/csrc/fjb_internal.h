@@ -26,6 +26,10 @@ enum class PixelStage : int {
     DensityToPrintRaw = 9,  // density planes -> the print's spectral integral (C, M, Y) into lin_r/g/b
     RawToOutput = 10,       // print spectral integral planes (print_raw_*) -> encoded output
     RawToLinearRgb = 11,    // print spectral integral planes -> linear output-RGB planes
+    DensityToEnlargerLinear = 12,      // capture density planes -> print-linear exposure (lin_r/g/b: C-, M-,
+                                       // Y-forming), the enlarger diffusion's input
+    EnlargerLinearToPrintDensity = 13, // diffused print-linear exposure (scan_density_*) -> print density
+                                       // planes (density_*)
 };
 
 cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStream_t stream);

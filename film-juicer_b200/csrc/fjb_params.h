@@ -63,6 +63,7 @@ struct PixelParams {
     int components; // 3 or 4, same for source and destination
     int route;      // Route
     int print_form; // PrintForm: arithmetic of the 81-wavelength print contraction
+    int print_done; // 1: the density planes already hold print density (enlarger diffusion), scan only
 
     // Optional carrier input: planar linear exposure (B, G, R) produced by the
     // camera optics stages. When set, exposure reconstruction is skipped.

@@ -21,7 +21,15 @@
 namespace fjb {
 
 enum InputKind : int { kInSource = 0, kInCarrier = 1, kInDensity = 2, kInPrintRaw = 3 };
-enum OutputKind : int { kOutEncoded = 0, kOutDensity = 1, kOutDirSource = 2, kOutLinearRgb = 3, kOutPrintRaw = 4 };
+enum OutputKind : int {
+    kOutEncoded = 0,
+    kOutDensity = 1,
+    kOutDirSource = 2,
+    kOutLinearRgb = 3,
+    kOutPrintRaw = 4,
+    kOutEnlargerLinear = 5,  // print-linear exposure planes before the enlarger diffusion
+    kOutEnlargerDevelop = 6, // print density from the diffused print-linear exposure
+};
 
 // Spatial-DIR source (src/Cuda/Film/JuicerCudaFilmPipeline.cu:124-214): raw log
 // exposure, pre-DIR layer densities and the donor corrections they release.
@@ -135,6 +143,26 @@ __global__ void __launch_bounds__(kPixelThreads) pixel_chain_kernel(const __grid
             continue;
         }
 
+        if constexpr (Out == kOutEnlargerLinear) {
+            // src/Cuda/Scan/JuicerCudaScanPipeline.cu:1392-1447 with print_inner_raw_device and
+            // print_linear_for_diffusion_device (src/Cuda/JuicerCudaDeviceHelpers.cuh:966-1010)
+            float raw[3];
+            print_spectral(p.spectral, d, raw);
+            float lin[3];
+            enlarger_linear(p, raw, p.film_dust ? p.film_dust[idx] : 1.0f, lin);
+            p.lin_r[idx] = lin[0];
+            p.lin_g[idx] = lin[1];
+            p.lin_b[idx] = lin[2];
+            continue;
+        }
+        if constexpr (Out == kOutEnlargerDevelop) {
+            // :1449-1488 with print_log_encode_diffused_device (:1025) and the print curves
+            for (int c = 0; c < 3; ++c) d[c] = curve_sample(blob, p.print_curve[c], log10f(fmaxf(d[c], 0.0f) + 1e-10f), 1.0f);
+            p.density_c[idx] = d[0];
+            p.density_m[idx] = d[1];
+            p.density_y[idx] = d[2];
+            continue;
+        }
         if constexpr (Out == kOutPrintRaw) {
             float raw[3];
             print_spectral(p.spectral, d, raw);
@@ -314,14 +342,14 @@ cudaError_t launch_camera_exposure(const PixelParams& p, float* b, float* g, flo
 cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStream_t stream) {
     const long long total = (long long)p.width * (long long)p.height;
     if (total <= 0) return cudaSuccess;
-    if (p.route == kRoutePrint && p.print_form != kPrintFp32 &&
+    if (p.route == kRoutePrint && p.print_form != kPrintFp32 && !p.print_done &&
         (stage == PixelStage::DensityToOutput || stage == PixelStage::DensityToLinearRgb ||
          stage == PixelStage::DensityToPrintRaw))
         return launch_print_tensor(p, stage, stream);
     if ((p.curve_blob_floats & 3) != 0) return cudaErrorInvalidValue;
     const size_t smem = (size_t)p.curve_blob_floats * sizeof(float);
     const int grid = persistent_grid(total);
-    const bool print = p.route == kRoutePrint;
+    const bool print = p.route == kRoutePrint && !p.print_done; // enlarger diffusion: scan the print density
     const bool sdir = p.dir_spatial != 0;
     switch (stage) {
         case PixelStage::SourceToOutput:
@@ -356,6 +384,10 @@ cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStrea
                          : launch_variant<kInDensity, kOutEncoded, false, false>(p, grid, smem, stream);
         case PixelStage::DensityToPrintRaw:
             return launch_variant<kInDensity, kOutPrintRaw, true, false>(p, grid, smem, stream);
+        case PixelStage::DensityToEnlargerLinear:
+            return launch_variant<kInDensity, kOutEnlargerLinear, true, false>(p, grid, smem, stream);
+        case PixelStage::EnlargerLinearToPrintDensity:
+            return launch_variant<kInDensity, kOutEnlargerDevelop, false, false>(p, grid, smem, stream);
         case PixelStage::RawToOutput:
             return launch_variant<kInPrintRaw, kOutEncoded, false, false>(p, grid, smem, stream);
         case PixelStage::RawToLinearRgb:

@@ -562,6 +562,20 @@ __device__ __forceinline__ void print_finish(const PixelParams& p, const float* 
     }
 }
 
+// Print-linear exposure for the enlarger diffusion (src/Cuda/JuicerCudaDeviceHelpers.cuh:966-1010
+// print_inner_raw_device + print_linear_for_diffusion_device): the spectral integral times
+// the dust transmittance and the mid-grey normaliser, plus preflash, then
+// (max(raw, 0) + 1e-10) times print exposure x route correction.
+__device__ __forceinline__ void enlarger_linear(const PixelParams& p, float raw[3], float dust, float lin[3]) {
+    if (dust != 1.0f)
+        for (int c = 0; c < 3; ++c) raw[c] *= dust;
+    for (int c = 0; c < 3; ++c) raw[c] *= p.print_midgray;
+    if (p.print_preflash_exposure > 0.0f)
+        for (int c = 0; c < 3; ++c) raw[c] += p.print_preflash_raw[c] * p.print_preflash_exposure;
+    const float outer = p.print_exposure * p.print_route_correction;
+    for (int c = 0; c < 3; ++c) lin[c] = (fmaxf(raw[c], 0.0f) + 1e-10f) * outer;
+}
+
 __device__ __forceinline__ void print_develop(const PixelParams& p, const float* __restrict__ blob, float d[3],
                                               float dust = 1.0f) {
     float raw[3];

@@ -29,6 +29,25 @@
 #include "fjb_recipe.h"
 #include "fjb_schedule.h"
 
+namespace fjb_sched {
+// Device tables of one diffusion stage, kept across frames while the descriptor (and,
+// for the FFT form, the frame size) stays the same.
+struct DiffusionCache {
+    float* psf = nullptr; // PSF rows of the last descriptor
+    size_t psf_bytes = 0;
+    uint64_t key = 0;
+    int taps = 0;
+    float* spectrum = nullptr; // FFT form: PSF spectrum of the last descriptor and frame size
+    size_t spectrum_bytes = 0;
+    uint64_t spectrum_key = 0;
+    void release() {
+        if (psf) cudaFree(psf);
+        if (spectrum) cudaFree(spectrum);
+        *this = DiffusionCache{};
+    }
+};
+} // namespace fjb_sched
+
 struct FjCuda {
     std::mutex gate;
     bool closed = false;
@@ -41,14 +60,9 @@ struct FjCuda {
     uintptr_t noise_key[3] = {0, 0, 0};
     fjb::DirPlan dir_plan;                   // spatial-DIR operator tables of the last frame geometry
     uint64_t dir_key = 0;
-    float* diffusion_psf = nullptr;          // camera-diffusion PSF rows of the last descriptor
-    size_t diffusion_psf_bytes = 0;
-    uint64_t diffusion_key = 0;
-    int diffusion_taps = 0;
-    float* diffusion_spectrum = nullptr;     // FFT form: PSF spectrum of the last descriptor and frame size
-    size_t diffusion_spectrum_bytes = 0;
-    uint64_t diffusion_spectrum_key = 0;
-    float* diffusion_fft_work = nullptr;     // FFT form: transposed row spectra of the frame
+    fjb_sched::DiffusionCache camera_diffusion;   // camera diffusion: PSF rows / spectrum of the last descriptor
+    fjb_sched::DiffusionCache enlarger_diffusion; // enlarger diffusion, likewise
+    float* diffusion_fft_work = nullptr;     // FFT form: transposed row spectra of the frame (both stages)
     size_t diffusion_fft_work_bytes = 0;
     void* boost_state = nullptr;             // highlight reconstruction: frame maximum and disposition
     float* post_taps = nullptr;              // scanner post-effect Gaussian taps of the last descriptor
@@ -102,14 +116,8 @@ void release_all(FjCuda* cuda) {
     cuda->noise = nullptr;
     cuda->dir_plan.release();
     cuda->dir_key = 0;
-    if (cuda->diffusion_psf) cudaFree(cuda->diffusion_psf);
-    cuda->diffusion_psf = nullptr;
-    cuda->diffusion_psf_bytes = 0;
-    cuda->diffusion_key = 0;
-    if (cuda->diffusion_spectrum) cudaFree(cuda->diffusion_spectrum);
-    cuda->diffusion_spectrum = nullptr;
-    cuda->diffusion_spectrum_bytes = 0;
-    cuda->diffusion_spectrum_key = 0;
+    cuda->camera_diffusion.release();
+    cuda->enlarger_diffusion.release();
     if (cuda->diffusion_fft_work) cudaFree(cuda->diffusion_fft_work);
     cuda->diffusion_fft_work = nullptr;
     cuda->diffusion_fft_work_bytes = 0;
@@ -207,8 +215,11 @@ bool same_rect(const FjRect& a, const FjRect& b) { return a.x1 == b.x1 && a.y1 =
 
 // Stages this build schedules; the others are rejected by name rather than skipped.
 bool stages_supported(const FjPreparedHostData& h, std::string& why) {
-    if (h.optics.flags & FJ_OPTICS_ENLARGER_DIFFUSION) {
-        why = "enlarger diffusion is not supported by this build";
+    // the reference admits enlarger diffusion on the print routes only
+    // (native/juicer_cuda_descriptors.cpp:206-216)
+    if ((h.optics.flags & FJ_OPTICS_ENLARGER_DIFFUSION) && h.route != FJ_ROUTE_NEGATIVE_PRINT &&
+        h.route != FJ_ROUTE_POSITIVE_PRINT) {
+        why = "invalid descriptor: optics.flags (enlarger diffusion needs a print route)";
         return false;
     }
     fjb::PostPlan post;
@@ -254,6 +265,72 @@ FjStatus ensure_noise(FjCuda* cuda, const FjStaticNoise& n, void* stream, const 
     cuda->noise_key[1] = k1;
     cuda->noise_key[2] = n.stbn.count;
     *out = fresh;
+    return fjb::ok_status();
+}
+
+// One diffusion stage (camera or enlarger, src/Cuda/Diffusion/JuicerCudaDiffusion.cu:779
+// launch_stage) from planes R, G, B `src` into `dst`: PSF rows built once per descriptor,
+// FFT form from radius 8 up (PSF spectrum once per descriptor and frame size), else the
+// direct form. Times the launch as `stage`.
+FjStatus apply_diffusion(FjCuda* cuda, fjb_sched::DiffusionCache& cache, const FjDiffusion& d, int stage,
+                         const float* src[3], float* dst[3], ptrdiff_t stride, int width, int height, void* vs,
+                         FjErrorBuffer* error) {
+    if (!(d.scatter_fraction >= 0.0 && d.scatter_fraction <= 1.0))
+        return fjb::fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "diffusion scatter fraction outside [0, 1]");
+    cudaError_t e = cudaSuccess;
+    const uint64_t key = diffusion_identity(d);
+    if (key != cache.key || !cache.psf) {
+        // PSF rows are built once per distinct descriptor and kept on the device
+        FjDiffusionComponents dc{};
+        FjStatus st = fjb_diffusion_components_host(&d, &dc, error);
+        if (st.category != FJ_STATUS_SUCCESS) return st;
+        const double* wts[3] = {dc.red_weights, dc.green_weights, dc.blue_weights};
+        std::vector<float> rows[3];
+        int taps = 0;
+        std::string why;
+        for (int c = 0; c < 3; ++c)
+            if (!fjb::diffusion_psf_rows(dc.lambda_px, wts[c], d.radius_px, rows[c], taps, why))
+                return fjb::fail_status(FJ_STATUS_PREPARATION_FAILURE, error, why);
+        const size_t bytes = 3 * rows[0].size() * sizeof(float);
+        cache.key = 0;
+        e = ensure_buffer(cache.psf, cache.psf_bytes, bytes);
+        if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion PSF");
+        for (int c = 0; c < 3 && e == cudaSuccess; ++c)
+            e = cudaMemcpy(cache.psf + c * rows[0].size(), rows[c].data(), rows[c].size() * sizeof(float),
+                           cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion PSF upload");
+        cache.key = key;
+        cache.taps = taps;
+    }
+    const size_t n = (size_t)(d.radius_px + 1) * (size_t)cache.taps;
+    const float* psf[3] = {cache.psf, cache.psf + n, cache.psf + 2 * n};
+    const cudaStream_t cs = reinterpret_cast<cudaStream_t>(vs);
+    fjb::DiffusionFftPlan plan;
+    const bool fft =
+        fjb::diffusion_prefers_fft(width, height, d.radius_px) && fjb::diffusion_fft_plan(width, height, d.radius_px, plan);
+    if (fft) {
+        // the PSF spectrum depends on the descriptor and the transform sizes
+        const uint64_t skey = (cache.key * 0x100000001b3ULL) ^ ((uint64_t)width << 32) ^ (uint64_t)height;
+        e = ensure_buffer(cuda->diffusion_fft_work, cuda->diffusion_fft_work_bytes, plan.work_floats * sizeof(float));
+        if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion FFT workspace");
+        if (skey != cache.spectrum_key || !cache.spectrum) {
+            cache.spectrum_key = 0;
+            e = ensure_buffer(cache.spectrum, cache.spectrum_bytes, plan.spectrum_floats * sizeof(float));
+            if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion PSF spectrum");
+            e = fjb::launch_diffusion_fft_spectrum(plan, psf, cache.taps, cache.spectrum, cuda->diffusion_fft_work, cs);
+            if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion PSF spectrum");
+            cache.spectrum_key = skey;
+        }
+    }
+    stage_begin(cuda, stage, vs);
+    if (fft)
+        e = fjb::launch_diffusion_fft(plan, cache.spectrum, (float)d.scatter_fraction, dst, src, stride,
+                                      cuda->diffusion_fft_work, cs);
+    else
+        e = fjb::launch_diffusion(psf, d.radius_px, cache.taps, (float)d.scatter_fraction, dst, src, stride, width,
+                                  height, cs);
+    stage_end(cuda, stage, vs);
+    if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion");
     return fjb::ok_status();
 }
 
@@ -318,73 +395,12 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
     }
     stage_end(cuda, FJB_STAGE_CAMERA_EXPOSURE, vs);
     if (camera_diffusion) {
-        const FjDiffusion& d = o.camera;
-        if (!(d.scatter_fraction >= 0.0 && d.scatter_fraction <= 1.0))
-            return fjb::fail_status(FJ_STATUS_PREPARATION_FAILURE, error, "diffusion scatter fraction outside [0, 1]");
-        const uint64_t key = diffusion_identity(d);
-        if (key != cuda->diffusion_key || !cuda->diffusion_psf) {
-            // PSF rows are built once per distinct descriptor and kept on the device
-            FjDiffusionComponents dc{};
-            st = fjb_diffusion_components_host(&d, &dc, error);
-            if (st.category != FJ_STATUS_SUCCESS) return st;
-            const double* wts[3] = {dc.red_weights, dc.green_weights, dc.blue_weights};
-            std::vector<float> rows[3];
-            int taps = 0;
-            std::string why;
-            for (int c = 0; c < 3; ++c)
-                if (!fjb::diffusion_psf_rows(dc.lambda_px, wts[c], d.radius_px, rows[c], taps, why))
-                    return fjb::fail_status(FJ_STATUS_PREPARATION_FAILURE, error, why);
-            const size_t bytes = 3 * rows[0].size() * sizeof(float);
-            cuda->diffusion_key = 0;
-            if (cuda->diffusion_psf_bytes < bytes) {
-                if (cuda->diffusion_psf) cudaFree(cuda->diffusion_psf);
-                cuda->diffusion_psf = nullptr;
-                cuda->diffusion_psf_bytes = 0;
-                e = cudaMalloc(&cuda->diffusion_psf, bytes);
-                if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion PSF");
-                cuda->diffusion_psf_bytes = bytes;
-            }
-            for (int c = 0; c < 3 && e == cudaSuccess; ++c)
-                e = cudaMemcpy(cuda->diffusion_psf + c * rows[0].size(), rows[c].data(), rows[c].size() * sizeof(float),
-                               cudaMemcpyHostToDevice);
-            if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion PSF upload");
-            cuda->diffusion_key = key;
-            cuda->diffusion_taps = taps;
-        }
-        const size_t n = (size_t)(d.radius_px + 1) * (size_t)cuda->diffusion_taps;
-        const float* psf[3] = {cuda->diffusion_psf, cuda->diffusion_psf + n, cuda->diffusion_psf + 2 * n};
-        // R, G, B planes into the density planes, which then carry the exposure
+        // R, G, B carrier planes into the density planes, which then carry the exposure
         float* ddst[3] = {density[2], density[1], density[0]};
         const float* dsrc[3] = {carrier[2], carrier[1], carrier[0]};
-        const cudaStream_t cs = reinterpret_cast<cudaStream_t>(vs);
-        fjb::DiffusionFftPlan plan;
-        const bool fft = fjb::diffusion_prefers_fft(width, height, d.radius_px) &&
-                         fjb::diffusion_fft_plan(width, height, d.radius_px, plan);
-        if (fft) {
-            // the PSF spectrum depends on the descriptor and the transform sizes
-            const uint64_t skey = (cuda->diffusion_key * 0x100000001b3ULL) ^ ((uint64_t)width << 32) ^ (uint64_t)height;
-            e = ensure_buffer(cuda->diffusion_fft_work, cuda->diffusion_fft_work_bytes, plan.work_floats * sizeof(float));
-            if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion FFT workspace");
-            if (skey != cuda->diffusion_spectrum_key || !cuda->diffusion_spectrum) {
-                cuda->diffusion_spectrum_key = 0;
-                e = ensure_buffer(cuda->diffusion_spectrum, cuda->diffusion_spectrum_bytes,
-                                  plan.spectrum_floats * sizeof(float));
-                if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion PSF spectrum");
-                e = fjb::launch_diffusion_fft_spectrum(plan, psf, cuda->diffusion_taps, cuda->diffusion_spectrum,
-                                                       cuda->diffusion_fft_work, cs);
-                if (e != cudaSuccess) return fjb::cuda_status(e, error, "diffusion PSF spectrum");
-                cuda->diffusion_spectrum_key = skey;
-            }
-        }
-        stage_begin(cuda, FJB_STAGE_CAMERA_DIFFUSION, vs);
-        if (fft)
-            e = fjb::launch_diffusion_fft(plan, cuda->diffusion_spectrum, (float)d.scatter_fraction, ddst, dsrc, stride,
-                                          cuda->diffusion_fft_work, cs);
-        else
-            e = fjb::launch_diffusion(psf, d.radius_px, cuda->diffusion_taps, (float)d.scatter_fraction, ddst, dsrc,
-                                      stride, width, height, cs);
-        stage_end(cuda, FJB_STAGE_CAMERA_DIFFUSION, vs);
-        if (e != cudaSuccess) return fjb::cuda_status(e, error, "camera diffusion");
+        st = apply_diffusion(cuda, cuda->camera_diffusion, o.camera, FJB_STAGE_CAMERA_DIFFUSION, dsrc, ddst, stride,
+                             width, height, vs, error);
+        if (st.category != FJ_STATUS_SUCCESS) return st;
         std::swap(carrier[0], density[0]);
         std::swap(carrier[1], density[1]);
         std::swap(carrier[2], density[2]);
@@ -451,6 +467,27 @@ FjStatus render_staged(FjCuda* cuda, FjbRecipe* recipe, const FjPreparedHostData
                                      reinterpret_cast<cudaStream_t>(vs), tables, table_bytes);
         stage_end(cuda, FJB_STAGE_FILM_DEFECTS, vs);
         if (e != cudaSuccess) return fjb::cuda_status(e, error, "film defects");
+    }
+    // Enlarger diffusion (src/Cuda/JuicerCudaExecutor.cpp:2292-2365): the print-linear
+    // exposure of the capture density (film dust applied there) into the carrier planes,
+    // the enlarger's diffusion back into the density planes, print development there;
+    // the scan then reads print density and the film dust is not applied again.
+    const bool enlarger = (o.flags & FJ_OPTICS_ENLARGER_DIFFUSION) != 0;
+    if (enlarger) {
+        st = fjb_enlarger_linear_exposure(recipe, density[0], density[1], density[2], dust, carrier[0], carrier[1],
+                                          carrier[2], width, height, vs, error);
+        if (st.category != FJ_STATUS_SUCCESS) return st;
+        const float* dsrc[3] = {carrier[0], carrier[1], carrier[2]}; // red-, green-, blue-sensitive layers
+        float* ddst[3] = {density[0], density[1], density[2]};
+        st = apply_diffusion(cuda, cuda->enlarger_diffusion, o.enlarger, FJB_STAGE_ENLARGER_DIFFUSION, dsrc, ddst,
+                             stride, width, height, vs, error);
+        if (st.category != FJ_STATUS_SUCCESS) return st;
+        st = fjb_enlarger_develop(recipe, density[0], density[1], density[2], density[0], density[1], density[2],
+                                  width, height, vs, error);
+        if (st.category != FJ_STATUS_SUCCESS) return st;
+        dust = nullptr;
+        recipe->r.params.print_done = 1;
+        if (aborted(abort_cb)) return fjb::fail_status(FJ_STATUS_CANCELLED, error, "abort requested");
     }
     if (planes_out) {
         fjb::OutputEffects out;
@@ -647,6 +684,7 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
             FjbRecipe* r;
             ~FrameState() {
                 r->r.params.auto_exposure_scale = nullptr;
+                r->r.params.print_done = 0;
                 fjb_recipe_set_spatial_dir_planes(r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
             }
         } frame_state{recipe};
@@ -713,8 +751,9 @@ FjRenderOutcome fj_cuda_render(FjCuda* cuda, const FjCudaContext* context, const
                 return out;
             }
         }
+        const bool enlarger = (optics & FJ_OPTICS_ENLARGER_DIFFUSION) != 0;
         if (!camera_diffusion && !halation && !spatial_dir && !grain && !post.active && !boost && !fx.film &&
-            !fx.gate_output) {
+            !fx.gate_output && !enlarger) {
             // Monolithic: one fused pass source -> output
             stage_begin(cuda, FJB_STAGE_MONOLITHIC, vs);
             st = fjb_render_pixels(recipe, src, srb, dst, drb, width, height, comps, vs, error);

@@ -20,12 +20,14 @@ class FrameRecord:
                  diffusion: bool = True, halation: bool = True, spatial_dir: bool = True, grain: bool = True,
                  auto_exposure: bool = False, noise: "grain_plan.Noise | None" = None,
                  pixel_size_um: float | None = None, frame_time: float = 0.0, descriptor_width: int | None = None,
-                 post=None, highlight_boost=None, effects=None):
+                 post=None, highlight_boost=None, effects=None, enlarger: bool = False):
         """descriptor_width: the frame width the pixel size and diffusion radius are
         derived for (defaults to `width`; a crop of a larger frame passes the full width);
         post: an FjScannerPostEffects record (descriptors.scanner_post_record);
         highlight_boost: an FjHighlightBoost record (descriptors.highlight_boost_record);
-        effects: an FjFilmEffects record (film / gate defects, weave)."""
+        effects: an FjFilmEffects record (film / gate defects, weave);
+        enlarger: enlarger diffusion (print routes; a warm family-0 filter of radius
+        0.3 % of the width on the print-linear exposure)."""
         self.width, self.height = width, height
         dw = descriptor_width or width
         self.pixel_size_um = pixel_size_um or 35000.0 / dw
@@ -45,6 +47,10 @@ class FrameRecord:
         if halation:
             h.optics.scatter_halation = prepare.scatter_halation_record(px)
             flags |= abi.FJ_OPTICS_SCATTER_HALATION
+        if enlarger:
+            h.optics.enlarger = descriptors.diffusion_record(px, dw, family=0, scatter_fraction=0.2, warmth=0.5,
+                                                             radius_fraction_of_width=0.003)
+            flags |= abi.FJ_OPTICS_ENLARGER_DIFFUSION
         if highlight_boost is not None:
             h.optics.highlight_boost = highlight_boost
             flags |= abi.FJ_OPTICS_HIGHLIGHT_BOOST

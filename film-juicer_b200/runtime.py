@@ -80,6 +80,36 @@ class DeviceRecipe:
                                     C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
         _check("fjb_print_raw", st, err)
 
+    def enlarger_linear_exposure(self, density, linear, dust=None, stream=None):
+        """Print-linear exposure planes (C-, M-, Y-forming) of capture density planes."""
+        c, m, y = density
+        h, w = c.shape
+        err = abi.ErrorText()
+        st = self.lib.fjb_enlarger_linear_exposure(self.handle, *[C.c_void_p(_ptr(t)) for t in (c, m, y)],
+                                                   C.c_void_p(_ptr(dust) if dust is not None else 0),
+                                                   *[C.c_void_p(_ptr(t)) for t in linear], w, h,
+                                                   C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+        _check("fjb_enlarger_linear_exposure", st, err)
+
+    def enlarger_develop(self, linear, density, stream=None):
+        """Print density planes C, M, Y of (diffused) print-linear exposure planes."""
+        h, w = linear[0].shape
+        err = abi.ErrorText()
+        st = self.lib.fjb_enlarger_develop(self.handle, *[C.c_void_p(_ptr(t)) for t in (*linear, *density)], w, h,
+                                           C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+        _check("fjb_enlarger_develop", st, err)
+
+    def render_from_print_density(self, density, src, dst, stream=None):
+        c, m, y = density
+        h, w, comps = dst.shape
+        err = abi.ErrorText()
+        st = self.lib.fjb_render_from_print_density(self.handle, C.c_void_p(_ptr(c)), C.c_void_p(_ptr(m)),
+                                                    C.c_void_p(_ptr(y)), C.c_void_p(_ptr(src) if src is not None else 0),
+                                                    (src.stride(0) * 4) if src is not None else 0, C.c_void_p(_ptr(dst)),
+                                                    dst.stride(0) * 4, w, h, comps, C.c_void_p(_stream_handle(stream)),
+                                                    C.byref(err.buf))
+        _check("fjb_render_from_print_density", st, err)
+
     def set_exposure_scale_device(self, tensor):
         err = abi.ErrorText()
         st = self.lib.fjb_recipe_set_exposure_scale_device(self.handle, C.c_void_p(_ptr(tensor) if tensor is not None

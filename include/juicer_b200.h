@@ -57,6 +57,26 @@ FjStatus fjb_print_raw(FjbRecipe* recipe, const float* density_c, const float* d
                        float* raw_c, float* raw_m, float* raw_y, int32_t width, int32_t height, void* stream,
                        FjErrorBuffer* error);
 
+/* Enlarger diffusion, stage by stage (reference
+ * src/Cuda/Scan/JuicerCudaScanPipeline.cu:2924 juicer_cuda_print_focused_enlarger_linear_exposure
+ * and :2943 juicer_cuda_print_focused_develop_from_enlarger_linear). The print-linear
+ * exposure of capture density planes C, M, Y (dust: film dust transmittance plane or
+ * NULL) into planes C-, M-, Y-forming (red-, green-, blue-sensitive layers of the
+ * paper: the R, G, B planes of fjb_diffusion with the enlarger record); after the
+ * diffusion, the print density C, M, Y from those planes (may be the same buffers);
+ * then the scan and output encoding of print density planes. Print route only. */
+FjStatus fjb_enlarger_linear_exposure(FjbRecipe* recipe, const float* density_c, const float* density_m,
+                                      const float* density_y, const float* dust, float* linear_c, float* linear_m,
+                                      float* linear_y, int32_t width, int32_t height, void* stream,
+                                      FjErrorBuffer* error);
+FjStatus fjb_enlarger_develop(FjbRecipe* recipe, const float* linear_c, const float* linear_m, const float* linear_y,
+                              float* density_c, float* density_m, float* density_y, int32_t width, int32_t height,
+                              void* stream, FjErrorBuffer* error);
+FjStatus fjb_render_from_print_density(FjbRecipe* recipe, const float* density_c, const float* density_m,
+                                       const float* density_y, const float* src, ptrdiff_t src_row_bytes, float* dst,
+                                       ptrdiff_t dst_row_bytes, int32_t width, int32_t height, uint32_t components,
+                                       void* stream, FjErrorBuffer* error);
+
 /* Device error word (bit 0 scan failure, bit 8 DIR failure, bits 9..11 DIR
  * channels B,G,R, bit 16 a tensor-core wait of the print stage gave up). Cleared by fjb_recipe_clear_flags, read by fjb_recipe_read_flags
  * (which synchronises `stream`). */
@@ -344,7 +364,8 @@ FjStatus fjb_visual_grain(FjbRecipe* recipe, const FjVisualGrain* grain, const F
 #define FJB_STAGE_PRINT_SCAN_OUTPUT 7
 #define FJB_STAGE_MONOLITHIC 8
 #define FJB_STAGE_FILM_DEFECTS 9
-#define FJB_STAGE_COUNT 10
+#define FJB_STAGE_ENLARGER_DIFFUSION 10
+#define FJB_STAGE_COUNT 11
 typedef struct FjbStageTimes {
     double total_ms[FJB_STAGE_COUNT];
     uint64_t frames[FJB_STAGE_COUNT];

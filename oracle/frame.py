@@ -1,7 +1,10 @@
 """The oracle's whole-frame chain for the staged schedule (test infrastructure only):
 camera exposure -> highlight reconstruction -> camera diffusion -> scatter/halation -> spatial DIR -> capture
-density -> grain -> print/scan/output, each stage the CPU restatement in oracle/."""
+density -> grain -> film defects -> (enlarger: print-linear exposure, enlarger diffusion, print development)
+-> print/scan/output, each stage the CPU restatement in oracle/."""
 from __future__ import annotations
+
+import contextlib
 
 import numpy as np
 
@@ -71,6 +74,26 @@ def render_frame(frame_record, recipe, src, threads: int = 1, frame_token: int =
         density, dust = orc.film_defects(fx, density)
     if gate_output and (fx.flags & abi.FJ_EFFECTS_GATE_TRANSMITTANCE):
         mask = orc.gate_mask(fx)
+    enlarger = bool(flags & abi.FJ_OPTICS_ENLARGER_DIFFUSION)
+    if enlarger:
+        # print-linear exposure (film dust applied here), the enlarger's diffusion, print
+        # development; the scan then reads print density
+        lin = ooptics.enlarger_linear(host, density, dust)
+        d = h.optics.enlarger
+        lam, w = ooptics.diffusion_components(d.family, list(d.group_weights), list(d.group_lambda_um), d.warmth,
+                                              d.spatial_scale, d.pixel_size_um)
+        if diffusion_form == "fft":
+            lin = ooptics.diffusion_fft(_Components(lam, w), d.radius_px, d.scatter_fraction, lin, workers=threads)
+        else:
+            lin = ooptics.diffusion(_Components(lam, w), d.radius_px, d.scatter_fraction, lin)
+        density = ooptics.enlarger_develop(host, lin)
+        dust = None
+    with (ooptics.print_done() if enlarger else contextlib.nullcontext()):
+        return _scan(host, h, fx, film, gate_output, dust, mask, density, src, threads, frame_token, abi)
+
+
+def _scan(host, h, fx, film, gate_output, dust, mask, density, src, threads, frame_token, abi):
+    """Print (unless the enlarger already developed it) / scan / output of the density planes."""
     if h.scanner_post.hash != 0 or film or gate_output:
         # linear planes before the encoding; the source origin of these frames is (0, 0)
         seed = orc.glare_seed(h.recipe_hash, frame_token, 0, 0)

@@ -188,3 +188,74 @@ def reference_highlight_boost(torch, descriptor, carrier_bgr):
     if rc != 0:
         raise RuntimeError(f"ref_highlight_boost failed with code {rc}")
     return disp.value
+
+
+def enlarger_linear(record, density_cmy, dust=None):
+    """Print-linear exposure planes (C-, M-, Y-forming) of capture density planes
+    (oracle_enlarger_linear)."""
+    lib = _o.load()
+    abi = _o._abi()
+    fn = lib.oracle_enlarger_linear
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(abi.FjPreparedHostData)] + [C.c_void_p] * 4 + [C.c_int, C.c_int] + [C.c_void_p] * 3
+    dens = [np.ascontiguousarray(p, dtype=np.float32) for p in density_cmy]
+    h, w = dens[0].shape
+    out = [np.zeros((h, w), np.float32) for _ in range(3)]
+    d = np.ascontiguousarray(dust, dtype=np.float32) if dust is not None else None
+    rc = fn(record.pointer(), *[C.c_void_p(p.ctypes.data) for p in dens],
+            C.c_void_p(d.ctypes.data) if d is not None else None, w, h, *[C.c_void_p(p.ctypes.data) for p in out])
+    if rc != 0:
+        raise RuntimeError("oracle_enlarger_linear failed")
+    return out
+
+
+def enlarger_develop(record, linear_cmy):
+    """Print density planes C, M, Y from the diffused print-linear exposure."""
+    lib = _o.load()
+    abi = _o._abi()
+    fn = lib.oracle_enlarger_develop
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(abi.FjPreparedHostData)] + [C.c_void_p] * 3 + [C.c_int, C.c_int] + [C.c_void_p] * 3
+    lin = [np.ascontiguousarray(p, dtype=np.float32) for p in linear_cmy]
+    h, w = lin[0].shape
+    out = [np.zeros((h, w), np.float32) for _ in range(3)]
+    if fn(record.pointer(), *[C.c_void_p(p.ctypes.data) for p in lin], w, h, *[C.c_void_p(p.ctypes.data) for p in out]):
+        raise RuntimeError("oracle_enlarger_develop failed")
+    return out
+
+
+class print_done:
+    """Within the block the oracle's render entry points scan the density planes as
+    print density (after the enlarger diffusion), without the print step."""
+
+    def __enter__(self):
+        _o.load().oracle_set_print_done(1)
+        return self
+
+    def __exit__(self, *exc):
+        _o.load().oracle_set_print_done(0)
+
+
+def reference_enlarger(torch, record, stage, planes, dust=None):
+    """The reference's own enlarger kernels on device copies of `planes`: stage 0 the
+    print-linear exposure of density planes C, M, Y, stage 1 the print density of
+    diffused linear planes. None when the harness is not built."""
+    lib = _o.load_reference()
+    if lib is None or not hasattr(lib, "ref_enlarger"):
+        return None
+    abi = _o._abi()
+    fn = lib.ref_enlarger
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(abi.FjPreparedHostData), C.POINTER(C.c_void_p), C.c_int] + [C.c_void_p] * 4 + \
+        [C.c_int, C.c_int] + [C.c_void_p] * 3
+    lut = _o.scanner_lut_for(record)
+    ptrs = (C.c_void_p * 6)(*[o.ctypes.data for o in lut])
+    dev = [torch.from_numpy(np.ascontiguousarray(p, dtype=np.float32)).cuda() for p in planes]
+    h, w = dev[0].shape
+    out = [torch.zeros((h, w), device="cuda") for _ in range(3)]
+    dd = torch.from_numpy(np.ascontiguousarray(dust, dtype=np.float32)).cuda() if dust is not None else None
+    rc = fn(record.pointer(), ptrs, stage, *[C.c_void_p(t.data_ptr()) for t in dev],
+            C.c_void_p(dd.data_ptr()) if dd is not None else None, w, h, *[C.c_void_p(t.data_ptr()) for t in out])
+    if rc != 0:
+        raise RuntimeError(f"reference enlarger stage returned {rc}")
+    return [t.cpu().numpy() for t in out]

@@ -457,12 +457,9 @@ static unsigned capture_density(const Pack* p, const float* e_in, float* d) {
 }
 
 /* :866-1071 (FP32, same accumulation order as the reference loop) */
-static void print_stage_dust(const Pack* p, float* D, float dust);
-static void print_stage(const Pack* p, float* D) { print_stage_dust(p, D, 1.0f); }
-
-/* src/Cuda/JuicerCudaDeviceHelpers.cuh:1047-1070: `dust` scales the spectral raw print
- * exposure before the exposure scales */
-static void print_stage_dust(const Pack* p, float* D, float dust) {
+/* The print's spectral integral raw_c = sum_l 10^-D(l) I(l) S_c(l) with the reference's
+ * NaN-sensitivity skips (src/Cuda/JuicerCudaDeviceHelpers.cuh:866-933). */
+static void print_spectral_raw(const Pack* p, const float* D, float raw[3]) {
     float ac = 0, am = 0, ay = 0;
     for (int i = 0; i < NL; ++i) {
         float sC = p->psens[i * 3], sM = p->psens[i * 3 + 1], sY = p->psens[i * 3 + 2];
@@ -476,7 +473,19 @@ static void print_stage_dust(const Pack* p, float* D, float dust) {
         if (aM) am += e * sM;
         if (aY) ay += e * sY;
     }
-    float raw[3] = {ac, am, ay};
+    raw[0] = ac;
+    raw[1] = am;
+    raw[2] = ay;
+}
+
+static void print_stage_dust(const Pack* p, float* D, float dust);
+static void print_stage(const Pack* p, float* D) { print_stage_dust(p, D, 1.0f); }
+
+/* src/Cuda/JuicerCudaDeviceHelpers.cuh:1047-1070: `dust` scales the spectral raw print
+ * exposure before the exposure scales */
+static void print_stage_dust(const Pack* p, float* D, float dust) {
+    float raw[3];
+    print_spectral_raw(p, D, raw);
     if (dust != 1.0f)
         for (int c = 0; c < 3; ++c) raw[c] *= dust;
     for (int c = 0; c < 3; ++c) raw[c] *= p->midgray;
@@ -673,6 +682,12 @@ typedef struct {
     float* lut_store;
 } Packed;
 
+/* 1 while the density planes handed to the render entry points already hold print
+ * density (after the enlarger diffusion): the scan then runs without the print step.
+ * Set by oracle_set_print_done; the oracle's Python wrappers reset it after the call. */
+static int g_print_done = 0;
+void oracle_set_print_done(int v) { g_print_done = v; }
+
 static int pack(const FjPreparedHostData* h, Packed* out) {
     memset(out, 0, sizeof(*out));
     Pack* p = &out->p;
@@ -712,7 +727,7 @@ static int pack(const FjPreparedHostData* h, Packed* out) {
             p->dirc[d] = (Curve){dir->compensated_axes_rgb[2 - d].data, dv->density_rgb.data + (2 - d), 3, n};
         }
     }
-    p->print = h->route == FJ_ROUTE_NEGATIVE_PRINT || h->route == FJ_ROUTE_POSITIVE_PRINT;
+    p->print = (h->route == FJ_ROUTE_NEGATIVE_PRINT || h->route == FJ_ROUTE_POSITIVE_PRINT) && !g_print_done;
     if (p->print) {
         const FjPrint* pr = &h->print;
         p->eps_c_src = pr->film_density_cmy.data;
@@ -1641,6 +1656,58 @@ int oracle_diffusion(const double* lambda_px, const double* weights /* [3][9] R,
             }
     }
     free(psf);
+    return 0;
+}
+
+/* ---------------- enlarger diffusion (src/Cuda/Scan/JuicerCudaScanPipeline.cu:1392-1488) ----------------
+ * Print-linear exposure of capture density planes: the spectral integral of the print
+ * stage times the dust transmittance and the mid-grey normaliser, plus preflash, then
+ * (max(raw, 0) + 1e-10) x print exposure x route correction
+ * (src/Cuda/JuicerCudaDeviceHelpers.cuh:966-1010); planes C-, M-, Y-forming out. */
+int oracle_enlarger_linear(const FjPreparedHostData* h, const float* dc, const float* dm, const float* dy,
+                           const float* dust, int W, int H, float* lc, float* lm, float* ly) {
+    Packed pk;
+    if (pack(h, &pk) || !pk.p.print) {
+        free(pk.lut_store);
+        return 1;
+    }
+    const Pack* p = &pk.p;
+    const float outer = p->print_exposure * p->print_route;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)W * H; ++i) {
+        float D[3] = {dc[i], dm[i], dy[i]}, raw[3];
+        print_spectral_raw(p, D, raw);
+        float t = dust ? dust[i] : 1.0f;
+        if (t != 1.0f)
+            for (int c = 0; c < 3; ++c) raw[c] *= t;
+        for (int c = 0; c < 3; ++c) raw[c] *= p->midgray;
+        if (p->preflash > 0.0f)
+            for (int c = 0; c < 3; ++c) raw[c] += p->preflash_raw[c] * p->preflash;
+        lc[i] = (fmaxf(raw[0], 0.0f) + 1e-10f) * outer;
+        lm[i] = (fmaxf(raw[1], 0.0f) + 1e-10f) * outer;
+        ly[i] = (fmaxf(raw[2], 0.0f) + 1e-10f) * outer;
+    }
+    free(pk.lut_store);
+    return 0;
+}
+
+/* Print density C, M, Y from the diffused print-linear exposure: log10(max(v, 0) +
+ * 1e-10) on the print curves (:1449-1488, src/Cuda/JuicerCudaDeviceHelpers.cuh:1025). */
+int oracle_enlarger_develop(const FjPreparedHostData* h, const float* lc, const float* lm, const float* ly, int W,
+                            int H, float* dc, float* dm, float* dy) {
+    Packed pk;
+    if (pack(h, &pk) || !pk.p.print) {
+        free(pk.lut_store);
+        return 1;
+    }
+    const Pack* p = &pk.p;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)W * H; ++i) {
+        const float v[3] = {lc[i], lm[i], ly[i]};
+        float* out[3] = {dc, dm, dy};
+        for (int c = 0; c < 3; ++c) out[c][i] = curve_at(&p->pdc[c], log10f(fmaxf(v[c], 0.0f) + 1e-10f), 1.0f);
+    }
+    free(pk.lut_store);
     return 0;
 }
 

@@ -954,3 +954,59 @@ extern "C" int ref_auto_exposure(const FjPreparedHostData* h, const float* const
     if (e == cudaSuccess) e = cudaMemcpy(scale_out, d_scale, sizeof(float), cudaMemcpyDeviceToHost);
     return e == cudaSuccess ? 0 : 1000 + (int)e;
 }
+
+// ---------------------------------------------------------------------------
+// Enlarger diffusion stages with the reference's launchers
+// (src/Cuda/Scan/JuicerCudaScanPipeline.cu:2924 print-linear exposure, :2943 print
+// development from the diffused planes). stage 0: density planes in0..2 (C, M, Y) ->
+// linear planes out0..2 (C-, M-, Y-forming), dust may be NULL; stage 1: linear planes
+// in0..2 -> print density out0..2. Device pointers, width-stride planes. Synchronous.
+// ---------------------------------------------------------------------------
+extern "C" cudaError_t juicer_cuda_print_focused_enlarger_linear_exposure(
+    const JuicerCuda::PrintPipelineRunParams*, const float*, const float*, const float*,
+    JuicerCuda::EnlargerPrintLinearExposurePlanes, const float*, void*);
+extern "C" cudaError_t juicer_cuda_print_focused_develop_from_enlarger_linear(
+    const JuicerCuda::PrintPipelineRunParams*, JuicerCuda::EnlargerPrintLinearExposurePlanes, float*, float*, float*,
+    void*);
+
+extern "C" int ref_enlarger(const FjPreparedHostData* h, const float* const* lut, int stage, float* in0, float* in1,
+                            float* in2, const float* dust, int width, int height, float* out0, float* out1,
+                            float* out2) {
+    Arena a;
+    unsigned* d_flags = nullptr;
+    if (cudaMalloc(&d_flags, sizeof(unsigned)) != cudaSuccess) return 2;
+    cudaMemset(d_flags, 0, sizeof(unsigned));
+    a.ptrs.push_back(d_flags);
+    JuicerCuda::PipelineRunParams p;
+    if (!pack(*h, lut, a, p, d_flags)) return 1;
+    JuicerCuda::PrintPipelineRunParams q{};
+    q.src = in0;
+    q.srcRowBytes = (size_t)width * sizeof(float);
+    q.dst = out0;
+    q.dstRowBytes = (size_t)width * sizeof(float);
+    q.width = width;
+    q.height = height;
+    q.nComponents = 3;
+    q.filmExpose = p.filmExpose;
+    q.filmDevelop = p.filmDevelop;
+    q.printExpose = p.printExpose;
+    q.printDevelop = p.printDevelop;
+    q.scanStage = p.scanStage;
+    q.filmRaw = p.filmRaw;
+    JuicerCuda::EnlargerPrintLinearExposurePlanes planes{};
+    planes.rowStrideFloats = (size_t)width;
+    cudaError_t e;
+    if (stage == 0) {
+        planes.redSensitiveCForming = out0;
+        planes.greenSensitiveMForming = out1;
+        planes.blueSensitiveYForming = out2;
+        e = juicer_cuda_print_focused_enlarger_linear_exposure(&q, in0, in1, in2, planes, dust, nullptr);
+    } else {
+        planes.redSensitiveCForming = in0;
+        planes.greenSensitiveMForming = in1;
+        planes.blueSensitiveYForming = in2;
+        e = juicer_cuda_print_focused_develop_from_enlarger_linear(&q, planes, out0, out1, out2, nullptr);
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return (int)e;
+}

@@ -94,11 +94,11 @@ def test_unsupported_stages_and_partial_windows_are_rejected(torch_cuda, recipes
     with runtime.Owner() as owner:
         with pytest.raises(runtime.FjError, match="complete frame"):
             owner.render(rec, src, d, window=(2, 2, w, h))
-        rec.host.h.optics.flags |= abi.FJ_OPTICS_ENLARGER_DIFFUSION
-        with pytest.raises(runtime.FjError, match="enlarger diffusion") as e:
-            owner.render(rec, src, d)
+        direct = frame_records.FrameRecord(recipes["direct"], w, h, grain=False, spatial_dir=False)
+        direct.host.h.optics.flags |= abi.FJ_OPTICS_ENLARGER_DIFFUSION
+        with pytest.raises(runtime.FjError, match="enlarger diffusion needs a print route") as e:
+            owner.render(direct, src, d)
         assert e.value.status.category == abi.FJ_STATUS_UNSUPPORTED_INPUT
-        rec.host.h.optics.flags &= ~abi.FJ_OPTICS_ENLARGER_DIFFUSION
         rec.host.h.scanner_post.flags = 6  # unknown post-effect flags
         rec.host.h.scanner_post.hash = 1
         with pytest.raises(runtime.FjError, match="post effects"):
