@@ -80,7 +80,61 @@ def load_profile(path: str) -> dict:
         out[key] = _nan_array(data[key])
     if "density_curves_layers" in data:
         out["density_curves_layers"] = _nan_array(data["density_curves_layers"])
+    if isinstance(data.get("density_curves_model"), dict):
+        out["density_curves_model"] = data["density_curves_model"]
     return out
+
+
+def density_model_samples(centers, amplitudes, sigmas, log_exposure, positive: bool = False):
+    """The Gaussian-CDF density model of a profile (model_type "norm_cdfs") sampled on a
+    log-exposure axis, as the reference's host evaluates it
+    (rust/film-juicer-core/src/profile.rs:482-520): per channel c and layer l, in FP32,
+    z = sign (E - center) / sigma, cdf = 0.5 erfc(-z / sqrt 2), value = amplitude cdf,
+    totals summed over the layers in layer order. Coefficient matrices are
+    [channel][layer] (f64, narrowed to f32); returns totals [n, 3] and layers
+    [n, layer, channel], float32.
+
+    The reference evaluates erfcf from the Rust libm crate (=0.2.15, a port of the
+    musl / FreeBSD single-precision erfc); here erfc is evaluated in FP64 (scipy) and
+    rounded to f32. On the reference's 19 235 frozen samples
+    (tests/profile/fixtures/density-samples.bin) the results are within 4 ulp, 86 %
+    bit-identical (tests/test_density_model.py)."""
+    from scipy.special import erfc
+
+    e = np.asarray(log_exposure, dtype=np.float64).astype(np.float32)
+    sign = np.float32(-1.0 if positive else 1.0)
+    inv_sqrt2 = np.float32(0.7071067811865475244)
+    totals = np.zeros((e.size, 3), np.float32)
+    layers = np.zeros((e.size, 3, 3), np.float32)
+    with np.errstate(over="ignore", invalid="ignore", divide="ignore"):
+        for c in range(3):
+            t = np.zeros(e.size, np.float32)
+            for l in range(3):
+                center = np.float32(centers[c][l])
+                amplitude = np.float32(amplitudes[c][l])
+                sigma = np.float32(sigmas[c][l])
+                z = (sign * (e - center)) / sigma
+                cdf = np.float32(0.5) * erfc(((-z) * inv_sqrt2).astype(np.float64)).astype(np.float32)
+                v = amplitude * cdf
+                layers[:, l, c] = v
+                t = t + v
+            totals[:, c] = t
+    return totals, layers
+
+
+def profile_density_curves(prof: dict):
+    """(totals [n, 3], layers [n, layer, channel]) of a loaded profile: the Gaussian
+    model on the profile's log-exposure axis when the profile carries one (what the
+    reference's host hands over), else the authored curves with their minimum
+    subtracted."""
+    m = prof.get("density_curves_model")
+    if m and m.get("model_type") == "norm_cdfs":
+        positive = prof["info"].get("type") == "positive"
+        return density_model_samples(m["centers"], m["amplitudes"], m["sigmas"], prof["log_exposure"], positive)
+    curves = prof["density_curves"].astype(np.float64)
+    curves = curves - np.nanmin(curves, axis=0, keepdims=True)
+    layers = prof.get("density_curves_layers")
+    return curves.astype(np.float32), (np.asarray(layers, np.float32) if layers is not None else None)
 
 
 def load_spectrum_csv(path: str) -> np.ndarray:
@@ -203,8 +257,8 @@ def prepare_recipe(resources: str, film: str, paper: str | None = None, *, dir_a
     route_scale = float(1.0 / g_grey)
 
     log_e = prof["log_exposure"].astype(np.float64)
-    curves = prof["density_curves"].astype(np.float64)
-    curves = curves - np.nanmin(curves, axis=0, keepdims=True)
+    model_totals, model_layers = profile_density_curves(prof)
+    curves = model_totals.astype(np.float64)
     n = log_e.size
 
     a: dict[str, np.ndarray] = {}
@@ -214,9 +268,9 @@ def prepare_recipe(resources: str, film: str, paper: str | None = None, *, dir_a
     a["tc_lut"] = f32(tc)
     a["log_exposure"] = f32(log_e)
     a["density_rgb"] = f32(curves)
-    if "density_curves_layers" in prof:
-        # sublayer curves [sample][layer][channel] as authored (the grain's layer model)
-        a["density_layers"] = f32(prof["density_curves_layers"])
+    if model_layers is not None:
+        # sublayer curves [sample][layer][channel] (the grain's layer model)
+        a["density_layers"] = f32(model_layers)
     s["route_correction_scale"] = route_scale
     s["manual_exposure_ev"] = exposure_ev
     # Mallett 2019 reconstruction tables (81 x 3 basis, the film's reference
@@ -286,8 +340,7 @@ def prepare_recipe(resources: str, film: str, paper: str | None = None, *, dir_a
             ym = np.clip(ym - np.linalg.solve(jac, err), 0.0, 0.99)
         raw, ill = raw_for(ym)
         ple = pp["log_exposure"].astype(np.float64)
-        pcurves = pp["density_curves"].astype(np.float64)
-        pcurves = pcurves - np.nanmin(pcurves, axis=0, keepdims=True)
+        pcurves = profile_density_curves(pp)[0].astype(np.float64)
         # Mid-grey negative lands on the paper's speed point (log exposure 0 on this axis).
         a["print_film_density_cmy"] = f32(neg_dyes)
         a["print_film_base_density"] = f32(neg_base)

@@ -20,6 +20,11 @@ container, where the reference is mounted read-only).
   (tests/grain/frame-fixtures/linux-release.json): inputs and exact native output
   fields of every successful case, and the gaussian / energy / period primitives.
 * wang_lut.json: the Wang tile index table of Resources/Noise/Wang/tiles.json.
+* density_model_cases.npz: the reference's density-model characterization
+  (tests/profile/fixtures/density.json + density-samples.bin): per case with frozen
+  samples, the model's centre / amplitude / sigma f64 bits ([channel][layer]), the
+  polarity, the log-exposure axis (f64 bits) and the 49-byte sample records (validity
+  byte, then totals C, M, Y and layers [layer][channel] as f32 bits).
 * output_encoding_cases.json: the reference's frozen output-encoding table
   (tests/scanner/output_encoding_native.inc): per output colour space index, the CCTF
   kind, its six f32 parameters (gamma, a, b, c, d, linear cutoff) and the DWG-to-output
@@ -269,6 +274,31 @@ def gamut_cases():
     print("gamut cases:", [(r["tag"], r["variant"], r["ok"]) for r in rows])
 
 
+def density_model_cases():
+    fx = os.path.join(REF, "tests", "profile", "fixtures")
+    with open(os.path.join(fx, "density.json")) as fh:
+        d = json.load(fh)
+    with open(os.path.join(fx, "density-samples.bin"), "rb") as fh:
+        raw = fh.read()
+    out, names = {}, []
+    for k, case in enumerate(d["cases"]):
+        if case.get("sample_start") is None or case.get("model") is None:
+            continue
+        axis = d["axes"][case["axis"]]
+        n = len(axis)
+        name = f"c{k:03d}"
+        names.append(name)
+        m = case["model"]
+        out[f"{name}__model"] = np.array([m["centers"], m["amplitudes"], m["sigmas"]], dtype=np.uint64)
+        out[f"{name}__positive"] = np.array([1 if case["positive"] else 0], dtype=np.uint8)
+        out[f"{name}__axis"] = np.array(axis, dtype=np.uint64)
+        s0 = case["sample_start"] * 49
+        out[f"{name}__records"] = np.frombuffer(raw[s0:s0 + n * 49], dtype=np.uint8).reshape(n, 49).copy()
+    out["names"] = np.array(names)
+    np.savez_compressed(os.path.join(HERE, "density_model_cases.npz"), **out)
+    print("density model cases:", len(names))
+
+
 def output_encoding_cases():
     import re
 
@@ -346,6 +376,7 @@ if __name__ == "__main__":
     effects_cases()
     tc_lut_cases()
     gamut_cases()
+    density_model_cases()
     output_encoding_cases()
     abi_layout()
     recipes()
