@@ -461,7 +461,7 @@ def run_b200(args):
         roof["kernel_stage"] = dominant
         roof["stage_ms"] = stages[dominant]
         traffic = None
-        prof = os.path.join(ROOT, "profiles", "frame_stages_4k.json")
+        prof = os.path.join(ROOT, "profiles", "stage_traffic_4k.json")
         if os.path.exists(prof):
             with open(prof) as fh:
                 traffic = json.load(fh).get(dominant, {}).get("dram_bytes_per_launch")
