@@ -68,6 +68,14 @@ _EXPORTS = {
     "fjb_recipe_set_exposure_scale_device": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
     "fjb_recipe_clear_flags": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
     "fjb_recipe_set_print_form": (abi.FjStatus, [C.c_void_p, C.c_int32, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_fit_defaults": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams), C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_fit_forward": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams), C.c_void_p, C.c_ssize_t, C.c_uint32,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
+                                       C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_fit_scratch_bytes": (C.c_size_t, []),
+    "fjb_fit_vjp": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams), C.c_void_p, C.c_ssize_t, C.c_uint32,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                   C.c_size_t, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
     "fjb_enlarger_linear_exposure": (abi.FjStatus, [C.c_void_p] + [C.c_void_p] * 7 + [C.c_int32, C.c_int32, C.c_void_p,
                                                                                        C.POINTER(abi.FjErrorBuffer)]),
     "fjb_enlarger_develop": (abi.FjStatus, [C.c_void_p] + [C.c_void_p] * 6 + [C.c_int32, C.c_int32, C.c_void_p,

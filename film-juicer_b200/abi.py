@@ -278,6 +278,12 @@ FjbScannerLutInput = _s("FjbScannerLutInput", [
 # print forms of the 81-wavelength contraction (fjb_recipe_set_print_form)
 FJB_PRINT_FP32, FJB_PRINT_TENSOR, FJB_PRINT_TENSOR_SPLIT = 0, 1, 2
 
+FjbFitParams = _s("FjbFitParams", [("exposure_ev", f32 * 3), ("film_gamma", f32 * 3), ("print_gamma", f32 * 3),
+                                   ("donor_k", f32 * 3), ("print_ev", f32)])
+FJB_FIT_PARAM_NAMES = ["exposure_ev_b", "exposure_ev_g", "exposure_ev_r", "film_gamma_b", "film_gamma_g",
+                       "film_gamma_r", "print_gamma_c", "print_gamma_m", "print_gamma_y", "donor_k_b", "donor_k_g",
+                       "donor_k_r", "print_ev"]
+
 ALL_RECORDS = [
     FjStatus, FjRenderOutcome, FjErrorBuffer, FjStringView, FjFloatSpan, FjByteSpan, FjCudaContext, FjRect,
     FjExtent, FjImage, FjEffectsGeometry, FjFrame, FjSubmission, FjAbortCallback, FjAutoExposure,
@@ -285,7 +291,7 @@ ALL_RECORDS = [
     FjScannerCorrection, FjScannerPostEffects, FjOutputEncoding, FjOutputColor, FjPrint, FjDiffusion,
     FjHalationGaussian, FjHalationChannel, FjScatterHalation, FjHighlightBoost, FjOptics, FjDirGaussian,
     FjSpatialDir, FjGrainGaussian, FjVisualGrain, FjDust, FjScratch, FjDefectOrigin, FjFilmEffects,
-    FjStaticNoise, FjPreparedHostData, FjbScannerLutInput, FjDiffusionComponents, FjbStageTimes,
+    FjStaticNoise, FjPreparedHostData, FjbScannerLutInput, FjDiffusionComponents, FjbStageTimes, FjbFitParams,
 ]
 
 

@@ -77,6 +77,37 @@ FjStatus fjb_render_from_print_density(FjbRecipe* recipe, const float* density_c
                                        ptrdiff_t dst_row_bytes, int32_t width, int32_t height, uint32_t components,
                                        void* stream, FjErrorBuffer* error);
 
+/* Parameter fitting (no counterpart in the reference, which renders only): the
+ * per-pixel chain of the recipe (camera exposure, film curves, runtime DIR, print
+ * exposure and curves on the print route, scanner LUT, correction and colour
+ * matrices) as a function of the parameters below, with its output the scanner's
+ * linear output RGB (before output gamut compression and encoding), and the
+ * hand-written adjoint of that chain. The default parameters (fjb_fit_defaults)
+ * reproduce the recipe. Channel orders: exposure_ev, film_gamma, donor_k B, G, R;
+ * print_gamma C, M, Y. */
+typedef struct FjbFitParams {
+    float exposure_ev[3]; /* film exposure of each layer times 2^ev */
+    float film_gamma[3];  /* gamma factor of the film and compensated curves */
+    float print_gamma[3]; /* gamma factor of the print curves (1 = the recipe's) */
+    float donor_k[3];     /* negative-donor Langmuir knee (> 0) */
+    float print_ev;       /* print exposure times 2^ev */
+} FjbFitParams;
+FjStatus fjb_fit_defaults(FjbRecipe* recipe, FjbFitParams* out, FjErrorBuffer* error);
+/* Linear output RGB planes of the source image (NaN where the chain rejects a pixel). */
+FjStatus fjb_fit_forward(FjbRecipe* recipe, const FjbFitParams* params, const float* src, ptrdiff_t src_row_bytes,
+                         uint32_t components, float* out_r, float* out_g, float* out_b, int32_t width, int32_t height,
+                         void* stream, FjErrorBuffer* error);
+/* grad_params[13] (device, FP64, FjbFitParams order) = sum over pixels of
+ * grad_rgb^T d rgb / d params: the adjoint recomputes each pixel's forward values,
+ * the 81 print transmittances included, instead of storing them. `scratch` holds
+ * fjb_fit_scratch_bytes() bytes of device memory (per-block partial sums, reduced in
+ * a fixed order: the result is deterministic). */
+size_t fjb_fit_scratch_bytes(void);
+FjStatus fjb_fit_vjp(FjbRecipe* recipe, const FjbFitParams* params, const float* src, ptrdiff_t src_row_bytes,
+                     uint32_t components, const float* grad_r, const float* grad_g, const float* grad_b,
+                     int32_t width, int32_t height, double* grad_params, void* scratch, size_t scratch_bytes,
+                     void* stream, FjErrorBuffer* error);
+
 /* Device error word (bit 0 scan failure, bit 8 DIR failure, bits 9..11 DIR
  * channels B,G,R, bit 16 a tensor-core wait of the print stage gave up). Cleared by fjb_recipe_clear_flags, read by fjb_recipe_read_flags
  * (which synchronises `stream`). */

@@ -810,7 +810,11 @@ static int pack(const FjPreparedHostData* h, Packed* out) {
 
 /* Stage selector: 0 = source -> encoded output; 1 = source -> capture density planes;
  * 2 = density planes -> encoded output; 3 = source -> camera exposure planes (B,G,R, no
- * route correction); 4 = carrier planes -> encoded output. */
+ * route correction); 4 = carrier planes -> encoded output; 5 = carrier planes -> capture
+ * density planes; 6 = source -> camera exposure planes with the route correction (the
+ * film exposure the capture development takes); 7 = source -> the scanner's linear
+ * output RGB planes R, G, B (before output gamut compression and encoding; NaN where the
+ * scan fails). */
 int oracle_render(const FjPreparedHostData* h, int stage, const float* src, long src_row_floats, int width,
                   int height, int comps, float* dst, long dst_row_floats, float* p0, float* p1, float* p2,
                   float auto_scale, int threads, unsigned* flags_out) {
@@ -821,6 +825,8 @@ int oracle_render(const FjPreparedHostData* h, int stage, const float* src, long
         return rc;
     }
     const Pack* p = &pk.p;
+    Pack linear_pack = pk.p; /* stage 7: the scan without output gamut compression */
+    linear_pack.gamut = 0;
     unsigned flags = 0;
 #if defined(_OPENMP)
 #pragma omp parallel for schedule(dynamic, 4) num_threads(threads > 0 ? threads : 1) reduction(| : flags)
@@ -848,7 +854,7 @@ int oracle_render(const FjPreparedHostData* h, int stage, const float* src, long
             } else {
                 float e[3];
                 film_exposure(p, s, auto_scale, stage == 3 ? 0 : 1, e);
-                if (stage == 3) {
+                if (stage == 3 || stage == 6) {
                     p0[i] = e[0];
                     p1[i] = e[1];
                     p2[i] = e[2];
@@ -864,6 +870,15 @@ int oracle_render(const FjPreparedHostData* h, int stage, const float* src, long
                 continue;
             }
             if (p->print) print_stage(p, D);
+            if (stage == 7) {
+                double lin[3];
+                const int ok = scan_lin(&linear_pack, D, lin, -1.0f);
+                if (!ok) flags |= 1u;
+                p0[i] = ok ? (float)lin[0] : nanf("");
+                p1[i] = ok ? (float)lin[1] : nanf("");
+                p2[i] = ok ? (float)lin[2] : nanf("");
+                continue;
+            }
             double rgb[3];
             float* o = dst + (size_t)y * dst_row_floats + (size_t)x * comps;
             if (!scan_out(p, D, rgb)) {
@@ -3123,5 +3138,80 @@ int oracle_gate_mask(const FjFilmEffects* e, float* mask, int W, int H) {
     od_family(e, 3, 0, 0, W, H, 2.0f, s);
     for (size_t i = 0; i < (size_t)W * H; ++i) mask[i] *= s[i];
     free(s);
+    return 0;
+}
+
+/* ---------------- tables of the parameter-fitting chain ----------------
+ * The packed tables (as the render packs them) that an FP64 transcription of the
+ * per-pixel chain needs: capture curves on the shared log-exposure axis and the DIR
+ * compensated axes (B, G, R), the DIR matrix, reference densities and donor knees in
+ * the same index space, the print's spectral tables and curves, the scan bounds,
+ * correction and colour matrices. The scanner LUT is the one oracle_scanner_lut builds
+ * from the same record. Returns 0, or 1 when a curve holds more than
+ * ORACLE_FIT_MAX_SAMPLES samples, 2 when packing fails. */
+#define ORACLE_FIT_MAX_SAMPLES 1024
+typedef struct {
+    int32_t n, dir_mode, print, np, medium_negative, res, corr_active, pad;
+    float log_exposure[ORACLE_FIT_MAX_SAMPLES];
+    float density_bgr[3][ORACLE_FIT_MAX_SAMPLES];
+    float axes_bgr[3][ORACLE_FIT_MAX_SAMPLES];
+    float gamma_bgr[3], dir_m[9], dir_dref[3], dir_k[3];
+    float eps_cmy[NL * 3], base[NL], illuminant[NL], sens_cmy[NL * 3];
+    float midgray, preflash, preflash_raw[3], print_exposure, print_route;
+    float print_log_exposure[ORACLE_FIT_MAX_SAMPLES];
+    float print_density_cmy[3][ORACLE_FIT_MAX_SAMPLES];
+    float min_cmy[3], inv_cmy[3], corr_slope, corr_offset, cat02[9], xyz_to_rgb[9];
+} OracleFitTables;
+
+int oracle_fit_tables(const FjPreparedHostData* h, OracleFitTables* t) {
+    Packed pk;
+    memset(t, 0, sizeof(*t));
+    if (pack(h, &pk)) {
+        free(pk.lut_store);
+        return 2;
+    }
+    const Pack* p = &pk.p;
+    free(pk.lut_store);
+    const int n = p->dens[0].n;
+    if (n > ORACLE_FIT_MAX_SAMPLES) return 1;
+    t->n = n;
+    t->dir_mode = p->dir_mode;
+    t->print = p->print;
+    t->medium_negative = p->medium_negative;
+    t->res = p->res;
+    t->corr_active = p->corr_active;
+    for (int i = 0; i < n; ++i) t->log_exposure[i] = p->dens[0].x[i];
+    for (int c = 0; c < 3; ++c) {
+        t->gamma_bgr[c] = p->gamma_bgr[c];
+        for (int i = 0; i < n; ++i) t->density_bgr[c][i] = p->dens[c].y[(size_t)i * p->dens[c].ystride];
+        if (p->dir_mode != FJ_DIR_INACTIVE)
+            for (int i = 0; i < n; ++i) t->axes_bgr[c][i] = p->dirc[c].x[i];
+        t->dir_dref[c] = p->dref[c];
+        t->dir_k[c] = p->dk[c];
+        t->min_cmy[c] = p->min_cmy[c];
+        t->inv_cmy[c] = p->inv_cmy[c];
+    }
+    memcpy(t->dir_m, p->M, sizeof(t->dir_m));
+    if (p->print) {
+        const int np = p->pdc[0].n;
+        if (np > ORACLE_FIT_MAX_SAMPLES) return 1;
+        t->np = np;
+        for (int i = 0; i < np; ++i) t->print_log_exposure[i] = p->pdc[0].x[i];
+        for (int c = 0; c < 3; ++c)
+            for (int i = 0; i < np; ++i) t->print_density_cmy[c][i] = p->pdc[c].y[(size_t)i * p->pdc[c].ystride];
+        memcpy(t->eps_cmy, p->eps_c_src, sizeof(t->eps_cmy));
+        memcpy(t->base, p->base_src, sizeof(t->base));
+        memcpy(t->illuminant, p->pillum, sizeof(t->illuminant));
+        memcpy(t->sens_cmy, p->psens, sizeof(t->sens_cmy));
+        t->midgray = p->midgray;
+        t->preflash = p->preflash;
+        memcpy(t->preflash_raw, p->preflash_raw, sizeof(t->preflash_raw));
+        t->print_exposure = p->print_exposure;
+        t->print_route = p->print_route;
+    }
+    t->corr_slope = p->corr_slope;
+    t->corr_offset = p->corr_offset;
+    memcpy(t->cat02, p->cat02, sizeof(t->cat02));
+    memcpy(t->xyz_to_rgb, p->xyz_rgb, sizeof(t->xyz_to_rgb));
     return 0;
 }

@@ -124,7 +124,10 @@ def render(record, src, *, stage: int = 0, planes=None, auto_scale: float = 1.0,
     stage 1: source -> capture density planes (returns 3 planes C, M, Y);
     stage 2: density planes -> encoded output; stage 3: source -> camera exposure
     planes B, G, R; stage 4: carrier planes B, G, R -> encoded output; stage 5:
-    carrier planes B, G, R -> capture density planes C, M, Y.
+    carrier planes B, G, R -> capture density planes C, M, Y; stage 6: source -> camera
+    exposure planes B, G, R with the route correction; stage 7: source -> the scanner's
+    linear output RGB planes (before output gamut compression and encoding, NaN where
+    the scan fails).
     Returns (result, flags).
     """
     import numpy as np
@@ -146,7 +149,7 @@ def render(record, src, *, stage: int = 0, planes=None, auto_scale: float = 1.0,
                            auto_scale, threads, C.byref(flags))
     if rc != 0:
         raise RuntimeError(f"oracle_render failed with code {rc}")
-    if stage in (1, 3, 5):
+    if stage in (1, 3, 5, 6, 7):
         return p, int(flags.value)
     return dst, int(flags.value)
 
