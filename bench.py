@@ -398,6 +398,15 @@ def run_b200(args):
     owner.render(record, src, dst, stream=stream)
     stream.synchronize()
 
+    # ---- differentiation: forward and adjoint of the fitting chain ----
+    # 16 seeded 512 x 512 crops as one 8192 x 512 image (the chain is per pixel), the
+    # bench's print recipe; the cotangent is the gradient of the mean squared error
+    # against the recipe's own render. Forward = fjb_fit_forward, backward = fjb_fit_vjp
+    # (which recomputes the forward); the pixel render of the same crops is timed
+    # beside them. The crops (50 MB in, 50 MB of cotangent) fit in L2: these kernels
+    # are issue-bound, so L2 residency does not change their time.
+    diff = fit_block(torch, prepare, runtime, recipe, args, stream, barrier, max_over_ranks)
+
     # ---- end to end through the C-ABI with host buffers ----
     # Frames are pipelined as a host would: while frame i renders on the render stream,
     # frame i+1's pixels go up on a copy stream and frame i-1's result comes down on
@@ -480,6 +489,7 @@ def run_b200(args):
             "stages_roofline": {k: {"frac": v["frac"], "bound": v["bound"]} for k, v in per_stage.items()},
             "print_forms": {"fp32": {"value": round(value, 2), "ms_per_step": round(ms, 4),
                                      "print_scan_output_ms": stages.get("print_scan_output")}, **forms},
+            "differentiation": diff,
             "cpu_baseline": cpu_baseline(args.cpu_seconds, W, H, args.next_rows) if world == 1 and args.cpu_seconds > 0 else None,
             "e2e": {"value": round(e2e, 2), "unit": "Mpix/s", "h2d_bytes_per_step": int(h_src.numel() * 4),
                     "d2h_bytes_per_step": int(h_dst[0].numel() * 4), "steps": e_steps,
@@ -494,6 +504,61 @@ def run_b200(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def fit_block(torch, prepare, runtime, recipe, args, stream, barrier, max_over_ranks):
+    """Forward, adjoint and pixel-render times on the differentiation workload (16 seeded
+    512 x 512 crops), K steps per timed region, median of 5 regions, max over ranks."""
+    from film_juicer_b200 import fitting
+
+    crops = [prepare.synthetic_frame(512, 512, seed=SEED + 100 + i) for i in range(16)]
+    import numpy as np
+
+    s = torch.from_numpy(np.ascontiguousarray(np.concatenate(crops, axis=0))).to("cuda")
+    dr = runtime.DeviceRecipe(prepare.HostRecord(recipe), stream=stream)
+    th0 = fitting.default_theta(dr)
+    thp = th0.clone()
+    thp[[0, 1, 2, 12]] += torch.tensor([0.1, -0.05, 0.08, -0.1], dtype=torch.float64)
+    with torch.cuda.stream(stream):
+        target = fitting.forward(dr, th0, s, stream=stream).clone()
+        out = torch.empty_like(target)
+        dst = torch.empty_like(s)
+        gout = torch.empty(fitting.N_PARAMS, dtype=torch.float64, device="cuda")
+    steps = max(3, min(args.steps, 50))
+
+    def timed(fn):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        stream.synchronize()
+        vals = []
+        for _ in range(5):
+            barrier()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(steps):
+                fn()
+            b.record(stream)
+            b.synchronize()
+            vals.append(a.elapsed_time(b) / steps)
+        return max_over_ranks(statistics.median(vals))
+
+    fwd = timed(lambda: fitting.forward(dr, thp, s, out, stream=stream))
+    with torch.cuda.stream(stream):
+        cot = (2.0 / out.numel()) * (out - target)
+    bwd = timed(lambda: fitting.vjp(dr, thp, s, cot, gout, stream=stream))
+    ren = timed(lambda: dr.render(s, dst, stream=stream))
+    stream.synchronize()
+    grad = gout.cpu()
+    dr.close()
+    px = s.shape[0] * s.shape[1]
+    return {"workload": "16 x 512 x 512 seeded crops, print route, 13 parameters (exposure_ev BGR, film_gamma BGR, "
+                        "print_gamma CMY, donor_k BGR, print_ev)",
+            "forward_ms": round(fwd, 4), "adjoint_ms": round(bwd, 4), "fwd_bwd_ms": round(fwd + bwd, 4),
+            "fwd_bwd_over_forward": round((fwd + bwd) / fwd, 3),
+            "pixel_render_ms": round(ren, 4), "fwd_bwd_over_pixel_render": round((fwd + bwd) / ren, 3),
+            "fwd_bwd_mpix_s": round(px / ((fwd + bwd) * 1e-3) / 1e6, 1),
+            "gradient_finite": bool(torch.isfinite(grad).all()), "steps": steps, "regions": 5}
 
 
 def run_precision(args):

@@ -10,7 +10,12 @@ reference's own CUDA kernels (oracle/_ref) and the oracle, through fjb_render_pi
   and DaVinci Intermediate CCTFs with their DWG-to-output matrices;
   src/Cuda/Scan/JuicerCudaScanPipeline.cu:99-152), encoded from DWG.
 Bound: the reference's processor-pixel bound 2e-4 + 3e-4 |ref| per encoded channel,
-and equal error flags."""
+and equal error flags. The pure power CCTF (kind 1, v^gamma) has an unbounded slope at
+black; for it the bound adds a linear-domain allowance of 4e-6 carried through the
+CCTF's slope at the encoded value (OkLch gamut compression of a saturated colour
+leaves a channel near zero as a difference of terms ~1e4 times larger, so FP32
+implementations of it differ there by a few 1e-6 in linear light: the reference's
+CUDA and the oracle differ by as much as this library does)."""
 import ctypes as C
 import json
 import os
@@ -37,6 +42,16 @@ def ref_lib(oracle):
     return lib
 
 
+def _cctf_allowance(rec, mine, ref):
+    """Linear-domain allowance 4e-6 through the slope of a pure power CCTF (kind 1)."""
+    if rec.h.output_color.encoding.cctf_kind != 1 or not (rec.h.output_color.flags & abi.FJ_COLOR_ENCODE_CCTF):
+        return 0.0
+    g = float(rec.h.output_color.encoding.gamma)
+    y = np.maximum(np.maximum(np.abs(ref), np.abs(mine)), 1e-3).astype(np.float64)
+    slope = g * np.power(y, (g - 1.0) / g)  # d(v^g)/dv at v = y^(1/g)
+    return 4e-6 * slope
+
+
 def _check(torch, ref_lib, oracle, rec, src):
     from film_juicer_b200 import runtime
 
@@ -60,6 +75,7 @@ def _check(torch, ref_lib, oracle, rec, src):
     orc, oflags = oracle.render(rec, src)
     assert flags == int(rflags.value) == oflags
     tol = 2e-4 + 3e-4 * np.abs(ref)
+    tol = tol + _cctf_allowance(rec, mine, ref) + _cctf_allowance(rec, orc, ref)
     assert np.all(np.isfinite(mine))
     assert np.all(np.abs(mine - ref) <= tol), float(np.max(np.abs(mine - ref)))
     assert np.all(np.abs(orc - ref) <= tol), float(np.max(np.abs(orc - ref)))
