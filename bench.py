@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--next-rows", action="store_true",
                     help="workload variant: add highlight reconstruction and scanner post effects (glare, lens blur, "
                          "the production unsharp 0.7 px / 0.7)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch block")
     ap.add_argument("--precision", action="store_true",
                     help="instead of timing: one frame against the oracle's stage chain (CIEDE2000 of the output)")
     args = ap.parse_args()
@@ -406,6 +407,8 @@ def run_b200(args):
     # beside them. The crops (50 MB in, 50 MB of cotangent) fit in L2: these kernels
     # are issue-bound, so L2 residency does not change their time.
     diff = fit_block(torch, prepare, runtime, recipe, args, stream, barrier, max_over_ranks)
+    batch = batch_block(torch, frame_records, prepare, owner, args, barrier, max_over_ranks) \
+        if not args.no_batch else None
 
     # ---- end to end through the C-ABI with host buffers ----
     # Frames are pipelined as a host would: while frame i renders on the render stream,
@@ -490,6 +493,7 @@ def run_b200(args):
             "print_forms": {"fp32": {"value": round(value, 2), "ms_per_step": round(ms, 4),
                                      "print_scan_output_ms": stages.get("print_scan_output")}, **forms},
             "differentiation": diff,
+            "batch": batch,
             "cpu_baseline": cpu_baseline(args.cpu_seconds, W, H, args.next_rows) if world == 1 and args.cpu_seconds > 0 else None,
             "e2e": {"value": round(e2e, 2), "unit": "Mpix/s", "h2d_bytes_per_step": int(h_src.numel() * 4),
                     "d2h_bytes_per_step": int(h_dst[0].numel() * 4), "steps": e_steps,
@@ -559,6 +563,67 @@ def fit_block(torch, prepare, runtime, recipe, args, stream, barrier, max_over_r
             "pixel_render_ms": round(ren, 4), "fwd_bwd_over_pixel_render": round((fwd + bwd) / ren, 3),
             "fwd_bwd_mpix_s": round(px / ((fwd + bwd) * 1e-3) / 1e6, 1),
             "gradient_finite": bool(torch.isfinite(grad).all()), "steps": steps, "regions": 5}
+
+
+BATCH_FRAMES = [(1920, 1080)] * 8 + [(3840, 2160)] * 4 + [(4096, 3072)] * 2
+BATCH_RECIPES = [("recipe_print.npz", 0xB001), ("recipe_gold200_endura.npz", 0xB002),
+                 ("recipe_c200_crystal.npz", 0xB003)]
+
+
+def batch_block(torch, frame_records, prepare, owner, args, barrier, max_over_ranks):
+    """The mixed batch: 8 x 1920x1080, 4 x 3840x2160 and 2 x 4096x3072 frames, three
+    capture stocks on two print papers (assigned in turn), every spatial stage, through
+    fjb_render_batch on one stream -- eagerly, and replayed from the captured CUDA graph
+    (one launch per batch) -- with diffusion-form autotuning on (on the process's one
+    owner, switched off again after). A step is one whole batch; CUDA events on the
+    batch stream, median of the timed steps, max over ranks."""
+    from film_juicer_b200 import grain_plan
+
+    recipes = [(prepare.PreparedRecipe.load(os.path.join(ROOT, "tests", "golden", f)), h) for f, h in BATCH_RECIPES]
+    noise = grain_plan.synthetic_noise()
+    recs, srcs, dsts = [], [], []
+    for i, (w, h) in enumerate(BATCH_FRAMES):
+        rcp, rh = recipes[i % len(recipes)]
+        recs.append(frame_records.FrameRecord(rcp, w, h, recipe_hash=rh, noise=noise))
+        srcs.append(torch.from_numpy(prepare.synthetic_frame(w, h, seed=SEED + 200 + i)).to("cuda"))
+        dsts.append(torch.empty_like(srcs[-1]))
+    px = sum(w * h for w, h in BATCH_FRAMES)
+    stream = torch.cuda.Stream()
+    owner.set_autotune(True)
+    steps = max(3, min(args.steps, 5))
+
+    def timed(token):
+        owner.render_batch(recs, srcs, dsts, stream, graph_token=token)  # warm-up (and capture)
+        captured = owner.last_batch_text == ""
+        vals = []
+        for _ in range(steps):
+            barrier()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            owner.render_batch(recs, srcs, dsts, stream, graph_token=token)
+            b.record(stream)
+            b.synchronize()
+            vals.append(a.elapsed_time(b))
+        return max_over_ranks(statistics.median(vals)), captured
+
+    eager_ms, _ = timed(0)
+    graph_ms, captured = timed(0xBA7C4)
+    finite = all(bool(torch.isfinite(d).all()) for d in dsts)
+    forms = {}
+    for w, h in sorted(set(BATCH_FRAMES)):
+        r = recs[BATCH_FRAMES.index((w, h))].host.h.optics.camera.radius_px
+        f = owner.diffusion_form(w, h, r)
+        forms[f"{w}x{h} r={r}"] = {0: "direct", 1: "fft"}.get(f, "undecided")
+    owner.set_autotune(False)
+    return {"workload": "8 x 1920x1080 + 4 x 3840x2160 + 2 x 4096x3072 full optical print frames, stocks "
+                        "kodak_portra_400 / kodak_gold_200 / fujifilm_c200 on papers kodak_portra_endura / "
+                        "fujifilm_crystal_archive_typeii, every spatial stage, one fjb_render_batch per step",
+            "frames": len(BATCH_FRAMES), "mpix_per_batch": round(px / 1e6, 2),
+            "value": round(px / (graph_ms * 1e-3) / 1e6, 2), "unit": "Mpix/s", "ms_per_batch": round(graph_ms, 3),
+            "graph_captured": captured,
+            "eager": {"value": round(px / (eager_ms * 1e-3) / 1e6, 2), "ms_per_batch": round(eager_ms, 3)},
+            "diffusion_forms": forms, "steps": steps, "output_finite": finite}
 
 
 def run_precision(args):

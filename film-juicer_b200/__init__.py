@@ -68,6 +68,12 @@ _EXPORTS = {
     "fjb_recipe_set_exposure_scale_device": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
     "fjb_recipe_clear_flags": (abi.FjStatus, [C.c_void_p, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
     "fjb_recipe_set_print_form": (abi.FjStatus, [C.c_void_p, C.c_int32, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_render_batch": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjCudaContext), C.POINTER(abi.FjFrame),
+                                        C.POINTER(abi.FjSubmission), C.POINTER(C.c_void_p), C.c_int32, C.c_void_p,
+                                        C.c_uint64, C.POINTER(abi.FjRenderOutcome), C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_owner_set_autotune": (abi.FjStatus, [C.c_void_p, C.c_int32, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_owner_diffusion_form": (abi.FjStatus, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                                C.POINTER(abi.FjErrorBuffer)]),
     "fjb_fit_defaults": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams), C.POINTER(abi.FjErrorBuffer)]),
     "fjb_fit_forward": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams), C.c_void_p, C.c_ssize_t, C.c_uint32,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,

@@ -278,6 +278,9 @@ FjbScannerLutInput = _s("FjbScannerLutInput", [
 # print forms of the 81-wavelength contraction (fjb_recipe_set_print_form)
 FJB_PRINT_FP32, FJB_PRINT_TENSOR, FJB_PRINT_TENSOR_SPLIT = 0, 1, 2
 
+FJB_DIFFUSION_DIRECT = 0
+FJB_DIFFUSION_FFT = 1
+
 FjbFitParams = _s("FjbFitParams", [("exposure_ev", f32 * 3), ("film_gamma", f32 * 3), ("print_gamma", f32 * 3),
                                    ("donor_k", f32 * 3), ("print_ev", f32)])
 FJB_FIT_PARAM_NAMES = ["exposure_ev_b", "exposure_ev_g", "exposure_ev_r", "film_gamma_b", "film_gamma_g",

@@ -366,9 +366,22 @@ class Owner:
         err = abi.ErrorText()
         _check("fjb_owner_set_print_form", self.lib.fjb_owner_set_print_form(self.handle, form, C.byref(err.buf)), err)
 
-    def render(self, prepared, src, dst, window=None, stream=None, abort=None, frame_token: int = 0):
-        """src/dst: (H, W, comps) float32 CUDA tensors covering the full frame; returns
-        the FjRenderOutcome (raises on a failed status)."""
+    def set_autotune(self, enable: bool):
+        """Diffusion form autotuning (fjb_owner_set_autotune)."""
+        err = abi.ErrorText()
+        _check("fjb_owner_set_autotune", self.lib.fjb_owner_set_autotune(self.handle, 1 if enable else 0,
+                                                                          C.byref(err.buf)), err)
+
+    def diffusion_form(self, width: int, height: int, radius_px: int) -> int:
+        """The owner's diffusion form decision (FJB_DIFFUSION_*, -1 undecided)."""
+        err = abi.ErrorText()
+        v = C.c_int32()
+        _check("fjb_owner_diffusion_form", self.lib.fjb_owner_diffusion_form(self.handle, width, height, radius_px,
+                                                                              C.byref(v), C.byref(err.buf)), err)
+        return int(v.value)
+
+    @staticmethod
+    def _frame(src, dst, window=None, stream=None):
         h, w, comps = src.shape
         fr = abi.FjFrame()
         for im, t in ((fr.source, src), (fr.destination, dst)):
@@ -382,6 +395,36 @@ class Owner:
         if stream is not None:
             fr.stream = _stream_handle(stream)
             fr.flags |= abi.FJ_FRAME_STREAM_PRESENT
+        return fr
+
+    def render_batch(self, prepared, srcs, dsts, stream, graph_token: int = 0, frame_tokens=None):
+        """fjb_render_batch over lists of records and (H, W, comps) float32 CUDA tensors,
+        on `stream` (a torch.cuda.Stream). Returns the list of FjRenderOutcome (raises on
+        a failed batch status); the diagnostic text is kept in `last_batch_text`."""
+        n = len(prepared)
+        frames = (abi.FjFrame * max(n, 1))()
+        subs = (abi.FjSubmission * max(n, 1))()
+        ptrs = (C.c_void_p * max(n, 1))()
+        for i in range(n):
+            frames[i] = self._frame(srcs[i], dsts[i])
+            subs[i].frame_token = frame_tokens[i] if frame_tokens else 0
+            ptrs[i] = C.cast(prepared[i].pointer(), C.c_void_p)
+        err = abi.ErrorText()
+        ctx = abi.FjCudaContext()
+        if n:
+            _check("fj_cuda_inspect", self.lib.fj_cuda_inspect(self.handle, C.byref(frames[0]), C.byref(ctx),
+                                                               C.byref(err.buf)), err)
+        outs = (abi.FjRenderOutcome * max(n, 1))()
+        st = self.lib.fjb_render_batch(self.handle, C.byref(ctx), frames, subs, ptrs, n,
+                                       C.c_void_p(_stream_handle(stream)), graph_token, outs, C.byref(err.buf))
+        _check("fjb_render_batch", st, err)
+        self.last_batch_text = err.text
+        return [outs[i] for i in range(n)]
+
+    def render(self, prepared, src, dst, window=None, stream=None, abort=None, frame_token: int = 0):
+        """src/dst: (H, W, comps) float32 CUDA tensors covering the full frame; returns
+        the FjRenderOutcome (raises on a failed status)."""
+        fr = self._frame(src, dst, window, stream)
         err = abi.ErrorText()
         ctx = abi.FjCudaContext()
         _check("fj_cuda_inspect", self.lib.fj_cuda_inspect(self.handle, C.byref(fr), C.byref(ctx), C.byref(err.buf)), err)

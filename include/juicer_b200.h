@@ -401,13 +401,44 @@ typedef struct FjbStageTimes {
     double total_ms[FJB_STAGE_COUNT];
     uint64_t frames[FJB_STAGE_COUNT];
 } FjbStageTimes;
-/* Turns stage timing on (enable != 0) or off and resets the totals. */
 /* The print form (FJB_PRINT_*) of every recipe this owner renders, from the next
  * fj_cuda_render on. No counterpart in the reference. */
 FjStatus fjb_owner_set_print_form(FjCuda* cuda, int32_t form, FjErrorBuffer* error);
+/* Turns stage timing on (enable != 0) or off and resets the totals (single frames
+ * through fj_cuda_render; batches are not timed per stage). */
 FjStatus fjb_owner_stage_timing(FjCuda* cuda, int32_t enable, FjErrorBuffer* error);
 /* Totals since the last fjb_owner_stage_timing call. */
 FjStatus fjb_owner_stage_times(FjCuda* cuda, FjbStageTimes* out, FjErrorBuffer* error);
+
+/* Batches of frames (no counterpart in the reference, which renders one frame per
+ * fj_cuda_render call). fjb_render_batch renders `count` frames -- any mix of sizes,
+ * stocks, papers and stage sets, each checked as fj_cuda_render checks it -- in order
+ * on `stream` (the frames' own stream fields are ignored), with one read-back of all
+ * frames' flag words at the end instead of one host round trip per frame.
+ * outcomes[i] is frame i's FjRenderOutcome; the return value is the first failing
+ * frame's status (no work is enqueued when a frame fails its checks).
+ *
+ * graph_token != 0 (and a non-null stream, and every frame with a non-zero
+ * recipe_hash): after the call's own eager render, the batch's work (every launch,
+ * flag copy and the read-back) is captured into a CUDA graph kept by the owner under
+ * that token. A later call with the same token and frame count replays the graph in
+ * one launch: the caller guarantees that the frames' buffers and descriptors are the
+ * ones of the captured call (pixel contents may change). A new token recaptures; the
+ * owner drops the graph whenever a buffer it references is regrown or freed.
+ * submissions may be null (frame tokens 0). */
+FjStatus fjb_render_batch(FjCuda* cuda, const FjCudaContext* context, const FjFrame* frames,
+                          const FjSubmission* submissions, const FjPreparedHostData* const* prepared, int32_t count,
+                          void* stream, uint64_t graph_token, FjRenderOutcome* outcomes, FjErrorBuffer* error);
+/* Diffusion form autotuning (no counterpart in the reference): with enable != 0 the
+ * owner times the direct and the FFT form of camera and enlarger diffusion on the
+ * first frame of each (width, height, radius) and keeps the faster; off (the default),
+ * the fixed size rule chooses. fjb_owner_diffusion_form reports the decision
+ * (FJB_DIFFUSION_*, -1 undecided). */
+#define FJB_DIFFUSION_DIRECT 0
+#define FJB_DIFFUSION_FFT 1
+FjStatus fjb_owner_set_autotune(FjCuda* cuda, int32_t enable, FjErrorBuffer* error);
+FjStatus fjb_owner_diffusion_form(FjCuda* cuda, int32_t width, int32_t height, int32_t radius_px, int32_t* form,
+                                  FjErrorBuffer* error);
 
 /* Kernel launches this library has made in the process so far (all entry points). */
 uint64_t fjb_kernel_launches(void);

@@ -363,6 +363,11 @@ def recipes():
     res = os.path.join(REF, "Resources")
     prepare.prepare_recipe(res, "kodak_portra_400").save(os.path.join(HERE, "recipe_direct.npz"))
     prepare.prepare_recipe(res, "kodak_portra_400", "kodak_portra_endura").save(os.path.join(HERE, "recipe_print.npz"))
+    # the mixed-stock batch: three capture stocks on two print papers
+    prepare.prepare_recipe(res, "kodak_gold_200", "kodak_portra_endura").save(
+        os.path.join(HERE, "recipe_gold200_endura.npz"))
+    prepare.prepare_recipe(res, "fujifilm_c200", "fujifilm_crystal_archive_typeii").save(
+        os.path.join(HERE, "recipe_c200_crystal.npz"))
     print("recipes written")
 
 
