@@ -79,6 +79,13 @@ _EXPORTS = {
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
                                        C.POINTER(abi.FjErrorBuffer)]),
     "fjb_fit_scratch_bytes": (C.c_size_t, []),
+    "fjb_fit_forward_carrier": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams), C.c_void_p, C.c_void_p,
+                                               C.c_void_p, C.c_ssize_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                               C.c_int32, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_fit_vjp_carrier": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams), C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_ssize_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                           C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_size_t, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
     "fjb_fit_vjp": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams), C.c_void_p, C.c_ssize_t, C.c_uint32,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                    C.c_size_t, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),

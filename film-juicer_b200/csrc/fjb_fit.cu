@@ -195,14 +195,16 @@ __device__ __forceinline__ void print_spectral_moments(const PrintSpectral& s, c
 // vector-Jacobian product g_rgb^T d rgb / d theta into g_th (FjbFitParams order).
 // False for a pixel the chain rejects (non-finite values, LUT failure); a rejected
 // pixel adds nothing (every rejection comes before the adjoint part).
-// `dldk` (kGrad with negative-donor DIR): d L(y_d[i], k_d) / d k_d for every donor d
-// and knot i of the compensated curves, [d * n + i].
+// `e0`: the pixel's film exposure B, G, R before the exposure parameters. `dldk` (kGrad
+// with negative-donor DIR): d L(y_d[i], k_d) / d k_d for every donor d and knot i of the
+// compensated curves, [d * n + i]. `g_e0` (kGrad, may be null) receives the gradient
+// with respect to e0.
 template <bool kPrint, bool kGrad>
-__device__ bool fit_pixel(const PixelParams& p, const float* __restrict__ blob, const FitTheta& th, const float in[3],
-                          double rgb[3], const float* g_rgb, FitAcc* g_th, const float* __restrict__ dldk) {
+__device__ bool fit_pixel(const PixelParams& p, const float* __restrict__ blob, const FitTheta& th, const float e0[3],
+                          double rgb[3], const float* g_rgb, FitAcc* g_th, const float* __restrict__ dldk,
+                          float* g_e0) {
     // ---- forward, keeping what the adjoint needs ----
-    float e0[3], e[3], logS[3], layer[3], sl[3];
-    camera_linear_exposure(p, in, true, e0);
+    float e[3], logS[3], layer[3], sl[3];
     for (int c = 0; c < 3; ++c) {
         e[c] = e0[c] * exp2f(th.ev[c]);
         logS[c] = log_exposure(e[c]);
@@ -362,6 +364,7 @@ __device__ bool fit_pixel(const PixelParams& p, const float* __restrict__ blob, 
         g_th[3 + c] += (g_layer[c] * sl[c] * logS[c]);
         const float g_e = e[c] > 0.0f ? g_logS[c] / ((e[c] + 1e-10f) * kLn10) : 0.0f;
         g_th[c] += (g_e * e[c] * kLn2);
+        if (g_e0) g_e0[c] = g_e * exp2f(th.ev[c]);
     }
     return true;
 }
@@ -405,27 +408,52 @@ inline size_t fit_vjp_smem(const PixelParams& p) {
     return ((size_t)fit_blob_floats(p) + 3 * (size_t)n) * sizeof(float);
 }
 
-__device__ __forceinline__ void load_pixel(const PixelParams& p, long long idx, float in[3]) {
+// Carrier-plane input (film exposure B, G, R before the route correction, as the
+// camera exposure stage writes it) and, for the adjoint, the optional gradient planes
+// with respect to it.
+struct FitCarrier {
+    const float* b;
+    const float* g;
+    const float* r;
+    long long stride;
+    float* gb;
+    float* gg;
+    float* gr;
+};
+
+// The film exposure e0 (B, G, R) of pixel idx: from the source RGB through the camera
+// exposure, or from the carrier planes as the capture stage reads them
+// (max(0, carrier x route correction)).
+template <bool kCarrier>
+__device__ __forceinline__ void load_exposure(const PixelParams& p, const FitCarrier& cr, long long idx, float e0[3]) {
     const int y = (int)(idx / p.width), x = (int)(idx - (long long)y * p.width);
-    const float* s = reinterpret_cast<const float*>(p.src + (long long)y * p.src_row_bytes) + (long long)x * p.components;
-    in[0] = s[0];
-    in[1] = s[1];
-    in[2] = s[2];
+    if constexpr (kCarrier) {
+        const long long ci = (long long)y * cr.stride + x;
+        e0[0] = fmaxf(0.0f, cr.b[ci] * p.route_correction_scale);
+        e0[1] = fmaxf(0.0f, cr.g[ci] * p.route_correction_scale);
+        e0[2] = fmaxf(0.0f, cr.r[ci] * p.route_correction_scale);
+    } else {
+        const float* s =
+            reinterpret_cast<const float*>(p.src + (long long)y * p.src_row_bytes) + (long long)x * p.components;
+        const float in[3] = {s[0], s[1], s[2]};
+        camera_linear_exposure(p, in, true, e0);
+    }
 }
 
 // Linear output RGB planes for theta (NaN where the chain rejects a pixel).
-template <bool kPrint>
-__global__ void __launch_bounds__(kFitThreads) fit_forward_kernel(const __grid_constant__ PixelParams p, FitTheta th,
-                                                                  float* out_r, float* out_g, float* out_b) {
+template <bool kPrint, bool kCarrier>
+__global__ void __launch_bounds__(kFitThreads, 2) fit_forward_kernel(const __grid_constant__ PixelParams p, FitTheta th,
+                                                                  FitCarrier cr, float* out_r, float* out_g,
+                                                                  float* out_b) {
     extern __shared__ float4 fit_smem4[];
     const float* blob = stage_blob(p, th, reinterpret_cast<float*>(fit_smem4));
     const long long total = (long long)p.width * p.height;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
-        float in[3];
-        load_pixel(p, idx, in);
+        float e0[3];
+        load_exposure<kCarrier>(p, cr, idx, e0);
         double rgb[3];
-        const bool ok = fit_pixel<kPrint, false>(p, blob, th, in, rgb, nullptr, nullptr, nullptr);
+        const bool ok = fit_pixel<kPrint, false>(p, blob, th, e0, rgb, nullptr, nullptr, nullptr, nullptr);
         out_r[idx] = ok ? (float)rgb[0] : nanf("");
         out_g[idx] = ok ? (float)rgb[1] : nanf("");
         out_b[idx] = ok ? (float)rgb[2] : nanf("");
@@ -434,10 +462,12 @@ __global__ void __launch_bounds__(kFitThreads) fit_forward_kernel(const __grid_c
 
 constexpr int kFitParams = 13;
 
-// Per-block sums (FP64, fixed order) of the pixels' vector-Jacobian products.
-template <bool kPrint>
+// Per-block sums (FP64, fixed order) of the pixels' vector-Jacobian products; with
+// carrier input and gradient planes, also d <g, rgb> / d carrier per pixel (zero where
+// the chain rejects the pixel or the cotangent is zero).
+template <bool kPrint, bool kCarrier>
 __global__ void __launch_bounds__(kFitThreads, 2) fit_vjp_kernel(const __grid_constant__ PixelParams p, FitTheta th,
-                                                              const float* __restrict__ g_r,
+                                                              FitCarrier cr, const float* __restrict__ g_r,
                                                               const float* __restrict__ g_g,
                                                               const float* __restrict__ g_b, double* partials) {
     extern __shared__ float4 fit_smem4[];
@@ -454,15 +484,28 @@ __global__ void __launch_bounds__(kFitThreads, 2) fit_vjp_kernel(const __grid_co
     __shared__ double red[kFitThreads];
     FitAcc acc[kFitParams];
     for (int k = 0; k < kFitParams; ++k) acc[k] = 0.0f;
+    const bool carrier_grad = kCarrier && cr.gb != nullptr;
     const long long total = (long long)p.width * p.height;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
         const float g[3] = {g_r[idx], g_g[idx], g_b[idx]};
-        if (g[0] == 0.0f && g[1] == 0.0f && g[2] == 0.0f) continue;
-        float in[3];
-        load_pixel(p, idx, in);
-        double rgb[3];
-        fit_pixel<kPrint, true>(p, blob, th, in, rgb, g, acc, dldk);
+        float ge[3] = {0.0f, 0.0f, 0.0f};
+        float e0[3] = {0.0f, 0.0f, 0.0f};
+        if (g[0] != 0.0f || g[1] != 0.0f || g[2] != 0.0f) {
+            load_exposure<kCarrier>(p, cr, idx, e0);
+            double rgb[3];
+            if (!fit_pixel<kPrint, true>(p, blob, th, e0, rgb, g, acc, dldk, carrier_grad ? ge : nullptr))
+                ge[0] = ge[1] = ge[2] = 0.0f;
+        }
+        if (carrier_grad) {
+            // e0 = max(0, carrier x route): the route factor inside, zero where clamped
+            const int y = (int)(idx / p.width), x = (int)(idx - (long long)y * p.width);
+            const long long ci = (long long)y * cr.stride + x;
+            const float rc = p.route_correction_scale;
+            cr.gb[ci] = e0[0] > 0.0f ? ge[0] * rc : 0.0f;
+            cr.gg[ci] = e0[1] > 0.0f ? ge[1] * rc : 0.0f;
+            cr.gr[ci] = e0[2] > 0.0f ? ge[2] * rc : 0.0f;
+        }
     }
     for (int k = 0; k < kFitParams; ++k) {
         red[threadIdx.x] = (double)acc[k];
@@ -509,6 +552,50 @@ bool theta_from(const FjbFitParams& f, FitTheta& th) {
 
 } // namespace fjb
 
+namespace fjb {
+namespace {
+
+template <bool kCarrier>
+cudaError_t launch_fit_forward(const PixelParams& p, const FitTheta& th, const FitCarrier& cr, float* out_r,
+                               float* out_g, float* out_b, cudaStream_t s) {
+    const size_t smem = (size_t)p.curve_blob_floats * sizeof(float);
+    count_launch();
+    if (p.route == kRoutePrint) {
+        cudaFuncSetAttribute(fit_forward_kernel<true, kCarrier>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        fit_forward_kernel<true, kCarrier><<<fit_blocks(), kFitThreads, smem, s>>>(p, th, cr, out_r, out_g, out_b);
+    } else {
+        cudaFuncSetAttribute(fit_forward_kernel<false, kCarrier>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        fit_forward_kernel<false, kCarrier><<<fit_blocks(), kFitThreads, smem, s>>>(p, th, cr, out_r, out_g, out_b);
+    }
+    return cudaGetLastError();
+}
+
+template <bool kCarrier>
+cudaError_t launch_fit_vjp(const PixelParams& p, const FitTheta& th, const FitCarrier& cr, const float* grad_r,
+                           const float* grad_g, const float* grad_b, double* partials, double* grad_params,
+                           cudaStream_t s) {
+    const int blocks = fit_blocks();
+    const size_t smem = fit_vjp_smem(p);
+    count_launch();
+    if (p.route == kRoutePrint) {
+        cudaFuncSetAttribute(fit_vjp_kernel<true, kCarrier>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        fit_vjp_kernel<true, kCarrier><<<blocks, kFitThreads, smem, s>>>(p, th, cr, grad_r, grad_g, grad_b, partials);
+    } else {
+        cudaFuncSetAttribute(fit_vjp_kernel<false, kCarrier>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        fit_vjp_kernel<false, kCarrier><<<blocks, kFitThreads, smem, s>>>(p, th, cr, grad_r, grad_g, grad_b, partials);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        count_launch();
+        fit_reduce_kernel<<<1, 32, 0, s>>>(partials, blocks, grad_params);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+} // namespace
+} // namespace fjb
+
 using fjb::cuda_status;
 using fjb::fail_status;
 using fjb::ok_status;
@@ -532,9 +619,9 @@ FjStatus fjb_fit_defaults(FjbRecipe* recipe, FjbFitParams* out, FjErrorBuffer* e
     return ok_status();
 }
 
-static FjStatus fit_check(FjbRecipe* recipe, const FjbFitParams* params, const float* src, uint32_t components,
+static FjStatus fit_check(FjbRecipe* recipe, const FjbFitParams* params, bool have_input, uint32_t components,
                           int32_t width, int32_t height, fjb::FitTheta& th, FjErrorBuffer* error) {
-    if (!recipe || !params || !src) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    if (!recipe || !params || !have_input) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
     if ((components != 3 && components != 4) || width < 0 || height < 0)
         return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "unsupported image geometry");
     const fjb::PixelParams& p = recipe->r.params;
@@ -547,35 +634,25 @@ static FjStatus fit_check(FjbRecipe* recipe, const FjbFitParams* params, const f
     return ok_status();
 }
 
+
 FjStatus fjb_fit_forward(FjbRecipe* recipe, const FjbFitParams* params, const float* src, ptrdiff_t src_row_bytes,
                          uint32_t components, float* out_r, float* out_g, float* out_b, int32_t width, int32_t height,
                          void* stream, FjErrorBuffer* error) {
     fjb::FitTheta th{};
-    FjStatus st = fit_check(recipe, params, src, components, width, height, th, error);
+    FjStatus st = fit_check(recipe, params, src != nullptr, components, width, height, th, error);
     if (st.category != FJ_STATUS_SUCCESS) return st;
     if (!out_r || !out_g || !out_b) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
-    if ((long long)width * height == 0) {
-        write_error(error, "");
-        return ok_status();
+    if ((long long)width * height > 0) {
+        fjb::PixelParams p = recipe->r.params;
+        p.src = reinterpret_cast<const char*>(src);
+        p.src_row_bytes = src_row_bytes;
+        p.components = (int)components;
+        p.width = width;
+        p.height = height;
+        const cudaError_t e = fjb::launch_fit_forward<false>(p, th, fjb::FitCarrier{}, out_r, out_g, out_b,
+                                                             reinterpret_cast<cudaStream_t>(stream));
+        if (e != cudaSuccess) return cuda_status(e, error, "fit forward");
     }
-    fjb::PixelParams p = recipe->r.params;
-    p.src = reinterpret_cast<const char*>(src);
-    p.src_row_bytes = src_row_bytes;
-    p.components = (int)components;
-    p.width = width;
-    p.height = height;
-    const size_t smem = (size_t)p.curve_blob_floats * sizeof(float);
-    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    fjb::count_launch();
-    if (p.route == fjb::kRoutePrint) {
-        cudaFuncSetAttribute(fjb::fit_forward_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        fjb::fit_forward_kernel<true><<<fjb::fit_blocks(), fjb::kFitThreads, smem, s>>>(p, th, out_r, out_g, out_b);
-    } else {
-        cudaFuncSetAttribute(fjb::fit_forward_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        fjb::fit_forward_kernel<false><<<fjb::fit_blocks(), fjb::kFitThreads, smem, s>>>(p, th, out_r, out_g, out_b);
-    }
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e, error, "fit forward");
     write_error(error, "");
     return ok_status();
 }
@@ -585,12 +662,11 @@ FjStatus fjb_fit_vjp(FjbRecipe* recipe, const FjbFitParams* params, const float*
                      int32_t width, int32_t height, double* grad_params, void* scratch, size_t scratch_bytes,
                      void* stream, FjErrorBuffer* error) {
     fjb::FitTheta th{};
-    FjStatus st = fit_check(recipe, params, src, components, width, height, th, error);
+    FjStatus st = fit_check(recipe, params, src != nullptr, components, width, height, th, error);
     if (st.category != FJ_STATUS_SUCCESS) return st;
     if (!grad_r || !grad_g || !grad_b || !grad_params || !scratch)
         return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
-    const int blocks = fjb::fit_blocks();
-    if (scratch_bytes < (size_t)blocks * fjb::kFitParams * sizeof(double))
+    if (scratch_bytes < (size_t)fjb::fit_blocks() * fjb::kFitParams * sizeof(double))
         return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "fit scratch smaller than fjb_fit_scratch_bytes()");
     fjb::PixelParams p = recipe->r.params;
     p.src = reinterpret_cast<const char*>(src);
@@ -598,23 +674,60 @@ FjStatus fjb_fit_vjp(FjbRecipe* recipe, const FjbFitParams* params, const float*
     p.components = (int)components;
     p.width = width;
     p.height = height;
-    const size_t smem = fjb::fit_vjp_smem(p);
-    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    double* partials = static_cast<double*>(scratch);
-    fjb::count_launch();
-    if (p.route == fjb::kRoutePrint) {
-        cudaFuncSetAttribute(fjb::fit_vjp_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        fjb::fit_vjp_kernel<true><<<blocks, fjb::kFitThreads, smem, s>>>(p, th, grad_r, grad_g, grad_b, partials);
-    } else {
-        cudaFuncSetAttribute(fjb::fit_vjp_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        fjb::fit_vjp_kernel<false><<<blocks, fjb::kFitThreads, smem, s>>>(p, th, grad_r, grad_g, grad_b, partials);
+    const cudaError_t e =
+        fjb::launch_fit_vjp<false>(p, th, fjb::FitCarrier{}, grad_r, grad_g, grad_b, static_cast<double*>(scratch),
+                                   grad_params, reinterpret_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_status(e, error, "fit adjoint");
+    write_error(error, "");
+    return ok_status();
+}
+
+FjStatus fjb_fit_forward_carrier(FjbRecipe* recipe, const FjbFitParams* params, const float* carrier_b,
+                                 const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                                 float* out_r, float* out_g, float* out_b, int32_t width, int32_t height, void* stream,
+                                 FjErrorBuffer* error) {
+    fjb::FitTheta th{};
+    FjStatus st = fit_check(recipe, params, carrier_b && carrier_g && carrier_r, 3, width, height, th, error);
+    if (st.category != FJ_STATUS_SUCCESS) return st;
+    if (!out_r || !out_g || !out_b || carrier_stride < width)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument or carrier stride below the width");
+    if ((long long)width * height > 0) {
+        fjb::PixelParams p = recipe->r.params;
+        p.width = width;
+        p.height = height;
+        const fjb::FitCarrier cr{carrier_b, carrier_g, carrier_r, (long long)carrier_stride, nullptr, nullptr, nullptr};
+        const cudaError_t e =
+            fjb::launch_fit_forward<true>(p, th, cr, out_r, out_g, out_b, reinterpret_cast<cudaStream_t>(stream));
+        if (e != cudaSuccess) return cuda_status(e, error, "fit forward");
     }
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) {
-        fjb::count_launch();
-        fjb::fit_reduce_kernel<<<1, 32, 0, s>>>(partials, blocks, grad_params);
-        e = cudaGetLastError();
-    }
+    write_error(error, "");
+    return ok_status();
+}
+
+FjStatus fjb_fit_vjp_carrier(FjbRecipe* recipe, const FjbFitParams* params, const float* carrier_b,
+                             const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                             const float* grad_r, const float* grad_g, const float* grad_b, int32_t width,
+                             int32_t height, double* grad_params, float* grad_carrier_b, float* grad_carrier_g,
+                             float* grad_carrier_r, void* scratch, size_t scratch_bytes, void* stream,
+                             FjErrorBuffer* error) {
+    fjb::FitTheta th{};
+    FjStatus st = fit_check(recipe, params, carrier_b && carrier_g && carrier_r, 3, width, height, th, error);
+    if (st.category != FJ_STATUS_SUCCESS) return st;
+    if (!grad_r || !grad_g || !grad_b || !grad_params || !scratch || carrier_stride < width)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument or carrier stride below the width");
+    const bool planes = grad_carrier_b || grad_carrier_g || grad_carrier_r;
+    if (planes && !(grad_carrier_b && grad_carrier_g && grad_carrier_r))
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "carrier gradient planes: all three or none");
+    if (scratch_bytes < (size_t)fjb::fit_blocks() * fjb::kFitParams * sizeof(double))
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "fit scratch smaller than fjb_fit_scratch_bytes()");
+    fjb::PixelParams p = recipe->r.params;
+    p.width = width;
+    p.height = height;
+    const fjb::FitCarrier cr{carrier_b,      carrier_g,      carrier_r,     (long long)carrier_stride,
+                             grad_carrier_b, grad_carrier_g, grad_carrier_r};
+    const cudaError_t e =
+        fjb::launch_fit_vjp<true>(p, th, cr, grad_r, grad_g, grad_b, static_cast<double*>(scratch), grad_params,
+                                  reinterpret_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_status(e, error, "fit adjoint");
     write_error(error, "");
     return ok_status();

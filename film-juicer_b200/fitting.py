@@ -178,3 +178,219 @@ def fit(recipe: DeviceRecipe, src, target, theta0, *, free=None, steps: int = 20
     theta = theta0.clone()
     theta[free] = var.detach()
     return theta, losses
+
+
+# ---------------------------------------------------------------------------
+# Whole frames with the optics on: camera diffusion (scatter fraction f) and emulsion
+# scatter (amount a) / halation back-reflection (strength s per channel) ahead of the
+# per-pixel chain. Both stages are linear in the carrier and act per channel, so the
+# exposure parameters (a per-channel scale) commute with them: the per-pixel chain runs
+# from the post-optics carrier (fjb_fit_*_carrier) with exact gradients, and each
+# optics parameter's gradient is <d L / d carrier, d carrier / d parameter>, the tangent
+# plane obtained by running the same linear stages forward on it:
+#   diffusion  x1 = (1 - f) x0 + f PSF*x0                 d x1 / d f = PSF*x0 - x0
+#   scatter    x2 = (1 - a) x1 + a S(x1)                  d x2 / d a = S(x1) - x1
+#   bounce     x3 = (x2 + s B(x2)) / (1 + s)  [renorm]    d x3 / d s = (B(x2) - x2) / (1 + s)^2
+#                   x2 + s B(x2)              [else]                  = B(x2)
+# with the tangents of f and a carried through the later stages (all linear).
+# ---------------------------------------------------------------------------
+OPTIC_NAMES = ("camera_scatter_fraction", "scatter_amount", "halation_strength_r", "halation_strength_g",
+               "halation_strength_b")
+
+
+def _copy(struct):
+    return type(struct).from_buffer_copy(struct)
+
+
+class FrameFit:
+    """A frame's fitting problem: the recipe, the frame's optics descriptors and its
+    camera exposure (computed once by the library: the optics parameters act after it).
+
+    host: the frame's FjPreparedHostData (a HostRecord's `.h`), with camera diffusion
+    and/or scatter/halation switched by its optics flags; spatial DIR, grain, enlarger
+    diffusion, highlight reconstruction and auto exposure are outside this chain and
+    must be off. src: (H, W, 3|4) float32 CUDA source."""
+
+    def __init__(self, recipe: DeviceRecipe, host, src, stream=None):
+        torch = _torch()
+        o = host.optics
+        if host.spatial_dir.component_count or (host.grain.flags & abi.FJ_GRAIN_ACTIVE) or \
+                (o.flags & (abi.FJ_OPTICS_ENLARGER_DIFFUSION | abi.FJ_OPTICS_HIGHLIGHT_BOOST)) or \
+                (host.film_exposure.flags & abi.FJ_FILM_AUTO_EXPOSURE):
+            raise ValueError("frame fitting covers camera diffusion and scatter/halation only")
+        self.recipe, self.stream = recipe, stream
+        self.diffusion_on = bool(o.flags & abi.FJ_OPTICS_CAMERA_DIFFUSION)
+        self.halation_on = bool(o.flags & abi.FJ_OPTICS_SCATTER_HALATION)
+        self.camera = _copy(o.camera)
+        self.halation = _copy(o.scatter_halation)
+        if self.diffusion_on:
+            from .runtime import diffusion_components
+
+            self.components = diffusion_components(self.camera)
+        h, w = src.shape[0], src.shape[1]
+        self.shape = (h, w)
+        planes = [torch.empty((h, w), dtype=torch.float32, device=src.device) for _ in range(3)]
+        recipe.camera_exposure(src, planes, stream=stream)  # B, G, R
+        self.x0 = [planes[2], planes[1], planes[0]]  # R, G, B
+        self._scratch = None
+
+    def optics_default(self):
+        """The frame's own optics parameters (OPTIC_NAMES order), float64 CPU."""
+        torch = _torch()
+        ch = self.halation.channels
+        return torch.tensor([self.camera.scatter_fraction, self.halation.scatter_amount, ch[0].total_strength,
+                             ch[1].total_strength, ch[2].total_strength], dtype=torch.float64)
+
+    # -- the linear optics stages, on three R, G, B planes --
+    def _diffuse(self, planes, fraction):
+        from .runtime import diffusion
+
+        torch = _torch()
+        out = [torch.empty_like(p) for p in planes]
+        diffusion(self.components, int(self.camera.radius_px), float(fraction), planes, out, stream=self.stream)
+        return out
+
+    def _halation(self, planes, amount, strengths, renormalize=None):
+        """In place: scatter with `amount`, then back-reflection with `strengths`."""
+        from .runtime import scatter_halation
+
+        d = _copy(self.halation)
+        d.scatter_amount = float(amount)
+        for c in range(3):
+            d.channels[c].total_strength = float(strengths[c])
+        if renormalize is not None:
+            d.renormalize = 1 if renormalize else 0
+        if d.scatter_amount == 0.0 and all(float(s) == 0.0 for s in strengths):
+            return planes
+        self._scratch = scatter_halation(d, planes, stream=self.stream, scratch=self._scratch)
+        return planes
+
+    def carriers(self, optics):
+        """(x1, x2, x3): after diffusion, after scatter, after back-reflection (R, G, B)."""
+        v = [float(x) for x in optics.detach().cpu().tolist()]
+        x1 = self._diffuse(self.x0, v[0]) if self.diffusion_on else [p.clone() for p in self.x0]
+        x2 = [p.clone() for p in x1]
+        x3 = [p.clone() for p in x1]
+        if self.halation_on:
+            self._halation(x2, v[1], (0.0, 0.0, 0.0))
+            x3 = [p.clone() for p in x2]
+            self._halation(x3, 0.0, v[2:5])
+        return x1, x2, x3
+
+    def tangents(self, optics, x1, x2):
+        """d carrier / d optics parameter, five lists of R, G, B planes (None where the
+        frame's stage is off, or for the halation strength of a channel the frame's
+        record gives no back-reflection: the carrier does not depend on it)."""
+        v = [float(x) for x in optics.detach().cpu().tolist()]
+        out = [None] * 5
+        if self.diffusion_on:
+            t = [a - b for a, b in zip(self._diffuse(self.x0, 1.0), self.x0)]
+            if self.halation_on:
+                self._halation(t, v[1], (0.0, 0.0, 0.0))
+                self._halation(t, 0.0, v[2:5])
+            out[0] = t
+        if self.halation_on:
+            s1 = self._halation([p.clone() for p in x1], 1.0, (0.0, 0.0, 0.0))
+            t = [a - b for a, b in zip(s1, x1)]
+            self._halation(t, 0.0, v[2:5])
+            out[1] = t
+            renorm = bool(self.halation.renormalize)
+            b1 = self._halation([p.clone() for p in x2], 0.0, (1.0, 1.0, 1.0), renormalize=False)
+            torch = _torch()
+            for c in range(3):
+                if self.halation.channels[c].total_strength == 0.0:
+                    # no back-reflection configured for this channel (its Gaussians are
+                    # not part of the record): not a free parameter
+                    continue
+                t = [torch.zeros_like(p) for p in x2]
+                bc = b1[c] - x2[c]  # B(x2) of channel c
+                t[c] = (bc - x2[c]) / (1.0 + v[2 + c]) ** 2 if renorm else bc
+                out[2 + c] = t
+        return out
+
+    def forward(self, theta, optics, out=None):
+        """Linear output RGB planes (3, H, W) of the frame for theta (13) and optics (5)."""
+        _, _, x3 = self.carriers(optics)
+        return forward_carrier(self.recipe, theta, x3, out=out, stream=self.stream)
+
+    def vjp(self, theta, optics, grad_rgb):
+        """(d L / d theta (13,), d L / d optics (5,)) for L = <grad_rgb, rgb>, float64 CPU."""
+        torch = _torch()
+        x1, x2, x3 = self.carriers(optics)
+        g_theta, g_carrier = vjp_carrier(self.recipe, theta, x3, grad_rgb, stream=self.stream)
+        g_opt = torch.zeros(len(OPTIC_NAMES), dtype=torch.float64)
+        for i, t in enumerate(self.tangents(optics, x1, x2)):
+            if t is not None:
+                g_opt[i] = sum(float((g.double() * p.double()).sum()) for g, p in zip(g_carrier, t))
+        return g_theta.cpu(), g_opt
+
+
+def forward_carrier(recipe: DeviceRecipe, theta, carrier_rgb, out=None, stream=None):
+    """fjb_fit_forward_carrier on carrier planes (R, G, B lists of (H, W) CUDA tensors)."""
+    torch = _torch()
+    r, g, b = carrier_rgb
+    h, w = r.shape
+    if out is None:
+        out = torch.empty((3, h, w), dtype=torch.float32, device=r.device)
+    params = _params(theta)
+    err = abi.ErrorText()
+    st = recipe.lib.fjb_fit_forward_carrier(recipe.handle, C.byref(params), *[C.c_void_p(_ptr(t)) for t in (b, g, r)],
+                                            r.stride(0), *[C.c_void_p(_ptr(out[c])) for c in range(3)], w, h,
+                                            C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+    _check("fjb_fit_forward_carrier", st, err)
+    return out
+
+
+def vjp_carrier(recipe: DeviceRecipe, theta, carrier_rgb, grad_rgb, stream=None):
+    """fjb_fit_vjp_carrier: (d L / d theta (13,) float64 CUDA, d L / d carrier as R, G, B
+    planes) for L = <grad_rgb, rgb>."""
+    torch = _torch()
+    r, g, b = carrier_rgb
+    h, w = r.shape
+    gr = grad_rgb.contiguous().to(torch.float32)
+    grad = torch.empty(N_PARAMS, dtype=torch.float64, device=r.device)
+    gc = [torch.empty((h, w), dtype=torch.float32, device=r.device) for _ in range(3)]  # B, G, R
+    scratch = _SCRATCH.get(torch, r.device)
+    params = _params(theta)
+    err = abi.ErrorText()
+    st = recipe.lib.fjb_fit_vjp_carrier(recipe.handle, C.byref(params), *[C.c_void_p(_ptr(t)) for t in (b, g, r)],
+                                        r.stride(0), *[C.c_void_p(_ptr(gr[c])) for c in range(3)], w, h,
+                                        C.c_void_p(_ptr(grad)), *[C.c_void_p(_ptr(t)) for t in gc],
+                                        C.c_void_p(_ptr(scratch)), scratch.numel(),
+                                        C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+    _check("fjb_fit_vjp_carrier", st, err)
+    return grad, [gc[2], gc[1], gc[0]]
+
+
+def _frame_function():
+    torch = _torch()
+
+    class FrameChain(torch.autograd.Function):
+        """rgb = chain(theta, optics; frame); backward: the carrier adjoint and the
+        optics tangents."""
+
+        @staticmethod
+        def forward(ctx, theta, optics, frame):
+            ctx.frame = frame
+            ctx.save_for_backward(theta, optics)
+            return frame.forward(theta, optics)
+
+        @staticmethod
+        def backward(ctx, grad_rgb):
+            theta, optics = ctx.saved_tensors
+            g_theta, g_opt = ctx.frame.vjp(theta, optics, grad_rgb)
+            return (g_theta.to(device=theta.device, dtype=theta.dtype),
+                    g_opt.to(device=optics.device, dtype=optics.dtype), None)
+
+    return FrameChain
+
+
+_FRAME_FN = None
+
+
+def frame_chain(theta, optics, frame: FrameFit):
+    """Differentiable linear output RGB (3, H, W) of a frame with its optics on."""
+    global _FRAME_FN
+    if _FRAME_FN is None:
+        _FRAME_FN = _frame_function()
+    return _FRAME_FN.apply(theta, optics, frame)

@@ -107,6 +107,23 @@ FjStatus fjb_fit_vjp(FjbRecipe* recipe, const FjbFitParams* params, const float*
                      uint32_t components, const float* grad_r, const float* grad_g, const float* grad_b,
                      int32_t width, int32_t height, double* grad_params, void* scratch, size_t scratch_bytes,
                      void* stream, FjErrorBuffer* error);
+/* The same chain from carrier planes (film exposure B, G, R before the route
+ * correction, as fjb_camera_exposure writes it and the optics stages leave it; row
+ * stride in floats) instead of the source RGB: on frames with camera diffusion and
+ * scatter/halation, whose stages are linear in the carrier, the exposure parameters
+ * scale the carrier after them exactly as before them. fjb_fit_vjp_carrier also
+ * writes d <grad_rgb, rgb> / d carrier into grad_carrier_* (all three or none; dense
+ * width x height planes), the cotangent for the optics stages' own parameters. */
+FjStatus fjb_fit_forward_carrier(FjbRecipe* recipe, const FjbFitParams* params, const float* carrier_b,
+                                 const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                                 float* out_r, float* out_g, float* out_b, int32_t width, int32_t height, void* stream,
+                                 FjErrorBuffer* error);
+FjStatus fjb_fit_vjp_carrier(FjbRecipe* recipe, const FjbFitParams* params, const float* carrier_b,
+                             const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                             const float* grad_r, const float* grad_g, const float* grad_b, int32_t width,
+                             int32_t height, double* grad_params, float* grad_carrier_b, float* grad_carrier_g,
+                             float* grad_carrier_r, void* scratch, size_t scratch_bytes, void* stream,
+                             FjErrorBuffer* error);
 
 /* Device error word (bit 0 scan failure, bit 8 DIR failure, bits 9..11 DIR
  * channels B,G,R, bit 16 a tensor-core wait of the print stage gave up). Cleared by fjb_recipe_clear_flags, read by fjb_recipe_read_flags
