@@ -123,3 +123,70 @@ def test_stage_times_against_reference_cuda(torch_cuda, recipes, prepare, oracle
             json.dump(table, fh, indent=1)
     for k, v in table.items():
         assert v["ours_ms"] <= 1.5 * v["reference_ms"], (k, v)
+
+
+def test_camera_diffusion_against_reference_cufft(torch_cuda, recipes, prepare):
+    """The reference's cuFFT camera diffusion (src/Cuda/Diffusion/JuicerCudaDiffusion.cu,
+    driven through its execution planner by oracle/ref_fft_shim.cu) against this
+    library's FFT form on the 4K carrier at radius 19: outputs within 2e-5 of the
+    frame's scale (both FP32 transforms of the same PSF), and device time no longer than
+    the reference's (its stage launch alone, mean of 5 after the first; ours the owner's
+    camera-diffusion stage time in fj_cuda_render frames)."""
+    import ctypes as C
+
+    torch = torch_cuda
+    from film_juicer_b200 import abi, frame_records, load_library, runtime
+
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                        "libjuicer_ref_fft.so")
+    if not os.path.exists(path):
+        pytest.skip("reference cuFFT diffusion harness not built")
+    ref = C.CDLL(path)
+    ref.ref_fft_diffusion.restype = C.c_int
+    ref.ref_fft_diffusion.argtypes = [C.POINTER(C.c_double)] * 4 + [C.c_int, C.c_double] + [C.c_void_p] * 6 + \
+        [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float)]
+    lib = load_library()
+    rec = frame_records.FrameRecord(recipes["print"], W, H)
+    desc = rec.host.h.optics.camera
+    assert desc.radius_px == 19
+    comps = runtime.diffusion_components(desc)
+    src = torch.from_numpy(np.ascontiguousarray(prepare.synthetic_frame(W, H, seed=20261205))).cuda()
+    dr = runtime.DeviceRecipe(rec.host)
+    bgr = [torch.empty((H, W), device="cuda") for _ in range(3)]
+    dr.camera_exposure(src, bgr)
+    rgb = [bgr[2], bgr[1], bgr[0]]
+    ours = [torch.empty_like(p) for p in rgb]
+    runtime.diffusion(comps, desc.radius_px, desc.scatter_fraction, rgb, ours)
+    theirs = [torch.empty_like(p) for p in rgb]
+    ms = C.c_float()
+    arr = lambda v: (C.c_double * 9)(*list(v))  # noqa: E731
+    rc = ref.ref_fft_diffusion(arr(comps.lambda_px), arr(comps.red_weights), arr(comps.green_weights),
+                               arr(comps.blue_weights), desc.radius_px, desc.scatter_fraction,
+                               *[C.c_void_p(p.data_ptr()) for p in rgb], *[C.c_void_p(p.data_ptr()) for p in theirs],
+                               W, H, 5, C.byref(ms))
+    assert rc == 0, rc
+    torch.cuda.synchronize()
+    for a, b in zip(ours, theirs):
+        scale = float(b.abs().max())
+        assert float((a - b).abs().max()) <= 2e-5 * scale, float((a - b).abs().max()) / scale
+    err = abi.ErrorText()
+    d = torch.empty_like(src)
+    with runtime.Owner() as owner:
+        owner.render(rec, src, d)
+        lib.fjb_owner_stage_timing(owner.handle, 1, C.byref(err.buf))
+        for _ in range(5):
+            owner.render(rec, src, d)
+        t = abi.FjbStageTimes()
+        lib.fjb_owner_stage_times(owner.handle, C.byref(t), C.byref(err.buf))
+        i = abi.FJB_STAGE_NAMES.index("camera_diffusion")
+        ours_ms = t.total_ms[i] / t.frames[i]
+    row = {"ours_ms": round(ours_ms, 4), "reference_ms": round(ms.value, 4), "speedup": round(ms.value / ours_ms, 2)}
+    print(json.dumps({"camera_diffusion": row}))
+    path = os.environ.get("FJB_SPEED_REPORT")
+    if path:
+        table = json.load(open(path)) if os.path.exists(path) else {}
+        table["camera_diffusion"] = row
+        with open(path, "w") as fh:
+            json.dump(table, fh, indent=1)
+    dr.close()
+    assert ours_ms <= ms.value, row
