@@ -28,14 +28,15 @@ constexpr int kDiffusionFftMinRadius = 8;
 struct DiffusionFftPlan {
     int width, height, radius;
     int m, log2m;     // nx / 2 complex points per row transform
-    int ny, log2ny;   // column transform length
-    int ntw, log2ntw; // twiddle table length (max(nx, ny))
+    int ny, log2ny;   // column transform length 2^a 3^ny3 (log2ny: a when ny3 == 0, else -1)
+    int ny3;          // factors of 3 in ny (0, 1 or 2)
+    int ntw, log2ntw; // row twiddle table length (nx)
     int ey;           // extended rows H + 2r
     int sy;           // rows per spectrum column in the work buffer (ey rounded up to 4)
     int rows_per_cta, cols_per_cta; // powers of two
     int log2_rows_per_cta;
     size_t work_floats;     // 3 channels x (m + 1) x sy complex
-    size_t spectrum_floats; // twiddles (2 ntw) + 3 channels x (m + 1) x ny reals
+    size_t spectrum_floats; // twiddles (2 ntw + 2 ny) + 3 channels x (m + 1) x ny reals
 };
 
 // False when the frame is too large for the transforms (then the direct form runs).

@@ -2,8 +2,9 @@
 //
 // Same result as the direct kernel of fjb_diffusion.cu up to FP32 round-off: the
 // reflect-extended frame (whole-sample reflection, r samples on every side) is
-// convolved circularly with the PSF on an nx x ny grid (powers of two, nx >= W + 2r,
-// ny >= H + 2r), which equals the linear convolution on the W x H interior. The
+// convolved circularly with the PSF on an nx x ny grid (nx >= W + 2r a power of two,
+// ny >= H + 2r the shortest of 2^a, 3 2^a and 9 2^a), which equals the linear
+// convolution on the W x H interior. The
 // reference reaches the same convolution with cuFFT on reflect-padded tiles
 // (src/Cuda/Diffusion/JuicerCudaDiffusion.cu:510-625); the transforms here are written
 // in this file.
@@ -23,7 +24,8 @@
 // column transforms over the PSF placed around the origin.
 //
 // Transforms: radix-8 Stockham stages (after one radix-2 or radix-4 stage for the
-// remainder) in shared memory, natural order in and out. Each thread keeps the values of its
+// remainder, and before one or two radix-3 stages when the column length is 3 2^a or
+// 9 2^a) in shared memory, natural order in and out. Each thread keeps the values of its
 // butterflies in registers across the stage barrier, so one buffer per line is
 // enough. Twiddles come from a table exp(-2 pi i k / N) built in FP64 and rounded.
 #include <cuda_runtime.h>
@@ -74,14 +76,25 @@ __global__ void twiddle_kernel(float2* tw, int n) {
     tw[k] = make_float2((float)c, (float)s);
 }
 
-// Size-R DFT in registers (R = 2, 4, 8); kInverse uses the conjugate roots.
+// Size-R DFT in registers (R = 2, 3, 4, 8); kInverse uses the conjugate roots.
 template <int R, bool kInverse>
 __device__ __forceinline__ void dft(float2 (&v)[R]) {
     auto add = [](float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); };
     auto sub = [](float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); };
     // multiply by -i (forward) or +i (inverse)
     auto rot = [](float2 a) { return kInverse ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x); };
-    if constexpr (R == 2) {
+    if constexpr (R == 3) {
+        // w = exp(-+2 pi i / 3) = -1/2 -+ i sqrt(3)/2:  X1 = v0 - (v1 + v2)/2 -+ i (sqrt(3)/2)(v1 - v2),
+        // X2 = the same with the sign of the last term flipped
+        constexpr float s3 = 0.86602540378443864676f; // sqrt(3) / 2
+        const float2 t1 = add(v[1], v[2]);
+        const float2 t2 = make_float2(v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y);
+        const float2 d = sub(v[1], v[2]);
+        const float2 sd = rot(make_float2(s3 * d.x, s3 * d.y));
+        v[0] = add(v[0], t1);
+        v[1] = add(t2, sd);
+        v[2] = sub(t2, sd);
+    } else if constexpr (R == 2) {
         const float2 a = v[0], b = v[1];
         v[0] = add(a, b);
         v[1] = sub(a, b);
@@ -197,9 +210,78 @@ __device__ void fft_lines(float2* data, int n, int log2n, int ls, int count, con
     for (; log2ns < log2n; log2ns += 3) fft_stage<8, kInverse>(data, log2n, ls, count, log2ns, tw, tw_shift);
 }
 
+// One Stockham stage of radix R (2, 3, 4 or 8) over `count` lines of any length n that
+// the stages' radices multiply to (line stride `ls`), Ns the product of the earlier
+// stages' radices; tw holds exp(-2 pi i k / n), k < n. The same butterflies as
+// fft_stage, with integer index arithmetic in place of shifts and masks.
+template <int R, bool kInverse>
+__device__ __forceinline__ void fft_stage_g(float2* data, int n, int ls, int count, int Ns, const float2* tw) {
+    constexpr int kMaxB = (kFftMaxValues - kFftMaxValues % R) / R;
+    const int nb = n / R;
+    const int total = count * nb;
+    const int step = n / (Ns * R); // twiddle index step n / (Ns R)
+    float2 v[kMaxB][R];
+#pragma unroll
+    for (int i = 0; i < kMaxB; ++i) {
+        const int b = threadIdx.x + i * blockDim.x;
+        if (b < total) {
+            const int line = b / nb, j = b - line * nb;
+            const float2* d = data + (size_t)line * ls;
+            const int jm = j % Ns;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[i][r] = d[swz(j + r * nb)];
+            if (jm != 0) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    float2 w = tw[r * jm * step];
+                    if (kInverse) w.y = -w.y;
+                    v[i][r] = cmul(v[i][r], w);
+                }
+            }
+            dft<R, kInverse>(v[i]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kMaxB; ++i) {
+        const int b = threadIdx.x + i * blockDim.x;
+        if (b < total) {
+            const int line = b / nb, j = b - line * nb;
+            float2* d = data + (size_t)line * ls;
+            const int jm = j % Ns;
+            const int base = (j - jm) * R + jm;
+#pragma unroll
+            for (int r = 0; r < R; ++r) d[swz(base + r * Ns)] = v[i][r];
+        }
+    }
+    __syncthreads();
+}
+
+// Unnormalised DFT of `count` lines of length n = 2^a 3^n3 (n3 <= 2): the power-of-two
+// stages as in fft_lines (one radix-2 or radix-4 stage, then radix 8), then n3 radix-3
+// stages. Caller synchronises before; ends with a barrier.
+template <bool kInverse>
+__device__ void fft_lines_g(float2* data, int n, int n3, int ls, int count, const float2* tw) {
+    int p2 = n;
+    for (int k = 0; k < n3; ++k) p2 /= 3;
+    int a = 0;
+    while ((1 << a) < p2) ++a;
+    int Ns = 1;
+    if (a % 3 == 1) {
+        fft_stage_g<2, kInverse>(data, n, ls, count, Ns, tw);
+        Ns = 2;
+    } else if (a % 3 == 2) {
+        fft_stage_g<4, kInverse>(data, n, ls, count, Ns, tw);
+        Ns = 4;
+    }
+    for (; Ns < p2; Ns *= 8) fft_stage_g<8, kInverse>(data, n, ls, count, Ns, tw);
+    for (int k = 0; k < n3; ++k, Ns *= 3) fft_stage_g<3, kInverse>(data, n, ls, count, Ns, tw);
+}
+
 struct FftPass {
     DiffusionFftPlan p;
-    const float2* tw;    // twiddle table, p.ntw entries
+    const float2* tw;    // row twiddle table, p.ntw entries
+    const float2* twc;   // column twiddle table exp(-2 pi i k / ny), p.ny entries
     float2* work[3];     // per channel: (m + 1) columns x sy rows (transposed spectrum)
     float* spectrum[3];  // per channel: (m + 1) x ny reals, scaled
     const float* src[3]; // frame planes (apply) or unused (spectrum build)
@@ -285,40 +367,47 @@ __global__ void __launch_bounds__(kFftThreads) columns_kernel(const __grid_const
     const float2* in = F.work[ch];
     const int rows = kBuild ? 2 * r + 1 : p.ey;
     float2* tws = fsm + (size_t)p.cols_per_cta * ny; // exp(-2 pi i k / ny), k < ny
-    stage_twiddles(tws, F.tw, p.log2ny, p.log2ntw);
-    #pragma unroll 8
-    for (int i = threadIdx.x; i < KC * ny; i += blockDim.x) {
-        const int c = i >> p.log2ny, ey = i & (ny - 1);
-        float2 v = make_float2(0.0f, 0.0f);
-        if (kBuild) {
-            // compact PSF row j holds dy = j - r, placed at dy mod ny
-            const int dy = ey <= r ? ey : ey - ny;
-            if (dy >= -r && dy <= r) v = in[(size_t)(k0 + c) * p.sy + dy + r];
-        } else if (ey < rows) {
-            v = in[(size_t)(k0 + c) * p.sy + ey];
+    for (int k = threadIdx.x; k < ny; k += blockDim.x) tws[k] = F.twc[k];
+    for (int c = 0; c < KC; ++c) {
+        #pragma unroll 4
+        for (int ey = threadIdx.x; ey < ny; ey += blockDim.x) {
+            float2 v = make_float2(0.0f, 0.0f);
+            if (kBuild) {
+                // compact PSF row j holds dy = j - r, placed at dy mod ny
+                const int dy = ey <= r ? ey : ey - ny;
+                if (dy >= -r && dy <= r) v = in[(size_t)(k0 + c) * p.sy + dy + r];
+            } else if (ey < rows) {
+                v = in[(size_t)(k0 + c) * p.sy + ey];
+            }
+            fsm[(size_t)c * ny + swz(ey)] = v;
         }
-        fsm[(size_t)c * ny + swz(ey)] = v;
     }
     __syncthreads();
-    fft_lines<false>(fsm, ny, p.log2ny, ny, KC, tws, p.log2ny);
+    if (p.ny3 == 0)
+        fft_lines<false>(fsm, ny, p.log2ny, ny, KC, tws, p.log2ny);
+    else
+        fft_lines_g<false>(fsm, ny, p.ny3, ny, KC, tws);
     float* spec = F.spectrum[ch];
-    if (kBuild) {
+    if constexpr (kBuild) {
         const float scale = 1.0f / ((float)p.m * (float)ny);
-        for (int i = threadIdx.x; i < KC * ny; i += blockDim.x) {
-            const int c = i >> p.log2ny, ky = i & (ny - 1);
-            spec[(size_t)k0 * ny + i] = fsm[(size_t)c * ny + swz(ky)].x * scale;
-        }
+        for (int c = 0; c < KC; ++c)
+            for (int ky = threadIdx.x; ky < ny; ky += blockDim.x)
+                spec[(size_t)(k0 + c) * ny + ky] = fsm[(size_t)c * ny + swz(ky)].x * scale;
         return;
     }
-    #pragma unroll 8
-    for (int i = threadIdx.x; i < KC * ny; i += blockDim.x) {
-        const int c = i >> p.log2ny, ky = i & (ny - 1);
-        const float s = spec[(size_t)k0 * ny + i];
-        float2& v = fsm[(size_t)c * ny + swz(ky)];
-        v = make_float2(v.x * s, v.y * s);
+    for (int c = 0; c < KC; ++c) {
+        #pragma unroll 4
+        for (int ky = threadIdx.x; ky < ny; ky += blockDim.x) {
+            const float s = spec[(size_t)(k0 + c) * ny + ky];
+            float2& v = fsm[(size_t)c * ny + swz(ky)];
+            v = make_float2(v.x * s, v.y * s);
+        }
     }
     __syncthreads();
-    fft_lines<true>(fsm, ny, p.log2ny, ny, KC, tws, p.log2ny);
+    if (p.ny3 == 0)
+        fft_lines<true>(fsm, ny, p.log2ny, ny, KC, tws, p.log2ny);
+    else
+        fft_lines_g<true>(fsm, ny, p.ny3, ny, KC, tws);
     float2* out = F.work[ch];
     const int H = p.height;
     for (int c = 0; c < KC; ++c)
@@ -428,29 +517,42 @@ bool diffusion_fft_plan(int width, int height, int radius, DiffusionFftPlan& p) 
     const long long wx = (long long)width + 2LL * radius, hy = (long long)height + 2LL * radius;
     if (wx > 2LL * kFftMaxLen || hy > kFftMaxLen) return false;
     const int nx = pow2_at_least((int)(wx < 16 ? 16 : wx));
-    const int ny = pow2_at_least((int)(hy < 16 ? 16 : hy));
+    // columns: the shortest 2^a, 3 2^a or 9 2^a (a >= 4, at most kFftMaxLen) holding the
+    // extended rows
+    int ny = 0, ny3 = 0;
+    for (int k = 0, f = 1; k <= 2; ++k, f *= 3) {
+        long long n = 16LL * f;
+        while (n < hy) n *= 2;
+        if (n <= kFftMaxLen && (ny == 0 || n < ny)) {
+            ny = (int)n;
+            ny3 = k;
+        }
+    }
+    if (ny == 0) return false;
     p.width = width;
     p.height = height;
     p.radius = radius;
     p.m = nx / 2;
     p.log2m = log2_exact(p.m);
     p.ny = ny;
-    p.log2ny = log2_exact(ny);
-    p.ntw = nx > ny ? nx : ny;
+    p.ny3 = ny3;
+    p.log2ny = ny3 == 0 ? log2_exact(ny) : -1;
+    p.ntw = nx;
     p.log2ntw = log2_exact(p.ntw);
     p.ey = height + 2 * radius;
     p.sy = (p.ey + 3) / 4 * 4;
     // every thread holds at most kFftMaxValues values of a stage
     p.rows_per_cta = (kFftThreads * kFftMaxValues) / p.m;
     if (p.rows_per_cta > 4) p.rows_per_cta = 4;
-    p.cols_per_cta = (kFftThreads * kFftMaxValues) / ny;
+    // a radix-3 stage holds 5 butterflies (15 values) per thread
+    p.cols_per_cta = (kFftThreads * (ny3 ? kFftMaxValues - kFftMaxValues % 3 : kFftMaxValues)) / ny;
     if (p.cols_per_cta > 2) p.cols_per_cta = 2;
     if (p.rows_per_cta < 1 || p.cols_per_cta < 1) return false;
     // the inverse split holds 2 values per (k, m - k) pair: (m/2 + 1) pairs per row
     if ((long long)p.rows_per_cta * (p.m / 2) > (long long)kFftThreads * kC2rPairs) return false;
     p.log2_rows_per_cta = log2_exact(p.rows_per_cta);
     p.work_floats = (size_t)3 * (p.m + 1) * p.sy * 2;
-    p.spectrum_floats = (size_t)2 * p.ntw + (size_t)3 * (p.m + 1) * ny;
+    p.spectrum_floats = (size_t)2 * p.ntw + (size_t)2 * ny + (size_t)3 * (p.m + 1) * ny;
     return true;
 }
 
@@ -465,8 +567,9 @@ cudaError_t launch_diffusion_fft_spectrum(const DiffusionFftPlan& p, const float
     F.p = p;
     float2* tw = reinterpret_cast<float2*>(spectrum);
     F.tw = tw;
+    F.twc = tw + p.ntw;
     for (int c = 0; c < 3; ++c) {
-        F.spectrum[c] = spectrum + (size_t)2 * p.ntw + (size_t)c * (p.m + 1) * p.ny;
+        F.spectrum[c] = spectrum + (size_t)2 * (p.ntw + p.ny) + (size_t)c * (p.m + 1) * p.ny;
         F.work[c] = reinterpret_cast<float2*>(work) + (size_t)c * (p.m + 1) * p.sy;
         F.psf[c] = psf_rows[c];
     }
@@ -474,6 +577,9 @@ cudaError_t launch_diffusion_fft_spectrum(const DiffusionFftPlan& p, const float
     cudaError_t e;
     fjb::count_launch();
     twiddle_kernel<<<(p.ntw + 255) / 256, 256, 0, stream>>>(tw, p.ntw);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    fjb::count_launch();
+    twiddle_kernel<<<(p.ny + 255) / 256, 256, 0, stream>>>(tw + p.ntw, p.ny);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const size_t rs = rows_smem(p), cs = cols_smem(p);
     if ((e = set_smem((const void*)rows_r2c_kernel<true>, rs)) != cudaSuccess) return e;
@@ -492,8 +598,9 @@ cudaError_t launch_diffusion_fft(const DiffusionFftPlan& p, const float* spectru
     FftPass F{};
     F.p = p;
     F.tw = reinterpret_cast<const float2*>(spectrum);
+    F.twc = F.tw + p.ntw;
     for (int c = 0; c < 3; ++c) {
-        F.spectrum[c] = const_cast<float*>(spectrum) + (size_t)2 * p.ntw + (size_t)c * (p.m + 1) * p.ny;
+        F.spectrum[c] = const_cast<float*>(spectrum) + (size_t)2 * (p.ntw + p.ny) + (size_t)c * (p.m + 1) * p.ny;
         F.work[c] = reinterpret_cast<float2*>(work) + (size_t)c * (p.m + 1) * p.sy;
         F.src[c] = src[c];
         F.dst[c] = dst[c];
