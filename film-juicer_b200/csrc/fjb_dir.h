@@ -48,6 +48,14 @@ struct DirComponentDev {
     double v_term[9];
     double seg[9]; // recursion state map over kDirSeg zero-input steps (row-major 3x3)
     double seg4[9]; // the same over 4 kDirSeg steps
+    // Factored FP32 form of the recursion (factored != 0): a unit-DC first-order section
+    // u += c0 (x - u) into the second-order section v = c2 v + c1 (u - y), y += v, with
+    // state (u, y, v); to_fac / from_fac map direct states (y[n-1], y[n-2], y[n-3]) to it
+    // and back, seg_f / seg4_f are its zero-input maps over kDirSeg and 4 kDirSeg steps.
+    int factored;
+    float fac[3];
+    double to_fac[9], from_fac[9];
+    double seg_f[9], seg4_f[9];
 };
 
 constexpr int kDirSeg = 64; // segment length of the block-parallel recursions

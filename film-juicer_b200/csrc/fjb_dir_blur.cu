@@ -562,7 +562,8 @@ constexpr int kColsThreads = 320, kColsBlocks = 2;
 constexpr size_t kSmemLimit = 200 * 1024;
 static_assert(kDirSeg == lines::kLineSeg, "segment maps are built for the line segment length");
 
-// One recursive component with its coefficients held in registers.
+// One recursive component with its coefficients held in registers: the reference's
+// FP64 direct form (state y[n-1], y[n-2], y[n-3]).
 struct DirStep {
     using Real = double;
     double ff, fb0, fb1, fb2;
@@ -579,7 +580,69 @@ struct DirStep {
     }
     __device__ __forceinline__ const double* map() const { return seg; }
     __device__ __forceinline__ const double* map4() const { return seg4; }
+    __device__ __forceinline__ void from_direct(double*) const {}
+    __device__ __forceinline__ void to_direct(const double* s, double d[3]) const {
+        d[0] = s[0];
+        d[1] = s[1];
+        d[2] = s[2];
+    }
 };
+
+// The same recursion in its factored FP32 form (state u, y, v: first-order output,
+// output, last output difference; factor_recursion in fjb_dir_host.cpp). The reflected
+// starts and the end block stay FP64 in the direct basis and are mapped at the ends of
+// each pass.
+struct DirStepF {
+    using Real = float;
+    float c0, c1, c2;
+    const double* seg;
+    const double* seg4;
+    const double* to_fac;
+    const double* from_fac;
+    __device__ explicit DirStepF(const DirComponentDev& c)
+        : c0(c.fac[0]), c1(c.fac[1]), c2(c.fac[2]), seg(c.seg_f), seg4(c.seg4_f), to_fac(c.to_fac),
+          from_fac(c.from_fac) {}
+    __device__ __forceinline__ float step(float x, float s[3]) const {
+        s[0] = fmaf(c0, x - s[0], s[0]);
+        s[2] = fmaf(c2, s[2], c1 * (s[0] - s[1]));
+        s[1] += s[2];
+        return s[1];
+    }
+    __device__ __forceinline__ const double* map() const { return seg; }
+    __device__ __forceinline__ const double* map4() const { return seg4; }
+    __device__ __forceinline__ void from_direct(double s[3]) const {
+        const double* T = to_fac;
+        const double o0 = T[0] * s[0] + T[1] * s[1] + T[2] * s[2];
+        const double o1 = T[3] * s[0] + T[4] * s[1] + T[5] * s[2];
+        const double o2 = T[6] * s[0] + T[7] * s[1] + T[8] * s[2];
+        s[0] = o0;
+        s[1] = o1;
+        s[2] = o2;
+    }
+    __device__ __forceinline__ void to_direct(const float* s, double d[3]) const {
+        const double* T = from_fac;
+        for (int r = 0; r < 3; ++r) d[r] = T[3 * r] * (double)s[0] + T[3 * r + 1] * (double)s[1] + T[3 * r + 2] * (double)s[2];
+    }
+};
+
+// Direct-form starts of L lines (doubles in `entry`) to the step's state, in place
+// (Step::Real). Ends with a barrier.
+template <typename Step>
+__device__ void starts_to_state(const Step& op, double* entry, int L) {
+    using R = typename Step::Real;
+    double s[3] = {0.0, 0.0, 0.0};
+    const int line = threadIdx.x;
+    if (line < L) {
+        for (int h = 0; h < 3; ++h) s[h] = entry[line * 3 + h];
+        op.from_direct(s);
+    }
+    __syncthreads();
+    if (line < L) {
+        R* e = reinterpret_cast<R*>(entry);
+        for (int h = 0; h < 3; ++h) e[line * 3 + h] = (R)s[h];
+    }
+    __syncthreads();
+}
 
 __host__ __device__ inline size_t carry_doubles(int L, int n) { return (size_t)L * lines::scan_chunks(lines::segs(n)) * 3; }
 
@@ -774,6 +837,62 @@ __device__ void reflected_starts(Buf buf, int L, int n, const double* w, int len
     __syncthreads();
 }
 
+// One recursive component over the L rows of the CTA, in place: the reflected start,
+// left to right, the end block at the last ts samples, right to left from it.
+template <typename Step, typename Buf>
+__device__ void yvv_rows(const DirComponentDev& c, Buf line, int L, int W, double* exits, double* entry,
+                         double* last, double* carry) {
+    using R = typename Step::Real;
+    const Step op(c);
+    reflected_starts<1, true>(line, L, W, c.h_init, c.h_len, exits, entry);
+    starts_to_state(op, entry, L);
+    lines::run_direction<1, true>(op, line, L, 0, W, reinterpret_cast<R*>(entry), reinterpret_cast<R*>(exits), carry,
+                                  reinterpret_cast<R*>(last), false);
+    const int ts = c.h_tsize;
+    for (int r = threadIdx.x; r < L; r += blockDim.x) {
+        double d[3], term[3] = {0.0, 0.0, 0.0};
+        op.to_direct(reinterpret_cast<R*>(last) + r * 3, d);
+        end_block(c.h_term, ts, d, term);
+        for (int q = 0; q < ts; ++q)
+            if (W - ts + q >= 0) line(r)[lines::at(W - ts + q)] = (float)term[q];
+        for (int h = 0; h < 3; ++h) entry[r * 3 + h] = h < ts ? term[h] : d[h];
+    }
+    __syncthreads();
+    starts_to_state(op, entry, L);
+    if (W - ts > 0)
+        lines::run_direction<1, false>(op, line, L, 0, W - ts, reinterpret_cast<R*>(entry), reinterpret_cast<R*>(exits),
+                                       carry, (R*)nullptr, false);
+}
+
+// One recursive component over the kStripCols columns of the CTA: from the visual top
+// (memory row H-1) down with the reflected start, the end block at rows [0, ts) (kept
+// in `terms`), back up from row ts.
+template <typename Step, typename Buf>
+__device__ void yvv_cols(const DirComponentDev& c, Buf column, int H, double* exits, double* entry, double* last,
+                         double* carry, double (*terms)[3]) {
+    using R = typename Step::Real;
+    const Step op(c);
+    const int ts = c.v_tsize;
+    reflected_starts<kStripCols, false>(column, kStripCols, H, c.v_init, c.v_len, exits, entry);
+    starts_to_state(op, entry, kStripCols);
+    lines::run_direction<kStripCols, false>(op, column, kStripCols, 0, H, reinterpret_cast<R*>(entry),
+                                            reinterpret_cast<R*>(exits), carry, reinterpret_cast<R*>(last), true);
+    for (int cc = threadIdx.x; cc < kStripCols; cc += blockDim.x) {
+        double d[3], term[3] = {0.0, 0.0, 0.0};
+        op.to_direct(reinterpret_cast<R*>(last) + cc * 3, d);
+        end_block(c.v_term, ts, d, term);
+        for (int h = 0; h < 3; ++h) {
+            terms[cc][h] = term[h];
+            entry[cc * 3 + h] = h < ts ? term[h] : d[h];
+        }
+    }
+    __syncthreads();
+    starts_to_state(op, entry, kStripCols);
+    if (H - ts > 0)
+        lines::run_direction<kStripCols, true>(op, column, kStripCols, ts, H - ts, reinterpret_cast<R*>(entry),
+                                               reinterpret_cast<R*>(exits), carry, (R*)nullptr, true);
+}
+
 // Rows: every component into its row-filtered plane (recursive: left to right, end
 // block, right to left; FIR: reflect taps in FP64).
 __global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) dir_rows_smem_kernel(const __grid_constant__ DirBlurParams p) {
@@ -821,20 +940,10 @@ __global__ void __launch_bounds__(kRowsThreads, kRowsBlocks) dir_rows_smem_kerne
         }
         if (c.op != kDirOpYvv) continue;
         lines::load_rows(buf, raw, W, row0, L, W);
-        reflected_starts<1, true>(line, L, W, c.h_init, c.h_len, exits, entry);
-        const DirStep op(c);
-        lines::run_direction<1, true>(op, line, L, 0, W, entry, exits, carry, last, false);
-        const int ts = c.h_tsize;
-        for (int r = threadIdx.x; r < L; r += blockDim.x) {
-            double term[3] = {0.0, 0.0, 0.0};
-            end_block(c.h_term, ts, last + r * 3, term);
-            for (int q = 0; q < ts; ++q)
-                if (W - ts + q >= 0) line(r)[lines::at(W - ts + q)] = (float)term[q];
-            for (int h = 0; h < 3; ++h) entry[r * 3 + h] = h < ts ? term[h] : last[r * 3 + h];
-        }
-        __syncthreads();
-        if (W - ts > 0)
-            lines::run_direction<1, false>(op, line, L, 0, W - ts, entry, exits, carry, (double*)nullptr, false);
+        if (c.factored)
+            yvv_rows<DirStepF>(c, line, L, W, exits, entry, last, carry);
+        else
+            yvv_rows<DirStep>(c, line, L, W, exits, entry, last, carry);
         lines::store_rows(buf, p.temp[ch][k], row0, L, W);
     }
 }
@@ -875,21 +984,10 @@ __global__ void __launch_bounds__(kColsThreads, kColsBlocks) dir_cols_smem_kerne
             lines::load_strip8(work, p.temp[ch][k], W, H, x0, C);
         const int ts = c.v_tsize;
         if (c.op == kDirOpYvv) {
-            reflected_starts<kStripCols, false>(column, kStripCols, H, c.v_init, c.v_len, exits, entry);
-            const DirStep op(c);
-            lines::run_direction<kStripCols, false>(op, column, kStripCols, 0, H, entry, exits, carry, last, true);
-            for (int cc = threadIdx.x; cc < kStripCols; cc += blockDim.x) {
-                double term[3] = {0.0, 0.0, 0.0};
-                end_block(c.v_term, ts, last + cc * 3, term);
-                for (int h = 0; h < 3; ++h) {
-                    terms[cc][h] = term[h];
-                    entry[cc * 3 + h] = h < ts ? term[h] : last[cc * 3 + h];
-                }
-            }
-            __syncthreads();
-            if (H - ts > 0)
-                lines::run_direction<kStripCols, true>(op, column, kStripCols, ts, H - ts, entry, exits, carry,
-                                                       (double*)nullptr, true);
+            if (c.factored)
+                yvv_cols<DirStepF>(c, column, H, exits, entry, last, carry, terms);
+            else
+                yvv_cols<DirStep>(c, column, H, exits, entry, last, carry, terms);
         }
         auto accumulate = [&](float blurred, float a) {
             const float weighted = blurred * c.weight;

@@ -273,6 +273,61 @@ size_t dir_scratch_floats(int width, int height) {
     return (size_t)(9 + 3 * kDirMaxComponents) * (size_t)width * (size_t)height;
 }
 
+namespace {
+
+void mat3_mul(const double* a, const double* b, double* o) {
+    double t[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) t[i * 3 + j] = a[i * 3] * b[j] + a[i * 3 + 1] * b[3 + j] + a[i * 3 + 2] * b[6 + j];
+    std::memcpy(o, t, sizeof(t));
+}
+
+// The recursion 1 / (1 - fb0 z^-1 - fb1 z^-2 - fb2 z^-3) as (1 - p z^-1)(1 - a1 z^-1 -
+// a2 z^-2): the real pole p by Newton's method from z = 1 (the Gaussian recursions
+// have one real pole in (0, 1) and a complex pair), then the FP32 coefficients
+// c0 = 1 - p, c2 = -a2, c1 = 1 - a1 - a2 and, from those rounded values, the basis
+// maps and zero-input state maps. In this form the state holds the first-order output,
+// the output and its last difference, so FP32 rounding is not amplified by the
+// recursion's DC gain as it is in the direct form (about 1 / ff). factored stays 0
+// (the FP64 direct form runs) when the coefficients do not have that structure.
+void factor_recursion(DirComponentDev& c) {
+    c.factored = 0;
+    double p = 1.0;
+    for (int it = 0; it < 200; ++it) {
+        const double f = ((p - c.fb[0]) * p - c.fb[1]) * p - c.fb[2];
+        const double d = (3.0 * p - 2.0 * c.fb[0]) * p - c.fb[1];
+        if (!(std::fabs(d) > 0.0)) return;
+        const double q = p - f / d;
+        const bool done = std::fabs(q - p) <= 1e-15 * std::fabs(q);
+        p = q;
+        if (done) break;
+    }
+    const double resid = ((p - c.fb[0]) * p - c.fb[1]) * p - c.fb[2];
+    if (!(p > 0.0 && p < 1.0) || !(std::fabs(resid) < 1e-12)) return;
+    const double a1 = c.fb[0] - p, a2 = c.fb[1] + p * a1;
+    const float c0 = (float)(1.0 - p), c2 = (float)(-a2), c1 = (float)(1.0 - a1 - a2);
+    if (!(c0 > 0.0f && c1 > 0.0f && c2 > 0.0f && c2 < 1.0f) || !std::isfinite(c1)) return;
+    // the rounded coefficients define the FP32 recursion; the maps describe it
+    const double P = 1.0 - (double)c0, C1 = c1, C2 = c2, A1 = 1.0 + C2 - C1, A2 = -C2;
+    const double T[9] = {1.0 / C1, -A1 / C1, -A2 / C1, 1, 0, 0, 1, -1, 0};
+    const double Ti[9] = {0, 1, 0, 0, 1, -1, -C1 / A2, (1.0 - A1) / A2, A1 / A2};
+    const double F[9] = {P, 0, 0, C1 * P, 1.0 - C1, C2, C1 * P, -C1, C2};
+    double r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    for (int step = 1; step <= 4 * kDirSeg; ++step) {
+        mat3_mul(F, r, r);
+        if (step == kDirSeg) std::memcpy(c.seg_f, r, sizeof(r));
+    }
+    std::memcpy(c.seg4_f, r, sizeof(r));
+    std::memcpy(c.to_fac, T, sizeof(T));
+    std::memcpy(c.from_fac, Ti, sizeof(Ti));
+    c.fac[0] = c0;
+    c.fac[1] = c1;
+    c.fac[2] = c2;
+    c.factored = 1;
+}
+
+} // namespace
+
 bool dir_plan_create(const FjSpatialDir& sd, int width, int height, cudaStream_t stream, DirPlan& plan,
                      std::string& why, cudaError_t& err) {
     err = cudaSuccess;
@@ -353,6 +408,7 @@ bool dir_plan_create(const FjSpatialDir& sd, int width, int height, cudaStream_t
                     }
                     std::memcpy(c.seg4, r, sizeof(r));
                 }
+                factor_recursion(c);
                 DirAxisBoundary hb, vb;
                 if (!dir_axis_boundary(g, width, hb, why) || !dir_axis_boundary(g, height, vb, why)) return false;
                 void* d = nullptr;

@@ -2,10 +2,12 @@
 FIR and reflected-boundary recursive Gaussians, and capture development with the
 filtered corrections, against the CPU oracle and the reference's own CUDA kernels.
 
-Both sides accumulate the FIR taps and the recursions in FP64 and round to FP32 at
-the same points; the B200 column pass evaluates all components in one sweep (the
-reference accumulates them one pass at a time) and may fuse multiply-adds, so
-results agree to FP32 rounding. Bounds: 1e-6 + 1e-5 |ref| on corrections (values
+Both sides accumulate the FIR taps in FP64 and round to FP32 at the same points; the
+recursions run here in their factored FP32 form (a unit-DC first-order section into a
+second-order section in difference form, the reflected starts and end blocks in FP64),
+the reference's in the FP64 direct form; the B200 column pass evaluates all components
+in one sweep (the reference accumulates them one pass at a time) and may fuse
+multiply-adds, so results agree to FP32 rounding. Bounds: 1e-6 + 1e-5 |ref| on corrections (values
 ~1e-2) and log exposure, 1e-4 + 1e-4 |ref| on developed density."""
 import numpy as np
 import pytest
