@@ -32,6 +32,13 @@ container, where the reference is mounted read-only).
 * abi_layout_reference.json: sizeof of every record of the reference's C-ABI header
   (native/juicer_cuda_api.h) and offsetof of every field, as the system C compiler
   lays them out; the drop-in boundary test compares the repository's header with it.
+* print_cases.npz: the reference's print characterizations (tests/print/
+  {balance,preflash,illuminant}-fixtures, linux-release native profile): the inputs
+  and exact f32 output words and hashes of the 42 balance cases and 60 balance product
+  records, the 19 preflash cases, the 127 filtered-illuminant literal cases (with the
+  Rust build's words beside the native ones), the distinct product main / preflash
+  illuminants on the TH-KG3 lamp, and the KG3 transmission rows (Resources/filters/
+  heat_absorbing/schott/KG3.csv) that lamp is built from.
 * recipe_direct.npz / recipe_print.npz: prepared recipes (film_juicer_b200.prepare)
   for kodak_portra_400 direct and kodak_portra_400 -> kodak_portra_endura print,
   built from the reference's Resources/ profiles and spectral tables.
@@ -353,6 +360,72 @@ def abi_layout():
     print("abi layout:", len(records), "records")
 
 
+def print_cases():
+    """Print balance, preflash and filtered-illuminant characterizations as f32 words."""
+    pdir = os.path.join(REF, "tests", "print")
+
+    def load(*parts):
+        with open(os.path.join(pdir, *parts)) as fh:
+            return json.load(fh)
+
+    u32 = lambda v: np.asarray(v, dtype=np.uint32)
+    out = {}
+    # Balance: the 42 characterization cases and the 60 product records that carry inputs.
+    bal = load("balance-fixtures", "linux-release.json")
+    rows = list(bal["cases"]) + [p for p in bal["products"] if "film_base_density" in p]
+    for key, n in (("film_base_density", 81), ("film_channel_density_cmy", 243), ("print_sensitivity_rgb", 243),
+                   ("filtered_main_illuminant", 81), ("baseline_density_cmy", 3), ("compensated_density_cmy", 3)):
+        out[f"balance_{key}"] = np.stack([u32(r[key]) for r in rows])
+        assert out[f"balance_{key}"].shape[1] == n
+    out["balance_reference_hash"] = np.asarray([r["reference_hash"] for r in rows], dtype=np.uint64)
+    out["balance_mode"] = np.asarray([r["normalization_mode"] for r in rows], dtype=np.int32)
+    out["balance_success"] = np.asarray([bool(r.get("success", True)) for r in rows])
+    out["balance_field"] = np.asarray([r.get("diagnostic", "").rsplit("field=", 1)[-1] if not r.get("success", True)
+                                       else "" for r in rows])
+    res = [r.get("balance") if r.get("success", True) else None for r in rows]
+    zero = {"baseline_raw_rgb": [0] * 3, "compensated_raw_rgb": [0] * 3, "scalars": [0] * 3,
+            "filtered_main_illuminant_hash": 0, "hash": 0}
+    res = [b if b is not None else zero for b in res]
+    out["balance_baseline_raw"] = np.stack([u32(b["baseline_raw_rgb"]) for b in res])
+    out["balance_compensated_raw"] = np.stack([u32(b["compensated_raw_rgb"]) for b in res])
+    out["balance_scalars"] = np.stack([u32(b["scalars"]) for b in res])
+    out["balance_illuminant_hash"] = np.asarray([b["filtered_main_illuminant_hash"] for b in res], dtype=np.uint64)
+    out["balance_hash"] = np.asarray([b["hash"] for b in res], dtype=np.uint64)
+    out["balance_id"] = np.asarray([r.get("id", f"product-{i}") for i, r in enumerate(rows)])
+    # Preflash raw integral
+    pre = load("preflash-fixtures", "linux-release.json")["cases"]
+    out["preflash_film_base_density"] = np.stack([u32(c["film_base_density"]) for c in pre])
+    out["preflash_filtered_illuminant"] = np.stack([u32(c["filtered_illuminant"]) for c in pre])
+    out["preflash_sensitivity_cmy"] = np.stack([u32(c["print_sensitivity_cmy"]) for c in pre])
+    out["preflash_raw"] = np.stack([u32(c["raw"]) if c["success"] else u32([0, 0, 0]) for c in pre])
+    out["preflash_success"] = np.asarray([c["success"] for c in pre])
+    out["preflash_id"] = np.asarray([c["id"] for c in pre])
+    # Filtered print illuminant: native (glibc erff) and Rust (libm 0.2.15 erff) expectations
+    lit = load("illuminant-fixtures", "linux-release-literal.json")["cases"]
+    rlit = {c["id"]: c for c in load("illuminant-fixtures", "linux-release-rust-literal.json")["cases"]}
+    for key in ("edges_nm", "transitions_nm", "cmy_cc", "source", "samples"):
+        out[f"illum_{key}"] = np.stack([u32(c[key]) for c in lit])
+    out["illum_rust_samples"] = np.stack([u32(rlit[c["id"]]["samples"]) for c in lit])
+    out["illum_success"] = np.asarray([c["success"] for c in lit])
+    assert all(rlit[c["id"]]["success"] == c["success"] for c in lit)
+    out["illum_id"] = np.asarray([c["id"] for c in lit])
+    # Product main / preflash illuminants on the TH-KG3 enlarger source (distinct records)
+    prods, seen = [], set()
+    for p in load("illuminant-fixtures", "linux-release-products.json")["products"]:
+        key = json.dumps([p.get("main_cmy"), p.get("main"), p.get("preflash_cmy"), p.get("preflash")])
+        if p.get("main_present") and key not in seen:
+            assert p["source_key"] == "TH-KG3"
+            seen.add(key)
+            prods.append(p)
+    for key in ("main_cmy", "main", "preflash_cmy", "preflash"):
+        out[f"product_{key}"] = np.stack([u32(p[key]) for p in prods])
+    # the enlarger source's inputs: the KG3 heat-absorbing glass transmission rows, as text
+    with open(os.path.join(REF, "Resources", "filters", "heat_absorbing", "schott", "KG3.csv")) as fh:
+        out["kg3_csv"] = np.asarray(fh.read())
+    np.savez_compressed(os.path.join(HERE, "print_cases.npz"), **out)
+    print("print cases: balance", len(rows), "preflash", len(pre), "illuminant", len(lit), "products", len(prods))
+
+
 def recipes():
     sys.path.insert(0, ROOT)
     import __graft_entry__
@@ -384,4 +457,5 @@ if __name__ == "__main__":
     density_model_cases()
     output_encoding_cases()
     abi_layout()
+    print_cases()
     recipes()
