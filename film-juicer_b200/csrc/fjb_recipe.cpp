@@ -340,6 +340,13 @@ bool create_recipe(const FjPreparedHostData& h, cudaStream_t stream, Recipe& r, 
                                     pr.sensitivity_cmy.data[l * 3 + 2]};
                 if (std::isnan(s[0]) && std::isnan(s[1]) && std::isnan(s[2])) continue;
                 const float il = pr.main_illuminant.data[l];
+                // a NaN dye or base density (or illuminant) makes the transmittance NaN
+                // for every pixel, and the print integral drops NaN transmittances
+                // (src/Cuda/JuicerCudaDeviceHelpers.cuh:860-864): the wavelength is idle
+                const float* eps = pr.film_density_cmy.data + l * 3;
+                if (std::isnan(eps[0]) || std::isnan(eps[1]) || std::isnan(eps[2]) ||
+                    std::isnan(pr.film_base_density.data[l]) || std::isnan(il))
+                    continue;
                 for (int c = 0; c < 3; ++c) p.spectral.nd[count][c] = -(pr.film_density_cmy.data[l * 3 + c] * kLog2Of10);
                 p.spectral.nd[count][3] = -(pr.film_base_density.data[l] * kLog2Of10);
                 for (int c = 0; c < 3; ++c)

@@ -11,9 +11,12 @@ packs them into the same C-ABI record the Rust host fills:
 * density curves: authored curves minus their per-channel minimum (film.rs:72-93);
 * DIR couplers: Langmuir donor model with compensated log-exposure axes that keep
   the neutral response (a simplified restatement of film/dir.rs:135-360);
-* print: negative dye spectra, paper sensitivity, lamp filtered by two dichroic
-  dials solved for a neutral mid-grey, mid-grey normalizer (print.rs:435-658,
-  simplified);
+* print: negative dye spectra, paper sensitivity (10^log in f32, non-finite -> 0),
+  the TH-KG3 enlarger lamp through the dichroics at the calibrated neutral
+  filtration, the preflash illuminant and raw integral, and the mid-grey balance
+  normaliser of the film's reference densities (print_prep: print.rs:120-658,
+  illuminant.rs:97-408, word for word; the reference densities come from this
+  module's film tables);
 * scanner: medium dye spectra with illuminant-weighted CIE 1931 CMFs
   (scanner.rs), density bounds of the medium;
 * output: CAT02 from the viewing illuminant to D65, XYZ->linear sRGB, sRGB CCTF,
@@ -33,7 +36,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import abi
+from . import abi, print_prep
 
 WAVELENGTHS = np.arange(380.0, 781.0, 5.0)
 N_LAMBDA = 81
@@ -191,12 +194,6 @@ def gamut_boundary_table(rows: int = 64, hues: int = 720, lmin: float = 0.02, lm
     return lo.astype(np.float32)
 
 
-def _smoothstep_filter(center: float, width: float, low_pass: bool) -> np.ndarray:
-    x = (WAVELENGTHS - center) / width
-    s = 0.5 * (1.0 + np.tanh(x))
-    return 1.0 - s if low_pass else s
-
-
 @dataclass
 class PreparedRecipe:
     """Arrays and scalars of one prepared render recipe (all float32 where the ABI is)."""
@@ -308,49 +305,53 @@ def prepare_recipe(resources: str, film: str, paper: str | None = None, *, dir_a
     if paper is not None:
         route = abi.FJ_ROUTE_NEGATIVE_PRINT
         pp = load_profile(os.path.join(resources, "profiles", f"{paper}.json"))
-        lamp = load_spectrum_csv(os.path.join(resources, "illuminants", "T.csv"))
-        psens = np.power(10.0, pp["log_sensitivity"])  # NaN stays NaN: skipped wavelengths
-        neg_dyes = np.nan_to_num(prof["channel_density"], nan=0.0)
-        neg_base = np.nan_to_num(prof["base_density"], nan=0.0)
-        mid = np.nan_to_num(prof["midscale_neutral_density"], nan=0.0)
-        t_mid = np.power(10.0, -mid)
-
-        def raw_for(filters):
-            y, m = filters
-            filt = (1 - y * _smoothstep_filter(505.0, 12.0, True)) * (1 - m * _smoothstep_filter(
-                540.0, 14.0, False) * _smoothstep_filter(590.0, 14.0, True))
-            ill = lamp * np.clip(filt, 0.0, 1.0)
-            return np.nansum((t_mid * ill)[:, None] * psens, axis=0), ill
-
-        # Solve the two dichroic dials so the mid-grey negative prints neutral (C = M = Y raw).
-        ym = np.array([0.5, 0.5])
-        for _ in range(60):
-            raw, _ = raw_for(ym)
-            lr = np.log10(raw)
-            err = np.array([lr[2] - lr[0], lr[1] - lr[0]])
-            if np.max(np.abs(err)) < 1e-7:
-                break
-            jac = np.zeros((2, 2))
-            for j in range(2):
-                dd = np.zeros(2)
-                dd[j] = 1e-5
-                r2, _ = raw_for(ym + dd)
-                l2 = np.log10(r2)
-                jac[:, j] = (np.array([l2[2] - l2[0], l2[1] - l2[0]]) - err) / 1e-5
-            ym = np.clip(ym - np.linalg.solve(jac, err), 0.0, 0.99)
-        raw, ill = raw_for(ym)
+        # The enlarger: the TH-KG3 lamp through the dichroics at the calibrated neutral
+        # filtration of this paper / lamp / film (recipe.rs:1709-1741, print.rs:120-158),
+        # the mid-grey balance of the film's reference densities under it (print.rs:435-523).
+        with open(os.path.join(resources, "filters", "heat_absorbing", "schott", "KG3.csv")) as fh:
+            lamp = print_prep.tungsten_kg3(print_prep.parse_csv_rows(fh.read()))
+        neutral, calibrated = print_prep.neutral_cmy_cc(resources, pp["info"].get("stock", paper), "TH-KG3",
+                                                        prof["info"].get("stock", film))
+        main_cc, preflash_cc = print_prep.filters(neutral)
+        main_ill = print_prep.filtered_illuminant(main_cc, lamp)
+        preflash_ill = print_prep.filtered_illuminant(preflash_cc, lamp)
+        psens = print_prep.linear_sensitivity(pp["log_sensitivity"])
+        neg_dyes = f32(prof["channel_density"])  # NaN kept: those wavelengths transmit nothing
+        neg_base = f32(prof["base_density"])
+        # The film's reference densities: the metered 18.4 % grey at 0 EV and at the
+        # manual exposure through the film's density curves (film/reference.rs:214-262).
+        # The reference's reconstruction balances that grey, so the metered grey lands at
+        # log exposure 0 in every channel (the reference's product records sit within
+        # 2e-4 of it) and at log10(2^ev) when compensated.
+        ax, cv = f32(log_e), f32(curves)
+        ref_density = []
+        for ev in (0.0, exposure_ev):
+            q = print_prep.F32(math.log10(2.0 ** ev))
+            ref_density.append(f32([print_prep.sample_density(q, ax, cv, c) for c in range(3)]))
+        ref_hash = print_prep.hash_u64s([print_prep.f32_bits(v) for v in np.concatenate(ref_density)])
+        balance = print_prep.Balance(ref_density[0], ref_density[1], ref_hash,
+                                     print_prep.normalization_mode(True, True), neg_base, neg_dyes, psens, main_ill)
+        preflash_raw = print_prep.preflash_raw(neg_base, preflash_ill, psens)
         ple = pp["log_exposure"].astype(np.float64)
         pcurves = profile_density_curves(pp)[0].astype(np.float64)
-        # Mid-grey negative lands on the paper's speed point (log exposure 0 on this axis).
-        a["print_film_density_cmy"] = f32(neg_dyes)
-        a["print_film_base_density"] = f32(neg_base)
+        a["print_film_density_cmy"] = neg_dyes
+        a["print_film_base_density"] = neg_base
         a["print_sensitivity_cmy"] = f32(psens)
         a["print_log_exposure"] = f32(ple)
         a["print_density_cmy"] = f32(pcurves)
-        a["print_main_illuminant"] = f32(ill)
+        a["print_main_illuminant"] = f32(main_ill)
+        a["print_preflash_illuminant"] = f32(preflash_ill)
         s["print_exposure"] = 1.0
-        s["print_normalizer"] = float(1.0 / raw[1])
-        s["print_filters_ym"] = ym.tolist()
+        s["print_normalizer"] = float(balance.normalizer)
+        s["print_reference_density_cmy"] = [[float(v) for v in d] for d in ref_density]
+        s["print_main_cc_cmy"] = [float(v) for v in main_cc]
+        s["print_preflash_cc_cmy"] = [float(v) for v in preflash_cc]
+        s["print_neutral_calibrated"] = bool(calibrated)
+        s["print_preflash_raw_cmy"] = [float(v) for v in preflash_raw]
+        s["print_balance_hash"] = str(balance.hash)
+        s["print_main_illuminant_hash"] = str(balance.filtered_main_illuminant_hash)
+        s["print_preflash_illuminant_hash"] = str(print_prep.hash_finite_f32s(preflash_ill) or 0)
+        s["print_preflash_raw_hash"] = str(print_prep.hash_finite_f32s(preflash_raw) or 0)
         medium_dyes = pp["channel_density"]
         medium_base = pp["base_density"]
         medium_curves = pcurves
@@ -517,7 +518,20 @@ class HostRecord:
             pr.main_illuminant = span(a["print_main_illuminant"])
             pr.exposure = s["print_exposure"]
             pr.normalizer = s["print_normalizer"]
-            pr.hash = pr.balance_hash = pr.film_density_hash = pr.profile_tables_hash = pr.main_illuminant_hash = 1
+            pr.hash = pr.film_density_hash = pr.profile_tables_hash = 1
+            pr.balance_hash = pr.main_illuminant_hash = 1
+            if "print_preflash_illuminant" in a:
+                pr.preflash_illuminant = span(a["print_preflash_illuminant"])
+                abi.set_floats(pr.main_cc_cmy, s["print_main_cc_cmy"])
+                abi.set_floats(pr.preflash_cc_cmy, s["print_preflash_cc_cmy"])
+                abi.set_floats(pr.preflash_raw_cmy, s["print_preflash_raw_cmy"])
+                pr.balance_hash = int(s["print_balance_hash"])
+                pr.main_illuminant_hash = int(s["print_main_illuminant_hash"])
+                pr.preflash_illuminant_hash = int(s["print_preflash_illuminant_hash"])
+                pr.preflash_raw_hash = int(s["print_preflash_raw_hash"])
+                pr.preflash_exposure = float(s.get("print_preflash_exposure", 0.0))
+                if pr.preflash_exposure > 0.0:
+                    pr.flags |= abi.FJ_PRINT_PREFLASH
 
         ae = h.auto_exposure
         ae.method = abi.FJ_METER_CENTER_WEIGHTED

@@ -17,6 +17,7 @@ computes them (rust/film-juicer-core/src/print.rs, recipe.rs, illuminant.rs).
 * `tungsten_kg3`: the enlarger lamp: a 3400 K Planck spectrum times the KG3 heat
   glass transmission resampled onto the axis by the reference's monotone cubic
   Hermite interpolation, normalised to mean 1 (illuminant.rs:97-128, 282-408);
+* `sample_density`: the reference densities' curve lookup (film/reference.rs:74-98);
 * `neutral_cmy_cc`: the calibrated neutral filtration of a paper / lamp / film
   triple, else the default (recipe.rs:1193-1215, 1709-1714).
 
@@ -404,6 +405,35 @@ def tungsten_kg3(kg3_rows) -> np.ndarray:
     with np.errstate(invalid="ignore"):
         samples = np.array([planck(_wavelength(i), 3400.0) * kg3[i] for i in range(N)], dtype=np.float32)
     return normalize_mean(samples)
+
+
+def sample_density(query, axis, curves, channel: int):
+    """Density of `channel` at log exposure `query` by linear interpolation on the
+    nondecreasing f32 axis, clamped to the end rows, in f32 (film/reference.rs:74-98);
+    None for a NaN query."""
+    q = F32(query)
+    if np.isnan(q):
+        return None
+    axis = np.asarray(axis, dtype=np.float32)
+    curves = np.asarray(curves, dtype=np.float32)
+    if q <= axis[0]:
+        return curves[0, channel]
+    if q >= axis[-1]:
+        return curves[-1, channel]
+    hi = int(np.searchsorted(axis, q, side="right"))
+    if hi == 0 or hi == axis.size:
+        return None
+    lo = hi - 1
+    span = axis[hi] - axis[lo]
+    t = (q - axis[lo]) / span if span > 0 else F32(0.0)
+    return curves[lo, channel] + t * (curves[hi, channel] - curves[lo, channel])
+
+
+def linear_sensitivity(log_sensitivity) -> np.ndarray:
+    """10^log in f32 through powf, non-finite -> 0 (profile/sampled.rs:419-424)."""
+    a = np.asarray(log_sensitivity, dtype=np.float32)
+    out = np.array([powf(10.0, v) for v in a.reshape(-1)], dtype=np.float32).reshape(a.shape)
+    return np.where(np.isfinite(out), out, np.float32(0.0)).astype(np.float32)
 
 
 def neutral_cmy_cc(resources: str, paper: str, illuminant: str, film: str):

@@ -76,9 +76,16 @@ def tables(record) -> dict:
         "corr_offset": float(t.corr_offset), "cat02": f(t.cat02), "xyz_to_rgb": f(t.xyz_to_rgb),
     }
     if t.print:
+        eps, base, ill = f(t.eps_cmy).reshape(NL, 3), f(t.base), f(t.illuminant)
+        sens = f(t.sens_cmy).reshape(NL, 3)
+        # A wavelength whose transmittance is NaN for every density (a NaN dye or base
+        # density, a NaN illuminant) contributes nothing, as the reference's print
+        # integral drops NaN transmittances (src/Cuda/JuicerCudaDeviceHelpers.cuh:860-864).
+        dead = np.isnan(eps).any(axis=1) | np.isnan(base) | np.isnan(ill)
+        eps[dead], base[dead], ill[dead], sens[dead] = 0.0, 0.0, 0.0, 0.0
         out.update({
-            "eps_cmy": f(t.eps_cmy).reshape(NL, 3), "base": f(t.base), "illuminant": f(t.illuminant),
-            "sens_cmy": f(t.sens_cmy).reshape(NL, 3), "midgray": float(t.midgray), "preflash": float(t.preflash),
+            "eps_cmy": eps, "base": base, "illuminant": ill,
+            "sens_cmy": sens, "midgray": float(t.midgray), "preflash": float(t.preflash),
             "preflash_raw": f(t.preflash_raw), "print_exposure": float(t.print_exposure),
             "print_route": float(t.print_route), "print_log_exposure": f(t.print_log_exposure, npr),
             "print_density_cmy": np.stack([f(t.print_density_cmy[c], npr) for c in range(3)]),

@@ -116,3 +116,40 @@ def test_filters_and_hash_helpers(pp):
     assert pp.hash_finite_f32s([1.0, np.nan]) is None
     assert pp.hash_u64s([]) == pp.FNV_OFFSET
     assert pp.f32_bits(pp.f32_from_decimal("0.1")) == 0x3DCCCCCD
+
+
+def test_print_recipe_tables_are_the_reference_products(cases, pp, recipes):
+    """kodak_portra_400 -> kodak_portra_endura (tests/golden/recipe_print.npz): the print
+    tables film_juicer_b200.prepare builds are the ones in the reference's balance
+    product records word for word (film base and dye densities, the paper's linear
+    sensitivity, the filtered TH-KG3 main illuminant at the calibrated neutral), the
+    balance of a product's reference densities on them is the product's balance word
+    for word, and the recipe's own normaliser (a metered grey at log exposure 0) is
+    within 2e-4 of that of the products at 0 EV whose reference densities lie within
+    2e-4 of the recipe's (the other products differ in reconstruction or
+    development settings)."""
+    rec = recipes["print"]
+    w = lambda a: np.ascontiguousarray(np.asarray(a, np.float32)).reshape(-1).view(np.uint32)  # noqa: E731
+    fields = (("film_base_density", "print_film_base_density"), ("film_channel_density_cmy", "print_film_density_cmy"),
+              ("print_sensitivity_rgb", "print_sensitivity_cmy"), ("filtered_main_illuminant", "print_main_illuminant"))
+    match = [i for i in range(len(cases["balance_id"]))
+             if cases["balance_success"][i] and int(cases["balance_mode"][i]) == 3
+             and all(np.array_equal(cases[f"balance_{k}"][i], w(rec.arrays[r])) for k, r in fields)]
+    assert len(match) >= 10
+    assert [float(v) for v in rec.scalars["print_main_cc_cmy"]] == [float(v) for v in _f(cases["product_main_cmy"][0])]
+    checked = 0
+    for i in match:
+        b = pp.Balance(_f(cases["balance_baseline_density_cmy"][i]), _f(cases["balance_compensated_density_cmy"][i]),
+                       int(cases["balance_reference_hash"][i]), 3, rec.arrays["print_film_base_density"],
+                       rec.arrays["print_film_density_cmy"], rec.arrays["print_sensitivity_cmy"],
+                       rec.arrays["print_main_illuminant"])
+        assert [pp.f32_bits(v) for v in b.scalars] == list(cases["balance_scalars"][i])
+        assert b.hash == int(cases["balance_hash"][i])
+        ours = np.asarray(rec.scalars["print_reference_density_cmy"][0])
+        theirs = _f(cases["balance_baseline_density_cmy"][i]).astype(np.float64)
+        if (np.array_equal(cases["balance_baseline_density_cmy"][i], cases["balance_compensated_density_cmy"][i])
+                and np.abs(ours - theirs).max() <= 2e-4):
+            checked += 1  # a product at 0 EV on the recipe's own reference densities
+            ref = float(_f(cases["balance_scalars"][i])[2])
+            assert abs(rec.scalars["print_normalizer"] - ref) <= 2e-4 * ref
+    assert checked >= 4
