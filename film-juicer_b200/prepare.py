@@ -8,9 +8,11 @@ packs them into the same C-ABI record the Rust host fills:
 * TC LUT: 192x192x81 Hanatos irradiance spectra contracted with the sensitivity,
   R,G,B,pad per node (reconstruction.rs:594-677; no spectral blur, no surface
   correction, no input-compression remap);
-* density curves: authored curves minus their per-channel minimum (film.rs:72-93);
-* DIR couplers: Langmuir donor model with compensated log-exposure axes that keep
-  the neutral response (a simplified restatement of film/dir.rs:135-360);
+* density curves: the profile's curves (the Gaussian density model where the profile
+  has one) minus their per-channel minimum, f32 (film.rs:72-93);
+* DIR couplers: the reference's capture recipe at the stock gammas (dir_prep:
+  film/dir.rs:135-365): coupler matrix, Langmuir knees and compensated log-exposure
+  axes, pinned on the reference's DIR characterization;
 * print: negative dye spectra, paper sensitivity (10^log in f32, non-finite -> 0),
   the TH-KG3 enlarger lamp through the dichroics at the calibrated neutral
   filtration, the preflash illuminant and raw integral, and the mid-grey balance
@@ -36,7 +38,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import abi, print_prep
+from . import abi, dir_prep, print_prep
 
 WAVELENGTHS = np.arange(380.0, 781.0, 5.0)
 N_LAMBDA = 81
@@ -215,20 +217,6 @@ class PreparedRecipe:
         return cls(int(z["route"]), arrays, json.loads(str(z["scalars"])))
 
 
-def _neutral_dir_axes(log_e, curves_rgb, matrix_rgb, dref, k):
-    """Compensated axes x'_c = x - correction_c(neutral layer densities at x).
-
-    A neutral exposure at x develops layer densities curves[x]; the donor Langmuir
-    term D (k + dref) / (k + D) feeds the receiver corrections through the coupler
-    matrix, and shifting the axis by that correction returns the authored density
-    for neutral input.
-    """
-    d = curves_rgb
-    donor = d * (k + dref)[None, :] / (k[None, :] + d)
-    corr = donor @ matrix_rgb  # [n, receiver RGB]
-    return np.stack([log_e - corr[:, c] for c in range(3)], axis=0)
-
-
 def prepare_recipe(resources: str, film: str, paper: str | None = None, *, dir_amount: float = 1.0,
                    lut_resolution: int = 17, gamut: bool = True, exposure_ev: float = 0.0) -> PreparedRecipe:
     """Builds a direct (paper=None) or print recipe from the profile directory `resources`."""
@@ -255,7 +243,10 @@ def prepare_recipe(resources: str, film: str, paper: str | None = None, *, dir_a
 
     log_e = prof["log_exposure"].astype(np.float64)
     model_totals, model_layers = profile_density_curves(prof)
-    curves = model_totals.astype(np.float64)
+    # the development's curves: the profile's curves minus their per-channel minimum,
+    # in f32 (film.rs:72-93), the curves the reference hands to the device
+    norm_curves, _, _, norm_hash = dir_prep.normalized_curves(model_totals)
+    curves = norm_curves.astype(np.float64)
     n = log_e.size
 
     a: dict[str, np.ndarray] = {}
@@ -284,19 +275,24 @@ def prepare_recipe(resources: str, film: str, paper: str | None = None, *, dir_a
     s["input_rgb_to_xyz"] = SRGB_TO_XYZ.ravel().tolist()
     s["xyz_to_linear_srgb"] = XYZ_TO_SRGB.ravel().tolist()
 
-    # DIR couplers (negative donor Langmuir), RGB order.
-    dmax = np.nanmax(curves, axis=0)
-    dref = 0.5 * dmax
-    kdon = np.full(3, 0.8)
-    inter = 0.25 * dir_amount
-    matrix = np.array([[1.0, inter, 0.4 * inter], [inter, 1.0, inter], [0.4 * inter, inter, 1.0]]) * 0.2 * dir_amount
-    s["dir_mode"] = 1 if dir_amount > 0 else 0
-    s["dir_matrix_rgb"] = matrix.ravel().tolist()
-    s["dir_dmax"] = dmax.tolist()
-    s["dir_dref"] = dref.tolist()
-    s["dir_donor_k"] = kdon.tolist()
-    if dir_amount > 0:
-        a["dir_axes_rgb"] = f32(_neutral_dir_axes(log_e, curves, matrix, dref, kdon))
+    # DIR couplers: the capture recipe at the stock gammas, amount `dir_amount`
+    # (film/dir.rs:135-365); matrix [donor][receiver], RGB order.
+    params = dir_prep.capture_defaults(active=dir_amount > 0)
+    params.amount = dir_amount
+    rec = dir_prep.DirRecipe(norm_curves, f32(log_e), prof["info"].get("type") == "positive", params,
+                             dir_prep.processing_defaults(prof["info"]), norm_hash)
+    s["dir_mode"] = int(rec.mode)
+    s["dir_matrix_rgb"] = [float(v) for v in rec.matrix_rgb.ravel()]
+    s["dir_dmax"] = [float(v) for v in rec.density_max_rgb]
+    s["dir_dref"] = [float(v) for v in rec.density_ref_rgb]
+    s["dir_donor_k"] = [float(v) for v in rec.donor_k_rgb]
+    s["dir_receiver_c_ref"] = [float(v) for v in rec.receiver_c_ref_rgb]
+    s["dir_receiver_kr"] = [float(v) for v in rec.receiver_kr_rgb]
+    s["dir_diffusion_um"] = [float(v) for v in rec.diffusion]
+    s["dir_hash"] = str(rec.hash)
+    s["dir_axes_hash"] = str(rec.axes_hash)
+    if rec.mode:
+        a["dir_axes_rgb"] = f32(rec.axes_rgb)
 
     route = abi.FJ_ROUTE_NEGATIVE_DIRECT
     medium_dyes = prof["channel_density"]
@@ -456,9 +452,12 @@ class HostRecord:
             abi.set_floats(dr.density_max_rgb, s["dir_dmax"])
             abi.set_floats(dr.density_ref_rgb, s["dir_dref"])
             abi.set_floats(dr.donor_k_rgb, s["dir_donor_k"])
+            abi.set_floats(dr.receiver_c_ref_rgb, s.get("dir_receiver_c_ref", [0.0] * 3))
+            abi.set_floats(dr.receiver_kr_rgb, s.get("dir_receiver_kr", [0.0] * 3))
             for c in range(3):
                 dr.compensated_axes_rgb[c] = span(a["dir_axes_rgb"][c])
-            dr.compensated_axes_hash = dr.hash = 1
+            dr.compensated_axes_hash = int(s.get("dir_axes_hash", 1)) or 1
+            dr.hash = int(s.get("dir_hash", 1)) or 1
 
         sb = h.scanner_bounds
         abi.set_floats(sb.min_cmy, s["scan_min_cmy"])

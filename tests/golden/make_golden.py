@@ -39,6 +39,10 @@ container, where the reference is mounted read-only).
   Rust build's words beside the native ones), the distinct product main / preflash
   illuminants on the TH-KG3 lamp, and the KG3 transmission rows (Resources/filters/
   heat_absorbing/schott/KG3.csv) that lamp is built from.
+* dir_recipe_cases.json: the reference's capture DIR characterization
+  (tests/film/dir-fixtures/linux.json, 64 products of four stocks): controls and the
+  exact words and hashes of each recipe, and per stock the profile's info block,
+  Gaussian density model and log-exposure axis.
 * recipe_direct.npz / recipe_print.npz: prepared recipes (film_juicer_b200.prepare)
   for kodak_portra_400 direct and kodak_portra_400 -> kodak_portra_endura print,
   built from the reference's Resources/ profiles and spectral tables.
@@ -426,6 +430,30 @@ def print_cases():
     print("print cases: balance", len(rows), "preflash", len(pre), "illuminant", len(lit), "products", len(prods))
 
 
+def dir_recipe_cases():
+    """Capture DIR recipe characterization (tests/film/dir-fixtures/linux.json): per case
+    the stock, its controls and the exact f32 words and hashes of the recipe; per stock
+    the profile's info block, Gaussian density model and log-exposure axis
+    (Resources/profiles) the development curves are sampled from."""
+    with open(os.path.join(REF, "tests", "film", "dir-fixtures", "linux.json")) as fh:
+        cases = json.load(fh)["cases"]
+    stocks = {}
+    for c in cases:
+        if c["key"] not in stocks:
+            with open(os.path.join(REF, "Resources", "profiles", f"{c['key']}.json")) as fh:
+                prof = json.load(fh)
+            stocks[c["key"]] = {"info": prof["info"], "model": prof["data"]["density_curves_model"],
+                                "log_exposure": prof["data"]["log_exposure"]}
+    keep = ("key", "kind", "route", "controls", "dir", "success", "diagnostic")
+    out = {"source": "tests/film/dir-fixtures/linux.json", "stocks": stocks,
+           "cases": [{k: c[k] for k in keep if k in c} | {"authored_minimum": c["bounds"]["authored_minimum"],
+                                                           "authored_maximum": c["bounds"]["authored_maximum"]}
+                     for c in cases]}
+    with open(os.path.join(HERE, "dir_recipe_cases.json"), "w") as fh:
+        json.dump(out, fh, separators=(",", ":"))
+    print("dir recipe cases:", len(cases), "stocks", len(stocks))
+
+
 def recipes():
     sys.path.insert(0, ROOT)
     import __graft_entry__
@@ -458,4 +486,5 @@ if __name__ == "__main__":
     output_encoding_cases()
     abi_layout()
     print_cases()
+    dir_recipe_cases()
     recipes()
