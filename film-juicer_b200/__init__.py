@@ -86,6 +86,18 @@ _EXPORTS = {
                                            C.c_void_p, C.c_ssize_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                            C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_size_t, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_fit_dir_source_carrier": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams)] + [C.c_void_p] * 3 +
+                                   [C.c_ssize_t] + [C.c_void_p] * 3 + [C.c_int32, C.c_int32, C.c_void_p,
+                                                                     C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_fit_forward_spatial_carrier": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams)] + [C.c_void_p] * 3 +
+                                        [C.c_ssize_t] + [C.c_void_p] * 6 + [C.c_int32, C.c_int32, C.c_void_p,
+                                                                          C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_fit_vjp_spatial_carrier": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams)] + [C.c_void_p] * 3 +
+                                    [C.c_ssize_t] + [C.c_void_p] * 6 + [C.c_int32, C.c_int32] + [C.c_void_p] * 8 +
+                                    [C.c_size_t, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_fit_dir_source_vjp_carrier": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams)] + [C.c_void_p] * 3 +
+                                       [C.c_ssize_t] + [C.c_void_p] * 3 + [C.c_int32, C.c_int32] +
+                                       [C.c_void_p] * 5 + [C.c_size_t, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
     "fjb_fit_vjp": (abi.FjStatus, [C.c_void_p, C.POINTER(abi.FjbFitParams), C.c_void_p, C.c_ssize_t, C.c_uint32,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                    C.c_size_t, C.c_void_p, C.POINTER(abi.FjErrorBuffer)]),
@@ -125,6 +137,9 @@ _EXPORTS = {
                                              C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_ssize_t, C.c_int32,
                                              C.c_int32] + [C.c_void_p] * 7 + [C.c_size_t, C.c_void_p,
                                                                                 C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_spatial_dir_blur": (abi.FjStatus, [C.POINTER(abi.FjSpatialDir)] + [C.c_void_p] * 6 +
+                             [C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, C.c_void_p,
+                              C.POINTER(abi.FjErrorBuffer)]),
     "fjb_recipe_set_spatial_dir_planes": (abi.FjStatus, [C.c_void_p] + [C.c_void_p] * 6 +
                                           [C.POINTER(abi.FjErrorBuffer)]),
     "fjb_dir_boundary_host": (abi.FjStatus, [C.POINTER(abi.FjDirGaussian), C.c_int32, C.POINTER(C.c_double),

@@ -22,6 +22,9 @@ using fjb::write_error;
 
 namespace fjb {
 
+cudaError_t dir_blur_planes(const DirPlan& plan, const float* const in[3], float* const out[3], int width, int height,
+                            float* scratch, cudaStream_t s);
+
 FjStatus spatial_dir_apply(FjbRecipe* recipe, const DirPlan& plan, const float* src, ptrdiff_t src_row_bytes,
                            uint32_t components, const float* carrier_b, const float* carrier_g, const float* carrier_r,
                            ptrdiff_t carrier_stride, int width, int height, float* filtered_y, float* filtered_m,
@@ -61,32 +64,41 @@ FjStatus spatial_dir_apply(FjbRecipe* recipe, const DirPlan& plan, const float* 
     p.dir_src_log_r = log_raw_r;
     cudaError_t e = launch_pixel_chain(p, carrier ? PixelStage::CarrierToDirSource : PixelStage::SourceToDirSource, s);
     if (e == cudaSuccess) {
-        DirBlurParams bp{};
-        bp.width = width;
-        bp.height = height;
-        {
-            const size_t planes_bytes =
-                ((size_t)(3 + 3 * kDirMaxComponents) * plane * sizeof(float) + 255) / 256 * 256;
-            char* rec = reinterpret_cast<char*>(scratch) + planes_bytes;
-            bp.lines_max = width > height ? width : height;
-            const int sw = dir_segments(width), sh = dir_segments(height);
-            bp.segs_max = sw > sh ? sw : sh;
-            bp.carry = reinterpret_cast<double*>(rec);
-            bp.start = bp.carry + (size_t)3 * kDirMaxComponents * bp.lines_max * bp.segs_max * 3;
-        }
-        bp.count = plan.count;
-        for (int k = 0; k < plan.count; ++k) bp.comp[k] = plan.comp[k];
+        const float* in[3] = {raw[0], raw[1], raw[2]};
         float* out[3] = {filtered_y, filtered_m, filtered_c};
-        for (int c = 0; c < 3; ++c) {
-            bp.raw[c] = raw[c];
-            bp.filtered[c] = out[c];
-            for (int k = 0; k < kDirMaxComponents; ++k)
-                bp.temp[c][k] = scratch + (3 + (size_t)c * kDirMaxComponents + k) * plane;
-        }
-        e = launch_dir_blur(bp, s);
+        e = dir_blur_planes(plan, in, out, width, height, scratch, s);
     }
     if (e != cudaSuccess) return cuda_status(e, error, "spatial DIR");
     return ok_status();
+}
+
+// The weighted Gaussian components of the plan on three dense width x height planes
+// (in -> out, Y, M, C), with the recursion buffers and component planes in `scratch`
+// (fjb_spatial_dir_scratch_bytes; its first three planes are not touched).
+cudaError_t dir_blur_planes(const DirPlan& plan, const float* const in[3], float* const out[3], int width, int height,
+                            float* scratch, cudaStream_t s) {
+    const size_t plane = (size_t)width * (size_t)height;
+    DirBlurParams bp{};
+    bp.width = width;
+    bp.height = height;
+    {
+        const size_t planes_bytes = ((size_t)(3 + 3 * kDirMaxComponents) * plane * sizeof(float) + 255) / 256 * 256;
+        char* rec = reinterpret_cast<char*>(scratch) + planes_bytes;
+        bp.lines_max = width > height ? width : height;
+        const int sw = dir_segments(width), sh = dir_segments(height);
+        bp.segs_max = sw > sh ? sw : sh;
+        bp.carry = reinterpret_cast<double*>(rec);
+        bp.start = bp.carry + (size_t)3 * kDirMaxComponents * bp.lines_max * bp.segs_max * 3;
+    }
+    bp.count = plan.count;
+    for (int k = 0; k < plan.count; ++k) bp.comp[k] = plan.comp[k];
+    for (int c = 0; c < 3; ++c) {
+        bp.raw[c] = in[c];
+        bp.filtered[c] = out[c];
+        for (int k = 0; k < kDirMaxComponents; ++k)
+            bp.temp[c][k] = scratch + (3 + (size_t)c * kDirMaxComponents + k) * plane;
+    }
+    return launch_dir_blur(bp, s);
 }
 
 } // namespace fjb
@@ -133,6 +145,50 @@ FjStatus fjb_spatial_dir_build(FjbRecipe* recipe, const FjSpatialDir* spatial_di
         return ok_status();
     } catch (...) {
         return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "unexpected exception in fjb_spatial_dir_build");
+    }
+}
+
+FjStatus fjb_spatial_dir_blur(const FjSpatialDir* spatial_dir, const float* in_y, const float* in_m,
+                              const float* in_c, float* out_y, float* out_m, float* out_c, int32_t width,
+                              int32_t height, float* scratch, size_t scratch_bytes, void* stream,
+                              FjErrorBuffer* error) {
+    try {
+        if (!spatial_dir || !in_y || !in_m || !in_c || !out_y || !out_m || !out_c)
+            return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+        if (width <= 0 || height <= 0) {
+            write_error(error, "");
+            return ok_status();
+        }
+        if (!scratch || scratch_bytes < fjb_spatial_dir_scratch_bytes(width, height))
+            return fail_status(FJ_STATUS_ALLOCATION_FAILURE, error, "spatial DIR scratch is too small");
+        if (reinterpret_cast<uintptr_t>(scratch) % 16 != 0)
+            return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "spatial DIR scratch must be 16-byte aligned");
+        const size_t plane = (size_t)width * (size_t)height;
+        const float* ins[3] = {in_y, in_m, in_c};
+        float* outs[3] = {out_y, out_m, out_c};
+        const float* region = scratch + 3 * plane;
+        for (int c = 0; c < 3; ++c)
+            if (ins[c] == outs[c] || (ins[c] >= scratch && ins[c] < region) || (outs[c] >= scratch && outs[c] < region))
+                return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "spatial DIR blur planes overlap");
+        cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+        fjb::DirPlan plan;
+        std::string why;
+        cudaError_t e = cudaSuccess;
+        if (!fjb::dir_plan_create(*spatial_dir, width, height, s, plan, why, e)) {
+            plan.release();
+            if (e != cudaSuccess) return cuda_status(e, error, "spatial DIR plan");
+            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, why);
+        }
+        e = fjb::dir_blur_planes(plan, ins, outs, width, height, scratch, s);
+        // the plan's device tables must outlive the kernels that read them
+        const cudaError_t e2 = cudaStreamSynchronize(s);
+        plan.release();
+        if (e != cudaSuccess) return cuda_status(e, error, "spatial DIR blur");
+        if (e2 != cudaSuccess) return cuda_status(e2, error, "spatial DIR blur");
+        write_error(error, "");
+        return ok_status();
+    } catch (...) {
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "unexpected exception in fjb_spatial_dir_blur");
     }
 }
 

@@ -199,10 +199,14 @@ __device__ __forceinline__ void print_spectral_moments(const PrintSpectral& s, c
 // with negative-donor DIR): d L(y_d[i], k_d) / d k_d for every donor d and knot i of the
 // compensated curves, [d * n + i]. `g_e0` (kGrad, may be null) receives the gradient
 // with respect to e0.
-template <bool kPrint, bool kGrad>
+// kSpatial (spatial DIR): the DIR corrections of the B, G, R receivers are the filtered
+// planes' values `cf` instead of the pixel's own donors (the capture development of
+// src/Cuda/JuicerCudaDeviceHelpers.cuh:1267-1328); the adjoint writes d / d cf into
+// `g_cf` and leaves the donors to the source stage's adjoint.
+template <bool kPrint, bool kGrad, bool kSpatial = false>
 __device__ bool fit_pixel(const PixelParams& p, const float* __restrict__ blob, const FitTheta& th, const float e0[3],
                           double rgb[3], const float* g_rgb, FitAcc* g_th, const float* __restrict__ dldk,
-                          float* g_e0) {
+                          float* g_e0, const float* cf = nullptr, float* g_cf = nullptr) {
     // ---- forward, keeping what the adjoint needs ----
     float e[3], logS[3], layer[3], sl[3];
     for (int c = 0; c < 3; ++c) {
@@ -218,19 +222,27 @@ __device__ bool fit_pixel(const PixelParams& p, const float* __restrict__ blob, 
     int dkn[3] = {-1, -1, -1};
     const bool dir = p.dir_mode == kDirNegativeDonor;
     if (dir) {
-        float donor[3];
-        for (int c = 0; c < 3; ++c) {
-            const float v = layer[c], k = th.k[c], r = p.dir_dref[c];
-            const float den = k + v;
-            donor[c] = v * (k + r) / den;
-            dv[c] = k * (k + r) / (den * den);
-            dk[c] = v * (v - r) / (den * den);
-            if (!isfinite(donor[c])) return false;
+        float corr[3];
+        if constexpr (kSpatial) {
+            for (int j = 0; j < 3; ++j) {
+                corr[j] = cf[j];
+                if (!isfinite(corr[j])) return false;
+            }
+        } else {
+            float donor[3];
+            for (int c = 0; c < 3; ++c) {
+                const float v = layer[c], k = th.k[c], r = p.dir_dref[c];
+                const float den = k + v;
+                donor[c] = v * (k + r) / den;
+                dv[c] = k * (k + r) / (den * den);
+                dk[c] = v * (v - r) / (den * den);
+                if (!isfinite(donor[c])) return false;
+            }
+            const float* M = p.dir_m;
+            for (int j = 0; j < 3; ++j) corr[j] = M[j] * donor[0] + M[3 + j] * donor[1] + M[6 + j] * donor[2];
         }
-        const float* M = p.dir_m;
         for (int j = 0; j < 3; ++j) {
-            const float corr = M[j] * donor[0] + M[3 + j] * donor[1] + M[6 + j] * donor[2];
-            logC[j] = logS[j] - corr;
+            logC[j] = logS[j] - corr[j];
             D[2 - j] = curve_with_slope(blob, p.dir_curve[j], logC[j], th.gamma[j], sd[j], dkn[j], dfr[j]);
         }
     } else {
@@ -335,10 +347,17 @@ __device__ bool fit_pixel(const PixelParams& p, const float* __restrict__ blob, 
             g_corr[j] = -g_logC;
         }
         const float* M = p.dir_m;
-        for (int i = 0; i < 3; ++i) {
-            const float g_donor = M[3 * i] * g_corr[0] + M[3 * i + 1] * g_corr[1] + M[3 * i + 2] * g_corr[2];
-            g_layer[i] = g_donor * dv[i];
-            g_th[9 + i] += (g_donor * dk[i]);
+        if constexpr (kSpatial) {
+            for (int j = 0; j < 3; ++j) {
+                g_cf[j] = g_corr[j];
+                g_layer[j] = 0.0f;
+            }
+        } else {
+            for (int i = 0; i < 3; ++i) {
+                const float g_donor = M[3 * i] * g_corr[0] + M[3 * i + 1] * g_corr[1] + M[3 * i + 2] * g_corr[2];
+                g_layer[i] = g_donor * dv[i];
+                g_th[9 + i] += (g_donor * dk[i]);
+            }
         }
         // The compensated axes depend on the knees (axis_j[i] = logE[i] - sum_d M[d][j]
         // L(y_d[i], k_d)): d D / d axis at the interval's knots is -slope (1 - t), -slope t.
@@ -419,6 +438,15 @@ struct FitCarrier {
     float* gb;
     float* gg;
     float* gr;
+    // spatial DIR: the filtered corrections of the B, G, R receivers (the Y, M, C
+    // planes of the spatial-DIR stage) and, for the adjoint, their gradient planes;
+    // all with the carrier's stride
+    const float* fy = nullptr;
+    const float* fm = nullptr;
+    const float* fc = nullptr;
+    float* gfy = nullptr;
+    float* gfm = nullptr;
+    float* gfc = nullptr;
 };
 
 // The film exposure e0 (B, G, R) of pixel idx: from the source RGB through the camera
@@ -440,8 +468,17 @@ __device__ __forceinline__ void load_exposure(const PixelParams& p, const FitCar
     }
 }
 
+// The filtered DIR corrections of pixel idx (spatial DIR, carrier layout).
+__device__ __forceinline__ void load_filtered(const PixelParams& p, const FitCarrier& cr, long long idx, float cf[3]) {
+    const int y = (int)(idx / p.width), x = (int)(idx - (long long)y * p.width);
+    const long long ci = (long long)y * cr.stride + x;
+    cf[0] = cr.fy[ci];
+    cf[1] = cr.fm[ci];
+    cf[2] = cr.fc[ci];
+}
+
 // Linear output RGB planes for theta (NaN where the chain rejects a pixel).
-template <bool kPrint, bool kCarrier>
+template <bool kPrint, bool kCarrier, bool kSpatial = false>
 __global__ void __launch_bounds__(kFitThreads, 2) fit_forward_kernel(const __grid_constant__ PixelParams p, FitTheta th,
                                                                   FitCarrier cr, float* out_r, float* out_g,
                                                                   float* out_b) {
@@ -450,10 +487,12 @@ __global__ void __launch_bounds__(kFitThreads, 2) fit_forward_kernel(const __gri
     const long long total = (long long)p.width * p.height;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
-        float e0[3];
+        float e0[3], cf[3] = {0.0f, 0.0f, 0.0f};
         load_exposure<kCarrier>(p, cr, idx, e0);
+        if constexpr (kSpatial) load_filtered(p, cr, idx, cf);
         double rgb[3];
-        const bool ok = fit_pixel<kPrint, false>(p, blob, th, e0, rgb, nullptr, nullptr, nullptr, nullptr);
+        const bool ok =
+            fit_pixel<kPrint, false, kSpatial>(p, blob, th, e0, rgb, nullptr, nullptr, nullptr, nullptr, cf, nullptr);
         out_r[idx] = ok ? (float)rgb[0] : nanf("");
         out_g[idx] = ok ? (float)rgb[1] : nanf("");
         out_b[idx] = ok ? (float)rgb[2] : nanf("");
@@ -465,7 +504,7 @@ constexpr int kFitParams = 13;
 // Per-block sums (FP64, fixed order) of the pixels' vector-Jacobian products; with
 // carrier input and gradient planes, also d <g, rgb> / d carrier per pixel (zero where
 // the chain rejects the pixel or the cotangent is zero).
-template <bool kPrint, bool kCarrier>
+template <bool kPrint, bool kCarrier, bool kSpatial = false>
 __global__ void __launch_bounds__(kFitThreads, 2) fit_vjp_kernel(const __grid_constant__ PixelParams p, FitTheta th,
                                                               FitCarrier cr, const float* __restrict__ g_r,
                                                               const float* __restrict__ g_g,
@@ -489,13 +528,25 @@ __global__ void __launch_bounds__(kFitThreads, 2) fit_vjp_kernel(const __grid_co
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
         const float g[3] = {g_r[idx], g_g[idx], g_b[idx]};
-        float ge[3] = {0.0f, 0.0f, 0.0f};
+        float ge[3] = {0.0f, 0.0f, 0.0f}, gcf[3] = {0.0f, 0.0f, 0.0f};
         float e0[3] = {0.0f, 0.0f, 0.0f};
         if (g[0] != 0.0f || g[1] != 0.0f || g[2] != 0.0f) {
             load_exposure<kCarrier>(p, cr, idx, e0);
+            float cf[3] = {0.0f, 0.0f, 0.0f};
+            if constexpr (kSpatial) load_filtered(p, cr, idx, cf);
             double rgb[3];
-            if (!fit_pixel<kPrint, true>(p, blob, th, e0, rgb, g, acc, dldk, carrier_grad ? ge : nullptr))
+            if (!fit_pixel<kPrint, true, kSpatial>(p, blob, th, e0, rgb, g, acc, dldk, carrier_grad ? ge : nullptr, cf,
+                                                   gcf)) {
                 ge[0] = ge[1] = ge[2] = 0.0f;
+                gcf[0] = gcf[1] = gcf[2] = 0.0f;
+            }
+        }
+        if constexpr (kSpatial) {
+            const int y = (int)(idx / p.width), x = (int)(idx - (long long)y * p.width);
+            const long long ci = (long long)y * cr.stride + x;
+            cr.gfy[ci] = gcf[0];
+            cr.gfm[ci] = gcf[1];
+            cr.gfc[ci] = gcf[2];
         }
         if (carrier_grad) {
             // e0 = max(0, carrier x route): the route factor inside, zero where clamped
@@ -527,6 +578,116 @@ __global__ void fit_reduce_kernel(const double* __restrict__ partials, int block
     out[k] = s;
 }
 
+// Spatial-DIR source of one pixel for theta (src/Cuda/Film/JuicerCudaFilmPipeline.cu:124-214):
+// the film exposure, the pre-DIR layer densities and the donor corrections they
+// release to the B, G, R receivers, corr_j = sum_d M[d][j] L(layer_d, k_d). With kGrad,
+// adds g_src^T d corr / d theta into g_th and writes d <g_src, corr> / d e0 into g_e0
+// (may be null). False (nothing added) where a value is not finite.
+template <bool kGrad>
+__device__ bool dir_source_pixel(const PixelParams& p, const float* __restrict__ blob, const FitTheta& th,
+                                 const float e0[3], float corr[3], const float* g_src, FitAcc* g_th, float* g_e0) {
+    float e[3], logS[3], layer[3], sl[3], donor[3], dv[3], dk[3];
+    for (int c = 0; c < 3; ++c) {
+        e[c] = e0[c] * exp2f(th.ev[c]);
+        logS[c] = log_exposure(e[c]);
+        if (!isfinite(logS[c])) return false;
+        int kn;
+        float fr;
+        layer[c] = curve_with_slope(blob, p.film_curve[c], logS[c], th.gamma[c], sl[c], kn, fr);
+        const float v = layer[c], k = th.k[c], r = p.dir_dref[c];
+        const float den = k + v;
+        donor[c] = v * (k + r) / den;
+        dv[c] = k * (k + r) / (den * den);
+        dk[c] = v * (v - r) / (den * den);
+        if (!isfinite(donor[c])) return false;
+    }
+    const float* M = p.dir_m;
+    for (int j = 0; j < 3; ++j) {
+        corr[j] = M[j] * donor[0] + M[3 + j] * donor[1] + M[6 + j] * donor[2];
+        if (!isfinite(corr[j])) return false;
+    }
+    if constexpr (kGrad) {
+        for (int i = 0; i < 3; ++i) {
+            const float g_donor = M[3 * i] * g_src[0] + M[3 * i + 1] * g_src[1] + M[3 * i + 2] * g_src[2];
+            const float g_layer = g_donor * dv[i];
+            g_th[9 + i] += (g_donor * dk[i]);
+            const float g_logS = g_layer * sl[i] * th.gamma[i];
+            g_th[3 + i] += (g_layer * sl[i] * logS[i]);
+            const float g_e = e[i] > 0.0f ? g_logS / ((e[i] + 1e-10f) * kLn10) : 0.0f;
+            g_th[i] += (g_e * e[i] * kLn2);
+            if (g_e0) g_e0[i] = g_e * exp2f(th.ev[i]);
+        }
+    }
+    return true;
+}
+
+// The source stage's correction planes (B, G, R receivers into cr.gfy/gfm/gfc's
+// layout: the Y, M, C planes), NaN where a pixel's source is not finite.
+template <bool kCarrier>
+__global__ void __launch_bounds__(kFitThreads, 2) fit_dir_source_kernel(const __grid_constant__ PixelParams p,
+                                                                     FitTheta th, FitCarrier cr, float* out_y,
+                                                                     float* out_m, float* out_c) {
+    extern __shared__ float4 fit_smem4[];
+    const float* blob = stage_blob(p, th, reinterpret_cast<float*>(fit_smem4));
+    const long long total = (long long)p.width * p.height;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        float e0[3], corr[3];
+        load_exposure<kCarrier>(p, cr, idx, e0);
+        const bool ok = dir_source_pixel<false>(p, blob, th, e0, corr, nullptr, nullptr, nullptr);
+        const int y = (int)(idx / p.width), x = (int)(idx - (long long)y * p.width);
+        const long long ci = (long long)y * cr.stride + x;
+        out_y[ci] = ok ? corr[0] : nanf("");
+        out_m[ci] = ok ? corr[1] : nanf("");
+        out_c[ci] = ok ? corr[2] : nanf("");
+    }
+}
+
+// Adjoint of the source stage: per-block FP64 sums of g_src^T d corr / d theta (g_src:
+// the cotangents of the correction planes before the spatial filter); with carrier
+// gradient planes, adds d <g_src, corr> / d carrier to them.
+template <bool kCarrier>
+__global__ void __launch_bounds__(kFitThreads, 2) fit_dir_source_vjp_kernel(const __grid_constant__ PixelParams p,
+                                                                         FitTheta th, FitCarrier cr,
+                                                                         const float* __restrict__ g_y,
+                                                                         const float* __restrict__ g_m,
+                                                                         const float* __restrict__ g_c,
+                                                                         double* partials) {
+    extern __shared__ float4 fit_smem4[];
+    const float* blob = stage_blob(p, th, reinterpret_cast<float*>(fit_smem4));
+    __shared__ double red[kFitThreads];
+    FitAcc acc[kFitParams];
+    for (int k = 0; k < kFitParams; ++k) acc[k] = 0.0f;
+    const bool carrier_grad = kCarrier && cr.gb != nullptr;
+    const long long total = (long long)p.width * p.height;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(idx / p.width), x = (int)(idx - (long long)y * p.width);
+        const long long ci = (long long)y * cr.stride + x;
+        const float g[3] = {g_y[ci], g_m[ci], g_c[ci]};
+        if (g[0] == 0.0f && g[1] == 0.0f && g[2] == 0.0f) continue;
+        float e0[3], corr[3], ge[3] = {0.0f, 0.0f, 0.0f};
+        load_exposure<kCarrier>(p, cr, idx, e0);
+        if (!dir_source_pixel<true>(p, blob, th, e0, corr, g, acc, carrier_grad ? ge : nullptr)) continue;
+        if (carrier_grad) {
+            const float rc = p.route_correction_scale;
+            if (e0[0] > 0.0f) cr.gb[ci] += ge[0] * rc;
+            if (e0[1] > 0.0f) cr.gg[ci] += ge[1] * rc;
+            if (e0[2] > 0.0f) cr.gr[ci] += ge[2] * rc;
+        }
+    }
+    for (int k = 0; k < kFitParams; ++k) {
+        red[threadIdx.x] = (double)acc[k];
+        __syncthreads();
+        for (int s = kFitThreads / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * kFitParams + k] = red[0];
+        __syncthreads();
+    }
+}
+
 int fit_blocks() {
     int device = 0, sms = 0;
     cudaGetDevice(&device);
@@ -555,22 +716,24 @@ bool theta_from(const FjbFitParams& f, FitTheta& th) {
 namespace fjb {
 namespace {
 
-template <bool kCarrier>
+template <bool kCarrier, bool kSpatial = false>
 cudaError_t launch_fit_forward(const PixelParams& p, const FitTheta& th, const FitCarrier& cr, float* out_r,
                                float* out_g, float* out_b, cudaStream_t s) {
     const size_t smem = (size_t)p.curve_blob_floats * sizeof(float);
     count_launch();
     if (p.route == kRoutePrint) {
-        cudaFuncSetAttribute(fit_forward_kernel<true, kCarrier>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        fit_forward_kernel<true, kCarrier><<<fit_blocks(), kFitThreads, smem, s>>>(p, th, cr, out_r, out_g, out_b);
+        auto* k = fit_forward_kernel<true, kCarrier, kSpatial>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<fit_blocks(), kFitThreads, smem, s>>>(p, th, cr, out_r, out_g, out_b);
     } else {
-        cudaFuncSetAttribute(fit_forward_kernel<false, kCarrier>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        fit_forward_kernel<false, kCarrier><<<fit_blocks(), kFitThreads, smem, s>>>(p, th, cr, out_r, out_g, out_b);
+        auto* k = fit_forward_kernel<false, kCarrier, kSpatial>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<fit_blocks(), kFitThreads, smem, s>>>(p, th, cr, out_r, out_g, out_b);
     }
     return cudaGetLastError();
 }
 
-template <bool kCarrier>
+template <bool kCarrier, bool kSpatial = false>
 cudaError_t launch_fit_vjp(const PixelParams& p, const FitTheta& th, const FitCarrier& cr, const float* grad_r,
                            const float* grad_g, const float* grad_b, double* partials, double* grad_params,
                            cudaStream_t s) {
@@ -578,12 +741,42 @@ cudaError_t launch_fit_vjp(const PixelParams& p, const FitTheta& th, const FitCa
     const size_t smem = fit_vjp_smem(p);
     count_launch();
     if (p.route == kRoutePrint) {
-        cudaFuncSetAttribute(fit_vjp_kernel<true, kCarrier>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        fit_vjp_kernel<true, kCarrier><<<blocks, kFitThreads, smem, s>>>(p, th, cr, grad_r, grad_g, grad_b, partials);
+        auto* k = fit_vjp_kernel<true, kCarrier, kSpatial>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<blocks, kFitThreads, smem, s>>>(p, th, cr, grad_r, grad_g, grad_b, partials);
     } else {
-        cudaFuncSetAttribute(fit_vjp_kernel<false, kCarrier>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        fit_vjp_kernel<false, kCarrier><<<blocks, kFitThreads, smem, s>>>(p, th, cr, grad_r, grad_g, grad_b, partials);
+        auto* k = fit_vjp_kernel<false, kCarrier, kSpatial>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<blocks, kFitThreads, smem, s>>>(p, th, cr, grad_r, grad_g, grad_b, partials);
     }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        count_launch();
+        fit_reduce_kernel<<<1, 32, 0, s>>>(partials, blocks, grad_params);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+cudaError_t launch_fit_dir_source(const PixelParams& p, const FitTheta& th, const FitCarrier& cr, float* out_y,
+                                  float* out_m, float* out_c, cudaStream_t s) {
+    const size_t smem = (size_t)p.curve_blob_floats * sizeof(float);
+    count_launch();
+    auto* k = fit_dir_source_kernel<true>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<fit_blocks(), kFitThreads, smem, s>>>(p, th, cr, out_y, out_m, out_c);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fit_dir_source_vjp(const PixelParams& p, const FitTheta& th, const FitCarrier& cr, const float* g_y,
+                                      const float* g_m, const float* g_c, double* partials, double* grad_params,
+                                      cudaStream_t s) {
+    const int blocks = fit_blocks();
+    const size_t smem = (size_t)p.curve_blob_floats * sizeof(float);
+    count_launch();
+    auto* k = fit_dir_source_vjp_kernel<true>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<blocks, kFitThreads, smem, s>>>(p, th, cr, g_y, g_m, g_c, partials);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) {
         count_launch();
@@ -729,6 +922,138 @@ FjStatus fjb_fit_vjp_carrier(FjbRecipe* recipe, const FjbFitParams* params, cons
         fjb::launch_fit_vjp<true>(p, th, cr, grad_r, grad_g, grad_b, static_cast<double*>(scratch), grad_params,
                                   reinterpret_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_status(e, error, "fit adjoint");
+    write_error(error, "");
+    return ok_status();
+}
+
+
+// ---- spatial DIR (carrier input) ----
+
+static FjStatus spatial_check(FjbRecipe* recipe, const FjbFitParams* params, const float* cb, const float* cg,
+                              const float* cr, ptrdiff_t stride, int32_t width, int32_t height, fjb::FitTheta& th,
+                              FjErrorBuffer* error) {
+    FjStatus st = fit_check(recipe, params, cb && cg && cr, 3, width, height, th, error);
+    if (st.category != FJ_STATUS_SUCCESS) return st;
+    if (recipe->r.params.dir_mode != fjb::kDirNegativeDonor)
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "spatial DIR fitting needs negative-donor DIR");
+    if (stride < width) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "carrier stride below the width");
+    return ok_status();
+}
+
+FjStatus fjb_fit_dir_source_carrier(FjbRecipe* recipe, const FjbFitParams* params, const float* carrier_b,
+                                    const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                                    float* corr_y, float* corr_m, float* corr_c, int32_t width, int32_t height,
+                                    void* stream, FjErrorBuffer* error) {
+    fjb::FitTheta th{};
+    FjStatus st = spatial_check(recipe, params, carrier_b, carrier_g, carrier_r, carrier_stride, width, height, th,
+                                error);
+    if (st.category != FJ_STATUS_SUCCESS) return st;
+    if (!corr_y || !corr_m || !corr_c) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    if ((long long)width * height > 0) {
+        fjb::PixelParams p = recipe->r.params;
+        p.width = width;
+        p.height = height;
+        const fjb::FitCarrier cr{carrier_b, carrier_g, carrier_r, (long long)carrier_stride, nullptr, nullptr, nullptr};
+        const cudaError_t e =
+            fjb::launch_fit_dir_source(p, th, cr, corr_y, corr_m, corr_c, reinterpret_cast<cudaStream_t>(stream));
+        if (e != cudaSuccess) return cuda_status(e, error, "fit DIR source");
+    }
+    write_error(error, "");
+    return ok_status();
+}
+
+FjStatus fjb_fit_forward_spatial_carrier(FjbRecipe* recipe, const FjbFitParams* params, const float* carrier_b,
+                                         const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                                         const float* filtered_y, const float* filtered_m, const float* filtered_c,
+                                         float* out_r, float* out_g, float* out_b, int32_t width, int32_t height,
+                                         void* stream, FjErrorBuffer* error) {
+    fjb::FitTheta th{};
+    FjStatus st = spatial_check(recipe, params, carrier_b, carrier_g, carrier_r, carrier_stride, width, height, th,
+                                error);
+    if (st.category != FJ_STATUS_SUCCESS) return st;
+    if (!out_r || !out_g || !out_b || !filtered_y || !filtered_m || !filtered_c)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    if ((long long)width * height > 0) {
+        fjb::PixelParams p = recipe->r.params;
+        p.width = width;
+        p.height = height;
+        fjb::FitCarrier cr{carrier_b, carrier_g, carrier_r, (long long)carrier_stride, nullptr, nullptr, nullptr};
+        cr.fy = filtered_y;
+        cr.fm = filtered_m;
+        cr.fc = filtered_c;
+        const cudaError_t e = fjb::launch_fit_forward<true, true>(p, th, cr, out_r, out_g, out_b,
+                                                                  reinterpret_cast<cudaStream_t>(stream));
+        if (e != cudaSuccess) return cuda_status(e, error, "fit forward");
+    }
+    write_error(error, "");
+    return ok_status();
+}
+
+FjStatus fjb_fit_vjp_spatial_carrier(FjbRecipe* recipe, const FjbFitParams* params, const float* carrier_b,
+                                     const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                                     const float* filtered_y, const float* filtered_m, const float* filtered_c,
+                                     const float* grad_r, const float* grad_g, const float* grad_b, int32_t width,
+                                     int32_t height, double* grad_params, float* grad_carrier_b, float* grad_carrier_g,
+                                     float* grad_carrier_r, float* grad_filtered_y, float* grad_filtered_m,
+                                     float* grad_filtered_c, void* scratch, size_t scratch_bytes, void* stream,
+                                     FjErrorBuffer* error) {
+    fjb::FitTheta th{};
+    FjStatus st = spatial_check(recipe, params, carrier_b, carrier_g, carrier_r, carrier_stride, width, height, th,
+                                error);
+    if (st.category != FJ_STATUS_SUCCESS) return st;
+    if (!grad_r || !grad_g || !grad_b || !grad_params || !scratch || !filtered_y || !filtered_m || !filtered_c ||
+        !grad_filtered_y || !grad_filtered_m || !grad_filtered_c)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    const bool planes = grad_carrier_b || grad_carrier_g || grad_carrier_r;
+    if (planes && !(grad_carrier_b && grad_carrier_g && grad_carrier_r))
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "carrier gradient planes: all three or none");
+    if (scratch_bytes < (size_t)fjb::fit_blocks() * fjb::kFitParams * sizeof(double))
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "fit scratch smaller than fjb_fit_scratch_bytes()");
+    fjb::PixelParams p = recipe->r.params;
+    p.width = width;
+    p.height = height;
+    fjb::FitCarrier cr{carrier_b,      carrier_g,      carrier_r,     (long long)carrier_stride,
+                       grad_carrier_b, grad_carrier_g, grad_carrier_r};
+    cr.fy = filtered_y;
+    cr.fm = filtered_m;
+    cr.fc = filtered_c;
+    cr.gfy = grad_filtered_y;
+    cr.gfm = grad_filtered_m;
+    cr.gfc = grad_filtered_c;
+    const cudaError_t e =
+        fjb::launch_fit_vjp<true, true>(p, th, cr, grad_r, grad_g, grad_b, static_cast<double*>(scratch), grad_params,
+                                        reinterpret_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_status(e, error, "fit adjoint");
+    write_error(error, "");
+    return ok_status();
+}
+
+FjStatus fjb_fit_dir_source_vjp_carrier(FjbRecipe* recipe, const FjbFitParams* params, const float* carrier_b,
+                                        const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                                        const float* grad_corr_y, const float* grad_corr_m, const float* grad_corr_c,
+                                        int32_t width, int32_t height, double* grad_params, float* grad_carrier_b,
+                                        float* grad_carrier_g, float* grad_carrier_r, void* scratch,
+                                        size_t scratch_bytes, void* stream, FjErrorBuffer* error) {
+    fjb::FitTheta th{};
+    FjStatus st = spatial_check(recipe, params, carrier_b, carrier_g, carrier_r, carrier_stride, width, height, th,
+                                error);
+    if (st.category != FJ_STATUS_SUCCESS) return st;
+    if (!grad_corr_y || !grad_corr_m || !grad_corr_c || !grad_params || !scratch)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    const bool planes = grad_carrier_b || grad_carrier_g || grad_carrier_r;
+    if (planes && !(grad_carrier_b && grad_carrier_g && grad_carrier_r))
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "carrier gradient planes: all three or none");
+    if (scratch_bytes < (size_t)fjb::fit_blocks() * fjb::kFitParams * sizeof(double))
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "fit scratch smaller than fjb_fit_scratch_bytes()");
+    fjb::PixelParams p = recipe->r.params;
+    p.width = width;
+    p.height = height;
+    const fjb::FitCarrier cr{carrier_b,      carrier_g,      carrier_r,     (long long)carrier_stride,
+                             grad_carrier_b, grad_carrier_g, grad_carrier_r};
+    const cudaError_t e = fjb::launch_fit_dir_source_vjp(p, th, cr, grad_corr_y, grad_corr_m, grad_corr_c,
+                                                         static_cast<double*>(scratch), grad_params,
+                                                         reinterpret_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_status(e, error, "fit DIR source adjoint");
     write_error(error, "");
     return ok_status();
 }

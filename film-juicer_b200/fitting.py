@@ -206,18 +206,26 @@ class FrameFit:
     """A frame's fitting problem: the recipe, the frame's optics descriptors and its
     camera exposure (computed once by the library: the optics parameters act after it).
 
-    host: the frame's FjPreparedHostData (a HostRecord's `.h`), with camera diffusion
-    and/or scatter/halation switched by its optics flags; spatial DIR, grain, enlarger
+    host: the frame's FjPreparedHostData (a HostRecord's `.h`), with camera diffusion,
+    scatter/halation and spatial DIR switched by its records; grain, enlarger
     diffusion, highlight reconstruction and auto exposure are outside this chain and
-    must be off. src: (H, W, 3|4) float32 CUDA source."""
+    must be off. src: (H, W, 3|4) float32 CUDA source.
+
+    With spatial DIR the development subtracts the filtered donor corrections: the
+    forward is the source stage, the frame's DIR filter and the development; the
+    adjoint runs the development's adjoint (theta, carrier and filtered-correction
+    gradients), filters the correction cotangent with the same filter (it is
+    symmetric, its own adjoint) and adds the source stage's adjoint."""
 
     def __init__(self, recipe: DeviceRecipe, host, src, stream=None):
         torch = _torch()
         o = host.optics
-        if host.spatial_dir.component_count or (host.grain.flags & abi.FJ_GRAIN_ACTIVE) or \
+        if (host.grain.flags & abi.FJ_GRAIN_ACTIVE) or \
                 (o.flags & (abi.FJ_OPTICS_ENLARGER_DIFFUSION | abi.FJ_OPTICS_HIGHLIGHT_BOOST)) or \
                 (host.film_exposure.flags & abi.FJ_FILM_AUTO_EXPOSURE):
-            raise ValueError("frame fitting covers camera diffusion and scatter/halation only")
+            raise ValueError("frame fitting covers camera diffusion, scatter/halation and spatial DIR only")
+        self.spatial = _copy(host.spatial_dir) if host.spatial_dir.component_count else None
+        self._dir_scratch = None
         self.recipe, self.stream = recipe, stream
         self.diffusion_on = bool(o.flags & abi.FJ_OPTICS_CAMERA_DIFFUSION)
         self.halation_on = bool(o.flags & abi.FJ_OPTICS_SCATTER_HALATION)
@@ -308,16 +316,46 @@ class FrameFit:
                 out[2 + c] = t
         return out
 
+    def dir_filter(self, planes_ymc):
+        """The frame's spatial DIR filter of three (H, W) planes (Y, M, C)."""
+        from .runtime import spatial_dir_blur
+
+        torch = _torch()
+        out = [torch.empty_like(p) for p in planes_ymc]
+        self._dir_scratch = spatial_dir_blur(self.spatial, [p.contiguous() for p in planes_ymc], out,
+                                             stream=self.stream, scratch=self._dir_scratch)
+        return out
+
+    def filtered_corrections(self, theta, carrier_rgb):
+        """Spatial DIR: the filtered donor corrections (Y, M, C) for theta."""
+        return self.dir_filter(dir_source_carrier(self.recipe, theta, carrier_rgb, stream=self.stream))
+
     def forward(self, theta, optics, out=None):
         """Linear output RGB planes (3, H, W) of the frame for theta (13) and optics (5)."""
         _, _, x3 = self.carriers(optics)
+        if self.spatial is not None:
+            cf = self.filtered_corrections(theta, x3)
+            return forward_spatial_carrier(self.recipe, theta, x3, cf, out=out, stream=self.stream)
         return forward_carrier(self.recipe, theta, x3, out=out, stream=self.stream)
+
+    def vjp_carrier(self, theta, carrier_rgb, grad_rgb):
+        """(d L / d theta (13,) float64 CUDA, d L / d carrier (R, G, B planes)) of the
+        chain after the optics, spatial DIR included."""
+        if self.spatial is None:
+            return vjp_carrier(self.recipe, theta, carrier_rgb, grad_rgb, stream=self.stream)
+        cf = self.filtered_corrections(theta, carrier_rgb)
+        g_dev, g_carrier, g_cf = vjp_spatial_carrier(self.recipe, theta, carrier_rgb, cf, grad_rgb,
+                                                     stream=self.stream)
+        g_src = self.dir_filter(g_cf)
+        g_source = dir_source_vjp_carrier(self.recipe, theta, carrier_rgb, g_src, grad_carrier_rgb=g_carrier,
+                                          stream=self.stream)
+        return g_dev + g_source, g_carrier
 
     def vjp(self, theta, optics, grad_rgb):
         """(d L / d theta (13,), d L / d optics (5,)) for L = <grad_rgb, rgb>, float64 CPU."""
         torch = _torch()
         x1, x2, x3 = self.carriers(optics)
-        g_theta, g_carrier = vjp_carrier(self.recipe, theta, x3, grad_rgb, stream=self.stream)
+        g_theta, g_carrier = self.vjp_carrier(theta, x3, grad_rgb)
         g_opt = torch.zeros(len(OPTIC_NAMES), dtype=torch.float64)
         for i, t in enumerate(self.tangents(optics, x1, x2)):
             if t is not None:
@@ -360,6 +398,86 @@ def vjp_carrier(recipe: DeviceRecipe, theta, carrier_rgb, grad_rgb, stream=None)
                                         C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
     _check("fjb_fit_vjp_carrier", st, err)
     return grad, [gc[2], gc[1], gc[0]]
+
+
+def _planes(ts):
+    return [C.c_void_p(_ptr(t)) for t in ts]
+
+
+def dir_source_carrier(recipe: DeviceRecipe, theta, carrier_rgb, stream=None):
+    """fjb_fit_dir_source_carrier: the donor corrections for theta as (Y, M, C) planes
+    (the B, G, R receivers), before the spatial DIR filter."""
+    torch = _torch()
+    r, g, b = carrier_rgb
+    h, w = r.shape
+    out = [torch.empty((h, w), dtype=torch.float32, device=r.device) for _ in range(3)]
+    params = _params(theta)
+    err = abi.ErrorText()
+    st = recipe.lib.fjb_fit_dir_source_carrier(recipe.handle, C.byref(params), *_planes((b, g, r)), r.stride(0),
+                                               *_planes(out), w, h, C.c_void_p(_stream_handle(stream)),
+                                               C.byref(err.buf))
+    _check("fjb_fit_dir_source_carrier", st, err)
+    return out
+
+
+def forward_spatial_carrier(recipe: DeviceRecipe, theta, carrier_rgb, filtered_ymc, out=None, stream=None):
+    """fjb_fit_forward_spatial_carrier: linear output RGB (3, H, W) developed with the
+    filtered DIR corrections (Y, M, C planes)."""
+    torch = _torch()
+    r, g, b = carrier_rgb
+    h, w = r.shape
+    if out is None:
+        out = torch.empty((3, h, w), dtype=torch.float32, device=r.device)
+    params = _params(theta)
+    err = abi.ErrorText()
+    st = recipe.lib.fjb_fit_forward_spatial_carrier(recipe.handle, C.byref(params), *_planes((b, g, r)), r.stride(0),
+                                                    *_planes(filtered_ymc), *_planes([out[c] for c in range(3)]), w, h,
+                                                    C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+    _check("fjb_fit_forward_spatial_carrier", st, err)
+    return out
+
+
+def vjp_spatial_carrier(recipe: DeviceRecipe, theta, carrier_rgb, filtered_ymc, grad_rgb, stream=None):
+    """fjb_fit_vjp_spatial_carrier: (d L / d theta of the development (13,) float64
+    CUDA, d L / d carrier (R, G, B planes), d L / d filtered corrections (Y, M, C))."""
+    torch = _torch()
+    r, g, b = carrier_rgb
+    h, w = r.shape
+    gr = grad_rgb.contiguous().to(torch.float32)
+    grad = torch.empty(N_PARAMS, dtype=torch.float64, device=r.device)
+    gc = [torch.empty((h, w), dtype=torch.float32, device=r.device) for _ in range(3)]  # B, G, R
+    gf = [torch.empty((h, w), dtype=torch.float32, device=r.device) for _ in range(3)]  # Y, M, C
+    scratch = _SCRATCH.get(torch, r.device)
+    params = _params(theta)
+    err = abi.ErrorText()
+    st = recipe.lib.fjb_fit_vjp_spatial_carrier(recipe.handle, C.byref(params), *_planes((b, g, r)), r.stride(0),
+                                                *_planes(filtered_ymc), *_planes([gr[c] for c in range(3)]), w, h,
+                                                C.c_void_p(_ptr(grad)), *_planes(gc), *_planes(gf),
+                                                C.c_void_p(_ptr(scratch)), scratch.numel(),
+                                                C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+    _check("fjb_fit_vjp_spatial_carrier", st, err)
+    return grad, [gc[2], gc[1], gc[0]], gf
+
+
+def dir_source_vjp_carrier(recipe: DeviceRecipe, theta, carrier_rgb, grad_corr_ymc, grad_carrier_rgb=None,
+                           stream=None):
+    """fjb_fit_dir_source_vjp_carrier: d L / d theta (13,) float64 CUDA of the source
+    stage for the corrections' cotangent; adds d L / d carrier into grad_carrier_rgb
+    (R, G, B planes) when given."""
+    torch = _torch()
+    r, g, b = carrier_rgb
+    h, w = r.shape
+    grad = torch.empty(N_PARAMS, dtype=torch.float64, device=r.device)
+    scratch = _SCRATCH.get(torch, r.device)
+    gc = [C.c_void_p(0)] * 3 if grad_carrier_rgb is None else _planes(grad_carrier_rgb[::-1])  # B, G, R
+    params = _params(theta)
+    err = abi.ErrorText()
+    st = recipe.lib.fjb_fit_dir_source_vjp_carrier(recipe.handle, C.byref(params), *_planes((b, g, r)), r.stride(0),
+                                                   *_planes(grad_corr_ymc), w, h, C.c_void_p(_ptr(grad)), *gc,
+                                                   C.c_void_p(_ptr(scratch)), scratch.numel(),
+                                                   C.c_void_p(_stream_handle(stream)), C.byref(err.buf))
+    _check("fjb_fit_dir_source_vjp_carrier", st, err)
+    return grad
 
 
 def _frame_function():

@@ -263,6 +263,26 @@ def auto_exposure(recipe: "DeviceRecipe", src, meter: "abi.FjAutoExposure", scal
     _check("fjb_auto_exposure", st, err)
 
 
+def spatial_dir_blur(spatial_dir: "abi.FjSpatialDir", planes_ymc, out_ymc, stream=None, scratch=None):
+    """fjb_spatial_dir_blur: the spatial DIR filter of three dense (H, W) float32 CUDA
+    planes (Y, M, C) into `out_ymc`; returns the scratch for reuse."""
+    torch = _torch()
+    lib = load_library()
+    h, w = planes_ymc[0].shape
+    for t in (*planes_ymc, *out_ymc):
+        if not t.is_contiguous() or tuple(t.shape) != (h, w):
+            raise ValueError("spatial DIR blur planes must be dense (H, W) tensors of one size")
+    need = int(lib.fjb_spatial_dir_scratch_bytes(w, h))
+    if scratch is None or scratch.numel() * 4 < need:
+        scratch = torch.empty(need // 4 + 1, dtype=torch.float32, device=planes_ymc[0].device)
+    err = abi.ErrorText()
+    st = lib.fjb_spatial_dir_blur(C.byref(spatial_dir), *[C.c_void_p(_ptr(t)) for t in (*planes_ymc, *out_ymc)], w, h,
+                                  C.c_void_p(_ptr(scratch)), scratch.numel() * 4, C.c_void_p(_stream_handle(stream)),
+                                  C.byref(err.buf))
+    _check("fjb_spatial_dir_blur", st, err)
+    return scratch
+
+
 def scatter_halation(descriptor: "abi.FjScatterHalation", planes_rgb, stream=None, scratch=None):
     """In-place scatter/halation on three CUDA planes (R, G, B), each (H, W) float32."""
     torch = _torch()

@@ -124,6 +124,39 @@ FjStatus fjb_fit_vjp_carrier(FjbRecipe* recipe, const FjbFitParams* params, cons
                              int32_t height, double* grad_params, float* grad_carrier_b, float* grad_carrier_g,
                              float* grad_carrier_r, void* scratch, size_t scratch_bytes, void* stream,
                              FjErrorBuffer* error);
+/* Spatial DIR (negative-donor couplers), in three steps around the frame's DIR filter
+ * (fjb_spatial_dir_blur): fjb_fit_dir_source_carrier writes the donor corrections of
+ * the B, G, R receivers (planes Y, M, C) for theta; the caller filters them;
+ * fjb_fit_forward_spatial_carrier develops with the filtered corrections. The adjoint
+ * runs backwards: fjb_fit_vjp_spatial_carrier gives the theta gradient of the
+ * development, the carrier gradient planes and d L / d filtered correction
+ * (grad_filtered_*); the filter is symmetric (its own adjoint), so the caller filters
+ * that cotangent and fjb_fit_dir_source_vjp_carrier adds the source stage's theta
+ * gradient (into its own grad_params) and ADDS its carrier gradient into grad_carrier_*.
+ * Every plane uses carrier_stride. */
+FjStatus fjb_fit_dir_source_carrier(FjbRecipe* recipe, const FjbFitParams* params, const float* carrier_b,
+                                    const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                                    float* corr_y, float* corr_m, float* corr_c, int32_t width, int32_t height,
+                                    void* stream, FjErrorBuffer* error);
+FjStatus fjb_fit_forward_spatial_carrier(FjbRecipe* recipe, const FjbFitParams* params, const float* carrier_b,
+                                         const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                                         const float* filtered_y, const float* filtered_m, const float* filtered_c,
+                                         float* out_r, float* out_g, float* out_b, int32_t width, int32_t height,
+                                         void* stream, FjErrorBuffer* error);
+FjStatus fjb_fit_vjp_spatial_carrier(FjbRecipe* recipe, const FjbFitParams* params, const float* carrier_b,
+                                     const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                                     const float* filtered_y, const float* filtered_m, const float* filtered_c,
+                                     const float* grad_r, const float* grad_g, const float* grad_b, int32_t width,
+                                     int32_t height, double* grad_params, float* grad_carrier_b, float* grad_carrier_g,
+                                     float* grad_carrier_r, float* grad_filtered_y, float* grad_filtered_m,
+                                     float* grad_filtered_c, void* scratch, size_t scratch_bytes, void* stream,
+                                     FjErrorBuffer* error);
+FjStatus fjb_fit_dir_source_vjp_carrier(FjbRecipe* recipe, const FjbFitParams* params, const float* carrier_b,
+                                        const float* carrier_g, const float* carrier_r, ptrdiff_t carrier_stride,
+                                        const float* grad_corr_y, const float* grad_corr_m, const float* grad_corr_c,
+                                        int32_t width, int32_t height, double* grad_params, float* grad_carrier_b,
+                                        float* grad_carrier_g, float* grad_carrier_r, void* scratch,
+                                        size_t scratch_bytes, void* stream, FjErrorBuffer* error);
 
 /* Device error word (bit 0 scan failure, bit 8 DIR failure, bits 9..11 DIR
  * channels B,G,R, bit 16 a tensor-core wait of the print stage gave up). Cleared by fjb_recipe_clear_flags, read by fjb_recipe_read_flags
@@ -317,6 +350,16 @@ FjStatus fjb_spatial_dir_build(FjbRecipe* recipe, const FjSpatialDir* spatial_di
                                int32_t width, int32_t height, float* filtered_y, float* filtered_m,
                                float* filtered_c, float* log_raw_b, float* log_raw_g, float* log_raw_r,
                                float* scratch, size_t scratch_bytes, void* stream, FjErrorBuffer* error);
+
+/* The spatial DIR filter alone (the weighted Gaussian components of `spatial_dir`) on
+ * three dense width x height planes Y, M, C, in -> out (distinct buffers). The
+ * operator is linear and symmetric (half-sample reflected boundaries, symmetric
+ * components), so it is also its own adjoint. `scratch` as for fjb_spatial_dir_build.
+ * Synchronises `stream`. */
+FjStatus fjb_spatial_dir_blur(const FjSpatialDir* spatial_dir, const float* in_y, const float* in_m,
+                              const float* in_c, float* out_y, float* out_m, float* out_c, int32_t width,
+                              int32_t height, float* scratch, size_t scratch_bytes, void* stream,
+                              FjErrorBuffer* error);
 
 /* Makes later capture-development calls on `recipe` use spatially filtered DIR
  * corrections and cached log exposure (all six device planes, or all NULL to return

@@ -224,9 +224,13 @@ class Chain:
         m = t["dir_m"].reshape(3, 3)  # [donor][receiver]
         return t["log_exposure"][None, :] - (m.T @ donors)
 
-    def __call__(self, e0, theta):
+    def __call__(self, e0, theta, spatial=None):
         """e0: camera exposure (3, N) B, G, R (float64 tensor); theta (13,) float64.
-        Returns the linear output RGB (3, N) (NaN where the LUT rejects a pixel)."""
+        Returns the linear output RGB (3, N) (NaN where the LUT rejects a pixel).
+        spatial: the spatial DIR filter, a differentiable map of the donor corrections
+        of the B, G, R receivers (3, N) to the filtered corrections the development
+        subtracts (src/Cuda/JuicerCudaDeviceHelpers.cuh:1267-1328); None for runtime
+        DIR, where each pixel subtracts its own corrections."""
         torch, t = self.torch, self.t
         ev, gam, pgam, k, pev = theta[0:3], theta[3:6], theta[6:9], theta[9:12], theta[12]
         e = e0 * torch.exp2(ev)[:, None]
@@ -237,6 +241,8 @@ class Chain:
             donor = _langmuir(torch, layer, k[:, None], t["dir_dref"][:, None])
             m = t["dir_m"].reshape(3, 3)
             corr = m.T @ donor
+            if spatial is not None:
+                corr = spatial(corr)
             logc = logs - corr
             ax = self.axes(k)
             dens_bgr = [_curve(torch, ax[j], t["density_bgr"][j], logc[j] * gam[j]) for j in range(3)]
