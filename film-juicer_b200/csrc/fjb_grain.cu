@@ -125,25 +125,27 @@ struct GrainRng {
         frame_row_base = (size_t)wf * (size_t)f->stbn_h;
     }
 
-    __device__ __forceinline__ float uniform() {
-        if (use_stbn) {
-            const uint32_t d = draw++;
-            const uint64_t h = splitmix64(seed + (uint64_t)d * 0x9E3779B97F4A7C15ULL);
-            const int ox = (int)(h & 0xFFFFu) + off_x;
-            const int oy = (int)((h >> 16) & 0xFFFFu) + off_y;
-            const int64_t xc = (int64_t)abs_x + (int64_t)ox + (int64_t)f->stbn_offset_x;
-            const int64_t yc = (int64_t)abs_y + (int64_t)oy + (int64_t)f->stbn_offset_y + pitch_offset;
-            int x, y;
-            if (mask_w >= 0) {
-                x = (int)((uint64_t)xc & (uint64_t)mask_w);
-                y = (int)((uint64_t)yc & (uint64_t)mask_h);
-            } else {
-                x = wrap_coordinate(xc, f->stbn_w);
-                y = wrap_coordinate(yc, f->stbn_h);
-            }
-            const uint8_t v = __ldg(f->stbn + ((frame_row_base + (size_t)y) * (size_t)f->stbn_w + (size_t)x));
-            return ((float)v + 0.5f) * (1.0f / 256.0f);
+    // The blue-noise uniform of draw d (its table address depends on d alone).
+    __device__ __forceinline__ float stbn_at(uint32_t d) const {
+        const uint64_t h = splitmix64(seed + (uint64_t)d * 0x9E3779B97F4A7C15ULL);
+        const int ox = (int)(h & 0xFFFFu) + off_x;
+        const int oy = (int)((h >> 16) & 0xFFFFu) + off_y;
+        const int64_t xc = (int64_t)abs_x + (int64_t)ox + (int64_t)f->stbn_offset_x;
+        const int64_t yc = (int64_t)abs_y + (int64_t)oy + (int64_t)f->stbn_offset_y + pitch_offset;
+        int x, y;
+        if (mask_w >= 0) {
+            x = (int)((uint64_t)xc & (uint64_t)mask_w);
+            y = (int)((uint64_t)yc & (uint64_t)mask_h);
+        } else {
+            x = wrap_coordinate(xc, f->stbn_w);
+            y = wrap_coordinate(yc, f->stbn_h);
         }
+        const uint8_t v = __ldg(f->stbn + ((frame_row_base + (size_t)y) * (size_t)f->stbn_w + (size_t)x));
+        return ((float)v + 0.5f) * (1.0f / 256.0f);
+    }
+
+    __device__ __forceinline__ float uniform() {
+        if (use_stbn) return stbn_at(draw++);
         // u01: x * 2^-32 + 2^-33 (the product is exact, so the fma is too)
         return __fmaf_rn((float)philox.next(), 1.0f / 4294967296.0f, 0.5f / 4294967296.0f);
     }
@@ -157,12 +159,36 @@ struct GrainRng {
     }
 };
 
+constexpr int kStbnBatch = 4;
+
 __device__ __forceinline__ int poisson(float lambda, GrainRng& rng) {
     if (!finite(lambda) || !(lambda > 0.0f)) return 0;
     if (lambda < 10.0f) {
         const float L = expf(-lambda);
         float p = 1.0f;
         int k = 0;
+        if (rng.use_stbn) {
+            // The same draws in the same order, fetched kStbnBatch at a time: the
+            // blue-noise addresses do not depend on earlier draws, so the table loads
+            // overlap instead of paying one cache latency per draw. Draws fetched past
+            // the stop are not consumed (the draw index advances by the draws used).
+            while (p > L && k < 1024) {
+                float u[kStbnBatch];
+#pragma unroll
+                for (int j = 0; j < kStbnBatch; ++j) u[j] = rng.stbn_at(rng.draw + (uint32_t)j);
+                uint32_t used = 0;
+#pragma unroll
+                for (int j = 0; j < kStbnBatch; ++j) {
+                    if (p > L && k < 1024) {
+                        ++k;
+                        ++used;
+                        p *= clamp01(u[j], 1e-7f, 1.0f);
+                    }
+                }
+                rng.draw += used;
+            }
+            return k - 1;
+        }
         while (p > L && k < 1024) {
             ++k;
             p *= clamp01(rng.uniform(), 1e-7f, 1.0f);
