@@ -108,13 +108,14 @@ struct GrainRng {
     int use_stbn, off_x, off_y;
     int64_t pitch_offset;
     size_t frame_row_base;
+    const uint8_t* frame_base; // the blue-noise frame's first row
     int mask_w, mask_h;
 
     __device__ GrainRng(const GrainFrame* frame, uint64_t s, uint64_t ax, uint64_t ay, int stbn, int frame_offset,
                         int wang_x, int wang_y)
         : philox(s, (uint32_t)ax, kPhiloxGlobalSeed, (uint32_t)ay), f(frame), abs_x(ax), abs_y(ay), seed(s),
-          draw(0), use_stbn(stbn), off_x(wang_x), off_y(wang_y), pitch_offset(0), frame_row_base(0), mask_w(-1),
-          mask_h(-1) {
+          draw(0), use_stbn(stbn), off_x(wang_x), off_y(wang_y), pitch_offset(0), frame_row_base(0),
+          frame_base(nullptr), mask_w(-1), mask_h(-1) {
         if (!use_stbn) return;
         if ((f->stbn_w & (f->stbn_w - 1)) == 0 && (f->stbn_h & (f->stbn_h - 1)) == 0) {
             mask_w = f->stbn_w - 1;
@@ -123,6 +124,7 @@ struct GrainRng {
         if (f->pitch_px > 0) pitch_offset = (int64_t)f->pitch_px * (f->frame_index + (int64_t)frame_offset);
         const int wf = wrap_coordinate((int64_t)f->stbn_frame + (int64_t)frame_offset, f->stbn_frames);
         frame_row_base = (size_t)wf * (size_t)f->stbn_h;
+        frame_base = f->stbn + frame_row_base * (size_t)f->stbn_w;
     }
 
     // The blue-noise uniform of draw d (its table address depends on d alone).
@@ -130,16 +132,19 @@ struct GrainRng {
         const uint64_t h = splitmix64(seed + (uint64_t)d * 0x9E3779B97F4A7C15ULL);
         const int ox = (int)(h & 0xFFFFu) + off_x;
         const int oy = (int)((h >> 16) & 0xFFFFu) + off_y;
+        if (mask_w >= 0) {
+            // power-of-two table: the masked coordinate keeps only low bits of the
+            // 64-bit sum, which the 32-bit sum of the addends' low words already has
+            const uint32_t xm = ((uint32_t)abs_x + (uint32_t)ox + (uint32_t)f->stbn_offset_x) & (uint32_t)mask_w;
+            const uint32_t ym =
+                ((uint32_t)abs_y + (uint32_t)oy + (uint32_t)f->stbn_offset_y + (uint32_t)pitch_offset) & (uint32_t)mask_h;
+            const uint8_t v = __ldg(frame_base + ((size_t)ym * (size_t)(uint32_t)f->stbn_w + xm));
+            return ((float)v + 0.5f) * (1.0f / 256.0f);
+        }
         const int64_t xc = (int64_t)abs_x + (int64_t)ox + (int64_t)f->stbn_offset_x;
         const int64_t yc = (int64_t)abs_y + (int64_t)oy + (int64_t)f->stbn_offset_y + pitch_offset;
-        int x, y;
-        if (mask_w >= 0) {
-            x = (int)((uint64_t)xc & (uint64_t)mask_w);
-            y = (int)((uint64_t)yc & (uint64_t)mask_h);
-        } else {
-            x = wrap_coordinate(xc, f->stbn_w);
-            y = wrap_coordinate(yc, f->stbn_h);
-        }
+        const int x = wrap_coordinate(xc, f->stbn_w);
+        const int y = wrap_coordinate(yc, f->stbn_h);
         const uint8_t v = __ldg(f->stbn + ((frame_row_base + (size_t)y) * (size_t)f->stbn_w + (size_t)x));
         return ((float)v + 0.5f) * (1.0f / 256.0f);
     }
