@@ -556,13 +556,50 @@ def fit_block(torch, prepare, runtime, recipe, args, stream, barrier, max_over_r
     grad = gout.cpu()
     dr.close()
     px = s.shape[0] * s.shape[1]
+    frame = frame_fit_block(torch, prepare, runtime, recipe, stream, th0, thp, timed)
     return {"workload": "16 x 512 x 512 seeded crops, print route, 13 parameters (exposure_ev BGR, film_gamma BGR, "
                         "print_gamma CMY, donor_k BGR, print_ev)",
             "forward_ms": round(fwd, 4), "adjoint_ms": round(bwd, 4), "fwd_bwd_ms": round(fwd + bwd, 4),
             "fwd_bwd_over_forward": round((fwd + bwd) / fwd, 3),
             "pixel_render_ms": round(ren, 4), "fwd_bwd_over_pixel_render": round((fwd + bwd) / ren, 3),
             "fwd_bwd_mpix_s": round(px / ((fwd + bwd) * 1e-3) / 1e6, 1),
-            "gradient_finite": bool(torch.isfinite(grad).all()), "steps": steps, "regions": 5}
+            "gradient_finite": bool(torch.isfinite(grad).all()), "steps": steps, "regions": 5, "frame": frame}
+
+
+def frame_fit_block(torch, prepare, runtime, recipe, stream, th0, thp, timed):
+    """Whole-frame fitting: a 1920x1080 print frame with camera diffusion,
+    scatter/halation and spatial DIR on (fitting.FrameFit): the forward (optics
+    stages, DIR source, DIR filter, development) and the adjoint (13 parameters and the
+    5 optics parameters: the development's adjoint, the filtered-correction cotangent
+    through the DIR filter, the source stage's adjoint, the optics tangents), timed
+    with CUDA events around the Python calls (host-side gaps included)."""
+    from film_juicer_b200 import fitting, frame_records
+
+    fw, fh = 1920, 1080
+    rec = frame_records.FrameRecord(recipe, fw, fh, recipe_hash=0xF17, grain=False)
+    dr = runtime.DeviceRecipe(rec.host, stream=stream)
+    src = torch.from_numpy(prepare.synthetic_frame(fw, fh, seed=SEED + 150)).to("cuda")
+    ff = fitting.FrameFit(dr, rec.host.h, src, stream=stream)
+    opt = ff.optics_default()
+    with torch.cuda.stream(stream):
+        target = ff.forward(th0, opt).clone()
+        out = torch.empty_like(target)
+    fwd = timed(lambda: ff.forward(thp, opt, out=out))
+    with torch.cuda.stream(stream):
+        cot = (2.0 / out.numel()) * (out - target)
+    grads = {}
+
+    def adjoint():
+        grads["g"] = ff.vjp(thp, opt, cot)
+
+    bwd = timed(adjoint)
+    g_theta, g_opt = grads["g"]
+    ff.close()
+    dr.close()
+    return {"workload": "1920x1080 print frame, camera diffusion + scatter/halation + spatial DIR, 13 + 5 parameters",
+            "forward_ms": round(fwd, 4), "adjoint_ms": round(bwd, 4), "fwd_bwd_ms": round(fwd + bwd, 4),
+            "fwd_bwd_over_forward": round((fwd + bwd) / fwd, 3),
+            "gradient_finite": bool(torch.isfinite(g_theta).all() and torch.isfinite(g_opt).all())}
 
 
 BATCH_FRAMES = [(1920, 1080)] * 8 + [(3840, 2160)] * 4 + [(4096, 3072)] * 2

@@ -140,6 +140,11 @@ _EXPORTS = {
     "fjb_spatial_dir_blur": (abi.FjStatus, [C.POINTER(abi.FjSpatialDir)] + [C.c_void_p] * 6 +
                              [C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, C.c_void_p,
                               C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_spatial_dir_filter_create": (abi.FjStatus, [C.POINTER(abi.FjSpatialDir), C.c_int32, C.c_int32, C.c_void_p,
+                                                     C.POINTER(C.c_void_p), C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_spatial_dir_filter_apply": (abi.FjStatus, [C.c_void_p] * 7 + [C.c_void_p, C.c_size_t, C.c_void_p,
+                                                                       C.POINTER(abi.FjErrorBuffer)]),
+    "fjb_spatial_dir_filter_destroy": (None, [C.c_void_p]),
     "fjb_recipe_set_spatial_dir_planes": (abi.FjStatus, [C.c_void_p] + [C.c_void_p] * 6 +
                                           [C.POINTER(abi.FjErrorBuffer)]),
     "fjb_dir_boundary_host": (abi.FjStatus, [C.POINTER(abi.FjDirGaussian), C.c_int32, C.POINTER(C.c_double),

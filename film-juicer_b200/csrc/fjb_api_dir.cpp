@@ -192,6 +192,66 @@ FjStatus fjb_spatial_dir_blur(const FjSpatialDir* spatial_dir, const float* in_y
     }
 }
 
+struct FjbDirFilter {
+    fjb::DirPlan plan;
+};
+
+FjStatus fjb_spatial_dir_filter_create(const FjSpatialDir* spatial_dir, int32_t width, int32_t height, void* stream,
+                                       FjbDirFilter** out, FjErrorBuffer* error) {
+    try {
+        if (!spatial_dir || !out) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+        *out = nullptr;
+        if (width <= 0 || height <= 0) return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "empty frame");
+        FjbDirFilter* f = new FjbDirFilter();
+        std::string why;
+        cudaError_t e = cudaSuccess;
+        if (!fjb::dir_plan_create(*spatial_dir, width, height, reinterpret_cast<cudaStream_t>(stream), f->plan, why,
+                                  e)) {
+            f->plan.release();
+            delete f;
+            if (e != cudaSuccess) return cuda_status(e, error, "spatial DIR plan");
+            return fail_status(FJ_STATUS_PREPARATION_FAILURE, error, why);
+        }
+        *out = f;
+        write_error(error, "");
+        return ok_status();
+    } catch (...) {
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "unexpected exception in fjb_spatial_dir_filter_create");
+    }
+}
+
+FjStatus fjb_spatial_dir_filter_apply(const FjbDirFilter* filter, const float* in_y, const float* in_m,
+                                      const float* in_c, float* out_y, float* out_m, float* out_c, float* scratch,
+                                      size_t scratch_bytes, void* stream, FjErrorBuffer* error) {
+    if (!filter || !in_y || !in_m || !in_c || !out_y || !out_m || !out_c)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "null argument");
+    const int width = filter->plan.width, height = filter->plan.height;
+    if (!scratch || scratch_bytes < fjb_spatial_dir_scratch_bytes(width, height))
+        return fail_status(FJ_STATUS_ALLOCATION_FAILURE, error, "spatial DIR scratch is too small");
+    if (reinterpret_cast<uintptr_t>(scratch) % 16 != 0)
+        return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "spatial DIR scratch must be 16-byte aligned");
+    const size_t plane = (size_t)width * (size_t)height;
+    const float* ins[3] = {in_y, in_m, in_c};
+    float* outs[3] = {out_y, out_m, out_c};
+    const float* region = scratch + 3 * plane;
+    for (int c = 0; c < 3; ++c)
+        if (ins[c] == outs[c] || (ins[c] >= scratch && ins[c] < region) || (outs[c] >= scratch && outs[c] < region))
+            return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "spatial DIR filter planes overlap");
+    const cudaError_t e =
+        fjb::dir_blur_planes(filter->plan, ins, outs, width, height, scratch, reinterpret_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_status(e, error, "spatial DIR filter");
+    write_error(error, "");
+    return ok_status();
+}
+
+void fjb_spatial_dir_filter_destroy(FjbDirFilter* filter) {
+    if (!filter) return;
+    // the filter's device tables may still be read by enqueued work
+    cudaDeviceSynchronize();
+    filter->plan.release();
+    delete filter;
+}
+
 FjStatus fjb_recipe_set_spatial_dir_planes(FjbRecipe* recipe, const float* filtered_y, const float* filtered_m,
                                            const float* filtered_c, const float* log_raw_b, const float* log_raw_g,
                                            const float* log_raw_r, FjErrorBuffer* error) {

@@ -225,7 +225,7 @@ class FrameFit:
                 (host.film_exposure.flags & abi.FJ_FILM_AUTO_EXPOSURE):
             raise ValueError("frame fitting covers camera diffusion, scatter/halation and spatial DIR only")
         self.spatial = _copy(host.spatial_dir) if host.spatial_dir.component_count else None
-        self._dir_scratch = None
+        self._dir_filter = None
         self.recipe, self.stream = recipe, stream
         self.diffusion_on = bool(o.flags & abi.FJ_OPTICS_CAMERA_DIFFUSION)
         self.halation_on = bool(o.flags & abi.FJ_OPTICS_SCATTER_HALATION)
@@ -317,14 +317,22 @@ class FrameFit:
         return out
 
     def dir_filter(self, planes_ymc):
-        """The frame's spatial DIR filter of three (H, W) planes (Y, M, C)."""
-        from .runtime import spatial_dir_blur
+        """The frame's spatial DIR filter of three (H, W) planes (Y, M, C), prepared once
+        per frame (runtime.DirFilter)."""
+        from .runtime import DirFilter
 
         torch = _torch()
+        if self._dir_filter is None:
+            h, w = self.shape
+            self._dir_filter = DirFilter(self.spatial, w, h, stream=self.stream)
         out = [torch.empty_like(p) for p in planes_ymc]
-        self._dir_scratch = spatial_dir_blur(self.spatial, [p.contiguous() for p in planes_ymc], out,
-                                             stream=self.stream, scratch=self._dir_scratch)
-        return out
+        return self._dir_filter.apply([p.contiguous() for p in planes_ymc], out, stream=self.stream)
+
+    def close(self):
+        """Frees the prepared DIR filter (also done when the object is collected)."""
+        if self._dir_filter is not None:
+            self._dir_filter.close()
+            self._dir_filter = None
 
     def filtered_corrections(self, theta, carrier_rgb):
         """Spatial DIR: the filtered donor corrections (Y, M, C) for theta."""

@@ -283,6 +283,48 @@ def spatial_dir_blur(spatial_dir: "abi.FjSpatialDir", planes_ymc, out_ymc, strea
     return scratch
 
 
+class DirFilter:
+    """A spatial DIR filter prepared once for a frame size (fjb_spatial_dir_filter_*);
+    `apply` enqueues it on three dense (H, W) planes (Y, M, C)."""
+
+    def __init__(self, spatial_dir: "abi.FjSpatialDir", width: int, height: int, stream=None):
+        self.lib = load_library()
+        self.width, self.height = width, height
+        self.handle = C.c_void_p()
+        self.scratch = None
+        err = abi.ErrorText()
+        _check("fjb_spatial_dir_filter_create",
+               self.lib.fjb_spatial_dir_filter_create(C.byref(spatial_dir), width, height,
+                                                      C.c_void_p(_stream_handle(stream)), C.byref(self.handle),
+                                                      C.byref(err.buf)), err)
+
+    def apply(self, planes_ymc, out_ymc, stream=None):
+        torch = _torch()
+        for t in (*planes_ymc, *out_ymc):
+            if not t.is_contiguous() or tuple(t.shape) != (self.height, self.width):
+                raise ValueError("spatial DIR filter planes must be dense (H, W) tensors of the filter's size")
+        need = int(self.lib.fjb_spatial_dir_scratch_bytes(self.width, self.height))
+        if self.scratch is None or self.scratch.numel() * 4 < need:
+            self.scratch = torch.empty(need // 4 + 1, dtype=torch.float32, device=planes_ymc[0].device)
+        err = abi.ErrorText()
+        _check("fjb_spatial_dir_filter_apply",
+               self.lib.fjb_spatial_dir_filter_apply(self.handle, *[C.c_void_p(_ptr(t)) for t in (*planes_ymc, *out_ymc)],
+                                                     C.c_void_p(_ptr(self.scratch)), self.scratch.numel() * 4,
+                                                     C.c_void_p(_stream_handle(stream)), C.byref(err.buf)), err)
+        return out_ymc
+
+    def close(self):
+        if self.handle:
+            self.lib.fjb_spatial_dir_filter_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def scatter_halation(descriptor: "abi.FjScatterHalation", planes_rgb, stream=None, scratch=None):
     """In-place scatter/halation on three CUDA planes (R, G, B), each (H, W) float32."""
     torch = _torch()

@@ -361,6 +361,18 @@ FjStatus fjb_spatial_dir_blur(const FjSpatialDir* spatial_dir, const float* in_y
                               int32_t height, float* scratch, size_t scratch_bytes, void* stream,
                               FjErrorBuffer* error);
 
+/* The same filter prepared once for a frame size (its components' device tables), for
+ * repeated use: fjb_spatial_dir_filter_apply only enqueues (dense width x height
+ * planes, in -> out distinct, scratch as for fjb_spatial_dir_build);
+ * fjb_spatial_dir_filter_destroy synchronises the device before it frees the tables. */
+typedef struct FjbDirFilter FjbDirFilter;
+FjStatus fjb_spatial_dir_filter_create(const FjSpatialDir* spatial_dir, int32_t width, int32_t height, void* stream,
+                                       FjbDirFilter** out, FjErrorBuffer* error);
+FjStatus fjb_spatial_dir_filter_apply(const FjbDirFilter* filter, const float* in_y, const float* in_m,
+                                      const float* in_c, float* out_y, float* out_m, float* out_c, float* scratch,
+                                      size_t scratch_bytes, void* stream, FjErrorBuffer* error);
+void fjb_spatial_dir_filter_destroy(FjbDirFilter* filter);
+
 /* Makes later capture-development calls on `recipe` use spatially filtered DIR
  * corrections and cached log exposure (all six device planes, or all NULL to return
  * to runtime DIR). */

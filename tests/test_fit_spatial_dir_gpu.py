@@ -1,10 +1,11 @@
 """Fitting through spatial DIR (the development subtracts spatially filtered donor
-corrections; fitting.FrameFit over fjb_fit_dir_source_carrier, fjb_spatial_dir_blur,
-fjb_fit_forward_spatial_carrier / fjb_fit_vjp_spatial_carrier and
-fjb_fit_dir_source_vjp_carrier):
+corrections; fitting.FrameFit over fjb_fit_dir_source_carrier, the prepared DIR filter
+(fjb_spatial_dir_filter_*), fjb_fit_forward_spatial_carrier / fjb_fit_vjp_spatial_carrier
+and fjb_fit_dir_source_vjp_carrier):
 
 * the DIR filter is symmetric, <G a, b> = <a, G b> within FP32 rounding, which makes
-  it its own adjoint (half-sample reflected boundaries and symmetric components);
+  it its own adjoint (half-sample reflected boundaries and symmetric components), and
+  the prepared filter equals the one-shot fjb_spatial_dir_blur bit for bit;
 * at the recipe's parameters the fitting source stage's filtered corrections equal the
   library's spatial-DIR stage (fjb_spatial_dir_build) on the same carrier;
 * the 13 per-pixel parameters' gradient and the carrier-gradient planes equal autograd
@@ -61,6 +62,13 @@ def test_dir_filter_is_symmetric(torch_cuda, recipes, prepare):
     a = [torch.randn((H, W), device="cuda", generator=gen) for _ in range(3)]
     b = [torch.randn((H, W), device="cuda", generator=gen) for _ in range(3)]
     ga, gb = ff.dir_filter(a), ff.dir_filter(b)
+    # the prepared filter (fjb_spatial_dir_filter_apply) equals the one-shot entry
+    from film_juicer_b200 import runtime
+
+    once = [torch.empty_like(p) for p in a]
+    runtime.spatial_dir_blur(rec.host.h.spatial_dir, a, once)
+    for x, y in zip(ga, once):
+        assert torch.equal(x, y)
     for c in range(3):
         lhs = float((ga[c].double() * b[c].double()).sum())
         rhs = float((a[c].double() * gb[c].double()).sum())
@@ -68,6 +76,7 @@ def test_dir_filter_is_symmetric(torch_cuda, recipes, prepare):
         assert abs(lhs - rhs) <= 1e-5 * scale, (c, lhs, rhs)
         # the filter does something: it is not the identity
         assert float((ga[c] - a[c]).abs().max()) > 1e-3
+    ff.close()
     dr.close()
 
 
