@@ -163,7 +163,8 @@ __device__ bool scan_lut_sample_d(const PixelParams& p, const double n[3], float
     return true;
 }
 
-// The print's spectral integral raw_c = sum_l T(l) sens_c(l), T(l) = 2^(D . nd(l) + nd3(l)),
+// The print's spectral integral raw_c = sum_l T(l) sens_c(l), T(l) = 2^(D . nd(l)) (the
+// film base folded into sens, fjb_params.h),
 // evaluated as print_spectral evaluates it (same operations and partial sums), with the
 // moments q[3c + j] = sum_l T(l) sens_c(l) nd_j(l) of the same pass: d raw_c / d D_j =
 // q[3c + j] ln 2. One exp2 per wavelength serves the value and its derivative.
@@ -174,7 +175,7 @@ __device__ __forceinline__ void print_spectral_moments(const PrintSpectral& s, c
     for (int k = 0; k < 9; ++k) q[k] = 0.0f;
 #pragma unroll
     for (int i = 0; i < kSpectralSamples; ++i) {
-        const float dl = fmaf(d[0], s.nd[i][0], fmaf(d[1], s.nd[i][1], fmaf(d[2], s.nd[i][2], s.nd[i][3])));
+        const float dl = fmaf(d[0], s.nd[i][0], fmaf(d[1], s.nd[i][1], d[2] * s.nd[i][2]));
         const float t = mufu_exp2(dl);
         float* a = (i & 1) ? a1 : a0;
 #pragma unroll

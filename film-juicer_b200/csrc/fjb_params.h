@@ -40,12 +40,14 @@ struct CurveRef {
 };
 
 // Print 81-lambda coefficients, pre-folded on the host:
-//   nd[l]   = -(eps_c, eps_m, eps_y, base) * log2(10)   (so T = 2^(D . nd))
-//   sens[l] = (sens_c, sens_m, sens_y) * filtered illuminant
-// Wavelengths whose three sensitivities are all NaN are dropped and the remaining
-// ones packed first; the unused tail slots hold (0, 0, 0, -inf) and zero
-// sensitivities, so they contribute exactly +0 for finite densities. A NaN channel of
-// a kept wavelength contributes zero.
+//   nd[l]   = (-(eps_c, eps_m, eps_y) * log2(10), 0)     (so T = 2^(D . nd))
+//   sens[l] = (sens_c, sens_m, sens_y) * filtered illuminant * 10^-base
+// (the film base's transmittance is the same at every pixel, so it sits in the
+// weights and the per-pixel exponent has the three dye terms only; nd[l][3] stays 0).
+// Wavelengths whose three sensitivities are all NaN, or whose dye or base density or
+// illuminant is NaN, are dropped and the remaining ones packed first; the unused tail
+// slots hold (0, 0, 0, -inf) and zero sensitivities, so they contribute exactly +0 for
+// finite densities. A NaN channel of a kept wavelength contributes zero.
 struct PrintSpectral {
     float nd[kSpectralSamples][4];
     float sens[kSpectralSamples][3];

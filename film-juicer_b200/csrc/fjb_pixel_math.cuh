@@ -517,14 +517,15 @@ static __device__ __noinline__ void print_spectral_nonfinite(const PrintSpectral
 
 __device__ __forceinline__ void print_spectral(const PrintSpectral& s, const float d[3], float raw[3]) {
     if (isfinite(d[0]) && isfinite(d[1]) && isfinite(d[2])) {
-        // Fast path: all 81 slots unrolled, coefficients are constant-bank operands.
+        // Fast path: all 81 slots unrolled, coefficients are constant-bank operands
+        // (one per instruction: the film base sits in the weights, fjb_params.h).
         // Finite densities give finite exponents, so no NaN guard is needed; padded
-        // slots evaluate 2^-inf * 0 = +0. Two partial sums per channel (even / odd
+        // slots evaluate 2^0 * 0 = +0. Two partial sums per channel (even / odd
         // wavelength) halve the dependent FMA chain.
         float a0[3] = {0.0f, 0.0f, 0.0f}, a1[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
         for (int i = 0; i < kSpectralSamples; ++i) {
-            const float dl = fmaf(d[0], s.nd[i][0], fmaf(d[1], s.nd[i][1], fmaf(d[2], s.nd[i][2], s.nd[i][3])));
+            const float dl = fmaf(d[0], s.nd[i][0], fmaf(d[1], s.nd[i][1], d[2] * s.nd[i][2]));
             const float t = mufu_exp2(dl);
             float* a = (i & 1) ? a1 : a0;
             a[0] = fmaf(t, s.sens[i][0], a[0]);

@@ -3,9 +3,9 @@
 //
 // Reference: print_spectral_integrate_device (src/Cuda/JuicerCudaDeviceHelpers.cuh:866-935)
 //   D(l) = sum_c d_c eps_c(l) + base(l),  T(l) = 10^-D(l) I_filt(l),  raw_c = sum_l T(l) S_c(l).
-// The recipe folds it into nd(l) = -(eps_c, eps_m, eps_y, base)(l) log2(10) and
-// sens(l) = S(l) I_filt(l) (fjb_params.h), so T(l) = 2^(d . nd(l) + nd3(l)) and
-// raw_c = sum_l T(l) sens_c(l).
+// The recipe folds it into nd(l) = -(eps_c, eps_m, eps_y)(l) log2(10), nd3(l) = 0 and
+// sens(l) = S(l) I_filt(l) 10^-base(l) (fjb_params.h), so T(l) = 2^(d . nd(l) + nd3(l))
+// and raw_c = sum_l T(l) sens_c(l); nd3 is -inf on the padded wavelengths.
 //
 // One persistent CTA of 128 threads takes tiles of 128 consecutive pixels (one per
 // thread, one TMEM lane per pixel):

@@ -348,9 +348,14 @@ bool create_recipe(const FjPreparedHostData& h, cudaStream_t stream, Recipe& r, 
                     std::isnan(pr.film_base_density.data[l]) || std::isnan(il))
                     continue;
                 for (int c = 0; c < 3; ++c) p.spectral.nd[count][c] = -(pr.film_density_cmy.data[l * 3 + c] * kLog2Of10);
-                p.spectral.nd[count][3] = -(pr.film_base_density.data[l] * kLog2Of10);
+                // the film base transmits the same 2^nd3 at every pixel: it is folded into
+                // the wavelength's weights, so the per-pixel exponent is d . nd alone
+                const float nd3 = -(pr.film_base_density.data[l] * kLog2Of10);
+                const double base_t = std::exp2((double)nd3);
+                p.spectral.nd[count][3] = 0.0f;
                 for (int c = 0; c < 3; ++c)
-                    p.spectral.sens[count][c] = (std::isnan(s[c]) || std::isnan(il)) ? 0.0f : s[c] * il;
+                    p.spectral.sens[count][c] =
+                        (std::isnan(s[c]) || std::isnan(il)) ? 0.0f : (float)((double)s[c] * (double)il * base_t);
                 ++count;
             }
             p.spectral.count = count;
