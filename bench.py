@@ -603,8 +603,8 @@ def frame_fit_block(torch, prepare, runtime, recipe, stream, th0, thp, timed):
 
 
 BATCH_FRAMES = [(1920, 1080)] * 8 + [(3840, 2160)] * 4 + [(4096, 3072)] * 2
-BATCH_RECIPES = [("recipe_print.npz", 0xB001), ("recipe_gold200_endura.npz", 0xB002),
-                 ("recipe_c200_crystal.npz", 0xB003)]
+BATCH_RECIPES = [("recipe_print.npz", 0xB001), ("recipe_vision3_500t_2383.npz", 0xB002),
+                 ("recipe_ektar100_endura.npz", 0xB003)]
 
 
 def batch_block(torch, frame_records, prepare, owner, args, barrier, max_over_ranks):
@@ -654,8 +654,8 @@ def batch_block(torch, frame_records, prepare, owner, args, barrier, max_over_ra
         forms[f"{w}x{h} r={r}"] = {0: "direct", 1: "fft"}.get(f, "undecided")
     owner.set_autotune(False)
     return {"workload": "8 x 1920x1080 + 4 x 3840x2160 + 2 x 4096x3072 full optical print frames, stocks "
-                        "kodak_portra_400 / kodak_gold_200 / fujifilm_c200 on papers kodak_portra_endura / "
-                        "fujifilm_crystal_archive_typeii, every spatial stage, one fjb_render_batch per step",
+                        "kodak_portra_400 / kodak_vision3_500t / kodak_ektar_100 on papers kodak_portra_endura / "
+                        "kodak_2383, every spatial stage, one fjb_render_batch per step",
             "frames": len(BATCH_FRAMES), "mpix_per_batch": round(px / 1e6, 2),
             "value": round(px / (graph_ms * 1e-3) / 1e6, 2), "unit": "Mpix/s", "ms_per_batch": round(graph_ms, 3),
             "graph_captured": captured,

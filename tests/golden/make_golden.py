@@ -44,8 +44,10 @@ container, where the reference is mounted read-only).
   exact words and hashes of each recipe, and per stock the profile's info block,
   Gaussian density model and log-exposure axis.
 * recipe_direct.npz / recipe_print.npz: prepared recipes (film_juicer_b200.prepare)
-  for kodak_portra_400 direct and kodak_portra_400 -> kodak_portra_endura print,
-  built from the reference's Resources/ profiles and spectral tables.
+  for kodak_portra_400 direct and kodak_portra_400 -> kodak_portra_endura print, and
+  recipe_vision3_500t_2383.npz / recipe_ektar100_endura.npz for the mixed-stock
+  batches (kodak_vision3_500t -> kodak_2383, kodak_ektar_100 -> kodak_portra_endura),
+  built from the reference's Resources/ profiles, spectral tables and filters.
 """
 from __future__ import annotations
 
@@ -465,10 +467,10 @@ def recipes():
     prepare.prepare_recipe(res, "kodak_portra_400").save(os.path.join(HERE, "recipe_direct.npz"))
     prepare.prepare_recipe(res, "kodak_portra_400", "kodak_portra_endura").save(os.path.join(HERE, "recipe_print.npz"))
     # the mixed-stock batch: three capture stocks on two print papers
-    prepare.prepare_recipe(res, "kodak_gold_200", "kodak_portra_endura").save(
-        os.path.join(HERE, "recipe_gold200_endura.npz"))
-    prepare.prepare_recipe(res, "fujifilm_c200", "fujifilm_crystal_archive_typeii").save(
-        os.path.join(HERE, "recipe_c200_crystal.npz"))
+    prepare.prepare_recipe(res, "kodak_vision3_500t", "kodak_2383").save(
+        os.path.join(HERE, "recipe_vision3_500t_2383.npz"))
+    prepare.prepare_recipe(res, "kodak_ektar_100", "kodak_portra_endura").save(
+        os.path.join(HERE, "recipe_ektar100_endura.npz"))
     print("recipes written")
 
 

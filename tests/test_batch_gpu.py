@@ -16,7 +16,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 SIZES = [(320, 180), (256, 256), (384, 216), (200, 150)]
-RECIPES = [("print", 0x1001), ("gold200_endura", 0x1002), ("c200_crystal", 0x1003)]
+RECIPES = [("print", 0x1001), ("vision3_500t_2383", 0x1002), ("ektar100_endura", 0x1003)]
 
 
 @pytest.fixture(scope="module")
