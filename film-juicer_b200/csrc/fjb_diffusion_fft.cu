@@ -546,7 +546,7 @@ bool diffusion_fft_plan(int width, int height, int radius, DiffusionFftPlan& p) 
     if (p.rows_per_cta > 4) p.rows_per_cta = 4;
     // a radix-3 stage holds 5 butterflies (15 values) per thread
     p.cols_per_cta = (kFftThreads * (ny3 ? kFftMaxValues - kFftMaxValues % 3 : kFftMaxValues)) / ny;
-    if (p.cols_per_cta > 2) p.cols_per_cta = 2;
+    if (p.cols_per_cta > 4) p.cols_per_cta = 4;
     if (p.rows_per_cta < 1 || p.cols_per_cta < 1) return false;
     // the inverse split holds 2 values per (k, m - k) pair: (m/2 + 1) pairs per row
     if ((long long)p.rows_per_cta * (p.m / 2) > (long long)kFftThreads * kC2rPairs) return false;
