@@ -294,12 +294,13 @@ def prepare_recipe(resources: str, film: str, paper: str | None = None, *, dir_a
     if rec.mode:
         a["dir_axes_rgb"] = f32(rec.axes_rgb)
 
-    route = abi.FJ_ROUTE_NEGATIVE_DIRECT
+    positive = prof["info"].get("type") == "positive"
+    route = abi.FJ_ROUTE_POSITIVE_DIRECT if positive else abi.FJ_ROUTE_NEGATIVE_DIRECT
     medium_dyes = prof["channel_density"]
     medium_base = prof["base_density"]
     medium_curves = curves
     if paper is not None:
-        route = abi.FJ_ROUTE_NEGATIVE_PRINT
+        route = abi.FJ_ROUTE_POSITIVE_PRINT if positive else abi.FJ_ROUTE_NEGATIVE_PRINT
         pp = load_profile(os.path.join(resources, "profiles", f"{paper}.json"))
         # The enlarger: the TH-KG3 lamp through the dichroics at the calibrated neutral
         # filtration of this paper / lamp / film (recipe.rs:1709-1741, print.rs:120-158),

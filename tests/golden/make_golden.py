@@ -47,6 +47,7 @@ container, where the reference is mounted read-only).
   for kodak_portra_400 direct and kodak_portra_400 -> kodak_portra_endura print, and
   recipe_vision3_500t_2383.npz / recipe_ektar100_endura.npz for the mixed-stock
   batches (kodak_vision3_500t -> kodak_2383, kodak_ektar_100 -> kodak_portra_endura),
+  and recipe_positive.npz (fujifilm_provia_100f scanned directly, the positive route),
   built from the reference's Resources/ profiles, spectral tables and filters.
 """
 from __future__ import annotations
@@ -467,6 +468,8 @@ def recipes():
     prepare.prepare_recipe(res, "kodak_portra_400").save(os.path.join(HERE, "recipe_direct.npz"))
     prepare.prepare_recipe(res, "kodak_portra_400", "kodak_portra_endura").save(os.path.join(HERE, "recipe_print.npz"))
     # the mixed-stock batch: three capture stocks on two print papers
+    # a reversal stock scanned directly (positive route, receiver-Langmuir DIR)
+    prepare.prepare_recipe(res, "fujifilm_provia_100f").save(os.path.join(HERE, "recipe_positive.npz"))
     prepare.prepare_recipe(res, "kodak_vision3_500t", "kodak_2383").save(
         os.path.join(HERE, "recipe_vision3_500t_2383.npz"))
     prepare.prepare_recipe(res, "kodak_ektar_100", "kodak_portra_endura").save(
