@@ -221,7 +221,10 @@ __device__ bool fit_pixel(const PixelParams& p, const float* __restrict__ blob, 
     float D[3], logC[3] = {0.0f, 0.0f, 0.0f}, sd[3] = {0.0f, 0.0f, 0.0f}, dv[3] = {0.0f, 0.0f, 0.0f},
                 dk[3] = {0.0f, 0.0f, 0.0f}, dfr[3] = {0.0f, 0.0f, 0.0f};
     int dkn[3] = {-1, -1, -1};
-    const bool dir = p.dir_mode == kDirNegativeDonor;
+    const bool dir = p.dir_mode == kDirNegativeDonor || p.dir_mode == kDirPositiveReceiver;
+    const bool positive = p.dir_mode == kDirPositiveReceiver;
+    // positive stocks: d (finalised correction) / d (coupler sum) per receiver
+    float dfin[3] = {1.0f, 1.0f, 1.0f};
     if (dir) {
         float corr[3];
         if constexpr (kSpatial) {
@@ -232,15 +235,38 @@ __device__ bool fit_pixel(const PixelParams& p, const float* __restrict__ blob, 
         } else {
             float donor[3];
             for (int c = 0; c < 3; ++c) {
-                const float v = layer[c], k = th.k[c], r = p.dir_dref[c];
-                const float den = k + v;
-                donor[c] = v * (k + r) / den;
-                dv[c] = k * (k + r) / (den * den);
-                dk[c] = v * (v - r) / (den * den);
+                const float v = layer[c];
+                if (positive) {
+                    // the donor is the density still to form (src/Cuda/JuicerCudaDeviceHelpers.cuh:1173)
+                    donor[c] = p.dir_dmax[c] - v;
+                    dv[c] = -1.0f;
+                    dk[c] = 0.0f;
+                } else {
+                    const float k = th.k[c], r = p.dir_dref[c];
+                    const float den = k + v;
+                    donor[c] = v * (k + r) / den;
+                    dv[c] = k * (k + r) / (den * den);
+                    dk[c] = v * (v - r) / (den * den);
+                }
                 if (!isfinite(donor[c])) return false;
             }
             const float* M = p.dir_m;
             for (int j = 0; j < 3; ++j) corr[j] = M[j] * donor[0] + M[3 + j] * donor[1] + M[6 + j] * donor[2];
+        }
+        if (positive) {
+            // receiver Langmuir: c (kr + cref) / (kr + c), zero where the receiver has no reference
+            for (int j = 0; j < 3; ++j) {
+                const float cref = p.dir_receiver_cref[j], kr = p.dir_receiver_kr[j];
+                if (cref == 0.0f) {
+                    corr[j] = 0.0f;
+                    dfin[j] = 0.0f;
+                    continue;
+                }
+                const float c = corr[j], den = kr + c;
+                corr[j] = c * (kr + cref) / den;
+                dfin[j] = kr * (kr + cref) / (den * den);
+                if (!isfinite(corr[j]) || !isfinite(dfin[j])) return false;
+            }
         }
         for (int j = 0; j < 3; ++j) {
             logC[j] = logS[j] - corr[j];
@@ -345,7 +371,7 @@ __device__ bool fit_pixel(const PixelParams& p, const float* __restrict__ blob, 
             const float g_logC = g * sd[j] * th.gamma[j];
             g_th[3 + j] += (g * sd[j] * logC[j]);
             g_logS[j] = g_logC;
-            g_corr[j] = -g_logC;
+            g_corr[j] = -g_logC * dfin[j];
         }
         const float* M = p.dir_m;
         if constexpr (kSpatial) {
@@ -362,9 +388,10 @@ __device__ bool fit_pixel(const PixelParams& p, const float* __restrict__ blob, 
         }
         // The compensated axes depend on the knees (axis_j[i] = logE[i] - sum_d M[d][j]
         // L(y_d[i], k_d)): d D / d axis at the interval's knots is -slope (1 - t), -slope t.
+        // (Positive stocks have no donor knees: their axes are the recipe's.)
         const int n = p.dir_curve[0].n;
         for (int j = 0; j < 3; ++j) {
-            if (dkn[j] < 0) continue;
+            if (positive || dkn[j] < 0) continue;
             const float w = g_D[2 - j] * sd[j];
             const int i0 = dkn[j];
             const float t = dfr[j];
@@ -581,7 +608,8 @@ __global__ void fit_reduce_kernel(const double* __restrict__ partials, int block
 
 // Spatial-DIR source of one pixel for theta (src/Cuda/Film/JuicerCudaFilmPipeline.cu:124-214):
 // the film exposure, the pre-DIR layer densities and the donor corrections they
-// release to the B, G, R receivers, corr_j = sum_d M[d][j] L(layer_d, k_d). With kGrad,
+// release to the B, G, R receivers, corr_j = sum_d M[d][j] donor_d (donor_d = L(layer_d, k_d),
+// or dmax_d - layer_d for positive stocks; the receiver Langmuir follows the filter). With kGrad,
 // adds g_src^T d corr / d theta into g_th and writes d <g_src, corr> / d e0 into g_e0
 // (may be null). False (nothing added) where a value is not finite.
 template <bool kGrad>
@@ -595,11 +623,18 @@ __device__ bool dir_source_pixel(const PixelParams& p, const float* __restrict__
         int kn;
         float fr;
         layer[c] = curve_with_slope(blob, p.film_curve[c], logS[c], th.gamma[c], sl[c], kn, fr);
-        const float v = layer[c], k = th.k[c], r = p.dir_dref[c];
-        const float den = k + v;
-        donor[c] = v * (k + r) / den;
-        dv[c] = k * (k + r) / (den * den);
-        dk[c] = v * (v - r) / (den * den);
+        const float v = layer[c];
+        if (p.dir_mode == kDirPositiveReceiver) {
+            donor[c] = p.dir_dmax[c] - v;
+            dv[c] = -1.0f;
+            dk[c] = 0.0f;
+        } else {
+            const float k = th.k[c], r = p.dir_dref[c];
+            const float den = k + v;
+            donor[c] = v * (k + r) / den;
+            dv[c] = k * (k + r) / (den * den);
+            dk[c] = v * (v - r) / (den * den);
+        }
         if (!isfinite(donor[c])) return false;
     }
     const float* M = p.dir_m;
@@ -819,8 +854,6 @@ static FjStatus fit_check(FjbRecipe* recipe, const FjbFitParams* params, bool ha
     if ((components != 3 && components != 4) || width < 0 || height < 0)
         return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "unsupported image geometry");
     const fjb::PixelParams& p = recipe->r.params;
-    if (p.dir_mode == fjb::kDirPositiveReceiver)
-        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "fitting covers inactive and negative-donor DIR");
     if (p.method == fjb::kMallett)
         return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "fitting covers the TC LUT reconstructions");
     if (!fjb::theta_from(*params, th))
@@ -935,8 +968,8 @@ static FjStatus spatial_check(FjbRecipe* recipe, const FjbFitParams* params, con
                               FjErrorBuffer* error) {
     FjStatus st = fit_check(recipe, params, cb && cg && cr, 3, width, height, th, error);
     if (st.category != FJ_STATUS_SUCCESS) return st;
-    if (recipe->r.params.dir_mode != fjb::kDirNegativeDonor)
-        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "spatial DIR fitting needs negative-donor DIR");
+    if (recipe->r.params.dir_mode == fjb::kDirInactive)
+        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "spatial DIR fitting needs active DIR couplers");
     if (stride < width) return fail_status(FJ_STATUS_INTERNAL_FAILURE, error, "carrier stride below the width");
     return ok_status();
 }

@@ -2,7 +2,8 @@
 library's fitting entry points (fjb_fit_forward, fjb_fit_vjp) and an Adam loop on it.
 
 The differentiable function is the per-pixel chain of a recipe (camera exposure, film
-curves, negative-donor DIR with its compensated axes, print exposure and curves on the
+curves, DIR couplers (negative-donor with its compensated axes, or the positive stocks'
+receiver Langmuir), print exposure and curves on the
 print route, scanner LUT, correction and colour matrices) from a source image to the
 scanner's linear output RGB, as a function of 13 parameters (FjbFitParams order):
 

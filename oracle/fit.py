@@ -9,9 +9,11 @@ The chain is the capture-to-scan chain of the render (src/Cuda/JuicerCudaDeviceH
 autograd, on the tables the oracle packs from the same FjPreparedHostData
 (oracle.c oracle_fit_tables, oracle_scanner_lut): the camera exposure of each pixel (the
 oracle's FP32 film exposure with the route correction) times 2^ev, log10, the film
-curves at logE * gamma, the negative-donor DIR (Langmuir donors, the coupler matrix and
-the compensated curves, whose axes are rebuilt from the donor knees as the reference's
-host builds them: rust/film-juicer-core/src/film/dir.rs:258-290), on the print route
+curves at logE * gamma, the DIR couplers (negative stocks: Langmuir donors, the coupler
+matrix and the compensated curves, whose axes are rebuilt from the donor knees as the
+reference's host builds them: rust/film-juicer-core/src/film/dir.rs:258-290; positive
+stocks: donors dmax - density, the coupler matrix and the receivers' Langmuir, on the
+recipe's axes), on the print route
 the spectral print exposure 10^-(D . eps + base) x illuminant x sensitivity with the
 mid-grey normaliser, preflash, print exposure x 2^print_ev and route correction, log10
 and the print curves at logP * print_gamma, then the scanner's PCHIP LUT (the reference's
@@ -50,6 +52,7 @@ class OracleFitTables(C.Structure):
         ("print_density_cmy", (C.c_float * MAX_SAMPLES) * 3),
         ("min_cmy", C.c_float * 3), ("inv_cmy", C.c_float * 3), ("corr_slope", C.c_float), ("corr_offset", C.c_float),
         ("cat02", C.c_float * 9), ("xyz_to_rgb", C.c_float * 9),
+        ("dir_dmax", C.c_float * 3), ("dir_rcref", C.c_float * 3), ("dir_rkr", C.c_float * 3),
     ]
 
 
@@ -74,6 +77,7 @@ def tables(record) -> dict:
         "gamma_bgr": f(t.gamma_bgr), "dir_m": f(t.dir_m), "dir_dref": f(t.dir_dref), "dir_k": f(t.dir_k),
         "min_cmy": f(t.min_cmy), "inv_cmy": f(t.inv_cmy), "corr_slope": float(t.corr_slope),
         "corr_offset": float(t.corr_offset), "cat02": f(t.cat02), "xyz_to_rgb": f(t.xyz_to_rgb),
+        "dir_dmax": f(t.dir_dmax), "dir_rcref": f(t.dir_rcref), "dir_rkr": f(t.dir_rkr),
     }
     if t.print:
         eps, base, ill = f(t.eps_cmy).reshape(NL, 3), f(t.base), f(t.illuminant)
@@ -220,8 +224,15 @@ class Chain:
         """DIR compensated axes (3, n) for donor knees k (B, G, R): log exposure minus
         the coupler-matrix sum of the Langmuir donors of the curve densities."""
         torch, t = self.torch, self.t
-        donors = _langmuir(torch, t["density_bgr"], k[:, None], t["dir_dref"][:, None])  # (3 donor, n)
         m = t["dir_m"].reshape(3, 3)  # [donor][receiver]
+        if t["dir_mode"] == 2:
+            # positive stocks: donors dmax - density, the receivers' Langmuir on the sums
+            # (film/dir.rs:271-299); the knees do not enter
+            c = m.T @ (t["dir_dmax"][:, None] - t["density_bgr"])
+            cref, kr = t["dir_rcref"][:, None], t["dir_rkr"][:, None]
+            fin = torch.where(cref == 0.0, torch.zeros_like(c), c * (kr + cref) / (kr + c))
+            return t["log_exposure"][None, :] - fin
+        donors = _langmuir(torch, t["density_bgr"], k[:, None], t["dir_dref"][:, None])  # (3 donor, n)
         return t["log_exposure"][None, :] - (m.T @ donors)
 
     def __call__(self, e0, theta, spatial=None):
@@ -246,10 +257,25 @@ class Chain:
             logc = logs - corr
             ax = self.axes(k)
             dens_bgr = [_curve(torch, ax[j], t["density_bgr"][j], logc[j] * gam[j]) for j in range(3)]
+        elif t["dir_mode"] == 2:
+            # positive stocks: donors are the density still to form; the receivers'
+            # Langmuir finalises the (filtered) coupler sums
+            # (src/Cuda/JuicerCudaDeviceHelpers.cuh:1173-1200)
+            donor = t["dir_dmax"][:, None] - layer
+            m = t["dir_m"].reshape(3, 3)
+            corr = m.T @ donor
+            if spatial is not None:
+                corr = spatial(corr)
+            cref, kr = t["dir_rcref"][:, None], t["dir_rkr"][:, None]
+            fin = corr * (kr + cref) / (kr + corr)
+            corr = torch.where(cref == 0.0, torch.zeros_like(fin), fin)
+            logc = logs - corr
+            ax = t["axes_bgr"]
+            dens_bgr = [_curve(torch, ax[j], t["density_bgr"][j], logc[j] * gam[j]) for j in range(3)]
         elif t["dir_mode"] == 0:
             dens_bgr = [layer[c] for c in range(3)]
         else:
-            raise ValueError("the fitting chain covers inactive and negative-donor DIR")
+            raise ValueError("unknown DIR mode")
         dens = torch.stack([dens_bgr[2], dens_bgr[1], dens_bgr[0]])  # C, M, Y
         if t["print"]:
             sens = t["sens_cmy"]

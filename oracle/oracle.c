@@ -3161,6 +3161,7 @@ typedef struct {
     float print_log_exposure[ORACLE_FIT_MAX_SAMPLES];
     float print_density_cmy[3][ORACLE_FIT_MAX_SAMPLES];
     float min_cmy[3], inv_cmy[3], corr_slope, corr_offset, cat02[9], xyz_to_rgb[9];
+    float dir_dmax[3], dir_rcref[3], dir_rkr[3]; /* positive stocks: donors and receivers */
 } OracleFitTables;
 
 int oracle_fit_tables(const FjPreparedHostData* h, OracleFitTables* t) {
@@ -3188,6 +3189,9 @@ int oracle_fit_tables(const FjPreparedHostData* h, OracleFitTables* t) {
             for (int i = 0; i < n; ++i) t->axes_bgr[c][i] = p->dirc[c].x[i];
         t->dir_dref[c] = p->dref[c];
         t->dir_k[c] = p->dk[c];
+        t->dir_dmax[c] = p->dmax[c];
+        t->dir_rcref[c] = p->rcref[c];
+        t->dir_rkr[c] = p->rkr[c];
         t->min_cmy[c] = p->min_cmy[c];
         t->inv_cmy[c] = p->inv_cmy[c];
     }

@@ -27,7 +27,7 @@ def prepare():
 @pytest.fixture(scope="session")
 def recipes(prepare):
     return {name: prepare.PreparedRecipe.load(os.path.join(GOLDEN, f"recipe_{name}.npz"))
-            for name in ("direct", "print")}
+            for name in ("direct", "print", "positive")}
 
 
 @pytest.fixture(scope="session")

@@ -35,7 +35,7 @@ def _grad_close(got, want, used, bound=BOUND):
         assert abs(g - w) <= bound * abs(w) + 1e-4 * scale, (got, want)
 
 
-@pytest.mark.parametrize("route", ["direct", "print"])
+@pytest.mark.parametrize("route", ["direct", "print", "positive"])
 def test_defaults_and_forward(torch_cuda, recipes, prepare, oracle, route):
     from film_juicer_b200 import fitting, runtime
     from oracle import fit
@@ -62,7 +62,7 @@ def test_defaults_and_forward(torch_cuda, recipes, prepare, oracle, route):
     dr.close()
 
 
-@pytest.mark.parametrize("route", ["direct", "print"])
+@pytest.mark.parametrize("route", ["direct", "print", "positive"])
 def test_adjoint_matches_fp64_autograd_on_crop_batch(torch_cuda, recipes, prepare, oracle, route):
     """16 seeded 512 x 512 crops; the cotangent is the gradient of the mean squared
     error against a target rendered at the recipe's own parameters."""
@@ -95,7 +95,7 @@ def test_adjoint_matches_fp64_autograd_on_crop_batch(torch_cuda, recipes, prepar
     dr.close()
 
 
-@pytest.mark.parametrize("route", ["direct", "print"])
+@pytest.mark.parametrize("route", ["direct", "print", "positive"])
 def test_adjoint_matches_central_differences(torch_cuda, recipes, prepare, oracle, route):
     from film_juicer_b200 import fitting, runtime
     from oracle import fit

@@ -26,7 +26,7 @@ def torch():
     return t
 
 
-@pytest.mark.parametrize("route", ["direct", "print"])
+@pytest.mark.parametrize("route", ["direct", "print", "positive"])
 def test_transcription_matches_oracle_linear_render(torch, recipes, prepare, oracle, route):
     from oracle import fit
 
@@ -53,7 +53,7 @@ def _fd_case(torch, fit, prepare, rec, seed):
     return ch, e0, theta0, w
 
 
-@pytest.mark.parametrize("route", ["direct", "print"])
+@pytest.mark.parametrize("route", ["direct", "print", "positive"])
 def test_transcription_gradient_matches_finite_differences(torch, recipes, prepare, oracle, route):
     from oracle import fit
 
