@@ -854,8 +854,6 @@ static FjStatus fit_check(FjbRecipe* recipe, const FjbFitParams* params, bool ha
     if ((components != 3 && components != 4) || width < 0 || height < 0)
         return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "unsupported image geometry");
     const fjb::PixelParams& p = recipe->r.params;
-    if (p.method == fjb::kMallett)
-        return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "fitting covers the TC LUT reconstructions");
     if (!fjb::theta_from(*params, th))
         return fail_status(FJ_STATUS_UNSUPPORTED_INPUT, error, "fit parameters must be finite, knees positive");
     return ok_status();

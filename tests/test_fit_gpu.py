@@ -7,18 +7,31 @@ torch.autograd.Function harness over them, against the oracle:
   2e-4 + 3e-4 |rgb| (the render's processor bound);
 * the hand-written adjoint on the differentiation workload (16 seeded 512 x 512 crops,
   one tall image) equals autograd of the FP64 transcription within 1e-3 relative
-  (gradient-vector norm; per parameter 1e-3 |g| + 1e-4 max |g|), both routes;
+  (gradient-vector norm; per parameter 1e-3 |g| + 1e-4 max |g|), on the negative
+  stock's direct and print routes, a positive stock scanned directly (receiver-Langmuir
+  DIR) and the direct recipe with the Mallett 2019 reconstruction;
 * it equals FP64 central differences (h = 1e-6) within the same bound, and the
   central differences (h = 1e-3) of the library's own FP32 forward within 2e-2 of the
   norm (a step of 1e-3 crosses the piecewise-linear curves' knots; the FP64 checks
   measure the function's exact derivative);
 * the autograd.Function's backward is the adjoint, and Adam on it recovers perturbed
   exposure, gamma and print-exposure parameters from a target render;
-* what the adjoint does not cover is rejected before any launch."""
+* invalid parameters are rejected before any launch, and so is spatial DIR on a recipe
+  without DIR couplers."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+
+def _record(prepare, recipes, route):
+    """The host record of a test route; "mallett" is the direct recipe with the Mallett
+    2019 spectral reconstruction in place of the TC LUT."""
+    from film_juicer_b200 import abi
+
+    if route == "mallett":
+        return prepare.HostRecord(recipes["direct"], method=abi.FJ_RAW_MALLETT_2019)
+    return prepare.HostRecord(recipes[route])
 BOUND = 1e-3
 
 
@@ -35,13 +48,13 @@ def _grad_close(got, want, used, bound=BOUND):
         assert abs(g - w) <= bound * abs(w) + 1e-4 * scale, (got, want)
 
 
-@pytest.mark.parametrize("route", ["direct", "print", "positive"])
+@pytest.mark.parametrize("route", ["direct", "print", "positive", "mallett"])
 def test_defaults_and_forward(torch_cuda, recipes, prepare, oracle, route):
     from film_juicer_b200 import fitting, runtime
     from oracle import fit
 
     torch = torch_cuda
-    rec = prepare.HostRecord(recipes[route])
+    rec = _record(prepare, recipes, route)
     dr = runtime.DeviceRecipe(rec)
     tab = fit.tables(rec)
     th0 = fitting.default_theta(dr)
@@ -62,7 +75,7 @@ def test_defaults_and_forward(torch_cuda, recipes, prepare, oracle, route):
     dr.close()
 
 
-@pytest.mark.parametrize("route", ["direct", "print", "positive"])
+@pytest.mark.parametrize("route", ["direct", "print", "positive", "mallett"])
 def test_adjoint_matches_fp64_autograd_on_crop_batch(torch_cuda, recipes, prepare, oracle, route):
     """16 seeded 512 x 512 crops; the cotangent is the gradient of the mean squared
     error against a target rendered at the recipe's own parameters."""
@@ -70,7 +83,7 @@ def test_adjoint_matches_fp64_autograd_on_crop_batch(torch_cuda, recipes, prepar
     from oracle import fit
 
     torch = torch_cuda
-    rec = prepare.HostRecord(recipes[route])
+    rec = _record(prepare, recipes, route)
     dr = runtime.DeviceRecipe(rec)
     tab = fit.tables(rec)
     src = _crops(prepare, 16, 512, 20261207)
@@ -95,13 +108,13 @@ def test_adjoint_matches_fp64_autograd_on_crop_batch(torch_cuda, recipes, prepar
     dr.close()
 
 
-@pytest.mark.parametrize("route", ["direct", "print", "positive"])
+@pytest.mark.parametrize("route", ["direct", "print", "positive", "mallett"])
 def test_adjoint_matches_central_differences(torch_cuda, recipes, prepare, oracle, route):
     from film_juicer_b200 import fitting, runtime
     from oracle import fit
 
     torch = torch_cuda
-    rec = prepare.HostRecord(recipes[route])
+    rec = _record(prepare, recipes, route)
     dr = runtime.DeviceRecipe(rec)
     tab = fit.tables(rec)
     src = np.ascontiguousarray(prepare.synthetic_frame(192, 128, seed=20261208))
@@ -193,9 +206,13 @@ def test_unsupported_cases_are_rejected(torch_cuda, recipes, prepare):
     with pytest.raises(runtime.FjError):
         fitting.vjp(dr, bad, src, g)
     dr.close()
-    rec = prepare.HostRecord(recipes["direct"], method=abi.FJ_RAW_MALLETT_2019)
+    # a recipe without DIR couplers is still a valid fitting problem; spatial DIR on it is not
+    rec = prepare.HostRecord(recipes["direct"])
+    rec.h.dir_couplers.mode = abi.FJ_DIR_INACTIVE
     dr = runtime.DeviceRecipe(rec)
+    planes = [torch.zeros((8, 8), device="cuda") for _ in range(3)]
+    assert torch.all(torch.isfinite(fitting.forward(dr, fitting.default_theta(dr), src)))
     with pytest.raises(runtime.FjError) as e:
-        fitting.forward(dr, fitting.default_theta(dr), src)
+        fitting.dir_source_carrier(dr, fitting.default_theta(dr), planes)
     assert e.value.status.category == abi.FJ_STATUS_UNSUPPORTED_INPUT
     dr.close()

@@ -19,6 +19,16 @@ import numpy as np
 import pytest
 
 
+
+def _record(prepare, recipes, route):
+    """The host record of a test route; "mallett" is the direct recipe with the Mallett
+    2019 spectral reconstruction in place of the TC LUT."""
+    from film_juicer_b200 import abi
+
+    if route == "mallett":
+        return prepare.HostRecord(recipes["direct"], method=abi.FJ_RAW_MALLETT_2019)
+    return prepare.HostRecord(recipes[route])
+
 @pytest.fixture(scope="module")
 def torch():
     import torch as t
@@ -26,11 +36,11 @@ def torch():
     return t
 
 
-@pytest.mark.parametrize("route", ["direct", "print", "positive"])
+@pytest.mark.parametrize("route", ["direct", "print", "positive", "mallett"])
 def test_transcription_matches_oracle_linear_render(torch, recipes, prepare, oracle, route):
     from oracle import fit
 
-    rec = prepare.HostRecord(recipes[route])
+    rec = _record(prepare, recipes, route)
     ch = fit.Chain(torch, rec)
     src = np.ascontiguousarray(prepare.synthetic_frame(96, 64, seed=7))
     e0 = fit.exposure(rec, src)
@@ -53,11 +63,11 @@ def _fd_case(torch, fit, prepare, rec, seed):
     return ch, e0, theta0, w
 
 
-@pytest.mark.parametrize("route", ["direct", "print", "positive"])
+@pytest.mark.parametrize("route", ["direct", "print", "positive", "mallett"])
 def test_transcription_gradient_matches_finite_differences(torch, recipes, prepare, oracle, route):
     from oracle import fit
 
-    rec = prepare.HostRecord(recipes[route])
+    rec = _record(prepare, recipes, route)
     ch, e0, theta0, w = _fd_case(torch, fit, prepare, rec, 11)
     th = theta0.clone().requires_grad_(True)
     (ch(e0, th) * w).sum().backward()
