@@ -208,8 +208,9 @@ class FrameFit:
     camera exposure (computed once by the library: the optics parameters act after it).
 
     host: the frame's FjPreparedHostData (a HostRecord's `.h`), with camera diffusion,
-    scatter/halation and spatial DIR switched by its records; grain, enlarger
-    diffusion, highlight reconstruction and auto exposure are outside this chain and
+    scatter/halation, spatial DIR and auto exposure switched by its records (the
+    metered scale is taken once from the source: it does not depend on the parameters);
+    grain, enlarger diffusion and highlight reconstruction are outside this chain and
     must be off. src: (H, W, 3|4) float32 CUDA source.
 
     With spatial DIR the development subtracts the filtered donor corrections: the
@@ -222,9 +223,8 @@ class FrameFit:
         torch = _torch()
         o = host.optics
         if (host.grain.flags & abi.FJ_GRAIN_ACTIVE) or \
-                (o.flags & (abi.FJ_OPTICS_ENLARGER_DIFFUSION | abi.FJ_OPTICS_HIGHLIGHT_BOOST)) or \
-                (host.film_exposure.flags & abi.FJ_FILM_AUTO_EXPOSURE):
-            raise ValueError("frame fitting covers camera diffusion, scatter/halation and spatial DIR only")
+                (o.flags & (abi.FJ_OPTICS_ENLARGER_DIFFUSION | abi.FJ_OPTICS_HIGHLIGHT_BOOST)):
+            raise ValueError("frame fitting covers camera diffusion, scatter/halation, spatial DIR and auto exposure")
         self.spatial = _copy(host.spatial_dir) if host.spatial_dir.component_count else None
         self._dir_filter = None
         self.recipe, self.stream = recipe, stream
@@ -239,7 +239,20 @@ class FrameFit:
         h, w = src.shape[0], src.shape[1]
         self.shape = (h, w)
         planes = [torch.empty((h, w), dtype=torch.float32, device=src.device) for _ in range(3)]
-        recipe.camera_exposure(src, planes, stream=stream)  # B, G, R
+        self.meter_scale = None
+        if host.film_exposure.flags & abi.FJ_FILM_AUTO_EXPOSURE:
+            # the metered scale is a function of the source alone: metered once, it sits
+            # in the carrier, and the parameters act after it as they do without metering
+            from .runtime import auto_exposure
+
+            self.meter_scale = torch.empty(1, dtype=torch.float32, device=src.device)
+            auto_exposure(recipe, src, host.auto_exposure, self.meter_scale, stream=stream)
+            recipe.set_exposure_scale_device(self.meter_scale)
+        try:
+            recipe.camera_exposure(src, planes, stream=stream)  # B, G, R
+        finally:
+            if self.meter_scale is not None:
+                recipe.set_exposure_scale_device(None)
         self.x0 = [planes[2], planes[1], planes[0]]  # R, G, B
         self._scratch = None
 

@@ -190,3 +190,39 @@ def test_frame_fit_recovers_optics(torch_cuda, recipes, prepare):
     assert losses[-1] <= 1e-4 * losses[0], (losses[0], losses[-1])
     assert float((var.detach() - truth[free]).abs().max()) <= 2e-3, (var, truth)
     dr.close()
+
+
+def test_auto_exposure_frame_meters_once(torch_cuda, recipes, prepare):
+    """With auto exposure on, FrameFit meters the source once (fjb_auto_exposure): its
+    carrier is the unmetered carrier times the metered scale, and the parameters'
+    gradient on it still equals FP64 autograd of the transcription."""
+    from film_juicer_b200 import fitting, frame_records, runtime
+    from oracle import fit
+
+    torch = torch_cuda
+    src = torch.from_numpy(np.ascontiguousarray(prepare.synthetic_frame(W, H, seed=20261216))).cuda()
+    plain = frame_records.FrameRecord(recipes["print"], W, H, recipe_hash=0x2002, diffusion=False, halation=True,
+                                      spatial_dir=False, grain=False, descriptor_width=W * 8)
+    metered = frame_records.FrameRecord(recipes["print"], W, H, recipe_hash=0x2003, diffusion=False, halation=True,
+                                        spatial_dir=False, grain=False, descriptor_width=W * 8, auto_exposure=True)
+    dp, dm = runtime.DeviceRecipe(plain.host), runtime.DeviceRecipe(metered.host)
+    fp, fm = fitting.FrameFit(dp, plain.host.h, src), fitting.FrameFit(dm, metered.host.h, src)
+    scale = float(fm.meter_scale.cpu())
+    assert np.isfinite(scale) and abs(scale - 1.0) > 1e-3
+    for a, b in zip(fm.x0, fp.x0):
+        err = (a.double() - b.double() * scale).abs()
+        assert float((err - 4e-7 * (b.double() * scale).abs()).max()) <= 1e-30
+    tab = fit.tables(metered.host)
+    thp = torch.from_numpy(fit.perturbed_theta(tab))
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    w = 1.0 + 0.25 * torch.randn((3, H, W), device="cuda", generator=gen)
+    g_theta, g_opt = fm.vjp(thp, fm.optics_default(), w)
+    _, _, x3 = fm.carriers(fm.optics_default())
+    ch = fit.Chain(torch, metered.host, device="cuda")
+    th = thp.clone().cuda().requires_grad_(True)
+    (ch(_e0(torch, metered, x3), th) * w.reshape(3, -1).double()).sum().backward()
+    used = fit.used_parameters(tab)
+    got, want = g_theta.numpy(), th.grad.cpu().numpy()
+    assert np.linalg.norm(got[used] - want[used]) <= 1e-3 * np.linalg.norm(want[used]), (got, want)
+    dp.close()
+    dm.close()
