@@ -208,10 +208,11 @@ class FrameFit:
     camera exposure (computed once by the library: the optics parameters act after it).
 
     host: the frame's FjPreparedHostData (a HostRecord's `.h`), with camera diffusion,
-    scatter/halation, spatial DIR and auto exposure switched by its records (the
-    metered scale is taken once from the source: it does not depend on the parameters);
-    grain, enlarger diffusion and highlight reconstruction are outside this chain and
-    must be off. src: (H, W, 3|4) float32 CUDA source.
+    scatter/halation, spatial DIR, auto exposure and highlight reconstruction switched
+    by its records (the metered scale and the reconstructed highlights are taken once
+    from the source: they do not depend on the parameters); grain and enlarger
+    diffusion are outside this chain and must be off. src: (H, W, 3|4) float32 CUDA
+    source.
 
     With spatial DIR the development subtracts the filtered donor corrections: the
     forward is the source stage, the frame's DIR filter and the development; the
@@ -222,9 +223,9 @@ class FrameFit:
     def __init__(self, recipe: DeviceRecipe, host, src, stream=None):
         torch = _torch()
         o = host.optics
-        if (host.grain.flags & abi.FJ_GRAIN_ACTIVE) or \
-                (o.flags & (abi.FJ_OPTICS_ENLARGER_DIFFUSION | abi.FJ_OPTICS_HIGHLIGHT_BOOST)):
-            raise ValueError("frame fitting covers camera diffusion, scatter/halation, spatial DIR and auto exposure")
+        if (host.grain.flags & abi.FJ_GRAIN_ACTIVE) or (o.flags & abi.FJ_OPTICS_ENLARGER_DIFFUSION):
+            raise ValueError("frame fitting covers camera diffusion, scatter/halation, spatial DIR, auto exposure "
+                             "and highlight reconstruction")
         self.spatial = _copy(host.spatial_dir) if host.spatial_dir.component_count else None
         self._dir_filter = None
         self.recipe, self.stream = recipe, stream
@@ -253,6 +254,12 @@ class FrameFit:
         finally:
             if self.meter_scale is not None:
                 recipe.set_exposure_scale_device(None)
+        if o.flags & abi.FJ_OPTICS_HIGHLIGHT_BOOST:
+            # highlight reconstruction acts on the camera exposure before the optics and
+            # depends on the source alone: applied once, it is part of the carrier
+            from .runtime import highlight_boost
+
+            highlight_boost(o.highlight_boost, planes, stream=stream)
         self.x0 = [planes[2], planes[1], planes[0]]  # R, G, B
         self._scratch = None
 

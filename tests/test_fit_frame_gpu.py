@@ -226,3 +226,37 @@ def test_auto_exposure_frame_meters_once(torch_cuda, recipes, prepare):
     assert np.linalg.norm(got[used] - want[used]) <= 1e-3 * np.linalg.norm(want[used]), (got, want)
     dp.close()
     dm.close()
+
+
+def test_highlight_reconstruction_frame(torch_cuda, recipes, prepare):
+    """With highlight reconstruction on, FrameFit's carrier is the camera exposure after
+    the reconstruction (fjb_highlight_boost on the camera exposure, applied once),
+    and the parameters' gradient on the post-optics carrier equals FP64 autograd."""
+    from film_juicer_b200 import descriptors, fitting, frame_records, runtime
+    from oracle import fit
+
+    torch = torch_cuda
+    src = torch.from_numpy(np.ascontiguousarray(prepare.synthetic_frame(W, H, seed=20261217))).cuda()
+    boost = descriptors.highlight_boost_record(protection=0.5, peak_gain=2.0)
+    rec = frame_records.FrameRecord(recipes["print"], W, H, recipe_hash=0x2004, diffusion=True, halation=True,
+                                    spatial_dir=False, grain=False, descriptor_width=W * 8, highlight_boost=boost)
+    dr = runtime.DeviceRecipe(rec.host)
+    ff = fitting.FrameFit(dr, rec.host.h, src)
+    planes = [torch.empty((H, W), device="cuda") for _ in range(3)]
+    dr.camera_exposure(src, planes)
+    assert runtime.highlight_boost(boost, planes) == 1
+    for a, b in zip(ff.x0, (planes[2], planes[1], planes[0])):
+        assert torch.equal(a, b)
+    tab = fit.tables(rec.host)
+    thp = torch.from_numpy(fit.perturbed_theta(tab))
+    gen = torch.Generator(device="cuda").manual_seed(12)
+    w = 1.0 + 0.25 * torch.randn((3, H, W), device="cuda", generator=gen)
+    g_theta, _ = ff.vjp(thp, ff.optics_default(), w)
+    _, _, x3 = ff.carriers(ff.optics_default())
+    ch = fit.Chain(torch, rec.host, device="cuda")
+    th = thp.clone().cuda().requires_grad_(True)
+    (ch(_e0(torch, rec, x3), th) * w.reshape(3, -1).double()).sum().backward()
+    used = fit.used_parameters(tab)
+    got, want = g_theta.numpy(), th.grad.cpu().numpy()
+    assert np.linalg.norm(got[used] - want[used]) <= 1e-3 * np.linalg.norm(want[used]), (got, want)
+    dr.close()
