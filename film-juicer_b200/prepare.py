@@ -307,7 +307,8 @@ def prepare_recipe(resources: str, film: str, paper: str | None = None, *, dir_a
         # the mid-grey balance of the film's reference densities under it (print.rs:435-523).
         with open(os.path.join(resources, "filters", "heat_absorbing", "schott", "KG3.csv")) as fh:
             lamp = print_prep.tungsten_kg3(print_prep.parse_csv_rows(fh.read()))
-        neutral, calibrated = print_prep.neutral_cmy_cc(resources, pp["info"].get("stock", paper), "TH-KG3",
+        lamp_key = print_prep.enlarger_illuminant()  # the host's default lamp control: TH-KG3
+        neutral, calibrated = print_prep.neutral_cmy_cc(resources, pp["info"].get("stock", paper), lamp_key,
                                                         prof["info"].get("stock", film))
         main_cc, preflash_cc = print_prep.filters(neutral)
         main_ill = print_prep.filtered_illuminant(main_cc, lamp)

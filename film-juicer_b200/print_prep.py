@@ -19,7 +19,8 @@ computes them (rust/film-juicer-core/src/print.rs, recipe.rs, illuminant.rs).
   Hermite interpolation, normalised to mean 1 (illuminant.rs:97-128, 282-408);
 * `sample_density`: the reference densities' curve lookup (film/reference.rs:74-98);
 * `neutral_cmy_cc`: the calibrated neutral filtration of a paper / lamp / film
-  triple, else the default (recipe.rs:1193-1215, 1709-1714).
+  triple, else the default (recipe.rs:1193-1215, 1709-1714), and `enlarger_illuminant`
+  the lamp key of the host's lamp control (recipe.rs:1181-1192).
 
 f32 arithmetic runs on NumPy float32 scalars (one rounding per operation, no fused
 multiply-add, as the reference compiles it); erf and the single-precision power are
@@ -49,6 +50,14 @@ DICHROIC_EDGES_NM = (516.0, 500.0, 610.0, 607.0)
 DICHROIC_TRANSITIONS_NM = (12.0, 8.0, 8.0, 8.0)
 DEFAULT_NEUTRAL_CMY_CC = (0.0, 65.0, 55.0)
 ENLARGER_ILLUMINANTS = {0: "D65", 1: "D55", 2: "D50", 4: "TH-KG3-L", 5: "T", 6: "K75P", 7: "EQUAL"}
+DEFAULT_ENLARGER_CHOICE = 3
+
+
+def enlarger_illuminant(choice: int = DEFAULT_ENLARGER_CHOICE) -> str:
+    """The enlarger lamp's key for the host's lamp control (recipe.rs:1181-1192): the
+    listed choices, TH-KG3 (tungsten halogen behind KG3 heat glass) otherwise."""
+    return ENLARGER_ILLUMINANTS.get(int(choice), "TH-KG3")
+
 
 _libm = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
 _libm.erff.argtypes = [ctypes.c_float]

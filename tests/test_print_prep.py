@@ -153,3 +153,9 @@ def test_print_recipe_tables_are_the_reference_products(cases, pp, recipes):
             ref = float(_f(cases["balance_scalars"][i])[2])
             assert abs(rec.scalars["print_normalizer"] - ref) <= 2e-4 * ref
     assert checked >= 4
+
+
+def test_enlarger_lamp_choice(pp):
+    assert pp.enlarger_illuminant() == "TH-KG3"
+    assert pp.enlarger_illuminant(4) == "TH-KG3-L" and pp.enlarger_illuminant(0) == "D65"
+    assert pp.enlarger_illuminant(99) == "TH-KG3"
