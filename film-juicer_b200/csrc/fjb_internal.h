@@ -11,7 +11,7 @@
 namespace fjb {
 
 constexpr int kPixelThreads = 256;
-constexpr int kPixelBlocksPerSm = 4;
+constexpr int kPixelBlocksPerSm = 4; // resident CTAs per SM when the occupancy query fails
 
 enum class PixelStage : int {
     SourceToOutput = 0,   // monolithic frame: source RGB -> encoded output

@@ -1,7 +1,7 @@
 // fjb_pixel_chain.cu -- the fused per-pixel film-process kernel (a1..a13).
 //
 // One persistent launch walks the frame with a grid-stride loop (grid sized to the
-// SM count). Each CTA stages the recipe's density curves into shared memory once;
+// SM count times the variant's resident CTAs per SM). Each CTA stages the recipe's density curves into shared memory once;
 // the print spectral coefficients are kernel parameters (constant bank); the TC LUT,
 // scanner nodes and gamut boundary are 16-byte-vector reads through L1/L2.
 //
@@ -287,17 +287,6 @@ __global__ void __launch_bounds__(kPixelThreads) encode_planes_kernel(const __gr
     }
 }
 
-template <int In, int Out, bool Print, bool SpatialDir>
-static cudaError_t launch_variant(const PixelParams& p, int grid, size_t smem, cudaStream_t stream) {
-    auto* k = pixel_chain_kernel<In, Out, Print, SpatialDir>;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    fjb::count_launch();
-    k<<<grid, kPixelThreads, smem, stream>>>(p);
-    return cudaGetLastError();
-}
 
 // Camera linear exposure (no route correction) into planar B, G, R carrier planes.
 __global__ void __launch_bounds__(kPixelThreads) camera_exposure_kernel(const __grid_constant__ PixelParams p,
@@ -319,15 +308,37 @@ __global__ void __launch_bounds__(kPixelThreads) camera_exposure_kernel(const __
     }
 }
 
-static int persistent_grid(long long total) {
+// Grid of a grid-stride pixel kernel: every CTA the device holds at once (the kernel's
+// own occupancy at kPixelThreads threads and `smem` bytes of shared memory, so kernels
+// with few registers fill the SMs), or one CTA per 256 pixels when that is fewer.
+static int persistent_grid(long long total, const void* kernel, size_t smem) {
     int device = 0;
     cudaGetDevice(&device);
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (sms <= 0) sms = 148;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPixelThreads, smem) != cudaSuccess ||
+        per_sm <= 0) {
+        cudaGetLastError(); // the query's own failure is not the launch's
+        per_sm = kPixelBlocksPerSm;
+    }
     const long long blocksNeeded = (total + kPixelThreads - 1) / kPixelThreads;
-    const long long cap = (long long)sms * kPixelBlocksPerSm;
+    const long long cap = (long long)sms * per_sm;
     return (int)(blocksNeeded < cap ? blocksNeeded : cap);
+}
+
+template <int In, int Out, bool Print, bool SpatialDir>
+static cudaError_t launch_variant(const PixelParams& p, long long total, size_t smem, cudaStream_t stream) {
+    auto* k = pixel_chain_kernel<In, Out, Print, SpatialDir>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    const int grid = persistent_grid(total, reinterpret_cast<const void*>(k), smem);
+    fjb::count_launch();
+    k<<<grid, kPixelThreads, smem, stream>>>(p);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_camera_exposure(const PixelParams& p, float* b, float* g, float* r, long long stride,
@@ -335,7 +346,8 @@ cudaError_t launch_camera_exposure(const PixelParams& p, float* b, float* g, flo
     const long long total = (long long)p.width * (long long)p.height;
     if (total <= 0) return cudaSuccess;
     fjb::count_launch();
-    camera_exposure_kernel<<<persistent_grid(total), kPixelThreads, 0, stream>>>(p, b, g, r, stride);
+    camera_exposure_kernel<<<persistent_grid(total, reinterpret_cast<const void*>(camera_exposure_kernel), 0),
+                             kPixelThreads, 0, stream>>>(p, b, g, r, stride);
     return cudaGetLastError();
 }
 
@@ -348,50 +360,50 @@ cudaError_t launch_pixel_chain(const PixelParams& p, PixelStage stage, cudaStrea
         return launch_print_tensor(p, stage, stream);
     if ((p.curve_blob_floats & 3) != 0) return cudaErrorInvalidValue;
     const size_t smem = (size_t)p.curve_blob_floats * sizeof(float);
-    const int grid = persistent_grid(total);
     const bool print = p.route == kRoutePrint && !p.print_done; // enlarger diffusion: scan the print density
     const bool sdir = p.dir_spatial != 0;
     switch (stage) {
         case PixelStage::SourceToOutput:
-            if (sdir) return print ? launch_variant<kInSource, kOutEncoded, true, true>(p, grid, smem, stream)
-                                   : launch_variant<kInSource, kOutEncoded, false, true>(p, grid, smem, stream);
-            return print ? launch_variant<kInSource, kOutEncoded, true, false>(p, grid, smem, stream)
-                         : launch_variant<kInSource, kOutEncoded, false, false>(p, grid, smem, stream);
+            if (sdir) return print ? launch_variant<kInSource, kOutEncoded, true, true>(p, total, smem, stream)
+                                   : launch_variant<kInSource, kOutEncoded, false, true>(p, total, smem, stream);
+            return print ? launch_variant<kInSource, kOutEncoded, true, false>(p, total, smem, stream)
+                         : launch_variant<kInSource, kOutEncoded, false, false>(p, total, smem, stream);
         case PixelStage::CarrierToOutput:
-            if (sdir) return print ? launch_variant<kInCarrier, kOutEncoded, true, true>(p, grid, smem, stream)
-                                   : launch_variant<kInCarrier, kOutEncoded, false, true>(p, grid, smem, stream);
-            return print ? launch_variant<kInCarrier, kOutEncoded, true, false>(p, grid, smem, stream)
-                         : launch_variant<kInCarrier, kOutEncoded, false, false>(p, grid, smem, stream);
+            if (sdir) return print ? launch_variant<kInCarrier, kOutEncoded, true, true>(p, total, smem, stream)
+                                   : launch_variant<kInCarrier, kOutEncoded, false, true>(p, total, smem, stream);
+            return print ? launch_variant<kInCarrier, kOutEncoded, true, false>(p, total, smem, stream)
+                         : launch_variant<kInCarrier, kOutEncoded, false, false>(p, total, smem, stream);
         case PixelStage::SourceToDensity:
-            return sdir ? launch_variant<kInSource, kOutDensity, false, true>(p, grid, smem, stream)
-                        : launch_variant<kInSource, kOutDensity, false, false>(p, grid, smem, stream);
+            return sdir ? launch_variant<kInSource, kOutDensity, false, true>(p, total, smem, stream)
+                        : launch_variant<kInSource, kOutDensity, false, false>(p, total, smem, stream);
         case PixelStage::CarrierToDensity:
-            return sdir ? launch_variant<kInCarrier, kOutDensity, false, true>(p, grid, smem, stream)
-                        : launch_variant<kInCarrier, kOutDensity, false, false>(p, grid, smem, stream);
+            return sdir ? launch_variant<kInCarrier, kOutDensity, false, true>(p, total, smem, stream)
+                        : launch_variant<kInCarrier, kOutDensity, false, false>(p, total, smem, stream);
         case PixelStage::SourceToDirSource:
-            return launch_variant<kInSource, kOutDirSource, false, false>(p, grid, smem, stream);
+            return launch_variant<kInSource, kOutDirSource, false, false>(p, total, smem, stream);
         case PixelStage::CarrierToDirSource:
-            return launch_variant<kInCarrier, kOutDirSource, false, false>(p, grid, smem, stream);
+            return launch_variant<kInCarrier, kOutDirSource, false, false>(p, total, smem, stream);
         case PixelStage::DensityToLinearRgb:
-            return print ? launch_variant<kInDensity, kOutLinearRgb, true, false>(p, grid, smem, stream)
-                         : launch_variant<kInDensity, kOutLinearRgb, false, false>(p, grid, smem, stream);
+            return print ? launch_variant<kInDensity, kOutLinearRgb, true, false>(p, total, smem, stream)
+                         : launch_variant<kInDensity, kOutLinearRgb, false, false>(p, total, smem, stream);
         case PixelStage::LinearRgbToOutput:
             fjb::count_launch();
-            encode_planes_kernel<<<grid, kPixelThreads, 0, stream>>>(p);
+            encode_planes_kernel<<<persistent_grid(total, reinterpret_cast<const void*>(encode_planes_kernel), 0),
+                                   kPixelThreads, 0, stream>>>(p);
             return cudaGetLastError();
         case PixelStage::DensityToOutput:
-            return print ? launch_variant<kInDensity, kOutEncoded, true, false>(p, grid, smem, stream)
-                         : launch_variant<kInDensity, kOutEncoded, false, false>(p, grid, smem, stream);
+            return print ? launch_variant<kInDensity, kOutEncoded, true, false>(p, total, smem, stream)
+                         : launch_variant<kInDensity, kOutEncoded, false, false>(p, total, smem, stream);
         case PixelStage::DensityToPrintRaw:
-            return launch_variant<kInDensity, kOutPrintRaw, true, false>(p, grid, smem, stream);
+            return launch_variant<kInDensity, kOutPrintRaw, true, false>(p, total, smem, stream);
         case PixelStage::DensityToEnlargerLinear:
-            return launch_variant<kInDensity, kOutEnlargerLinear, true, false>(p, grid, smem, stream);
+            return launch_variant<kInDensity, kOutEnlargerLinear, true, false>(p, total, smem, stream);
         case PixelStage::EnlargerLinearToPrintDensity:
-            return launch_variant<kInDensity, kOutEnlargerDevelop, false, false>(p, grid, smem, stream);
+            return launch_variant<kInDensity, kOutEnlargerDevelop, false, false>(p, total, smem, stream);
         case PixelStage::RawToOutput:
-            return launch_variant<kInPrintRaw, kOutEncoded, false, false>(p, grid, smem, stream);
+            return launch_variant<kInPrintRaw, kOutEncoded, false, false>(p, total, smem, stream);
         case PixelStage::RawToLinearRgb:
-            return launch_variant<kInPrintRaw, kOutLinearRgb, false, false>(p, grid, smem, stream);
+            return launch_variant<kInPrintRaw, kOutLinearRgb, false, false>(p, total, smem, stream);
     }
     return cudaErrorInvalidValue;
 }
