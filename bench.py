@@ -684,14 +684,28 @@ def run_precision(args):
     with runtime.Owner() as owner:
         owner.render(record, src, dst)
     got = dst.cpu().numpy()
+    from film_juicer_b200 import staged as fstaged
+
+    staged = fstaged.render_staged(record, src)
     t0 = time.perf_counter()
-    want, _ = oframe.render_frame(record, recipe, host, threads=os.cpu_count() or 1)
+    ref_stages = {}
+    want, _ = oframe.render_frame(record, recipe, host, threads=os.cpu_count() or 1, stages=ref_stages)
     t_oracle = time.perf_counter() - t0
     stats = color.delta_e_stats(got, want)
+    per_stage = {}
+    for name, planes in staged.items():
+        ref = want if name == "output" else ref_stages[name]
+        if name == "output":
+            planes = [planes[..., c] for c in range(3)]
+            ref = [ref[..., c] for c in range(3)]
+        per_stage[name] = {"max_abs": float(max(np.abs(a - b).max() for a, b in zip(planes, ref))),
+                           "mean_abs": float(np.mean([np.abs(a - b).mean() for a, b in zip(planes, ref)])),
+                           "max_value": float(max(np.abs(b).max() for b in ref))}
     line = {"precision": {"workload": f"{W}x{H} full optical print through fj_cuda_render", "dtype": "f32",
                           "delta_e00_vs_oracle": {k: round(v, 6) for k, v in stats.items()},
                           "max_abs_encoded": float(np.abs(got - want).max()),
                           "mean_abs_encoded": float(np.abs(got - want).mean()),
+                          "stages_vs_oracle": per_stage,
                           "oracle_seconds": round(t_oracle, 1), "oracle_threads": os.cpu_count()}}
     print(json.dumps(line), flush=True)
 

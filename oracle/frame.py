@@ -19,14 +19,22 @@ class _Components:
         self.lambda_px, self.red_weights, self.green_weights, self.blue_weights = lam, w[0], w[1], w[2]
 
 
-def render_frame(frame_record, recipe, src, threads: int = 1, frame_token: int = 0, diffusion_form: str = "direct"):
+def render_frame(frame_record, recipe, src, threads: int = 1, frame_token: int = 0, diffusion_form: str = "direct",
+                 stages: dict | None = None):
     """frame_record: film_juicer_b200.frame_records.FrameRecord; recipe: the
     PreparedRecipe it was built from; src: (H, W, comps) float32. Returns the encoded
     output (H, W, comps) and the error flags. `threads` parallelises the per-pixel
     stages and the FFT (the line stages use the oracle's OpenMP default).
     diffusion_form: "direct" (FP64 direct sum, the parity form) or "fft" (the
     reference's FFT convolution in FP64, same results after float rounding; the CPU
-    baseline's form)."""
+    baseline's form). stages: when a dict, it receives a copy of each stage's planes
+    (camera_exposure, camera_diffusion, scatter_halation: B, G, R carrier;
+    spatial_dir_filtered: Y, M, C; capture_density, grain: C, M, Y density)."""
+
+    def keep(name, planes):
+        if stages is not None:
+            stages[name] = [np.array(q, dtype=np.float32, copy=True) for q in planes]
+
     abi = orc._abi()
     host = frame_record.host
     h = host.h
@@ -34,6 +42,7 @@ def render_frame(frame_record, recipe, src, threads: int = 1, frame_token: int =
     if h.film_exposure.flags & abi.FJ_FILM_AUTO_EXPOSURE:
         scale = orc.auto_exposure(host, h.auto_exposure, src)
     carrier, _ = orc.render(host, src, stage=3, auto_scale=scale, threads=threads)  # B, G, R
+    keep("camera_exposure", carrier)
     flags = h.optics.flags
     if flags & abi.FJ_OPTICS_HIGHLIGHT_BOOST:
         carrier, disp = ooptics.highlight_boost(h.optics.highlight_boost, carrier)
@@ -50,21 +59,26 @@ def render_frame(frame_record, recipe, src, threads: int = 1, frame_token: int =
         else:
             r, g, b = ooptics.diffusion(_Components(lam, w), d.radius_px, d.scatter_fraction, planes)
         carrier = [b, g, r]
+        keep("camera_diffusion", carrier)
     if flags & abi.FJ_OPTICS_SCATTER_HALATION:
         r, g, b = ooptics.scatter_halation(h.optics.scatter_halation, [carrier[2], carrier[1], carrier[0]])
         carrier = [b, g, r]
+        keep("scatter_halation", carrier)
     if h.spatial_dir.component_count > 0:
         filtered, log_raw, _ = odir.spatial_dir(host, h.spatial_dir, carrier=carrier, width=src.shape[1],
                                                height=src.shape[0])
+        keep("spatial_dir_filtered", filtered)
         density, _ = odir.develop_spatial(host, filtered, log_raw)
     else:
         density, _ = orc.render(host, None, stage=5, planes=carrier, threads=threads)
+    keep("capture_density", density)
     if h.grain.flags & abi.FJ_GRAIN_ACTIVE:
         a = recipe.arrays
         layers = [[a["density_layers"][:, l, c] for c in range(3)] for l in range(3)]
         base = [a["density_rgb"][:, c] for c in range(3)]
         noise = frame_record.noise.record if frame_record.noise is not None else None
         density = ograin.visual_grain(h.grain, noise, base, layers, h.capture_polarity == 1, density)
+        keep("grain", density)
     fx = h.effects
     film = bool(fx.flags & abi.FJ_EFFECTS_FILM)
     gate_output = bool(fx.flags & abi.FJ_EFFECTS_GATE_OUTPUT)

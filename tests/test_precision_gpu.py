@@ -1,7 +1,12 @@
 """Output precision of the whole print frame (1920x1080, every spatial stage on, the
 scope table's second configuration) through fj_cuda_render against the oracle's stage
 chain: CIEDE2000 p99 <= 0.5 (the precision target of the path) and, since this build
-computes in FP32 throughout, a much tighter p99 <= 0.05 and max <= 1.0."""
+computes in FP32 throughout, a much tighter p99 <= 0.05 and max <= 1.0. The same frame
+one library call per stage (film_juicer_b200.staged) against the oracle's intermediates:
+each stage's largest absolute difference within its bound (the linear optics stages to
+4e-6 / 1e-5 of the carrier's peak, the DIR corrections to 1e-5, the capture density to
+1e-4; grain's densities can differ by a flipped particle count, so it is bounded by
+its mean difference), and the staged output equal to fj_cuda_render's within 1e-5."""
 import numpy as np
 import pytest
 
@@ -9,7 +14,7 @@ pytestmark = pytest.mark.gpu
 
 
 def test_print_frame_delta_e(torch_cuda, recipes, prepare):
-    from film_juicer_b200 import frame_records, runtime
+    from film_juicer_b200 import frame_records, runtime, staged
     from oracle import color
     from oracle import frame as oframe
     import os
@@ -22,7 +27,20 @@ def test_print_frame_delta_e(torch_cuda, recipes, prepare):
     with runtime.Owner() as owner:
         owner.render(rec, s, d)
     got = d.cpu().numpy()
-    want, _ = oframe.render_frame(rec, recipes["print"], src, threads=os.cpu_count() or 1)
+    ref_stages = {}
+    want, _ = oframe.render_frame(rec, recipes["print"], src, threads=os.cpu_count() or 1, stages=ref_stages)
     st = color.delta_e_stats(got, want)
     assert st["p99"] <= 0.5, st
     assert st["p99"] <= 0.05 and st["max"] <= 1.0, st
+
+    mine = staged.render_staged(rec, s)
+    assert set(ref_stages) <= set(mine)
+    peak = float(max(np.abs(q).max() for q in ref_stages["camera_exposure"]))
+    bounds = {"camera_exposure": 4e-6 * peak, "camera_diffusion": 4e-6 * peak, "scatter_halation": 1e-5 * peak,
+              "spatial_dir_filtered": 1e-5, "capture_density": 1e-4}
+    for name, bound in bounds.items():
+        worst = max(float(np.abs(a - b).max()) for a, b in zip(mine[name], ref_stages[name]))
+        assert worst <= bound, (name, worst, bound)
+    mean = float(np.mean([np.abs(a - b).mean() for a, b in zip(mine["grain"], ref_stages["grain"])]))
+    assert mean <= 1e-5, mean
+    assert float(np.abs(mine["output"] - got).max()) <= 1e-5

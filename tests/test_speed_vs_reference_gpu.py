@@ -1,7 +1,7 @@
 """Device time of each stage against the reference's own CUDA kernels on the same 4K
 frame (the reference compiled for sm_100a into the test harness; its launchers timed
 with CUDA events after every upload). Guards against regressions: no stage may be
-more than 1.5x slower than the reference's. Set FJB_SPEED_REPORT to a path to keep
+slower than the reference's. Set FJB_SPEED_REPORT to a path to keep
 the table as JSON."""
 import ctypes as C
 import json
@@ -122,7 +122,7 @@ def test_stage_times_against_reference_cuda(torch_cuda, recipes, prepare, oracle
         with open(path, "w") as fh:
             json.dump(table, fh, indent=1)
     for k, v in table.items():
-        assert v["ours_ms"] <= 1.5 * v["reference_ms"], (k, v)
+        assert v["ours_ms"] <= v["reference_ms"], (k, v)
 
 
 def test_camera_diffusion_against_reference_cufft(torch_cuda, recipes, prepare):
